@@ -1,0 +1,297 @@
+/*
+ * dmrgb200 — B200 (sm_100a) implementation of the QCMaquis DMRG hot path
+ * behind a C ABI: the symmetry-blocked effective-Hamiltonian product H·psi and
+ * the left/right boundary updates.
+ *
+ * Conventions
+ *  - All numeric data is FP64, column-major, as in the reference's
+ *    alps::numeric::matrix (dmrg/framework/alps/matrix/matrix.ipp:122).
+ *  - Device pointers are plain CUDA device addresses; host pointers are plain
+ *    host addresses.  No torch or C++ types cross this interface.
+ *  - Every call returns dmrgb200_status; a call never exits the process.
+ *    dmrgb200_last_error() returns a thread-local message for the last failure.
+ *  - Calls are stream-ordered on the stream given (NULL = legacy default stream)
+ *    and thread-compatible: one context per host thread.
+ *
+ * Two ways to obtain a plan:
+ *  (1) dmrgb200_plan_create(): the caller flattens its own schedule
+ *      (the reference's ScheduleNew / MPSBlock / Cohort) into
+ *      dmrgb200_plan_desc.  This is the drop-in seam for the reference's
+ *      C++ host code; see INTEGRATION.md.
+ *  (2) dmrgb200_*_plan_build(): the library's own schedule builder (a C++
+ *      restatement of the reference's create_contraction_schedule and the
+ *      lshtm_* / rshtm_* builders) from index, MPO and boundary descriptions.
+ */
+#ifndef DMRGB200_H
+#define DMRGB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    DMRGB200_OK = 0,
+    DMRGB200_INVALID_ARGUMENT = 1,
+    DMRGB200_INVALID_PLAN = 2,
+    DMRGB200_OUT_OF_MEMORY = 3,
+    DMRGB200_DEVICE_ERROR = 4,
+    DMRGB200_TIMEOUT = 5,
+    DMRGB200_NUMERIC = 6,
+    DMRGB200_NOT_SUPPORTED = 7
+} dmrgb200_status;
+
+typedef enum {
+    DMRGB200_PREC_FP64 = 0,          /* native FP64 */
+    DMRGB200_PREC_FP64_EMULATED = 1  /* split-precision FP64 emulation on the tensor cores */
+} dmrgb200_precision;
+
+typedef enum {
+    DMRGB200_PLAN_HPSI = 0,        /* H·psi (super_hamil_mv) */
+    DMRGB200_PLAN_LEFT_STEP = 1,   /* overlap_mpo_left_step */
+    DMRGB200_PLAN_RIGHT_STEP = 2   /* overlap_mpo_right_step */
+} dmrgb200_plan_kind;
+
+typedef enum { DMRGB200_U1 = 1, DMRGB200_TWOU1 = 2, DMRGB200_SU2U1 = 3 } dmrgb200_symmetry;
+
+typedef struct dmrgb200_context_s* dmrgb200_context_t;
+typedef struct dmrgb200_plan_s* dmrgb200_plan_t;
+typedef struct dmrgb200_mpo_s* dmrgb200_mpo_t;
+
+const char* dmrgb200_status_string(dmrgb200_status s);
+const char* dmrgb200_last_error(void);
+int dmrgb200_abi_version(void);
+
+/* ---- context ------------------------------------------------------------ */
+/* Replaces accelerator::gpu / accelerator::device setup
+ * (dmrg/framework/dmrg/solver/accelerator.h:36-135, accelerator.cpp:52-328). */
+dmrgb200_status dmrgb200_context_create(int device, dmrgb200_context_t* out);
+dmrgb200_status dmrgb200_context_destroy(dmrgb200_context_t ctx);
+
+/* ---- flat plan description (the drop-in seam) ---------------------------- */
+/* A flattened ScheduleNew (dmrg/framework/dmrg/solver/tasks.h:287-348).
+ * Index arrays are host pointers; the library copies what it needs.
+ *
+ * Blocks ("in" = the right-paired input tensor psi / ket; "out" = the output
+ * vector for H·psi, the bra tensor for boundary steps):
+ *   element (r, c) of block b lives at base + off[b] + r + c*rows[b].
+ * T tasks (MPSBlock::t_schedule, tasks.h:234-239): task t combines a column
+ *   slice of in-block t_lb[t] (first column t_col[t]) with boundary cohort
+ *   t_ci[t] (storage cohort ci_eff) that holds t_nb[t] blocks of logical size
+ *   t_brows[t] x t_bcols[t] (stored transposed when t_trans[t]).
+ *   H·psi / right step (MPSBlock::create_T, tasks.cpp:650-705):
+ *     T_b = in[:, t_col + (0..t_brows)] * B_b            (rows x t_bcols)
+ *   left step (MPSBlock::create_T_left, tasks.cpp:545-601):
+ *     T_b = B_b * in[:, t_col + (0..t_width)] restricted to t_bcols rows
+ *                                                        (t_brows x t_width)
+ * Cohorts (Cohort, tasks.h:50-190): c_lb / c_rb / c_ls / c_rs as in the
+ *   reference (for H·psi: input block, output block, their row counts),
+ *   c_ci / c_trans the other boundary's storage cohort (H·psi only),
+ *   c_nsrows S row blocks, c_stripe S columns, units [c_unit[c], c_unit[c+1]).
+ *   For step plans c_out_ci is the new boundary's cohort index.
+ * Units (SUnit): u_offset, u_ms, lines [u_line[u], u_line[u+1]).
+ * Lines (one per b2s entry): l_b1 (S row block), terms [l_term[l], l_term[l+1]).
+ * Terms: alpha, T task index (global), boundary column (tidx pair).
+ * Task groups (one MPSBlock each): T tasks [g_t[g], g_t[g+1]) and cohorts
+ * [g_c[g], g_c[g+1]); a cohort's terms reference T tasks of its own group. */
+typedef struct {
+    dmrgb200_plan_kind kind;
+    uint32_t n_groups;
+    const uint32_t* g_t; /* n_groups + 1 */
+    const uint32_t* g_c; /* n_groups + 1 */
+    uint32_t n_in_blocks;
+    const uint32_t* in_rows;
+    const uint32_t* in_cols;
+    const uint64_t* in_off;
+    uint64_t in_size;
+    uint32_t n_out_blocks;
+    const uint32_t* out_rows;
+    const uint32_t* out_cols;
+    const uint64_t* out_off;
+    uint64_t out_size;
+
+    uint32_t n_t;
+    const uint32_t* t_lb;
+    const uint32_t* t_col;
+    const uint32_t* t_ci;
+    const uint8_t* t_trans;
+    const uint32_t* t_nb;
+    const uint32_t* t_brows;
+    const uint32_t* t_bcols;
+    const uint32_t* t_width; /* left step only (may be NULL otherwise) */
+
+    uint32_t n_cohorts;
+    const uint32_t* c_lb;
+    const uint32_t* c_rb;
+    const uint32_t* c_ls;
+    const uint32_t* c_rs;
+    const uint32_t* c_ci;
+    const uint8_t* c_trans;
+    const uint32_t* c_nsrows;
+    const uint32_t* c_stripe;
+    const uint32_t* c_out_ci;
+    const uint32_t* c_unit; /* n_cohorts + 1 */
+
+    uint32_t n_units;
+    const uint32_t* u_offset;
+    const uint32_t* u_ms;
+    const uint32_t* u_line; /* n_units + 1 */
+
+    uint32_t n_lines;
+    const uint32_t* l_b1;
+    const uint32_t* l_term; /* n_lines + 1 */
+
+    uint32_t n_terms;
+    const double* term_alpha;
+    const uint32_t* term_t;
+    const uint32_t* term_col;
+} dmrgb200_plan_desc;
+
+/* Boundary cohort storage bound to a plan: n_cohorts device pointers, one per
+ * cohort index ci (NULL for Hermitian-complement cohorts without storage);
+ * replaces BoundaryView (dmrg/framework/dmrg/solver/solver.h:38-43). */
+typedef struct {
+    uint32_t n_cohorts;
+    const double* const* cohort_ptr; /* host array of device pointers */
+} dmrgb200_boundary_view;
+
+/* Build an executable plan from a flattened schedule.  For H·psi, `left` is
+ * the left boundary L and `other` the right boundary R (both stay resident and
+ * must outlive the plan).  For a left step `left` is the input boundary; for a
+ * right step `other` is.  Replaces ScheduleNew::stage_gpu (tasks.cpp:918-977). */
+dmrgb200_status dmrgb200_plan_create(dmrgb200_context_t ctx, const dmrgb200_plan_desc* desc,
+                                     const dmrgb200_boundary_view* left, const dmrgb200_boundary_view* other,
+                                     dmrgb200_plan_t* out);
+dmrgb200_status dmrgb200_plan_destroy(dmrgb200_plan_t plan);
+
+/* Algorithmic FP64 flop count of one execution, the reference's formula
+ * (Cohort::n_flops tasks.cpp:388-398 + MPSBlock::n_flops :777-796). */
+dmrgb200_status dmrgb200_plan_flops(dmrgb200_plan_t plan, uint64_t* flops);
+/* Device scratch (T and S intermediates) the plan holds, in bytes. */
+dmrgb200_status dmrgb200_plan_scratch_bytes(dmrgb200_plan_t plan, uint64_t* bytes);
+
+/* ---- H·psi -------------------------------------------------------------- */
+/* y = H_eff x for a DMRGB200_PLAN_HPSI plan.  x and y are device vectors laid
+ * out as the plan's in/out blocks (DavidsonVector layout,
+ * davidson_vector.cpp:87-152); y's block elements are overwritten, its padding
+ * is left untouched.  Replaces super_hamil_mv (super_hamil_mv.hpp:100-155) and
+ * ietl::mult (ietl_interface_dv.h:112-118). */
+dmrgb200_status dmrgb200_hpsi(dmrgb200_plan_t plan, const double* x, double* y, dmrgb200_precision prec,
+                              void* cuda_stream);
+
+/* ---- boundary steps on a flattened plan --------------------------------- */
+/* Execute a LEFT_STEP / RIGHT_STEP plan.  ket: right-paired device tensor
+ * (plan in-blocks); bra: left-paired (left step) or right-paired (right step)
+ * device tensor (plan out-blocks); out: device pointers of the new boundary's
+ * cohorts (indexed by c_out_ci); every stored element of those cohorts is
+ * written.
+ * Replaces the GPU branches of overlap_mpo_left_step / overlap_mpo_right_step
+ * (move_boundary.hpp:215-259, :342-384). */
+dmrgb200_status dmrgb200_step_execute(dmrgb200_plan_t plan, const double* ket, const double* bra,
+                                      const dmrgb200_boundary_view* out, void* cuda_stream);
+
+/* ---- library-side schedule builder (host only) -------------------------- */
+/* Index description: n sectors, charges[2*i+0..1] (U1 uses component 0),
+ * sizes[i]. */
+typedef struct {
+    uint32_t n;
+    const int32_t* charges;
+    const uint32_t* sizes;
+} dmrgb200_index_desc;
+
+/* MPO tensor description (MPOTensor, dmrg/framework/dmrg/mp_tensors/mpotensor.h:45-135).
+ * Terms (b1, b2, op, scale) must be sorted by (b1, b2); several terms may share
+ * (b1, b2).  Operators: op_block[o]..op_block[o+1] index blocks; block k has
+ * input charge blk_in[2k..], output charge blk_out[2k..] and entries
+ * blk_entry[k]..blk_entry[k+1] (row, col, row spin, col spin, coeff) in
+ * row-major order (SparseOperator, block_matrix/sparse_operator.h:35-235).
+ * Spins and Hermitian data may be NULL (no SU2, no Hermitian partners). */
+typedef struct {
+    dmrgb200_symmetry symm;
+    uint32_t row_dim, col_dim;
+    const int32_t* left_spin;
+    const int32_t* right_spin;
+    const uint32_t* left_herm;   /* partner index or UINT32_MAX */
+    const int32_t* left_phase;
+    const uint32_t* right_herm;
+    const int32_t* right_phase;
+    uint32_t n_terms;
+    const uint32_t* term_b1;
+    const uint32_t* term_b2;
+    const uint32_t* term_op;
+    const double* term_scale;
+    uint32_t n_ops;
+    const int32_t* op_spin;
+    const uint32_t* op_block; /* n_ops + 1 */
+    const int32_t* blk_in;
+    const int32_t* blk_out;
+    const uint32_t* blk_entry; /* n_blocks + 1 */
+    const uint32_t* e_row;
+    const uint32_t* e_col;
+    const int32_t* e_row_spin;
+    const int32_t* e_col_spin;
+    const double* e_coeff;
+} dmrgb200_mpo_desc;
+
+typedef struct dmrgb200_bindex_s* dmrgb200_bindex_t;     /* boundary index */
+typedef struct dmrgb200_schedule_s* dmrgb200_schedule_t; /* host-side flat plan */
+
+dmrgb200_status dmrgb200_mpo_create(const dmrgb200_mpo_desc* desc, dmrgb200_mpo_t* out);
+dmrgb200_status dmrgb200_mpo_destroy(dmrgb200_mpo_t mpo);
+
+/* Boundary index (BoundaryIndex, mp_tensors/boundary.h:76-234) with the
+ * library's storage layout: every cohort with storage occupies
+ * cohort_size doubles at a 32-double aligned storage offset of one buffer of
+ * n_elements doubles.  The caller owns the buffer (host or device).
+ * Edge index: the reference's Boundary(ud, ld, ad) (boundary.h:257-283), one
+ * diagonal cohort per sector with aux_dim blocks; its values are all ones. */
+dmrgb200_status dmrgb200_bindex_create_edge(dmrgb200_symmetry symm, const dmrgb200_index_desc* index,
+                                            uint32_t aux_dim, dmrgb200_bindex_t* out);
+dmrgb200_status dmrgb200_bindex_destroy(dmrgb200_bindex_t b);
+dmrgb200_status dmrgb200_bindex_info(dmrgb200_bindex_t b, uint32_t* n_cohorts, uint32_t* aux_dim,
+                                     uint64_t* n_elements);
+/* Per cohort ci: bra block, ket block, tr flag, storage offset (UINT64_MAX
+ * without storage), left/right size, n_blocks; per (ci, b): offset (-1 absent),
+ * conjugate scale, transposed flag.  Any output pointer may be NULL. */
+dmrgb200_status dmrgb200_bindex_describe(dmrgb200_bindex_t b, uint32_t* lb, uint32_t* rb, uint8_t* tr,
+                                         uint64_t* storage_off, uint32_t* lsize, uint32_t* rsize,
+                                         uint32_t* nblocks, int64_t* offsets, double* conj_scales,
+                                         uint8_t* transposes);
+
+/* H·psi schedule (create_contraction_schedule, site_hamil_schedule.hpp:40-93)
+ * for a right-paired psi with the given physical, left and right indices. */
+dmrgb200_status dmrgb200_schedule_hpsi(const dmrgb200_index_desc* phys, const dmrgb200_index_desc* left_i,
+                                       const dmrgb200_index_desc* right_i, dmrgb200_mpo_t mpo,
+                                       dmrgb200_bindex_t L, dmrgb200_bindex_t R, dmrgb200_schedule_t* out);
+/* Left-step schedule (overlap_mpo_left_step, move_boundary.hpp:147-279) for a
+ * site tensor with bra = ket indices; returns the new boundary index. */
+dmrgb200_status dmrgb200_schedule_left_step(const dmrgb200_index_desc* phys, const dmrgb200_index_desc* left_i,
+                                            const dmrgb200_index_desc* right_i, dmrgb200_mpo_t mpo,
+                                            dmrgb200_bindex_t L, int symmetric, dmrgb200_schedule_t* out,
+                                            dmrgb200_bindex_t* new_index);
+/* Right-step schedule (overlap_mpo_right_step, move_boundary.hpp:281-404). */
+dmrgb200_status dmrgb200_schedule_right_step(const dmrgb200_index_desc* phys, const dmrgb200_index_desc* left_i,
+                                             const dmrgb200_index_desc* right_i, dmrgb200_mpo_t mpo,
+                                             dmrgb200_bindex_t R, int symmetric, dmrgb200_schedule_t* out,
+                                             dmrgb200_bindex_t* new_index);
+/* Flat description of a schedule (arrays owned by the schedule). */
+dmrgb200_status dmrgb200_schedule_export(dmrgb200_schedule_t s, dmrgb200_plan_desc* desc);
+dmrgb200_status dmrgb200_schedule_flops(dmrgb200_schedule_t s, uint64_t* flops);
+dmrgb200_status dmrgb200_schedule_destroy(dmrgb200_schedule_t s);
+
+/* Block layout of an MPS tensor: right-paired (left_paired = 0: one block per
+ * left sector, rows = left size, cols = sum over sigma of d_sigma * right size)
+ * or left-paired (one block per right sector).  Offsets are 128-element padded
+ * (davidson_vector.cpp:96-97).  Arrays have room for the number of blocks
+ * (left_i->n or right_i->n); *n_blocks receives the count and *total the size. */
+dmrgb200_status dmrgb200_tensor_layout(const dmrgb200_index_desc* phys, const dmrgb200_index_desc* left_i,
+                                       const dmrgb200_index_desc* right_i, int left_paired, uint32_t* n_blocks,
+                                       uint32_t* rows, uint32_t* cols, uint64_t* offsets, uint64_t* total);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DMRGB200_H */

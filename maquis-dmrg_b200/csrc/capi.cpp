@@ -1,0 +1,599 @@
+// C ABI of libdmrgb200 (declarations in include/dmrgb200.h).
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <exception>
+#include <limits>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/dmrgb200.h"
+#include "device.hpp"
+#include "plan.hpp"
+#include "schedule.hpp"
+
+using namespace dmrgb200;
+
+struct dmrgb200_context_s {
+    int device = 0;
+};
+
+struct dmrgb200_mpo_s {
+    MPOTensor mpo;
+    Symm symm = Symm::U1;
+};
+
+struct dmrgb200_bindex_s {
+    BoundaryIndex idx;
+    std::vector<uint64_t> coh_off;  // storage offset per cohort, UINT64_MAX without storage
+    uint64_t n_elems = 0;
+
+    // 32-double aligned storage of every cohort that owns data
+    void layout() {
+        coh_off.assign(idx.n_cohorts(), std::numeric_limits<uint64_t>::max());
+        n_elems = 0;
+        for (unsigned ci = 0; ci < idx.n_cohorts(); ++ci) {
+            uint64_t sz = idx.cohort_size(ci);
+            if (!sz) continue;
+            coh_off[ci] = n_elems;
+            n_elems += round_up(sz, 32);
+        }
+    }
+};
+
+struct dmrgb200_schedule_s {
+    FlatPlan flat;
+};
+
+struct dmrgb200_plan_s {
+    FlatPlan flat;
+    DeviceProgram prog;
+    bool compiled = false;
+    double* T = nullptr;
+    double* S = nullptr;
+    std::vector<uint64_t> stage1_bnd, stage3_bnd;
+    int device = 0;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+dmrgb200_status fail(dmrgb200_status s, std::string const& msg) {
+    g_last_error = msg;
+    return s;
+}
+
+dmrgb200_status cuda_fail(cudaError_t e, const char* where) {
+    return fail(e == cudaErrorMemoryAllocation ? DMRGB200_OUT_OF_MEMORY : DMRGB200_DEVICE_ERROR,
+                std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define DMRGB200_TRY try {
+#define DMRGB200_CATCH                                                              \
+    }                                                                               \
+    catch (std::bad_alloc const&) {                                                 \
+        return fail(DMRGB200_OUT_OF_MEMORY, "host allocation failed");              \
+    }                                                                               \
+    catch (std::exception const& ex) {                                              \
+        return fail(DMRGB200_INVALID_ARGUMENT, ex.what());                          \
+    }
+
+Symm to_symm(dmrgb200_symmetry s) {
+    switch (s) {
+        case DMRGB200_U1: return Symm::U1;
+        case DMRGB200_TWOU1: return Symm::TwoU1;
+        case DMRGB200_SU2U1: return Symm::SU2U1;
+    }
+    throw std::runtime_error("unknown symmetry");
+}
+
+Index to_index(const dmrgb200_index_desc* d) {
+    if (!d) throw std::runtime_error("null index description");
+    Index ix;
+    for (uint32_t i = 0; i < d->n; ++i) {
+        Charge c(d->charges[2 * i], d->charges[2 * i + 1]);
+        if (ix.position(c) != ix.size()) throw std::runtime_error("duplicate charge in index");
+        ix.push(c, d->sizes[i]);
+    }
+    return ix;
+}
+
+template <class T>
+std::vector<T> vec(const T* p, size_t n) {
+    if (n && !p) throw std::runtime_error("null array in plan description");
+    return std::vector<T>(p, p + n);
+}
+
+dmrgb200_status alloc_scratch(dmrgb200_plan_s* p) {
+    cudaError_t e;
+    if (p->prog.t_elems && (e = cudaMalloc(&p->T, p->prog.t_elems * sizeof(double))) != cudaSuccess)
+        return cuda_fail(e, "T scratch allocation");
+    if (p->prog.s_elems && (e = cudaMalloc(&p->S, p->prog.s_elems * sizeof(double))) != cudaSuccess)
+        return cuda_fail(e, "S scratch allocation");
+    return DMRGB200_OK;
+}
+
+std::vector<uint64_t> view_ptrs(const dmrgb200_boundary_view* v) {
+    if (!v) return {};
+    if (v->n_cohorts && !v->cohort_ptr) throw std::runtime_error("boundary view without cohort pointers");
+    std::vector<uint64_t> p(v->n_cohorts);
+    for (uint32_t i = 0; i < v->n_cohorts; ++i) p[i] = reinterpret_cast<uint64_t>(v->cohort_ptr[i]);
+    return p;
+}
+
+std::string check_bound(FlatPlan const& f, std::vector<uint64_t> const& s1, std::vector<uint64_t> const& s3) {
+    for (uint32_t t = 0; t < f.n_t(); ++t)
+        if (f.t_ci[t] >= s1.size() || !s1[f.t_ci[t]]) return "T task reads a boundary cohort without storage";
+    if (f.kind == KIND_HPSI)
+        for (uint32_t c = 0; c < f.n_cohorts(); ++c)
+            if (f.c_ci[c] >= s3.size() || !s3[f.c_ci[c]]) return "cohort reads a left cohort without storage";
+    return std::string();
+}
+
+dmrgb200_status finish_plan(std::unique_ptr<dmrgb200_plan_s>& p, dmrgb200_plan_t* out) {
+    std::string err = p->flat.validate();
+    if (!err.empty()) return fail(DMRGB200_INVALID_PLAN, err);
+    err = check_bound(p->flat, p->stage1_bnd, p->stage3_bnd);
+    if (!err.empty()) return fail(DMRGB200_INVALID_PLAN, err);
+    cudaGetDevice(&p->device);
+    if (p->flat.kind == KIND_HPSI) {
+        compile_program(p->flat, p->stage3_bnd, p->stage1_bnd, {}, p->prog);
+        cudaError_t e = upload_program(p->prog);
+        if (e != cudaSuccess) {
+            free_program(p->prog);
+            return cuda_fail(e, "plan upload");
+        }
+        p->compiled = true;
+        dmrgb200_status s = alloc_scratch(p.get());
+        if (s != DMRGB200_OK) {
+            free_program(p->prog);
+            cudaFree(p->T);
+            cudaFree(p->S);
+            return s;
+        }
+    }
+    *out = p.release();
+    return DMRGB200_OK;
+}
+
+// Execute a step plan whose output cohort pointers are `outp`; scratch and the
+// lowered program live only for this call.
+dmrgb200_status run_step(dmrgb200_plan_s* p, const double* ket, const double* bra, std::vector<uint64_t> const& outp,
+                         cudaStream_t stream) {
+    for (uint32_t c = 0; c < p->flat.n_cohorts(); ++c)
+        if (p->flat.c_out_ci[c] >= outp.size() || !outp[p->flat.c_out_ci[c]])
+            return fail(DMRGB200_INVALID_ARGUMENT, "output boundary view misses a cohort");
+    DeviceProgram prog;
+    compile_program(p->flat, {}, p->stage1_bnd, outp, prog);
+    cudaError_t e = upload_program(prog);
+    if (e != cudaSuccess) {
+        free_program(prog);
+        return cuda_fail(e, "step plan upload");
+    }
+    double *T = nullptr, *S = nullptr;
+    if (prog.t_elems && (e = cudaMallocAsync(&T, prog.t_elems * sizeof(double), stream)) != cudaSuccess) {
+        free_program(prog);
+        return cuda_fail(e, "step T scratch");
+    }
+    if (prog.s_elems && (e = cudaMallocAsync(&S, prog.s_elems * sizeof(double), stream)) != cudaSuccess) {
+        cudaFreeAsync(T, stream);
+        free_program(prog);
+        return cuda_fail(e, "step S scratch");
+    }
+    e = run_program(prog, reinterpret_cast<uint64_t>(ket), reinterpret_cast<uint64_t>(bra), T, S, stream);
+    cudaFreeAsync(T, stream);
+    cudaFreeAsync(S, stream);
+    cudaError_t e2 = cudaStreamSynchronize(stream);
+    free_program(prog);
+    if (e != cudaSuccess) return cuda_fail(e, "step launch");
+    if (e2 != cudaSuccess) return cuda_fail(e2, "step execution");
+    return DMRGB200_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* dmrgb200_status_string(dmrgb200_status s) {
+    switch (s) {
+        case DMRGB200_OK: return "ok";
+        case DMRGB200_INVALID_ARGUMENT: return "invalid argument";
+        case DMRGB200_INVALID_PLAN: return "invalid plan";
+        case DMRGB200_OUT_OF_MEMORY: return "out of memory";
+        case DMRGB200_DEVICE_ERROR: return "device error";
+        case DMRGB200_TIMEOUT: return "timeout";
+        case DMRGB200_NUMERIC: return "numeric error";
+        case DMRGB200_NOT_SUPPORTED: return "not supported";
+    }
+    return "unknown status";
+}
+
+const char* dmrgb200_last_error(void) { return g_last_error.c_str(); }
+
+int dmrgb200_abi_version(void) { return 1; }
+
+dmrgb200_status dmrgb200_context_create(int device, dmrgb200_context_t* out) {
+    if (!out) return fail(DMRGB200_INVALID_ARGUMENT, "null output");
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    auto* c = new dmrgb200_context_s;
+    c->device = device;
+    *out = c;
+    return DMRGB200_OK;
+}
+
+dmrgb200_status dmrgb200_context_destroy(dmrgb200_context_t ctx) {
+    delete ctx;
+    return DMRGB200_OK;
+}
+
+dmrgb200_status dmrgb200_plan_create(dmrgb200_context_t ctx, const dmrgb200_plan_desc* d,
+                                     const dmrgb200_boundary_view* left, const dmrgb200_boundary_view* other,
+                                     dmrgb200_plan_t* out) {
+    DMRGB200_TRY
+    if (!ctx || !d || !out) return fail(DMRGB200_INVALID_ARGUMENT, "null argument");
+    auto p = std::make_unique<dmrgb200_plan_s>();
+    FlatPlan& f = p->flat;
+    f.kind = d->kind;
+    f.g_t = vec(d->g_t, size_t(d->n_groups) + 1);
+    f.g_c = vec(d->g_c, size_t(d->n_groups) + 1);
+    f.in_rows = vec(d->in_rows, d->n_in_blocks);
+    f.in_cols = vec(d->in_cols, d->n_in_blocks);
+    f.in_off = vec(d->in_off, d->n_in_blocks);
+    f.in_size = d->in_size;
+    f.out_rows = vec(d->out_rows, d->n_out_blocks);
+    f.out_cols = vec(d->out_cols, d->n_out_blocks);
+    f.out_off = vec(d->out_off, d->n_out_blocks);
+    f.out_size = d->out_size;
+    f.t_lb = vec(d->t_lb, d->n_t);
+    f.t_col = vec(d->t_col, d->n_t);
+    f.t_ci = vec(d->t_ci, d->n_t);
+    f.t_trans = vec(d->t_trans, d->n_t);
+    f.t_nb = vec(d->t_nb, d->n_t);
+    f.t_brows = vec(d->t_brows, d->n_t);
+    f.t_bcols = vec(d->t_bcols, d->n_t);
+    if (d->kind == DMRGB200_PLAN_LEFT_STEP) f.t_width = vec(d->t_width, d->n_t);
+    f.c_lb = vec(d->c_lb, d->n_cohorts);
+    f.c_rb = vec(d->c_rb, d->n_cohorts);
+    f.c_ls = vec(d->c_ls, d->n_cohorts);
+    f.c_rs = vec(d->c_rs, d->n_cohorts);
+    f.c_nsrows = vec(d->c_nsrows, d->n_cohorts);
+    f.c_stripe = vec(d->c_stripe, d->n_cohorts);
+    f.c_unit = vec(d->c_unit, size_t(d->n_cohorts) + 1);
+    if (d->kind == DMRGB200_PLAN_HPSI) {
+        f.c_ci = vec(d->c_ci, d->n_cohorts);
+        f.c_trans = vec(d->c_trans, d->n_cohorts);
+        f.c_out_ci.assign(d->n_cohorts, 0);
+    } else {
+        f.c_ci.assign(d->n_cohorts, 0);
+        f.c_trans.assign(d->n_cohorts, 0);
+        f.c_out_ci = vec(d->c_out_ci, d->n_cohorts);
+    }
+    f.u_offset = vec(d->u_offset, d->n_units);
+    f.u_ms = vec(d->u_ms, d->n_units);
+    f.u_line = vec(d->u_line, size_t(d->n_units) + 1);
+    f.l_b1 = vec(d->l_b1, d->n_lines);
+    f.l_term = vec(d->l_term, size_t(d->n_lines) + 1);
+    f.term_alpha = vec(d->term_alpha, d->n_terms);
+    f.term_t = vec(d->term_t, d->n_terms);
+    f.term_col = vec(d->term_col, d->n_terms);
+    if (d->kind == DMRGB200_PLAN_HPSI) {
+        p->stage3_bnd = view_ptrs(left);
+        p->stage1_bnd = view_ptrs(other);
+    } else if (d->kind == DMRGB200_PLAN_LEFT_STEP) {
+        p->stage1_bnd = view_ptrs(left);
+    } else {
+        p->stage1_bnd = view_ptrs(other);
+    }
+    return finish_plan(p, out);
+    DMRGB200_CATCH
+}
+
+dmrgb200_status dmrgb200_plan_destroy(dmrgb200_plan_t plan) {
+    if (!plan) return DMRGB200_OK;
+    if (plan->compiled) free_program(plan->prog);
+    cudaFree(plan->T);
+    cudaFree(plan->S);
+    delete plan;
+    return DMRGB200_OK;
+}
+
+dmrgb200_status dmrgb200_plan_flops(dmrgb200_plan_t plan, uint64_t* flops) {
+    if (!plan || !flops) return fail(DMRGB200_INVALID_ARGUMENT, "null argument");
+    *flops = plan->flat.flops();
+    return DMRGB200_OK;
+}
+
+dmrgb200_status dmrgb200_plan_scratch_bytes(dmrgb200_plan_t plan, uint64_t* bytes) {
+    if (!plan || !bytes) return fail(DMRGB200_INVALID_ARGUMENT, "null argument");
+    *bytes = (plan->prog.t_elems + plan->prog.s_elems) * sizeof(double);
+    return DMRGB200_OK;
+}
+
+dmrgb200_status dmrgb200_hpsi(dmrgb200_plan_t plan, const double* x, double* y, dmrgb200_precision prec,
+                              void* cuda_stream) {
+    if (!plan || !x || !y) return fail(DMRGB200_INVALID_ARGUMENT, "null argument");
+    if (plan->flat.kind != KIND_HPSI) return fail(DMRGB200_INVALID_PLAN, "plan is not an H psi plan");
+    if (prec != DMRGB200_PREC_FP64) return fail(DMRGB200_NOT_SUPPORTED, "precision not available in this build");
+    cudaError_t e = run_program(plan->prog, reinterpret_cast<uint64_t>(x), reinterpret_cast<uint64_t>(y), plan->T,
+                                plan->S, static_cast<cudaStream_t>(cuda_stream));
+    if (e != cudaSuccess) return cuda_fail(e, "hpsi launch");
+    return DMRGB200_OK;
+}
+
+dmrgb200_status dmrgb200_step_execute(dmrgb200_plan_t plan, const double* ket, const double* bra,
+                                      const dmrgb200_boundary_view* out, void* cuda_stream) {
+    DMRGB200_TRY
+    if (!plan || !ket || !bra || !out) return fail(DMRGB200_INVALID_ARGUMENT, "null argument");
+    if (plan->flat.kind == KIND_HPSI) return fail(DMRGB200_INVALID_PLAN, "plan is not a boundary-step plan");
+    return run_step(plan, ket, bra, view_ptrs(out), static_cast<cudaStream_t>(cuda_stream));
+    DMRGB200_CATCH
+}
+
+dmrgb200_status dmrgb200_mpo_create(const dmrgb200_mpo_desc* d, dmrgb200_mpo_t* out) {
+    DMRGB200_TRY
+    if (!d || !out) return fail(DMRGB200_INVALID_ARGUMENT, "null argument");
+    auto m = std::make_unique<dmrgb200_mpo_s>();
+    m->symm = to_symm(d->symm);
+    MPOTensor& t = m->mpo;
+    t.row_dim = d->row_dim;
+    t.col_dim = d->col_dim;
+    if (d->left_spin) t.left_spin.assign(d->left_spin, d->left_spin + d->row_dim);
+    if (d->right_spin) t.right_spin.assign(d->right_spin, d->right_spin + d->col_dim);
+    t.left_herm = d->left_herm ? Hermitian(std::vector<unsigned>(d->left_herm, d->left_herm + d->row_dim),
+                                           std::vector<int>(d->left_phase, d->left_phase + d->row_dim))
+                               : Hermitian(d->row_dim);
+    t.right_herm = d->right_herm ? Hermitian(std::vector<unsigned>(d->right_herm, d->right_herm + d->col_dim),
+                                             std::vector<int>(d->right_phase, d->right_phase + d->col_dim))
+                                 : Hermitian(d->col_dim);
+    for (uint32_t o = 0; o < d->n_ops; ++o) {
+        SiteOp op;
+        op.spin = d->op_spin ? d->op_spin[o] : 0;
+        for (uint32_t k = d->op_block[o]; k < d->op_block[o + 1]; ++k) {
+            OpBlock blk;
+            blk.left = Charge(d->blk_in[2 * k], d->blk_in[2 * k + 1]);
+            blk.right = Charge(d->blk_out[2 * k], d->blk_out[2 * k + 1]);
+            for (uint32_t e = d->blk_entry[k]; e < d->blk_entry[k + 1]; ++e)
+                blk.entries.push_back(SparseEntry{d->e_row[e], d->e_col[e], d->e_row_spin ? d->e_row_spin[e] : 0,
+                                                  d->e_col_spin ? d->e_col_spin[e] : 0, d->e_coeff[e]});
+            op.blocks.push_back(std::move(blk));
+        }
+        t.ops.push_back(std::move(op));
+    }
+    t.rows.assign(t.row_dim, {});
+    t.cols.assign(t.col_dim, {});
+    for (uint32_t i = 0; i < d->n_terms; ++i) {
+        uint32_t b1 = d->term_b1[i], b2 = d->term_b2[i];
+        if (b1 >= t.row_dim || b2 >= t.col_dim || d->term_op[i] >= d->n_ops)
+            return fail(DMRGB200_INVALID_ARGUMENT, "MPO term index out of range");
+        auto& row = t.rows[b1];
+        if (row.empty() || row.back().other != b2) {
+            if (!row.empty() && row.back().other > b2)
+                return fail(DMRGB200_INVALID_ARGUMENT, "MPO terms must be sorted by (b1, b2)");
+            row.push_back(MPOEntry{b2, {}});
+        }
+        row.back().terms.push_back(TermRef{d->term_op[i], d->term_scale[i]});
+    }
+    for (uint32_t b1 = 0; b1 < t.row_dim; ++b1)
+        for (auto const& e : t.rows[b1]) t.cols[e.other].push_back(MPOEntry{b1, e.terms});
+    *out = m.release();
+    return DMRGB200_OK;
+    DMRGB200_CATCH
+}
+
+dmrgb200_status dmrgb200_mpo_destroy(dmrgb200_mpo_t mpo) {
+    delete mpo;
+    return DMRGB200_OK;
+}
+
+dmrgb200_status dmrgb200_bindex_create_edge(dmrgb200_symmetry symm, const dmrgb200_index_desc* index,
+                                            uint32_t aux_dim, dmrgb200_bindex_t* out) {
+    DMRGB200_TRY
+    if (!index || !out || aux_dim == 0) return fail(DMRGB200_INVALID_ARGUMENT, "invalid argument");
+    Index ix = to_index(index);
+    auto b = std::make_unique<dmrgb200_bindex_s>();
+    b->idx = BoundaryIndex(to_symm(symm), ix, ix);
+    for (unsigned i = 0; i < ix.size(); ++i) {
+        std::vector<long> off(aux_dim);
+        for (uint32_t a = 0; a < aux_dim; ++a) off[a] = long(a) * ix.block_size(i) * ix.block_size(i);
+        b->idx.add_cohort(i, i, off);
+    }
+    b->layout();
+    *out = b.release();
+    return DMRGB200_OK;
+    DMRGB200_CATCH
+}
+
+dmrgb200_status dmrgb200_bindex_destroy(dmrgb200_bindex_t b) {
+    delete b;
+    return DMRGB200_OK;
+}
+
+dmrgb200_status dmrgb200_bindex_info(dmrgb200_bindex_t b, uint32_t* n_cohorts, uint32_t* aux_dim,
+                                     uint64_t* n_elements) {
+    if (!b) return fail(DMRGB200_INVALID_ARGUMENT, "null boundary index");
+    if (n_cohorts) *n_cohorts = b->idx.n_cohorts();
+    if (aux_dim) *aux_dim = uint32_t(b->idx.aux_dim());
+    if (n_elements) *n_elements = b->n_elems;
+    return DMRGB200_OK;
+}
+
+dmrgb200_status dmrgb200_bindex_describe(dmrgb200_bindex_t b, uint32_t* lb, uint32_t* rb, uint8_t* tr,
+                                         uint64_t* storage_off, uint32_t* lsize, uint32_t* rsize,
+                                         uint32_t* nblocks, int64_t* offsets, double* conj_scales,
+                                         uint8_t* transposes) {
+    if (!b) return fail(DMRGB200_INVALID_ARGUMENT, "null boundary index");
+    BoundaryIndex const& ix = b->idx;
+    size_t aux = ix.aux_dim();
+    std::vector<uint32_t> clb(ix.n_cohorts(), 0), crb(ix.n_cohorts(), 0);
+    for (unsigned l = 0; l < ix.bra().size(); ++l)
+        for (unsigned r = 0; r < ix.ket().size(); ++r) {
+            unsigned ci = ix.cohort_index(l, r);
+            if (ci < ix.n_cohorts()) {
+                clb[ci] = l;
+                crb[ci] = r;
+            }
+        }
+    for (unsigned ci = 0; ci < ix.n_cohorts(); ++ci) {
+        if (lb) lb[ci] = clb[ci];
+        if (rb) rb[ci] = crb[ci];
+        if (tr) tr[ci] = ix.tr(ci);
+        if (storage_off) storage_off[ci] = b->coh_off[ci];
+        if (lsize) lsize[ci] = uint32_t(ix.left_size(ci));
+        if (rsize) rsize[ci] = uint32_t(ix.right_size(ci));
+        if (nblocks) nblocks[ci] = uint32_t(ix.n_blocks(ci));
+        for (size_t a = 0; a < aux; ++a) {
+            if (offsets) offsets[ci * aux + a] = ix.offset(ci, unsigned(a));
+            if (conj_scales) conj_scales[ci * aux + a] = ix.conjugate_scale(ci, unsigned(a));
+            if (transposes) transposes[ci * aux + a] = ix.trans(ci, unsigned(a));
+        }
+    }
+    return DMRGB200_OK;
+}
+
+dmrgb200_status dmrgb200_schedule_hpsi(const dmrgb200_index_desc* phys, const dmrgb200_index_desc* left_i,
+                                       const dmrgb200_index_desc* right_i, dmrgb200_mpo_t mpo,
+                                       dmrgb200_bindex_t L, dmrgb200_bindex_t R, dmrgb200_schedule_t* out) {
+    DMRGB200_TRY
+    if (!mpo || !L || !R || !out) return fail(DMRGB200_INVALID_ARGUMENT, "null argument");
+    Index ph = to_index(phys), li = to_index(left_i), ri = to_index(right_i);
+    Schedule s = create_contraction_schedule(mpo->symm, ph, li, ri, L->idx, R->idx, mpo->mpo);
+    auto sc = std::make_unique<dmrgb200_schedule_s>();
+    sc->flat = flatten_hpsi(s, right_paired_layout(ph, li, ri), L->idx, R->idx);
+    std::string err = sc->flat.validate();
+    if (!err.empty()) return fail(DMRGB200_INVALID_PLAN, "builder produced an inconsistent plan: " + err);
+    *out = sc.release();
+    return DMRGB200_OK;
+    DMRGB200_CATCH
+}
+
+dmrgb200_status dmrgb200_schedule_left_step(const dmrgb200_index_desc* phys, const dmrgb200_index_desc* left_i,
+                                            const dmrgb200_index_desc* right_i, dmrgb200_mpo_t mpo,
+                                            dmrgb200_bindex_t L, int symmetric, dmrgb200_schedule_t* out,
+                                            dmrgb200_bindex_t* new_index) {
+    DMRGB200_TRY
+    if (!mpo || !L || !out || !new_index) return fail(DMRGB200_INVALID_ARGUMENT, "null argument");
+    Index ph = to_index(phys), li = to_index(left_i), ri = to_index(right_i);
+    auto nb = std::make_unique<dmrgb200_bindex_s>();
+    Schedule s = left_step_schedule(mpo->symm, ph, li, ri, li, ri, L->idx, mpo->mpo, symmetric != 0, nb->idx);
+    nb->layout();
+    auto sc = std::make_unique<dmrgb200_schedule_s>();
+    sc->flat = flatten_left_step(s, right_paired_layout(ph, li, ri), left_paired_layout(ph, li, ri), ri, L->idx,
+                                 nb->idx);
+    std::string err = sc->flat.validate();
+    if (!err.empty()) return fail(DMRGB200_INVALID_PLAN, "builder produced an inconsistent plan: " + err);
+    *out = sc.release();
+    *new_index = nb.release();
+    return DMRGB200_OK;
+    DMRGB200_CATCH
+}
+
+dmrgb200_status dmrgb200_schedule_right_step(const dmrgb200_index_desc* phys, const dmrgb200_index_desc* left_i,
+                                             const dmrgb200_index_desc* right_i, dmrgb200_mpo_t mpo,
+                                             dmrgb200_bindex_t R, int symmetric, dmrgb200_schedule_t* out,
+                                             dmrgb200_bindex_t* new_index) {
+    DMRGB200_TRY
+    if (!mpo || !R || !out || !new_index) return fail(DMRGB200_INVALID_ARGUMENT, "null argument");
+    Index ph = to_index(phys), li = to_index(left_i), ri = to_index(right_i);
+    auto nb = std::make_unique<dmrgb200_bindex_s>();
+    Schedule s = right_step_schedule(mpo->symm, ph, li, ri, li, R->idx, mpo->mpo, symmetric != 0, nb->idx);
+    nb->layout();
+    auto sc = std::make_unique<dmrgb200_schedule_s>();
+    TensorLayout rp = right_paired_layout(ph, li, ri);
+    sc->flat = flatten_right_step(s, rp, rp, R->idx, nb->idx);
+    std::string err = sc->flat.validate();
+    if (!err.empty()) return fail(DMRGB200_INVALID_PLAN, "builder produced an inconsistent plan: " + err);
+    *out = sc.release();
+    *new_index = nb.release();
+    return DMRGB200_OK;
+    DMRGB200_CATCH
+}
+
+static void export_flat(FlatPlan const& f, dmrgb200_plan_desc* d);
+
+dmrgb200_status dmrgb200_schedule_export(dmrgb200_schedule_t sc, dmrgb200_plan_desc* d) {
+    if (!sc || !d) return fail(DMRGB200_INVALID_ARGUMENT, "null argument");
+    export_flat(sc->flat, d);
+    return DMRGB200_OK;
+}
+
+dmrgb200_status dmrgb200_schedule_flops(dmrgb200_schedule_t sc, uint64_t* flops) {
+    if (!sc || !flops) return fail(DMRGB200_INVALID_ARGUMENT, "null argument");
+    *flops = sc->flat.flops();
+    return DMRGB200_OK;
+}
+
+dmrgb200_status dmrgb200_schedule_destroy(dmrgb200_schedule_t sc) {
+    delete sc;
+    return DMRGB200_OK;
+}
+
+dmrgb200_status dmrgb200_tensor_layout(const dmrgb200_index_desc* phys, const dmrgb200_index_desc* left_i,
+                                       const dmrgb200_index_desc* right_i, int left_paired, uint32_t* n_blocks,
+                                       uint32_t* rows, uint32_t* cols, uint64_t* offsets, uint64_t* total) {
+    DMRGB200_TRY
+    Index ph = to_index(phys), li = to_index(left_i), ri = to_index(right_i);
+    TensorLayout t = left_paired ? left_paired_layout(ph, li, ri) : right_paired_layout(ph, li, ri);
+    if (n_blocks) *n_blocks = uint32_t(t.rows.size());
+    for (size_t b = 0; b < t.rows.size(); ++b) {
+        if (rows) rows[b] = t.rows[b];
+        if (cols) cols[b] = t.cols[b];
+        if (offsets) offsets[b] = t.off[b];
+    }
+    if (total) *total = t.total;
+    return DMRGB200_OK;
+    DMRGB200_CATCH
+}
+
+static void export_flat(FlatPlan const& f, dmrgb200_plan_desc* d) {
+    std::memset(d, 0, sizeof(*d));
+    d->kind = dmrgb200_plan_kind(f.kind);
+    d->n_groups = f.n_groups();
+    d->g_t = f.g_t.data();
+    d->g_c = f.g_c.data();
+    d->n_in_blocks = uint32_t(f.in_rows.size());
+    d->in_rows = f.in_rows.data();
+    d->in_cols = f.in_cols.data();
+    d->in_off = f.in_off.data();
+    d->in_size = f.in_size;
+    d->n_out_blocks = uint32_t(f.out_rows.size());
+    d->out_rows = f.out_rows.data();
+    d->out_cols = f.out_cols.data();
+    d->out_off = f.out_off.data();
+    d->out_size = f.out_size;
+    d->n_t = f.n_t();
+    d->t_lb = f.t_lb.data();
+    d->t_col = f.t_col.data();
+    d->t_ci = f.t_ci.data();
+    d->t_trans = f.t_trans.data();
+    d->t_nb = f.t_nb.data();
+    d->t_brows = f.t_brows.data();
+    d->t_bcols = f.t_bcols.data();
+    d->t_width = f.t_width.empty() ? nullptr : f.t_width.data();
+    d->n_cohorts = f.n_cohorts();
+    d->c_lb = f.c_lb.data();
+    d->c_rb = f.c_rb.data();
+    d->c_ls = f.c_ls.data();
+    d->c_rs = f.c_rs.data();
+    d->c_ci = f.c_ci.data();
+    d->c_trans = f.c_trans.data();
+    d->c_nsrows = f.c_nsrows.data();
+    d->c_stripe = f.c_stripe.data();
+    d->c_out_ci = f.c_out_ci.data();
+    d->c_unit = f.c_unit.data();
+    d->n_units = f.n_units();
+    d->u_offset = f.u_offset.data();
+    d->u_ms = f.u_ms.data();
+    d->u_line = f.u_line.data();
+    d->n_lines = f.n_lines();
+    d->l_b1 = f.l_b1.data();
+    d->l_term = f.l_term.data();
+    d->n_terms = f.n_terms();
+    d->term_alpha = f.term_alpha.data();
+    d->term_t = f.term_t.data();
+    d->term_col = f.term_col.data();
+}
+
+}  // extern "C"

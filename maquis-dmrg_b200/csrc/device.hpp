@@ -1,0 +1,102 @@
+// Device program: a flat plan lowered to grouped-GEMM tile lists and S-build
+// line lists, plus the launch entry points.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "plan.hpp"
+
+namespace dmrgb200 {
+
+// Operand of a grouped GEMM: element (r, c) of batch b lives at
+//   base[buf] + off + b * bstride + (trans ? c + r * ld : r + c * ld)
+// (row r = M/K index of A / B, column c = K/N index).
+struct DevOp {
+    uint64_t off;
+    uint64_t bstride;
+    uint32_t ld;
+    uint16_t buf;
+    uint16_t trans;
+};
+
+struct DevProb {
+    DevOp C;
+    uint32_t M, N;
+    uint32_t seg_begin, seg_end;
+};
+
+struct DevSeg {
+    DevOp A, B;
+    uint32_t K;
+    uint32_t pad;
+};
+
+struct DevTile {
+    uint32_t prob, batch, m0, n0;
+};
+
+struct DevSLine {
+    uint64_t s_base;
+    uint32_t ld_s, rows, cols, ld_t;
+    uint32_t term_begin, term_end;
+};
+
+struct DevSTerm {
+    double alpha;
+    uint64_t t_base;
+};
+
+enum BufId : uint16_t { BUF_IN = 0, BUF_OUT = 1, BUF_T = 2, BUF_S = 3, BUF_ABS = 4, NBUF = 8 };
+
+struct Bases {
+    uint64_t b[NBUF];
+};
+
+template <class T>
+struct DevArray {
+    T* ptr = nullptr;
+    size_t n = 0;
+};
+
+struct GemmList {
+    std::vector<DevProb> probs;
+    std::vector<DevSeg> segs;
+    std::vector<DevTile> tiles;
+};
+
+struct DeviceProgram {
+    GemmList stage1, stage3;
+    std::vector<DevSLine> lines;
+    std::vector<DevSTerm> terms;
+    uint64_t t_elems = 0, s_elems = 0;
+
+    // device copies
+    DevProb* d_p1 = nullptr;
+    DevSeg* d_s1 = nullptr;
+    DevTile* d_t1 = nullptr;
+    DevProb* d_p3 = nullptr;
+    DevSeg* d_s3 = nullptr;
+    DevTile* d_t3 = nullptr;
+    DevSLine* d_lines = nullptr;
+    DevSTerm* d_terms = nullptr;
+    uint32_t n_t1 = 0, n_t3 = 0, n_lines = 0;
+};
+
+// Lower a flat plan.  lptr/rptr: device address of each cohort's storage of the
+// boundary read by stage 3 (H psi: L) and by stage 1 (H psi, right step: R;
+// left step: L).  outptr: device address of each output boundary cohort (steps).
+void compile_program(FlatPlan const& p, std::vector<uint64_t> const& stage3_bnd, std::vector<uint64_t> const& stage1_bnd,
+                     std::vector<uint64_t> const& outptr, DeviceProgram& prog);
+cudaError_t upload_program(DeviceProgram& prog);
+void free_program(DeviceProgram& prog);
+
+// Launch the three stages on a stream; T and S are the scratch buffers.
+cudaError_t run_program(DeviceProgram const& prog, uint64_t in, uint64_t out, double* T, double* S,
+                        cudaStream_t stream);
+
+int device_sm_count();
+
+}  // namespace dmrgb200

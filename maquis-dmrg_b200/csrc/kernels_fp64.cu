@@ -1,0 +1,416 @@
+// Native-FP64 execution of a lowered plan on sm_100a.
+//
+// Stage 1 (T tasks) and stage 3 (cohort contractions) run as grouped,
+// persistent GEMM launches over precomputed tile lists; every output tile is
+// owned by exactly one CTA, which loops over the tile's K segments (for H psi:
+// every cohort that writes the output block), so the result is written once,
+// without atomics, and is bitwise reproducible.  Stage 2 (S build) gathers
+// alpha-weighted T columns (Cohort::create_s_r / create_s, tasks.cpp:425-494).
+//
+// The FP64 inner product uses the FP64 tensor-core instruction
+// mma.sync.m8n8k4.f64 (DMMA) on 64x64x16 CTA tiles, 4 warps of 32x32.
+#include <algorithm>
+#include <cstdio>
+#include <numeric>
+
+#include "device.hpp"
+
+namespace dmrgb200 {
+
+namespace {
+
+constexpr int BM = 64, BN = 64, BK = 16, PAD = 4, NTHREADS = 128;
+
+__device__ __forceinline__ const double* op_base(Bases const& bs, DevOp const& op, uint32_t batch) {
+    return reinterpret_cast<const double*>(bs.b[op.buf] + 8ull * (op.off + uint64_t(batch) * op.bstride));
+}
+
+__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(NTHREADS) gemm_f64_grouped(const DevProb* __restrict__ probs,
+                                                             const DevSeg* __restrict__ segs,
+                                                             const DevTile* __restrict__ tiles, uint32_t n_tiles,
+                                                             Bases bases) {
+    __shared__ double As[BK][BM + PAD];
+    __shared__ double Bs[BK][BN + PAD];
+
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    const int g = lane >> 2, q = lane & 3;
+
+    for (uint32_t ti = blockIdx.x; ti < n_tiles; ti += gridDim.x) {
+        const DevTile tl = tiles[ti];
+        const DevProb pr = probs[tl.prob];
+        const uint32_t M = pr.M, N = pr.N;
+        double acc[4][4][2];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+        for (uint32_t s = pr.seg_begin; s < pr.seg_end; ++s) {
+            const DevSeg sg = segs[s];
+            const double* A = op_base(bases, sg.A, tl.batch);
+            const double* B = op_base(bases, sg.B, tl.batch);
+            const uint64_t lda = sg.A.ld, ldb = sg.B.ld;
+            const uint32_t K = sg.K;
+            for (uint32_t k0 = 0; k0 < K; k0 += BK) {
+                // A tile: BM x BK -> As[k][m]
+#pragma unroll
+                for (int j = 0; j < (BM * BK) / NTHREADS; ++j) {
+                    int idx = tid + j * NTHREADS;
+                    int m, k;
+                    if (!sg.A.trans) {
+                        m = idx % BM;
+                        k = idx / BM;
+                    } else {
+                        k = idx % BK;
+                        m = idx / BK;
+                    }
+                    uint32_t gm = tl.m0 + m, gk = k0 + k;
+                    double v = 0.0;
+                    if (gm < M && gk < K) v = sg.A.trans ? A[gk + gm * lda] : A[gm + gk * lda];
+                    As[k][m] = v;
+                }
+                // B tile: BK x BN -> Bs[k][n]
+#pragma unroll
+                for (int j = 0; j < (BN * BK) / NTHREADS; ++j) {
+                    int idx = tid + j * NTHREADS;
+                    int n, k;
+                    if (!sg.B.trans) {
+                        k = idx % BK;
+                        n = idx / BK;
+                    } else {
+                        n = idx % BN;
+                        k = idx / BN;
+                    }
+                    uint32_t gn = tl.n0 + n, gk = k0 + k;
+                    double v = 0.0;
+                    if (gn < N && gk < K) v = sg.B.trans ? B[gn + gk * ldb] : B[gk + gn * ldb];
+                    Bs[k][n] = v;
+                }
+                __syncthreads();
+#pragma unroll
+                for (int kk = 0; kk < BK; kk += 4) {
+                    double a[4], b[4];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) a[i] = As[kk + q][wm + i * 8 + g];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) b[j] = Bs[kk + q][wn + j * 8 + g];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+                }
+                __syncthreads();
+            }
+        }
+
+        double* C = const_cast<double*>(op_base(bases, pr.C, tl.batch));
+        const uint64_t ldc = pr.C.ld;
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    uint32_t r = tl.m0 + wm + i * 8 + g;
+                    uint32_t c = tl.n0 + wn + j * 8 + q * 2 + e;
+                    if (r < M && c < N) C[r + c * ldc] = acc[i][j][e];
+                }
+    }
+}
+
+// S build: every line writes rows x cols elements of S as the alpha-weighted sum
+// of its T sources, summed in term order like the reference's axpy sequence.
+__global__ void __launch_bounds__(256) sbuild_lines(const DevSLine* __restrict__ lines,
+                                                    const DevSTerm* __restrict__ terms, uint32_t n_lines,
+                                                    double* __restrict__ S, const double* __restrict__ T) {
+    for (uint32_t li = blockIdx.x; li < n_lines; li += gridDim.x) {
+        const DevSLine L = lines[li];
+        const uint64_t n = uint64_t(L.rows) * L.cols;
+        for (uint64_t idx = threadIdx.x; idx < n; idx += blockDim.x) {
+            uint32_t i = uint32_t(idx % L.rows), c = uint32_t(idx / L.rows);
+            double v = 0.0;
+            for (uint32_t t = L.term_begin; t < L.term_end; ++t) {
+                const DevSTerm tm = terms[t];
+                v += tm.alpha * T[tm.t_base + i + uint64_t(c) * L.ld_t];
+            }
+            S[L.s_base + i + uint64_t(c) * L.ld_s] = v;
+        }
+    }
+}
+
+// --- host-side lowering ---------------------------------------------------------
+
+void add_tiles(GemmList& gl, uint32_t prob, uint32_t nbatch) {
+    DevProb const& p = gl.probs[prob];
+    for (uint32_t b = 0; b < nbatch; ++b)
+        for (uint32_t m0 = 0; m0 < std::max<uint32_t>(p.M, 1); m0 += BM)
+            for (uint32_t n0 = 0; n0 < std::max<uint32_t>(p.N, 1); n0 += BN) gl.tiles.push_back(DevTile{prob, b, m0, n0});
+}
+
+// Order tiles by decreasing K work so that the static round-robin of the
+// persistent grid starts with the longest tiles (LPT-style balance).
+void sort_tiles(GemmList& gl) {
+    std::vector<uint64_t> kwork(gl.probs.size(), 0);
+    for (size_t p = 0; p < gl.probs.size(); ++p)
+        for (uint32_t s = gl.probs[p].seg_begin; s < gl.probs[p].seg_end; ++s) kwork[p] += gl.segs[s].K;
+    std::stable_sort(gl.tiles.begin(), gl.tiles.end(),
+                     [&](DevTile const& a, DevTile const& b) { return kwork[a.prob] > kwork[b.prob]; });
+}
+
+DevOp op(uint16_t buf, uint64_t off, uint32_t ld, bool trans, uint64_t bstride = 0) {
+    DevOp o;
+    o.off = off;
+    o.bstride = bstride;
+    o.ld = ld;
+    o.buf = buf;
+    o.trans = trans ? 1 : 0;
+    return o;
+}
+
+}  // namespace
+
+void compile_program(FlatPlan const& p, std::vector<uint64_t> const& stage3_bnd,
+                     std::vector<uint64_t> const& stage1_bnd, std::vector<uint64_t> const& outptr,
+                     DeviceProgram& prog) {
+    prog = DeviceProgram();
+    const uint32_t nt = p.n_t(), nc = p.n_cohorts();
+    std::vector<uint64_t> t_off(nt);
+    uint64_t tsum = 0;
+    for (uint32_t t = 0; t < nt; ++t) {
+        t_off[t] = tsum;
+        tsum += round_up(p.t_size(t), 32);
+    }
+    prog.t_elems = tsum;
+
+    // ---- stage 1 ----
+    GemmList& g1 = prog.stage1;
+    for (uint32_t t = 0; t < nt; ++t) {
+        DevProb pr;
+        DevSeg sg{};
+        uint64_t bnd = stage1_bnd.at(p.t_ci[t]) / 8;
+        if (p.kind == KIND_LEFT) {
+            uint32_t M = p.t_brows[t], N = p.t_width[t], K = p.t_bcols[t];
+            sg.A = op(BUF_ABS, bnd, p.t_trans[t] ? K : M, p.t_trans[t], uint64_t(M) * K);
+            sg.B = op(BUF_IN, p.in_off[p.t_lb[t]] + uint64_t(p.t_col[t]) * K, K, false, 0);
+            sg.K = K;
+            pr.C = op(BUF_T, t_off[t], M, false, uint64_t(M) * N);
+            pr.M = M;
+            pr.N = N;
+        } else {
+            uint32_t M = p.in_rows[p.t_lb[t]], N = p.t_bcols[t], K = p.t_brows[t];
+            sg.A = op(BUF_IN, p.in_off[p.t_lb[t]] + uint64_t(p.t_col[t]) * M, M, false, 0);
+            sg.B = op(BUF_ABS, bnd, p.t_trans[t] ? N : K, p.t_trans[t], uint64_t(K) * N);
+            sg.K = K;
+            pr.C = op(BUF_T, t_off[t], M, false, uint64_t(M) * N);
+            pr.M = M;
+            pr.N = N;
+        }
+        pr.seg_begin = uint32_t(g1.segs.size());
+        g1.segs.push_back(sg);
+        pr.seg_end = uint32_t(g1.segs.size());
+        g1.probs.push_back(pr);
+        add_tiles(g1, uint32_t(g1.probs.size() - 1), p.t_nb[t]);
+    }
+    sort_tiles(g1);
+
+    // ---- stage 2 (S lines) ----
+    std::vector<uint64_t> s_off(nc);
+    uint64_t ssum = 0;
+    for (uint32_t c = 0; c < nc; ++c) {
+        s_off[c] = ssum;
+        ssum += round_up(uint64_t(p.c_nsrows[c]) * p.c_stripe[c] * (p.kind == KIND_LEFT ? p.c_rs[c] : p.c_ls[c]), 32);
+    }
+    prog.s_elems = ssum;
+    for (uint32_t c = 0; c < nc; ++c) {
+        for (uint32_t u = p.c_unit[c]; u < p.c_unit[c + 1]; ++u)
+            for (uint32_t l = p.u_line[u]; l < p.u_line[u + 1]; ++l) {
+                DevSLine L;
+                L.term_begin = uint32_t(prog.terms.size());
+                if (p.kind == KIND_LEFT) {
+                    L.ld_s = p.c_stripe[c];
+                    L.rows = p.u_ms[u];
+                    L.cols = p.c_rs[c];
+                    L.ld_t = p.u_ms[u];
+                    L.s_base = s_off[c] + p.u_offset[u] + uint64_t(p.l_b1[l]) * p.c_rs[c] * p.c_stripe[c];
+                    for (uint32_t k = p.l_term[l]; k < p.l_term[l + 1]; ++k)
+                        prog.terms.push_back(
+                            DevSTerm{p.term_alpha[k], t_off[p.term_t[k]] + uint64_t(p.term_col[k]) * p.c_rs[c]});
+                } else {
+                    uint32_t ls = p.c_ls[c];
+                    L.ld_s = p.c_nsrows[c] * ls;
+                    L.rows = ls;
+                    L.cols = p.u_ms[u];
+                    L.ld_t = ls;
+                    L.s_base = s_off[c] + uint64_t(p.l_b1[l]) * ls + uint64_t(p.u_offset[u]) * L.ld_s;
+                    for (uint32_t k = p.l_term[l]; k < p.l_term[l + 1]; ++k)
+                        prog.terms.push_back(
+                            DevSTerm{p.term_alpha[k], t_off[p.term_t[k]] + uint64_t(p.term_col[k]) * ls});
+                }
+                L.term_end = uint32_t(prog.terms.size());
+                prog.lines.push_back(L);
+            }
+    }
+
+    // ---- stage 3 ----
+    GemmList& g3 = prog.stage3;
+    if (p.kind == KIND_HPSI) {
+        std::vector<std::vector<uint32_t>> by_out(p.out_rows.size());
+        for (uint32_t c = 0; c < nc; ++c) by_out[p.c_rb[c]].push_back(c);
+        for (uint32_t ob = 0; ob < p.out_rows.size(); ++ob) {
+            DevProb pr;
+            pr.M = p.out_rows[ob];
+            pr.N = p.out_cols[ob];
+            pr.C = op(BUF_OUT, p.out_off[ob], pr.M, false, 0);
+            pr.seg_begin = uint32_t(g3.segs.size());
+            for (uint32_t c : by_out[ob]) {
+                uint32_t ls = p.c_ls[c], rs = p.c_rs[c], ns = p.c_nsrows[c];
+                uint64_t lbase = stage3_bnd.at(p.c_ci[c]) / 8;
+                if (!p.c_trans[c]) {
+                    DevSeg sg{};
+                    sg.A = op(BUF_ABS, lbase, rs, false);
+                    sg.B = op(BUF_S, s_off[c], ns * ls, false);
+                    sg.K = ns * ls;
+                    g3.segs.push_back(sg);
+                } else {
+                    // each stored block (ls x rs) is read transposed: one segment per MPO row block
+                    for (uint32_t b = 0; b < ns; ++b) {
+                        DevSeg sg{};
+                        sg.A = op(BUF_ABS, lbase + uint64_t(b) * ls * rs, ls, true);
+                        sg.B = op(BUF_S, s_off[c] + uint64_t(b) * ls, ns * ls, false);
+                        sg.K = ls;
+                        g3.segs.push_back(sg);
+                    }
+                }
+            }
+            pr.seg_end = uint32_t(g3.segs.size());
+            g3.probs.push_back(pr);
+            add_tiles(g3, uint32_t(g3.probs.size() - 1), 1);
+        }
+    } else if (p.kind == KIND_RIGHT) {
+        for (uint32_t c = 0; c < nc; ++c) {
+            uint32_t ls = p.c_ls[c], rs = p.c_rs[c], ns = p.c_nsrows[c];
+            DevProb pr;
+            pr.M = ls;
+            pr.N = rs;
+            pr.C = op(BUF_ABS, outptr.at(p.c_out_ci[c]) / 8, ls, false, uint64_t(ls) * rs);
+            DevSeg sg{};
+            sg.A = op(BUF_S, s_off[c], ns * ls, false, ls);
+            sg.B = op(BUF_OUT, p.out_off[p.c_rb[c]], rs, true, 0);
+            sg.K = p.c_stripe[c];
+            pr.seg_begin = uint32_t(g3.segs.size());
+            g3.segs.push_back(sg);
+            pr.seg_end = uint32_t(g3.segs.size());
+            g3.probs.push_back(pr);
+            add_tiles(g3, uint32_t(g3.probs.size() - 1), ns);
+        }
+    } else {
+        for (uint32_t c = 0; c < nc; ++c) {
+            uint32_t ls = p.c_ls[c], rs = p.c_rs[c], ns = p.c_nsrows[c], stripe = p.c_stripe[c];
+            DevProb pr;
+            pr.M = ls;
+            pr.N = ns * rs;
+            pr.C = op(BUF_ABS, outptr.at(p.c_out_ci[c]) / 8, ls, false, 0);
+            DevSeg sg{};
+            sg.A = op(BUF_OUT, p.out_off[p.c_lb[c]], stripe, true, 0);
+            sg.B = op(BUF_S, s_off[c], stripe, false, 0);
+            sg.K = stripe;
+            pr.seg_begin = uint32_t(g3.segs.size());
+            g3.segs.push_back(sg);
+            pr.seg_end = uint32_t(g3.segs.size());
+            g3.probs.push_back(pr);
+            add_tiles(g3, uint32_t(g3.probs.size() - 1), 1);
+        }
+    }
+    sort_tiles(g3);
+}
+
+namespace {
+template <class T>
+cudaError_t up(std::vector<T> const& v, T** d) {
+    *d = nullptr;
+    if (v.empty()) return cudaSuccess;
+    cudaError_t e = cudaMalloc(d, v.size() * sizeof(T));
+    if (e != cudaSuccess) return e;
+    return cudaMemcpy(*d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+}
+}  // namespace
+
+cudaError_t upload_program(DeviceProgram& prog) {
+    cudaError_t e;
+    if ((e = up(prog.stage1.probs, &prog.d_p1)) != cudaSuccess) return e;
+    if ((e = up(prog.stage1.segs, &prog.d_s1)) != cudaSuccess) return e;
+    if ((e = up(prog.stage1.tiles, &prog.d_t1)) != cudaSuccess) return e;
+    if ((e = up(prog.stage3.probs, &prog.d_p3)) != cudaSuccess) return e;
+    if ((e = up(prog.stage3.segs, &prog.d_s3)) != cudaSuccess) return e;
+    if ((e = up(prog.stage3.tiles, &prog.d_t3)) != cudaSuccess) return e;
+    if ((e = up(prog.lines, &prog.d_lines)) != cudaSuccess) return e;
+    if ((e = up(prog.terms, &prog.d_terms)) != cudaSuccess) return e;
+    prog.n_t1 = uint32_t(prog.stage1.tiles.size());
+    prog.n_t3 = uint32_t(prog.stage3.tiles.size());
+    prog.n_lines = uint32_t(prog.lines.size());
+    return cudaSuccess;
+}
+
+void free_program(DeviceProgram& prog) {
+    cudaFree(prog.d_p1);
+    cudaFree(prog.d_s1);
+    cudaFree(prog.d_t1);
+    cudaFree(prog.d_p3);
+    cudaFree(prog.d_s3);
+    cudaFree(prog.d_t3);
+    cudaFree(prog.d_lines);
+    cudaFree(prog.d_terms);
+    prog.d_p1 = nullptr;
+    prog.d_s1 = nullptr;
+    prog.d_t1 = nullptr;
+    prog.d_p3 = nullptr;
+    prog.d_s3 = nullptr;
+    prog.d_t3 = nullptr;
+    prog.d_lines = nullptr;
+    prog.d_terms = nullptr;
+}
+
+int device_sm_count() {
+    int dev = 0, n = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 148;
+}
+
+cudaError_t run_program(DeviceProgram const& prog, uint64_t in, uint64_t out, double* T, double* S,
+                        cudaStream_t stream) {
+    Bases bs{};
+    bs.b[BUF_IN] = in;
+    bs.b[BUF_OUT] = out;
+    bs.b[BUF_T] = reinterpret_cast<uint64_t>(T);
+    bs.b[BUF_S] = reinterpret_cast<uint64_t>(S);
+    bs.b[BUF_ABS] = 0;
+    const int sms = device_sm_count();
+    if (prog.n_t1) {
+        uint32_t grid = std::min<uint32_t>(prog.n_t1, uint32_t(sms) * 4);
+        gemm_f64_grouped<<<grid, NTHREADS, 0, stream>>>(prog.d_p1, prog.d_s1, prog.d_t1, prog.n_t1, bs);
+    }
+    if (prog.s_elems) {
+        cudaError_t e = cudaMemsetAsync(S, 0, prog.s_elems * sizeof(double), stream);
+        if (e != cudaSuccess) return e;
+    }
+    if (prog.n_lines) {
+        uint32_t grid = std::min<uint32_t>(prog.n_lines, uint32_t(sms) * 8);
+        sbuild_lines<<<grid, 256, 0, stream>>>(prog.d_lines, prog.d_terms, prog.n_lines, S, T);
+    }
+    if (prog.n_t3) {
+        uint32_t grid = std::min<uint32_t>(prog.n_t3, uint32_t(sms) * 4);
+        gemm_f64_grouped<<<grid, NTHREADS, 0, stream>>>(prog.d_p3, prog.d_s3, prog.d_t3, prog.n_t3, bs);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace dmrgb200

@@ -1,0 +1,195 @@
+"""Host-side driver of the hot path over the C ABI.
+
+* schedule building (host, libdmrgb200's C++ builder): H·psi and left/right
+  boundary-step plans, returned as flat numpy plan dictionaries;
+* device execution: plans bound to device-resident boundaries (torch CUDA
+  tensors used as plain device buffers) and run by the library's sm_100a
+  kernels; there is no CPU execution path here.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _capi as capi
+from .models import MPOHandle
+
+
+class IndexArrays:
+    """dmrgb200_index_desc over a [(charge, size)] list."""
+
+    def __init__(self, idx):
+        self.charges = np.ascontiguousarray(np.array([list(c) for c, _ in idx], dtype=np.int32).reshape(-1))
+        self.sizes = np.ascontiguousarray(np.array([m for _, m in idx], dtype=np.uint32))
+        self.desc = capi.IndexDesc()
+        self.desc.n = len(idx)
+        self.desc.charges = capi.ptr(self.charges, C.c_int32) if len(idx) else None
+        self.desc.sizes = capi.ptr(self.sizes, C.c_uint32) if len(idx) else None
+
+    @property
+    def ref(self):
+        return C.byref(self.desc)
+
+
+class BIndex:
+    """A boundary index handle plus its described storage layout."""
+
+    def __init__(self, handle):
+        self.handle = handle
+        nc, aux, ne = C.c_uint32(), C.c_uint32(), C.c_uint64()
+        capi.check(capi.lib.dmrgb200_bindex_info(handle, C.byref(nc), C.byref(aux), C.byref(ne)), "bindex_info")
+        self.n_cohorts, self.aux, self.n_elems = nc.value, aux.value, ne.value
+        n, a = self.n_cohorts, max(self.aux, 1)
+        self.lb = np.zeros(n, np.uint32)
+        self.rb = np.zeros(n, np.uint32)
+        self.tr = np.zeros(n, np.uint8)
+        self.storage_off = np.zeros(n, np.uint64)
+        self.lsize = np.zeros(n, np.uint32)
+        self.rsize = np.zeros(n, np.uint32)
+        self.nblocks = np.zeros(n, np.uint32)
+        self.offsets = np.zeros(n * a, np.int64)
+        self.conj = np.zeros(n * a, np.float64)
+        self.trans = np.zeros(n * a, np.uint8)
+        capi.check(capi.lib.dmrgb200_bindex_describe(
+            handle, capi.ptr(self.lb, C.c_uint32), capi.ptr(self.rb, C.c_uint32), capi.ptr(self.tr, C.c_uint8),
+            capi.ptr(self.storage_off, C.c_uint64), capi.ptr(self.lsize, C.c_uint32),
+            capi.ptr(self.rsize, C.c_uint32), capi.ptr(self.nblocks, C.c_uint32), capi.ptr(self.offsets, C.c_int64),
+            capi.ptr(self.conj, C.c_double), capi.ptr(self.trans, C.c_uint8)), "bindex_describe")
+        self.offsets = self.offsets.reshape(n, a)
+        self.conj = self.conj.reshape(n, a)
+        self.trans = self.trans.reshape(n, a)
+
+    def has_storage(self, ci):
+        return self.storage_off[ci] != np.uint64(0xFFFFFFFFFFFFFFFF)
+
+    def cohort_addresses(self, base: int) -> np.ndarray:
+        """Address of each cohort's storage for a buffer at `base` (0 without storage)."""
+        out = np.zeros(self.n_cohorts, dtype=np.uint64)
+        for ci in range(self.n_cohorts):
+            if self.has_storage(ci):
+                out[ci] = np.uint64(base + 8 * int(self.storage_off[ci]))
+        return out
+
+    def edge_values(self) -> np.ndarray:
+        """Storage filled with ones (an edge boundary, boundary.h:257-283)."""
+        v = np.zeros(self.n_elems)
+        for ci in range(self.n_cohorts):
+            if self.has_storage(ci):
+                o = int(self.storage_off[ci])
+                v[o:o + int(self.lsize[ci]) * int(self.rsize[ci]) * int(self.nblocks[ci])] = 1.0
+        return v
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            capi.lib.dmrgb200_bindex_destroy(self.handle)
+            self.handle = None
+
+
+def edge_bindex(symm: int, index, aux: int = 1) -> BIndex:
+    ia = IndexArrays(index)
+    h = C.c_void_p()
+    capi.check(capi.lib.dmrgb200_bindex_create_edge(symm, ia.ref, aux, C.byref(h)), "bindex_create_edge")
+    return BIndex(h)
+
+
+class Schedule:
+    """A host-side flat plan (dmrgb200_schedule_t) and its numpy export."""
+
+    def __init__(self, handle):
+        self.handle = handle
+        d = capi.PlanDesc()
+        capi.check(capi.lib.dmrgb200_schedule_export(handle, C.byref(d)), "schedule_export")
+        self.plan = capi.desc_to_numpy(d)
+        f = C.c_uint64()
+        capi.check(capi.lib.dmrgb200_schedule_flops(handle, C.byref(f)), "schedule_flops")
+        self.flops = f.value
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            capi.lib.dmrgb200_schedule_destroy(self.handle)
+            self.handle = None
+
+
+def schedule_hpsi(phys, left, right, mpo: MPOHandle, L: BIndex, R: BIndex) -> Schedule:
+    p, l, r = IndexArrays(phys), IndexArrays(left), IndexArrays(right)
+    h = C.c_void_p()
+    capi.check(capi.lib.dmrgb200_schedule_hpsi(p.ref, l.ref, r.ref, mpo.handle, L.handle, R.handle, C.byref(h)),
+               "schedule_hpsi")
+    return Schedule(h)
+
+
+def schedule_left_step(phys, left, right, mpo: MPOHandle, L: BIndex, symmetric=True):
+    p, l, r = IndexArrays(phys), IndexArrays(left), IndexArrays(right)
+    h, nb = C.c_void_p(), C.c_void_p()
+    capi.check(capi.lib.dmrgb200_schedule_left_step(p.ref, l.ref, r.ref, mpo.handle, L.handle, int(symmetric),
+                                                    C.byref(h), C.byref(nb)), "schedule_left_step")
+    return Schedule(h), BIndex(nb)
+
+
+def schedule_right_step(phys, left, right, mpo: MPOHandle, R: BIndex, symmetric=True):
+    p, l, r = IndexArrays(phys), IndexArrays(left), IndexArrays(right)
+    h, nb = C.c_void_p(), C.c_void_p()
+    capi.check(capi.lib.dmrgb200_schedule_right_step(p.ref, l.ref, r.ref, mpo.handle, R.handle, int(symmetric),
+                                                     C.byref(h), C.byref(nb)), "schedule_right_step")
+    return Schedule(h), BIndex(nb)
+
+
+# ---- device side --------------------------------------------------------------------
+
+def _view(addresses: np.ndarray):
+    arr = (C.c_void_p * max(len(addresses), 1))(*[int(a) if a else None for a in addresses])
+    v = capi.BoundaryView()
+    v.n_cohorts = len(addresses)
+    v.cohort_ptr = C.cast(arr, C.POINTER(C.c_void_p))
+    return v, arr
+
+
+class Context:
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        capi.check(capi.lib.dmrgb200_context_create(device, C.byref(h)), "context_create")
+        self.handle = h
+        self.device = device
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            capi.lib.dmrgb200_context_destroy(self.handle)
+            self.handle = None
+
+
+class DevicePlan:
+    """A plan bound to device boundaries (dmrgb200_plan_create)."""
+
+    def __init__(self, ctx: Context, plan: dict, left_addr=None, other_addr=None):
+        desc, self._keep = capi.numpy_to_desc(plan)
+        lv = ov = None
+        if left_addr is not None:
+            lv, la = _view(left_addr)
+            self._keep.append(la)
+        if other_addr is not None:
+            ov, oa = _view(other_addr)
+            self._keep.append(oa)
+        h = C.c_void_p()
+        capi.check(capi.lib.dmrgb200_plan_create(ctx.handle, C.byref(desc), C.byref(lv) if lv else None,
+                                                 C.byref(ov) if ov else None, C.byref(h)), "plan_create")
+        self.handle = h
+        self.plan = plan
+        f, s = C.c_uint64(), C.c_uint64()
+        capi.check(capi.lib.dmrgb200_plan_flops(h, C.byref(f)), "plan_flops")
+        capi.check(capi.lib.dmrgb200_plan_scratch_bytes(h, C.byref(s)), "plan_scratch_bytes")
+        self.flops, self.scratch_bytes = f.value, s.value
+
+    def hpsi(self, x_ptr: int, y_ptr: int, prec: int = capi.PREC_FP64, stream: int = 0) -> None:
+        capi.check(capi.lib.dmrgb200_hpsi(self.handle, x_ptr, y_ptr, prec, stream or None), "dmrgb200_hpsi")
+
+    def step(self, ket_ptr: int, bra_ptr: int, out_addr: np.ndarray, stream: int = 0) -> None:
+        v, arr = _view(out_addr)
+        capi.check(capi.lib.dmrgb200_step_execute(self.handle, ket_ptr, bra_ptr, C.byref(v), stream or None),
+                   "dmrgb200_step_execute")
+        del arr
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            capi.lib.dmrgb200_plan_destroy(self.handle)
+            self.handle = None

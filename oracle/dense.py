@@ -1,0 +1,128 @@
+"""ORACLE — test infrastructure only.  Dense exact references for small chains.
+
+* dense Hamiltonians built directly from each model's term list (fermionic
+  operators with explicit Jordan-Wigner strings), independent of the MPO code;
+* exact ground states by diagonalisation in a fixed charge sector;
+* the dense embedding P of a two-site tensor into the full Hilbert space, so that
+  H_eff = P^T H P is the matrix the schedule-based H·psi must apply.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from dmrgb200 import models as M
+from dmrgb200 import mps as S
+
+
+def local_charges(model: M.Model):
+    return [c for c, d in model.phys for _ in range(d)]
+
+
+def dense_hamiltonian(model: M.Model, L: int) -> np.ndarray:
+    d = sum(dd for _, dd in model.phys)
+    F = model.local.get("fill")
+    I = np.eye(d)
+
+    def site_op(name, p):
+        O = model.local[name]
+        mats = []
+        for q in range(L):
+            if q == p:
+                mats.append(O)
+            elif q < p and name in model.fermionic_ops:
+                mats.append(F)
+            else:
+                mats.append(I)
+        out = mats[0]
+        for m in mats[1:]:
+            out = np.kron(out, m)
+        return out
+
+    H = np.zeros((d ** L, d ** L))
+    for coeff, factors in model.dense_terms:
+        term = np.eye(d ** L)
+        for p, name in factors:
+            term = term @ site_op(name, p)
+        H += coeff * term
+    return H
+
+
+def sector_mask(model: M.Model, L: int, total) -> np.ndarray:
+    ch = local_charges(model)
+    d = len(ch)
+    q = np.zeros((d ** L, 2), dtype=int)
+    for idx in range(d ** L):
+        rem = idx
+        tot = [0, 0]
+        for p in range(L - 1, -1, -1):
+            s = rem % d
+            rem //= d
+            tot[0] += ch[s][0]
+            tot[1] += ch[s][1]
+        q[idx] = tot
+    return (q[:, 0] == total[0]) & (q[:, 1] == total[1])
+
+
+def ground_energy(model: M.Model, L: int) -> float:
+    H = dense_hamiltonian(model, L)
+    mask = sector_mask(model, L, model.total_charge)
+    Hs = H[np.ix_(mask, mask)]
+    return float(np.linalg.eigvalsh(Hs)[0])
+
+
+def mps_dense(tensors) -> np.ndarray:
+    """Contract site tensors (dense [Dl, d, Dr]) into a vector (site 0 most significant)."""
+    v = tensors[0]
+    for t in tensors[1:]:
+        v = np.tensordot(v, t, axes=([v.ndim - 1], [0]))
+    return v.reshape(-1)
+
+
+def twosite_dense(phys1, phys2, psi: S.SiteTensor) -> np.ndarray:
+    """Dense [Dl, d1, d2, Dr] of a two-site tensor whose physical index is the
+    fused basis of models.fuse_phys(phys1, phys2)."""
+    A = psi.dense()  # [Dl, d12, Dr] in fused-basis order
+    p12, offs = M.fuse_phys(phys1, phys2)
+    poff12 = {}
+    o = 0
+    for c, d in p12:
+        poff12[c] = o
+        o += d
+    d1s, d2s = dict(phys1), dict(phys2)
+    o1 = np.cumsum([0] + [d for _, d in phys1])
+    o2 = np.cumsum([0] + [d for _, d in phys2])
+    out = np.zeros((A.shape[0], o1[-1], o2[-1], A.shape[2]))
+    for a, (c1, _) in enumerate(phys1):
+        for b, (c2, _) in enumerate(phys2):
+            f = (c1[0] + c2[0], c1[1] + c2[1])
+            for i1 in range(d1s[c1]):
+                for i2 in range(d2s[c2]):
+                    k = poff12[f] + offs[(c1, c2)] + i1 * d2s[c2] + i2
+                    out[:, o1[a] + i1, o2[b] + i2, :] = A[:, k, :]
+    return out
+
+
+def embedding(mps_left, mps_right, phys1, phys2, left, right, p12) -> np.ndarray:
+    """Columns: dense states of every unit two-site tensor (P of H_eff = P^T H P)."""
+    tmpl = S.SiteTensor(p12, left, right)
+    n = tmpl.rp.total
+    cols = []
+    lefts = [t.dense() for t in mps_left]
+    rights = [t.dense() for t in mps_right]
+    valid = np.zeros(n, dtype=bool)
+    for b in range(len(tmpl.rp.rows)):
+        valid[tmpl.rp.offs[b]:tmpl.rp.offs[b] + tmpl.rp.rows[b] * tmpl.rp.cols[b]] = True
+    P = []
+    for k in range(n):
+        if not valid[k]:
+            P.append(None)
+            continue
+        e = np.zeros(n)
+        e[k] = 1.0
+        psi = S.SiteTensor(p12, left, right, e)
+        core = twosite_dense(phys1, phys2, psi)
+        D = core.shape
+        core = core.reshape(D[0], D[1] * D[2], D[3])
+        P.append(mps_dense(lefts + [core] + rights))
+    dim = len(next(p for p in P if p is not None))
+    return np.stack([p if p is not None else np.zeros(dim) for p in P], axis=1)

@@ -1,0 +1,324 @@
+"""H·psi throughput benchmark of the DMRG hot path on B200.
+
+Workload (N=1): the two-site H·psi at the middle of a 1D Fermi-Hubbard open
+chain, L=64, t=1, U=4, half filling (32 up / 32 down), TwoU1 symmetry, bond
+dimension m=1024 (synthetic sector distribution, seeded random MPS; the
+boundaries are built on the device by the library's boundary steps).  One step
+= one H·psi application (dmrgb200_hpsi).  Inputs are smaller than L2, so L2 is
+flushed (256 MiB write) between timed steps.
+
+value   = H·psi GFLOP/s (the reference's flop formula) with x, y resident in HBM
+e2e     = same through the C ABI with pinned host buffers: H2D of psi, H·psi,
+          D2H of the result inside each timed step
+--impl reference: the reference's CPU schedule execution (the oracle's
+          restatement: OpenMP over task groups + OpenBLAS) on all host cores.
+Multi-GPU: replicas only (the path is one GPU per site problem); value sums
+the ranks' work over the max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+for _p in (ROOT / "maquis-dmrg_b200", ROOT / "oracle"):
+    sys.path.insert(0, str(_p))
+
+L_SITES, M_BOND, RADIUS, SEED = 64, 1024, 3.5, 2
+WORKLOAD = "fermi_hubbard_L64_twou1_m1024_twosite_hpsi_middle"
+METRIC = "H·psi GFLOP/s (FP64)"
+
+
+def build_workload(ctx=None, device=0):
+    from dmrgb200 import engine as E
+    from dmrgb200 import models as M
+    from dmrgb200 import mps as S
+
+    model = M.fermi_hubbard(L_SITES, t=1.0, U=4.0)
+    bonds = S.synthetic_bonds(model.phys, L_SITES, model.total_charge, M_BOND, RADIUS)
+    rng = np.random.default_rng(SEED)
+    tensors = S.random_mps(model.phys, bonds, rng)
+    i = L_SITES // 2 - 1
+    psi = S.SiteTensor(M.fuse_phys(model.phys, model.phys)[0], bonds[i], bonds[i + 2])
+    for b in range(len(psi.rp.rows)):
+        n = psi.rp.rows[b] * psi.rp.cols[b]
+        psi.data[psi.rp.offs[b]:psi.rp.offs[b] + n] = rng.random(n)
+    psi.data /= np.linalg.norm(psi.data)
+    return model, bonds, tensors, i, psi
+
+
+def sbuild_bytes(plan) -> int:
+    """Algorithmic bytes of the S build: every source element read once per
+    term, every S element of a line written once (FP64)."""
+    tot = 0
+    for c in range(len(plan["c_lb"])):
+        ls = int(plan["c_ls"][c])
+        for u in range(plan["c_unit"][c], plan["c_unit"][c + 1]):
+            ms = int(plan["u_ms"][u])
+            for ln in range(plan["u_line"][u], plan["u_line"][u + 1]):
+                nt = int(plan["l_term"][ln + 1] - plan["l_term"][ln])
+                tot += (nt + 1) * ls * ms * 8
+    return tot
+
+
+def hbm_peak() -> float:
+    try:
+        return float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"])
+    except (OSError, ValueError, KeyError):
+        return 6650.0
+
+
+def clocks_sampler(path):
+    cmd = ["nvidia-smi", "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+           "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+           "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+           "--format=csv,noheader,nounits", "-lms", "200"]
+    try:
+        return subprocess.Popen(cmd, stdout=open(path, "w"), stderr=subprocess.DEVNULL)
+    except (FileNotFoundError, OSError):
+        return None
+
+
+def clocks_summary(path, device):
+    sm, mx, reasons = [], None, set()
+    try:
+        for line in open(path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9 or f[0] != str(device):
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"), f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+    except OSError:
+        pass
+    return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+            "samples": len(sm)}
+
+
+def cpu_reference(model, bonds, tensors, i, psi, seconds=15.0, threads=None):
+    """The reference's CPU execution (oracle restatement) of the same H·psi."""
+    import oracle as O
+    from dmrgb200 import engine as E
+    from dmrgb200 import models as M
+
+    threads = threads or os.cpu_count() or 1
+    O.set_threads(threads)
+    Lidx = E.edge_bindex(model.symm, bonds[0])
+    Lval = Lidx.edge_values()
+    for p in range(i):
+        W = M.MPOHandle(model.mpo[p], model.symm)
+        sch, nidx = E.schedule_left_step(model.phys, bonds[p], bonds[p + 1], W, Lidx, True)
+        Lval = O.left_step(sch.plan, Lval, Lidx, tensors[p].data, tensors[p].left_paired(), nidx)
+        Lidx = nidx
+    Ridx = E.edge_bindex(model.symm, bonds[-1])
+    Rval = Ridx.edge_values()
+    for p in range(len(tensors) - 1, i + 1, -1):
+        W = M.MPOHandle(model.mpo[p], model.symm)
+        sch, nidx = E.schedule_right_step(model.phys, bonds[p], bonds[p + 1], W, Ridx, True)
+        Rval = O.right_step(sch.plan, Rval, Ridx, tensors[p].data, tensors[p].data, nidx)
+        Ridx = nidx
+    p12, _ = M.fuse_phys(model.phys, model.phys)
+    W12 = M.MPOHandle(M.twosite_mpo(model.mpo[i], model.mpo[i + 1], model.phys, model.phys), model.symm)
+    sch = E.schedule_hpsi(p12, bonds[i], bonds[i + 2], W12, Lidx, Ridx)
+    O.hpsi(sch.plan, Lval, Lidx, Rval, Ridx, psi.data)  # warm-up
+    n, t0 = 0, time.perf_counter()
+    while True:
+        y = O.hpsi(sch.plan, Lval, Lidx, Rval, Ridx, psi.data)
+        n += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or n >= 2000:
+            break
+    return {"gflops": sch.flops * n / el / 1e9, "calls": n, "seconds": el, "threads": threads,
+            "flops": sch.flops, "y": y, "boundaries": (Lidx, Lval, Ridx, Rval, sch)}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        model, bonds, tensors, i, psi = build_workload()
+        res = cpu_reference(model, bonds, tensors, i, psi, seconds=max(2.0, args.cpu_seconds))
+        per = res["seconds"] / res["calls"]
+        line = {"metric": METRIC, "value": res["gflops"], "unit": "GFLOP/s", "n_gpus": args.gpus,
+                "steps": res["calls"], "warmup": 1, "ms_per_step": per * 1e3, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "impl": "reference",
+                "config": {"workload": WORKLOAD, "sites": L_SITES, "bond_dim": M_BOND, "symmetry": "TwoU1",
+                           "parallelism": "cpu"},
+                "cpu_baseline": {"value": res["gflops"], "unit": "GFLOP/s", "cores": res["threads"],
+                                 "kind": "port",
+                                 "sample": f"{res['calls']} H·psi of the full workload in {res['seconds']:.1f} s"},
+                "e2e": {"value": res["gflops"], "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from dmrgb200 import _capi as capi
+    from dmrgb200 import engine as E
+
+    ctx = E.Context(local)
+    model, bonds, tensors, i, psi = build_workload()
+    sp = E.SiteProblem(ctx, model, tensors, bonds, i)
+    flops = sp.plan.flops
+    dev = torch.device(f"cuda:{local}")
+    stream = torch.cuda.current_stream(dev)
+    sh = stream.cuda_stream
+    xd = E.to_device(psi.data, local)
+    yd = torch.zeros_like(xd)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    for _ in range(args.warmup):
+        sp.plan.hpsi(xd.data_ptr(), yd.data_ptr(), capi.PREC_FP64, sh)
+    torch.cuda.synchronize(dev)
+
+    clk_path = tempfile.mktemp(suffix=".csv")
+    sampler = clocks_sampler(clk_path)
+    time.sleep(0.3)
+
+    # device-resident timing, one event pair per step, L2 flushed between steps
+    capi.check(capi.lib.dmrgb200_plan_set_timing(sp.plan.handle, 1), "set_timing")
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        ev[k][0].record(stream)
+        sp.plan.hpsi(xd.data_ptr(), yd.data_ptr(), capi.PREC_FP64, sh)
+        ev[k][1].record(stream)
+    torch.cuda.synchronize(dev)
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = sum(step_ms)
+    import ctypes as C
+    ms3 = (C.c_double * 3)()
+    fl3 = (C.c_uint64 * 3)()
+    calls = C.c_uint64()
+    capi.check(capi.lib.dmrgb200_plan_stage_times(sp.plan.handle, ms3, fl3, C.byref(calls)), "stage_times")
+    capi.check(capi.lib.dmrgb200_plan_set_timing(sp.plan.handle, 0), "set_timing")
+
+    # end to end through the C ABI with pinned host buffers
+    xh = torch.from_numpy(psi.data.copy()).pin_memory()
+    yh = torch.empty_like(xh).pin_memory()
+    for _ in range(2):
+        xd.copy_(xh, non_blocking=True)
+        sp.plan.hpsi(xd.data_ptr(), yd.data_ptr(), capi.PREC_FP64, sh)
+        yh.copy_(yd, non_blocking=True)
+    torch.cuda.synchronize(dev)
+    e2e_ms = []
+    for k in range(args.steps):
+        flush.fill_(float(k))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        xd.copy_(xh, non_blocking=True)
+        sp.plan.hpsi(xd.data_ptr(), yd.data_ptr(), capi.PREC_FP64, sh)
+        yh.copy_(yd, non_blocking=True)
+        b.record(stream)
+        b.synchronize()
+        e2e_ms.append(a.elapsed_time(b))
+    if sampler:
+        sampler.terminate()
+        sampler.wait()
+    clocks = clocks_summary(clk_path, local)
+
+    per_ms = total_ms / args.steps
+    e2e_per_ms = sum(e2e_ms) / len(e2e_ms)
+    if dist:
+        t = torch.tensor([per_ms, e2e_per_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        per_ms, e2e_per_ms = float(t[0]), float(t[1])
+    value = world * flops / (per_ms * 1e-3) / 1e9
+    e2e_value = world * flops / (e2e_per_ms * 1e-3) / 1e9
+
+    if rank == 0:
+        fp64_peak = C.c_double()
+        capi.check(capi.lib.dmrgb200_calibrate(0, C.byref(fp64_peak)), "calibrate")
+        nc = int(calls.value) or 1
+        stage_ms = [ms3[s] / nc for s in range(3)]
+        dom = int(np.argmax(stage_ms))
+        names = ["stage1_gemm", "sbuild", "stage3_gemm"]
+        if dom == 1:
+            sbytes = sbuild_bytes(sp.schedule.plan)
+            ach, peak, unit, bound = sbytes / (stage_ms[1] * 1e-3) / 1e9, hbm_peak(), "GB/s", "hbm"
+            peak_src = "MEASURED_PEAKS.json hbm_gbs"
+        else:
+            ach, peak, unit, bound = fl3[dom] / (stage_ms[dom] * 1e-3) / 1e12, fp64_peak.value, "TFLOP/s", "tensor"
+            peak_src = "measured FP64 DMMA loop on this GPU (dmrgb200_calibrate)"
+        traffic = None
+        tpath = ROOT / "profiles" / "traffic.json"
+        if tpath.exists():
+            try:
+                traffic = json.loads(tpath.read_text()).get(names[dom])
+            except (ValueError, OSError):
+                traffic = None
+        cpu = None
+        if os.environ.get("BENCH_SKIP_CPU") != "1":
+            res = cpu_reference(model, bonds, tensors, i, psi, seconds=args.cpu_seconds)
+            cpu = {"value": res["gflops"], "unit": "GFLOP/s", "cores": res["threads"], "kind": "port",
+                   "sample": f"{res['calls']} H·psi of the full workload in {res['seconds']:.1f} s "
+                             f"(oracle restatement of the reference CPU path, OpenMP + OpenBLAS)"}
+            y = yd.cpu().numpy()
+            err = float(np.linalg.norm(y - res["y"]) / np.linalg.norm(res["y"]))
+        else:
+            err = None
+        line = {
+            "metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": per_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sites": L_SITES, "bond_dim": M_BOND, "symmetry": "TwoU1",
+                       "psi_elements": int(sp.size), "flops_per_step": int(flops), "l2": "flushed (256 MiB write)",
+                       "parallelism": "replicas" if world > 1 else "single"},
+            "e2e": {"value": e2e_value, "unit": "GFLOP/s", "h2d_bytes_per_step": int(psi.data.nbytes),
+                    "d2h_bytes_per_step": int(psi.data.nbytes), "ms_per_step": e2e_per_ms},
+            "gpu_launches": 3 * args.steps,
+            "roofline": {"bound": bound, "kernel": names[dom], "achieved": ach, "peak": peak, "unit": unit,
+                         "frac": ach / peak if peak else None, "peak_source": peak_src, "traffic": traffic,
+                         "stage_ms": stage_ms, "stage_flops": [int(f) for f in fl3],
+                         "fp64_dmma_peak_tflops": fp64_peak.value},
+            "cpu_baseline": cpu,
+            "max_rel_err_vs_cpu": err,
+            "clocks": clocks,
+        }
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -166,6 +166,11 @@ dmrgb200_status dmrgb200_plan_create(dmrgb200_context_t ctx, const dmrgb200_plan
                                      dmrgb200_plan_t* out);
 dmrgb200_status dmrgb200_plan_destroy(dmrgb200_plan_t plan);
 
+/* Host-only structural validation of a plan description (no device needed):
+ * array lengths, index ranges, slice bounds and shape consistency.  Returns
+ * DMRGB200_INVALID_PLAN with a message for inconsistent input. */
+dmrgb200_status dmrgb200_plan_validate(const dmrgb200_plan_desc* desc);
+
 /* Algorithmic FP64 flop count of one execution, the reference's formula
  * (Cohort::n_flops tasks.cpp:388-398 + MPSBlock::n_flops :777-796). */
 dmrgb200_status dmrgb200_plan_flops(dmrgb200_plan_t plan, uint64_t* flops);
@@ -180,6 +185,20 @@ dmrgb200_status dmrgb200_plan_scratch_bytes(dmrgb200_plan_t plan, uint64_t* byte
  * ietl::mult (ietl_interface_dv.h:112-118). */
 dmrgb200_status dmrgb200_hpsi(dmrgb200_plan_t plan, const double* x, double* y, dmrgb200_precision prec,
                               void* cuda_stream);
+
+/* Per-stage timing of H·psi executions: when enabled, every dmrgb200_hpsi call
+ * records CUDA events around its stages on the call's stream.
+ * dmrgb200_plan_stage_times synchronises the last recorded events and returns
+ * the accumulated milliseconds and the number of timed calls; stage 0 = T
+ * GEMMs (create_T), 1 = S build (create_s_r), 2 = cohort contraction
+ * (contract).  Algorithmic flops per stage per call are returned in flops[3]. */
+dmrgb200_status dmrgb200_plan_set_timing(dmrgb200_plan_t plan, int enable);
+dmrgb200_status dmrgb200_plan_stage_times(dmrgb200_plan_t plan, double ms[3], uint64_t flops[3], uint64_t* calls);
+
+/* Roofline calibration on the current device: what = 0 measures the FP64
+ * tensor-core (DMMA) rate of a register-resident loop in TFLOP/s.  Used as the
+ * denominator of the native-FP64 roofline. */
+dmrgb200_status dmrgb200_calibrate(int what, double* value);
 
 /* ---- boundary steps on a flattened plan --------------------------------- */
 /* Execute a LEFT_STEP / RIGHT_STEP plan.  ket: right-paired device tensor

@@ -54,6 +54,24 @@ struct dmrgb200_plan_s {
     double* S = nullptr;
     std::vector<uint64_t> stage1_bnd, stage3_bnd;
     int device = 0;
+    // per-stage timing
+    bool timing = false;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    bool pending = false;
+    double stage_ms[3] = {0, 0, 0};
+    uint64_t timed_calls = 0;
+
+    void collect() {
+        if (!pending) return;
+        cudaEventSynchronize(ev[3]);
+        for (int i = 0; i < 3; ++i) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
+            stage_ms[i] += ms;
+        }
+        ++timed_calls;
+        pending = false;
+    }
 };
 
 namespace {
@@ -104,6 +122,52 @@ template <class T>
 std::vector<T> vec(const T* p, size_t n) {
     if (n && !p) throw std::runtime_error("null array in plan description");
     return std::vector<T>(p, p + n);
+}
+
+void desc_to_flat(const dmrgb200_plan_desc* d, FlatPlan& f) {
+    f.kind = d->kind;
+    f.g_t = vec(d->g_t, size_t(d->n_groups) + 1);
+    f.g_c = vec(d->g_c, size_t(d->n_groups) + 1);
+    f.in_rows = vec(d->in_rows, d->n_in_blocks);
+    f.in_cols = vec(d->in_cols, d->n_in_blocks);
+    f.in_off = vec(d->in_off, d->n_in_blocks);
+    f.in_size = d->in_size;
+    f.out_rows = vec(d->out_rows, d->n_out_blocks);
+    f.out_cols = vec(d->out_cols, d->n_out_blocks);
+    f.out_off = vec(d->out_off, d->n_out_blocks);
+    f.out_size = d->out_size;
+    f.t_lb = vec(d->t_lb, d->n_t);
+    f.t_col = vec(d->t_col, d->n_t);
+    f.t_ci = vec(d->t_ci, d->n_t);
+    f.t_trans = vec(d->t_trans, d->n_t);
+    f.t_nb = vec(d->t_nb, d->n_t);
+    f.t_brows = vec(d->t_brows, d->n_t);
+    f.t_bcols = vec(d->t_bcols, d->n_t);
+    if (d->kind == DMRGB200_PLAN_LEFT_STEP) f.t_width = vec(d->t_width, d->n_t);
+    f.c_lb = vec(d->c_lb, d->n_cohorts);
+    f.c_rb = vec(d->c_rb, d->n_cohorts);
+    f.c_ls = vec(d->c_ls, d->n_cohorts);
+    f.c_rs = vec(d->c_rs, d->n_cohorts);
+    f.c_nsrows = vec(d->c_nsrows, d->n_cohorts);
+    f.c_stripe = vec(d->c_stripe, d->n_cohorts);
+    f.c_unit = vec(d->c_unit, size_t(d->n_cohorts) + 1);
+    if (d->kind == DMRGB200_PLAN_HPSI) {
+        f.c_ci = vec(d->c_ci, d->n_cohorts);
+        f.c_trans = vec(d->c_trans, d->n_cohorts);
+        f.c_out_ci.assign(d->n_cohorts, 0);
+    } else {
+        f.c_ci.assign(d->n_cohorts, 0);
+        f.c_trans.assign(d->n_cohorts, 0);
+        f.c_out_ci = vec(d->c_out_ci, d->n_cohorts);
+    }
+    f.u_offset = vec(d->u_offset, d->n_units);
+    f.u_ms = vec(d->u_ms, d->n_units);
+    f.u_line = vec(d->u_line, size_t(d->n_units) + 1);
+    f.l_b1 = vec(d->l_b1, d->n_lines);
+    f.l_term = vec(d->l_term, size_t(d->n_lines) + 1);
+    f.term_alpha = vec(d->term_alpha, d->n_terms);
+    f.term_t = vec(d->term_t, d->n_terms);
+    f.term_col = vec(d->term_col, d->n_terms);
 }
 
 dmrgb200_status alloc_scratch(dmrgb200_plan_s* p) {
@@ -235,50 +299,7 @@ dmrgb200_status dmrgb200_plan_create(dmrgb200_context_t ctx, const dmrgb200_plan
     DMRGB200_TRY
     if (!ctx || !d || !out) return fail(DMRGB200_INVALID_ARGUMENT, "null argument");
     auto p = std::make_unique<dmrgb200_plan_s>();
-    FlatPlan& f = p->flat;
-    f.kind = d->kind;
-    f.g_t = vec(d->g_t, size_t(d->n_groups) + 1);
-    f.g_c = vec(d->g_c, size_t(d->n_groups) + 1);
-    f.in_rows = vec(d->in_rows, d->n_in_blocks);
-    f.in_cols = vec(d->in_cols, d->n_in_blocks);
-    f.in_off = vec(d->in_off, d->n_in_blocks);
-    f.in_size = d->in_size;
-    f.out_rows = vec(d->out_rows, d->n_out_blocks);
-    f.out_cols = vec(d->out_cols, d->n_out_blocks);
-    f.out_off = vec(d->out_off, d->n_out_blocks);
-    f.out_size = d->out_size;
-    f.t_lb = vec(d->t_lb, d->n_t);
-    f.t_col = vec(d->t_col, d->n_t);
-    f.t_ci = vec(d->t_ci, d->n_t);
-    f.t_trans = vec(d->t_trans, d->n_t);
-    f.t_nb = vec(d->t_nb, d->n_t);
-    f.t_brows = vec(d->t_brows, d->n_t);
-    f.t_bcols = vec(d->t_bcols, d->n_t);
-    if (d->kind == DMRGB200_PLAN_LEFT_STEP) f.t_width = vec(d->t_width, d->n_t);
-    f.c_lb = vec(d->c_lb, d->n_cohorts);
-    f.c_rb = vec(d->c_rb, d->n_cohorts);
-    f.c_ls = vec(d->c_ls, d->n_cohorts);
-    f.c_rs = vec(d->c_rs, d->n_cohorts);
-    f.c_nsrows = vec(d->c_nsrows, d->n_cohorts);
-    f.c_stripe = vec(d->c_stripe, d->n_cohorts);
-    f.c_unit = vec(d->c_unit, size_t(d->n_cohorts) + 1);
-    if (d->kind == DMRGB200_PLAN_HPSI) {
-        f.c_ci = vec(d->c_ci, d->n_cohorts);
-        f.c_trans = vec(d->c_trans, d->n_cohorts);
-        f.c_out_ci.assign(d->n_cohorts, 0);
-    } else {
-        f.c_ci.assign(d->n_cohorts, 0);
-        f.c_trans.assign(d->n_cohorts, 0);
-        f.c_out_ci = vec(d->c_out_ci, d->n_cohorts);
-    }
-    f.u_offset = vec(d->u_offset, d->n_units);
-    f.u_ms = vec(d->u_ms, d->n_units);
-    f.u_line = vec(d->u_line, size_t(d->n_units) + 1);
-    f.l_b1 = vec(d->l_b1, d->n_lines);
-    f.l_term = vec(d->l_term, size_t(d->n_lines) + 1);
-    f.term_alpha = vec(d->term_alpha, d->n_terms);
-    f.term_t = vec(d->term_t, d->n_terms);
-    f.term_col = vec(d->term_col, d->n_terms);
+    desc_to_flat(d, p->flat);
     if (d->kind == DMRGB200_PLAN_HPSI) {
         p->stage3_bnd = view_ptrs(left);
         p->stage1_bnd = view_ptrs(other);
@@ -291,9 +312,32 @@ dmrgb200_status dmrgb200_plan_create(dmrgb200_context_t ctx, const dmrgb200_plan
     DMRGB200_CATCH
 }
 
+dmrgb200_status dmrgb200_calibrate(int what, double* value) {
+    if (!value || what != 0) return fail(DMRGB200_INVALID_ARGUMENT, "unknown calibration");
+    *value = calibrate_fp64_tflops();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "calibration");
+    return DMRGB200_OK;
+}
+
+dmrgb200_status dmrgb200_plan_validate(const dmrgb200_plan_desc* d) {
+    DMRGB200_TRY
+    if (!d) return fail(DMRGB200_INVALID_ARGUMENT, "null plan description");
+    if (d->kind < DMRGB200_PLAN_HPSI || d->kind > DMRGB200_PLAN_RIGHT_STEP)
+        return fail(DMRGB200_INVALID_PLAN, "unknown plan kind");
+    FlatPlan f;
+    desc_to_flat(d, f);
+    std::string err = f.validate();
+    if (!err.empty()) return fail(DMRGB200_INVALID_PLAN, err);
+    return DMRGB200_OK;
+    DMRGB200_CATCH
+}
+
 dmrgb200_status dmrgb200_plan_destroy(dmrgb200_plan_t plan) {
     if (!plan) return DMRGB200_OK;
     if (plan->compiled) free_program(plan->prog);
+    for (auto& e : plan->ev)
+        if (e) cudaEventDestroy(e);
     cudaFree(plan->T);
     cudaFree(plan->S);
     delete plan;
@@ -317,9 +361,35 @@ dmrgb200_status dmrgb200_hpsi(dmrgb200_plan_t plan, const double* x, double* y, 
     if (!plan || !x || !y) return fail(DMRGB200_INVALID_ARGUMENT, "null argument");
     if (plan->flat.kind != KIND_HPSI) return fail(DMRGB200_INVALID_PLAN, "plan is not an H psi plan");
     if (prec != DMRGB200_PREC_FP64) return fail(DMRGB200_NOT_SUPPORTED, "precision not available in this build");
+    if (plan->timing) plan->collect();
     cudaError_t e = run_program(plan->prog, reinterpret_cast<uint64_t>(x), reinterpret_cast<uint64_t>(y), plan->T,
-                                plan->S, static_cast<cudaStream_t>(cuda_stream));
+                                plan->S, static_cast<cudaStream_t>(cuda_stream), plan->timing ? plan->ev : nullptr);
     if (e != cudaSuccess) return cuda_fail(e, "hpsi launch");
+    if (plan->timing) plan->pending = true;
+    return DMRGB200_OK;
+}
+
+dmrgb200_status dmrgb200_plan_set_timing(dmrgb200_plan_t plan, int enable) {
+    if (!plan) return fail(DMRGB200_INVALID_ARGUMENT, "null plan");
+    if (enable && !plan->ev[0])
+        for (auto& e : plan->ev) {
+            cudaError_t r = cudaEventCreate(&e);
+            if (r != cudaSuccess) return cuda_fail(r, "event creation");
+        }
+    plan->collect();
+    plan->timing = enable != 0;
+    plan->stage_ms[0] = plan->stage_ms[1] = plan->stage_ms[2] = 0.0;
+    plan->timed_calls = 0;
+    return DMRGB200_OK;
+}
+
+dmrgb200_status dmrgb200_plan_stage_times(dmrgb200_plan_t plan, double ms[3], uint64_t flops[3], uint64_t* calls) {
+    if (!plan) return fail(DMRGB200_INVALID_ARGUMENT, "null plan");
+    plan->collect();
+    if (ms)
+        for (int i = 0; i < 3; ++i) ms[i] = plan->stage_ms[i];
+    if (flops) plan->flat.stage_flops(flops);
+    if (calls) *calls = plan->timed_calls;
     return DMRGB200_OK;
 }
 

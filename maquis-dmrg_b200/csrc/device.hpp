@@ -94,9 +94,11 @@ cudaError_t upload_program(DeviceProgram& prog);
 void free_program(DeviceProgram& prog);
 
 // Launch the three stages on a stream; T and S are the scratch buffers.
+// ev (optional): four events recorded before stage 1 and after stages 1, 2, 3.
 cudaError_t run_program(DeviceProgram const& prog, uint64_t in, uint64_t out, double* T, double* S,
-                        cudaStream_t stream);
+                        cudaStream_t stream, cudaEvent_t const* ev = nullptr);
 
 int device_sm_count();
+double calibrate_fp64_tflops();
 
 }  // namespace dmrgb200

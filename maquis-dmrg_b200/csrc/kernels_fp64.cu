@@ -146,6 +146,22 @@ __global__ void __launch_bounds__(256) sbuild_lines(const DevSLine* __restrict__
     }
 }
 
+// Register-resident DMMA loop for the FP64 tensor-core rate (calibration).
+__global__ void __launch_bounds__(128) dmma_rate_loop(int iters, double* sink) {
+    double acc[8][2];
+    double a = 1.0 + threadIdx.x * 1e-9, b = 1.0 - threadIdx.x * 1e-9;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) acc[i][0] = acc[i][1] = 0.0;
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) dmma(acc[i][0], acc[i][1], a, b);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) s += acc[i][0] + acc[i][1];
+    if (s == 1.2345) sink[threadIdx.x] = s;
+}
+
 // --- host-side lowering ---------------------------------------------------------
 
 void add_tiles(GemmList& gl, uint32_t prob, uint32_t nbatch) {
@@ -378,6 +394,29 @@ void free_program(DeviceProgram& prog) {
     prog.d_terms = nullptr;
 }
 
+double calibrate_fp64_tflops() {
+    const int sms = device_sm_count();
+    double* sink = nullptr;
+    cudaMalloc(&sink, 128 * sizeof(double));
+    const int iters = 20000, blocks = sms * 8;
+    dmma_rate_loop<<<blocks, 128>>>(1000, sink);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0);
+    dmma_rate_loop<<<blocks, 128>>>(iters, sink);
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(sink);
+    // one m8n8k4 DMMA = 8*8*4 FMA = 512 flops per warp instruction
+    double flops = double(blocks) * 4 /*warps*/ * iters * 8 * 512.0;
+    return ms > 0 ? flops / (ms * 1e-3) / 1e12 : 0.0;
+}
+
 int device_sm_count() {
     int dev = 0, n = 0;
     cudaGetDevice(&dev);
@@ -386,7 +425,7 @@ int device_sm_count() {
 }
 
 cudaError_t run_program(DeviceProgram const& prog, uint64_t in, uint64_t out, double* T, double* S,
-                        cudaStream_t stream) {
+                        cudaStream_t stream, cudaEvent_t const* ev) {
     Bases bs{};
     bs.b[BUF_IN] = in;
     bs.b[BUF_OUT] = out;
@@ -394,10 +433,12 @@ cudaError_t run_program(DeviceProgram const& prog, uint64_t in, uint64_t out, do
     bs.b[BUF_S] = reinterpret_cast<uint64_t>(S);
     bs.b[BUF_ABS] = 0;
     const int sms = device_sm_count();
+    if (ev) cudaEventRecord(ev[0], stream);
     if (prog.n_t1) {
         uint32_t grid = std::min<uint32_t>(prog.n_t1, uint32_t(sms) * 4);
         gemm_f64_grouped<<<grid, NTHREADS, 0, stream>>>(prog.d_p1, prog.d_s1, prog.d_t1, prog.n_t1, bs);
     }
+    if (ev) cudaEventRecord(ev[1], stream);
     if (prog.s_elems) {
         cudaError_t e = cudaMemsetAsync(S, 0, prog.s_elems * sizeof(double), stream);
         if (e != cudaSuccess) return e;
@@ -406,10 +447,12 @@ cudaError_t run_program(DeviceProgram const& prog, uint64_t in, uint64_t out, do
         uint32_t grid = std::min<uint32_t>(prog.n_lines, uint32_t(sms) * 8);
         sbuild_lines<<<grid, 256, 0, stream>>>(prog.d_lines, prog.d_terms, prog.n_lines, S, T);
     }
+    if (ev) cudaEventRecord(ev[2], stream);
     if (prog.n_t3) {
         uint32_t grid = std::min<uint32_t>(prog.n_t3, uint32_t(sms) * 4);
         gemm_f64_grouped<<<grid, NTHREADS, 0, stream>>>(prog.d_p3, prog.d_s3, prog.d_t3, prog.n_t3, bs);
     }
+    if (ev) cudaEventRecord(ev[3], stream);
     return cudaGetLastError();
 }
 

@@ -23,6 +23,20 @@ uint64_t FlatPlan::flops() const {
     return f;
 }
 
+void FlatPlan::stage_flops(uint64_t out[3]) const {
+    out[0] = out[1] = out[2] = 0;
+    for (uint32_t t = 0; t < n_t(); ++t) {
+        uint64_t csz = uint64_t(t_nb[t]) * t_brows[t] * t_bcols[t];
+        uint64_t m = (kind == KIND_LEFT) ? t_width[t] : in_rows[t_lb[t]];
+        out[0] += 2 * m * csz;
+    }
+    for (uint32_t c = 0; c < n_cohorts(); ++c) {
+        out[2] += 2ull * c_rs[c] * c_ls[c] * c_nsrows[c] * c_stripe[c];
+        for (uint32_t u = c_unit[c]; u < c_unit[c + 1]; ++u)
+            out[1] += 2ull * c_ls[c] * u_ms[u] * (l_term[u_line[u + 1]] - l_term[u_line[u]]);
+    }
+}
+
 std::string FlatPlan::validate() const {
     std::ostringstream e;
     auto bad = [&](const char* what, uint64_t i) {

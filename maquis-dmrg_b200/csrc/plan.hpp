@@ -44,6 +44,8 @@ struct FlatPlan {
 
     // reference flop formula (tasks.cpp:388-398, :777-796)
     uint64_t flops() const;
+    // the same formula split into stage 1 (T), stage 2 (S build), stage 3 (contract)
+    void stage_flops(uint64_t out[3]) const;
     // T rows / T-block columns per task, following the plan kind
     uint64_t t_rows(uint32_t t) const { return kind == KIND_LEFT ? t_brows[t] : in_rows[t_lb[t]]; }
     uint64_t t_block_cols(uint32_t t) const { return kind == KIND_LEFT ? t_width[t] : t_bcols[t]; }

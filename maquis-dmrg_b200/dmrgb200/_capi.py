@@ -94,9 +94,13 @@ _sigs = {
     "dmrgb200_plan_create": ([vp, C.POINTER(PlanDesc), C.POINTER(BoundaryView), C.POINTER(BoundaryView),
                               C.POINTER(vp)], C.c_int),
     "dmrgb200_plan_destroy": ([vp], C.c_int),
+    "dmrgb200_plan_validate": ([C.POINTER(PlanDesc)], C.c_int),
+    "dmrgb200_calibrate": ([C.c_int, f64p], C.c_int),
     "dmrgb200_plan_flops": ([vp, u64p], C.c_int),
     "dmrgb200_plan_scratch_bytes": ([vp, u64p], C.c_int),
     "dmrgb200_hpsi": ([vp, vp, vp, C.c_int, vp], C.c_int),
+    "dmrgb200_plan_set_timing": ([vp, C.c_int], C.c_int),
+    "dmrgb200_plan_stage_times": ([vp, f64p, u64p, u64p], C.c_int),
     "dmrgb200_step_execute": ([vp, vp, vp, C.POINTER(BoundaryView), vp], C.c_int),
     "dmrgb200_mpo_create": ([C.POINTER(MpoDesc), C.POINTER(vp)], C.c_int),
     "dmrgb200_mpo_destroy": ([vp], C.c_int),

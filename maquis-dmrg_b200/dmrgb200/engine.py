@@ -193,3 +193,79 @@ class DevicePlan:
         if getattr(self, "handle", None):
             capi.lib.dmrgb200_plan_destroy(self.handle)
             self.handle = None
+
+
+# ---- device chains ---------------------------------------------------------------
+
+def _torch():
+    import torch
+    return torch
+
+
+def to_device(a: np.ndarray, device: int = 0):
+    torch = _torch()
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(f"cuda:{device}")
+
+
+def device_left_step(ctx: Context, phys, left, right, mpo: MPOHandle, Lidx: BIndex, Lbuf, ket_rp, bra_lp,
+                     symmetric=True, stream: int = 0):
+    """overlap_mpo_left_step on the device: returns (new index, new device buffer)."""
+    torch = _torch()
+    sched, nidx = schedule_left_step(phys, left, right, mpo, Lidx, symmetric)
+    plan = DevicePlan(ctx, sched.plan, left_addr=Lidx.cohort_addresses(Lbuf.data_ptr()))
+    out = torch.zeros(max(nidx.n_elems, 1), dtype=torch.float64, device=Lbuf.device)
+    plan.step(ket_rp.data_ptr(), bra_lp.data_ptr(), nidx.cohort_addresses(out.data_ptr()), stream)
+    return nidx, out
+
+
+def device_right_step(ctx: Context, phys, left, right, mpo: MPOHandle, Ridx: BIndex, Rbuf, ket_rp, bra_rp,
+                      symmetric=True, stream: int = 0):
+    """overlap_mpo_right_step on the device: returns (new index, new device buffer)."""
+    torch = _torch()
+    sched, nidx = schedule_right_step(phys, left, right, mpo, Ridx, symmetric)
+    plan = DevicePlan(ctx, sched.plan, other_addr=Ridx.cohort_addresses(Rbuf.data_ptr()))
+    out = torch.zeros(max(nidx.n_elems, 1), dtype=torch.float64, device=Rbuf.device)
+    plan.step(ket_rp.data_ptr(), bra_rp.data_ptr(), nidx.cohort_addresses(out.data_ptr()), stream)
+    return nidx, out
+
+
+class SiteProblem:
+    """H·psi at sites (i, i+1) of a chain with device-resident boundaries.
+
+    Boundaries are built by device boundary steps from the chain ends with the
+    given site tensors (ket = bra), as the optimizer's boundary caches are
+    (optimize.h:134-195)."""
+
+    def __init__(self, ctx: Context, model, tensors, bonds, i: int, symmetric=True, stream: int = 0):
+        from . import models as M
+        torch = _torch()
+        self.ctx, self.model, self.i = ctx, model, i
+        dev = ctx.device
+        L = len(tensors)
+        Lidx = edge_bindex(model.symm, bonds[0])
+        Lbuf = to_device(Lidx.edge_values(), dev)
+        for p in range(i):
+            W = M.MPOHandle(model.mpo[p], model.symm)
+            t = tensors[p]
+            Lidx, Lbuf = device_left_step(ctx, model.phys, bonds[p], bonds[p + 1], W, Lidx, Lbuf,
+                                          to_device(t.data, dev), to_device(t.left_paired(), dev), symmetric, stream)
+        Ridx = edge_bindex(model.symm, bonds[L])
+        Rbuf = to_device(Ridx.edge_values(), dev)
+        for p in range(L - 1, i + 1, -1):
+            W = M.MPOHandle(model.mpo[p], model.symm)
+            t = tensors[p]
+            td = to_device(t.data, dev)
+            Ridx, Rbuf = device_right_step(ctx, model.phys, bonds[p], bonds[p + 1], W, Ridx, Rbuf, td, td,
+                                           symmetric, stream)
+        self.Lidx, self.Lbuf, self.Ridx, self.Rbuf = Lidx, Lbuf, Ridx, Rbuf
+        self.p12, _ = M.fuse_phys(model.phys, model.phys)
+        self.W12 = M.MPOHandle(M.twosite_mpo(model.mpo[i], model.mpo[i + 1], model.phys, model.phys), model.symm)
+        self.left, self.right = bonds[i], bonds[i + 2]
+        self.schedule = schedule_hpsi(self.p12, self.left, self.right, self.W12, Lidx, Ridx)
+        self.plan = DevicePlan(ctx, self.schedule.plan, left_addr=Lidx.cohort_addresses(Lbuf.data_ptr()),
+                               other_addr=Ridx.cohort_addresses(Rbuf.data_ptr()))
+        self.size = int(self.schedule.plan["in_size"])
+        torch.cuda.synchronize(dev)
+
+    def hpsi(self, x, y, prec: int = capi.PREC_FP64, stream: int = 0):
+        self.plan.hpsi(x.data_ptr(), y.data_ptr(), prec, stream)

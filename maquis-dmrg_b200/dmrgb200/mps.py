@@ -152,22 +152,34 @@ def allowed_sectors(phys, L, total, Mmax):
     return out
 
 
-def synthetic_sectors(phys, L, total, m, i, width=None, rng=None):
+def synthetic_bonds(phys, L, total, m, radius=3.5):
+    """synthetic_sectors for every bond 0..L."""
+    allowed = allowed_sectors(phys, L, total, 10 ** 9)
+    return [synthetic_sectors(phys, L, total, m, i, radius, allowed) for i in range(L + 1)]
+
+
+def synthetic_sectors(phys, L, total, m, i, radius=3.5, allowed_all=None):
     """Bond-i sectors of a synthetic state of total bond dimension about m.
 
-    The allowed charges of bond i get weights exp(-|q - q_mean|^2 / (2 w^2)),
-    q_mean = total * i / L (the mean charge of the left block) and
-    w = width or sqrt(i (L - i) / L) / 2; each sector receives a share of m
-    proportional to its weight, at least 1, capped by the allowed multiplicity
-    (the exact Schmidt-rank bound), and sectors with a share below 0.5 are
-    dropped.  This mimics the charge distribution of a DMRG ground state."""
-    allowed = dict(allowed_sectors(phys, L, total, 10 ** 9)[i])
+    Converged DMRG states concentrate their Schmidt spectrum on charges near the
+    mean charge of the left block, with the number of kept states falling off
+    roughly quadratically in the charge deviation.  Here every allowed charge q
+    of bond i gets the weight max(0, 1 - |q - q_mean|^2 / radius^2), with
+    q_mean = total * i / L (radius in units of the charge lattice); each sector
+    receives a share of m proportional to its weight, at least 1, capped by the
+    exact multiplicity bound of allowed_sectors, and sectors whose share is
+    below 0.5 are dropped."""
+    if allowed_all is None:
+        allowed_all = allowed_sectors(phys, L, total, 10 ** 9)
+    allowed = dict(allowed_all[i])
     if i == 0 or i == L:
         return sorted(allowed.items())
     qm = (total[0] * i / L, total[1] * i / L)
-    w = width if width is not None else max(math.sqrt(i * (L - i) / L) / 2.0, 0.5)
-    wts = {c: math.exp(-((c[0] - qm[0]) ** 2 + (c[1] - qm[1]) ** 2) / (2 * w * w)) for c in allowed}
+    wts = {c: max(0.0, 1.0 - ((c[0] - qm[0]) ** 2 + (c[1] - qm[1]) ** 2) / radius ** 2) for c in allowed}
     tot = sum(wts.values())
+    if tot == 0:
+        best = min(allowed, key=lambda c: (c[0] - qm[0]) ** 2 + (c[1] - qm[1]) ** 2)
+        return [(best, int(min(allowed[best], m)))]
     out = []
     for c in sorted(allowed):
         share = m * wts[c] / tot

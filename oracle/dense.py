@@ -126,3 +126,34 @@ def embedding(mps_left, mps_right, phys1, phys2, left, right, p12) -> np.ndarray
         P.append(mps_dense(lefts + [core] + rights))
     dim = len(next(p for p in P if p is not None))
     return np.stack([p if p is not None else np.zeros(dim) for p in P], axis=1)
+
+
+def mpo_dense(model: M.Model, L: int) -> np.ndarray:
+    """Dense H from the site MPOs: contract W_0 ... W_{L-1} over the bond indices."""
+    d = sum(dd for _, dd in model.phys)
+    offs = {}
+    o = 0
+    for c, dd in model.phys:
+        offs[c] = o
+        o += dd
+
+    def dense_op(op):
+        O = np.zeros((d, d))
+        for (cin, cout), B in op.blocks.items():
+            for i in range(B.shape[0]):
+                for j in range(B.shape[1]):
+                    O[offs[cout] + j, offs[cin] + i] += B[i, j]
+        return O
+
+    # env[b] = operator on sites < p ending in bond state b
+    env = {0: np.eye(1)}
+    for p in range(L):
+        W = model.mpo[p]
+        new = {}
+        for (b1, b2), terms in W.terms.items():
+            if b1 not in env:
+                continue
+            O = sum(sc * dense_op(op) for op, sc in terms)
+            new[b2] = new.get(b2, 0) + np.kron(env[b1], O)
+        env = new
+    return env[0]

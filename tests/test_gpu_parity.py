@@ -1,0 +1,130 @@
+"""GPU parity: the sm_100a kernels behind the C ABI against the CPU oracle on
+identical inputs (FP64: relative error <= 1e-12 per H·psi and per boundary)."""
+import numpy as np
+import pytest
+
+from dmrgb200 import engine as E
+from dmrgb200 import models as M
+from helpers import OracleChain, make_chain, random_psi
+
+import oracle as O
+
+TOL = 1e-12
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    assert torch.cuda.is_available(), "GPU tests need a CUDA device"
+    return E.Context(0)
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def _gpu_hpsi(ctx, ch, x):
+    Lb, Rb = E.to_device(ch.Lval), E.to_device(ch.Rval)
+    plan = E.DevicePlan(ctx, ch.sched.plan, left_addr=ch.Lidx.cohort_addresses(Lb.data_ptr()),
+                        other_addr=ch.Ridx.cohort_addresses(Rb.data_ptr()))
+    xd = E.to_device(x)
+    yd = torch.zeros_like(xd)
+    plan.hpsi(xd.data_ptr(), yd.data_ptr())
+    torch.cuda.synchronize()
+    return yd.cpu().numpy(), (plan, Lb, Rb, xd, yd)
+
+
+@pytest.mark.parametrize("name,L,Mmax", [("heisenberg", 8, 6), ("hubbard", 6, 8), ("bose", 6, 4)])
+def test_hpsi_every_site(ctx, name, L, Mmax):
+    model, bonds, tensors, rng = make_chain(name, L, Mmax, seed=21)
+    for i in range(L - 1):
+        ch = OracleChain(model, bonds, tensors, i)
+        x = random_psi(ch.p12, ch.left, ch.right, rng).data
+        y, _ = _gpu_hpsi(ctx, ch, x)
+        assert _rel(y, ch.hpsi(x)) <= TOL, (name, i)
+
+
+@pytest.mark.parametrize("name,L,m", [("hubbard", 16, 96), ("heisenberg", 24, 64), ("bose", 12, 64)])
+def test_hpsi_synthetic_bond_dimension(ctx, name, L, m):
+    model, bonds, tensors, rng = make_chain(name, L, 0, seed=7, synthetic_m=m)
+    ch = OracleChain(model, bonds, tensors, L // 2 - 1)
+    x = random_psi(ch.p12, ch.left, ch.right, rng).data
+    y, _ = _gpu_hpsi(ctx, ch, x)
+    assert _rel(y, ch.hpsi(x)) <= TOL
+
+
+def test_hpsi_bitwise_reproducible(ctx):
+    model, bonds, tensors, rng = make_chain("hubbard", 12, 0, seed=4, synthetic_m=64)
+    ch = OracleChain(model, bonds, tensors, 5)
+    x = random_psi(ch.p12, ch.left, ch.right, rng).data
+    y1, keep = _gpu_hpsi(ctx, ch, x)
+    plan, Lb, Rb, xd, yd = keep
+    yd.zero_()
+    plan.hpsi(xd.data_ptr(), yd.data_ptr())
+    torch.cuda.synchronize()
+    assert np.array_equal(y1, yd.cpu().numpy())
+
+
+@pytest.mark.parametrize("symmetric", [True, False])
+def test_boundary_steps_match_oracle(ctx, symmetric):
+    model, bonds, tensors, rng = make_chain("hubbard", 10, 0, seed=9, synthetic_m=48)
+    # left chain on the device vs the oracle, step by step
+    Lidx = E.edge_bindex(model.symm, bonds[0])
+    Lval = Lidx.edge_values()
+    Lbuf = E.to_device(Lval)
+    for p in range(6):
+        W = M.MPOHandle(model.mpo[p], model.symm)
+        t = tensors[p]
+        sch, nidx = E.schedule_left_step(model.phys, bonds[p], bonds[p + 1], W, Lidx, symmetric)
+        ref = O.left_step(sch.plan, Lval, Lidx, t.data, t.left_paired(), nidx)
+        nidx2, Lbuf = E.device_left_step(ctx, model.phys, bonds[p], bonds[p + 1], W, Lidx, Lbuf,
+                                         E.to_device(t.data), E.to_device(t.left_paired()), symmetric)
+        got = Lbuf.cpu().numpy()[:nidx.n_elems]
+        assert _rel(got, ref) <= TOL, p
+        Lidx, Lval = nidx2, ref
+    Ridx = E.edge_bindex(model.symm, bonds[10])
+    Rval = Ridx.edge_values()
+    Rbuf = E.to_device(Rval)
+    for p in range(9, 4, -1):
+        W = M.MPOHandle(model.mpo[p], model.symm)
+        t = tensors[p]
+        sch, nidx = E.schedule_right_step(model.phys, bonds[p], bonds[p + 1], W, Ridx, symmetric)
+        ref = O.right_step(sch.plan, Rval, Ridx, t.data, t.data, nidx)
+        td = E.to_device(t.data)
+        nidx2, Rbuf = E.device_right_step(ctx, model.phys, bonds[p], bonds[p + 1], W, Ridx, Rbuf, td, td, symmetric)
+        got = Rbuf.cpu().numpy()[:nidx.n_elems]
+        assert _rel(got, ref) <= TOL, p
+        Ridx, Rval = nidx2, ref
+
+
+def test_site_problem_end_to_end(ctx):
+    """Boundaries and H·psi entirely on the device vs the oracle chain."""
+    model, bonds, tensors, rng = make_chain("hubbard", 12, 0, seed=13, synthetic_m=64)
+    sp = E.SiteProblem(ctx, model, tensors, bonds, 5)
+    ch = OracleChain(model, bonds, tensors, 5)
+    x = random_psi(ch.p12, ch.left, ch.right, rng).data
+    xd = E.to_device(x)
+    yd = torch.zeros_like(xd)
+    sp.hpsi(xd, yd)
+    torch.cuda.synchronize()
+    assert _rel(yd.cpu().numpy(), ch.hpsi(x)) <= TOL
+
+
+def test_stage_timing_reports(ctx):
+    model, bonds, tensors, rng = make_chain("hubbard", 12, 0, seed=1, synthetic_m=64)
+    ch = OracleChain(model, bonds, tensors, 5)
+    x = random_psi(ch.p12, ch.left, ch.right, rng).data
+    _, keep = _gpu_hpsi(ctx, ch, x)
+    plan, Lb, Rb, xd, yd = keep
+    import ctypes as C
+    from dmrgb200 import _capi as capi
+    capi.check(capi.lib.dmrgb200_plan_set_timing(plan.handle, 1), "timing")
+    for _ in range(3):
+        plan.hpsi(xd.data_ptr(), yd.data_ptr())
+    ms = (C.c_double * 3)()
+    fl = (C.c_uint64 * 3)()
+    calls = C.c_uint64()
+    capi.check(capi.lib.dmrgb200_plan_stage_times(plan.handle, ms, fl, C.byref(calls)), "stage_times")
+    assert calls.value == 3 and all(v > 0 for v in ms) and sum(fl) == plan.flops

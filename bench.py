@@ -153,6 +153,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--profile", action="store_true",
+                    help="only warm-up and timed H·psi steps (for ncu launch lists and captures)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -224,6 +226,11 @@ def main():
         ev[k][1].record(stream)
     torch.cuda.synchronize(dev)
     step_ms = [a.elapsed_time(b) for a, b in ev]
+    if args.profile:
+        if sampler:
+            sampler.terminate()
+        print(json.dumps({"profile": True, "ms_per_step": sum(step_ms) / len(step_ms), "flops": int(flops)}))
+        return
     total_ms = sum(step_ms)
     import ctypes as C
     ms3 = (C.c_double * 3)()

@@ -19,10 +19,22 @@ namespace dmrgb200 {
 
 namespace {
 
-constexpr int BM = 64, BN = 64, BK = 16, PAD = 4, NTHREADS = 128;
+constexpr int BM = 32, BN = 64, BK = 16, NTHREADS = 128;
+constexpr int LDA_S = BM + 4, LDB_S = BN + 4;  // row strides = 8 words mod 32: conflict-free fragment loads
+constexpr int STAGES = 2;
+
+__device__ __forceinline__ uint64_t base_of(Bases const& bs, uint32_t buf) {
+    // a select chain keeps the kernel-parameter array out of local memory
+    uint64_t b = bs.b[0];
+    b = buf == 1 ? bs.b[1] : b;
+    b = buf == 2 ? bs.b[2] : b;
+    b = buf == 3 ? bs.b[3] : b;
+    b = buf == 4 ? bs.b[4] : b;
+    return b;
+}
 
 __device__ __forceinline__ const double* op_base(Bases const& bs, DevOp const& op, uint32_t batch) {
-    return reinterpret_cast<const double*>(bs.b[op.buf] + 8ull * (op.off + uint64_t(batch) * op.bstride));
+    return reinterpret_cast<const double*>(base_of(bs, op.buf) + 8ull * (op.off + uint64_t(batch) * op.bstride));
 }
 
 __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
@@ -31,90 +43,135 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
                  : "d"(a), "d"(b));
 }
 
-__global__ void __launch_bounds__(NTHREADS) gemm_f64_grouped(const DevProb* __restrict__ probs,
-                                                             const DevSeg* __restrict__ segs,
-                                                             const DevTile* __restrict__ tiles, uint32_t n_tiles,
-                                                             Bases bases) {
-    __shared__ double As[BK][BM + PAD];
-    __shared__ double Bs[BK][BN + PAD];
+// 8-byte asynchronous global->shared copy; src_bytes = 0 writes a zero (out-of-range element).
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem, bool valid) {
+    unsigned saddr = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    int n = valid ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(saddr), "l"(gmem), "r"(n));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_0() { asm volatile("cp.async.wait_group 0;\n" ::); }
+
+struct TileCursor {
+    uint32_t seg, k0;
+};
+
+// Issue the copies of one K tile (segment sg, rows k0..k0+BK) into stage buffers.
+__device__ __forceinline__ void load_tile(double (*As)[LDA_S], double (*Bs)[LDB_S], DevSeg const& sg,
+                                          const double* A, const double* B, uint32_t m0, uint32_t n0, uint32_t M,
+                                          uint32_t N, uint32_t k0, int tid) {
+    const uint64_t lda = sg.A.ld, ldb = sg.B.ld;
+    const uint32_t K = sg.K;
+#pragma unroll
+    for (int j = 0; j < (BM * BK) / NTHREADS; ++j) {
+        int idx = tid + j * NTHREADS;
+        int m, k;
+        if (!sg.A.trans) {
+            m = idx % BM;
+            k = idx / BM;
+        } else {
+            k = idx % BK;
+            m = idx / BK;
+        }
+        uint32_t gm = m0 + m, gk = k0 + k;
+        bool ok = gm < M && gk < K;
+        const double* src = ok ? (sg.A.trans ? A + gk + gm * lda : A + gm + gk * lda) : A;
+        cp_async8(&As[k][m], src, ok);
+    }
+#pragma unroll
+    for (int j = 0; j < (BN * BK) / NTHREADS; ++j) {
+        int idx = tid + j * NTHREADS;
+        int n, k;
+        if (!sg.B.trans) {
+            k = idx % BK;
+            n = idx / BK;
+        } else {
+            n = idx % BN;
+            k = idx / BN;
+        }
+        uint32_t gn = n0 + n, gk = k0 + k;
+        bool ok = gn < N && gk < K;
+        const double* src = ok ? (sg.B.trans ? B + gn + gk * ldb : B + gk + gn * ldb) : B;
+        cp_async8(&Bs[k][n], src, ok);
+    }
+}
+
+// Grouped, persistent FP64 GEMM over a tile list.  Each CTA owns whole output
+// tiles (BM x BN) and walks every K tile of every segment of its problem with a
+// two-stage cp.async pipeline; 4 warps in a 2 x 2 grid, warp tile 16 x 32,
+// DMMA m8n8k4.
+__global__ void __launch_bounds__(NTHREADS, 4) gemm_f64_grouped(const DevProb* __restrict__ probs,
+                                                                const DevSeg* __restrict__ segs,
+                                                                const DevTile* __restrict__ tiles, uint32_t n_tiles,
+                                                                Bases bases) {
+    __shared__ __align__(16) double As[STAGES][BK][LDA_S];
+    __shared__ __align__(16) double Bs[STAGES][BK][LDB_S];
 
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
-    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    const int wm = (warp >> 1) * 16, wn = (warp & 1) * 32;
     const int g = lane >> 2, q = lane & 3;
 
     for (uint32_t ti = blockIdx.x; ti < n_tiles; ti += gridDim.x) {
         const DevTile tl = tiles[ti];
         const DevProb pr = probs[tl.prob];
         const uint32_t M = pr.M, N = pr.N;
-        double acc[4][4][2];
+        double acc[2][4][2];
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < 2; ++i)
 #pragma unroll
             for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
-        for (uint32_t s = pr.seg_begin; s < pr.seg_end; ++s) {
-            const DevSeg sg = segs[s];
-            const double* A = op_base(bases, sg.A, tl.batch);
-            const double* B = op_base(bases, sg.B, tl.batch);
-            const uint64_t lda = sg.A.ld, ldb = sg.B.ld;
-            const uint32_t K = sg.K;
-            for (uint32_t k0 = 0; k0 < K; k0 += BK) {
-                // A tile: BM x BK -> As[k][m]
-#pragma unroll
-                for (int j = 0; j < (BM * BK) / NTHREADS; ++j) {
-                    int idx = tid + j * NTHREADS;
-                    int m, k;
-                    if (!sg.A.trans) {
-                        m = idx % BM;
-                        k = idx / BM;
-                    } else {
-                        k = idx % BK;
-                        m = idx / BK;
-                    }
-                    uint32_t gm = tl.m0 + m, gk = k0 + k;
-                    double v = 0.0;
-                    if (gm < M && gk < K) v = sg.A.trans ? A[gk + gm * lda] : A[gm + gk * lda];
-                    As[k][m] = v;
-                }
-                // B tile: BK x BN -> Bs[k][n]
-#pragma unroll
-                for (int j = 0; j < (BN * BK) / NTHREADS; ++j) {
-                    int idx = tid + j * NTHREADS;
-                    int n, k;
-                    if (!sg.B.trans) {
-                        k = idx % BK;
-                        n = idx / BK;
-                    } else {
-                        n = idx % BN;
-                        k = idx / BN;
-                    }
-                    uint32_t gn = tl.n0 + n, gk = k0 + k;
-                    double v = 0.0;
-                    if (gn < N && gk < K) v = sg.B.trans ? B[gn + gk * ldb] : B[gk + gn * ldb];
-                    Bs[k][n] = v;
-                }
-                __syncthreads();
-#pragma unroll
-                for (int kk = 0; kk < BK; kk += 4) {
-                    double a[4], b[4];
-#pragma unroll
-                    for (int i = 0; i < 4; ++i) a[i] = As[kk + q][wm + i * 8 + g];
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) b[j] = Bs[kk + q][wn + j * 8 + g];
-#pragma unroll
-                    for (int i = 0; i < 4; ++i)
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
-                }
-                __syncthreads();
-            }
+        // flattened (segment, k0) sequence
+        TileCursor cur{pr.seg_begin, 0};
+        while (cur.seg < pr.seg_end && segs[cur.seg].K == 0) ++cur.seg;
+        if (cur.seg < pr.seg_end) {
+            DevSeg sg = segs[cur.seg];
+            load_tile(As[0], Bs[0], sg, op_base(bases, sg.A, tl.batch), op_base(bases, sg.B, tl.batch), tl.m0,
+                      tl.n0, M, N, 0, tid);
         }
+        cp_async_commit();
+        int stage = 0;
+        while (cur.seg < pr.seg_end) {
+            // advance to the next K tile and prefetch it
+            TileCursor nxt = cur;
+            nxt.k0 += BK;
+            if (nxt.k0 >= segs[nxt.seg].K) {
+                nxt.k0 = 0;
+                ++nxt.seg;
+                while (nxt.seg < pr.seg_end && segs[nxt.seg].K == 0) ++nxt.seg;
+            }
+            if (nxt.seg < pr.seg_end) {
+                DevSeg sg = segs[nxt.seg];
+                load_tile(As[stage ^ 1], Bs[stage ^ 1], sg, op_base(bases, sg.A, tl.batch),
+                          op_base(bases, sg.B, tl.batch), tl.m0, tl.n0, M, N, nxt.k0, tid);
+            }
+            cp_async_commit();
+            cp_async_wait_1();
+            __syncthreads();
+#pragma unroll
+            for (int kk = 0; kk < BK; kk += 4) {
+                double a[2], b[4];
+#pragma unroll
+                for (int i = 0; i < 2; ++i) a[i] = As[stage][kk + q][wm + i * 8 + g];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) b[j] = Bs[stage][kk + q][wn + j * 8 + g];
+#pragma unroll
+                for (int i = 0; i < 2; ++i)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+            }
+            __syncthreads();
+            stage ^= 1;
+            cur = nxt;
+        }
+        cp_async_wait_0();
 
         double* C = const_cast<double*>(op_base(bases, pr.C, tl.batch));
         const uint64_t ldc = pr.C.ld;
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < 2; ++i)
 #pragma unroll
             for (int j = 0; j < 4; ++j)
 #pragma unroll
@@ -126,8 +183,10 @@ __global__ void __launch_bounds__(NTHREADS) gemm_f64_grouped(const DevProb* __re
     }
 }
 
-// S build: every line writes rows x cols elements of S as the alpha-weighted sum
-// of its T sources, summed in term order like the reference's axpy sequence.
+// S build: S is tiled by cells (one per unit and MPO row block); a cell with a
+// line writes the alpha-weighted sum of its T sources (summed in term order like
+// the reference's axpy sequence), a cell without one writes zeros, so S needs
+// no separate clearing.
 __global__ void __launch_bounds__(256) sbuild_lines(const DevSLine* __restrict__ lines,
                                                     const DevSTerm* __restrict__ terms, uint32_t n_lines,
                                                     double* __restrict__ S, const double* __restrict__ T) {
@@ -228,6 +287,16 @@ void compile_program(FlatPlan const& p, std::vector<uint64_t> const& stage3_bnd,
             pr.C = op(BUF_T, t_off[t], M, false, uint64_t(M) * N);
             pr.M = M;
             pr.N = N;
+            if (!p.t_trans[t]) {
+                // the nb stored blocks are adjacent K x N column blocks: one GEMM of width nb * N
+                pr.N = N * p.t_nb[t];
+                pr.seg_begin = uint32_t(g1.segs.size());
+                g1.segs.push_back(sg);
+                pr.seg_end = uint32_t(g1.segs.size());
+                g1.probs.push_back(pr);
+                add_tiles(g1, uint32_t(g1.probs.size() - 1), 1);
+                continue;
+            }
         }
         pr.seg_begin = uint32_t(g1.segs.size());
         g1.segs.push_back(sg);
@@ -245,34 +314,42 @@ void compile_program(FlatPlan const& p, std::vector<uint64_t> const& stage3_bnd,
         ssum += round_up(uint64_t(p.c_nsrows[c]) * p.c_stripe[c] * (p.kind == KIND_LEFT ? p.c_rs[c] : p.c_ls[c]), 32);
     }
     prog.s_elems = ssum;
+    // units tile the S columns (rows for the left step) and b1 its row blocks, so
+    // the cells (unit, b1) cover S exactly once
     for (uint32_t c = 0; c < nc; ++c) {
-        for (uint32_t u = p.c_unit[c]; u < p.c_unit[c + 1]; ++u)
-            for (uint32_t l = p.u_line[u]; l < p.u_line[u + 1]; ++l) {
+        for (uint32_t u = p.c_unit[c]; u < p.c_unit[c + 1]; ++u) {
+            std::vector<int64_t> line_of(p.c_nsrows[c], -1);
+            for (uint32_t l = p.u_line[u]; l < p.u_line[u + 1]; ++l) line_of[p.l_b1[l]] = l;
+            for (uint32_t b1 = 0; b1 < p.c_nsrows[c]; ++b1) {
                 DevSLine L;
                 L.term_begin = uint32_t(prog.terms.size());
+                int64_t l = line_of[b1];
                 if (p.kind == KIND_LEFT) {
                     L.ld_s = p.c_stripe[c];
                     L.rows = p.u_ms[u];
                     L.cols = p.c_rs[c];
                     L.ld_t = p.u_ms[u];
-                    L.s_base = s_off[c] + p.u_offset[u] + uint64_t(p.l_b1[l]) * p.c_rs[c] * p.c_stripe[c];
-                    for (uint32_t k = p.l_term[l]; k < p.l_term[l + 1]; ++k)
-                        prog.terms.push_back(
-                            DevSTerm{p.term_alpha[k], t_off[p.term_t[k]] + uint64_t(p.term_col[k]) * p.c_rs[c]});
+                    L.s_base = s_off[c] + p.u_offset[u] + uint64_t(b1) * p.c_rs[c] * p.c_stripe[c];
+                    if (l >= 0)
+                        for (uint32_t k = p.l_term[l]; k < p.l_term[l + 1]; ++k)
+                            prog.terms.push_back(
+                                DevSTerm{p.term_alpha[k], t_off[p.term_t[k]] + uint64_t(p.term_col[k]) * p.c_rs[c]});
                 } else {
                     uint32_t ls = p.c_ls[c];
                     L.ld_s = p.c_nsrows[c] * ls;
                     L.rows = ls;
                     L.cols = p.u_ms[u];
                     L.ld_t = ls;
-                    L.s_base = s_off[c] + uint64_t(p.l_b1[l]) * ls + uint64_t(p.u_offset[u]) * L.ld_s;
-                    for (uint32_t k = p.l_term[l]; k < p.l_term[l + 1]; ++k)
-                        prog.terms.push_back(
-                            DevSTerm{p.term_alpha[k], t_off[p.term_t[k]] + uint64_t(p.term_col[k]) * ls});
+                    L.s_base = s_off[c] + uint64_t(b1) * ls + uint64_t(p.u_offset[u]) * L.ld_s;
+                    if (l >= 0)
+                        for (uint32_t k = p.l_term[l]; k < p.l_term[l + 1]; ++k)
+                            prog.terms.push_back(
+                                DevSTerm{p.term_alpha[k], t_off[p.term_t[k]] + uint64_t(p.term_col[k]) * ls});
                 }
                 L.term_end = uint32_t(prog.terms.size());
-                prog.lines.push_back(L);
+                if (uint64_t(L.rows) * L.cols) prog.lines.push_back(L);
             }
+        }
     }
 
     // ---- stage 3 ----
@@ -434,22 +511,23 @@ cudaError_t run_program(DeviceProgram const& prog, uint64_t in, uint64_t out, do
     bs.b[BUF_ABS] = 0;
     const int sms = device_sm_count();
     if (ev) cudaEventRecord(ev[0], stream);
+    static int occ = 0;
+    if (!occ) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, gemm_f64_grouped, NTHREADS, 0);
+        if (occ <= 0) occ = 1;
+    }
     if (prog.n_t1) {
-        uint32_t grid = std::min<uint32_t>(prog.n_t1, uint32_t(sms) * 4);
+        uint32_t grid = std::min<uint32_t>(prog.n_t1, uint32_t(sms) * occ);
         gemm_f64_grouped<<<grid, NTHREADS, 0, stream>>>(prog.d_p1, prog.d_s1, prog.d_t1, prog.n_t1, bs);
     }
     if (ev) cudaEventRecord(ev[1], stream);
-    if (prog.s_elems) {
-        cudaError_t e = cudaMemsetAsync(S, 0, prog.s_elems * sizeof(double), stream);
-        if (e != cudaSuccess) return e;
-    }
     if (prog.n_lines) {
         uint32_t grid = std::min<uint32_t>(prog.n_lines, uint32_t(sms) * 8);
         sbuild_lines<<<grid, 256, 0, stream>>>(prog.d_lines, prog.d_terms, prog.n_lines, S, T);
     }
     if (ev) cudaEventRecord(ev[2], stream);
     if (prog.n_t3) {
-        uint32_t grid = std::min<uint32_t>(prog.n_t3, uint32_t(sms) * 4);
+        uint32_t grid = std::min<uint32_t>(prog.n_t3, uint32_t(sms) * occ);
         gemm_f64_grouped<<<grid, NTHREADS, 0, stream>>>(prog.d_p3, prog.d_s3, prog.d_t3, prog.n_t3, bs);
     }
     if (ev) cudaEventRecord(ev[3], stream);

@@ -200,6 +200,27 @@ dmrgb200_status dmrgb200_plan_stage_times(dmrgb200_plan_t plan, double ms[3], ui
  * denominator of the native-FP64 roofline. */
 dmrgb200_status dmrgb200_calibrate(int what, double* value);
 
+/* ---- H·psi for callers that cannot allocate device memory --------------- */
+/* No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * when they need an H·psi (a custom allocator or memory pool owns the device
+ * memory and forbids further allocations, or the host only hands the library
+ * pre-placed buffers): y = H_eff x from the flat plan description, the caller's
+ * device boundaries (left = L, right = R) and device vectors x, y, with every
+ * other device byte (lowered tile tables and the T / S intermediates) taken
+ * from one static device array of DMRGB200_NOALLOC_BYTES that each GPU loading
+ * the library holds until the process exits.  The call allocates no device
+ * memory.  Plans needing more than that return DMRGB200_OUT_OF_MEMORY with a
+ * message giving the required size.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) with that device current; make
+ * that first call before any stream capture.  All calls share the one array
+ * (it keeps the last call's contents; nothing in it needs to start at zero), so
+ * calls whose executions overlap on the GPU race: serialise them, e.g. on one
+ * stream.  The call returns after its work on `cuda_stream` has finished. */
+#define DMRGB200_NOALLOC_BYTES (64ull << 20)
+dmrgb200_status dmrgb200_hpsi_noalloc(const dmrgb200_plan_desc* desc, const dmrgb200_boundary_view* left,
+                                      const dmrgb200_boundary_view* right, const double* x, double* y,
+                                      void* cuda_stream);
+
 /* ---- boundary steps on a flattened plan --------------------------------- */
 /* Execute a LEFT_STEP / RIGHT_STEP plan.  ket: right-paired device tensor
  * (plan in-blocks); bra: left-paired (left step) or right-paired (right step)

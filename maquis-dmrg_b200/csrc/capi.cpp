@@ -258,6 +258,11 @@ dmrgb200_status run_step(dmrgb200_plan_s* p, const double* ket, const double* br
 
 }  // namespace
 
+namespace dmrgb200 {
+dmrgb200_status noalloc_fail(dmrgb200_status s, std::string const& msg) { return fail(s, msg); }
+void noalloc_desc_to_flat(const dmrgb200_plan_desc* d, FlatPlan& f) { desc_to_flat(d, f); }
+}  // namespace dmrgb200
+
 extern "C" {
 
 const char* dmrgb200_status_string(dmrgb200_status s) {

@@ -101,6 +101,8 @@ _sigs = {
     "dmrgb200_hpsi": ([vp, vp, vp, C.c_int, vp], C.c_int),
     "dmrgb200_plan_set_timing": ([vp, C.c_int], C.c_int),
     "dmrgb200_plan_stage_times": ([vp, f64p, u64p, u64p], C.c_int),
+    "dmrgb200_hpsi_noalloc": ([C.POINTER(PlanDesc), C.POINTER(BoundaryView), C.POINTER(BoundaryView), vp, vp, vp],
+                              C.c_int),
     "dmrgb200_step_execute": ([vp, vp, vp, C.POINTER(BoundaryView), vp], C.c_int),
     "dmrgb200_mpo_create": ([C.POINTER(MpoDesc), C.POINTER(vp)], C.c_int),
     "dmrgb200_mpo_destroy": ([vp], C.c_int),

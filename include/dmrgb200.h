@@ -200,6 +200,25 @@ dmrgb200_status dmrgb200_plan_stage_times(dmrgb200_plan_t plan, double ms[3], ui
  * denominator of the native-FP64 roofline. */
 dmrgb200_status dmrgb200_calibrate(int what, double* value);
 
+/* ---- eigensolver ---------------------------------------------------------- */
+/* Lowest eigenpair of H_eff by Jacobi-Davidson in FP64 on the device
+ * (solve<double>, dmrg/framework/dmrg/solver/solver.cpp:13-28 ->
+ * solve_ietl_jcd, solver/ietl_jacobi_davidson.h:35-76 -> ietl/jacobi.h:386-520,
+ * with ietl_jcd_gmres = 0): MGS with refinement (kappa 0.25), projection of the
+ * n_ortho orthogonal vectors (host array of device vectors), Rayleigh-Ritz,
+ * convergence |r| <= tol |theta| or |r| < tol, at most max_iter (1..32) H·psi
+ * applications.  x0 and x_out are device vectors of n doubles in the plan's
+ * block layout with zero padding.  *energy = theta (no core energy). */
+typedef struct {
+    uint32_t iterations;
+    int32_t converged;
+    double residual;
+    double hpsi_ms;
+} dmrgb200_solve_stats;
+dmrgb200_status dmrgb200_solve(dmrgb200_plan_t plan, uint64_t n, const double* x0, const double* const* ortho,
+                               uint32_t n_ortho, double tol, uint32_t max_iter, double* energy, double* x_out,
+                               dmrgb200_solve_stats* stats, void* cuda_stream);
+
 /* ---- H·psi for callers that cannot allocate device memory --------------- */
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc
  * when they need an H·psi (a custom allocator or memory pool owns the device

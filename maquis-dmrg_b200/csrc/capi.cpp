@@ -260,6 +260,11 @@ dmrgb200_status run_step(dmrgb200_plan_s* p, const double* ket, const double* br
 
 namespace dmrgb200 {
 dmrgb200_status noalloc_fail(dmrgb200_status s, std::string const& msg) { return fail(s, msg); }
+cudaError_t plan_hpsi_launch(dmrgb200_plan_t plan, const double* x, double* y, cudaStream_t stream) {
+    if (plan->flat.kind != KIND_HPSI || !plan->compiled) return cudaErrorInvalidValue;
+    return run_program(plan->prog, reinterpret_cast<uint64_t>(x), reinterpret_cast<uint64_t>(y), plan->T, plan->S,
+                       stream);
+}
 void noalloc_desc_to_flat(const dmrgb200_plan_desc* d, FlatPlan& f) { desc_to_flat(d, f); }
 }  // namespace dmrgb200
 

@@ -80,6 +80,11 @@ class MpoDesc(C.Structure):
     ]
 
 
+class SolveStats(C.Structure):
+    _fields_ = [("iterations", C.c_uint32), ("converged", C.c_int32), ("residual", C.c_double),
+                ("hpsi_ms", C.c_double)]
+
+
 class BoundaryView(C.Structure):
     _fields_ = [("n_cohorts", C.c_uint32), ("cohort_ptr", C.POINTER(C.c_void_p))]
 
@@ -101,6 +106,8 @@ _sigs = {
     "dmrgb200_hpsi": ([vp, vp, vp, C.c_int, vp], C.c_int),
     "dmrgb200_plan_set_timing": ([vp, C.c_int], C.c_int),
     "dmrgb200_plan_stage_times": ([vp, f64p, u64p, u64p], C.c_int),
+    "dmrgb200_solve": ([vp, C.c_uint64, vp, C.POINTER(vp), C.c_uint32, C.c_double, C.c_uint32, f64p, vp,
+                        C.POINTER(SolveStats), vp], C.c_int),
     "dmrgb200_hpsi_noalloc": ([C.POINTER(PlanDesc), C.POINTER(BoundaryView), C.POINTER(BoundaryView), vp, vp, vp],
                               C.c_int),
     "dmrgb200_step_execute": ([vp, vp, vp, C.POINTER(BoundaryView), vp], C.c_int),

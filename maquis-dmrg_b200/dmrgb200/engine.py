@@ -183,6 +183,17 @@ class DevicePlan:
     def hpsi(self, x_ptr: int, y_ptr: int, prec: int = capi.PREC_FP64, stream: int = 0) -> None:
         capi.check(capi.lib.dmrgb200_hpsi(self.handle, x_ptr, y_ptr, prec, stream or None), "dmrgb200_hpsi")
 
+    def solve(self, x0_ptr: int, x_out_ptr: int, n: int, ortho_ptrs=(), tol: float = 1e-8, max_iter: int = 8,
+              stream: int = 0):
+        """Jacobi-Davidson lowest eigenpair (dmrgb200_solve); returns (energy, stats)."""
+        e = C.c_double()
+        st = capi.SolveStats()
+        arr = (C.c_void_p * max(len(ortho_ptrs), 1))(*[int(p) for p in ortho_ptrs])
+        capi.check(capi.lib.dmrgb200_solve(self.handle, n, x0_ptr, C.cast(arr, C.POINTER(C.c_void_p)),
+                                           len(ortho_ptrs), tol, max_iter, C.byref(e), x_out_ptr, C.byref(st),
+                                           stream or None), "dmrgb200_solve")
+        return e.value, st
+
     def step(self, ket_ptr: int, bra_ptr: int, out_addr: np.ndarray, stream: int = 0) -> None:
         v, arr = _view(out_addr)
         capi.check(capi.lib.dmrgb200_step_execute(self.handle, ket_ptr, bra_ptr, C.byref(v), stream or None),

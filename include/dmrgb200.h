@@ -200,6 +200,17 @@ dmrgb200_status dmrgb200_plan_stage_times(dmrgb200_plan_t plan, double ms[3], ui
  * denominator of the native-FP64 roofline. */
 dmrgb200_status dmrgb200_calibrate(int what, double* value);
 
+/* ---- SU(2) recoupling utilities (arguments are twice the angular momenta) --- */
+/* The coefficients the SU2U1 schedule builder folds into alpha: Wigner 6j and
+ * 9j symbols (the reference links GSL's gsl_sf_coupling_6j/9j,
+ * block_matrix/symmetry/gsl_coupling.h:30-34) and the four reduced-matrix-element
+ * couplings of set_coupling (gsl_coupling.h:72-92). */
+double dmrgb200_wigner6j(int two_j1, int two_j2, int two_j3, int two_j4, int two_j5, int two_j6);
+double dmrgb200_wigner9j(int two_j1, int two_j2, int two_j3, int two_j4, int two_j5, int two_j6, int two_j7,
+                         int two_j8, int two_j9);
+void dmrgb200_set_coupling(int a, int b, int c, int d, int e, int f, int g, int h, int i, double init,
+                           double couplings[4]);
+
 /* ---- eigensolver ---------------------------------------------------------- */
 /* Lowest eigenpair of H_eff by Jacobi-Davidson in FP64 on the device
  * (solve<double>, dmrg/framework/dmrg/solver/solver.cpp:13-28 ->

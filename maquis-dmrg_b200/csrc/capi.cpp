@@ -12,6 +12,7 @@
 #include "device.hpp"
 #include "plan.hpp"
 #include "schedule.hpp"
+#include "coupling.hpp"
 
 using namespace dmrgb200;
 
@@ -287,6 +288,15 @@ const char* dmrgb200_status_string(dmrgb200_status s) {
 const char* dmrgb200_last_error(void) { return g_last_error.c_str(); }
 
 int dmrgb200_abi_version(void) { return 1; }
+
+double dmrgb200_wigner6j(int a, int b, int c, int d, int e, int f) { return wigner6j(a, b, c, d, e, f); }
+double dmrgb200_wigner9j(int a, int b, int c, int d, int e, int f, int g, int h, int i) {
+    return wigner9j(a, b, c, d, e, f, g, h, i);
+}
+void dmrgb200_set_coupling(int a, int b, int c, int d, int e, int f, int g, int h, int i, double init,
+                           double couplings[4]) {
+    set_coupling(a, b, c, d, e, f, g, h, i, init, couplings);
+}
 
 dmrgb200_status dmrgb200_context_create(int device, dmrgb200_context_t* out) {
     if (!out) return fail(DMRGB200_INVALID_ARGUMENT, "null output");

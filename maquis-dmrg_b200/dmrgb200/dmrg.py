@@ -1,0 +1,268 @@
+"""Two-site DMRG sweeps driving the device hot path.
+
+The optimizer mirrors the reference's ts_optimize::sweep
+(dmrg/framework/dmrg/optimize/ts_optimize.hpp:114-362) and its boundary caches
+(optimize/optimize.h:71-195): for every site pair the two-site tensor is
+formed, its lowest eigenpair is found by Jacobi-Davidson on the device
+(dmrgb200_solve over a dmrgb200 H·psi plan), the result is split by a
+block-wise SVD truncated to the bond dimension, and the left (right) boundary
+is advanced by a device boundary step.  The SVD split and the two-site tensor
+formation run on the host in FP64 (numpy/LAPACK).
+"""
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import engine as E
+from . import models as M
+from . import mps as S
+
+
+def _sub(t: S.SiteTensor, lb, s, ss):
+    r0, c0, ml, mr, rb = t.rp.sub[(lb, s, ss)]
+    return S.block_view(t.data, t.rp, lb)[:, c0:c0 + mr], rb
+
+
+def twosite(A: S.SiteTensor, B: S.SiteTensor, p12, offs) -> S.SiteTensor:
+    """psi = A . B over the shared bond, physical index fused (TwoSiteTensor,
+    mp_tensors/twositetensor.hpp:28-43)."""
+    psi = S.SiteTensor(p12, A.left, B.right)
+    p12pos = {c: k for k, (c, _) in enumerate(p12)}
+    d1 = dict(A.phys)
+    d2 = dict(B.phys)
+    for (lb, s1, i1), (_, c0a, ml, mm, mb) in A.rp.sub.items():
+        a = S.block_view(A.data, A.rp, lb)[:, c0a:c0a + mm]
+        c1 = A.phys[s1][0]
+        for s2, (c2, dd2) in enumerate(B.phys):
+            for i2 in range(dd2):
+                key = (mb, s2, i2)
+                if key not in B.rp.sub:
+                    continue
+                b, rb = _sub(B, mb, s2, i2)
+                f = (c1[0] + c2[0], c1[1] + c2[1])
+                ss = offs[(c1, c2)] + i1 * d2[c2] + i2
+                k = (lb, p12pos[f], ss)
+                if k not in psi.rp.sub:
+                    continue
+                _, c0, _, mr, _ = psi.rp.sub[k]
+                S.block_view(psi.data, psi.rp, lb)[:, c0:c0 + mr] += a @ b
+    del d1
+    return psi
+
+
+@dataclass
+class SplitResult:
+    A: S.SiteTensor
+    B: S.SiteTensor
+    truncated_weight: float
+    bond: list
+
+
+def split(psi: S.SiteTensor, phys1, phys2, offs, m: int, cutoff: float, left_to_right: bool) -> SplitResult:
+    """SVD split of a two-site tensor with truncation to m states and relative
+    cutoff (svd_truncate, block_matrix/block_matrix_algorithms.h:185-298):
+    left-to-right keeps U left-normalised and moves S V^T right, right-to-left
+    keeps V^T right-normalised and moves U S left."""
+    left, right = psi.left, psi.right
+    lpos = {c: i for i, (c, _) in enumerate(left)}
+    rpos = {c: i for i, (c, _) in enumerate(right)}
+    p12pos = {c: k for k, (c, _) in enumerate(psi.phys)}
+    # rows (s1, i1, lc) and columns (s2, i2, rc) of every middle charge
+    mids = {}
+    for s1, (c1, d1) in enumerate(phys1):
+        for lc, ml in left:
+            mc = (lc[0] + c1[0], lc[1] + c1[1])
+            for i1 in range(d1):
+                mids.setdefault(mc, [[], []])[0].append((s1, i1, lc, ml))
+    for mc in list(mids):
+        for s2, (c2, d2) in enumerate(phys2):
+            rc = (mc[0] + c2[0], mc[1] + c2[1])
+            if rc not in rpos:
+                continue
+            for i2 in range(d2):
+                mids[mc][1].append((s2, i2, rc, right[rpos[rc]][1]))
+    d2s = dict(phys2)
+    svds = {}
+    for mc, (rows, cols) in mids.items():
+        nr, nc = sum(r[3] for r in rows), sum(c[3] for c in cols)
+        if nr == 0 or nc == 0:
+            continue
+        Th = np.zeros((nr, nc))
+        ro = 0
+        for (s1, i1, lc, ml) in rows:
+            co = 0
+            c1 = phys1[s1][0]
+            for (s2, i2, rc, mr) in cols:
+                c2 = phys2[s2][0]
+                f = (c1[0] + c2[0], c1[1] + c2[1])
+                k = (lpos[lc], p12pos[f], offs[(c1, c2)] + i1 * d2s[c2] + i2)
+                if k in psi.rp.sub:
+                    _, c0, _, _, _ = psi.rp.sub[k]
+                    Th[ro:ro + ml, co:co + mr] = S.block_view(psi.data, psi.rp, lpos[lc])[:, c0:c0 + mr]
+                co += mr
+            ro += ml
+        U, sv, Vt = np.linalg.svd(Th, full_matrices=False)
+        svds[mc] = (U, sv, Vt, rows, cols)
+    allsv = np.concatenate([v[1] for v in svds.values()]) if svds else np.zeros(0)
+    total = float(np.sum(allsv ** 2))
+    order = np.sort(allsv)[::-1]
+    keep_n = min(m, int(np.sum(order > cutoff * (order[0] if order.size else 0))))
+    thresh = order[keep_n - 1] if keep_n > 0 else np.inf
+    kept, bond = {}, []
+    count = 0
+    for mc in sorted(svds):
+        sv = svds[mc][1]
+        k = int(np.sum(sv >= thresh))
+        k = min(k, keep_n - count)
+        if k > 0:
+            kept[mc] = k
+            count += k
+    bond = [(mc, kept[mc]) for mc in sorted(kept)]
+    tw = 1.0 - float(sum(np.sum(svds[mc][1][:kept[mc]] ** 2) for mc in kept)) / total if total > 0 else 0.0
+    A = S.SiteTensor(phys1, left, bond)
+    B = S.SiteTensor(phys2, bond, right)
+    bpos = {c: i for i, (c, _) in enumerate(bond)}
+    for mc, k in kept.items():
+        U, sv, Vt, rows, cols = svds[mc]
+        if left_to_right:
+            Uk, Vk = U[:, :k], sv[:k, None] * Vt[:k, :]
+        else:
+            Uk, Vk = U[:, :k] * sv[None, :k], Vt[:k, :]
+        ro = 0
+        for (s1, i1, lc, ml) in rows:
+            key = (lpos[lc], s1, i1)
+            if key in A.rp.sub:
+                _, c0, _, mr, rb = A.rp.sub[key]
+                assert rb == bpos[mc]
+                S.block_view(A.data, A.rp, lpos[lc])[:, c0:c0 + mr] = Uk[ro:ro + ml, :]
+            ro += ml
+        co = 0
+        for (s2, i2, rc, mr) in cols:
+            key = (bpos[mc], s2, i2)
+            _, c0, _, _, _ = B.rp.sub[key]
+            S.block_view(B.data, B.rp, bpos[mc])[:, c0:c0 + mr] = Vk[:, co:co + mr]
+            co += mr
+    return SplitResult(A, B, tw, bond)
+
+
+def right_canonicalize(tensors):
+    """Make sites 1..L-1 right-normalised by per-charge SVDs, absorbing the
+    remainder into the left neighbour."""
+    out = list(tensors)
+    for j in range(len(out) - 1, 0, -1):
+        t = out[j]
+        new_left, Vs, absorb = [], {}, {}
+        for lb, (lc, ml) in enumerate(t.left):
+            blk = S.block_view(t.data, t.rp, lb)
+            if blk.size == 0:
+                continue
+            U, sv, Vt = np.linalg.svd(blk, full_matrices=False)
+            k = int(np.sum(sv > 1e-14 * max(sv[0], 1e-300))) if sv.size else 0
+            if k == 0:
+                continue
+            new_left.append((lc, k))
+            Vs[lc] = Vt[:k]
+            absorb[lc] = U[:, :k] * sv[None, :k]
+        nt = S.SiteTensor(t.phys, new_left, t.right)
+        for lb, (lc, k) in enumerate(new_left):
+            S.block_view(nt.data, nt.rp, lb)[:, :] = Vs[lc]
+        prev = out[j - 1]
+        np_ = S.SiteTensor(prev.phys, prev.left, new_left)
+        npos = {c: i for i, (c, _) in enumerate(new_left)}
+        for (lb, s, ss), (_, c0, ml, mr, rb) in prev.rp.sub.items():
+            mc = prev.right[rb][0]
+            if mc not in npos:
+                continue
+            key = (lb, s, ss)
+            _, c1, _, k, _ = np_.rp.sub[key]
+            S.block_view(np_.data, np_.rp, lb)[:, c1:c1 + k] = \
+                S.block_view(prev.data, prev.rp, lb)[:, c0:c0 + mr] @ absorb[mc]
+        out[j] = nt
+        out[j - 1] = np_
+    n = out[0].norm()
+    out[0].data /= n
+    return out
+
+
+@dataclass
+class SweepLog:
+    energies: list = field(default_factory=list)      # (sweep, site, energy, iterations, truncated weight)
+    sweep_seconds: list = field(default_factory=list)
+    hpsi_calls: int = 0
+    hpsi_ms: float = 0.0
+
+
+class TwoSiteDMRG:
+    def __init__(self, ctx: E.Context, model: M.Model, tensors, m: int, cutoff: float = 1e-16,
+                 jd_tol: float = 1e-8, jd_maxiter: int = 8):
+        import torch
+        self.torch = torch
+        self.ctx, self.model, self.m, self.cutoff = ctx, model, m, cutoff
+        self.jd_tol, self.jd_maxiter = jd_tol, jd_maxiter
+        self.L = len(tensors)
+        self.A = right_canonicalize(tensors)
+        self.p12, self.offs = M.fuse_phys(model.phys, model.phys)
+        self.W = [M.MPOHandle(w, model.symm) for w in model.mpo]
+        self.W12 = [M.MPOHandle(M.twosite_mpo(model.mpo[i], model.mpo[i + 1], model.phys, model.phys), model.symm)
+                    for i in range(self.L - 1)]
+        dev = ctx.device
+        bonds0 = self.A[0].left
+        self.Lidx = [None] * (self.L + 1)
+        self.Lbuf = [None] * (self.L + 1)
+        self.Ridx = [None] * (self.L + 1)
+        self.Rbuf = [None] * (self.L + 1)
+        self.Lidx[0] = E.edge_bindex(model.symm, bonds0)
+        self.Lbuf[0] = E.to_device(self.Lidx[0].edge_values(), dev)
+        self.Ridx[self.L] = E.edge_bindex(model.symm, self.A[-1].right)
+        self.Rbuf[self.L] = E.to_device(self.Ridx[self.L].edge_values(), dev)
+        for j in range(self.L - 1, 1, -1):
+            self._right_step(j)
+        self.log = SweepLog()
+
+    def _left_step(self, j):
+        t = self.A[j]
+        dev = self.ctx.device
+        self.Lidx[j + 1], self.Lbuf[j + 1] = E.device_left_step(
+            self.ctx, self.model.phys, t.left, t.right, self.W[j], self.Lidx[j], self.Lbuf[j],
+            E.to_device(t.data, dev), E.to_device(t.left_paired(), dev), True)
+
+    def _right_step(self, j):
+        t = self.A[j]
+        td = E.to_device(t.data, self.ctx.device)
+        self.Ridx[j], self.Rbuf[j] = E.device_right_step(
+            self.ctx, self.model.phys, t.left, t.right, self.W[j], self.Ridx[j + 1], self.Rbuf[j + 1], td, td, True)
+
+    def optimize_pair(self, i, left_to_right):
+        torch = self.torch
+        psi = twosite(self.A[i], self.A[i + 1], self.p12, self.offs)
+        sched = E.schedule_hpsi(self.p12, psi.left, psi.right, self.W12[i], self.Lidx[i], self.Ridx[i + 2])
+        plan = E.DevicePlan(self.ctx, sched.plan, left_addr=self.Lidx[i].cohort_addresses(self.Lbuf[i].data_ptr()),
+                            other_addr=self.Ridx[i + 2].cohort_addresses(self.Rbuf[i + 2].data_ptr()))
+        xd = E.to_device(psi.data, self.ctx.device)
+        xo = torch.zeros_like(xd)
+        energy, st = plan.solve(xd.data_ptr(), xo.data_ptr(), xd.numel(), tol=self.jd_tol, max_iter=self.jd_maxiter)
+        self.log.hpsi_calls += st.iterations
+        self.log.hpsi_ms += st.hpsi_ms
+        psi.data = xo.cpu().numpy()
+        res = split(psi, self.model.phys, self.model.phys, self.offs, self.m, self.cutoff, left_to_right)
+        self.A[i], self.A[i + 1] = res.A, res.B
+        if left_to_right:
+            self._left_step(i)
+        else:
+            self._right_step(i + 1)
+        return energy, st.iterations, res.truncated_weight
+
+    def sweep(self, sweep_index: int):
+        t0 = time.perf_counter()
+        for i in range(0, self.L - 1):
+            e, it, tw = self.optimize_pair(i, True)
+            self.log.energies.append((sweep_index, i, e, it, tw))
+        for i in range(self.L - 2, -1, -1):
+            e, it, tw = self.optimize_pair(i, False)
+            self.log.energies.append((sweep_index, i, e, it, tw))
+        self.torch.cuda.synchronize(self.ctx.device)
+        self.log.sweep_seconds.append(time.perf_counter() - t0)
+        return self.log.energies[-1][2]

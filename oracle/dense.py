@@ -9,6 +9,8 @@
 from __future__ import annotations
 
 import numpy as np
+import scipy.sparse as sp
+import scipy.sparse.linalg as spl
 
 from dmrgb200 import models as M
 from dmrgb200 import mps as S
@@ -18,56 +20,53 @@ def local_charges(model: M.Model):
     return [c for c, d in model.phys for _ in range(d)]
 
 
-def dense_hamiltonian(model: M.Model, L: int) -> np.ndarray:
+def sparse_hamiltonian(model: M.Model, L: int):
+    """H from the model's term list (sparse CSR), fermionic operators carrying
+    explicit Jordan-Wigner strings on the sites to their left."""
     d = sum(dd for _, dd in model.phys)
-    F = model.local.get("fill")
-    I = np.eye(d)
+    F = sp.csr_matrix(model.local["fill"]) if "fill" in model.local else None
+    I = sp.identity(d, format="csr")
 
     def site_op(name, p):
-        O = model.local[name]
-        mats = []
+        O = sp.csr_matrix(model.local[name])
+        out = None
         for q in range(L):
-            if q == p:
-                mats.append(O)
-            elif q < p and name in model.fermionic_ops:
-                mats.append(F)
-            else:
-                mats.append(I)
-        out = mats[0]
-        for m in mats[1:]:
-            out = np.kron(out, m)
+            mq = O if q == p else (F if (q < p and name in model.fermionic_ops) else I)
+            out = mq if out is None else sp.kron(out, mq, format="csr")
         return out
 
-    H = np.zeros((d ** L, d ** L))
+    H = sp.csr_matrix((d ** L, d ** L))
     for coeff, factors in model.dense_terms:
-        term = np.eye(d ** L)
+        term = None
         for p, name in factors:
-            term = term @ site_op(name, p)
-        H += coeff * term
-    return H
+            o = site_op(name, p)
+            term = o if term is None else term @ o
+        H = H + coeff * term
+    return H.tocsr()
+
+
+def dense_hamiltonian(model: M.Model, L: int) -> np.ndarray:
+    return sparse_hamiltonian(model, L).toarray()
 
 
 def sector_mask(model: M.Model, L: int, total) -> np.ndarray:
-    ch = local_charges(model)
+    ch = np.array(local_charges(model))
     d = len(ch)
     q = np.zeros((d ** L, 2), dtype=int)
-    for idx in range(d ** L):
-        rem = idx
-        tot = [0, 0]
-        for p in range(L - 1, -1, -1):
-            s = rem % d
-            rem //= d
-            tot[0] += ch[s][0]
-            tot[1] += ch[s][1]
-        q[idx] = tot
+    idx = np.arange(d ** L)
+    for p in range(L - 1, -1, -1):
+        q += ch[idx % d]
+        idx //= d
     return (q[:, 0] == total[0]) & (q[:, 1] == total[1])
 
 
 def ground_energy(model: M.Model, L: int) -> float:
-    H = dense_hamiltonian(model, L)
-    mask = sector_mask(model, L, model.total_charge)
-    Hs = H[np.ix_(mask, mask)]
-    return float(np.linalg.eigvalsh(Hs)[0])
+    H = sparse_hamiltonian(model, L)
+    idx = np.nonzero(sector_mask(model, L, model.total_charge))[0]
+    Hs = H[idx][:, idx]
+    if Hs.shape[0] <= 2000:
+        return float(np.linalg.eigvalsh(Hs.toarray())[0])
+    return float(spl.eigsh(Hs, k=1, which="SA", tol=1e-13, maxiter=100000)[0][0])
 
 
 def mps_dense(tensors) -> np.ndarray:

@@ -1,0 +1,59 @@
+"""Host-side pieces of the sweep driver: two-site formation, SVD split and
+right canonicalisation preserve the state (dense comparison on small chains)."""
+import numpy as np
+import pytest
+
+import dense as D
+from dmrgb200 import dmrg as G
+from dmrgb200 import models as M
+from dmrgb200 import mps as S
+
+
+@pytest.mark.parametrize("name", ["heisenberg", "hubbard", "bose"])
+def test_split_of_twosite_reproduces_state(name):
+    L = 5
+    model = {"heisenberg": M.heisenberg(L), "hubbard": M.fermi_hubbard(L, n_up=2, n_down=2),
+             "bose": M.bose_hubbard(L, N=2)}[name]
+    rng = np.random.default_rng(0)
+    bonds = S.allowed_sectors(model.phys, L, model.total_charge, 6)
+    A = S.random_mps(model.phys, bonds, rng)
+    p12, offs = M.fuse_phys(model.phys, model.phys)
+    psi = G.twosite(A[1], A[2], p12, offs)
+    ref = D.mps_dense([t.dense() for t in A])
+    for l2r in (True, False):
+        res = G.split(psi, model.phys, model.phys, offs, 10 ** 6, 0.0, l2r)
+        B = list(A)
+        B[1], B[2] = res.A, res.B
+        assert res.truncated_weight < 1e-12
+        assert np.allclose(D.mps_dense([t.dense() for t in B]), ref, atol=1e-12)
+    # two-site tensor matches the dense contraction of the pair
+    core = D.twosite_dense(model.phys, model.phys, psi)
+    pair = np.tensordot(A[1].dense(), A[2].dense(), axes=([2], [0]))
+    assert np.allclose(core, pair, atol=1e-13)
+
+
+def test_right_canonicalize_preserves_state_and_normalises():
+    model = M.fermi_hubbard(6)
+    rng = np.random.default_rng(1)
+    bonds = S.allowed_sectors(model.phys, 6, model.total_charge, 8)
+    A = S.random_mps(model.phys, bonds, rng)
+    ref = D.mps_dense([t.dense() for t in A])
+    B = G.right_canonicalize(A)
+    got = D.mps_dense([t.dense() for t in B])
+    assert np.allclose(got, ref / np.linalg.norm(ref), atol=1e-12)
+    for t in B[1:]:
+        Td = t.dense()
+        X = Td.reshape(Td.shape[0], -1)
+        assert np.allclose(X @ X.T, np.eye(X.shape[0]), atol=1e-12)
+
+
+def test_truncation_keeps_largest_states():
+    model = M.heisenberg(8)
+    rng = np.random.default_rng(2)
+    bonds = S.allowed_sectors(model.phys, 8, model.total_charge, 16)
+    A = S.random_mps(model.phys, bonds, rng)
+    p12, offs = M.fuse_phys(model.phys, model.phys)
+    psi = G.twosite(A[3], A[4], p12, offs)
+    res = G.split(psi, model.phys, model.phys, offs, 5, 0.0, True)
+    assert sum(k for _, k in res.bond) == 5
+    assert 0.0 < res.truncated_weight < 1.0

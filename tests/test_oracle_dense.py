@@ -51,3 +51,13 @@ def test_symmetric_and_full_boundaries_agree():
     x = random_psi(a.p12, a.left, a.right, rng).data
     ya, yb = a.hpsi(x), b.hpsi(x)
     assert np.linalg.norm(ya - yb) <= 1e-13 * np.linalg.norm(ya)
+
+
+def test_bose_hubbard_model_matches_reference_known_answer():
+    """The reference's coded Bose-Hubbard regression test
+    (regression/applications/dmrg/test_coded_bh_ts.py:16-53) quotes
+    E = -6.881090360639349 (tolerance 1e-3) for L=10, Nmax=2, t=1, U=8, N=5.
+    Exact diagonalisation of the model as built here reproduces it."""
+    from dmrgb200 import models as M
+    e = D.ground_energy(M.bose_hubbard(10, t=1.0, U=8.0, Nmax=2, N=5), 10)
+    assert abs(e - (-6.881090360639349)) <= 1e-9

@@ -1,0 +1,76 @@
+"""ORACLE — test infrastructure only.  Python front-end of oracle/_ref/libmaquis_ref.so:
+the reference's own solver core (tasks.cpp) driven with flat plans
+(ref_adapter.cpp).  Available where oracle/build_ref.sh could compile the
+reference sources (the reference tree and this image's compilers)."""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+from dmrgb200 import _capi as capi
+
+LIB = Path(__file__).resolve().parent / "_ref" / "libmaquis_ref.so"
+_lib = None
+
+
+def available() -> bool:
+    return LIB.exists()
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        _lib = C.CDLL(str(LIB))
+        PD = C.POINTER(capi.PlanDesc)
+        u32 = C.POINTER(C.c_uint32)
+        pp = C.POINTER(C.c_void_p)
+        _lib.ref_hpsi.argtypes = [PD, C.c_uint32, u32, u32, u32, pp, C.c_uint32, pp, C.c_void_p, C.c_void_p]
+        _lib.ref_left_step.argtypes = [PD, C.c_uint32, u32, u32, u32, pp, C.c_void_p, C.c_void_p, pp]
+        _lib.ref_right_step.argtypes = [PD, C.c_uint32, u32, u32, u32, pp, C.c_void_p, C.c_void_p, pp]
+    return _lib
+
+
+def _ptrs(storage, bidx):
+    addr = bidx.cohort_addresses(storage.ctypes.data)
+    return (C.c_void_p * max(len(addr), 1))(*[int(a) if a else None for a in addr])
+
+
+def _u32(a):
+    return np.ascontiguousarray(a, dtype=np.uint32)
+
+
+def hpsi(plan, L, Lidx, R, Ridx, x):
+    desc, keep = capi.numpy_to_desc(plan)
+    y = np.zeros(plan["out_size"])
+    ls, rs, nb = _u32(Ridx.lsize), _u32(Ridx.rsize), _u32(Ridx.nblocks)
+    u = lambda a: a.ctypes.data_as(C.POINTER(C.c_uint32))
+    rc = lib().ref_hpsi(C.byref(desc), Ridx.n_cohorts, u(ls), u(rs), u(nb), _ptrs(L, Lidx), Lidx.n_cohorts,
+                        _ptrs(R, Ridx), np.ascontiguousarray(x).ctypes.data, y.ctypes.data)
+    assert rc == 0
+    return y
+
+
+def left_step(plan, L, Lidx, ket_rp, bra_lp, new_idx):
+    desc, keep = capi.numpy_to_desc(plan)
+    out = np.zeros(new_idx.n_elems)
+    ls, rs, nb = _u32(Lidx.lsize), _u32(Lidx.rsize), _u32(Lidx.nblocks)
+    u = lambda a: a.ctypes.data_as(C.POINTER(C.c_uint32))
+    rc = lib().ref_left_step(C.byref(desc), Lidx.n_cohorts, u(ls), u(rs), u(nb), _ptrs(L, Lidx),
+                             np.ascontiguousarray(ket_rp).ctypes.data, np.ascontiguousarray(bra_lp).ctypes.data,
+                             _ptrs(out, new_idx))
+    assert rc == 0
+    return out
+
+
+def right_step(plan, R, Ridx, ket_rp, bra_rp, new_idx):
+    desc, keep = capi.numpy_to_desc(plan)
+    out = np.zeros(new_idx.n_elems)
+    ls, rs, nb = _u32(Ridx.lsize), _u32(Ridx.rsize), _u32(Ridx.nblocks)
+    u = lambda a: a.ctypes.data_as(C.POINTER(C.c_uint32))
+    rc = lib().ref_right_step(C.byref(desc), Ridx.n_cohorts, u(ls), u(rs), u(nb), _ptrs(R, Ridx),
+                              np.ascontiguousarray(ket_rp).ctypes.data, np.ascontiguousarray(bra_rp).ctypes.data,
+                              _ptrs(out, new_idx))
+    assert rc == 0
+    return out

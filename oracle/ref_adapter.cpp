@@ -1,0 +1,159 @@
+// ORACLE — test infrastructure only.  Drives the reference's own solver core
+// (dmrg/framework/dmrg/solver/tasks.cpp, compiled from the read-only reference
+// tree by oracle/build_ref.sh into oracle/_ref/) with a flat plan: the plan is
+// replayed into ScheduleNew / MPSBlock / Cohort through their public API
+// (tasks.h:50-348: Cohort(...), add_unit, push_back, add_line, finalize,
+// MPSBlock::t_schedule) and executed by the reference's CPU kernels
+// create_T / contract (super_hamil_mv.hpp:121-132), create_T_left / prop_l
+// (move_boundary.hpp:260-276) and create_T / prop_r (move_boundary.hpp:385-401).
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <vector>
+
+#include "dmrg/solver/tasks.h"
+#include "../include/dmrgb200.h"
+
+using contraction::common::Cohort;
+using contraction::common::MPSBlock;
+using contraction::common::ScheduleNew;
+
+namespace {
+
+// cohort sizes of a boundary plus one Hermitian-complement entry per stored
+// cohort (index n + ci) with swapped sizes, so that T tasks can name a virtual ci
+BoundaryIndexRT make_rt(uint32_t n, const uint32_t* lsz, const uint32_t* rsz, const uint32_t* nb) {
+    BoundaryIndexRT rt;
+    for (uint32_t i = 0; i < n; ++i) {
+        rt.lszs().push_back(lsz[i]);
+        rt.rszs().push_back(rsz[i]);
+        rt.nbs().push_back(nb[i]);
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        rt.lszs().push_back(rsz[i]);
+        rt.rszs().push_back(lsz[i]);
+        rt.nbs().push_back(0);
+    }
+    return rt;
+}
+
+void fill_group(dmrgb200_plan_desc const& d, uint32_t g, uint32_t nbnd, MPSBlock<double>& mb, bool left, bool finalize,
+                bool hpsi) {
+    for (uint32_t t = d.g_t[g]; t < d.g_t[g + 1]; ++t) {
+        unsigned ci = d.t_trans[t] ? nbnd + d.t_ci[t] : d.t_ci[t];
+        mb.t_schedule.push_back(std::make_tuple(d.t_col[t], ci, d.t_ci[t], d.t_lb[t], size_t(0)));
+    }
+    for (uint32_t c = d.g_c[g]; c < d.g_c[g + 1]; ++c) {
+        uint32_t nu = d.c_unit[c + 1] - d.c_unit[c];
+        std::vector<std::size_t> phys(nu, 1);
+        unsigned ci = 0, ci_eff = 0;
+        if (hpsi) {
+            ci_eff = d.c_ci[c];
+            ci = d.c_trans[c] ? ci_eff + 1 + 1000000 : ci_eff;
+        }
+        // H psi: (lb_in, lb_out, ls_in, ls_out); left step: (rb_bra, rb_ket = group); right step:
+        // (lb_ket = group, lb_bra) -- site_hamil_tasks.hpp:78, left_tasks.hpp:113, right_tasks.hpp:110
+        Cohort<double> coh =
+            hpsi ? Cohort<double>(phys, d.c_lb[c], d.c_rb[c], d.c_ls[c], d.c_rs[c], ci, ci_eff, d.c_nsrows[c], false)
+            : left ? Cohort<double>(phys, d.c_lb[c], g, d.c_ls[c], d.c_rs[c], 0, 0, d.c_nsrows[c], true)
+                   : Cohort<double>(phys, g, d.c_rb[c], d.c_ls[c], d.c_rs[c], 0, 0, d.c_nsrows[c], false);
+        for (uint32_t u = d.c_unit[c]; u < d.c_unit[c + 1]; ++u) {
+            unsigned s = u - d.c_unit[c];
+            coh.add_unit(s, 1, d.u_ms[u], d.u_offset[u]);
+        }
+        for (uint32_t u = d.c_unit[c]; u < d.c_unit[c + 1]; ++u) {
+            unsigned s = u - d.c_unit[c];
+            for (uint32_t l = d.u_line[u]; l < d.u_line[u + 1]; ++l) {
+                for (uint32_t k = d.l_term[l]; k < d.l_term[l + 1]; ++k)
+                    coh.push_back(s, 0, d.term_alpha[k], d.term_t[k] - d.g_t[g], d.term_col[k]);
+                coh.add_line(d.l_b1[l]);
+            }
+        }
+        if (finalize) coh.finalize();
+        mb.push_back(std::move(coh));
+    }
+}
+
+std::vector<const double*> block_views(const double* base, const uint64_t* off, uint32_t n) {
+    std::vector<const double*> v(n);
+    for (uint32_t i = 0; i < n; ++i) v[i] = base + off[i];
+    return v;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ref_hpsi(const dmrgb200_plan_desc* dp, uint32_t nR, const uint32_t* R_lsz, const uint32_t* R_rsz,
+             const uint32_t* R_nb, const double* const* L, uint32_t nL, const double* const* R, const double* x,
+             double* y) {
+    dmrgb200_plan_desc const& d = *dp;
+    if (d.kind != DMRGB200_PLAN_HPSI) return 1;
+    BoundaryIndexRT rrt = make_rt(nR, R_lsz, R_rsz, R_nb), lrt;
+    std::vector<std::size_t> lr(d.in_rows, d.in_rows + d.n_in_blocks), mpsbs(d.n_in_blocks, 0);
+    ScheduleNew<double> tasks(mpsbs, lr, lrt, rrt);
+    for (uint32_t g = 0; g < d.n_groups; ++g) fill_group(d, g, nR, tasks[g], false, false, true);
+    std::vector<const double*> lv(L, L + nL), rv(R, R + nR);
+    auto xv = block_views(x, d.in_off, d.n_in_blocks);
+    for (uint32_t b = 0; b < d.n_out_blocks; ++b)
+        std::memset(y + d.out_off[b], 0, sizeof(double) * size_t(d.out_rows[b]) * d.out_cols[b]);
+    std::vector<std::mutex> mutexes(d.n_out_blocks);
+    int ng = int(d.n_groups);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int g = 0; g < ng; ++g) {
+        auto T = tasks[g].create_T(rv, xv);
+        for (auto it = tasks[g].begin(); it != tasks[g].end(); ++it)
+            it->contract(lv, T, y + d.out_off[it->get_rb()], mutexes[it->get_rb()]);
+    }
+    return 0;
+}
+
+int ref_left_step(const dmrgb200_plan_desc* dp, uint32_t nL, const uint32_t* L_lsz, const uint32_t* L_rsz,
+                  const uint32_t* L_nb, const double* const* L, const double* ket, const double* bra,
+                  double* const* out) {
+    dmrgb200_plan_desc const& d = *dp;
+    if (d.kind != DMRGB200_PLAN_LEFT_STEP) return 1;
+    BoundaryIndexRT lrt = make_rt(nL, L_lsz, L_rsz, L_nb);
+    std::vector<std::size_t> widths(d.n_groups, 0), mpsbs(d.n_in_blocks, 0);
+    for (uint32_t g = 0; g < d.n_groups; ++g) {
+        if (d.g_t[g] < d.g_t[g + 1]) widths[g] = d.t_width[d.g_t[g]];
+        else if (d.g_c[g] < d.g_c[g + 1]) widths[g] = d.c_rs[d.g_c[g]];
+    }
+    ScheduleNew<double> tasks(mpsbs, widths, lrt, lrt);
+    for (uint32_t g = 0; g < d.n_groups; ++g) fill_group(d, g, nL, tasks[g], true, true, false);
+    std::vector<const double*> lv(L, L + nL);
+    auto kv = block_views(ket, d.in_off, d.n_in_blocks);
+    int ng = int(d.n_groups);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int g = 0; g < ng; ++g) {
+        auto T = tasks[g].create_T_left(lv, kv);
+        uint32_t c = d.g_c[g];
+        for (auto it = tasks[g].begin(); it != tasks[g].end(); ++it, ++c)
+            it->prop_l(bra + d.out_off[it->get_lb()], T, out[d.c_out_ci[c]]);
+    }
+    return 0;
+}
+
+int ref_right_step(const dmrgb200_plan_desc* dp, uint32_t nR, const uint32_t* R_lsz, const uint32_t* R_rsz,
+                   const uint32_t* R_nb, const double* const* R, const double* ket, const double* bra,
+                   double* const* out) {
+    dmrgb200_plan_desc const& d = *dp;
+    if (d.kind != DMRGB200_PLAN_RIGHT_STEP) return 1;
+    BoundaryIndexRT rrt = make_rt(nR, R_lsz, R_rsz, R_nb);
+    std::vector<std::size_t> lr(d.in_rows, d.in_rows + d.n_in_blocks), mpsbs(d.n_in_blocks, 0);
+    ScheduleNew<double> tasks(mpsbs, lr, rrt, rrt);
+    for (uint32_t g = 0; g < d.n_groups; ++g) fill_group(d, g, nR, tasks[g], false, true, false);
+    std::vector<const double*> rv(R, R + nR);
+    auto kv = block_views(ket, d.in_off, d.n_in_blocks);
+    int ng = int(d.n_groups);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int g = 0; g < ng; ++g) {
+        auto T = tasks[g].create_T(rv, kv);
+        uint32_t c = d.g_c[g];
+        for (auto it = tasks[g].begin(); it != tasks[g].end(); ++it, ++c)
+            it->prop_r(bra + d.out_off[it->get_rb()], T, out[d.c_out_ci[c]]);
+    }
+    return 0;
+}
+
+}  // extern "C"

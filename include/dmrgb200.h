@@ -211,6 +211,16 @@ double dmrgb200_wigner9j(int two_j1, int two_j2, int two_j3, int two_j4, int two
 void dmrgb200_set_coupling(int a, int b, int c, int d, int e, int f, int g, int h, int i, double init,
                            double couplings[4]);
 
+/* ---- FP64 GEMM emulated on the INT8 tensor cores --------------------------- */
+/* C = A * B (column-major FP64, A M x K, B K x N) computed with `slices`
+ * (2..8) signed 7-bit digit planes per operand on tcgen05 INT8 MMAs with exact
+ * INT32 accumulation and FP64 recombination (Ozaki scheme, integer variant);
+ * relative accuracy about 2^(-7 slices) of the row/column maxima.  Requires
+ * K * slices <= 2^17.  Stream-ordered; returns after completion. */
+dmrgb200_status dmrgb200_dgemm_emulated(uint32_t M, uint32_t N, uint32_t K, const double* A, uint64_t lda,
+                                        const double* B, uint64_t ldb, double* C, uint64_t ldc, int slices,
+                                        void* cuda_stream);
+
 /* ---- eigensolver ---------------------------------------------------------- */
 /* Lowest eigenpair of H_eff by Jacobi-Davidson in FP64 on the device
  * (solve<double>, dmrg/framework/dmrg/solver/solver.cpp:13-28 ->

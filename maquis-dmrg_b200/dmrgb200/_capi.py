@@ -109,6 +109,8 @@ _sigs = {
     "dmrgb200_hpsi": ([vp, vp, vp, C.c_int, vp], C.c_int),
     "dmrgb200_plan_set_timing": ([vp, C.c_int], C.c_int),
     "dmrgb200_plan_stage_times": ([vp, f64p, u64p, u64p], C.c_int),
+    "dmrgb200_dgemm_emulated": ([C.c_uint32, C.c_uint32, C.c_uint32, vp, C.c_uint64, vp, C.c_uint64, vp,
+                                 C.c_uint64, C.c_int, vp], C.c_int),
     "dmrgb200_solve": ([vp, C.c_uint64, vp, C.POINTER(vp), C.c_uint32, C.c_double, C.c_uint32, f64p, vp,
                         C.POINTER(SolveStats), vp], C.c_int),
     "dmrgb200_hpsi_noalloc": ([C.POINTER(PlanDesc), C.POINTER(BoundaryView), C.POINTER(BoundaryView), vp, vp, vp],

@@ -274,14 +274,10 @@ def main():
         sampler.wait()
     clocks = clocks_summary(clk_path, local)
 
-    per_ms = total_ms / args.steps
-    e2e_per_ms = sum(e2e_ms) / len(e2e_ms)
-    if dist:
-        t = torch.tensor([per_ms, e2e_per_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        per_ms, e2e_per_ms = float(t[0]), float(t[1])
-    value = world * flops / (per_ms * 1e-3) / 1e9
-    e2e_value = world * flops / (e2e_per_ms * 1e-3) / 1e9
+    from dmrgb200.replicas import job_throughput
+
+    (per_ms, e2e_per_ms), (value, e2e_value) = job_throughput(
+        [total_ms / args.steps, sum(e2e_ms) / len(e2e_ms)], flops / 1e9, world, dist, dev)
 
     if rank == 0:
         fp64_peak = C.c_double()

@@ -171,6 +171,18 @@ dmrgb200_status dmrgb200_plan_destroy(dmrgb200_plan_t plan);
  * DMRGB200_INVALID_PLAN with a message for inconsistent input. */
 dmrgb200_status dmrgb200_plan_validate(const dmrgb200_plan_desc* desc);
 
+/* Batched H·psi (independent site problems in one plan): n H·psi plan
+ * descriptions with their left / right boundary views are concatenated so that
+ * each stage of dmrgb200_hpsi is one launch over the tiles of all instances.
+ * Instance i's vector occupies the elements [in_base[i], in_base[i] + size_i)
+ * of the batched x and y (128-element aligned), returned in in_base (n entries,
+ * may be NULL); dmrgb200_plan_flops reports the sum over instances.  No
+ * counterpart in the reference, which runs one site problem at a time. */
+dmrgb200_status dmrgb200_plan_create_batched(dmrgb200_context_t ctx, uint32_t n, const dmrgb200_plan_desc* descs,
+                                             const dmrgb200_boundary_view* lefts,
+                                             const dmrgb200_boundary_view* rights, uint64_t* in_base,
+                                             uint64_t* total_size, dmrgb200_plan_t* out);
+
 /* Algorithmic FP64 flop count of one execution, the reference's formula
  * (Cohort::n_flops tasks.cpp:388-398 + MPSBlock::n_flops :777-796). */
 dmrgb200_status dmrgb200_plan_flops(dmrgb200_plan_t plan, uint64_t* flops);

@@ -353,6 +353,35 @@ dmrgb200_status dmrgb200_plan_validate(const dmrgb200_plan_desc* d) {
     DMRGB200_CATCH
 }
 
+dmrgb200_status dmrgb200_plan_create_batched(dmrgb200_context_t ctx, uint32_t n, const dmrgb200_plan_desc* descs,
+                                             const dmrgb200_boundary_view* lefts,
+                                             const dmrgb200_boundary_view* rights, uint64_t* in_base,
+                                             uint64_t* total_size, dmrgb200_plan_t* out) {
+    DMRGB200_TRY
+    if (!ctx || !descs || !lefts || !rights || !out || n == 0) return fail(DMRGB200_INVALID_ARGUMENT, "null argument");
+    std::vector<FlatPlan> plans(n);
+    std::vector<uint32_t> lbase(n), rbase(n);
+    auto p = std::make_unique<dmrgb200_plan_s>();
+    for (uint32_t i = 0; i < n; ++i) {
+        if (descs[i].kind != DMRGB200_PLAN_HPSI) return fail(DMRGB200_INVALID_PLAN, "batched plans must be H psi plans");
+        desc_to_flat(&descs[i], plans[i]);
+        std::string err = plans[i].validate();
+        if (!err.empty()) return fail(DMRGB200_INVALID_PLAN, "instance " + std::to_string(i) + ": " + err);
+        lbase[i] = uint32_t(p->stage3_bnd.size());
+        rbase[i] = uint32_t(p->stage1_bnd.size());
+        auto lp = view_ptrs(&lefts[i]), rp = view_ptrs(&rights[i]);
+        p->stage3_bnd.insert(p->stage3_bnd.end(), lp.begin(), lp.end());
+        p->stage1_bnd.insert(p->stage1_bnd.end(), rp.begin(), rp.end());
+    }
+    std::vector<uint64_t> ib, ob;
+    p->flat = merge_plans(plans, lbase, rbase, ib, ob);
+    if (in_base)
+        for (uint32_t i = 0; i < n; ++i) in_base[i] = ib[i];
+    if (total_size) *total_size = p->flat.in_size;
+    return finish_plan(p, out);
+    DMRGB200_CATCH
+}
+
 dmrgb200_status dmrgb200_plan_destroy(dmrgb200_plan_t plan) {
     if (!plan) return DMRGB200_OK;
     if (plan->compiled) free_program(plan->prog);

@@ -1,6 +1,7 @@
 #include "plan.hpp"
 
 #include <sstream>
+#include <stdexcept>
 
 namespace dmrgb200 {
 
@@ -121,6 +122,81 @@ std::string FlatPlan::validate() const {
         }
     }
     return std::string();
+}
+
+FlatPlan merge_plans(std::vector<FlatPlan> const& plans, std::vector<uint32_t> const& left_ci_base,
+                     std::vector<uint32_t> const& right_ci_base, std::vector<uint64_t>& in_base,
+                     std::vector<uint64_t>& out_base) {
+    FlatPlan m;
+    m.kind = KIND_HPSI;
+    m.g_t.push_back(0);
+    m.g_c.push_back(0);
+    m.c_unit.push_back(0);
+    m.u_line.push_back(0);
+    m.l_term.push_back(0);
+    in_base.clear();
+    out_base.clear();
+    for (size_t i = 0; i < plans.size(); ++i) {
+        FlatPlan const& p = plans[i];
+        if (p.kind != KIND_HPSI) throw std::runtime_error("only H psi plans can be batched");
+        const uint64_t ib = round_up(m.in_size, 128), ob = round_up(m.out_size, 128);
+        in_base.push_back(ib);
+        out_base.push_back(ob);
+        const uint32_t nb_in = uint32_t(m.in_rows.size()), nb_out = uint32_t(m.out_rows.size());
+        const uint32_t t0 = m.n_t(), c0 = m.n_cohorts(), u0 = m.n_units(), l0 = m.n_lines(), k0 = m.n_terms();
+        for (size_t b = 0; b < p.in_rows.size(); ++b) {
+            m.in_rows.push_back(p.in_rows[b]);
+            m.in_cols.push_back(p.in_cols[b]);
+            m.in_off.push_back(ib + p.in_off[b]);
+        }
+        for (size_t b = 0; b < p.out_rows.size(); ++b) {
+            m.out_rows.push_back(p.out_rows[b]);
+            m.out_cols.push_back(p.out_cols[b]);
+            m.out_off.push_back(ob + p.out_off[b]);
+        }
+        m.in_size = ib + p.in_size;
+        m.out_size = ob + p.out_size;
+        for (uint32_t t = 0; t < p.n_t(); ++t) {
+            m.t_lb.push_back(nb_in + p.t_lb[t]);
+            m.t_col.push_back(p.t_col[t]);
+            m.t_ci.push_back(right_ci_base[i] + p.t_ci[t]);
+            m.t_trans.push_back(p.t_trans[t]);
+            m.t_nb.push_back(p.t_nb[t]);
+            m.t_brows.push_back(p.t_brows[t]);
+            m.t_bcols.push_back(p.t_bcols[t]);
+        }
+        for (uint32_t c = 0; c < p.n_cohorts(); ++c) {
+            m.c_lb.push_back(nb_in + p.c_lb[c]);
+            m.c_rb.push_back(nb_out + p.c_rb[c]);
+            m.c_ls.push_back(p.c_ls[c]);
+            m.c_rs.push_back(p.c_rs[c]);
+            m.c_ci.push_back(left_ci_base[i] + p.c_ci[c]);
+            m.c_trans.push_back(p.c_trans[c]);
+            m.c_nsrows.push_back(p.c_nsrows[c]);
+            m.c_stripe.push_back(p.c_stripe[c]);
+            m.c_out_ci.push_back(0);
+            m.c_unit.push_back(u0 + p.c_unit[c + 1]);
+        }
+        for (uint32_t u = 0; u < p.n_units(); ++u) {
+            m.u_offset.push_back(p.u_offset[u]);
+            m.u_ms.push_back(p.u_ms[u]);
+            m.u_line.push_back(l0 + p.u_line[u + 1]);
+        }
+        for (uint32_t l = 0; l < p.n_lines(); ++l) {
+            m.l_b1.push_back(p.l_b1[l]);
+            m.l_term.push_back(k0 + p.l_term[l + 1]);
+        }
+        for (uint32_t k = 0; k < p.n_terms(); ++k) {
+            m.term_alpha.push_back(p.term_alpha[k]);
+            m.term_t.push_back(t0 + p.term_t[k]);
+            m.term_col.push_back(p.term_col[k]);
+        }
+        for (uint32_t g = 0; g < p.n_groups(); ++g) {
+            m.g_t.push_back(t0 + p.g_t[g + 1]);
+            m.g_c.push_back(c0 + p.g_c[g + 1]);
+        }
+    }
+    return m;
 }
 
 TensorLayout right_paired_layout(Index const& phys, Index const& left, Index const& right) {

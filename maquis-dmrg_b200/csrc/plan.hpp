@@ -66,6 +66,14 @@ TensorLayout left_paired_layout(Index const& phys, Index const& left, Index cons
 
 inline uint64_t round_up(uint64_t v, uint64_t a) { return (v + a - 1) / a * a; }
 
+// Concatenate independent H psi plans into one: instance i's in/out blocks are
+// shifted by in_base[i] / out_base[i] (returned), its T tasks, cohorts, units,
+// lines, terms and groups are renumbered, and its boundary cohort indices are
+// shifted by the given per-instance offsets into the concatenated views.
+FlatPlan merge_plans(std::vector<FlatPlan> const& plans, std::vector<uint32_t> const& left_ci_base,
+                     std::vector<uint32_t> const& right_ci_base, std::vector<uint64_t>& in_base,
+                     std::vector<uint64_t>& out_base);
+
 // Flatten a built schedule.  `other` is the boundary read by the T tasks
 // (R for H psi and the right step, L for the left step); `lbnd` is L for H psi.
 FlatPlan flatten_hpsi(Schedule const& s, TensorLayout const& psi, BoundaryIndex const& L, BoundaryIndex const& R);

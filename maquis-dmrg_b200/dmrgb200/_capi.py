@@ -102,6 +102,8 @@ _sigs = {
     "dmrgb200_plan_create": ([vp, C.POINTER(PlanDesc), C.POINTER(BoundaryView), C.POINTER(BoundaryView),
                               C.POINTER(vp)], C.c_int),
     "dmrgb200_plan_destroy": ([vp], C.c_int),
+    "dmrgb200_plan_create_batched": ([vp, C.c_uint32, C.POINTER(PlanDesc), C.POINTER(BoundaryView),
+                                      C.POINTER(BoundaryView), u64p, u64p, C.POINTER(vp)], C.c_int),
     "dmrgb200_plan_validate": ([C.POINTER(PlanDesc)], C.c_int),
     "dmrgb200_calibrate": ([C.c_int, f64p], C.c_int),
     "dmrgb200_plan_flops": ([vp, u64p], C.c_int),

@@ -280,3 +280,39 @@ class SiteProblem:
 
     def hpsi(self, x, y, prec: int = capi.PREC_FP64, stream: int = 0):
         self.plan.hpsi(x.data_ptr(), y.data_ptr(), prec, stream)
+
+
+class BatchedPlan(DevicePlan):
+    """Independent H·psi problems merged into one plan (dmrgb200_plan_create_batched).
+
+    `items` is a list of (plan dict, left cohort addresses, right cohort
+    addresses); instance i occupies x[in_base[i] : in_base[i] + in_size_i]."""
+
+    def __init__(self, ctx: Context, items):
+        n = len(items)
+        descs = (capi.PlanDesc * n)()
+        lviews = (capi.BoundaryView * n)()
+        rviews = (capi.BoundaryView * n)()
+        self._keep = []
+        for i, (plan, la, ra) in enumerate(items):
+            d, k = capi.numpy_to_desc(plan)
+            descs[i] = d
+            self._keep.append(k)
+            lv, larr = _view(la)
+            rv, rarr = _view(ra)
+            lviews[i], rviews[i] = lv, rv
+            self._keep += [larr, rarr]
+        base = (C.c_uint64 * n)()
+        total = C.c_uint64()
+        h = C.c_void_p()
+        capi.check(capi.lib.dmrgb200_plan_create_batched(ctx.handle, n, descs, lviews, rviews, base, C.byref(total),
+                                                         C.byref(h)), "plan_create_batched")
+        self.handle = h
+        self.in_base = [int(b) for b in base]
+        self.total_size = total.value
+        self.sizes = [int(p["in_size"]) for p, _, _ in items]
+        f, s = C.c_uint64(), C.c_uint64()
+        capi.check(capi.lib.dmrgb200_plan_flops(h, C.byref(f)), "plan_flops")
+        capi.check(capi.lib.dmrgb200_plan_scratch_bytes(h, C.byref(s)), "plan_scratch_bytes")
+        self.flops, self.scratch_bytes = f.value, s.value
+        self.plan = None

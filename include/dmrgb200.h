@@ -194,9 +194,17 @@ dmrgb200_status dmrgb200_plan_scratch_bytes(dmrgb200_plan_t plan, uint64_t* byte
  * out as the plan's in/out blocks (DavidsonVector layout,
  * davidson_vector.cpp:87-152); y's block elements are overwritten, its padding
  * is left untouched.  Replaces super_hamil_mv (super_hamil_mv.hpp:100-155) and
- * ietl::mult (ietl_interface_dv.h:112-118). */
+ * ietl::mult (ietl_interface_dv.h:112-118).  DMRGB200_PREC_FP64_EMULATED runs
+ * the T and cohort contractions on the INT8 tensor cores (Ozaki split, see
+ * dmrgb200_plan_set_slices) and the S build in FP64; it synchronises the
+ * stream before returning. */
 dmrgb200_status dmrgb200_hpsi(dmrgb200_plan_t plan, const double* x, double* y, dmrgb200_precision prec,
                               void* cuda_stream);
+
+/* Digit planes per operand (2..8, default 7) used by DMRGB200_PREC_FP64_EMULATED:
+ * the relative error of each emulated contraction is about 2^(-7 slices) of
+ * its row / column maxima (7: below 1e-13, 6: about 1e-11, 5: about 1e-9). */
+dmrgb200_status dmrgb200_plan_set_slices(dmrgb200_plan_t plan, int slices);
 
 /* Per-stage timing of H·psi executions: when enabled, every dmrgb200_hpsi call
  * records CUDA events around its stages on the call's stream.

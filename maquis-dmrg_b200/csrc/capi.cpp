@@ -1,6 +1,7 @@
 // C ABI of libdmrgb200 (declarations in include/dmrgb200.h).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <exception>
 #include <limits>
@@ -61,6 +62,12 @@ struct dmrgb200_plan_s {
     bool pending = false;
     double stage_ms[3] = {0, 0, 0};
     uint64_t timed_calls = 0;
+    // FP64 emulated on the INT8 tensor cores (built on first use)
+    int slices = 7;
+    OzProgram* oz1 = nullptr;
+    OzProgram* oz3 = nullptr;
+    void* oz_scratch = nullptr;
+    uint64_t oz_scratch_size = 0;
 
     void collect() {
         if (!pending) return;
@@ -257,6 +264,45 @@ dmrgb200_status run_step(dmrgb200_plan_s* p, const double* ket, const double* br
     return DMRGB200_OK;
 }
 
+// Stage 1 and stage 3 on the INT8 tensor cores (Ozaki split with plan->slices
+// digit planes), the S build in FP64 between them.  Synchronises the stream to
+// report pipeline timeouts.
+dmrgb200_status hpsi_emulated(dmrgb200_plan_s* plan, const double* x, double* y, cudaStream_t st) {
+    const uint64_t klim = (1ull << 17) / uint64_t(plan->slices);
+    if (!plan->oz1) {
+        if (max_k_total(plan->prog.stage1) > klim || max_k_total(plan->prog.stage3) > klim)
+            return fail(DMRGB200_NOT_SUPPORTED, "a contraction is longer than the exact INT32 range of the emulation");
+        plan->oz1 = oz_build(plan->prog.stage1);
+        plan->oz3 = oz_build(plan->prog.stage3);
+        if (!plan->oz1 || !plan->oz3) return fail(DMRGB200_OUT_OF_MEMORY, "emulation tables");
+    }
+    uint64_t need = std::max(oz_scratch_bytes(plan->oz1, plan->slices), oz_scratch_bytes(plan->oz3, plan->slices));
+    if (need > plan->oz_scratch_size) {
+        cudaFree(plan->oz_scratch);
+        plan->oz_scratch = nullptr;
+        plan->oz_scratch_size = 0;
+        cudaError_t e = cudaMalloc(&plan->oz_scratch, need);
+        if (e != cudaSuccess) return cuda_fail(e, "emulation scratch");
+        plan->oz_scratch_size = need;
+    }
+    Bases bs{};
+    bs.b[BUF_IN] = reinterpret_cast<uint64_t>(x);
+    bs.b[BUF_OUT] = reinterpret_cast<uint64_t>(y);
+    bs.b[BUF_T] = reinterpret_cast<uint64_t>(plan->T);
+    bs.b[BUF_S] = reinterpret_cast<uint64_t>(plan->S);
+    cudaError_t e = oz_run(plan->oz1, bs, plan->slices, plan->oz_scratch, st);
+    if (e != cudaSuccess) return cuda_fail(e, "emulated stage 1");
+    if (oz_timed_out(plan->oz1, plan->oz_scratch, plan->slices, st))
+        return fail(DMRGB200_TIMEOUT, "emulated stage 1: a pipeline wait timed out");
+    e = run_sbuild(plan->prog, plan->T, plan->S, st);
+    if (e != cudaSuccess) return cuda_fail(e, "S build");
+    e = oz_run(plan->oz3, bs, plan->slices, plan->oz_scratch, st);
+    if (e != cudaSuccess) return cuda_fail(e, "emulated stage 3");
+    if (oz_timed_out(plan->oz3, plan->oz_scratch, plan->slices, st))
+        return fail(DMRGB200_TIMEOUT, "emulated stage 3: a pipeline wait timed out");
+    return DMRGB200_OK;
+}
+
 }  // namespace
 
 namespace dmrgb200 {
@@ -385,6 +431,9 @@ dmrgb200_status dmrgb200_plan_create_batched(dmrgb200_context_t ctx, uint32_t n,
 dmrgb200_status dmrgb200_plan_destroy(dmrgb200_plan_t plan) {
     if (!plan) return DMRGB200_OK;
     if (plan->compiled) free_program(plan->prog);
+    oz_free(plan->oz1);
+    oz_free(plan->oz3);
+    cudaFree(plan->oz_scratch);
     for (auto& e : plan->ev)
         if (e) cudaEventDestroy(e);
     cudaFree(plan->T);
@@ -409,12 +458,24 @@ dmrgb200_status dmrgb200_hpsi(dmrgb200_plan_t plan, const double* x, double* y, 
                               void* cuda_stream) {
     if (!plan || !x || !y) return fail(DMRGB200_INVALID_ARGUMENT, "null argument");
     if (plan->flat.kind != KIND_HPSI) return fail(DMRGB200_INVALID_PLAN, "plan is not an H psi plan");
-    if (prec != DMRGB200_PREC_FP64) return fail(DMRGB200_NOT_SUPPORTED, "precision not available in this build");
+    if (prec == DMRGB200_PREC_FP64_EMULATED) return hpsi_emulated(plan, x, y, static_cast<cudaStream_t>(cuda_stream));
+    if (prec != DMRGB200_PREC_FP64) return fail(DMRGB200_INVALID_ARGUMENT, "unknown precision");
     if (plan->timing) plan->collect();
     cudaError_t e = run_program(plan->prog, reinterpret_cast<uint64_t>(x), reinterpret_cast<uint64_t>(y), plan->T,
                                 plan->S, static_cast<cudaStream_t>(cuda_stream), plan->timing ? plan->ev : nullptr);
     if (e != cudaSuccess) return cuda_fail(e, "hpsi launch");
     if (plan->timing) plan->pending = true;
+    return DMRGB200_OK;
+}
+
+dmrgb200_status dmrgb200_plan_set_slices(dmrgb200_plan_t plan, int slices) {
+    if (!plan || slices < 2 || slices > 8) return fail(DMRGB200_INVALID_ARGUMENT, "slices must be 2..8");
+    if (slices != plan->slices) {
+        plan->slices = slices;
+        oz_free(plan->oz1);
+        oz_free(plan->oz3);
+        plan->oz1 = plan->oz3 = nullptr;
+    }
     return DMRGB200_OK;
 }
 

@@ -55,6 +55,19 @@ struct Bases {
     uint64_t b[NBUF];
 };
 
+#ifdef __CUDACC__
+// device address of buffer `buf`: a select chain keeps the kernel-parameter
+// array out of local memory
+__device__ __forceinline__ uint64_t base_of(Bases const& bs, uint32_t buf) {
+    uint64_t b = bs.b[0];
+    b = buf == 1 ? bs.b[1] : b;
+    b = buf == 2 ? bs.b[2] : b;
+    b = buf == 3 ? bs.b[3] : b;
+    b = buf == 4 ? bs.b[4] : b;
+    return b;
+}
+#endif
+
 template <class T>
 struct DevArray {
     T* ptr = nullptr;
@@ -99,6 +112,21 @@ cudaError_t run_program(DeviceProgram const& prog, uint64_t in, uint64_t out, do
                         cudaStream_t stream, cudaEvent_t const* ev = nullptr);
 
 int device_sm_count();
+// stage 2 only (S build), for the emulated path
+cudaError_t run_sbuild(DeviceProgram const& prog, double* T, double* S, cudaStream_t stream);
+// largest K of any output matrix of a GEMM list (emulation needs K * slices <= 2^17)
+uint64_t max_k_total(GemmList const& gl);
+
+// ---- FP64 emulated on the INT8 tensor cores (ozaki.cu) ----
+struct OzProgram;  // lowered grouped problem list
+OzProgram* oz_build(GemmList const& gl);
+void oz_free(OzProgram* oz);
+// device bytes the program needs for s digit planes (digits, exponents, error flag)
+uint64_t oz_scratch_bytes(OzProgram const* oz, int s);
+// run on the stream with scratch of oz_scratch_bytes(oz, s); returns a CUDA error
+cudaError_t oz_run(OzProgram* oz, Bases const& bs, int s, void* scratch, cudaStream_t st);
+// non-zero when a pipeline wait of the last run timed out (synchronises the stream)
+int oz_timed_out(OzProgram const* oz, void* scratch, int s, cudaStream_t st);
 double calibrate_fp64_tflops();
 
 }  // namespace dmrgb200

@@ -23,16 +23,6 @@ constexpr int BM = 32, BN = 64, BK = 16, NTHREADS = 128;
 constexpr int LDA_S = BM + 4, LDB_S = BN + 4;  // row strides = 8 words mod 32: conflict-free fragment loads
 constexpr int STAGES = 2;
 
-__device__ __forceinline__ uint64_t base_of(Bases const& bs, uint32_t buf) {
-    // a select chain keeps the kernel-parameter array out of local memory
-    uint64_t b = bs.b[0];
-    b = buf == 1 ? bs.b[1] : b;
-    b = buf == 2 ? bs.b[2] : b;
-    b = buf == 3 ? bs.b[3] : b;
-    b = buf == 4 ? bs.b[4] : b;
-    return b;
-}
-
 __device__ __forceinline__ const double* op_base(Bases const& bs, DevOp const& op, uint32_t batch) {
     return reinterpret_cast<const double*>(base_of(bs, op.buf) + 8ull * (op.off + uint64_t(batch) * op.bstride));
 }
@@ -492,6 +482,24 @@ double calibrate_fp64_tflops() {
     // one m8n8k4 DMMA = 8*8*4 FMA = 512 flops per warp instruction
     double flops = double(blocks) * 4 /*warps*/ * iters * 8 * 512.0;
     return ms > 0 ? flops / (ms * 1e-3) / 1e12 : 0.0;
+}
+
+cudaError_t run_sbuild(DeviceProgram const& prog, double* T, double* S, cudaStream_t stream) {
+    if (prog.n_lines) {
+        uint32_t grid = std::min<uint32_t>(prog.n_lines, uint32_t(device_sm_count()) * 8);
+        sbuild_lines<<<grid, 256, 0, stream>>>(prog.d_lines, prog.d_terms, prog.n_lines, S, T);
+    }
+    return cudaGetLastError();
+}
+
+uint64_t max_k_total(GemmList const& gl) {
+    uint64_t m = 0;
+    for (auto const& p : gl.probs) {
+        uint64_t k = 0;
+        for (uint32_t s = p.seg_begin; s < p.seg_end; ++s) k += gl.segs[s].K;
+        m = std::max(m, k);
+    }
+    return m;
 }
 
 int device_sm_count() {

@@ -23,6 +23,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include "../../include/dmrgb200.h"
 #include "device.hpp"
@@ -127,65 +128,111 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, int32_t (&v)[16]) {
 
 // ---- digit extraction --------------------------------------------------------------
 
-// per-row (A) or per-column (B) power-of-two exponent: |x 2^-e| < 1 for the whole row
-__global__ void row_exponents(const double* __restrict__ X, uint64_t ld, uint32_t rows, uint32_t cols,
-                              int along_rows, int* __restrict__ e) {
-    // along_rows = 1: row r spans X[r + c*ld] (A rows); 0: column r spans X[c + r*ld] (B columns)
-    uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (warp >= rows) return;
-    double m = 0.0;
-    for (uint32_t c = lane; c < cols; c += 32) {
-        double v = along_rows ? X[warp + c * ld] : X[c + uint64_t(warp) * ld];
-        m = fmax(m, fabs(v));
-    }
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if (lane == 0) e[warp] = (m > 0.0) ? ilogb(m) + 1 : 0;
+// One operand of one segment to be cut into digit planes.  For an A operand the
+// digit matrix is A itself (row r, column k); for a B operand it is B^T (row n,
+// column k), both stored K-major in 8 KB (A, 128 rows) or 4 KB (B, 64 rows)
+// tiles: tile (rt, ks) at out_base + (rt * KS + ks) * tile_bytes.
+struct OzSplit {
+    DevOp op;           // batch already folded into op.off
+    uint32_t rows, K;   // logical rows (M or N) and K of the segment
+    uint32_t RT, KS;    // row tiles, K slabs
+    uint64_t out_base;  // byte offset inside a digit plane
+    uint64_t e_off;     // exponent array offset of row 0
+    uint32_t is_b;      // 0: A operand, 1: B operand (read transposed)
+    uint32_t pad;
+};
+
+__device__ __forceinline__ double op_elem(Bases const& bs, OzSplit const& j, uint32_t r, uint32_t k) {
+    const double* base = reinterpret_cast<const double*>(base_of(bs, j.op.buf) + 8ull * j.op.off);
+    const uint64_t ld = j.op.ld;
+    if (!j.is_b) return j.op.trans ? base[k + uint64_t(r) * ld] : base[r + uint64_t(k) * ld];
+    // B(k, r): non-transposed B[k + r * ld], transposed B[r + k * ld]
+    return j.op.trans ? base[r + uint64_t(k) * ld] : base[k + uint64_t(r) * ld];
 }
 
-// digits of A (rows x K, element (r, k) at X[r + k*ld] when along_rows, else
-// X[k + r*ld] for B^T) into s tiled digit planes of shape (RT*128 or NT*64) x (KT*64)
-template <int TR>
-__global__ void split_digits(const double* __restrict__ X, uint64_t ld, uint32_t rows, uint32_t K, int along_rows,
-                             const int* __restrict__ e, int s, int8_t* __restrict__ out, uint32_t row_tiles,
-                             uint32_t k_tiles) {
-    const uint64_t plane = uint64_t(row_tiles) * k_tiles * TR * OZ_BK;
-    const uint64_t total = uint64_t(row_tiles) * TR * k_tiles * OZ_BK;
-    for (uint64_t idx = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; idx < total;
-         idx += uint64_t(gridDim.x) * blockDim.x) {
-        uint32_t r, k;
-        if (along_rows) {  // consecutive threads walk rows (contiguous in A)
-            r = uint32_t(idx % (uint64_t(row_tiles) * TR));
-            k = uint32_t(idx / (uint64_t(row_tiles) * TR));
-        } else {           // consecutive threads walk K (contiguous in B)
-            k = uint32_t(idx % (uint64_t(k_tiles) * OZ_BK));
-            r = uint32_t(idx / (uint64_t(k_tiles) * OZ_BK));
+__global__ void fill_int(int* __restrict__ p, uint64_t n, int v) {
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
+        p[i] = v;
+}
+
+// exponent of every row of every job (max over segments by atomicMax):
+// |x 2^-e| < 1 for the whole row of the output matrix
+__global__ void __launch_bounds__(256) oz_exponents(const OzSplit* __restrict__ jobs, uint32_t njobs, Bases bs,
+                                                    int* __restrict__ e) {
+    const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    for (uint32_t j = blockIdx.x; j < njobs; j += gridDim.x) {
+        const OzSplit job = jobs[j];
+        for (uint32_t r = wib; r < job.rows; r += blockDim.x >> 5) {
+            double m = 0.0;
+            for (uint32_t k = lane; k < job.K; k += 32) m = fmax(m, fabs(op_elem(bs, job, r, k)));
+            for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+            if (lane == 0 && m > 0.0) atomicMax(&e[job.e_off + r], ilogb(m) + 1);
         }
-        double x = 0.0;
-        if (r < rows && k < K) x = along_rows ? X[r + uint64_t(k) * ld] : X[k + uint64_t(r) * ld];
-        if (r < rows) x = ldexp(x, -e[r]);
-        uint64_t tile = uint64_t(r / TR) * k_tiles + (k / OZ_BK);
-        uint64_t off = tile * (TR * OZ_BK) + tile_off(r % TR, k % OZ_BK);
-        for (int p = 0; p < s; ++p) {
-            double t = x * 128.0;       // exact
-            double d = trunc(t);        // |d| <= 127
-            x = t - d;                  // exact
-            out[p * plane + off] = static_cast<int8_t>(d);
+    }
+}
+
+__global__ void __launch_bounds__(256) oz_split(const OzSplit* __restrict__ jobs, uint32_t njobs, Bases bs,
+                                                const int* __restrict__ e, int s, uint64_t a_plane,
+                                                int8_t* __restrict__ A8, uint64_t b_plane, int8_t* __restrict__ B8) {
+    for (uint32_t j = blockIdx.y; j < njobs; j += gridDim.y) {
+        const OzSplit job = jobs[j];
+        int8_t* out = job.is_b ? B8 : A8;
+        const uint64_t plane = job.is_b ? b_plane : a_plane;
+        const uint32_t TR = job.is_b ? uint32_t(OZ_BN) : uint32_t(OZ_BM);
+        const uint32_t tile_bytes = TR * OZ_BK;
+        const uint64_t total = uint64_t(job.RT) * TR * job.KS * OZ_BK;
+        for (uint64_t idx = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; idx < total;
+             idx += uint64_t(gridDim.x) * blockDim.x) {
+            uint32_t r, k;
+            if (!job.is_b && !job.op.trans) {  // walk rows: contiguous in a column-major A
+                r = uint32_t(idx % (uint64_t(job.RT) * TR));
+                k = uint32_t(idx / (uint64_t(job.RT) * TR));
+            } else {                             // walk K
+                k = uint32_t(idx % (uint64_t(job.KS) * OZ_BK));
+                r = uint32_t(idx / (uint64_t(job.KS) * OZ_BK));
+            }
+            double x = 0.0;
+            if (r < job.rows && k < job.K) x = ldexp(op_elem(bs, job, r, k), -e[job.e_off + r]);
+            const uint64_t off = job.out_base + (uint64_t(r / TR) * job.KS + k / OZ_BK) * tile_bytes +
+                                 tile_off(r % TR, k % OZ_BK);
+            for (int p = 0; p < s; ++p) {
+                const double t = x * 128.0;  // exact
+                const double d = trunc(t);   // |d| <= 127
+                x = t - d;                   // exact
+                out[p * plane + off] = static_cast<int8_t>(d);
+            }
         }
     }
 }
 
 // ---- MMA kernel ------------------------------------------------------------------------
 
+struct OzPB {  // one output matrix (a GEMM problem of one batch index)
+    uint32_t M, N, MT, NT;
+    uint32_t slab_begin, slab_end;  // K slabs (over all segments) in OzSlab
+    uint64_t e_off, f_off;          // exponents of its rows / columns
+    DevOp C;                        // destination (batch folded into C.off)
+    uint32_t beta, pad;
+};
+struct OzSlab {  // K slab: A tile of row tile mt at a_off + mt * a_ts, B tile of nt at b_off + nt * b_ts
+    uint64_t a_off, b_off;
+    uint32_t a_ts, b_ts;
+};
+struct OzTile {
+    uint32_t pb, mt, nt, pad;
+};
+
 struct OzArgs {
-    const int8_t* A8;  // s planes of MT x KT tiles (8 KB each)
-    const int8_t* B8;  // s planes of NT x KT tiles (4 KB each)
-    const int* e;      // row exponents of A (M)
-    const int* f;      // column exponents of B (N)
-    double* C;
-    uint64_t ldc;
-    uint32_t M, N, MT, NT, KT;
+    const int8_t* A8;
+    const int8_t* B8;
+    uint64_t a_plane, b_plane;  // bytes per digit plane
+    const int* e;
+    const OzPB* pbs;
+    const OzSlab* slabs;
+    const OzTile* tiles;
+    uint32_t n_tiles;
     int s;
-    int beta;          // 0: C = A B, 1: C += A B
+    Bases bases;
     int* err;
 };
 
@@ -199,7 +246,6 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_mma(OzArgs a) {
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t ncols = (s * OZ_BN <= 256) ? ((s * OZ_BN <= 128) ? 128u : 256u) : 512u;
-    const uint64_t a_plane = uint64_t(a.MT) * a.KT * A_TILE, b_plane = uint64_t(a.NT) * a.KT * B_TILE;
     const uint32_t idesc = idesc_i8(OZ_BM, OZ_BN);
     volatile int* verr = a.err;
 
@@ -224,26 +270,30 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_mma(OzArgs a) {
     // running slab / tile counters: every arrival on every barrier is waited for exactly once, in order
     uint32_t slab0 = 0, tiles = 0, issued = 0, consumed = 0;
     bool failed = false;
-    for (uint32_t tile = blockIdx.x; tile < a.MT * a.NT && !failed; tile += gridDim.x) {
-        const uint32_t mt = tile % a.MT, nt = tile / a.MT;
+    for (uint32_t tile = blockIdx.x; tile < a.n_tiles && !failed; tile += gridDim.x) {
+        const OzTile tl = a.tiles[tile];
+        const OzPB pb = a.pbs[tl.pb];
+        const uint32_t mt = tl.mt, nt = tl.nt;
+        const uint32_t KT = pb.slab_end - pb.slab_begin;
         if (threadIdx.x == 0) {
             auto load = [&](uint32_t kt) -> bool {
                 const uint32_t gs = slab0 + kt, st = gs % OZ_STAGES;
                 if (gs >= OZ_STAGES && !mbar_wait(&empty[st], ((gs - OZ_STAGES) / OZ_STAGES) & 1u, a.err)) return false;
+                const OzSlab sl = a.slabs[pb.slab_begin + kt];
                 unsigned char* base = smem + st * stage_bytes;
                 mbar_expect_tx(&full[st], stage_bytes);
                 for (int p = 0; p < s; ++p) {
-                    bulk_load(base + p * A_TILE, a.A8 + p * a_plane + (uint64_t(mt) * a.KT + kt) * A_TILE, A_TILE,
+                    bulk_load(base + p * A_TILE, a.A8 + p * a.a_plane + sl.a_off + uint64_t(mt) * sl.a_ts, A_TILE,
                               &full[st]);
-                    bulk_load(base + s * A_TILE + p * B_TILE,
-                              a.B8 + p * b_plane + (uint64_t(nt) * a.KT + kt) * B_TILE, B_TILE, &full[st]);
+                    bulk_load(base + s * A_TILE + p * B_TILE, a.B8 + p * a.b_plane + sl.b_off + uint64_t(nt) * sl.b_ts,
+                              B_TILE, &full[st]);
                 }
                 ++issued;
                 return true;
             };
             bool ok = true;
-            for (uint32_t kt = 0; kt < a.KT && kt < OZ_STAGES && ok; ++kt) ok = load(kt);
-            for (uint32_t kt = 0; kt < a.KT && ok; ++kt) {
+            for (uint32_t kt = 0; kt < KT && kt < OZ_STAGES && ok; ++kt) ok = load(kt);
+            for (uint32_t kt = 0; kt < KT && ok; ++kt) {
                 const uint32_t gs = slab0 + kt, st = gs % OZ_STAGES;
                 ok = mbar_wait(&full[st], (gs / OZ_STAGES) & 1u, a.err);
                 if (!ok) break;
@@ -260,12 +310,12 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_mma(OzArgs a) {
                             umma_i8(tmem + uint32_t(g * OZ_BN), da, db, idesc, accum);
                         }
                 umma_commit(&empty[st]);
-                if (kt + OZ_STAGES < a.KT) ok = load(kt + OZ_STAGES);
+                if (kt + OZ_STAGES < KT) ok = load(kt + OZ_STAGES);
             }
             if (!ok) atomicExch(a.err, 1);
             umma_commit(done);  // arrives once every MMA issued so far has completed
         }
-        slab0 += a.KT;
+        slab0 += KT;
         __syncwarp();
         const bool ready = mbar_wait(done, tiles & 1u, a.err);
         ++tiles;
@@ -273,26 +323,27 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_mma(OzArgs a) {
         const bool go = __all_sync(0xffffffffu, ready && *verr == 0);
         if (go) {
             const uint32_t row = mt * OZ_BM + warp * 32 + lane;
-            const double escale = (row < a.M) ? ldexp(1.0, a.e[row]) : 0.0;
+            const int erow = (row < pb.M) ? a.e[pb.e_off + row] : 0;
+            double* Cb = reinterpret_cast<double*>(base_of(a.bases, pb.C.buf) + 8ull * pb.C.off);
             for (int c0 = 0; c0 < OZ_BN; c0 += 16) {
                 double acc[16];
 #pragma unroll
                 for (int j = 0; j < 16; ++j) acc[j] = 0.0;
-                for (int g = s - 1; g >= 0; --g) {
+                for (int g = s - 1; g >= 0 && KT > 0; --g) {
                     int32_t v[16];
                     tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + uint32_t(g * OZ_BN + c0), v);
                     const double w = ldexp(1.0, -7 * (g + 2));
 #pragma unroll
                     for (int j = 0; j < 16; ++j) acc[j] += double(v[j]) * w;
                 }
-                if (row < a.M) {
+                if (row < pb.M) {
 #pragma unroll
                     for (int j = 0; j < 16; ++j) {
                         const uint32_t col = nt * OZ_BN + c0 + j;
-                        if (col < a.N) {
-                            double val = acc[j] * escale * ldexp(1.0, a.f[col]);
-                            double* dst = a.C + row + uint64_t(col) * a.ldc;
-                            *dst = a.beta ? *dst + val : val;
+                        if (col < pb.N) {
+                            const double val = ldexp(acc[j], erow + a.e[pb.f_off + col]);
+                            double* dst = Cb + row + uint64_t(col) * pb.C.ld;
+                            *dst = pb.beta ? *dst + val : val;
                         }
                     }
                 }
@@ -322,41 +373,166 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_mma(OzArgs a) {
 
 size_t ozaki_smem_bytes(int s) { return size_t(OZ_STAGES) * s * (A_TILE + B_TILE) + 8 * (2 * OZ_STAGES + 1) + 16; }
 
-// C (M x N, ldc) = A (M x K, lda) * B (K x N, ldb), all column-major FP64, on the stream.
-// Scratch digit planes are allocated stream-ordered.
-cudaError_t ozaki_dgemm(uint32_t M, uint32_t N, uint32_t K, const double* A, uint64_t lda, const double* B,
-                        uint64_t ldb, double* C, uint64_t ldc, int s, int beta, cudaStream_t st, int* err_flag) {
-    const uint32_t MT = (M + OZ_BM - 1) / OZ_BM, NT = (N + OZ_BN - 1) / OZ_BN, KT = (K + OZ_BK - 1) / OZ_BK;
-    if (!M || !N) return cudaSuccess;
-    const uint64_t a_bytes = uint64_t(s) * MT * KT * A_TILE, b_bytes = uint64_t(s) * NT * KT * B_TILE;
-    int8_t *A8 = nullptr, *B8 = nullptr;
-    int *e = nullptr, *f = nullptr;
-    cudaError_t r;
-    if ((r = cudaMallocAsync(&A8, a_bytes, st)) != cudaSuccess) return r;
-    if ((r = cudaMallocAsync(&B8, b_bytes, st)) != cudaSuccess) return r;
-    if ((r = cudaMallocAsync(&e, sizeof(int) * MT * OZ_BM, st)) != cudaSuccess) return r;
-    if ((r = cudaMallocAsync(&f, sizeof(int) * NT * OZ_BN, st)) != cudaSuccess) return r;
-    cudaMemsetAsync(e, 0, sizeof(int) * MT * OZ_BM, st);
-    cudaMemsetAsync(f, 0, sizeof(int) * NT * OZ_BN, st);
-    const int sms = device_sm_count();
-    row_exponents<<<(M * 32 + 255) / 256, 256, 0, st>>>(A, lda, M, K, 1, e);
-    row_exponents<<<(N * 32 + 255) / 256, 256, 0, st>>>(B, ldb, N, K, 0, f);
-    split_digits<OZ_BM><<<sms * 8, 256, 0, st>>>(A, lda, M, K, 1, e, s, A8, MT, KT);
-    split_digits<OZ_BN><<<sms * 8, 256, 0, st>>>(B, ldb, N, K, 0, f, s, B8, NT, KT);
-    OzArgs args{A8, B8, e, f, C, ldc, M, N, MT, NT, KT, s, beta, err_flag};
-    const size_t smem = ozaki_smem_bytes(s);
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(ozaki_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, int(ozaki_smem_bytes(OZ_MAX_SLICES)));
-        attr = true;
+struct OzProgram {
+    std::vector<OzSplit> jobs;
+    std::vector<OzPB> pbs;
+    std::vector<OzSlab> slabs;
+    std::vector<OzTile> tiles;
+    uint64_t a_plane = 0, b_plane = 0, n_exp = 0;
+    OzSplit* d_jobs = nullptr;
+    OzPB* d_pbs = nullptr;
+    OzSlab* d_slabs = nullptr;
+    OzTile* d_tiles = nullptr;
+};
+
+OzProgram* oz_build(GemmList const& gl) {
+    auto* oz = new OzProgram;
+    std::vector<uint32_t> nbatch(gl.probs.size(), 0);
+    for (auto const& t : gl.tiles) nbatch[t.prob] = std::max(nbatch[t.prob], t.batch + 1);
+    for (uint32_t p = 0; p < gl.probs.size(); ++p) {
+        DevProb const& pr = gl.probs[p];
+        for (uint32_t b = 0; b < nbatch[p]; ++b) {
+            OzPB pb{};
+            pb.M = pr.M;
+            pb.N = pr.N;
+            pb.MT = std::max<uint32_t>(1, (pr.M + OZ_BM - 1) / OZ_BM);
+            pb.NT = std::max<uint32_t>(1, (pr.N + OZ_BN - 1) / OZ_BN);
+            pb.e_off = oz->n_exp;
+            oz->n_exp += uint64_t(pb.MT) * OZ_BM;
+            pb.f_off = oz->n_exp;
+            oz->n_exp += uint64_t(pb.NT) * OZ_BN;
+            pb.C = pr.C;
+            pb.C.off += uint64_t(b) * pr.C.bstride;
+            pb.beta = 0;
+            pb.slab_begin = uint32_t(oz->slabs.size());
+            for (uint32_t sgi = pr.seg_begin; sgi < pr.seg_end; ++sgi) {
+                DevSeg const& sg = gl.segs[sgi];
+                if (!sg.K) continue;
+                const uint32_t KS = (sg.K + OZ_BK - 1) / OZ_BK;
+                OzSplit ja{}, jb{};
+                ja.op = sg.A;
+                ja.op.off += uint64_t(b) * sg.A.bstride;
+                ja.rows = pr.M;
+                ja.K = sg.K;
+                ja.RT = pb.MT;
+                ja.KS = KS;
+                ja.out_base = oz->a_plane;
+                ja.e_off = pb.e_off;
+                ja.is_b = 0;
+                oz->a_plane += uint64_t(pb.MT) * KS * A_TILE;
+                jb.op = sg.B;
+                jb.op.off += uint64_t(b) * sg.B.bstride;
+                jb.rows = pr.N;
+                jb.K = sg.K;
+                jb.RT = pb.NT;
+                jb.KS = KS;
+                jb.out_base = oz->b_plane;
+                jb.e_off = pb.f_off;
+                jb.is_b = 1;
+                oz->b_plane += uint64_t(pb.NT) * KS * B_TILE;
+                for (uint32_t ks = 0; ks < KS; ++ks)
+                    oz->slabs.push_back(OzSlab{ja.out_base + uint64_t(ks) * A_TILE, jb.out_base + uint64_t(ks) * B_TILE,
+                                               KS * uint32_t(A_TILE), KS * uint32_t(B_TILE)});
+                oz->jobs.push_back(ja);
+                oz->jobs.push_back(jb);
+            }
+            pb.slab_end = uint32_t(oz->slabs.size());
+            uint32_t pbi = uint32_t(oz->pbs.size());
+            oz->pbs.push_back(pb);
+            for (uint32_t mt = 0; mt < pb.MT; ++mt)
+                for (uint32_t nt = 0; nt < pb.NT; ++nt) oz->tiles.push_back(OzTile{pbi, mt, nt, 0});
+        }
     }
-    ozaki_mma<<<std::min<uint32_t>(MT * NT, uint32_t(sms)), OZ_THREADS, smem, st>>>(args);
-    r = cudaGetLastError();
-    cudaFreeAsync(A8, st);
-    cudaFreeAsync(B8, st);
-    cudaFreeAsync(e, st);
-    cudaFreeAsync(f, st);
-    return r;
+    // longest K first for the static round-robin over the persistent grid
+    std::stable_sort(oz->tiles.begin(), oz->tiles.end(), [&](OzTile const& x, OzTile const& y) {
+        auto kx = oz->pbs[x.pb].slab_end - oz->pbs[x.pb].slab_begin;
+        auto ky = oz->pbs[y.pb].slab_end - oz->pbs[y.pb].slab_begin;
+        return kx > ky;
+    });
+    auto up = [](auto const& v, auto** d) -> cudaError_t {
+        *d = nullptr;
+        if (v.empty()) return cudaSuccess;
+        cudaError_t e = cudaMalloc(d, v.size() * sizeof(v[0]));
+        if (e != cudaSuccess) return e;
+        return cudaMemcpy(*d, v.data(), v.size() * sizeof(v[0]), cudaMemcpyHostToDevice);
+    };
+    if (up(oz->jobs, &oz->d_jobs) != cudaSuccess || up(oz->pbs, &oz->d_pbs) != cudaSuccess ||
+        up(oz->slabs, &oz->d_slabs) != cudaSuccess || up(oz->tiles, &oz->d_tiles) != cudaSuccess) {
+        oz_free(oz);
+        return nullptr;
+    }
+    return oz;
+}
+
+void oz_free(OzProgram* oz) {
+    if (!oz) return;
+    cudaFree(oz->d_jobs);
+    cudaFree(oz->d_pbs);
+    cudaFree(oz->d_slabs);
+    cudaFree(oz->d_tiles);
+    delete oz;
+}
+
+namespace {
+struct OzScratch {
+    int8_t* A8;
+    int8_t* B8;
+    int* e;
+    int* err;
+};
+OzScratch carve(OzProgram const* oz, int s, void* scratch) {
+    auto* p = static_cast<unsigned char*>(scratch);
+    OzScratch c;
+    c.A8 = reinterpret_cast<int8_t*>(p);
+    p += round_up(uint64_t(s) * oz->a_plane, 256);
+    c.B8 = reinterpret_cast<int8_t*>(p);
+    p += round_up(uint64_t(s) * oz->b_plane, 256);
+    c.e = reinterpret_cast<int*>(p);
+    p += round_up(oz->n_exp * sizeof(int), 256);
+    c.err = reinterpret_cast<int*>(p);
+    return c;
+}
+}  // namespace
+
+uint64_t oz_scratch_bytes(OzProgram const* oz, int s) {
+    return round_up(uint64_t(s) * oz->a_plane, 256) + round_up(uint64_t(s) * oz->b_plane, 256) +
+           round_up(oz->n_exp * sizeof(int), 256) + 256;
+}
+
+cudaError_t oz_run(OzProgram* oz, Bases const& bs, int s, void* scratch, cudaStream_t st) {
+    if (s < 2 || s > OZ_MAX_SLICES) return cudaErrorInvalidValue;
+    OzScratch c = carve(oz, s, scratch);
+    const int sms = device_sm_count();
+    cudaMemsetAsync(c.err, 0, sizeof(int), st);
+    if (oz->n_exp)
+        fill_int<<<std::min<uint64_t>((oz->n_exp + 255) / 256, 4096), 256, 0, st>>>(c.e, oz->n_exp, -100000);
+    const uint32_t nj = uint32_t(oz->jobs.size());
+    if (nj) {
+        oz_exponents<<<std::min<uint32_t>(nj, uint32_t(sms) * 8), 256, 0, st>>>(oz->d_jobs, nj, bs, c.e);
+        dim3 grid(16, std::min<uint32_t>(nj, 65535u));
+        oz_split<<<grid, 256, 0, st>>>(oz->d_jobs, nj, bs, c.e, s, oz->a_plane, c.A8, oz->b_plane, c.B8);
+    }
+    if (!oz->tiles.empty()) {
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(ozaki_mma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(ozaki_smem_bytes(OZ_MAX_SLICES)));
+            attr = true;
+        }
+        OzArgs args{c.A8, c.B8, oz->a_plane, oz->b_plane, c.e, oz->d_pbs, oz->d_slabs, oz->d_tiles,
+                    uint32_t(oz->tiles.size()), s, bs, c.err};
+        ozaki_mma<<<std::min<uint32_t>(uint32_t(oz->tiles.size()), uint32_t(sms)), OZ_THREADS, ozaki_smem_bytes(s),
+                    st>>>(args);
+    }
+    return cudaGetLastError();
+}
+
+int oz_timed_out(OzProgram const* oz, void* scratch, int s, cudaStream_t st) {
+    OzScratch c = carve(oz, s, scratch);
+    int h = 0;
+    cudaMemcpyAsync(&h, c.err, sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    return h;
 }
 
 }  // namespace dmrgb200
@@ -372,17 +548,37 @@ extern "C" dmrgb200_status dmrgb200_dgemm_emulated(uint32_t M, uint32_t N, uint3
         return noalloc_fail(DMRGB200_INVALID_ARGUMENT, "K * slices exceeds the exact INT32 accumulation range");
     if (lda < M || ldb < K || ldc < M) return noalloc_fail(DMRGB200_INVALID_ARGUMENT, "leading dimension too small");
     cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
-    int* err = nullptr;
-    cudaError_t r = cudaMallocAsync(&err, sizeof(int), st);
-    if (r != cudaSuccess) return noalloc_fail(DMRGB200_OUT_OF_MEMORY, cudaGetErrorString(r));
-    cudaMemsetAsync(err, 0, sizeof(int), st);
-    r = ozaki_dgemm(M, N, K, A, lda, B, ldb, C, ldc, slices, 0, st, err);
-    int h_err = 0;
-    cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, st);
+    GemmList gl;
+    DevProb pr{};
+    pr.M = M;
+    pr.N = N;
+    pr.C = DevOp{reinterpret_cast<uint64_t>(C) / 8, 0, uint32_t(ldc), uint16_t(BUF_ABS), 0};
+    pr.seg_begin = 0;
+    pr.seg_end = 1;
+    DevSeg sg{};
+    sg.A = DevOp{reinterpret_cast<uint64_t>(A) / 8, 0, uint32_t(lda), uint16_t(BUF_ABS), 0};
+    sg.B = DevOp{reinterpret_cast<uint64_t>(B) / 8, 0, uint32_t(ldb), uint16_t(BUF_ABS), 0};
+    sg.K = K;
+    gl.probs.push_back(pr);
+    gl.segs.push_back(sg);
+    gl.tiles.push_back(DevTile{0, 0, 0, 0});
+    OzProgram* oz = oz_build(gl);
+    if (!oz) return noalloc_fail(DMRGB200_OUT_OF_MEMORY, "emulated GEMM tables");
+    void* scratch = nullptr;
+    cudaError_t r = cudaMallocAsync(&scratch, oz_scratch_bytes(oz, slices), st);
+    if (r != cudaSuccess) {
+        oz_free(oz);
+        return noalloc_fail(DMRGB200_OUT_OF_MEMORY, cudaGetErrorString(r));
+    }
+    Bases bs{};
+    r = oz_run(oz, bs, slices, scratch, st);
+    int to = oz_timed_out(oz, scratch, slices, st);
     cudaError_t r2 = cudaStreamSynchronize(st);
-    cudaFree(err);
+    cudaFreeAsync(scratch, st);
+    cudaStreamSynchronize(st);
+    oz_free(oz);
     if (r != cudaSuccess) return noalloc_fail(DMRGB200_DEVICE_ERROR, std::string("emulated GEMM: ") + cudaGetErrorString(r));
     if (r2 != cudaSuccess) return noalloc_fail(DMRGB200_DEVICE_ERROR, std::string("emulated GEMM: ") + cudaGetErrorString(r2));
-    if (h_err) return noalloc_fail(DMRGB200_TIMEOUT, "emulated GEMM: a pipeline wait timed out");
+    if (to) return noalloc_fail(DMRGB200_TIMEOUT, "emulated GEMM: a pipeline wait timed out");
     return DMRGB200_OK;
 }

@@ -155,6 +155,99 @@ def cpu_reference(model, bonds, tensors, i, psi, seconds=15.0, threads=None):
                      if use_ref else "oracle restatement of the reference CPU path") + ", OpenMP + OpenBLAS"}
 
 
+def sweep_workload(args):
+    """Heisenberg L=32, J=1, U1 (Sz=0), two-site DMRG, m=128,
+    4 sweeps, JD tol 1e-8 (max 8 iterations), seeded random initial MPS (every
+    allowed sector of dimension <= 5, uniform[0,1) blocks, normalised).  The same
+    sweeps are replayed on the CPU oracle (reference JD + schedule execution
+    restatements) and the per-site energies compared."""
+    import torch
+    from dmrgb200 import dmrg as G
+    from dmrgb200 import engine as E
+    from dmrgb200 import models as M
+    from dmrgb200 import mps as S
+    from sweep_backend import OracleBackend
+
+    L, m, nsweeps = 32, 128, 4
+    model = M.heisenberg(L)
+    rng = np.random.default_rng(1)
+    A = S.random_mps(model.phys, S.allowed_sectors(model.phys, L, model.total_charge, 5), rng)
+    ctx = E.Context(0)
+    dev = G.TwoSiteDMRG(G.DeviceBackend(ctx), model, list(A), m, jd_tol=1e-8, jd_maxiter=8)
+    for sw in range(nsweeps):
+        dev.sweep(sw)
+    cpu_t0 = time.perf_counter()
+    cpu = G.TwoSiteDMRG(OracleBackend(), model, list(A), m, jd_tol=1e-8, jd_maxiter=8)
+    for sw in range(nsweeps):
+        cpu.sweep(sw)
+    cpu_s = time.perf_counter() - cpu_t0
+    ed = np.array([e[2] for e in dev.log.energies])
+    ec = np.array([e[2] for e in cpu.log.energies])
+    line = {"metric": "two-site sweep time (s)", "value": float(np.mean(dev.log.sweep_seconds)), "unit": "s",
+            "higher_is_better": False, "n_gpus": 1, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "heisenberg_L32_u1_m128_4sweeps", "sites": L, "bond_dim": m, "sweeps": nsweeps},
+            "sweep_seconds": dev.log.sweep_seconds, "final_energy": float(ed[-1]),
+            "max_abs_energy_diff_vs_oracle": float(np.max(np.abs(ed - ec))),
+            "hpsi_calls": dev.log.hpsi_calls, "hpsi_device_ms": dev.log.hpsi_ms,
+            "cpu_oracle_sweep_seconds": cpu.log.sweep_seconds, "cpu_oracle_final_energy": float(ec[-1]),
+            "note": "two-site formation and SVD truncation on the host (numpy); H·psi, JD and boundary steps on the device"}
+    print(json.dumps(line), flush=True)
+
+
+def batched_workload(args):
+    """64 independent site problems (32 Heisenberg U1, 32
+    Fermi-Hubbard TwoU1, chains of 32 sites, middle two-site problem), bond
+    dimensions log-uniform in [64, 1024] (seed 6), merged into one batched plan:
+    every H·psi stage is a single launch over all instances.  20 H·psi steps
+    (the Davidson iterations' products) are timed in FP64 and emulated FP64."""
+    import torch
+    from dmrgb200 import _capi as capi
+    from dmrgb200 import engine as E
+    from dmrgb200 import models as M
+    from dmrgb200 import mps as S
+
+    rng = np.random.default_rng(6)
+    ctx = E.Context(0)
+    items, keep, xs = [], [], []
+    for k in range(64):
+        L = 32
+        model = M.heisenberg(L) if k % 2 == 0 else M.fermi_hubbard(L)
+        m = int(round(np.exp(rng.uniform(np.log(64), np.log(1024)))))
+        radius = 10.0 if k % 2 == 0 else 3.5
+        bonds = S.synthetic_bonds(model.phys, L, model.total_charge, m, radius)
+        tensors = S.random_mps(model.phys, bonds, rng)
+        sp = E.SiteProblem(ctx, model, tensors, bonds, L // 2 - 1)
+        items.append((sp.schedule.plan, sp.Lidx.cohort_addresses(sp.Lbuf.data_ptr()),
+                      sp.Ridx.cohort_addresses(sp.Rbuf.data_ptr())))
+        keep.append(sp)
+    bp = E.BatchedPlan(ctx, items)
+    x = torch.rand(bp.total_size, dtype=torch.float64, device="cuda")
+    y = torch.zeros_like(x)
+    res = {}
+    for name, prec in (("fp64", capi.PREC_FP64), ("emulated", capi.PREC_FP64_EMULATED)):
+        for _ in range(3):
+            bp.hpsi(x.data_ptr(), y.data_ptr(), prec)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(20):
+            bp.hpsi(x.data_ptr(), y.data_ptr(), prec)
+        b.record()
+        b.synchronize()
+        ms = a.elapsed_time(b) / 20
+        res[name] = {"ms_per_step": ms, "value": bp.flops / (ms * 1e-3) / 1e9, "unit": "GFLOP/s"}
+        if name == "fp64":
+            y64 = y.clone()
+        else:
+            res[name]["rel_err_vs_fp64"] = float(torch.linalg.norm(y - y64) / torch.linalg.norm(y64))
+    line = {"metric": "batched H·psi GFLOP/s (FP64)", "value": res["fp64"]["value"], "unit": "GFLOP/s",
+            "higher_is_better": True, "n_gpus": 1, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "64_instances_heisenberg_u1_hubbard_twou1_L32_m_loguniform_64_1024",
+                       "instances": 64, "flops_per_step": int(bp.flops), "psi_elements": int(bp.total_size)},
+            "fp64": res["fp64"], "emulated": res["emulated"]}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -162,10 +255,21 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--workload", default="hpsi", choices=["hpsi", "sweep", "batched"],
+                    help="hpsi: the headline H·psi line (default); sweep: config-1 sweeps; batched: config-5")
+    ap.add_argument("--prec", default="fp64", choices=["fp64", "emulated"],
+                    help="precision of the --profile steps")
     ap.add_argument("--profile", action="store_true",
                     help="only warm-up and timed H·psi steps (for ncu launch lists and captures)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+
+    if args.workload == "sweep":
+        sweep_workload(args)
+        os._exit(0)
+    if args.workload == "batched":
+        batched_workload(args)
+        os._exit(0)
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -216,8 +320,9 @@ def main():
     yd = torch.zeros_like(xd)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
+    prof_prec = capi.PREC_FP64_EMULATED if (args.profile and args.prec == "emulated") else capi.PREC_FP64
     for _ in range(args.warmup):
-        sp.plan.hpsi(xd.data_ptr(), yd.data_ptr(), capi.PREC_FP64, sh)
+        sp.plan.hpsi(xd.data_ptr(), yd.data_ptr(), prof_prec, sh)
     torch.cuda.synchronize(dev)
 
     clk_path = tempfile.mktemp(suffix=".csv")
@@ -233,7 +338,7 @@ def main():
     for k in range(args.steps):
         flush.fill_(float(k))
         ev[k][0].record(stream)
-        sp.plan.hpsi(xd.data_ptr(), yd.data_ptr(), capi.PREC_FP64, sh)
+        sp.plan.hpsi(xd.data_ptr(), yd.data_ptr(), prof_prec, sh)
         ev[k][1].record(stream)
     torch.cuda.synchronize(dev)
     step_ms = [a.elapsed_time(b) for a, b in ev]

@@ -195,12 +195,44 @@ class SweepLog:
     hpsi_ms: float = 0.0
 
 
-class TwoSiteDMRG:
-    def __init__(self, ctx: E.Context, model: M.Model, tensors, m: int, cutoff: float = 1e-16,
-                 jd_tol: float = 1e-8, jd_maxiter: int = 8):
+class DeviceBackend:
+    """Hot-path operations on the device through libdmrgb200: boundary steps,
+    H·psi plans and the Jacobi-Davidson solver (dmrgb200_solve)."""
+
+    def __init__(self, ctx: E.Context):
         import torch
-        self.torch = torch
-        self.ctx, self.model, self.m, self.cutoff = ctx, model, m, cutoff
+        self.torch, self.ctx = torch, ctx
+
+    def edge(self, symm, index):
+        idx = E.edge_bindex(symm, index)
+        return idx, E.to_device(idx.edge_values(), self.ctx.device)
+
+    def left_step(self, model, W, Lidx, Lbuf, t: S.SiteTensor):
+        dev = self.ctx.device
+        return E.device_left_step(self.ctx, model.phys, t.left, t.right, W, Lidx, Lbuf, E.to_device(t.data, dev),
+                                  E.to_device(t.left_paired(), dev), True)
+
+    def right_step(self, model, W, Ridx, Rbuf, t: S.SiteTensor):
+        td = E.to_device(t.data, self.ctx.device)
+        return E.device_right_step(self.ctx, model.phys, t.left, t.right, W, Ridx, Rbuf, td, td, True)
+
+    def solve(self, p12, psi: S.SiteTensor, W12, Lidx, Lbuf, Ridx, Rbuf, tol, max_iter):
+        sched = E.schedule_hpsi(p12, psi.left, psi.right, W12, Lidx, Ridx)
+        plan = E.DevicePlan(self.ctx, sched.plan, left_addr=Lidx.cohort_addresses(Lbuf.data_ptr()),
+                            other_addr=Ridx.cohort_addresses(Rbuf.data_ptr()))
+        xd = E.to_device(psi.data, self.ctx.device)
+        xo = self.torch.zeros_like(xd)
+        energy, st = plan.solve(xd.data_ptr(), xo.data_ptr(), xd.numel(), tol=tol, max_iter=max_iter)
+        return energy, xo.cpu().numpy(), st.iterations, st.hpsi_ms
+
+    def sync(self):
+        self.torch.cuda.synchronize(self.ctx.device)
+
+
+class TwoSiteDMRG:
+    def __init__(self, backend, model: M.Model, tensors, m: int, cutoff: float = 1e-16, jd_tol: float = 1e-8,
+                 jd_maxiter: int = 8):
+        self.be, self.model, self.m, self.cutoff = backend, model, m, cutoff
         self.jd_tol, self.jd_maxiter = jd_tol, jd_maxiter
         self.L = len(tensors)
         self.A = right_canonicalize(tensors)
@@ -208,52 +240,38 @@ class TwoSiteDMRG:
         self.W = [M.MPOHandle(w, model.symm) for w in model.mpo]
         self.W12 = [M.MPOHandle(M.twosite_mpo(model.mpo[i], model.mpo[i + 1], model.phys, model.phys), model.symm)
                     for i in range(self.L - 1)]
-        dev = ctx.device
-        bonds0 = self.A[0].left
         self.Lidx = [None] * (self.L + 1)
         self.Lbuf = [None] * (self.L + 1)
         self.Ridx = [None] * (self.L + 1)
         self.Rbuf = [None] * (self.L + 1)
-        self.Lidx[0] = E.edge_bindex(model.symm, bonds0)
-        self.Lbuf[0] = E.to_device(self.Lidx[0].edge_values(), dev)
-        self.Ridx[self.L] = E.edge_bindex(model.symm, self.A[-1].right)
-        self.Rbuf[self.L] = E.to_device(self.Ridx[self.L].edge_values(), dev)
+        self.Lidx[0], self.Lbuf[0] = self.be.edge(model.symm, self.A[0].left)
+        self.Ridx[self.L], self.Rbuf[self.L] = self.be.edge(model.symm, self.A[-1].right)
         for j in range(self.L - 1, 1, -1):
             self._right_step(j)
         self.log = SweepLog()
 
     def _left_step(self, j):
-        t = self.A[j]
-        dev = self.ctx.device
-        self.Lidx[j + 1], self.Lbuf[j + 1] = E.device_left_step(
-            self.ctx, self.model.phys, t.left, t.right, self.W[j], self.Lidx[j], self.Lbuf[j],
-            E.to_device(t.data, dev), E.to_device(t.left_paired(), dev), True)
+        self.Lidx[j + 1], self.Lbuf[j + 1] = self.be.left_step(self.model, self.W[j], self.Lidx[j], self.Lbuf[j],
+                                                               self.A[j])
 
     def _right_step(self, j):
-        t = self.A[j]
-        td = E.to_device(t.data, self.ctx.device)
-        self.Ridx[j], self.Rbuf[j] = E.device_right_step(
-            self.ctx, self.model.phys, t.left, t.right, self.W[j], self.Ridx[j + 1], self.Rbuf[j + 1], td, td, True)
+        self.Ridx[j], self.Rbuf[j] = self.be.right_step(self.model, self.W[j], self.Ridx[j + 1], self.Rbuf[j + 1],
+                                                        self.A[j])
 
     def optimize_pair(self, i, left_to_right):
-        torch = self.torch
         psi = twosite(self.A[i], self.A[i + 1], self.p12, self.offs)
-        sched = E.schedule_hpsi(self.p12, psi.left, psi.right, self.W12[i], self.Lidx[i], self.Ridx[i + 2])
-        plan = E.DevicePlan(self.ctx, sched.plan, left_addr=self.Lidx[i].cohort_addresses(self.Lbuf[i].data_ptr()),
-                            other_addr=self.Ridx[i + 2].cohort_addresses(self.Rbuf[i + 2].data_ptr()))
-        xd = E.to_device(psi.data, self.ctx.device)
-        xo = torch.zeros_like(xd)
-        energy, st = plan.solve(xd.data_ptr(), xo.data_ptr(), xd.numel(), tol=self.jd_tol, max_iter=self.jd_maxiter)
-        self.log.hpsi_calls += st.iterations
-        self.log.hpsi_ms += st.hpsi_ms
-        psi.data = xo.cpu().numpy()
+        energy, xo, iters, ms = self.be.solve(self.p12, psi, self.W12[i], self.Lidx[i], self.Lbuf[i],
+                                              self.Ridx[i + 2], self.Rbuf[i + 2], self.jd_tol, self.jd_maxiter)
+        self.log.hpsi_calls += iters
+        self.log.hpsi_ms += ms
+        psi.data = xo
         res = split(psi, self.model.phys, self.model.phys, self.offs, self.m, self.cutoff, left_to_right)
         self.A[i], self.A[i + 1] = res.A, res.B
         if left_to_right:
             self._left_step(i)
         else:
             self._right_step(i + 1)
-        return energy, st.iterations, res.truncated_weight
+        return energy, iters, res.truncated_weight
 
     def sweep(self, sweep_index: int):
         t0 = time.perf_counter()
@@ -263,6 +281,6 @@ class TwoSiteDMRG:
         for i in range(self.L - 2, -1, -1):
             e, it, tw = self.optimize_pair(i, False)
             self.log.energies.append((sweep_index, i, e, it, tw))
-        self.torch.cuda.synchronize(self.ctx.device)
+        self.be.sync()
         self.log.sweep_seconds.append(time.perf_counter() - t0)
         return self.log.energies[-1][2]

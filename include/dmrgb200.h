@@ -201,6 +201,24 @@ dmrgb200_status dmrgb200_plan_scratch_bytes(dmrgb200_plan_t plan, uint64_t* byte
 dmrgb200_status dmrgb200_hpsi(dmrgb200_plan_t plan, const double* x, double* y, dmrgb200_precision prec,
                               void* cuda_stream);
 
+/* Adjoint of H·psi (no counterpart in the reference, which has no derivative
+ * code).  With the plan's terms y = sum_k alpha_k H_k x, one call gives
+ *   gx          = H^T w                      (the plan's in layout; may be NULL)
+ *   galpha[k]   = <w | H_k x>  = d<w|H x>/d alpha_k, k in plan term order
+ *                                            (device, n_terms doubles; may be NULL)
+ * in native FP64: T = x-slices * R (create_T), G = L^T w per cohort (the
+ * transpose of contract), galpha[k] = <G cell, T cell> (the transpose of
+ * create_s_r), gT = sum_k alpha_k G cells, gx = gT * R^T (the transpose of
+ * create_T).  w uses the out layout and x the in layout.  gx is overwritten over
+ * its whole padded range (uncovered columns and padding become zero).  For a
+ * Hermitian effective Hamiltonian (a Hermitian MPO with boundaries of one MPS)
+ * H^T w = H w, and d<psi|H|psi>/d psi = 2 H psi.  Derivatives with respect to
+ * the MPO term scales follow from galpha and dmrgb200_schedule_term_sources.
+ * Bitwise reproducible; returns DMRGB200_INVALID_PLAN for plans whose T-task
+ * slices of one input block overlap (no such plan comes from the builders). */
+dmrgb200_status dmrgb200_hpsi_adjoint(dmrgb200_plan_t plan, const double* w, const double* x, double* gx,
+                                      double* galpha, void* cuda_stream);
+
 /* Digit planes per operand (2..8, default 7) used by DMRGB200_PREC_FP64_EMULATED:
  * the relative error of each emulated contraction is about 2^(-7 slices) of
  * its row / column maxima (7: below 1e-13, 6: about 1e-11, 5: about 1e-9). */
@@ -379,6 +397,15 @@ dmrgb200_status dmrgb200_schedule_right_step(const dmrgb200_index_desc* phys, co
 /* Flat description of a schedule (arrays owned by the schedule). */
 dmrgb200_status dmrgb200_schedule_export(dmrgb200_schedule_t s, dmrgb200_plan_desc* desc);
 dmrgb200_status dmrgb200_schedule_flops(dmrgb200_schedule_t s, uint64_t* flops);
+/* Provenance of the exported terms of an H·psi schedule, in plan term order:
+ * term_src[k] = index of the MPO term (in the dmrgb200_mpo_desc order) that
+ * produced term k and term_dscale[k] = d alpha_k / d term_scale[term_src[k]]
+ * (alpha is linear in each term scale: it is coefficient * SU2 coupling *
+ * boundary conjugate scales * term scale, op_iterate.hpp:37-69,
+ * site_hamil_tasks.hpp:120-125).  So d<w|H x>/d term_scale[j] =
+ * sum over k with term_src[k] = j of term_dscale[k] * galpha[k].  Arrays hold
+ * n_terms entries; either may be NULL. */
+dmrgb200_status dmrgb200_schedule_term_sources(dmrgb200_schedule_t s, uint32_t* term_src, double* term_dscale);
 dmrgb200_status dmrgb200_schedule_destroy(dmrgb200_schedule_t s);
 
 /* Block layout of an MPS tensor: right-paired (left_paired = 0: one block per

@@ -1,0 +1,267 @@
+// Adjoint of the H psi plan in native FP64.
+//
+// The forward product is y = sum_c L_c S_c with S_c cells = sum_k alpha_k T
+// cells and T_t = x-slice * R_t (create_T, create_s_r, contract;
+// solver/tasks.cpp:650-705, 466-494, 286-313).  Its transpose runs the stages
+// backwards on the same scratch buffers:
+//   G_c  = L_c^T w                 grouped GEMM, into the S scratch
+//   galpha[k] = <G cell(k), T cell(k)>   (T from the forward stage 1 on x)
+//   gT cell   = sum_k alpha_k G cell(k)  into the T scratch (after galpha)
+//   gx slice  = sum over the slice's T tasks of gT_t R_t^T   grouped GEMM
+// Every output (G cell, galpha entry, gT block, gx tile) has exactly one
+// writer, so the result is bitwise reproducible without atomics.
+#include <algorithm>
+#include <map>
+#include <tuple>
+
+#include "device.hpp"
+
+namespace dmrgb200 {
+
+namespace {
+
+// galpha: one warp per term, fixed-order lane sums and a butterfly reduction
+__global__ void __launch_bounds__(256) alpha_grad(const DevATerm* __restrict__ at, uint32_t n,
+                                                  const double* __restrict__ G, const double* __restrict__ T,
+                                                  double* __restrict__ galpha) {
+    const uint32_t lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+    for (uint32_t i = blockIdx.x * warps + (threadIdx.x >> 5); i < n; i += gridDim.x * warps) {
+        const DevATerm a = at[i];
+        const uint64_t cnt = uint64_t(a.rows) * a.cols;
+        double s = 0.0;
+        for (uint64_t idx = lane; idx < cnt; idx += 32) {
+            uint32_t r = uint32_t(idx % a.rows), c = uint32_t(idx / a.rows);
+            s = fma(G[a.g_base + r + uint64_t(c) * a.ld_g], T[a.t_base + r + uint64_t(c) * a.ld_t], s);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) galpha[a.k] = s;
+    }
+}
+
+// gT: one block per T block; every element is the alpha-weighted sum of its
+// G sources in plan term order (a block without sources becomes zero)
+__global__ void __launch_bounds__(256) tgrad_cells(const DevSLine* __restrict__ lines,
+                                                   const DevGTerm* __restrict__ terms, uint32_t n_lines,
+                                                   double* __restrict__ gT, const double* __restrict__ G) {
+    for (uint32_t li = blockIdx.x; li < n_lines; li += gridDim.x) {
+        const DevSLine L = lines[li];
+        const uint64_t n = uint64_t(L.rows) * L.cols;
+        for (uint64_t idx = threadIdx.x; idx < n; idx += blockDim.x) {
+            uint32_t i = uint32_t(idx % L.rows), c = uint32_t(idx / L.rows);
+            double v = 0.0;
+            for (uint32_t t = L.term_begin; t < L.term_end; ++t) {
+                const DevGTerm tm = terms[t];
+                v += tm.alpha * G[tm.g_base + i + uint64_t(c) * tm.ld];
+            }
+            gT[L.s_base + i + uint64_t(c) * L.ld_s] = v;
+        }
+    }
+}
+
+template <class T>
+cudaError_t up(std::vector<T> const& v, T** d) {
+    *d = nullptr;
+    if (v.empty()) return cudaSuccess;
+    cudaError_t e = cudaMalloc(d, v.size() * sizeof(T));
+    if (e != cudaSuccess) return e;
+    return cudaMemcpy(*d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+}  // namespace
+
+std::string compile_adjoint(FlatPlan const& p, std::vector<uint64_t> const& stage3_bnd,
+                            std::vector<uint64_t> const& stage1_bnd, AdjointProgram& a) {
+    a = AdjointProgram();
+    if (p.kind != KIND_HPSI) return "the adjoint exists for H psi plans only";
+    const uint32_t nt = p.n_t(), nc = p.n_cohorts();
+    std::vector<uint64_t> t_off = t_offsets(p, nullptr);
+    std::vector<uint64_t> s_off = s_offsets(p, nullptr);
+
+    // ---- G = L^T w per cohort (transpose of the stage-3 contraction) ----
+    for (uint32_t c = 0; c < nc; ++c) {
+        const uint32_t ls = p.c_ls[c], rs = p.c_rs[c], ns = p.c_nsrows[c], ob = p.c_rb[c];
+        if (p.c_stripe[c] != p.out_cols[ob] || rs != p.out_rows[ob]) return "cohort shape differs from its output block";
+        const uint64_t lbase = stage3_bnd.at(p.c_ci[c]) / 8;
+        DevProb pr;
+        DevSeg sg{};
+        sg.B = dev_op(BUF_W, p.out_off[ob], rs, false);
+        sg.K = rs;
+        pr.N = p.c_stripe[c];
+        uint32_t nbatch = 1;
+        if (!p.c_trans[c]) {
+            // L_c is rs x (ns*ls) with leading dimension rs: read it transposed
+            pr.M = ns * ls;
+            sg.A = dev_op(BUF_ABS, lbase, rs, true);
+            pr.C = dev_op(BUF_S, s_off[c], ns * ls, false);
+        } else {
+            // stored blocks are ls x rs (used transposed forward): G row block b = block_b * w
+            pr.M = ls;
+            sg.A = dev_op(BUF_ABS, lbase, ls, false, uint64_t(ls) * rs);
+            pr.C = dev_op(BUF_S, s_off[c], ns * ls, false, ls);
+            nbatch = ns;
+        }
+        pr.seg_begin = uint32_t(a.g3.segs.size());
+        a.g3.segs.push_back(sg);
+        pr.seg_end = uint32_t(a.g3.segs.size());
+        a.g3.probs.push_back(pr);
+        gemm_add_tiles(a.g3, uint32_t(a.g3.probs.size() - 1), nbatch);
+    }
+    gemm_sort_tiles(a.g3);
+
+    // ---- term cells: galpha sources and gT sources ----
+    // every term must read one whole T block: ms = T block width, column on a block boundary
+    std::vector<std::vector<uint32_t>> block_terms;  // per (t, b), flattened below
+    std::vector<uint64_t> tb_base(nt + 1, 0);
+    for (uint32_t t = 0; t < nt; ++t) tb_base[t + 1] = tb_base[t] + p.t_nb[t];
+    block_terms.resize(tb_base[nt]);
+    a.aterms.reserve(p.n_terms());
+    for (uint32_t c = 0; c < nc; ++c) {
+        const uint32_t ls = p.c_ls[c], ns = p.c_nsrows[c];
+        for (uint32_t u = p.c_unit[c]; u < p.c_unit[c + 1]; ++u)
+            for (uint32_t l = p.u_line[u]; l < p.u_line[u + 1]; ++l)
+                for (uint32_t k = p.l_term[l]; k < p.l_term[l + 1]; ++k) {
+                    const uint32_t t = p.term_t[k], w = p.t_bcols[t];
+                    if (p.in_rows[p.t_lb[t]] != ls) return "term T rows differ from its cohort";
+                    if (p.u_ms[u] != w || (w && p.term_col[k] % w)) return "term does not read one whole T block";
+                    const uint32_t b = w ? p.term_col[k] / w : 0;
+                    if (w && b >= p.t_nb[t]) return "term T block out of range";
+                    DevATerm at{};
+                    at.g_base = s_off[c] + uint64_t(p.l_b1[l]) * ls + uint64_t(p.u_offset[u]) * ns * ls;
+                    at.t_base = t_off[t] + uint64_t(p.term_col[k]) * ls;
+                    at.rows = ls;
+                    at.cols = p.u_ms[u];
+                    at.ld_g = ns * ls;
+                    at.ld_t = ls;
+                    at.k = k;
+                    a.aterms.push_back(at);
+                    if (w) block_terms[tb_base[t] + b].push_back(uint32_t(a.aterms.size() - 1));
+                }
+    }
+    for (uint32_t t = 0; t < nt; ++t) {
+        const uint32_t M = p.in_rows[p.t_lb[t]], N = p.t_bcols[t];
+        for (uint32_t b = 0; b < p.t_nb[t]; ++b) {
+            DevSLine L{};
+            L.s_base = t_off[t] + uint64_t(b) * M * N;
+            L.ld_s = M;
+            L.rows = M;
+            L.cols = N;
+            L.ld_t = M;
+            L.term_begin = uint32_t(a.gterms.size());
+            for (uint32_t i : block_terms[tb_base[t] + b]) {
+                DevATerm const& at = a.aterms[i];
+                a.gterms.push_back(DevGTerm{p.term_alpha[at.k], at.g_base, at.ld_g, 0});
+            }
+            L.term_end = uint32_t(a.gterms.size());
+            if (uint64_t(M) * N) a.tlines.push_back(L);
+        }
+    }
+
+    // ---- gx slices: sum over the slice's T tasks of gT_t R_t^T (transpose of stage 1) ----
+    std::map<std::pair<uint32_t, uint32_t>, std::vector<uint32_t>> slices;  // (block, column) -> tasks
+    for (uint32_t t = 0; t < nt; ++t) slices[{p.t_lb[t], p.t_col[t]}].push_back(t);
+    uint32_t prev_lb = UINT32_MAX;
+    uint64_t prev_end = 0;
+    for (auto const& kv : slices) {
+        const uint32_t lb = kv.first.first, col = kv.first.second;
+        const uint32_t M = p.in_rows[lb], W = p.t_brows[kv.second.front()];
+        for (uint32_t t : kv.second)
+            if (p.t_brows[t] != W) return "T tasks of one slice differ in width";
+        if (lb == prev_lb && col < prev_end) return "T-task slices of an input block overlap";
+        prev_lb = lb;
+        prev_end = uint64_t(col) + W;
+        DevProb pr;
+        pr.M = M;
+        pr.N = W;
+        pr.C = dev_op(BUF_OUT, p.in_off[lb] + uint64_t(col) * M, M, false);
+        pr.seg_begin = uint32_t(a.g1.segs.size());
+        for (uint32_t t : kv.second) {
+            const uint32_t Nf = p.t_bcols[t], nb = p.t_nb[t];
+            const uint64_t bnd = stage1_bnd.at(p.t_ci[t]) / 8;
+            if (!p.t_trans[t]) {
+                // R_t is W x (nb*Nf) with leading dimension W: read it transposed
+                DevSeg sg{};
+                sg.A = dev_op(BUF_T, t_off[t], M, false);
+                sg.B = dev_op(BUF_ABS, bnd, W, true);
+                sg.K = nb * Nf;
+                a.g1.segs.push_back(sg);
+            } else {
+                // stored blocks are Nf x W (used transposed forward): one segment per block
+                for (uint32_t b = 0; b < nb; ++b) {
+                    DevSeg sg{};
+                    sg.A = dev_op(BUF_T, t_off[t] + uint64_t(b) * M * Nf, M, false);
+                    sg.B = dev_op(BUF_ABS, bnd + uint64_t(b) * W * Nf, Nf, false);
+                    sg.K = Nf;
+                    a.g1.segs.push_back(sg);
+                }
+            }
+        }
+        pr.seg_end = uint32_t(a.g1.segs.size());
+        a.g1.probs.push_back(pr);
+        gemm_add_tiles(a.g1, uint32_t(a.g1.probs.size() - 1), 1);
+    }
+    gemm_sort_tiles(a.g1);
+    return std::string();
+}
+
+cudaError_t upload_adjoint(AdjointProgram& a) {
+    cudaError_t e;
+    if ((e = upload_gemm(a.g3, a.d3)) != cudaSuccess) return e;
+    if ((e = upload_gemm(a.g1, a.d1)) != cudaSuccess) return e;
+    if ((e = up(a.aterms, &a.d_aterms)) != cudaSuccess) return e;
+    if ((e = up(a.tlines, &a.d_tlines)) != cudaSuccess) return e;
+    if ((e = up(a.gterms, &a.d_gterms)) != cudaSuccess) return e;
+    a.n_aterms = uint32_t(a.aterms.size());
+    a.n_tlines = uint32_t(a.tlines.size());
+    return cudaSuccess;
+}
+
+void free_adjoint(AdjointProgram& a) {
+    free_gemm(a.d3);
+    free_gemm(a.d1);
+    cudaFree(a.d_aterms);
+    cudaFree(a.d_tlines);
+    cudaFree(a.d_gterms);
+    a.d_aterms = nullptr;
+    a.d_tlines = nullptr;
+    a.d_gterms = nullptr;
+}
+
+cudaError_t run_adjoint(DeviceProgram const& fwd, AdjointProgram const& a, uint64_t w, uint64_t x, double* gx,
+                        uint64_t gx_elems, double* galpha, double* T, double* S, cudaStream_t stream) {
+    Bases bs{};
+    bs.b[BUF_IN] = x;
+    bs.b[BUF_OUT] = reinterpret_cast<uint64_t>(gx);
+    bs.b[BUF_T] = reinterpret_cast<uint64_t>(T);
+    bs.b[BUF_S] = reinterpret_cast<uint64_t>(S);
+    bs.b[BUF_W] = w;
+    const uint32_t sms = uint32_t(device_sm_count());
+    cudaError_t e;
+    if (!gx && !galpha) return cudaSuccess;
+    if ((e = launch_gemm(a.d3, bs, stream)) != cudaSuccess) return e;  // G into S
+    if (galpha) {
+        GemmDev f1;
+        f1.p = fwd.d_p1;
+        f1.s = fwd.d_s1;
+        f1.t = fwd.d_t1;
+        f1.n = fwd.n_t1;
+        if ((e = launch_gemm(f1, bs, stream)) != cudaSuccess) return e;  // T = x-slices * R
+        if (a.n_aterms) {
+            uint32_t grid = std::min<uint32_t>((a.n_aterms + 7) / 8, sms * 8);
+            alpha_grad<<<grid, 256, 0, stream>>>(a.d_aterms, a.n_aterms, S, T, galpha);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        }
+    }
+    if (gx) {
+        if (a.n_tlines) {
+            uint32_t grid = std::min<uint32_t>(a.n_tlines, sms * 8);
+            tgrad_cells<<<grid, 256, 0, stream>>>(a.d_tlines, a.d_gterms, a.n_tlines, T, S);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        }
+        if ((e = cudaMemsetAsync(gx, 0, gx_elems * sizeof(double), stream)) != cudaSuccess) return e;
+        if ((e = launch_gemm(a.d1, bs, stream)) != cudaSuccess) return e;  // gx = gT * R^T
+    }
+    return cudaSuccess;
+}
+
+}  // namespace dmrgb200

@@ -68,6 +68,10 @@ struct dmrgb200_plan_s {
     OzProgram* oz3 = nullptr;
     void* oz_scratch = nullptr;
     uint64_t oz_scratch_size = 0;
+    // adjoint program (built on first use)
+    bool adj_built = false;
+    std::string adj_err;
+    AdjointProgram adj;
 
     void collect() {
         if (!pending) return;
@@ -431,6 +435,7 @@ dmrgb200_status dmrgb200_plan_create_batched(dmrgb200_context_t ctx, uint32_t n,
 dmrgb200_status dmrgb200_plan_destroy(dmrgb200_plan_t plan) {
     if (!plan) return DMRGB200_OK;
     if (plan->compiled) free_program(plan->prog);
+    if (plan->adj_built) free_adjoint(plan->adj);
     oz_free(plan->oz1);
     oz_free(plan->oz3);
     cudaFree(plan->oz_scratch);
@@ -466,6 +471,31 @@ dmrgb200_status dmrgb200_hpsi(dmrgb200_plan_t plan, const double* x, double* y, 
     if (e != cudaSuccess) return cuda_fail(e, "hpsi launch");
     if (plan->timing) plan->pending = true;
     return DMRGB200_OK;
+}
+
+dmrgb200_status dmrgb200_hpsi_adjoint(dmrgb200_plan_t plan, const double* w, const double* x, double* gx,
+                                      double* galpha, void* cuda_stream) {
+    DMRGB200_TRY
+    if (!plan || !w || (galpha && !x)) return fail(DMRGB200_INVALID_ARGUMENT, "null argument");
+    if (plan->flat.kind != KIND_HPSI) return fail(DMRGB200_INVALID_PLAN, "plan is not an H psi plan");
+    if (!plan->adj_built) {
+        plan->adj_err = compile_adjoint(plan->flat, plan->stage3_bnd, plan->stage1_bnd, plan->adj);
+        if (plan->adj_err.empty()) {
+            cudaError_t e = upload_adjoint(plan->adj);
+            if (e != cudaSuccess) {
+                free_adjoint(plan->adj);
+                return cuda_fail(e, "adjoint program upload");
+            }
+        }
+        plan->adj_built = true;
+    }
+    if (!plan->adj_err.empty()) return fail(DMRGB200_INVALID_PLAN, "no adjoint for this plan: " + plan->adj_err);
+    cudaError_t e = run_adjoint(plan->prog, plan->adj, reinterpret_cast<uint64_t>(w), reinterpret_cast<uint64_t>(x),
+                                gx, plan->flat.in_size, galpha, plan->T, plan->S,
+                                static_cast<cudaStream_t>(cuda_stream));
+    if (e != cudaSuccess) return cuda_fail(e, "adjoint launch");
+    return DMRGB200_OK;
+    DMRGB200_CATCH
 }
 
 dmrgb200_status dmrgb200_plan_set_slices(dmrgb200_plan_t plan, int slices) {
@@ -554,7 +584,7 @@ dmrgb200_status dmrgb200_mpo_create(const dmrgb200_mpo_desc* d, dmrgb200_mpo_t* 
                 return fail(DMRGB200_INVALID_ARGUMENT, "MPO terms must be sorted by (b1, b2)");
             row.push_back(MPOEntry{b2, {}});
         }
-        row.back().terms.push_back(TermRef{d->term_op[i], d->term_scale[i]});
+        row.back().terms.push_back(TermRef{d->term_op[i], d->term_scale[i], i});
     }
     for (uint32_t b1 = 0; b1 < t.row_dim; ++b1)
         for (auto const& e : t.rows[b1]) t.cols[e.other].push_back(MPOEntry{b1, e.terms});
@@ -702,6 +732,16 @@ dmrgb200_status dmrgb200_schedule_export(dmrgb200_schedule_t sc, dmrgb200_plan_d
 dmrgb200_status dmrgb200_schedule_flops(dmrgb200_schedule_t sc, uint64_t* flops) {
     if (!sc || !flops) return fail(DMRGB200_INVALID_ARGUMENT, "null argument");
     *flops = sc->flat.flops();
+    return DMRGB200_OK;
+}
+
+dmrgb200_status dmrgb200_schedule_term_sources(dmrgb200_schedule_t sc, uint32_t* term_src, double* term_dscale) {
+    if (!sc) return fail(DMRGB200_INVALID_ARGUMENT, "null schedule");
+    FlatPlan const& f = sc->flat;
+    if (f.kind != KIND_HPSI || f.term_src.size() != f.n_terms())
+        return fail(DMRGB200_NOT_SUPPORTED, "term provenance is recorded for H psi schedules only");
+    if (term_src) std::copy(f.term_src.begin(), f.term_src.end(), term_src);
+    if (term_dscale) std::copy(f.term_dscale.begin(), f.term_dscale.end(), term_dscale);
     return DMRGB200_OK;
 }
 

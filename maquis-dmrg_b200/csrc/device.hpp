@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <string>
 #include <vector>
 
 #include "plan.hpp"
@@ -49,7 +50,7 @@ struct DevSTerm {
     uint64_t t_base;
 };
 
-enum BufId : uint16_t { BUF_IN = 0, BUF_OUT = 1, BUF_T = 2, BUF_S = 3, BUF_ABS = 4, NBUF = 8 };
+enum BufId : uint16_t { BUF_IN = 0, BUF_OUT = 1, BUF_T = 2, BUF_S = 3, BUF_ABS = 4, BUF_W = 5, NBUF = 8 };
 
 struct Bases {
     uint64_t b[NBUF];
@@ -64,6 +65,7 @@ __device__ __forceinline__ uint64_t base_of(Bases const& bs, uint32_t buf) {
     b = buf == 2 ? bs.b[2] : b;
     b = buf == 3 ? bs.b[3] : b;
     b = buf == 4 ? bs.b[4] : b;
+    b = buf == 5 ? bs.b[5] : b;
     return b;
 }
 #endif
@@ -112,6 +114,60 @@ cudaError_t run_program(DeviceProgram const& prog, uint64_t in, uint64_t out, do
                         cudaStream_t stream, cudaEvent_t const* ev = nullptr);
 
 int device_sm_count();
+
+// ---- lowering helpers shared by the forward and adjoint programs ----
+DevOp dev_op(uint16_t buf, uint64_t off, uint32_t ld, bool trans, uint64_t bstride = 0);
+void gemm_add_tiles(GemmList& gl, uint32_t prob, uint32_t nbatch);
+void gemm_sort_tiles(GemmList& gl);
+// element offsets of the plan's T matrices / S matrices in the scratch buffers
+std::vector<uint64_t> t_offsets(FlatPlan const& p, uint64_t* total);
+std::vector<uint64_t> s_offsets(FlatPlan const& p, uint64_t* total);
+
+struct GemmDev {
+    DevProb* p = nullptr;
+    DevSeg* s = nullptr;
+    DevTile* t = nullptr;
+    uint32_t n = 0;
+};
+cudaError_t upload_gemm(GemmList const& gl, GemmDev& d);
+void free_gemm(GemmDev& d);
+// one persistent grouped-GEMM launch over the tile list
+cudaError_t launch_gemm(GemmDev const& d, Bases const& bs, cudaStream_t stream);
+
+// ---- adjoint of H psi (adjoint.cu) ----
+// galpha term: <G cell, T cell> for plan term k
+struct DevATerm {
+    uint64_t g_base, t_base;
+    uint32_t rows, cols, ld_g, ld_t;
+    uint32_t k, pad;
+};
+// gT source: alpha * G cell at g_base with leading dimension ld
+struct DevGTerm {
+    double alpha;
+    uint64_t g_base;
+    uint32_t ld, pad;
+};
+struct AdjointProgram {
+    GemmList g3;                    // G = L^T w per cohort (into the S scratch)
+    GemmList g1;                    // gx slice = sum over its T tasks of gT * R^T
+    std::vector<DevATerm> aterms;   // one per plan term
+    std::vector<DevSLine> tlines;   // one per T block: gT cell = sum of its sources
+    std::vector<DevGTerm> gterms;
+    GemmDev d3, d1;
+    DevATerm* d_aterms = nullptr;
+    DevSLine* d_tlines = nullptr;
+    DevGTerm* d_gterms = nullptr;
+    uint32_t n_aterms = 0, n_tlines = 0;
+};
+// Lower the adjoint of an H psi plan; returns an empty string, or why the plan
+// has none (overlapping T slices, a term that is not one whole T block).
+std::string compile_adjoint(FlatPlan const& p, std::vector<uint64_t> const& stage3_bnd,
+                            std::vector<uint64_t> const& stage1_bnd, AdjointProgram& a);
+cudaError_t upload_adjoint(AdjointProgram& a);
+void free_adjoint(AdjointProgram& a);
+// gx = H^T w (NULL: skipped), galpha[k] = <w|H_k x> (NULL: skipped)
+cudaError_t run_adjoint(DeviceProgram const& fwd, AdjointProgram const& a, uint64_t w, uint64_t x, double* gx,
+                        uint64_t gx_elems, double* galpha, double* T, double* S, cudaStream_t stream);
 // stage 2 only (S build), for the emulated path
 cudaError_t run_sbuild(DeviceProgram const& prog, double* T, double* S, cudaStream_t stream);
 // largest K of any output matrix of a GEMM list (emulation needs K * slices <= 2^17)

@@ -242,18 +242,40 @@ DevOp op(uint16_t buf, uint64_t off, uint32_t ld, bool trans, uint64_t bstride =
 
 }  // namespace
 
+DevOp dev_op(uint16_t buf, uint64_t off, uint32_t ld, bool trans, uint64_t bstride) {
+    return op(buf, off, ld, trans, bstride);
+}
+void gemm_add_tiles(GemmList& gl, uint32_t prob, uint32_t nbatch) { add_tiles(gl, prob, nbatch); }
+void gemm_sort_tiles(GemmList& gl) { sort_tiles(gl); }
+
+std::vector<uint64_t> t_offsets(FlatPlan const& p, uint64_t* total) {
+    std::vector<uint64_t> off(p.n_t());
+    uint64_t sum = 0;
+    for (uint32_t t = 0; t < p.n_t(); ++t) {
+        off[t] = sum;
+        sum += round_up(p.t_size(t), 32);
+    }
+    if (total) *total = sum;
+    return off;
+}
+
+std::vector<uint64_t> s_offsets(FlatPlan const& p, uint64_t* total) {
+    std::vector<uint64_t> off(p.n_cohorts());
+    uint64_t sum = 0;
+    for (uint32_t c = 0; c < p.n_cohorts(); ++c) {
+        off[c] = sum;
+        sum += round_up(uint64_t(p.c_nsrows[c]) * p.c_stripe[c] * (p.kind == KIND_LEFT ? p.c_rs[c] : p.c_ls[c]), 32);
+    }
+    if (total) *total = sum;
+    return off;
+}
+
 void compile_program(FlatPlan const& p, std::vector<uint64_t> const& stage3_bnd,
                      std::vector<uint64_t> const& stage1_bnd, std::vector<uint64_t> const& outptr,
                      DeviceProgram& prog) {
     prog = DeviceProgram();
     const uint32_t nt = p.n_t(), nc = p.n_cohorts();
-    std::vector<uint64_t> t_off(nt);
-    uint64_t tsum = 0;
-    for (uint32_t t = 0; t < nt; ++t) {
-        t_off[t] = tsum;
-        tsum += round_up(p.t_size(t), 32);
-    }
-    prog.t_elems = tsum;
+    std::vector<uint64_t> t_off = t_offsets(p, &prog.t_elems);
 
     // ---- stage 1 ----
     GemmList& g1 = prog.stage1;
@@ -297,13 +319,7 @@ void compile_program(FlatPlan const& p, std::vector<uint64_t> const& stage3_bnd,
     sort_tiles(g1);
 
     // ---- stage 2 (S lines) ----
-    std::vector<uint64_t> s_off(nc);
-    uint64_t ssum = 0;
-    for (uint32_t c = 0; c < nc; ++c) {
-        s_off[c] = ssum;
-        ssum += round_up(uint64_t(p.c_nsrows[c]) * p.c_stripe[c] * (p.kind == KIND_LEFT ? p.c_rs[c] : p.c_ls[c]), 32);
-    }
-    prog.s_elems = ssum;
+    std::vector<uint64_t> s_off = s_offsets(p, &prog.s_elems);
     // units tile the S columns (rows for the left step) and b1 its row blocks, so
     // the cells (unit, b1) cover S exactly once
     for (uint32_t c = 0; c < nc; ++c) {
@@ -484,6 +500,41 @@ double calibrate_fp64_tflops() {
     return ms > 0 ? flops / (ms * 1e-3) / 1e12 : 0.0;
 }
 
+cudaError_t upload_gemm(GemmList const& gl, GemmDev& d) {
+    cudaError_t e;
+    if ((e = up(gl.probs, &d.p)) != cudaSuccess) return e;
+    if ((e = up(gl.segs, &d.s)) != cudaSuccess) return e;
+    if ((e = up(gl.tiles, &d.t)) != cudaSuccess) return e;
+    d.n = uint32_t(gl.tiles.size());
+    return cudaSuccess;
+}
+
+void free_gemm(GemmDev& d) {
+    cudaFree(d.p);
+    cudaFree(d.s);
+    cudaFree(d.t);
+    d = GemmDev();
+}
+
+namespace {
+int gemm_occupancy() {
+    static int occ = 0;
+    if (!occ) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, gemm_f64_grouped, NTHREADS, 0);
+        if (occ <= 0) occ = 1;
+    }
+    return occ;
+}
+}  // namespace
+
+cudaError_t launch_gemm(GemmDev const& d, Bases const& bs, cudaStream_t stream) {
+    if (d.n) {
+        uint32_t grid = std::min<uint32_t>(d.n, uint32_t(device_sm_count()) * gemm_occupancy());
+        gemm_f64_grouped<<<grid, NTHREADS, 0, stream>>>(d.p, d.s, d.t, d.n, bs);
+    }
+    return cudaGetLastError();
+}
+
 cudaError_t run_sbuild(DeviceProgram const& prog, double* T, double* S, cudaStream_t stream) {
     if (prog.n_lines) {
         uint32_t grid = std::min<uint32_t>(prog.n_lines, uint32_t(device_sm_count()) * 8);
@@ -519,11 +570,7 @@ cudaError_t run_program(DeviceProgram const& prog, uint64_t in, uint64_t out, do
     bs.b[BUF_ABS] = 0;
     const int sms = device_sm_count();
     if (ev) cudaEventRecord(ev[0], stream);
-    static int occ = 0;
-    if (!occ) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, gemm_f64_grouped, NTHREADS, 0);
-        if (occ <= 0) occ = 1;
-    }
+    const int occ = gemm_occupancy();
     if (prog.n_t1) {
         uint32_t grid = std::min<uint32_t>(prog.n_t1, uint32_t(sms) * occ);
         gemm_f64_grouped<<<grid, NTHREADS, 0, stream>>>(prog.d_p1, prog.d_s1, prog.d_t1, prog.n_t1, bs);

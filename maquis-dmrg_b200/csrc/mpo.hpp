@@ -56,6 +56,7 @@ private:
 struct TermRef {
     unsigned op;
     double scale;
+    unsigned id = 0;  // position of the term in the MPO description (term provenance of the schedule)
 };
 
 struct MPOEntry {

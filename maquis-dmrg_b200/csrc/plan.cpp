@@ -70,6 +70,8 @@ std::string FlatPlan::validate() const {
     if (u_line.size() != u_offset.size() + 1 || u_ms.size() != u_offset.size()) return "unit arrays differ in length";
     if (l_term.size() != l_b1.size() + 1) return "line arrays differ in length";
     if (term_t.size() != term_alpha.size() || term_col.size() != term_alpha.size()) return "term arrays differ";
+    if ((!term_src.empty() && term_src.size() != term_alpha.size()) || term_src.size() != term_dscale.size())
+        return "term provenance arrays differ";
     if (!c_unit.empty() && c_unit.back() != u_offset.size()) return "cohort unit ranges do not cover the units";
     if (!u_line.empty() && u_line.back() != l_b1.size()) return "unit line ranges do not cover the lines";
     if (!l_term.empty() && l_term.back() != term_alpha.size()) return "line term ranges do not cover the terms";
@@ -276,6 +278,8 @@ void append_groups(FlatPlan& p, Schedule const& s, TaskDims tdims, CohortExtra c
                         p.term_alpha.push_back(u.alpha[ia]);
                         p.term_t.push_back(tbase + u.tidx[2 * ia]);
                         p.term_col.push_back(u.tidx[2 * ia + 1]);
+                        p.term_src.push_back(u.src[ia]);
+                        p.term_dscale.push_back(u.dscale[ia]);
                     }
                     seek += u.b2s[l];
                     p.l_term.push_back(uint32_t(p.term_alpha.size()));

@@ -34,6 +34,10 @@ struct FlatPlan {
     std::vector<uint32_t> l_b1, l_term;
     std::vector<double> term_alpha;
     std::vector<uint32_t> term_t, term_col;
+    // builder provenance (empty for plans from a caller's description): MPO term
+    // of each plan term and d alpha / d (that term's scale); H psi plans only
+    std::vector<uint32_t> term_src;
+    std::vector<double> term_dscale;
 
     uint32_t n_groups() const { return g_t.empty() ? 0 : uint32_t(g_t.size() - 1); }
     uint32_t n_t() const { return uint32_t(t_lb.size()); }

@@ -52,9 +52,13 @@ namespace {
 
 std::vector<unsigned> phys_sizes_of(Index const& phys) { return phys.sz; }
 
-// Expand one operator block into cohort pushes (op_iterate.hpp:37-69)
-void op_iterate(OpBlock const& blk, double const couplings[4], Cohort& cg, unsigned s, unsigned m2_size,
-                MPSBlock const& mpsb, unsigned mps_offset, unsigned ci, unsigned boundary_col) {
+// Expand one operator block into cohort pushes (op_iterate.hpp:37-69).  `from`
+// is the MPO term the block belongs to; dcouplings (may be NULL) are the
+// couplings with the term's scale set to one, so that e.coeff * dcouplings[c]
+// is the derivative of the pushed alpha with respect to that scale.
+void op_iterate(OpBlock const& blk, double const couplings[4], double const* dcouplings, unsigned from, Cohort& cg,
+                unsigned s, unsigned m2_size, MPSBlock const& mpsb, unsigned mps_offset, unsigned ci,
+                unsigned boundary_col) {
     for (auto const& e : blk.entries) {
         unsigned casenr = 0;
         if (e.row_spin == 2 && e.col_spin == 2)
@@ -64,18 +68,21 @@ void op_iterate(OpBlock const& blk, double const couplings[4], Cohort& cg, unsig
         else if (e.col_spin == 2)
             casenr = 2;
         double scale = e.coeff * couplings[casenr];
+        double dsc = dcouplings ? e.coeff * dcouplings[casenr] : 0.0;
         unsigned ti = mpsb.get_ti(mps_offset + e.row * m2_size, ci);
-        if (ti != 0xFFFFFFFFu) cg.push_back(s, e.col, scale, ti, boundary_col);
+        if (ti != 0xFFFFFFFFu) cg.push_back(s, e.col, scale, ti, boundary_col, from, dsc);
     }
 }
 
 // Couplings of the H psi / right-step builders.  The reference reads them from
 // a per-(J, I, I') table indexed by a hash of (A, K, A') and multiplies by the
 // scale afterwards (gsl_coupling.h:145-223); the same table slot is used here.
+// `unit` (may be NULL) receives the couplings for scale one.
 void w9j_couplings(Symm symm, Charge lc, Charge mc, Charge rc, int A, int K, int Ap, Charge jp, double scale,
-                   double out[4]) {
+                   double out[4], double* unit = nullptr) {
     if (!has_su2(symm)) {
         out[0] = out[1] = out[2] = out[3] = scale;
+        if (unit) unit[0] = unit[1] = unit[2] = unit[3] = 1.0;
         return;
     }
     int J = spin_of(mc), I = spin_of(lc), Ip = spin_of(rc), Jp = spin_of(jp);
@@ -88,6 +95,8 @@ void w9j_couplings(Symm symm, Charge lc, Charge mc, Charge rc, int A, int K, int
     double base[4];
     set_coupling(J, std::abs(J - Jp), Jp, A, Ktab[slot], Aptab[slot], I, std::abs(I - Ip), Ip, 1.0, base);
     for (int c = 0; c < 4; ++c) out[c] = base[c] * scale;
+    if (unit)
+        for (int c = 0; c < 4; ++c) unit[c] = base[c];
 }
 
 void lshtm_couplings(Symm symm, Charge lc_ket, Charge rc_ket, int A, int K, int Ap, Charge lc_bra, Charge rc_bra,
@@ -171,10 +180,12 @@ void shtm_tasks(Symm symm, MPOTensor const& mpo, BoundaryIndex const& left, Boun
                             unsigned in_offset = static_cast<unsigned>(right_pb(phys_in, rc_in));
                             long right_offset = right.offset(ci_right, b2);
 
-                            double couplings[4];
+                            double couplings[4], unit[4], dcouplings[4];
+                            double cscale = right.conjugate_scale(ci_right, b2) * left.conjugate_scale(ci, b1);
                             double scale = right.conjugate_scale(ci_right, b2) * tr.scale * left.conjugate_scale(ci, b1);
-                            w9j_couplings(symm, lc_out, lc_in, rc_out, A, K, Ap, rc_in, scale, couplings);
-                            op_iterate(blk, couplings, cohort, s, rs_in, mpsb, in_offset, ci_right,
+                            w9j_couplings(symm, lc_out, lc_in, rc_out, A, K, Ap, rc_in, scale, couplings, unit);
+                            for (int c = 0; c < 4; ++c) dcouplings[c] = unit[c] * cscale;
+                            op_iterate(blk, couplings, dcouplings, tr.id, cohort, s, rs_in, mpsb, in_offset, ci_right,
                                        static_cast<unsigned>(right_offset / rs_in));
                         }
                     }
@@ -237,7 +248,7 @@ void rshtm_tasks(Symm symm, MPOTensor const& mpo, BoundaryIndex const& right, In
                             double couplings[4];
                             double scale = right.conjugate_scale(ci, b2) * tr.scale;
                             w9j_couplings(symm, lc_bra, lc_ket, rc_bra, A, K, Ap, rc_ket, scale, couplings);
-                            op_iterate(blk, couplings, cohort, s, rs_ket, mpsb, ket_offset, ci,
+                            op_iterate(blk, couplings, nullptr, tr.id, cohort, s, rs_ket, mpsb, ket_offset, ci,
                                        static_cast<unsigned>(right_offset / rs_ket));
                         }
                     }
@@ -323,7 +334,7 @@ void lshtm_tasks(Symm symm, MPOTensor const& mpo, Index const& phys_i, Index con
                             double couplings[4];
                             double scale = left.conjugate_scale(ci, b1) * tr.scale;
                             lshtm_couplings(symm, lc_ket, rc_ket, A, K, Ap, lc_bra, rc_bra, scale, couplings);
-                            op_iterate(blk, couplings, cohort, s, rs_ket, mpsb, ket_offset, ci,
+                            op_iterate(blk, couplings, nullptr, tr.id, cohort, s, rs_ket, mpsb, ket_offset, ci,
                                        static_cast<unsigned>(left_offset / ls_ket));
                         }
                     }

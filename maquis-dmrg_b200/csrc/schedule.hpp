@@ -32,10 +32,15 @@ struct SUnit {
     std::vector<double> alpha;
     std::vector<unsigned> b2s;   // terms per line
     std::vector<unsigned> b1;    // S row-block of each line
+    // provenance of each term: the MPO term it comes from and d alpha / d (MPO term scale)
+    std::vector<unsigned> src;
+    std::vector<double> dscale;
     unsigned b2count = 0;
 
-    void push_back(double scale, unsigned ti, unsigned col) {
+    void push_back(double scale, unsigned ti, unsigned col, unsigned from, double dsc) {
         alpha.push_back(scale);
+        src.push_back(from);
+        dscale.push_back(dsc);
         ++b2count;
         tidx.push_back(ti);
         tidx.push_back(col);
@@ -58,8 +63,8 @@ public:
     Cohort(std::vector<unsigned> const& phys_sizes, unsigned lb, unsigned rb, unsigned ls, unsigned rs, unsigned ci,
            unsigned ci_eff, unsigned mpodim, bool left = false);
 
-    void push_back(unsigned s, unsigned ss2, double scale, unsigned ti, unsigned col) {
-        suv_[sfold_[s] + ss2].push_back(scale, ti, col);
+    void push_back(unsigned s, unsigned ss2, double scale, unsigned ti, unsigned col, unsigned from, double dsc) {
+        suv_[sfold_[s] + ss2].push_back(scale, ti, col, from, dsc);
     }
     void add_line(unsigned b1) {
         for (auto& u : suv_) mpo_offsets_[b1] += u.add_line(b1);

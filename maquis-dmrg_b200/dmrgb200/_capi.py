@@ -109,6 +109,7 @@ _sigs = {
     "dmrgb200_plan_flops": ([vp, u64p], C.c_int),
     "dmrgb200_plan_scratch_bytes": ([vp, u64p], C.c_int),
     "dmrgb200_hpsi": ([vp, vp, vp, C.c_int, vp], C.c_int),
+    "dmrgb200_hpsi_adjoint": ([vp, vp, vp, vp, vp, vp], C.c_int),
     "dmrgb200_plan_set_timing": ([vp, C.c_int], C.c_int),
     "dmrgb200_plan_set_slices": ([vp, C.c_int], C.c_int),
     "dmrgb200_plan_stage_times": ([vp, f64p, u64p, u64p], C.c_int),
@@ -133,6 +134,7 @@ _sigs = {
                                       C.c_int, C.POINTER(vp), C.POINTER(vp)], C.c_int),
     "dmrgb200_schedule_export": ([vp, C.POINTER(PlanDesc)], C.c_int),
     "dmrgb200_schedule_flops": ([vp, u64p], C.c_int),
+    "dmrgb200_schedule_term_sources": ([vp, u32p, f64p], C.c_int),
     "dmrgb200_schedule_destroy": ([vp], C.c_int),
     "dmrgb200_tensor_layout": ([C.POINTER(IndexDesc), C.POINTER(IndexDesc), C.POINTER(IndexDesc), C.c_int, u32p,
                                 u32p, u32p, u64p, u64p], C.c_int),

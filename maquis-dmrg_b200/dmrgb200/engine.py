@@ -105,6 +105,24 @@ class Schedule:
         capi.check(capi.lib.dmrgb200_schedule_flops(handle, C.byref(f)), "schedule_flops")
         self.flops = f.value
 
+    def term_sources(self):
+        """(src, dscale) per plan term: the MPO term it comes from and d alpha / d scale
+        (dmrgb200_schedule_term_sources; H·psi schedules only)."""
+        n = len(self.plan["term_alpha"])
+        src = np.zeros(max(n, 1), dtype=np.uint32)
+        dsc = np.zeros(max(n, 1), dtype=np.float64)
+        capi.check(capi.lib.dmrgb200_schedule_term_sources(
+            self.handle, src.ctypes.data_as(C.POINTER(C.c_uint32)), dsc.ctypes.data_as(C.POINTER(C.c_double))),
+            "schedule_term_sources")
+        return src[:n], dsc[:n]
+
+    def mpo_term_grad(self, galpha: np.ndarray, n_mpo_terms: int) -> np.ndarray:
+        """d<w|H x>/d (MPO term scale) from the per-term derivatives galpha."""
+        src, dsc = self.term_sources()
+        g = np.zeros(n_mpo_terms)
+        np.add.at(g, src, dsc * np.asarray(galpha, dtype=np.float64))
+        return g
+
     def __del__(self):
         if getattr(self, "handle", None):
             capi.lib.dmrgb200_schedule_destroy(self.handle)
@@ -182,6 +200,11 @@ class DevicePlan:
 
     def hpsi(self, x_ptr: int, y_ptr: int, prec: int = capi.PREC_FP64, stream: int = 0) -> None:
         capi.check(capi.lib.dmrgb200_hpsi(self.handle, x_ptr, y_ptr, prec, stream or None), "dmrgb200_hpsi")
+
+    def adjoint(self, w_ptr: int, x_ptr: int, gx_ptr: int, galpha_ptr: int, stream: int = 0) -> None:
+        """gx = H^T w and galpha[k] = <w|H_k x> (dmrgb200_hpsi_adjoint; 0 skips an output)."""
+        capi.check(capi.lib.dmrgb200_hpsi_adjoint(self.handle, w_ptr, x_ptr or None, gx_ptr or None,
+                                                  galpha_ptr or None, stream or None), "dmrgb200_hpsi_adjoint")
 
     def solve(self, x0_ptr: int, x_out_ptr: int, n: int, ortho_ptrs=(), tol: float = 1e-8, max_iter: int = 8,
               stream: int = 0):

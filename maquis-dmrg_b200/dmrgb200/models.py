@@ -43,6 +43,7 @@ class MPOTensor:
     right_phase: list = None
     left_spin: list = None
     right_spin: list = None
+    sources: dict = None     # (b1, b2) -> per-term provenance (twosite_mpo(merge=False))
 
 
 @dataclass
@@ -246,16 +247,32 @@ def kron_op(A: SiteOp, B: SiteOp, p1, p2) -> SiteOp:
     return SiteOp(blocks=blocks, name=f"({A.name}x{B.name})")
 
 
-def twosite_mpo(W1: MPOTensor, W2: MPOTensor, p1, p2) -> MPOTensor:
+def twosite_mpo(W1: MPOTensor, W2: MPOTensor, p1, p2, merge: bool = True) -> MPOTensor:
     """W12(b1, b3) = sum_b2 W1(b1, b2) x W2(b2, b3) (make_twosite_mpo, ts_ops.hpp:96-158):
     a single summand keeps its kron'd operator with the product of scales, several
-    summands are added into one operator with scale 1."""
+    summands are added into one operator with scale 1.
+
+    merge=False keeps every summand as its own (operator, s1 * s2) term -- the same
+    operator sum -- and records in `sources[(b1, b3)]` the pair of site terms
+    ((b1, b2, j1), (b2, b3, j2)) of each, so that derivatives with respect to the
+    two-site term scales map back to the site MPO coefficients."""
     assert W1.col_dim == W2.row_dim
     terms = {}
+    sources = {}
     for b1 in range(W1.row_dim):
         for b3 in range(W2.col_dim):
             summands = [b2 for b2 in range(W1.col_dim) if (b1, b2) in W1.terms and (b2, b3) in W2.terms]
             if not summands:
+                continue
+            if not merge:
+                lst, src = [], []
+                for b2 in summands:
+                    for j1, (o1, s1) in enumerate(W1.terms[(b1, b2)]):
+                        for j2, (o2, s2) in enumerate(W2.terms[(b2, b3)]):
+                            lst.append((kron_op(o1, o2, p1, p2), s1 * s2))
+                            src.append(((b1, b2, j1), (b2, b3, j2)))
+                terms[(b1, b3)] = lst
+                sources[(b1, b3)] = src
                 continue
             if len(summands) == 1 and len(W1.terms[(b1, summands[0])]) == 1 and len(W2.terms[(summands[0], b3)]) == 1:
                 (o1, s1), = W1.terms[(b1, summands[0])]
@@ -276,8 +293,11 @@ def twosite_mpo(W1: MPOTensor, W2: MPOTensor, p1, p2) -> MPOTensor:
                 acc.blocks = {k: v for k, v in acc.blocks.items() if np.any(v != 0)}
                 if acc.blocks:
                     terms[(b1, b3)] = [(acc, 1.0)]
-    return MPOTensor(W1.row_dim, W2.col_dim, terms, W1.left_herm, W1.left_phase, W2.right_herm, W2.right_phase,
-                     W1.left_spin, W2.right_spin)
+    W = MPOTensor(W1.row_dim, W2.col_dim, terms, W1.left_herm, W1.left_phase, W2.right_herm, W2.right_phase,
+                  W1.left_spin, W2.right_spin)
+    if not merge:
+        W.sources = sources
+    return W
 
 
 # ---- C description ------------------------------------------------------------------
@@ -288,8 +308,10 @@ class MPOHandle:
     def __init__(self, W: MPOTensor, symm: int):
         ops, op_ids = [], {}
         tb1, tb2, top, tsc = [], [], [], []
+        self.term_keys = []   # (b1, b2, j) of each described term, in description order
         for (b1, b2) in sorted(W.terms):
-            for op, sc in W.terms[(b1, b2)]:
+            for j, (op, sc) in enumerate(W.terms[(b1, b2)]):
+                self.term_keys.append((b1, b2, j))
                 if id(op) not in op_ids:
                     op_ids[id(op)] = len(ops)
                     ops.append(op)
@@ -356,6 +378,8 @@ class MPOHandle:
         capi.check(capi.lib.dmrgb200_mpo_create(capi.C.byref(d), capi.C.byref(h)), "dmrgb200_mpo_create")
         self.handle = h
         self.row_dim, self.col_dim = W.row_dim, W.col_dim
+        self.term_scale = np.array(tsc, dtype=np.float64)
+        self.n_terms = len(tsc)
 
     def __del__(self):
         if getattr(self, "handle", None):

@@ -46,6 +46,7 @@ def lib():
         _lib.oracle_hpsi.argtypes = [PD, pp, pp, C.c_void_p, C.c_void_p]
         _lib.oracle_left_step.argtypes = [PD, pp, C.c_void_p, C.c_void_p, pp]
         _lib.oracle_right_step.argtypes = [PD, pp, C.c_void_p, C.c_void_p, pp]
+        _lib.oracle_hpsi_adjoint.argtypes = [PD, pp, pp, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib.oracle_set_threads.argtypes = [C.c_int]
         _lib.oracle_set_threads(int(os.environ.get("ORACLE_THREADS", os.cpu_count() or 1)))
     return _lib
@@ -72,6 +73,22 @@ def hpsi(plan: dict, L: np.ndarray, Lidx: engine.BIndex, R: np.ndarray, Ridx: en
     assert rc == 0
     del keep
     return y
+
+
+def hpsi_adjoint(plan: dict, L: np.ndarray, Lidx: engine.BIndex, R: np.ndarray, Ridx: engine.BIndex,
+                 w: np.ndarray, x: np.ndarray):
+    """(gx, galpha): gx = H^T w, galpha[k] = <w | H_k x> (plan_exec.cpp oracle_hpsi_adjoint)."""
+    desc, keep = capi.numpy_to_desc(plan)
+    gx = np.zeros(plan["in_size"])
+    galpha = np.zeros(len(plan["term_alpha"]))
+    la, ra = _ptrs(L, Lidx), _ptrs(R, Ridx)
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    rc = lib().oracle_hpsi_adjoint(C.byref(desc), la, ra, w.ctypes.data, x.ctypes.data, gx.ctypes.data,
+                                   galpha.ctypes.data)
+    assert rc == 0
+    del keep
+    return gx, galpha
 
 
 def left_step(plan: dict, L: np.ndarray, Lidx: engine.BIndex, ket_rp: np.ndarray, bra_lp: np.ndarray,

@@ -225,4 +225,75 @@ int oracle_right_step(const dmrgb200_plan_desc* dp, const double* const* R, cons
     return 0;
 }
 
+// Adjoint of H psi on the plan (the reference has no derivative code; this is
+// the transpose of the three stages above, run per task group):
+//   G_c = L_c^T w[rb]  (transpose of contract, tasks.cpp:286-313)
+//   galpha[k] = <G cell(k), T cell(k)>, gT cell(k) += alpha_k G cell(k)
+//                      (transpose of create_s_r, tasks.cpp:466-494)
+//   gx slice += gT_t R_t^T  (transpose of create_T, tasks.cpp:650-705)
+// gx (whole in_size range) is overwritten; galpha has n_terms entries.  Either
+// output may be NULL.  A task group owns its input block, so gx needs no lock.
+int oracle_hpsi_adjoint(const dmrgb200_plan_desc* dp, const double* const* L, const double* const* R,
+                        const double* w, const double* x, double* gx, double* galpha) {
+    dmrgb200_plan_desc const& d = *dp;
+    if (d.kind != DMRGB200_PLAN_HPSI) return 1;
+    if (gx) std::memset(gx, 0, sizeof(double) * d.in_size);
+    int ng = int(d.n_groups);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int gi = 0; gi < ng; ++gi) {
+        const uint32_t t0 = d.g_t[gi], t1 = d.g_t[gi + 1];
+        std::vector<std::vector<double>> T, gT;
+        for (uint32_t t = t0; t < t1; ++t) {
+            if (galpha) T.push_back(create_T(d, t, R, x));
+            gT.emplace_back(size_t(d.in_rows[d.t_lb[t]]) * d.t_bcols[t] * d.t_nb[t], 0.0);
+        }
+        for (uint32_t c = d.g_c[gi]; c < d.g_c[gi + 1]; ++c) {
+            int M = int(d.c_rs[c]), N = int(d.c_stripe[c]), K = int(d.c_nsrows[c] * d.c_ls[c]);
+            const double* luse = L[d.c_ci[c]];
+            std::vector<double> lbuf;
+            if (d.c_trans[c]) {
+                lbuf.resize(size_t(M) * K);
+                tr_tile_v(d.c_ls[c], d.c_rs[c], d.c_nsrows[c], L[d.c_ci[c]], lbuf.data());
+                luse = lbuf.data();
+            }
+            std::vector<double> G(size_t(K) * N);
+            gemm('T', 'N', K, N, M, 1.0, luse, M, w + d.out_off[d.c_rb[c]], M, 0.0, G.data(), K);
+            size_t ls = d.c_ls[c];
+            for (uint32_t u = d.c_unit[c]; u < d.c_unit[c + 1]; ++u) {
+                size_t ms = d.u_ms[u];
+                for (uint32_t l = d.u_line[u]; l < d.u_line[u + 1]; ++l) {
+                    const double* gcell = G.data() + size_t(d.l_b1[l]) * ls + size_t(d.u_offset[u]) * K;
+                    for (uint32_t k = d.l_term[l]; k < d.l_term[l + 1]; ++k) {
+                        size_t toff = size_t(d.term_col[k]) * ls;
+                        if (galpha) {
+                            const double* tc = T[d.term_t[k] - t0].data() + toff;
+                            double s = 0.0;
+                            for (size_t j = 0; j < ms; ++j)
+                                for (size_t r = 0; r < ls; ++r) s += gcell[r + j * K] * tc[r + j * ls];
+                            galpha[k] = s;
+                        }
+                        double* gc = gT[d.term_t[k] - t0].data() + toff;
+                        for (size_t j = 0; j < ms; ++j)
+                            for (size_t r = 0; r < ls; ++r) gc[r + j * ls] += d.term_alpha[k] * gcell[r + j * K];
+                    }
+                }
+            }
+        }
+        if (!gx) continue;
+        for (uint32_t t = t0; t < t1; ++t) {
+            int M = int(d.in_rows[d.t_lb[t]]), K = int(d.t_brows[t]), N = int(d.t_bcols[t]);
+            double* out = gx + d.in_off[d.t_lb[t]] + size_t(M) * d.t_col[t];
+            for (uint32_t b = 0; b < d.t_nb[t]; ++b) {
+                const double* rb = R[d.t_ci[t]] + size_t(b) * K * N;
+                const double* g = gT[t - t0].data() + size_t(b) * M * N;
+                if (d.t_trans[t])
+                    gemm('N', 'N', M, K, N, 1.0, g, M, rb, N, 1.0, out, M);
+                else
+                    gemm('N', 'T', M, K, N, 1.0, g, M, rb, K, 1.0, out, M);
+            }
+        }
+    }
+    return 0;
+}
+
 }  // extern "C"

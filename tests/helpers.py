@@ -25,7 +25,7 @@ class OracleChain:
     """Boundaries L (bond i) and R (bond i+2) from oracle boundary steps and the
     two-site H·psi schedule at sites (i, i+1)."""
 
-    def __init__(self, model, bonds, tensors, i, symmetric=True):
+    def __init__(self, model, bonds, tensors, i, symmetric=True, merge=True):
         self.model, self.bonds, self.tensors, self.i = model, bonds, tensors, i
         L = len(tensors)
         Lidx = E.edge_bindex(model.symm, bonds[0])
@@ -44,7 +44,8 @@ class OracleChain:
             Ridx = nidx
         self.Lidx, self.Lval, self.Ridx, self.Rval = Lidx, Lval, Ridx, Rval
         self.p12, _ = M.fuse_phys(model.phys, model.phys)
-        self.W12 = M.MPOHandle(M.twosite_mpo(model.mpo[i], model.mpo[i + 1], model.phys, model.phys), model.symm)
+        self.W12mpo = M.twosite_mpo(model.mpo[i], model.mpo[i + 1], model.phys, model.phys, merge=merge)
+        self.W12 = M.MPOHandle(self.W12mpo, model.symm)
         self.left, self.right = bonds[i], bonds[i + 2]
         self.sched = E.schedule_hpsi(self.p12, self.left, self.right, self.W12, Lidx, Ridx)
 
@@ -63,3 +64,45 @@ def make_chain(name, L, Mmax, seed=0, synthetic_m=None):
         bonds = [S.synthetic_sectors(model.phys, L, model.total_charge, synthetic_m, i) for i in range(L + 1)]
     tensors = S.random_mps(model.phys, bonds, rng)
     return model, bonds, tensors, rng
+
+
+# ---- adjoint fixtures ---------------------------------------------------------------
+
+def perturbed_mpo(W: M.MPOTensor, key, delta: float) -> M.MPOTensor:
+    """Copy of W with the scale of term key = (b1, b2, j) shifted by delta."""
+    import copy
+    terms = {k: list(v) for k, v in W.terms.items()}
+    b1, b2, j = key
+    op, sc = terms[(b1, b2)][j]
+    terms[(b1, b2)][j] = (op, sc + delta)
+    Wp = copy.copy(W)
+    Wp.terms = terms
+    return Wp
+
+
+def hubbard_center_terms(handle: M.MPOHandle, W12: M.MPOTensor):
+    """Two-site (unmerged) term indices of the Fermi-Hubbard FSM MPO whose scale is
+    proportional to the hopping across the centre bond (0 -> {1..4} -> 5), to U of
+    the first site (0 -> 5 -> 5) and to U of the second site (0 -> 0 -> 5)."""
+    out = {"t": [], "U1": [], "U2": []}
+    for idx, (b1, b3, j) in enumerate(handle.term_keys):
+        (_, b2, _), _ = W12.sources[(b1, b3)][j]
+        if (b1, b3) != (0, 5):
+            continue
+        if b2 in (1, 2, 3, 4):
+            out["t"].append(idx)
+        elif b2 == 5:
+            out["U1"].append(idx)
+        elif b2 == 0:
+            out["U2"].append(idx)
+    return out
+
+
+def hubbard_derivative_ops(model, i: int):
+    """dH/dt of the hopping across bond (i, i+1) and dH/dU of sites i and i+1, as
+    term lists of the model's dense builder."""
+    hop = []
+    for s in ("up", "down"):
+        hop.append((-1.0, [(i, "cdag_" + s), (i + 1, "c_" + s)]))
+        hop.append((-1.0, [(i + 1, "cdag_" + s), (i, "c_" + s)]))
+    return {"t": hop, "U1": [(1.0, [(i, "docc")])], "U2": [(1.0, [(i + 1, "docc")])]}

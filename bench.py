@@ -375,6 +375,24 @@ def main():
         emu_err = str(exc)
     yd.copy_(y64)
 
+    # Jacobi-Davidson solve of this site problem (8 iterations at most, tol 1e-8): the
+    # graph-captured solver against the stepwise one (host reads the scalars each iteration)
+    jd = {}
+    xo = torch.zeros_like(xd)
+    for name, mode in (("graph", capi.SOLVER_GRAPH), ("stepwise", capi.SOLVER_STEPWISE)):
+        sp.plan.set_solver(mode)
+        times = []
+        for k in range(4):
+            t0 = time.perf_counter()
+            e, st = sp.plan.solve(xd.data_ptr(), xo.data_ptr(), xd.numel(), tol=1e-8, max_iter=8, stream=sh)
+            wall = (time.perf_counter() - t0) * 1e3
+            if k > 0:
+                times.append((st.solve_ms, wall))
+        jd[name] = {"solve_ms_device": statistics.mean(t[0] for t in times),
+                    "solve_ms_wall": statistics.mean(t[1] for t in times), "iterations": int(st.iterations),
+                    "energy": e}
+    sp.plan.set_solver(capi.SOLVER_GRAPH)
+
     # end to end through the C ABI with pinned host buffers
     xh = torch.from_numpy(psi.data.copy()).pin_memory()
     yh = torch.empty_like(xh).pin_memory()
@@ -453,6 +471,7 @@ def main():
                          "frac": ach / peak if peak else None, "peak_source": peak_src, "traffic": traffic,
                          "stage_ms": stage_ms, "stage_flops": [int(f) for f in fl3],
                          "fp64_dmma_peak_tflops": fp64_peak.value},
+            "jd_solve": jd,
             "cpu_baseline": cpu,
             "max_rel_err_vs_cpu": err,
             "clocks": clocks,

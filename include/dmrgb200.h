@@ -272,11 +272,22 @@ typedef struct {
     uint32_t iterations;
     int32_t converged;
     double residual;
-    double hpsi_ms;
+    double hpsi_ms;  /* device time in H·psi (stepwise solver; 0 for the graph solver) */
+    double solve_ms; /* device time of the whole solve */
 } dmrgb200_solve_stats;
 dmrgb200_status dmrgb200_solve(dmrgb200_plan_t plan, uint64_t n, const double* x0, const double* const* ortho,
                                uint32_t n_ortho, double tol, uint32_t max_iter, double* energy, double* x_out,
                                dmrgb200_solve_stats* stats, void* cuda_stream);
+
+/* How dmrgb200_solve drives the iteration.
+ * DMRGB200_SOLVER_GRAPH (default): all scalars stay on the device and the whole
+ *   solve is one CUDA graph launch (one iteration = the body of a conditional
+ *   WHILE node), built on the first solve and reused while n, max_iter,
+ *   n_ortho and tol stay the same; one host synchronisation per solve.
+ * DMRGB200_SOLVER_STEPWISE: the host reads the scalars each iteration (as the
+ *   reference's solver does) and times each H·psi. */
+enum { DMRGB200_SOLVER_GRAPH = 0, DMRGB200_SOLVER_STEPWISE = 1 };
+dmrgb200_status dmrgb200_plan_set_solver(dmrgb200_plan_t plan, int mode);
 
 /* ---- H·psi for callers that cannot allocate device memory --------------- */
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc

@@ -68,6 +68,9 @@ struct dmrgb200_plan_s {
     OzProgram* oz3 = nullptr;
     void* oz_scratch = nullptr;
     uint64_t oz_scratch_size = 0;
+    // Jacobi-Davidson: solver mode and the cached solver graph
+    int solver_mode = DMRGB200_SOLVER_GRAPH;
+    void* jd = nullptr;
     // adjoint program (built on first use)
     bool adj_built = false;
     std::string adj_err;
@@ -317,6 +320,8 @@ cudaError_t plan_hpsi_launch(dmrgb200_plan_t plan, const double* x, double* y, c
                        stream);
 }
 void noalloc_desc_to_flat(const dmrgb200_plan_desc* d, FlatPlan& f) { desc_to_flat(d, f); }
+int plan_solver_mode(dmrgb200_plan_t plan) { return plan->solver_mode; }
+void** plan_jd_cache(dmrgb200_plan_t plan) { return &plan->jd; }
 }  // namespace dmrgb200
 
 extern "C" {
@@ -436,6 +441,7 @@ dmrgb200_status dmrgb200_plan_destroy(dmrgb200_plan_t plan) {
     if (!plan) return DMRGB200_OK;
     if (plan->compiled) free_program(plan->prog);
     if (plan->adj_built) free_adjoint(plan->adj);
+    jd_graph_free(plan->jd);
     oz_free(plan->oz1);
     oz_free(plan->oz3);
     cudaFree(plan->oz_scratch);
@@ -496,6 +502,13 @@ dmrgb200_status dmrgb200_hpsi_adjoint(dmrgb200_plan_t plan, const double* w, con
     if (e != cudaSuccess) return cuda_fail(e, "adjoint launch");
     return DMRGB200_OK;
     DMRGB200_CATCH
+}
+
+dmrgb200_status dmrgb200_plan_set_solver(dmrgb200_plan_t plan, int mode) {
+    if (!plan || (mode != DMRGB200_SOLVER_GRAPH && mode != DMRGB200_SOLVER_STEPWISE))
+        return fail(DMRGB200_INVALID_ARGUMENT, "unknown solver mode");
+    plan->solver_mode = mode;
+    return DMRGB200_OK;
 }
 
 dmrgb200_status dmrgb200_plan_set_slices(dmrgb200_plan_t plan, int slices) {

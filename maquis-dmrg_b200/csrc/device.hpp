@@ -184,5 +184,7 @@ cudaError_t oz_run(OzProgram* oz, Bases const& bs, int s, void* scratch, cudaStr
 // non-zero when a pipeline wait of the last run timed out (synchronises the stream)
 int oz_timed_out(OzProgram const* oz, void* scratch, int s, cudaStream_t st);
 double calibrate_fp64_tflops();
+// solver graph cache of a plan (jd_graph.cu)
+void jd_graph_free(void* g);
 
 }  // namespace dmrgb200

@@ -28,6 +28,11 @@ namespace dmrgb200 {
 
 dmrgb200_status noalloc_fail(dmrgb200_status s, std::string const& msg);  // error recording (capi.cpp)
 cudaError_t plan_hpsi_launch(dmrgb200_plan_t plan, const double* x, double* y, cudaStream_t stream);
+int plan_solver_mode(dmrgb200_plan_t plan);
+void** plan_jd_cache(dmrgb200_plan_t plan);
+dmrgb200_status solve_graph(dmrgb200_plan_t plan, void** cache, uint64_t n, const double* x0,
+                            const double* const* ortho, uint32_t n_ortho, double tol, uint32_t max_iter,
+                            double* energy, double* x_out, dmrgb200_solve_stats* stats, cudaStream_t s);
 
 namespace {
 
@@ -178,6 +183,8 @@ extern "C" dmrgb200_status dmrgb200_solve(dmrgb200_plan_t plan, uint64_t n, cons
     if (max_iter < 1 || max_iter > 32) return noalloc_fail(DMRGB200_INVALID_ARGUMENT, "max_iter must be in 1..32");
     if (n_ortho > 8) return noalloc_fail(DMRGB200_INVALID_ARGUMENT, "at most 8 orthogonal vectors");
     cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+    if (plan_solver_mode(plan) == DMRGB200_SOLVER_GRAPH)
+        return solve_graph(plan, plan_jd_cache(plan), n, x0, ortho, n_ortho, tol, max_iter, energy, x_out, stats, st);
     const int nv = int(2 * max_iter + 2 + n_ortho);
     Workspace w;
     cudaError_t e;
@@ -263,9 +270,12 @@ extern "C" dmrgb200_status dmrgb200_solve(dmrgb200_plan_t plan, uint64_t n, cons
     uint32_t iter = 0;
     bool converged = false;
     float hpsi_ms = 0.f;
-    cudaEvent_t e0, e1;
+    cudaEvent_t e0, e1, s0, s1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
+    cudaEventCreate(&s0);
+    cudaEventCreate(&s1);
+    cudaEventRecord(s0, st);
 
     CK(cudaMemcpyAsync(V(0), x0, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
     CK(project(V(0)));
@@ -283,6 +293,8 @@ extern "C" dmrgb200_status dmrgb200_solve(dmrgb200_plan_t plan, uint64_t n, cons
         if (!(tn > 0.0)) {
             cudaEventDestroy(e0);
             cudaEventDestroy(e1);
+            cudaEventDestroy(s0);
+            cudaEventDestroy(s1);
             return noalloc_fail(DMRGB200_NUMERIC, "Davidson direction vanished");
         }
         scal_host<<<EB, ET, 0, st>>>(t, n, 1.0 / tn);
@@ -329,15 +341,21 @@ extern "C" dmrgb200_status dmrgb200_solve(dmrgb200_plan_t plan, uint64_t n, cons
         CK(cudaGetLastError());
     }
     CK(cudaMemcpyAsync(x_out, u, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    cudaEventRecord(s1, st);
     CK(cudaStreamSynchronize(st));
+    float solve_ms = 0.f;
+    cudaEventElapsedTime(&solve_ms, s0, s1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    cudaEventDestroy(s0);
+    cudaEventDestroy(s1);
     *energy = theta;
     if (stats) {
         stats->iterations = iter;
         stats->converged = converged ? 1 : 0;
         stats->residual = rnorm;
         stats->hpsi_ms = hpsi_ms;
+        stats->solve_ms = solve_ms;
     }
 #undef CK
     return DMRGB200_OK;

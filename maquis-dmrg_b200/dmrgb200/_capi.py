@@ -34,6 +34,7 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "invalid plan", 3: "out of memory",
 PLAN_HPSI, PLAN_LEFT, PLAN_RIGHT = 0, 1, 2
 U1, TWOU1, SU2U1 = 1, 2, 3
 PREC_FP64, PREC_FP64_EMULATED = 0, 1
+SOLVER_GRAPH, SOLVER_STEPWISE = 0, 1
 
 
 class DmrgError(RuntimeError):
@@ -82,7 +83,7 @@ class MpoDesc(C.Structure):
 
 class SolveStats(C.Structure):
     _fields_ = [("iterations", C.c_uint32), ("converged", C.c_int32), ("residual", C.c_double),
-                ("hpsi_ms", C.c_double)]
+                ("hpsi_ms", C.c_double), ("solve_ms", C.c_double)]
 
 
 class BoundaryView(C.Structure):
@@ -112,6 +113,7 @@ _sigs = {
     "dmrgb200_hpsi_adjoint": ([vp, vp, vp, vp, vp, vp], C.c_int),
     "dmrgb200_plan_set_timing": ([vp, C.c_int], C.c_int),
     "dmrgb200_plan_set_slices": ([vp, C.c_int], C.c_int),
+    "dmrgb200_plan_set_solver": ([vp, C.c_int], C.c_int),
     "dmrgb200_plan_stage_times": ([vp, f64p, u64p, u64p], C.c_int),
     "dmrgb200_dgemm_emulated": ([C.c_uint32, C.c_uint32, C.c_uint32, vp, C.c_uint64, vp, C.c_uint64, vp,
                                  C.c_uint64, C.c_int, vp], C.c_int),

@@ -206,6 +206,10 @@ class DevicePlan:
         capi.check(capi.lib.dmrgb200_hpsi_adjoint(self.handle, w_ptr, x_ptr or None, gx_ptr or None,
                                                   galpha_ptr or None, stream or None), "dmrgb200_hpsi_adjoint")
 
+    def set_solver(self, mode: int) -> None:
+        """capi.SOLVER_GRAPH (default: one CUDA graph per solve) or capi.SOLVER_STEPWISE."""
+        capi.check(capi.lib.dmrgb200_plan_set_solver(self.handle, mode), "dmrgb200_plan_set_solver")
+
     def solve(self, x0_ptr: int, x_out_ptr: int, n: int, ortho_ptrs=(), tol: float = 1e-8, max_iter: int = 8,
               stream: int = 0):
         """Jacobi-Davidson lowest eigenpair (dmrgb200_solve); returns (energy, stats)."""

@@ -188,7 +188,7 @@ def sweep_workload(args):
             "config": {"workload": "heisenberg_L32_u1_m128_4sweeps", "sites": L, "bond_dim": m, "sweeps": nsweeps},
             "sweep_seconds": dev.log.sweep_seconds, "final_energy": float(ed[-1]),
             "max_abs_energy_diff_vs_oracle": float(np.max(np.abs(ed - ec))),
-            "hpsi_calls": dev.log.hpsi_calls, "hpsi_device_ms": dev.log.hpsi_ms,
+            "hpsi_calls": dev.log.hpsi_calls, "solve_device_ms": dev.log.solve_ms,
             "cpu_oracle_sweep_seconds": cpu.log.sweep_seconds, "cpu_oracle_final_energy": float(ec[-1]),
             "note": "two-site formation and SVD truncation on the host (numpy); H·psi, JD and boundary steps on the device"}
     print(json.dumps(line), flush=True)
@@ -321,6 +321,11 @@ def main():
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
     prof_prec = capi.PREC_FP64_EMULATED if (args.profile and args.prec == "emulated") else capi.PREC_FP64
+    import ctypes as C
+    chosen = (C.c_int32 * 2)()
+    capi.check(capi.lib.dmrgb200_plan_autotune(sp.plan.handle, xd.data_ptr(), yd.data_ptr(), sh, chosen), "autotune")
+    autotune = {"stage1_gemm": capi.lib.dmrgb200_gemm_variant_name(chosen[0]).decode(),
+                "stage3_gemm": capi.lib.dmrgb200_gemm_variant_name(chosen[1]).decode()}
     for _ in range(args.warmup):
         sp.plan.hpsi(xd.data_ptr(), yd.data_ptr(), prof_prec, sh)
     torch.cuda.synchronize(dev)
@@ -348,7 +353,6 @@ def main():
         print(json.dumps({"profile": True, "ms_per_step": sum(step_ms) / len(step_ms), "flops": int(flops)}))
         return
     total_ms = sum(step_ms)
-    import ctypes as C
     ms3 = (C.c_double * 3)()
     fl3 = (C.c_uint64 * 3)()
     calls = C.c_uint64()
@@ -375,8 +379,9 @@ def main():
         emu_err = str(exc)
     yd.copy_(y64)
 
-    # Jacobi-Davidson solve of this site problem (8 iterations at most, tol 1e-8): the
-    # graph-captured solver against the stepwise one (host reads the scalars each iteration)
+    # Jacobi-Davidson solve of this site problem, 8 iterations (the reference's
+    # ietl_jcd_maxiter; tol 0 so that every iteration runs): the graph-captured solver
+    # against the stepwise one (host reads the scalars each iteration)
     jd = {}
     xo = torch.zeros_like(xd)
     for name, mode in (("graph", capi.SOLVER_GRAPH), ("stepwise", capi.SOLVER_STEPWISE)):
@@ -384,7 +389,7 @@ def main():
         times = []
         for k in range(4):
             t0 = time.perf_counter()
-            e, st = sp.plan.solve(xd.data_ptr(), xo.data_ptr(), xd.numel(), tol=1e-8, max_iter=8, stream=sh)
+            e, st = sp.plan.solve(xd.data_ptr(), xo.data_ptr(), xd.numel(), tol=0.0, max_iter=8, stream=sh)
             wall = (time.perf_counter() - t0) * 1e3
             if k > 0:
                 times.append((st.solve_ms, wall))
@@ -472,6 +477,7 @@ def main():
                          "stage_ms": stage_ms, "stage_flops": [int(f) for f in fl3],
                          "fp64_dmma_peak_tflops": fp64_peak.value},
             "jd_solve": jd,
+            "autotune": autotune,
             "cpu_baseline": cpu,
             "max_rel_err_vs_cpu": err,
             "clocks": clocks,

@@ -201,6 +201,17 @@ dmrgb200_status dmrgb200_plan_scratch_bytes(dmrgb200_plan_t plan, uint64_t* byte
 dmrgb200_status dmrgb200_hpsi(dmrgb200_plan_t plan, const double* x, double* y, dmrgb200_precision prec,
                               void* cuda_stream);
 
+/* Autotuning of the grouped FP64 GEMMs: every variant (pipeline depth x CTAs
+ * per SM) is timed on the plan's stage-1 and stage-3 tile lists and the
+ * fastest is kept per stage.  The first FP64 dmrgb200_hpsi / dmrgb200_solve of
+ * a plan of at least 50 MFLOP per H·psi does this by itself (environment
+ * DMRGB200_AUTOTUNE=0 keeps the default variant); this call re-tunes now, using x (in layout) and y (out
+ * layout, overwritten), and returns the chosen variant per stage.  No
+ * counterpart in the reference (its cuBLAS calls are untuned). */
+dmrgb200_status dmrgb200_plan_autotune(dmrgb200_plan_t plan, const double* x, double* y, void* cuda_stream,
+                                       int32_t variants[2]);
+const char* dmrgb200_gemm_variant_name(int variant);
+
 /* Adjoint of H·psi (no counterpart in the reference, which has no derivative
  * code).  With the plan's terms y = sum_k alpha_k H_k x, one call gives
  *   gx          = H^T w                      (the plan's in layout; may be NULL)

@@ -238,13 +238,17 @@ cudaError_t run_adjoint(DeviceProgram const& fwd, AdjointProgram const& a, uint6
     const uint32_t sms = uint32_t(device_sm_count());
     cudaError_t e;
     if (!gx && !galpha) return cudaSuccess;
-    if ((e = launch_gemm(a.d3, bs, stream)) != cudaSuccess) return e;  // G into S
+    GemmDev d3 = a.d3, d1 = a.d1;  // the transposed stages use the forward stages' tuned variants
+    d3.var = fwd.var3;
+    d1.var = fwd.var1;
+    if ((e = launch_gemm(d3, bs, stream)) != cudaSuccess) return e;  // G into S
     if (galpha) {
         GemmDev f1;
         f1.p = fwd.d_p1;
         f1.s = fwd.d_s1;
         f1.t = fwd.d_t1;
         f1.n = fwd.n_t1;
+        f1.var = fwd.var1;
         if ((e = launch_gemm(f1, bs, stream)) != cudaSuccess) return e;  // T = x-slices * R
         if (a.n_aterms) {
             uint32_t grid = std::min<uint32_t>((a.n_aterms + 7) / 8, sms * 8);
@@ -259,7 +263,7 @@ cudaError_t run_adjoint(DeviceProgram const& fwd, AdjointProgram const& a, uint6
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
         if ((e = cudaMemsetAsync(gx, 0, gx_elems * sizeof(double), stream)) != cudaSuccess) return e;
-        if ((e = launch_gemm(a.d1, bs, stream)) != cudaSuccess) return e;  // gx = gT * R^T
+        if ((e = launch_gemm(d1, bs, stream)) != cudaSuccess) return e;  // gx = gT * R^T
     }
     return cudaSuccess;
 }

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <exception>
 #include <limits>
@@ -321,6 +322,24 @@ cudaError_t plan_hpsi_launch(dmrgb200_plan_t plan, const double* x, double* y, c
 }
 void noalloc_desc_to_flat(const dmrgb200_plan_desc* d, FlatPlan& f) { desc_to_flat(d, f); }
 int plan_solver_mode(dmrgb200_plan_t plan) { return plan->solver_mode; }
+// Autotune the plan's grouped GEMMs once, outside any stream capture (DMRGB200_AUTOTUNE=0
+// keeps the default variant, and so do plans below 50 MFLOP per H psi).
+cudaError_t plan_ensure_tuned(dmrgb200_plan_t plan, const double* x, double* y, cudaStream_t stream) {
+    if (plan->prog.tuned || !plan->compiled) return cudaSuccess;
+    static const bool enabled = [] {
+        const char* v = std::getenv("DMRGB200_AUTOTUNE");
+        return !(v && v[0] == '0');
+    }();
+    // small plans keep the default variant: tuning would cost more than it saves
+    if (!enabled || plan->flat.flops() < 50000000ull) {
+        plan->prog.tuned = true;
+        return cudaSuccess;
+    }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return cudaSuccess;
+    return tune_program(plan->prog, reinterpret_cast<uint64_t>(x), reinterpret_cast<uint64_t>(y), plan->T, plan->S,
+                        stream);
+}
 void** plan_jd_cache(dmrgb200_plan_t plan) { return &plan->jd; }
 }  // namespace dmrgb200
 
@@ -472,6 +491,10 @@ dmrgb200_status dmrgb200_hpsi(dmrgb200_plan_t plan, const double* x, double* y, 
     if (prec == DMRGB200_PREC_FP64_EMULATED) return hpsi_emulated(plan, x, y, static_cast<cudaStream_t>(cuda_stream));
     if (prec != DMRGB200_PREC_FP64) return fail(DMRGB200_INVALID_ARGUMENT, "unknown precision");
     if (plan->timing) plan->collect();
+    {
+        cudaError_t te = plan_ensure_tuned(plan, x, y, static_cast<cudaStream_t>(cuda_stream));
+        if (te != cudaSuccess) return cuda_fail(te, "grouped GEMM autotuning");
+    }
     cudaError_t e = run_program(plan->prog, reinterpret_cast<uint64_t>(x), reinterpret_cast<uint64_t>(y), plan->T,
                                 plan->S, static_cast<cudaStream_t>(cuda_stream), plan->timing ? plan->ev : nullptr);
     if (e != cudaSuccess) return cuda_fail(e, "hpsi launch");
@@ -503,6 +526,24 @@ dmrgb200_status dmrgb200_hpsi_adjoint(dmrgb200_plan_t plan, const double* w, con
     return DMRGB200_OK;
     DMRGB200_CATCH
 }
+
+dmrgb200_status dmrgb200_plan_autotune(dmrgb200_plan_t plan, const double* x, double* y, void* cuda_stream,
+                                       int32_t variants[2]) {
+    if (!plan || !x || !y) return fail(DMRGB200_INVALID_ARGUMENT, "null argument");
+    if (plan->flat.kind != KIND_HPSI) return fail(DMRGB200_INVALID_PLAN, "plan is not an H psi plan");
+    plan->prog.tuned = false;
+    cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+    cudaError_t e = tune_program(plan->prog, reinterpret_cast<uint64_t>(x), reinterpret_cast<uint64_t>(y), plan->T,
+                                 plan->S, st);
+    if (e != cudaSuccess) return cuda_fail(e, "grouped GEMM autotuning");
+    if (variants) {
+        variants[0] = plan->prog.var1;
+        variants[1] = plan->prog.var3;
+    }
+    return DMRGB200_OK;
+}
+
+const char* dmrgb200_gemm_variant_name(int variant) { return gemm_variant_name(variant); }
 
 dmrgb200_status dmrgb200_plan_set_solver(dmrgb200_plan_t plan, int mode) {
     if (!plan || (mode != DMRGB200_SOLVER_GRAPH && mode != DMRGB200_SOLVER_STEPWISE))

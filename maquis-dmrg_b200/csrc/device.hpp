@@ -37,6 +37,7 @@ struct DevSeg {
 
 struct DevTile {
     uint32_t prob, batch, m0, n0;
+    uint32_t nsteps;  // K steps of the tile over all its segments (at least 1)
 };
 
 struct DevSLine {
@@ -98,6 +99,9 @@ struct DeviceProgram {
     DevSLine* d_lines = nullptr;
     DevSTerm* d_terms = nullptr;
     uint32_t n_t1 = 0, n_t3 = 0, n_lines = 0;
+    // grouped-GEMM variant per stage (autotuned by tune_program)
+    int var1 = 0, var3 = 0;
+    bool tuned = false;
 };
 
 // Lower a flat plan.  lptr/rptr: device address of each cohort's storage of the
@@ -128,7 +132,15 @@ struct GemmDev {
     DevSeg* s = nullptr;
     DevTile* t = nullptr;
     uint32_t n = 0;
+    int var = 0;  // grouped-GEMM variant
 };
+// grouped-GEMM variants (pipeline depth x CTAs per SM)
+constexpr int N_GEMM_VARIANTS = 4;
+const char* gemm_variant_name(int v);
+// Time every variant on the program's stage-1 and stage-3 tile lists (on the given
+// buffers, whose contents are overwritten as by an H psi) and keep the fastest per
+// stage.  Must not run during stream capture.
+cudaError_t tune_program(DeviceProgram& prog, uint64_t in, uint64_t out, double* T, double* S, cudaStream_t stream);
 cudaError_t upload_gemm(GemmList const& gl, GemmDev& d);
 void free_gemm(GemmDev& d);
 // one persistent grouped-GEMM launch over the tile list

@@ -26,6 +26,7 @@ namespace dmrgb200 {
 
 dmrgb200_status noalloc_fail(dmrgb200_status s, std::string const& msg);
 cudaError_t plan_hpsi_launch(dmrgb200_plan_t plan, const double* x, double* y, cudaStream_t stream);
+cudaError_t plan_ensure_tuned(dmrgb200_plan_t plan, const double* x, double* y, cudaStream_t stream);
 
 namespace {
 
@@ -441,6 +442,10 @@ cudaError_t build_graph(JdGraph& g, dmrgb200_plan_t plan, cudaStream_t s) {
     a.st = g.st;
     a.partial = g.partial;
 
+    // the grouped GEMMs are tuned before capture (on the zeroed t and y slots)
+    if ((e = plan_ensure_tuned(plan, g.vec + n * (2 * g.max_iter + 2), g.vec + n * (2 * g.max_iter + 3), s)) !=
+        cudaSuccess)
+        return e;
     if ((e = cudaGraphCreate(&g.graph, 0)) != cudaSuccess) return e;
     if ((e = cudaGraphConditionalHandleCreate(&a.cond, g.graph, 1, cudaGraphCondAssignDefault)) != cudaSuccess)
         return e;

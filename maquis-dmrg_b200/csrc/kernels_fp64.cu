@@ -40,8 +40,10 @@ __device__ __forceinline__ void cp_async8(double* smem, const double* gmem, bool
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(saddr), "l"(gmem), "r"(n));
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;\n" ::); }
-__device__ __forceinline__ void cp_async_wait_0() { asm volatile("cp.async.wait_group 0;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
 
 struct TileCursor {
     uint32_t seg, k0;
@@ -88,13 +90,22 @@ __device__ __forceinline__ void load_tile(double (*As)[LDA_S], double (*Bs)[LDB_
 }
 
 // Grouped, persistent FP64 GEMM over a tile list.  Each CTA owns whole output
-// tiles (BM x BN) and walks every K tile of every segment of its problem with a
-// two-stage cp.async pipeline; 4 warps in a 2 x 2 grid, warp tile 16 x 32,
-// DMMA m8n8k4.
-__global__ void __launch_bounds__(NTHREADS, 4) gemm_f64_grouped(const DevProb* __restrict__ probs,
-                                                                const DevSeg* __restrict__ segs,
-                                                                const DevTile* __restrict__ tiles, uint32_t n_tiles,
-                                                                Bases bases) {
+// tiles (BM x BN) and walks every K step of every segment of its problem; the
+// CTA's K steps over all its tiles form one stream, so the cp.async pipeline
+// (STAGES deep) keeps loading the next tile's operands while the current tile
+// finishes and stores.  4 warps in a 2 x 2 grid, warp tile 16 x 32, DMMA
+// m8n8k4.  A tile whose segments are all empty (one step, no copies) stores
+// zeros.
+struct LoadCursor {
+    uint32_t ti, seg, seg_end, k0;
+    bool valid;
+};
+
+template <int STAGES, int MINB>
+__global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb* __restrict__ probs,
+                                                                   const DevSeg* __restrict__ segs,
+                                                                   const DevTile* __restrict__ tiles, uint32_t n_tiles,
+                                                                   Bases bases) {
     __shared__ __align__(16) double As[STAGES][BK][LDA_S];
     __shared__ __align__(16) double Bs[STAGES][BK][LDB_S];
 
@@ -103,61 +114,80 @@ __global__ void __launch_bounds__(NTHREADS, 4) gemm_f64_grouped(const DevProb* _
     const int wm = (warp >> 1) * 16, wn = (warp & 1) * 32;
     const int g = lane >> 2, q = lane & 3;
 
-    for (uint32_t ti = blockIdx.x; ti < n_tiles; ti += gridDim.x) {
-        const DevTile tl = tiles[ti];
-        const DevProb pr = probs[tl.prob];
-        const uint32_t M = pr.M, N = pr.N;
-        double acc[2][4][2];
-#pragma unroll
-        for (int i = 0; i < 2; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-
-        // flattened (segment, k0) sequence
-        TileCursor cur{pr.seg_begin, 0};
-        while (cur.seg < pr.seg_end && segs[cur.seg].K == 0) ++cur.seg;
-        if (cur.seg < pr.seg_end) {
-            DevSeg sg = segs[cur.seg];
-            load_tile(As[0], Bs[0], sg, op_base(bases, sg.A, tl.batch), op_base(bases, sg.B, tl.batch), tl.m0,
-                      tl.n0, M, N, 0, tid);
+    // ---- producer: walks (tile, segment, k0) and issues one K step per call ----
+    LoadCursor L{blockIdx.x, 0, 0, 0, false};
+    auto enter_tile = [&]() {
+        L.valid = L.ti < n_tiles;
+        if (!L.valid) return;
+        const DevProb& pr = probs[tiles[L.ti].prob];
+        L.seg = pr.seg_begin;
+        L.seg_end = pr.seg_end;
+        L.k0 = 0;
+        while (L.seg < L.seg_end && segs[L.seg].K == 0) ++L.seg;
+    };
+    auto issue = [&](int slot) {
+        if (!L.valid) return;
+        if (L.seg < L.seg_end) {  // an empty tile issues no copies
+            const DevTile tl = tiles[L.ti];
+            const DevProb& pr = probs[tl.prob];
+            const DevSeg sg = segs[L.seg];
+            load_tile(As[slot], Bs[slot], sg, op_base(bases, sg.A, tl.batch), op_base(bases, sg.B, tl.batch), tl.m0,
+                      tl.n0, pr.M, pr.N, L.k0, tid);
+            L.k0 += BK;
+            if (L.k0 < sg.K) return;
+            L.k0 = 0;
+            ++L.seg;
+            while (L.seg < L.seg_end && segs[L.seg].K == 0) ++L.seg;
+            if (L.seg < L.seg_end) return;
         }
+        L.ti += gridDim.x;
+        enter_tile();
+    };
+
+    enter_tile();
+#pragma unroll
+    for (int s = 0; s < STAGES - 1; ++s) {
+        issue(s);
         cp_async_commit();
-        int stage = 0;
-        while (cur.seg < pr.seg_end) {
-            // advance to the next K tile and prefetch it
-            TileCursor nxt = cur;
-            nxt.k0 += BK;
-            if (nxt.k0 >= segs[nxt.seg].K) {
-                nxt.k0 = 0;
-                ++nxt.seg;
-                while (nxt.seg < pr.seg_end && segs[nxt.seg].K == 0) ++nxt.seg;
-            }
-            if (nxt.seg < pr.seg_end) {
-                DevSeg sg = segs[nxt.seg];
-                load_tile(As[stage ^ 1], Bs[stage ^ 1], sg, op_base(bases, sg.A, tl.batch),
-                          op_base(bases, sg.B, tl.batch), tl.m0, tl.n0, M, N, nxt.k0, tid);
-            }
+    }
+
+    double acc[2][4][2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+    // ---- consumer: tiles in the same order, nsteps K steps each ----
+    int slot = 0;
+    for (uint32_t ti = blockIdx.x; ti < n_tiles; ti += gridDim.x) {
+        const uint32_t nsteps = tiles[ti].nsteps;
+        for (uint32_t st = 0; st < nsteps; ++st) {
+            issue((slot + STAGES - 1) % STAGES);
             cp_async_commit();
-            cp_async_wait_1();
+            cp_async_wait<STAGES - 1>();
             __syncthreads();
 #pragma unroll
             for (int kk = 0; kk < BK; kk += 4) {
                 double a[2], b[4];
 #pragma unroll
-                for (int i = 0; i < 2; ++i) a[i] = As[stage][kk + q][wm + i * 8 + g];
+                for (int i = 0; i < 2; ++i) a[i] = As[slot][kk + q][wm + i * 8 + g];
 #pragma unroll
-                for (int j = 0; j < 4; ++j) b[j] = Bs[stage][kk + q][wn + j * 8 + g];
+                for (int j = 0; j < 4; ++j) b[j] = Bs[slot][kk + q][wn + j * 8 + g];
 #pragma unroll
                 for (int i = 0; i < 2; ++i)
 #pragma unroll
                     for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
             }
             __syncthreads();
-            stage ^= 1;
-            cur = nxt;
+            slot = (slot + 1) % STAGES;
         }
-        cp_async_wait_0();
-
+        // epilogue (the next tile's first steps are already in flight); an empty
+        // tile's single step multiplied zero-filled or stale shared memory, so its
+        // accumulators are cleared instead of stored
+        const DevTile tl = tiles[ti];
+        const DevProb pr = probs[tl.prob];
+        bool empty = true;
+        for (uint32_t sg = pr.seg_begin; sg < pr.seg_end; ++sg) empty = empty && segs[sg].K == 0;
         double* C = const_cast<double*>(op_base(bases, pr.C, tl.batch));
         const uint64_t ldc = pr.C.ld;
 #pragma unroll
@@ -168,9 +198,11 @@ __global__ void __launch_bounds__(NTHREADS, 4) gemm_f64_grouped(const DevProb* _
                 for (int e = 0; e < 2; ++e) {
                     uint32_t r = tl.m0 + wm + i * 8 + g;
                     uint32_t c = tl.n0 + wn + j * 8 + q * 2 + e;
-                    if (r < M && c < N) C[r + c * ldc] = acc[i][j][e];
+                    if (r < pr.M && c < pr.N) C[r + c * ldc] = empty ? 0.0 : acc[i][j][e];
+                    acc[i][j][e] = 0.0;
                 }
     }
+    cp_async_wait<0>();
 }
 
 // S build: S is tiled by cells (one per unit and MPO row block); a cell with a
@@ -215,9 +247,13 @@ __global__ void __launch_bounds__(128) dmma_rate_loop(int iters, double* sink) {
 
 void add_tiles(GemmList& gl, uint32_t prob, uint32_t nbatch) {
     DevProb const& p = gl.probs[prob];
+    uint32_t nsteps = 0;
+    for (uint32_t s = p.seg_begin; s < p.seg_end; ++s) nsteps += (gl.segs[s].K + BK - 1) / BK;
+    nsteps = std::max<uint32_t>(nsteps, 1);  // an empty problem: one step that issues no copies
     for (uint32_t b = 0; b < nbatch; ++b)
         for (uint32_t m0 = 0; m0 < std::max<uint32_t>(p.M, 1); m0 += BM)
-            for (uint32_t n0 = 0; n0 < std::max<uint32_t>(p.N, 1); n0 += BN) gl.tiles.push_back(DevTile{prob, b, m0, n0});
+            for (uint32_t n0 = 0; n0 < std::max<uint32_t>(p.N, 1); n0 += BN)
+                gl.tiles.push_back(DevTile{prob, b, m0, n0, nsteps});
 }
 
 // Order tiles by decreasing K work so that the static round-robin of the
@@ -517,22 +553,96 @@ void free_gemm(GemmDev& d) {
 }
 
 namespace {
-int gemm_occupancy() {
-    static int occ = 0;
-    if (!occ) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, gemm_f64_grouped, NTHREADS, 0);
-        if (occ <= 0) occ = 1;
+using GemmKernel = void (*)(const DevProb*, const DevSeg*, const DevTile*, uint32_t, Bases);
+
+// pipeline depth x CTAs per SM of the grouped GEMM, chosen per stage by the autotuner
+struct GemmVariant {
+    GemmKernel fn;
+    const char* name;
+};
+const GemmVariant kVariants[N_GEMM_VARIANTS] = {
+    {gemm_f64_grouped<2, 4>, "stages2_ctas4"},
+    {gemm_f64_grouped<3, 4>, "stages3_ctas4"},
+    {gemm_f64_grouped<2, 5>, "stages2_ctas5"},
+    {gemm_f64_grouped<3, 5>, "stages3_ctas5"},
+};
+
+int variant_occupancy(int v) {
+    static int occ[N_GEMM_VARIANTS] = {0};
+    if (!occ[v]) {
+        int o = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kVariants[v].fn, NTHREADS, 0);
+        occ[v] = o > 0 ? o : 1;
     }
-    return occ;
+    return occ[v];
+}
+
+cudaError_t launch_variant(int v, const DevProb* p, const DevSeg* sg, const DevTile* t, uint32_t n, Bases const& bs,
+                           cudaStream_t stream) {
+    if (!n) return cudaSuccess;
+    if (v < 0 || v >= N_GEMM_VARIANTS) v = 0;
+    uint32_t grid = std::min<uint32_t>(n, uint32_t(device_sm_count()) * variant_occupancy(v));
+    kVariants[v].fn<<<grid, NTHREADS, 0, stream>>>(p, sg, t, n, bs);
+    return cudaGetLastError();
 }
 }  // namespace
 
+const char* gemm_variant_name(int v) { return (v >= 0 && v < N_GEMM_VARIANTS) ? kVariants[v].name : "?"; }
+
 cudaError_t launch_gemm(GemmDev const& d, Bases const& bs, cudaStream_t stream) {
-    if (d.n) {
-        uint32_t grid = std::min<uint32_t>(d.n, uint32_t(device_sm_count()) * gemm_occupancy());
-        gemm_f64_grouped<<<grid, NTHREADS, 0, stream>>>(d.p, d.s, d.t, d.n, bs);
+    return launch_variant(d.var, d.p, d.s, d.t, d.n, bs, stream);
+}
+
+cudaError_t tune_program(DeviceProgram& prog, uint64_t in, uint64_t out, double* T, double* S, cudaStream_t stream) {
+    Bases bs{};
+    bs.b[BUF_IN] = in;
+    bs.b[BUF_OUT] = out;
+    bs.b[BUF_T] = reinterpret_cast<uint64_t>(T);
+    bs.b[BUF_S] = reinterpret_cast<uint64_t>(S);
+    cudaEvent_t e0, e1;
+    cudaError_t e;
+    if ((e = cudaEventCreate(&e0)) != cudaSuccess) return e;
+    if ((e = cudaEventCreate(&e1)) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return e;
     }
-    return cudaGetLastError();
+    struct Stage {
+        const DevProb* p;
+        const DevSeg* s;
+        const DevTile* t;
+        uint32_t n;
+        int* var;
+    } stages[2] = {{prog.d_p1, prog.d_s1, prog.d_t1, prog.n_t1, &prog.var1},
+                   {prog.d_p3, prog.d_s3, prog.d_t3, prog.n_t3, &prog.var3}};
+    // stage 1 writes T, read by nothing else here; stage 3 reads S: both are timed on the
+    // plan's current scratch contents (the kernels' speed does not depend on the values)
+    for (auto& st : stages) {
+        if (!st.n) continue;
+        float best = 1e30f;
+        int bv = 0;
+        for (int v = 0; v < N_GEMM_VARIANTS && e == cudaSuccess; ++v) {
+            e = launch_variant(v, st.p, st.s, st.t, st.n, bs, stream);  // warm
+            float tot = 0.f;
+            for (int r = 0; r < 2 && e == cudaSuccess; ++r) {
+                cudaEventRecord(e0, stream);
+                e = launch_variant(v, st.p, st.s, st.t, st.n, bs, stream);
+                cudaEventRecord(e1, stream);
+                if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                tot += ms;
+            }
+            if (tot < best) {
+                best = tot;
+                bv = v;
+            }
+        }
+        *st.var = bv;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    prog.tuned = e == cudaSuccess;
+    return e;
 }
 
 cudaError_t run_sbuild(DeviceProgram const& prog, double* T, double* S, cudaStream_t stream) {
@@ -570,21 +680,14 @@ cudaError_t run_program(DeviceProgram const& prog, uint64_t in, uint64_t out, do
     bs.b[BUF_ABS] = 0;
     const int sms = device_sm_count();
     if (ev) cudaEventRecord(ev[0], stream);
-    const int occ = gemm_occupancy();
-    if (prog.n_t1) {
-        uint32_t grid = std::min<uint32_t>(prog.n_t1, uint32_t(sms) * occ);
-        gemm_f64_grouped<<<grid, NTHREADS, 0, stream>>>(prog.d_p1, prog.d_s1, prog.d_t1, prog.n_t1, bs);
-    }
+    launch_variant(prog.var1, prog.d_p1, prog.d_s1, prog.d_t1, prog.n_t1, bs, stream);
     if (ev) cudaEventRecord(ev[1], stream);
     if (prog.n_lines) {
         uint32_t grid = std::min<uint32_t>(prog.n_lines, uint32_t(sms) * 8);
         sbuild_lines<<<grid, 256, 0, stream>>>(prog.d_lines, prog.d_terms, prog.n_lines, S, T);
     }
     if (ev) cudaEventRecord(ev[2], stream);
-    if (prog.n_t3) {
-        uint32_t grid = std::min<uint32_t>(prog.n_t3, uint32_t(sms) * occ);
-        gemm_f64_grouped<<<grid, NTHREADS, 0, stream>>>(prog.d_p3, prog.d_s3, prog.d_t3, prog.n_t3, bs);
-    }
+    launch_variant(prog.var3, prog.d_p3, prog.d_s3, prog.d_t3, prog.n_t3, bs, stream);
     if (ev) cudaEventRecord(ev[3], stream);
     return cudaGetLastError();
 }

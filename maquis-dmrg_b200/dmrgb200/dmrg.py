@@ -192,7 +192,7 @@ class SweepLog:
     energies: list = field(default_factory=list)      # (sweep, site, energy, iterations, truncated weight)
     sweep_seconds: list = field(default_factory=list)
     hpsi_calls: int = 0
-    hpsi_ms: float = 0.0
+    solve_ms: float = 0.0   # device time of the eigen-solves
 
 
 class DeviceBackend:
@@ -223,7 +223,7 @@ class DeviceBackend:
         xd = E.to_device(psi.data, self.ctx.device)
         xo = self.torch.zeros_like(xd)
         energy, st = plan.solve(xd.data_ptr(), xo.data_ptr(), xd.numel(), tol=tol, max_iter=max_iter)
-        return energy, xo.cpu().numpy(), st.iterations, st.hpsi_ms
+        return energy, xo.cpu().numpy(), st.iterations, st.solve_ms
 
     def sync(self):
         self.torch.cuda.synchronize(self.ctx.device)
@@ -263,7 +263,7 @@ class TwoSiteDMRG:
         energy, xo, iters, ms = self.be.solve(self.p12, psi, self.W12[i], self.Lidx[i], self.Lbuf[i],
                                               self.Ridx[i + 2], self.Rbuf[i + 2], self.jd_tol, self.jd_maxiter)
         self.log.hpsi_calls += iters
-        self.log.hpsi_ms += ms
+        self.log.solve_ms += ms
         psi.data = xo
         res = split(psi, self.model.phys, self.model.phys, self.offs, self.m, self.cutoff, left_to_right)
         self.A[i], self.A[i + 1] = res.A, res.B

@@ -80,7 +80,8 @@ struct DevArray {
 struct GemmList {
     std::vector<DevProb> probs;
     std::vector<DevSeg> segs;
-    std::vector<DevTile> tiles;
+    std::vector<DevTile> tiles;        // 32 x 64 tiles, 16-deep K steps
+    std::vector<DevTile> tiles_small;  // 16 x 64 tiles, 8-deep K steps
 };
 
 struct DeviceProgram {
@@ -99,6 +100,9 @@ struct DeviceProgram {
     DevSLine* d_lines = nullptr;
     DevSTerm* d_terms = nullptr;
     uint32_t n_t1 = 0, n_t3 = 0, n_lines = 0;
+    DevTile* d_t1s = nullptr;  // small-tile lists
+    DevTile* d_t3s = nullptr;
+    uint32_t n_t1s = 0, n_t3s = 0;
     // grouped-GEMM variant per stage (autotuned by tune_program)
     int var1 = 0, var3 = 0;
     bool tuned = false;
@@ -132,10 +136,12 @@ struct GemmDev {
     DevSeg* s = nullptr;
     DevTile* t = nullptr;
     uint32_t n = 0;
+    DevTile* ts = nullptr;  // small-tile list
+    uint32_t ns = 0;
     int var = 0;  // grouped-GEMM variant
 };
-// grouped-GEMM variants (pipeline depth x CTAs per SM)
-constexpr int N_GEMM_VARIANTS = 4;
+// grouped-GEMM variants (tile shape x pipeline depth x CTAs per SM)
+constexpr int N_GEMM_VARIANTS = 8;
 const char* gemm_variant_name(int v);
 // Time every variant on the program's stage-1 and stage-3 tile lists (on the given
 // buffers, whose contents are overwritten as by an H psi) and keep the fastest per

@@ -19,9 +19,8 @@ namespace dmrgb200 {
 
 namespace {
 
-constexpr int BM = 32, BN = 64, BK = 16, NTHREADS = 128;
-constexpr int LDA_S = BM + 4, LDB_S = BN + 4;  // row strides = 8 words mod 32: conflict-free fragment loads
-constexpr int STAGES = 2;
+constexpr int BN = 64, NTHREADS = 128;
+constexpr int LDB_S = BN + 4;  // row strides = 8 words mod 32: conflict-free fragment loads
 
 __device__ __forceinline__ const double* op_base(Bases const& bs, DevOp const& op, uint32_t batch) {
     return reinterpret_cast<const double*>(base_of(bs, op.buf) + 8ull * (op.off + uint64_t(batch) * op.bstride));
@@ -49,22 +48,23 @@ struct TileCursor {
     uint32_t seg, k0;
 };
 
-// Issue the copies of one K tile (segment sg, rows k0..k0+BK) into stage buffers.
-__device__ __forceinline__ void load_tile(double (*As)[LDA_S], double (*Bs)[LDB_S], DevSeg const& sg,
+// Issue the copies of one K tile (segment sg, rows k0..k0+BK_) into stage buffers.
+template <int BM_, int BK_>
+__device__ __forceinline__ void load_tile(double (*As)[BM_ + 4], double (*Bs)[LDB_S], DevSeg const& sg,
                                           const double* A, const double* B, uint32_t m0, uint32_t n0, uint32_t M,
                                           uint32_t N, uint32_t k0, int tid) {
     const uint64_t lda = sg.A.ld, ldb = sg.B.ld;
     const uint32_t K = sg.K;
 #pragma unroll
-    for (int j = 0; j < (BM * BK) / NTHREADS; ++j) {
+    for (int j = 0; j < (BM_ * BK_) / NTHREADS; ++j) {
         int idx = tid + j * NTHREADS;
         int m, k;
         if (!sg.A.trans) {
-            m = idx % BM;
-            k = idx / BM;
+            m = idx % BM_;
+            k = idx / BM_;
         } else {
-            k = idx % BK;
-            m = idx / BK;
+            k = idx % BK_;
+            m = idx / BK_;
         }
         uint32_t gm = m0 + m, gk = k0 + k;
         bool ok = gm < M && gk < K;
@@ -72,12 +72,12 @@ __device__ __forceinline__ void load_tile(double (*As)[LDA_S], double (*Bs)[LDB_
         cp_async8(&As[k][m], src, ok);
     }
 #pragma unroll
-    for (int j = 0; j < (BN * BK) / NTHREADS; ++j) {
+    for (int j = 0; j < (BN * BK_) / NTHREADS; ++j) {
         int idx = tid + j * NTHREADS;
         int n, k;
         if (!sg.B.trans) {
-            k = idx % BK;
-            n = idx / BK;
+            k = idx % BK_;
+            n = idx / BK_;
         } else {
             n = idx % BN;
             k = idx / BN;
@@ -90,28 +90,29 @@ __device__ __forceinline__ void load_tile(double (*As)[LDA_S], double (*Bs)[LDB_
 }
 
 // Grouped, persistent FP64 GEMM over a tile list.  Each CTA owns whole output
-// tiles (BM x BN) and walks every K step of every segment of its problem; the
-// CTA's K steps over all its tiles form one stream, so the cp.async pipeline
-// (STAGES deep) keeps loading the next tile's operands while the current tile
-// finishes and stores.  4 warps in a 2 x 2 grid, warp tile 16 x 32, DMMA
-// m8n8k4.  A tile whose segments are all empty (one step, no copies) stores
-// zeros.
+// tiles (BM_ x 64) and walks every K step (BK_ deep) of every segment of its
+// problem; the CTA's K steps over all its tiles form one stream, so the
+// cp.async pipeline (STAGES deep) keeps loading the next tile's operands while
+// the current tile finishes and stores.  4 warps: 2 x 2 of 16 x 32 (BM_ = 32)
+// or 1 x 4 of 16 x 16 (BM_ = 16), DMMA m8n8k4.  A tile whose segments are all
+// empty (one step, no copies) stores zeros.
 struct LoadCursor {
     uint32_t ti, seg, seg_end, k0;
     bool valid;
 };
 
-template <int STAGES, int MINB>
+template <int BM_, int BK_, int STAGES, int MINB>
 __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb* __restrict__ probs,
                                                                    const DevSeg* __restrict__ segs,
                                                                    const DevTile* __restrict__ tiles, uint32_t n_tiles,
                                                                    Bases bases) {
-    __shared__ __align__(16) double As[STAGES][BK][LDA_S];
-    __shared__ __align__(16) double Bs[STAGES][BK][LDB_S];
+    constexpr int WARPS_M = BM_ / 16, WN = BN / (4 / WARPS_M), NJ = WN / 8;
+    __shared__ __align__(16) double As[STAGES][BK_][BM_ + 4];
+    __shared__ __align__(16) double Bs[STAGES][BK_][LDB_S];
 
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
-    const int wm = (warp >> 1) * 16, wn = (warp & 1) * 32;
+    const int wm = (warp % WARPS_M) * 16, wn = (warp / WARPS_M) * WN;
     const int g = lane >> 2, q = lane & 3;
 
     // ---- producer: walks (tile, segment, k0) and issues one K step per call ----
@@ -131,9 +132,9 @@ __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb
             const DevTile tl = tiles[L.ti];
             const DevProb& pr = probs[tl.prob];
             const DevSeg sg = segs[L.seg];
-            load_tile(As[slot], Bs[slot], sg, op_base(bases, sg.A, tl.batch), op_base(bases, sg.B, tl.batch), tl.m0,
-                      tl.n0, pr.M, pr.N, L.k0, tid);
-            L.k0 += BK;
+            load_tile<BM_, BK_>(As[slot], Bs[slot], sg, op_base(bases, sg.A, tl.batch),
+                                op_base(bases, sg.B, tl.batch), tl.m0, tl.n0, pr.M, pr.N, L.k0, tid);
+            L.k0 += BK_;
             if (L.k0 < sg.K) return;
             L.k0 = 0;
             ++L.seg;
@@ -151,11 +152,11 @@ __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb
         cp_async_commit();
     }
 
-    double acc[2][4][2];
+    double acc[2][NJ][2];
 #pragma unroll
     for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+        for (int j = 0; j < NJ; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
     // ---- consumer: tiles in the same order, nsteps K steps each ----
     int slot = 0;
@@ -167,16 +168,16 @@ __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb
             cp_async_wait<STAGES - 1>();
             __syncthreads();
 #pragma unroll
-            for (int kk = 0; kk < BK; kk += 4) {
-                double a[2], b[4];
+            for (int kk = 0; kk < BK_; kk += 4) {
+                double a[2], b[NJ];
 #pragma unroll
                 for (int i = 0; i < 2; ++i) a[i] = As[slot][kk + q][wm + i * 8 + g];
 #pragma unroll
-                for (int j = 0; j < 4; ++j) b[j] = Bs[slot][kk + q][wn + j * 8 + g];
+                for (int j = 0; j < NJ; ++j) b[j] = Bs[slot][kk + q][wn + j * 8 + g];
 #pragma unroll
                 for (int i = 0; i < 2; ++i)
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+                    for (int j = 0; j < NJ; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
             }
             __syncthreads();
             slot = (slot + 1) % STAGES;
@@ -193,7 +194,7 @@ __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb
 #pragma unroll
         for (int i = 0; i < 2; ++i)
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
+            for (int j = 0; j < NJ; ++j)
 #pragma unroll
                 for (int e = 0; e < 2; ++e) {
                     uint32_t r = tl.m0 + wm + i * 8 + g;
@@ -208,19 +209,46 @@ __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb
 // S build: S is tiled by cells (one per unit and MPO row block); a cell with a
 // line writes the alpha-weighted sum of its T sources (summed in term order like
 // the reference's axpy sequence), a cell without one writes zeros, so S needs
-// no separate clearing.
+// no separate clearing.  A line's terms are staged in shared memory first, so
+// the T loads of one element do not wait on each other.
+constexpr int SB_TERMS = 64;
 __global__ void __launch_bounds__(256) sbuild_lines(const DevSLine* __restrict__ lines,
                                                     const DevSTerm* __restrict__ terms, uint32_t n_lines,
                                                     double* __restrict__ S, const double* __restrict__ T) {
+    __shared__ double s_alpha[SB_TERMS];
+    __shared__ uint64_t s_base[SB_TERMS];
     for (uint32_t li = blockIdx.x; li < n_lines; li += gridDim.x) {
         const DevSLine L = lines[li];
+        const uint32_t nt = L.term_end - L.term_begin;
+        const bool staged = nt <= SB_TERMS;
+        __syncthreads();  // the previous line's readers are done
+        if (staged && threadIdx.x < nt) {
+            const DevSTerm tm = terms[L.term_begin + threadIdx.x];
+            s_alpha[threadIdx.x] = tm.alpha;
+            s_base[threadIdx.x] = tm.t_base;
+        }
+        __syncthreads();
         const uint64_t n = uint64_t(L.rows) * L.cols;
         for (uint64_t idx = threadIdx.x; idx < n; idx += blockDim.x) {
-            uint32_t i = uint32_t(idx % L.rows), c = uint32_t(idx / L.rows);
+            const uint32_t i = uint32_t(idx % L.rows), c = uint32_t(idx / L.rows);
+            const uint64_t off = i + uint64_t(c) * L.ld_t;
             double v = 0.0;
-            for (uint32_t t = L.term_begin; t < L.term_end; ++t) {
-                const DevSTerm tm = terms[t];
-                v += tm.alpha * T[tm.t_base + i + uint64_t(c) * L.ld_t];
+            if (staged) {
+                uint32_t t = 0;
+                for (; t + 4 <= nt; t += 4) {
+                    const double x0 = T[s_base[t] + off], x1 = T[s_base[t + 1] + off];
+                    const double x2 = T[s_base[t + 2] + off], x3 = T[s_base[t + 3] + off];
+                    v += s_alpha[t] * x0;
+                    v += s_alpha[t + 1] * x1;
+                    v += s_alpha[t + 2] * x2;
+                    v += s_alpha[t + 3] * x3;
+                }
+                for (; t < nt; ++t) v += s_alpha[t] * T[s_base[t] + off];
+            } else {
+                for (uint32_t t = L.term_begin; t < L.term_end; ++t) {
+                    const DevSTerm tm = terms[t];
+                    v += tm.alpha * T[tm.t_base + off];
+                }
             }
             S[L.s_base + i + uint64_t(c) * L.ld_s] = v;
         }
@@ -245,15 +273,22 @@ __global__ void __launch_bounds__(128) dmma_rate_loop(int iters, double* sink) {
 
 // --- host-side lowering ---------------------------------------------------------
 
+// tile classes: 0 = 32 x 64 tiles with 16-deep K steps, 1 = 16 x 64 with 8-deep steps
+constexpr int CLASS_BM[2] = {32, 16}, CLASS_BK[2] = {16, 8};
+
 void add_tiles(GemmList& gl, uint32_t prob, uint32_t nbatch) {
     DevProb const& p = gl.probs[prob];
-    uint32_t nsteps = 0;
-    for (uint32_t s = p.seg_begin; s < p.seg_end; ++s) nsteps += (gl.segs[s].K + BK - 1) / BK;
-    nsteps = std::max<uint32_t>(nsteps, 1);  // an empty problem: one step that issues no copies
-    for (uint32_t b = 0; b < nbatch; ++b)
-        for (uint32_t m0 = 0; m0 < std::max<uint32_t>(p.M, 1); m0 += BM)
-            for (uint32_t n0 = 0; n0 < std::max<uint32_t>(p.N, 1); n0 += BN)
-                gl.tiles.push_back(DevTile{prob, b, m0, n0, nsteps});
+    for (int c = 0; c < 2; ++c) {
+        const uint32_t bm = CLASS_BM[c], bk = CLASS_BK[c];
+        uint32_t nsteps = 0;
+        for (uint32_t s = p.seg_begin; s < p.seg_end; ++s) nsteps += (gl.segs[s].K + bk - 1) / bk;
+        nsteps = std::max<uint32_t>(nsteps, 1);  // an empty problem: one step that issues no copies
+        auto& out = c == 0 ? gl.tiles : gl.tiles_small;
+        for (uint32_t b = 0; b < nbatch; ++b)
+            for (uint32_t m0 = 0; m0 < std::max<uint32_t>(p.M, 1); m0 += bm)
+                for (uint32_t n0 = 0; n0 < std::max<uint32_t>(p.N, 1); n0 += BN)
+                    out.push_back(DevTile{prob, b, m0, n0, nsteps});
+    }
 }
 
 // Order tiles by decreasing K work so that the static round-robin of the
@@ -262,8 +297,9 @@ void sort_tiles(GemmList& gl) {
     std::vector<uint64_t> kwork(gl.probs.size(), 0);
     for (size_t p = 0; p < gl.probs.size(); ++p)
         for (uint32_t s = gl.probs[p].seg_begin; s < gl.probs[p].seg_end; ++s) kwork[p] += gl.segs[s].K;
-    std::stable_sort(gl.tiles.begin(), gl.tiles.end(),
-                     [&](DevTile const& a, DevTile const& b) { return kwork[a.prob] > kwork[b.prob]; });
+    for (auto* tl : {&gl.tiles, &gl.tiles_small})
+        std::stable_sort(tl->begin(), tl->end(),
+                         [&](DevTile const& a, DevTile const& b) { return kwork[a.prob] > kwork[b.prob]; });
 }
 
 DevOp op(uint16_t buf, uint64_t off, uint32_t ld, bool trans, uint64_t bstride = 0) {
@@ -486,6 +522,10 @@ cudaError_t upload_program(DeviceProgram& prog) {
     if ((e = up(prog.stage3.probs, &prog.d_p3)) != cudaSuccess) return e;
     if ((e = up(prog.stage3.segs, &prog.d_s3)) != cudaSuccess) return e;
     if ((e = up(prog.stage3.tiles, &prog.d_t3)) != cudaSuccess) return e;
+    if ((e = up(prog.stage1.tiles_small, &prog.d_t1s)) != cudaSuccess) return e;
+    if ((e = up(prog.stage3.tiles_small, &prog.d_t3s)) != cudaSuccess) return e;
+    prog.n_t1s = uint32_t(prog.stage1.tiles_small.size());
+    prog.n_t3s = uint32_t(prog.stage3.tiles_small.size());
     if ((e = up(prog.lines, &prog.d_lines)) != cudaSuccess) return e;
     if ((e = up(prog.terms, &prog.d_terms)) != cudaSuccess) return e;
     prog.n_t1 = uint32_t(prog.stage1.tiles.size());
@@ -501,6 +541,9 @@ void free_program(DeviceProgram& prog) {
     cudaFree(prog.d_p3);
     cudaFree(prog.d_s3);
     cudaFree(prog.d_t3);
+    cudaFree(prog.d_t1s);
+    cudaFree(prog.d_t3s);
+    prog.d_t1s = prog.d_t3s = nullptr;
     cudaFree(prog.d_lines);
     cudaFree(prog.d_terms);
     prog.d_p1 = nullptr;
@@ -541,7 +584,9 @@ cudaError_t upload_gemm(GemmList const& gl, GemmDev& d) {
     if ((e = up(gl.probs, &d.p)) != cudaSuccess) return e;
     if ((e = up(gl.segs, &d.s)) != cudaSuccess) return e;
     if ((e = up(gl.tiles, &d.t)) != cudaSuccess) return e;
+    if ((e = up(gl.tiles_small, &d.ts)) != cudaSuccess) return e;
     d.n = uint32_t(gl.tiles.size());
+    d.ns = uint32_t(gl.tiles_small.size());
     return cudaSuccess;
 }
 
@@ -549,6 +594,7 @@ void free_gemm(GemmDev& d) {
     cudaFree(d.p);
     cudaFree(d.s);
     cudaFree(d.t);
+    cudaFree(d.ts);
     d = GemmDev();
 }
 
@@ -559,12 +605,17 @@ using GemmKernel = void (*)(const DevProb*, const DevSeg*, const DevTile*, uint3
 struct GemmVariant {
     GemmKernel fn;
     const char* name;
+    int tile_class;  // which tile list it runs on
 };
 const GemmVariant kVariants[N_GEMM_VARIANTS] = {
-    {gemm_f64_grouped<2, 4>, "stages2_ctas4"},
-    {gemm_f64_grouped<3, 4>, "stages3_ctas4"},
-    {gemm_f64_grouped<2, 5>, "stages2_ctas5"},
-    {gemm_f64_grouped<3, 5>, "stages3_ctas5"},
+    {gemm_f64_grouped<32, 16, 2, 4>, "tile32x64_k16_stages2_ctas4", 0},
+    {gemm_f64_grouped<32, 16, 3, 4>, "tile32x64_k16_stages3_ctas4", 0},
+    {gemm_f64_grouped<32, 16, 2, 5>, "tile32x64_k16_stages2_ctas5", 0},
+    {gemm_f64_grouped<32, 16, 3, 5>, "tile32x64_k16_stages3_ctas5", 0},
+    {gemm_f64_grouped<16, 8, 3, 6>, "tile16x64_k8_stages3_ctas6", 1},
+    {gemm_f64_grouped<16, 8, 4, 6>, "tile16x64_k8_stages4_ctas6", 1},
+    {gemm_f64_grouped<16, 8, 3, 8>, "tile16x64_k8_stages3_ctas8", 1},
+    {gemm_f64_grouped<16, 8, 4, 8>, "tile16x64_k8_stages4_ctas8", 1},
 };
 
 int variant_occupancy(int v) {
@@ -577,10 +628,15 @@ int variant_occupancy(int v) {
     return occ[v];
 }
 
-cudaError_t launch_variant(int v, const DevProb* p, const DevSeg* sg, const DevTile* t, uint32_t n, Bases const& bs,
-                           cudaStream_t stream) {
+// t / n: the tile list of class 0; ts / ns: class 1 (NULL / 0 when absent: class 0 is used)
+cudaError_t launch_variant(int v, const DevProb* p, const DevSeg* sg, const DevTile* t, uint32_t n, const DevTile* ts,
+                           uint32_t ns, Bases const& bs, cudaStream_t stream) {
     if (!n) return cudaSuccess;
-    if (v < 0 || v >= N_GEMM_VARIANTS) v = 0;
+    if (v < 0 || v >= N_GEMM_VARIANTS || (kVariants[v].tile_class == 1 && !ts)) v = 0;
+    if (kVariants[v].tile_class == 1) {
+        t = ts;
+        n = ns;
+    }
     uint32_t grid = std::min<uint32_t>(n, uint32_t(device_sm_count()) * variant_occupancy(v));
     kVariants[v].fn<<<grid, NTHREADS, 0, stream>>>(p, sg, t, n, bs);
     return cudaGetLastError();
@@ -590,7 +646,7 @@ cudaError_t launch_variant(int v, const DevProb* p, const DevSeg* sg, const DevT
 const char* gemm_variant_name(int v) { return (v >= 0 && v < N_GEMM_VARIANTS) ? kVariants[v].name : "?"; }
 
 cudaError_t launch_gemm(GemmDev const& d, Bases const& bs, cudaStream_t stream) {
-    return launch_variant(d.var, d.p, d.s, d.t, d.n, bs, stream);
+    return launch_variant(d.var, d.p, d.s, d.t, d.n, d.ts, d.ns, bs, stream);
 }
 
 cudaError_t tune_program(DeviceProgram& prog, uint64_t in, uint64_t out, double* T, double* S, cudaStream_t stream) {
@@ -611,9 +667,11 @@ cudaError_t tune_program(DeviceProgram& prog, uint64_t in, uint64_t out, double*
         const DevSeg* s;
         const DevTile* t;
         uint32_t n;
+        const DevTile* ts;
+        uint32_t ns;
         int* var;
-    } stages[2] = {{prog.d_p1, prog.d_s1, prog.d_t1, prog.n_t1, &prog.var1},
-                   {prog.d_p3, prog.d_s3, prog.d_t3, prog.n_t3, &prog.var3}};
+    } stages[2] = {{prog.d_p1, prog.d_s1, prog.d_t1, prog.n_t1, prog.d_t1s, prog.n_t1s, &prog.var1},
+                   {prog.d_p3, prog.d_s3, prog.d_t3, prog.n_t3, prog.d_t3s, prog.n_t3s, &prog.var3}};
     // stage 1 writes T, read by nothing else here; stage 3 reads S: both are timed on the
     // plan's current scratch contents (the kernels' speed does not depend on the values)
     for (auto& st : stages) {
@@ -621,11 +679,11 @@ cudaError_t tune_program(DeviceProgram& prog, uint64_t in, uint64_t out, double*
         float best = 1e30f;
         int bv = 0;
         for (int v = 0; v < N_GEMM_VARIANTS && e == cudaSuccess; ++v) {
-            e = launch_variant(v, st.p, st.s, st.t, st.n, bs, stream);  // warm
+            e = launch_variant(v, st.p, st.s, st.t, st.n, st.ts, st.ns, bs, stream);  // warm
             float tot = 0.f;
             for (int r = 0; r < 2 && e == cudaSuccess; ++r) {
                 cudaEventRecord(e0, stream);
-                e = launch_variant(v, st.p, st.s, st.t, st.n, bs, stream);
+                e = launch_variant(v, st.p, st.s, st.t, st.n, st.ts, st.ns, bs, stream);
                 cudaEventRecord(e1, stream);
                 if (e == cudaSuccess) e = cudaEventSynchronize(e1);
                 float ms = 0.f;
@@ -680,14 +738,14 @@ cudaError_t run_program(DeviceProgram const& prog, uint64_t in, uint64_t out, do
     bs.b[BUF_ABS] = 0;
     const int sms = device_sm_count();
     if (ev) cudaEventRecord(ev[0], stream);
-    launch_variant(prog.var1, prog.d_p1, prog.d_s1, prog.d_t1, prog.n_t1, bs, stream);
+    launch_variant(prog.var1, prog.d_p1, prog.d_s1, prog.d_t1, prog.n_t1, prog.d_t1s, prog.n_t1s, bs, stream);
     if (ev) cudaEventRecord(ev[1], stream);
     if (prog.n_lines) {
         uint32_t grid = std::min<uint32_t>(prog.n_lines, uint32_t(sms) * 8);
         sbuild_lines<<<grid, 256, 0, stream>>>(prog.d_lines, prog.d_terms, prog.n_lines, S, T);
     }
     if (ev) cudaEventRecord(ev[2], stream);
-    launch_variant(prog.var3, prog.d_p3, prog.d_s3, prog.d_t3, prog.n_t3, bs, stream);
+    launch_variant(prog.var3, prog.d_p3, prog.d_s3, prog.d_t3, prog.n_t3, prog.d_t3s, prog.n_t3s, bs, stream);
     if (ev) cudaEventRecord(ev[3], stream);
     return cudaGetLastError();
 }

@@ -194,6 +194,37 @@ def sweep_workload(args):
     print(json.dumps(line), flush=True)
 
 
+def solve_workload(args):
+    """Jacobi-Davidson solves of the config-2 site problem (8 iterations each, tol 0 so
+    that every iteration runs), graph-captured and stepwise; one JSON line."""
+    import torch
+
+    from dmrgb200 import _capi as capi
+    from dmrgb200 import engine as E
+
+    ctx = E.Context(0)
+    model, bonds, tensors, i, psi = build_workload()
+    sp = E.SiteProblem(ctx, model, tensors, bonds, i)
+    xd = E.to_device(psi.data, 0)
+    xo = torch.zeros_like(xd)
+    out = {}
+    for name, mode in (("graph", capi.SOLVER_GRAPH), ("stepwise", capi.SOLVER_STEPWISE)):
+        sp.plan.set_solver(mode)
+        dev, wall = [], []
+        for k in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            e, st = sp.plan.solve(xd.data_ptr(), xo.data_ptr(), xd.numel(), tol=0.0, max_iter=8)
+            if k >= args.warmup:
+                wall.append((time.perf_counter() - t0) * 1e3)
+                dev.append(st.solve_ms)
+        out[name] = {"solve_ms_device": statistics.mean(dev), "solve_ms_wall": statistics.mean(wall),
+                     "iterations": int(st.iterations)}
+    hp = sp.plan.flops * 8 / 1e9
+    print(json.dumps({"metric": "Jacobi-Davidson solve time (ms, 8 H·psi)", "value": out["graph"]["solve_ms_wall"],
+                      "unit": "ms", "higher_is_better": False, "n_gpus": 1, "dtype": "f64", "data": "synthetic",
+                      "config": {"workload": WORKLOAD + "_jd8", "hpsi_gflop_per_solve": hp}, **out}), flush=True)
+
+
 def batched_workload(args):
     """64 independent site problems (32 Heisenberg U1, 32
     Fermi-Hubbard TwoU1, chains of 32 sites, middle two-site problem), bond
@@ -255,8 +286,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap.add_argument("--workload", default="hpsi", choices=["hpsi", "sweep", "batched"],
-                    help="hpsi: the headline H·psi line (default); sweep: config-1 sweeps; batched: config-5")
+    ap.add_argument("--workload", default="hpsi", choices=["hpsi", "sweep", "batched", "solve"],
+                    help="hpsi: the headline H·psi line (default); sweep: config-1 sweeps; batched: config-5; "
+                         "solve: Jacobi-Davidson solves of the config-2 site problem")
     ap.add_argument("--prec", default="fp64", choices=["fp64", "emulated"],
                     help="precision of the --profile steps")
     ap.add_argument("--profile", action="store_true",
@@ -269,6 +301,9 @@ def main():
         os._exit(0)
     if args.workload == "batched":
         batched_workload(args)
+        os._exit(0)
+    if args.workload == "solve":
+        solve_workload(args)
         os._exit(0)
 
     rank = int(os.environ.get("RANK", "0"))

@@ -128,6 +128,13 @@ void smallest_eigenpair(std::vector<double> A, int k, double& theta, std::vector
                 double apq = A[p + q * k];
                 if (apq == 0.0) continue;
                 double app = A[p + p * k], aqq = A[q + q * k];
+                // negligible against both diagonal entries: drop it (the sweep then ends
+                // with an exactly diagonal matrix instead of running out of sweeps)
+                if (std::fabs(app) + 100.0 * std::fabs(apq) == std::fabs(app) &&
+                    std::fabs(aqq) + 100.0 * std::fabs(apq) == std::fabs(aqq)) {
+                    A[p + q * k] = A[q + p * k] = 0.0;
+                    continue;
+                }
                 double tau = (aqq - app) / (2.0 * apq);
                 double t = (tau >= 0 ? 1.0 : -1.0) / (std::fabs(tau) + std::sqrt(1.0 + tau * tau));
                 double c = 1.0 / std::sqrt(1.0 + t * t), sn = t * c;

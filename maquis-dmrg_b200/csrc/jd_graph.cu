@@ -293,6 +293,13 @@ __global__ void __launch_bounds__(32) jd_ritz(JdArgs a) {
                 const double apq = A[p][q];
                 if (apq == 0.0) continue;
                 const double app = A[p][p], aqq = A[q][q];
+                // negligible against both diagonal entries: drop it (as in jd.cu)
+                if (fabs(app) + 100.0 * fabs(apq) == fabs(app) && fabs(aqq) + 100.0 * fabs(apq) == fabs(aqq)) {
+                    __syncwarp();
+                    if (r == 0) A[p][q] = A[q][p] = 0.0;
+                    __syncwarp();
+                    continue;
+                }
                 const double tau = (aqq - app) / (2.0 * apq);
                 const double tt = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
                 const double c = 1.0 / sqrt(1.0 + tt * tt), sn = tt * c;

@@ -225,6 +225,49 @@ def solve_workload(args):
                       "config": {"workload": WORKLOAD + "_jd8", "hpsi_gflop_per_solve": hp}, **out}), flush=True)
 
 
+def gemm_workload(args):
+    """The grouped DMMA GEMM on one regular 4096^3 problem, every variant, next to
+    torch's FP64 matmul (cuBLAS) and the calibrated DMMA peak; one JSON line."""
+    import ctypes as C
+
+    import torch
+
+    from dmrgb200 import _capi as capi
+
+    n = 4096
+    A = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    B = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    Cm = torch.empty(n, n, dtype=torch.float64, device="cuda")
+    flops = 2.0 * n ** 3
+    res = {}
+    for v in range(8):
+        name = capi.lib.dmrgb200_gemm_variant_name(v).decode()
+        ts = []
+        for k in range(args.warmup + 3):
+            t0 = time.perf_counter()
+            capi.check(capi.lib.dmrgb200_dgemm_f64(n, n, n, A.data_ptr(), n, B.data_ptr(), n, Cm.data_ptr(), n, v,
+                                                   None), "dgemm_f64")
+            if k >= args.warmup:
+                ts.append(time.perf_counter() - t0)
+        res[name] = flops / min(ts) / 1e12
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    for _ in range(args.warmup):
+        torch.matmul(A, B, out=Cm)
+    ev[0].record()
+    for _ in range(3):
+        torch.matmul(A, B, out=Cm)
+    ev[1].record()
+    torch.cuda.synchronize()
+    cublas = flops * 3 / (ev[0].elapsed_time(ev[1]) * 1e-3) / 1e12
+    peak = C.c_double()
+    capi.check(capi.lib.dmrgb200_calibrate(0, C.byref(peak)), "calibrate")
+    best = max(res.values())
+    print(json.dumps({"metric": "FP64 GEMM TFLOP/s, 4096^3", "value": best, "unit": "TFLOP/s",
+                      "higher_is_better": True, "n_gpus": 1, "dtype": "f64", "data": "synthetic",
+                      "config": {"workload": "dgemm_4096"}, "variants": res, "cublas_dgemm": cublas,
+                      "fp64_dmma_peak": peak.value}), flush=True)
+
+
 def batched_workload(args):
     """64 independent site problems (32 Heisenberg U1, 32
     Fermi-Hubbard TwoU1, chains of 32 sites, middle two-site problem), bond
@@ -286,9 +329,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap.add_argument("--workload", default="hpsi", choices=["hpsi", "sweep", "batched", "solve"],
+    ap.add_argument("--workload", default="hpsi", choices=["hpsi", "sweep", "batched", "solve", "gemm"],
                     help="hpsi: the headline H·psi line (default); sweep: config-1 sweeps; batched: config-5; "
-                         "solve: Jacobi-Davidson solves of the config-2 site problem")
+                         "solve: Jacobi-Davidson solves of the config-2 site problem; gemm: the DMMA kernel on "
+                         "a regular 4096^3 GEMM")
     ap.add_argument("--prec", default="fp64", choices=["fp64", "emulated"],
                     help="precision of the --profile steps")
     ap.add_argument("--profile", action="store_true",
@@ -304,6 +348,9 @@ def main():
         os._exit(0)
     if args.workload == "solve":
         solve_workload(args)
+        os._exit(0)
+    if args.workload == "gemm":
+        gemm_workload(args)
         os._exit(0)
 
     rank = int(os.environ.get("RANK", "0"))

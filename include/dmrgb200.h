@@ -260,6 +260,16 @@ double dmrgb200_wigner9j(int two_j1, int two_j2, int two_j3, int two_j4, int two
 void dmrgb200_set_coupling(int a, int b, int c, int d, int e, int f, int g, int h, int i, double init,
                            double couplings[4]);
 
+/* ---- plain FP64 GEMM on the grouped DMMA kernel --------------------------- */
+/* C = A * B (column-major FP64, A M x K, B K x N) with grouped-GEMM variant
+ * `variant` (0 .. 7, see dmrgb200_gemm_variant_name) as one problem; for
+ * measuring the H·psi kernel on regular shapes.  No counterpart in the
+ * reference (it calls BLAS).  Allocates its tile tables per call; returns
+ * after completion. */
+dmrgb200_status dmrgb200_dgemm_f64(uint32_t M, uint32_t N, uint32_t K, const double* A, uint64_t lda,
+                                   const double* B, uint64_t ldb, double* C, uint64_t ldc, int variant,
+                                   void* cuda_stream);
+
 /* ---- FP64 GEMM emulated on the INT8 tensor cores --------------------------- */
 /* C = A * B (column-major FP64, A M x K, B K x N) computed with `slices`
  * (2..8) signed 7-bit digit planes per operand on tcgen05 INT8 MMAs with exact

@@ -59,14 +59,21 @@ __global__ void __launch_bounds__(RED_THREADS) dot_partials(const double* const*
     }
 }
 
-// out[v] = sum_b partial[b * nvec + v] in block order
-__global__ void dot_finish(const double* __restrict__ partial, int nvec, int nblocks, double* __restrict__ out) {
-    int v = threadIdx.x;
-    if (v < nvec) {
-        double s = 0.0;
-        for (int b = 0; b < nblocks; ++b) s += partial[b * nvec + v];
-        out[v] = s;
+// out[v] = sum over blocks of partial[b * nvec + v]; one block per vector: every
+// thread sums a fixed subset of the blocks in order, then a fixed tree
+__global__ void __launch_bounds__(RED_THREADS) dot_finish(const double* __restrict__ partial, int nvec, int nblocks,
+                                                          double* __restrict__ out) {
+    __shared__ double red[RED_THREADS];
+    const int v = blockIdx.x;
+    double s = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += RED_THREADS) s += partial[b * nvec + v];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = RED_THREADS / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
     }
+    if (threadIdx.x == 0) out[v] = red[0];
 }
 
 // y += a * x with a = sign * num / den read from device memory (den == nullptr: a = sign * num)
@@ -218,7 +225,7 @@ extern "C" dmrgb200_status dmrgb200_solve(dmrgb200_plan_t plan, uint64_t n, cons
         cudaError_t r = cudaMemcpyAsync(w.ptrs, ptr_host.data(), xs.size() * sizeof(double*), cudaMemcpyHostToDevice, st);
         if (r != cudaSuccess) return r;
         dot_partials<<<RED_BLOCKS, RED_THREADS, 0, st>>>(w.ptrs, int(xs.size()), y, n, w.partial);
-        dot_finish<<<1, 64, 0, st>>>(w.partial, int(xs.size()), RED_BLOCKS, w.scal);
+        dot_finish<<<int(xs.size()), RED_THREADS, 0, st>>>(w.partial, int(xs.size()), RED_BLOCKS, w.scal);
         return cudaGetLastError();
     };
     auto fetch = [&](int k, double* out) -> cudaError_t {

@@ -97,11 +97,13 @@ __device__ bool arrive(JdState* st) {
     return last;
 }
 
-// sum of row r of the partial table over all blocks, in block order
+// sum of row r of the partial table over all blocks, by the whole (last) block:
+// every thread sums a fixed subset in order, then the fixed block tree; the
+// result is valid in thread 0
 __device__ double gather(JdArgs const& a, int r) {
     double s = 0.0;
-    for (unsigned b = 0; b < gridDim.x; ++b) s += __ldcg(a.partial + uint64_t(r) * gridDim.x + b);
-    return s;
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += JT) s += __ldcg(a.partial + uint64_t(r) * gridDim.x + b);
+    return block_sum(s);
 }
 
 __device__ void finish(JdArgs const& a) {
@@ -129,7 +131,8 @@ __global__ void __launch_bounds__(JT) jd_oo(JdArgs a, int i) {
     double p = slice_dot(a, Ov(a, i), Ov(a, i));
     if (threadIdx.x == 0) a.partial[blockIdx.x] = p;
     if (arrive(a.st)) {
-        if (threadIdx.x == 0) a.st->oo[i] = gather(a, 0);
+        const double g = gather(a, 0);
+        if (threadIdx.x == 0) a.st->oo[i] = g;
         finish(a);
     }
 }
@@ -149,7 +152,8 @@ __global__ void __launch_bounds__(JT) jd_proj(JdArgs a, int i, int target) {
     double p = slice_dot(a, Ov(a, i), x);
     if (threadIdx.x == 0) a.partial[blockIdx.x] = p;
     if (arrive(a.st)) {
-        if (threadIdx.x == 0) a.st->pc[i] = gather(a, 0) / a.st->oo[i];
+        const double g = gather(a, 0);
+        if (threadIdx.x == 0) a.st->pc[i] = g / a.st->oo[i];
         finish(a);
     }
 }
@@ -166,7 +170,8 @@ __global__ void __launch_bounds__(JT) jd_tau(JdArgs a) {
     double p = slice_dot(a, Tv(a), Tv(a));
     if (threadIdx.x == 0) a.partial[blockIdx.x] = p;
     if (arrive(a.st)) {
-        if (threadIdx.x == 0) a.st->tau = sqrt(gather(a, 0));
+        const double g = gather(a, 0);
+        if (threadIdx.x == 0) a.st->tau = sqrt(g);
         finish(a);
     }
 }
@@ -184,7 +189,8 @@ __global__ void __launch_bounds__(JT) jd_mgs(JdArgs a, int j, int pass) {
     double p = slice_dot(a, V(a, j), t);
     if (threadIdx.x == 0) a.partial[blockIdx.x] = p;
     if (arrive(st)) {
-        if (threadIdx.x == 0) st->c[pass][j] = gather(a, 0);
+        const double g = gather(a, 0);
+        if (threadIdx.x == 0) st->c[pass][j] = g;
         finish(a);
     }
 }
@@ -204,8 +210,9 @@ __global__ void __launch_bounds__(JT) jd_mgs_close(JdArgs a, int pass) {
     double p = slice_dot(a, t, t);
     if (threadIdx.x == 0) a.partial[blockIdx.x] = p;
     if (arrive(st)) {
+        const double g = gather(a, 0);
         if (threadIdx.x == 0) {
-            st->tn = sqrt(gather(a, 0));
+            st->tn = sqrt(g);
             st->refine = (it > 0 && st->tn < 0.25 * st->tau) ? 1 : 0;
         }
         finish(a);
@@ -217,9 +224,10 @@ __global__ void __launch_bounds__(JT) jd_tnorm(JdArgs a) {
     double p = slice_dot(a, Tv(a), Tv(a));
     if (threadIdx.x == 0) a.partial[blockIdx.x] = p;
     if (arrive(a.st)) {
+        const double g = gather(a, 0);
         if (threadIdx.x == 0) {
             JdState* st = a.st;
-            st->tn = sqrt(gather(a, 0));
+            st->tn = sqrt(g);
             if (!(st->tn > 0.0)) {
                 st->status = 1;
                 st->done = 1;
@@ -254,7 +262,10 @@ __global__ void __launch_bounds__(JT) jd_mcol(JdArgs a) {
         if (threadIdx.x == 0) a.partial[uint64_t(j) * gridDim.x + blockIdx.x] = p;
     }
     if (arrive(st)) {
-        if (threadIdx.x <= unsigned(it)) st->M[threadIdx.x + it * MAXK] = gather(a, int(threadIdx.x));
+        for (int j = 0; j <= it; ++j) {
+            const double g = gather(a, j);
+            if (threadIdx.x == 0) st->M[j + it * MAXK] = g;
+        }
         finish(a);
     }
 }
@@ -371,9 +382,9 @@ __global__ void __launch_bounds__(JT) jd_residual(JdArgs a) {
         a.partial[2 * gridDim.x + blockIdx.x] = uu;
     }
     if (arrive(st)) {
+        const double rrs = gather(a, 0), rus = gather(a, 1), uus = gather(a, 2);
         if (threadIdx.x == 0) {
-            st->rnorm = sqrt(gather(a, 0));
-            const double rus = gather(a, 1), uus = gather(a, 2);
+            st->rnorm = sqrt(rrs);
             st->corr = rus / uus;
             st->iter += 1;
             const bool conv = st->rnorm <= a.tol * fabs(theta) || st->rnorm < a.tol;

@@ -12,7 +12,9 @@
 #include <algorithm>
 #include <cstdio>
 #include <numeric>
+#include <string>
 
+#include "../../include/dmrgb200.h"
 #include "device.hpp"
 
 namespace dmrgb200 {
@@ -751,3 +753,47 @@ cudaError_t run_program(DeviceProgram const& prog, uint64_t in, uint64_t out, do
 }
 
 }  // namespace dmrgb200
+
+using namespace dmrgb200;
+
+namespace dmrgb200 {
+dmrgb200_status noalloc_fail(dmrgb200_status s, std::string const& msg);
+}
+
+extern "C" dmrgb200_status dmrgb200_dgemm_f64(uint32_t M, uint32_t N, uint32_t K, const double* A, uint64_t lda,
+                                              const double* B, uint64_t ldb, double* C, uint64_t ldc, int variant,
+                                              void* cuda_stream) {
+    if (!A || !B || !C) return noalloc_fail(DMRGB200_INVALID_ARGUMENT, "null argument");
+    if (lda < M || ldb < K || ldc < M) return noalloc_fail(DMRGB200_INVALID_ARGUMENT, "leading dimension too small");
+    if (variant < 0 || variant >= N_GEMM_VARIANTS) return noalloc_fail(DMRGB200_INVALID_ARGUMENT, "unknown variant");
+    if (lda > UINT32_MAX || ldb > UINT32_MAX || ldc > UINT32_MAX)
+        return noalloc_fail(DMRGB200_INVALID_ARGUMENT, "leading dimension above 2^32");
+    cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+    GemmList gl;
+    DevProb pr{};
+    pr.M = M;
+    pr.N = N;
+    pr.C = DevOp{reinterpret_cast<uint64_t>(C) / 8, 0, uint32_t(ldc), uint16_t(BUF_ABS), 0};
+    pr.seg_begin = 0;
+    pr.seg_end = 1;
+    DevSeg sg{};
+    sg.A = DevOp{reinterpret_cast<uint64_t>(A) / 8, 0, uint32_t(lda), uint16_t(BUF_ABS), 0};
+    sg.B = DevOp{reinterpret_cast<uint64_t>(B) / 8, 0, uint32_t(ldb), uint16_t(BUF_ABS), 0};
+    sg.K = K;
+    gl.probs.push_back(pr);
+    gl.segs.push_back(sg);
+    add_tiles(gl, 0, 1);
+    GemmDev d;
+    cudaError_t e = upload_gemm(gl, d);
+    if (e == cudaSuccess) {
+        d.var = variant;
+        e = launch_gemm(d, Bases{}, st);
+    }
+    cudaError_t e2 = cudaStreamSynchronize(st);
+    free_gemm(d);
+    if (e == cudaSuccess) e = e2;
+    if (e != cudaSuccess)
+        return noalloc_fail(e == cudaErrorMemoryAllocation ? DMRGB200_OUT_OF_MEMORY : DMRGB200_DEVICE_ERROR,
+                            std::string("FP64 GEMM: ") + cudaGetErrorString(e));
+    return DMRGB200_OK;
+}

@@ -19,8 +19,8 @@ def test_dgemm_f64_matches_torch(variant, M, N, K, pad):
     assert torch.cuda.is_available()
     g = torch.Generator(device="cuda").manual_seed(M * 131 + N * 7 + K + variant)
     lda, ldb, ldc = M + pad, K + pad, M + 2 * pad
-    A = torch.randn(max(K, 1) * lda, dtype=torch.float64, device="cuda", generator=g)
-    B = torch.randn(max(N, 1) * ldb, dtype=torch.float64, device="cuda", generator=g)
+    A = torch.randn(max(K * lda, 1), dtype=torch.float64, device="cuda", generator=g)
+    B = torch.randn(max(N * ldb, 1), dtype=torch.float64, device="cuda", generator=g)
     Cm = torch.full((N * ldc,), float("nan"), dtype=torch.float64, device="cuda")
     capi.check(capi.lib.dmrgb200_dgemm_f64(M, N, K, A.data_ptr(), lda, B.data_ptr(), ldb, Cm.data_ptr(), ldc,
                                            variant, None), "dgemm_f64")

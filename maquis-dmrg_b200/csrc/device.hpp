@@ -77,11 +77,21 @@ struct DevArray {
     size_t n = 0;
 };
 
+// tile classes of the grouped GEMM: 0 = 32 x 64 tiles with 16-deep K steps,
+// 1 = 16 x 64 with 8-deep steps, 2 = 64 x 64 with 16-deep steps
+constexpr int N_TILE_CLASSES = 3;
+
 struct GemmList {
     std::vector<DevProb> probs;
     std::vector<DevSeg> segs;
-    std::vector<DevTile> tiles;        // 32 x 64 tiles, 16-deep K steps
-    std::vector<DevTile> tiles_small;  // 16 x 64 tiles, 8-deep K steps
+    std::vector<DevTile> tiles;                        // class 0
+    std::vector<DevTile> tiles_cls[N_TILE_CLASSES];    // classes 1.. (entry 0 unused)
+};
+
+// device tile lists of the classes above 0
+struct TileLists {
+    DevTile* t[N_TILE_CLASSES] = {};
+    uint32_t n[N_TILE_CLASSES] = {};
 };
 
 struct DeviceProgram {
@@ -100,9 +110,7 @@ struct DeviceProgram {
     DevSLine* d_lines = nullptr;
     DevSTerm* d_terms = nullptr;
     uint32_t n_t1 = 0, n_t3 = 0, n_lines = 0;
-    DevTile* d_t1s = nullptr;  // small-tile lists
-    DevTile* d_t3s = nullptr;
-    uint32_t n_t1s = 0, n_t3s = 0;
+    TileLists x1, x3;  // tile lists of the other classes
     // grouped-GEMM variant per stage (autotuned by tune_program)
     int var1 = 0, var3 = 0;
     bool tuned = false;
@@ -136,12 +144,11 @@ struct GemmDev {
     DevSeg* s = nullptr;
     DevTile* t = nullptr;
     uint32_t n = 0;
-    DevTile* ts = nullptr;  // small-tile list
-    uint32_t ns = 0;
+    TileLists x;  // tile lists of the other classes
     int var = 0;  // grouped-GEMM variant
 };
 // grouped-GEMM variants (tile shape x pipeline depth x CTAs per SM)
-constexpr int N_GEMM_VARIANTS = 8;
+constexpr int N_GEMM_VARIANTS = 10;
 const char* gemm_variant_name(int v);
 // Time every variant on the program's stage-1 and stage-3 tile lists (on the given
 // buffers, whose contents are overwritten as by an H psi) and keep the fastest per

@@ -95,8 +95,8 @@ __device__ __forceinline__ void load_tile(double (*As)[BM_ + 4], double (*Bs)[LD
 // tiles (BM_ x 64) and walks every K step (BK_ deep) of every segment of its
 // problem; the CTA's K steps over all its tiles form one stream, so the
 // cp.async pipeline (STAGES deep) keeps loading the next tile's operands while
-// the current tile finishes and stores.  4 warps: 2 x 2 of 16 x 32 (BM_ = 32)
-// or 1 x 4 of 16 x 16 (BM_ = 16), DMMA m8n8k4.  A tile whose segments are all
+// the current tile finishes and stores.  4 warps: 2 x 2 of (BM_/2) x 32 (BM_ =
+// 32, 64) or 1 x 4 of 16 x 16 (BM_ = 16), DMMA m8n8k4.  A tile whose segments are all
 // empty (one step, no copies) stores zeros.
 struct LoadCursor {
     uint32_t ti, seg, seg_end, k0;
@@ -108,13 +108,15 @@ __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb
                                                                    const DevSeg* __restrict__ segs,
                                                                    const DevTile* __restrict__ tiles, uint32_t n_tiles,
                                                                    Bases bases) {
-    constexpr int WARPS_M = BM_ / 16, WN = BN / (4 / WARPS_M), NJ = WN / 8;
+    // warps: 2 x 2 for BM_ >= 32 (warp tiles BM_/2 x 32), 1 x 4 for BM_ = 16 (16 x 16)
+    constexpr int WARPS_M = BM_ >= 32 ? 2 : 1, WM = BM_ / WARPS_M, MI = WM / 8;
+    constexpr int WN = BN / (4 / WARPS_M), NJ = WN / 8;
     __shared__ __align__(16) double As[STAGES][BK_][BM_ + 4];
     __shared__ __align__(16) double Bs[STAGES][BK_][LDB_S];
 
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
-    const int wm = (warp % WARPS_M) * 16, wn = (warp / WARPS_M) * WN;
+    const int wm = (warp % WARPS_M) * WM, wn = (warp / WARPS_M) * WN;
     const int g = lane >> 2, q = lane & 3;
 
     // ---- producer: walks (tile, segment, k0) and issues one K step per call ----
@@ -154,9 +156,9 @@ __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb
         cp_async_commit();
     }
 
-    double acc[2][NJ][2];
+    double acc[MI][NJ][2];
 #pragma unroll
-    for (int i = 0; i < 2; ++i)
+    for (int i = 0; i < MI; ++i)
 #pragma unroll
         for (int j = 0; j < NJ; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
@@ -171,13 +173,13 @@ __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb
             __syncthreads();
 #pragma unroll
             for (int kk = 0; kk < BK_; kk += 4) {
-                double a[2], b[NJ];
+                double a[MI], b[NJ];
 #pragma unroll
-                for (int i = 0; i < 2; ++i) a[i] = As[slot][kk + q][wm + i * 8 + g];
+                for (int i = 0; i < MI; ++i) a[i] = As[slot][kk + q][wm + i * 8 + g];
 #pragma unroll
                 for (int j = 0; j < NJ; ++j) b[j] = Bs[slot][kk + q][wn + j * 8 + g];
 #pragma unroll
-                for (int i = 0; i < 2; ++i)
+                for (int i = 0; i < MI; ++i)
 #pragma unroll
                     for (int j = 0; j < NJ; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
             }
@@ -194,7 +196,7 @@ __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb
         double* C = const_cast<double*>(op_base(bases, pr.C, tl.batch));
         const uint64_t ldc = pr.C.ld;
 #pragma unroll
-        for (int i = 0; i < 2; ++i)
+        for (int i = 0; i < MI; ++i)
 #pragma unroll
             for (int j = 0; j < NJ; ++j)
 #pragma unroll
@@ -276,16 +278,16 @@ __global__ void __launch_bounds__(128) dmma_rate_loop(int iters, double* sink) {
 // --- host-side lowering ---------------------------------------------------------
 
 // tile classes: 0 = 32 x 64 tiles with 16-deep K steps, 1 = 16 x 64 with 8-deep steps
-constexpr int CLASS_BM[2] = {32, 16}, CLASS_BK[2] = {16, 8};
+constexpr int CLASS_BM[N_TILE_CLASSES] = {32, 16, 64}, CLASS_BK[N_TILE_CLASSES] = {16, 8, 16};
 
 void add_tiles(GemmList& gl, uint32_t prob, uint32_t nbatch) {
     DevProb const& p = gl.probs[prob];
-    for (int c = 0; c < 2; ++c) {
+    for (int c = 0; c < N_TILE_CLASSES; ++c) {
         const uint32_t bm = CLASS_BM[c], bk = CLASS_BK[c];
         uint32_t nsteps = 0;
         for (uint32_t s = p.seg_begin; s < p.seg_end; ++s) nsteps += (gl.segs[s].K + bk - 1) / bk;
         nsteps = std::max<uint32_t>(nsteps, 1);  // an empty problem: one step that issues no copies
-        auto& out = c == 0 ? gl.tiles : gl.tiles_small;
+        auto& out = c == 0 ? gl.tiles : gl.tiles_cls[c];
         for (uint32_t b = 0; b < nbatch; ++b)
             for (uint32_t m0 = 0; m0 < std::max<uint32_t>(p.M, 1); m0 += bm)
                 for (uint32_t n0 = 0; n0 < std::max<uint32_t>(p.N, 1); n0 += BN)
@@ -299,7 +301,7 @@ void sort_tiles(GemmList& gl) {
     std::vector<uint64_t> kwork(gl.probs.size(), 0);
     for (size_t p = 0; p < gl.probs.size(); ++p)
         for (uint32_t s = gl.probs[p].seg_begin; s < gl.probs[p].seg_end; ++s) kwork[p] += gl.segs[s].K;
-    for (auto* tl : {&gl.tiles, &gl.tiles_small})
+    for (auto* tl : {&gl.tiles, &gl.tiles_cls[1], &gl.tiles_cls[2]})
         std::stable_sort(tl->begin(), tl->end(),
                          [&](DevTile const& a, DevTile const& b) { return kwork[a.prob] > kwork[b.prob]; });
 }
@@ -524,10 +526,12 @@ cudaError_t upload_program(DeviceProgram& prog) {
     if ((e = up(prog.stage3.probs, &prog.d_p3)) != cudaSuccess) return e;
     if ((e = up(prog.stage3.segs, &prog.d_s3)) != cudaSuccess) return e;
     if ((e = up(prog.stage3.tiles, &prog.d_t3)) != cudaSuccess) return e;
-    if ((e = up(prog.stage1.tiles_small, &prog.d_t1s)) != cudaSuccess) return e;
-    if ((e = up(prog.stage3.tiles_small, &prog.d_t3s)) != cudaSuccess) return e;
-    prog.n_t1s = uint32_t(prog.stage1.tiles_small.size());
-    prog.n_t3s = uint32_t(prog.stage3.tiles_small.size());
+    for (int c = 1; c < N_TILE_CLASSES; ++c) {
+        if ((e = up(prog.stage1.tiles_cls[c], &prog.x1.t[c])) != cudaSuccess) return e;
+        if ((e = up(prog.stage3.tiles_cls[c], &prog.x3.t[c])) != cudaSuccess) return e;
+        prog.x1.n[c] = uint32_t(prog.stage1.tiles_cls[c].size());
+        prog.x3.n[c] = uint32_t(prog.stage3.tiles_cls[c].size());
+    }
     if ((e = up(prog.lines, &prog.d_lines)) != cudaSuccess) return e;
     if ((e = up(prog.terms, &prog.d_terms)) != cudaSuccess) return e;
     prog.n_t1 = uint32_t(prog.stage1.tiles.size());
@@ -543,9 +547,12 @@ void free_program(DeviceProgram& prog) {
     cudaFree(prog.d_p3);
     cudaFree(prog.d_s3);
     cudaFree(prog.d_t3);
-    cudaFree(prog.d_t1s);
-    cudaFree(prog.d_t3s);
-    prog.d_t1s = prog.d_t3s = nullptr;
+    for (int c = 1; c < N_TILE_CLASSES; ++c) {
+        cudaFree(prog.x1.t[c]);
+        cudaFree(prog.x3.t[c]);
+    }
+    prog.x1 = TileLists();
+    prog.x3 = TileLists();
     cudaFree(prog.d_lines);
     cudaFree(prog.d_terms);
     prog.d_p1 = nullptr;
@@ -586,9 +593,12 @@ cudaError_t upload_gemm(GemmList const& gl, GemmDev& d) {
     if ((e = up(gl.probs, &d.p)) != cudaSuccess) return e;
     if ((e = up(gl.segs, &d.s)) != cudaSuccess) return e;
     if ((e = up(gl.tiles, &d.t)) != cudaSuccess) return e;
-    if ((e = up(gl.tiles_small, &d.ts)) != cudaSuccess) return e;
+    for (int c = 1; c < N_TILE_CLASSES; ++c) {
+        if ((e = up(gl.tiles_cls[c], &d.x.t[c])) != cudaSuccess) return e;
+        d.x.n[c] = uint32_t(gl.tiles_cls[c].size());
+    }
     d.n = uint32_t(gl.tiles.size());
-    d.ns = uint32_t(gl.tiles_small.size());
+
     return cudaSuccess;
 }
 
@@ -596,7 +606,7 @@ void free_gemm(GemmDev& d) {
     cudaFree(d.p);
     cudaFree(d.s);
     cudaFree(d.t);
-    cudaFree(d.ts);
+    for (int c = 1; c < N_TILE_CLASSES; ++c) cudaFree(d.x.t[c]);
     d = GemmDev();
 }
 
@@ -618,6 +628,8 @@ const GemmVariant kVariants[N_GEMM_VARIANTS] = {
     {gemm_f64_grouped<16, 8, 4, 6>, "tile16x64_k8_stages4_ctas6", 1},
     {gemm_f64_grouped<16, 8, 3, 8>, "tile16x64_k8_stages3_ctas8", 1},
     {gemm_f64_grouped<16, 8, 4, 8>, "tile16x64_k8_stages4_ctas8", 1},
+    {gemm_f64_grouped<64, 16, 2, 3>, "tile64x64_k16_stages2_ctas3", 2},
+    {gemm_f64_grouped<64, 16, 2, 2>, "tile64x64_k16_stages2_ctas2", 2},
 };
 
 int variant_occupancy(int v) {
@@ -630,14 +642,17 @@ int variant_occupancy(int v) {
     return occ[v];
 }
 
-// t / n: the tile list of class 0; ts / ns: class 1 (NULL / 0 when absent: class 0 is used)
-cudaError_t launch_variant(int v, const DevProb* p, const DevSeg* sg, const DevTile* t, uint32_t n, const DevTile* ts,
-                           uint32_t ns, Bases const& bs, cudaStream_t stream) {
+// t / n: the tile list of class 0; x: the other classes (a variant whose list is
+// absent falls back to variant 0)
+cudaError_t launch_variant(int v, const DevProb* p, const DevSeg* sg, const DevTile* t, uint32_t n,
+                           TileLists const& x, Bases const& bs, cudaStream_t stream) {
     if (!n) return cudaSuccess;
-    if (v < 0 || v >= N_GEMM_VARIANTS || (kVariants[v].tile_class == 1 && !ts)) v = 0;
-    if (kVariants[v].tile_class == 1) {
-        t = ts;
-        n = ns;
+    if (v < 0 || v >= N_GEMM_VARIANTS) v = 0;
+    const int c = kVariants[v].tile_class;
+    if (c > 0 && !x.t[c]) v = 0;
+    if (kVariants[v].tile_class > 0) {
+        t = x.t[c];
+        n = x.n[c];
     }
     uint32_t grid = std::min<uint32_t>(n, uint32_t(device_sm_count()) * variant_occupancy(v));
     kVariants[v].fn<<<grid, NTHREADS, 0, stream>>>(p, sg, t, n, bs);
@@ -648,7 +663,7 @@ cudaError_t launch_variant(int v, const DevProb* p, const DevSeg* sg, const DevT
 const char* gemm_variant_name(int v) { return (v >= 0 && v < N_GEMM_VARIANTS) ? kVariants[v].name : "?"; }
 
 cudaError_t launch_gemm(GemmDev const& d, Bases const& bs, cudaStream_t stream) {
-    return launch_variant(d.var, d.p, d.s, d.t, d.n, d.ts, d.ns, bs, stream);
+    return launch_variant(d.var, d.p, d.s, d.t, d.n, d.x, bs, stream);
 }
 
 cudaError_t tune_program(DeviceProgram& prog, uint64_t in, uint64_t out, double* T, double* S, cudaStream_t stream) {
@@ -669,11 +684,10 @@ cudaError_t tune_program(DeviceProgram& prog, uint64_t in, uint64_t out, double*
         const DevSeg* s;
         const DevTile* t;
         uint32_t n;
-        const DevTile* ts;
-        uint32_t ns;
+        TileLists x;
         int* var;
-    } stages[2] = {{prog.d_p1, prog.d_s1, prog.d_t1, prog.n_t1, prog.d_t1s, prog.n_t1s, &prog.var1},
-                   {prog.d_p3, prog.d_s3, prog.d_t3, prog.n_t3, prog.d_t3s, prog.n_t3s, &prog.var3}};
+    } stages[2] = {{prog.d_p1, prog.d_s1, prog.d_t1, prog.n_t1, prog.x1, &prog.var1},
+                   {prog.d_p3, prog.d_s3, prog.d_t3, prog.n_t3, prog.x3, &prog.var3}};
     // stage 1 writes T, read by nothing else here; stage 3 reads S: both are timed on the
     // plan's current scratch contents (the kernels' speed does not depend on the values)
     for (auto& st : stages) {
@@ -681,11 +695,11 @@ cudaError_t tune_program(DeviceProgram& prog, uint64_t in, uint64_t out, double*
         float best = 1e30f;
         int bv = 0;
         for (int v = 0; v < N_GEMM_VARIANTS && e == cudaSuccess; ++v) {
-            e = launch_variant(v, st.p, st.s, st.t, st.n, st.ts, st.ns, bs, stream);  // warm
+            e = launch_variant(v, st.p, st.s, st.t, st.n, st.x, bs, stream);  // warm
             float tot = 0.f;
             for (int r = 0; r < 2 && e == cudaSuccess; ++r) {
                 cudaEventRecord(e0, stream);
-                e = launch_variant(v, st.p, st.s, st.t, st.n, st.ts, st.ns, bs, stream);
+                e = launch_variant(v, st.p, st.s, st.t, st.n, st.x, bs, stream);
                 cudaEventRecord(e1, stream);
                 if (e == cudaSuccess) e = cudaEventSynchronize(e1);
                 float ms = 0.f;
@@ -740,14 +754,14 @@ cudaError_t run_program(DeviceProgram const& prog, uint64_t in, uint64_t out, do
     bs.b[BUF_ABS] = 0;
     const int sms = device_sm_count();
     if (ev) cudaEventRecord(ev[0], stream);
-    launch_variant(prog.var1, prog.d_p1, prog.d_s1, prog.d_t1, prog.n_t1, prog.d_t1s, prog.n_t1s, bs, stream);
+    launch_variant(prog.var1, prog.d_p1, prog.d_s1, prog.d_t1, prog.n_t1, prog.x1, bs, stream);
     if (ev) cudaEventRecord(ev[1], stream);
     if (prog.n_lines) {
         uint32_t grid = std::min<uint32_t>(prog.n_lines, uint32_t(sms) * 8);
         sbuild_lines<<<grid, 256, 0, stream>>>(prog.d_lines, prog.d_terms, prog.n_lines, S, T);
     }
     if (ev) cudaEventRecord(ev[2], stream);
-    launch_variant(prog.var3, prog.d_p3, prog.d_s3, prog.d_t3, prog.n_t3, prog.d_t3s, prog.n_t3s, bs, stream);
+    launch_variant(prog.var3, prog.d_p3, prog.d_s3, prog.d_t3, prog.n_t3, prog.x3, bs, stream);
     if (ev) cudaEventRecord(ev[3], stream);
     return cudaGetLastError();
 }

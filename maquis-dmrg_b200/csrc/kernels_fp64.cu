@@ -50,6 +50,13 @@ struct TileCursor {
     uint32_t seg, k0;
 };
 
+// Shared-memory column swizzle of the operand tiles: row k stores column c at
+// c ^ ((k >> 2) & 3).  With row pitches of 8 words mod 32, copies in which
+// consecutive threads take consecutive k (the coalesced order for K-contiguous
+// operands) then hit distinct banks, and the fragment loads of one 4-deep K
+// step (one XOR constant) stay conflict-free.
+__device__ __forceinline__ int swz(int k) { return (k >> 2) & 3; }
+
 // Issue the copies of one K tile (segment sg, rows k0..k0+BK_) into stage buffers.
 template <int BM_, int BK_>
 __device__ __forceinline__ void load_tile(double (*As)[BM_ + 4], double (*Bs)[LDB_S], DevSeg const& sg,
@@ -71,7 +78,7 @@ __device__ __forceinline__ void load_tile(double (*As)[BM_ + 4], double (*Bs)[LD
         uint32_t gm = m0 + m, gk = k0 + k;
         bool ok = gm < M && gk < K;
         const double* src = ok ? (sg.A.trans ? A + gk + gm * lda : A + gm + gk * lda) : A;
-        cp_async8(&As[k][m], src, ok);
+        cp_async8(&As[k][m ^ swz(k)], src, ok);
     }
 #pragma unroll
     for (int j = 0; j < (BN * BK_) / NTHREADS; ++j) {
@@ -87,7 +94,7 @@ __device__ __forceinline__ void load_tile(double (*As)[BM_ + 4], double (*Bs)[LD
         uint32_t gn = n0 + n, gk = k0 + k;
         bool ok = gn < N && gk < K;
         const double* src = ok ? (sg.B.trans ? B + gn + gk * ldb : B + gk + gn * ldb) : B;
-        cp_async8(&Bs[k][n], src, ok);
+        cp_async8(&Bs[k][n ^ swz(k)], src, ok);
     }
 }
 
@@ -175,9 +182,9 @@ __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb
             for (int kk = 0; kk < BK_; kk += 4) {
                 double a[MI], b[NJ];
 #pragma unroll
-                for (int i = 0; i < MI; ++i) a[i] = As[slot][kk + q][wm + i * 8 + g];
+                for (int i = 0; i < MI; ++i) a[i] = As[slot][kk + q][(wm + i * 8 + g) ^ (kk >> 2)];
 #pragma unroll
-                for (int j = 0; j < NJ; ++j) b[j] = Bs[slot][kk + q][wn + j * 8 + g];
+                for (int j = 0; j < NJ; ++j) b[j] = Bs[slot][kk + q][(wn + j * 8 + g) ^ (kk >> 2)];
 #pragma unroll
                 for (int i = 0; i < MI; ++i)
 #pragma unroll

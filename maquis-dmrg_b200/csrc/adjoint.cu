@@ -249,6 +249,7 @@ cudaError_t run_adjoint(DeviceProgram const& fwd, AdjointProgram const& a, uint6
         f1.t = fwd.d_t1;
         f1.n = fwd.n_t1;
         f1.x = fwd.x1;
+        f1.r = fwd.d_r1;
         f1.var = fwd.var1;
         if ((e = launch_gemm(f1, bs, stream)) != cudaSuccess) return e;  // T = x-slices * R
         if (a.n_aterms) {

@@ -219,7 +219,7 @@ dmrgb200_status finish_plan(std::unique_ptr<dmrgb200_plan_s>& p, dmrgb200_plan_t
     if (!err.empty()) return fail(DMRGB200_INVALID_PLAN, err);
     cudaGetDevice(&p->device);
     if (p->flat.kind == KIND_HPSI) {
-        compile_program(p->flat, p->stage3_bnd, p->stage1_bnd, {}, p->prog);
+        compile_program(p->flat, p->stage3_bnd, p->stage1_bnd, {}, p->prog, true);
         cudaError_t e = upload_program(p->prog);
         if (e != cudaSuccess) {
             free_program(p->prog);
@@ -278,9 +278,10 @@ dmrgb200_status run_step(dmrgb200_plan_s* p, const double* ket, const double* br
 dmrgb200_status hpsi_emulated(dmrgb200_plan_s* plan, const double* x, double* y, cudaStream_t st) {
     const uint64_t klim = (1ull << 17) / uint64_t(plan->slices);
     if (!plan->oz1) {
-        if (max_k_total(plan->prog.stage1) > klim || max_k_total(plan->prog.stage3) > klim)
+        GemmList const& s1 = plan->prog.stage1_tasks.probs.empty() ? plan->prog.stage1 : plan->prog.stage1_tasks;
+        if (max_k_total(s1) > klim || max_k_total(plan->prog.stage3) > klim)
             return fail(DMRGB200_NOT_SUPPORTED, "a contraction is longer than the exact INT32 range of the emulation");
-        plan->oz1 = oz_build(plan->prog.stage1);
+        plan->oz1 = oz_build(s1);
         plan->oz3 = oz_build(plan->prog.stage3);
         if (!plan->oz1 || !plan->oz3) return fail(DMRGB200_OUT_OF_MEMORY, "emulation tables");
     }

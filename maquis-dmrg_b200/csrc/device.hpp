@@ -27,6 +27,18 @@ struct DevProb {
     DevOp C;
     uint32_t M, N;
     uint32_t seg_begin, seg_end;
+    // row-table problems: row r of A and C is described by rowtab[rows + r] (the
+    // A operand of every segment is then read through the table, not through A.off
+    // and A.ld); NO_ROWS for plain problems
+    uint32_t rows = NO_ROWS;
+    static constexpr uint32_t NO_ROWS = 0xFFFFFFFFu;
+};
+
+// one row of a row-table problem: A(r, k) = base(A.buf)[a_off + k * ld] and
+// C(r, c) of batch b = base(C.buf)[c_off + b * cbs + c * ld]
+struct DevRow {
+    uint64_t a_off, c_off, cbs;
+    uint32_t ld, pad;
 };
 
 struct DevSeg {
@@ -86,6 +98,7 @@ struct GemmList {
     std::vector<DevSeg> segs;
     std::vector<DevTile> tiles;                        // class 0
     std::vector<DevTile> tiles_cls[N_TILE_CLASSES];    // classes 1.. (entry 0 unused)
+    std::vector<DevRow> rowtab;                        // rows of row-table problems
 };
 
 // device tile lists of the classes above 0
@@ -111,6 +124,8 @@ struct DeviceProgram {
     DevSTerm* d_terms = nullptr;
     uint32_t n_t1 = 0, n_t3 = 0, n_lines = 0;
     TileLists x1, x3;  // tile lists of the other classes
+    DevRow* d_r1 = nullptr;  // stage-1 row table (stacked T tasks)
+    GemmList stage1_tasks;   // stage 1 as one problem per T task (when stage1 is stacked)
     // grouped-GEMM variant per stage (autotuned by tune_program)
     int var1 = 0, var3 = 0;
     bool tuned = false;
@@ -119,8 +134,11 @@ struct DeviceProgram {
 // Lower a flat plan.  lptr/rptr: device address of each cohort's storage of the
 // boundary read by stage 3 (H psi: L) and by stage 1 (H psi, right step: R;
 // left step: L).  outptr: device address of each output boundary cohort (steps).
+// stack_rows: stage 1 of H psi / right step as one row-table problem per set of
+// T tasks that share their boundary cohort (rows of all those tasks stacked);
+// the per-task list is kept in prog.stage1_tasks.
 void compile_program(FlatPlan const& p, std::vector<uint64_t> const& stage3_bnd, std::vector<uint64_t> const& stage1_bnd,
-                     std::vector<uint64_t> const& outptr, DeviceProgram& prog);
+                     std::vector<uint64_t> const& outptr, DeviceProgram& prog, bool stack_rows = false);
 cudaError_t upload_program(DeviceProgram& prog);
 void free_program(DeviceProgram& prog);
 
@@ -145,10 +163,11 @@ struct GemmDev {
     DevTile* t = nullptr;
     uint32_t n = 0;
     TileLists x;  // tile lists of the other classes
+    DevRow* r = nullptr;  // row table
     int var = 0;  // grouped-GEMM variant
 };
 // grouped-GEMM variants (tile shape x pipeline depth x CTAs per SM)
-constexpr int N_GEMM_VARIANTS = 10;
+constexpr int N_GEMM_VARIANTS = 15;
 const char* gemm_variant_name(int v);
 // Time every variant on the program's stage-1 and stage-3 tile lists (on the given
 // buffers, whose contents are overwritten as by an H psi) and keep the fastest per

@@ -11,7 +11,9 @@
 // mma.sync.m8n8k4.f64 (DMMA) on 64x64x16 CTA tiles, 4 warps of 32x32.
 #include <algorithm>
 #include <cstdio>
+#include <map>
 #include <numeric>
+#include <tuple>
 #include <string>
 
 #include "../../include/dmrgb200.h"
@@ -32,6 +34,24 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
                  : "+d"(c0), "+d"(c1)
                  : "d"(a), "d"(b));
+}
+
+// D += A B on 16 x 8 x 16 and 16 x 8 x 8 FP64 tensor-core tiles.  Fragments per
+// lane (g = lane / 4, q = lane % 4): a[v0 + 2 v1] = A(g + 8 v0, q + 4 v1),
+// b[v] = B(q + 4 v, g), d[e + 2 h] = D(g + 8 h, 2 q + e).
+__device__ __forceinline__ void mma16x8x16(double (&d)[4], const double (&a)[8], const double (&b)[4]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+        "{%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
+        : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]),
+          "d"(b[1]), "d"(b[2]), "d"(b[3]));
+}
+__device__ __forceinline__ void mma16x8x8(double (&d)[4], const double (&a)[4], const double (&b)[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+        : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
 // 8-byte asynchronous global->shared copy; src_bytes = 0 writes a zero (out-of-range element).
@@ -58,12 +78,24 @@ struct TileCursor {
 __device__ __forceinline__ int swz(int k) { return (k >> 2) & 3; }
 
 // Issue the copies of one K tile (segment sg, rows k0..k0+BK_) into stage buffers.
+// arow (row-table problems): this thread's A row (its m is tid % BM_ in every
+// copy), NULL beyond the problem's rows; ald its leading dimension.
 template <int BM_, int BK_>
 __device__ __forceinline__ void load_tile(double (*As)[BM_ + 4], double (*Bs)[LDB_S], DevSeg const& sg,
                                           const double* A, const double* B, uint32_t m0, uint32_t n0, uint32_t M,
-                                          uint32_t N, uint32_t k0, int tid) {
+                                          uint32_t N, uint32_t k0, int tid, bool rowmode, const double* arow,
+                                          uint32_t ald) {
     const uint64_t lda = sg.A.ld, ldb = sg.B.ld;
     const uint32_t K = sg.K;
+    if (rowmode) {
+#pragma unroll
+        for (int j = 0; j < (BM_ * BK_) / NTHREADS; ++j) {
+            const int idx = tid + j * NTHREADS, m = idx % BM_, k = idx / BM_;
+            const uint32_t gk = k0 + k;
+            const bool ok = arow != nullptr && gk < K;
+            cp_async8(&As[k][m ^ swz(k)], ok ? arow + uint64_t(gk) * ald : B, ok);
+        }
+    } else
 #pragma unroll
     for (int j = 0; j < (BM_ * BK_) / NTHREADS; ++j) {
         int idx = tid + j * NTHREADS;
@@ -107,17 +139,21 @@ __device__ __forceinline__ void load_tile(double (*As)[BM_ + 4], double (*Bs)[LD
 // empty (one step, no copies) stores zeros.
 struct LoadCursor {
     uint32_t ti, seg, seg_end, k0;
-    bool valid;
+    bool valid, rowmode;
+    const double* arow;  // row-table problems: this thread's A row
+    uint32_t ald;
 };
 
-template <int BM_, int BK_, int STAGES, int MINB>
+template <int BM_, int BK_, int STAGES, int MINB, bool BIG>
 __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb* __restrict__ probs,
                                                                    const DevSeg* __restrict__ segs,
                                                                    const DevTile* __restrict__ tiles, uint32_t n_tiles,
-                                                                   Bases bases) {
+                                                                   const DevRow* __restrict__ rowtab, Bases bases) {
     // warps: 2 x 2 for BM_ >= 32 (warp tiles BM_/2 x 32), 1 x 4 for BM_ = 16 (16 x 16)
-    constexpr int WARPS_M = BM_ >= 32 ? 2 : 1, WM = BM_ / WARPS_M, MI = WM / 8;
+    constexpr int WARPS_M = BM_ >= 32 ? 2 : 1, WM = BM_ / WARPS_M;
     constexpr int WN = BN / (4 / WARPS_M), NJ = WN / 8;
+    // accumulator tiles: 16 x 8 (BIG: m16n8k16 / m16n8k8 MMAs) or 8 x 8 (m8n8k4)
+    constexpr int MI = BIG ? WM / 16 : WM / 8, AE = BIG ? 4 : 2;
     __shared__ __align__(16) double As[STAGES][BK_][BM_ + 4];
     __shared__ __align__(16) double Bs[STAGES][BK_][LDB_S];
 
@@ -127,15 +163,26 @@ __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb
     const int g = lane >> 2, q = lane & 3;
 
     // ---- producer: walks (tile, segment, k0) and issues one K step per call ----
-    LoadCursor L{blockIdx.x, 0, 0, 0, false};
+    LoadCursor L{blockIdx.x, 0, 0, 0, false, false, nullptr, 0};
     auto enter_tile = [&]() {
         L.valid = L.ti < n_tiles;
         if (!L.valid) return;
-        const DevProb& pr = probs[tiles[L.ti].prob];
+        const DevTile tl = tiles[L.ti];
+        const DevProb& pr = probs[tl.prob];
         L.seg = pr.seg_begin;
         L.seg_end = pr.seg_end;
         L.k0 = 0;
         while (L.seg < L.seg_end && segs[L.seg].K == 0) ++L.seg;
+        L.rowmode = pr.rows != DevProb::NO_ROWS;
+        L.arow = nullptr;
+        if (L.rowmode && L.seg < L.seg_end) {
+            const uint32_t gm = tl.m0 + uint32_t(tid % BM_);
+            if (gm < pr.M) {
+                const DevRow rw = rowtab[pr.rows + gm];
+                L.arow = reinterpret_cast<const double*>(base_of(bases, segs[L.seg].A.buf) + 8ull * rw.a_off);
+                L.ald = rw.ld;
+            }
+        }
     };
     auto issue = [&](int slot) {
         if (!L.valid) return;
@@ -144,7 +191,8 @@ __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb
             const DevProb& pr = probs[tl.prob];
             const DevSeg sg = segs[L.seg];
             load_tile<BM_, BK_>(As[slot], Bs[slot], sg, op_base(bases, sg.A, tl.batch),
-                                op_base(bases, sg.B, tl.batch), tl.m0, tl.n0, pr.M, pr.N, L.k0, tid);
+                                op_base(bases, sg.B, tl.batch), tl.m0, tl.n0, pr.M, pr.N, L.k0, tid, L.rowmode,
+                                L.arow, L.ald);
             L.k0 += BK_;
             if (L.k0 < sg.K) return;
             L.k0 = 0;
@@ -163,11 +211,13 @@ __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb
         cp_async_commit();
     }
 
-    double acc[MI][NJ][2];
+    double acc[MI][NJ][AE];
 #pragma unroll
     for (int i = 0; i < MI; ++i)
 #pragma unroll
-        for (int j = 0; j < NJ; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+        for (int j = 0; j < NJ; ++j)
+#pragma unroll
+            for (int e = 0; e < AE; ++e) acc[i][j][e] = 0.0;
 
     // ---- consumer: tiles in the same order, nsteps K steps each ----
     int slot = 0;
@@ -178,17 +228,44 @@ __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb
             cp_async_commit();
             cp_async_wait<STAGES - 1>();
             __syncthreads();
+            if constexpr (BIG) {
+                // one m16n8k(BK_) MMA per 16 x 8 accumulator tile; row k = q + 4 v of the
+                // K step sits behind swizzle constant v
+                constexpr int KV = BK_ / 4;
+                double b[NJ][KV];
 #pragma unroll
-            for (int kk = 0; kk < BK_; kk += 4) {
-                double a[MI], b[NJ];
+                for (int j = 0; j < NJ; ++j)
 #pragma unroll
-                for (int i = 0; i < MI; ++i) a[i] = As[slot][kk + q][(wm + i * 8 + g) ^ (kk >> 2)];
+                    for (int v = 0; v < KV; ++v) b[j][v] = Bs[slot][q + 4 * v][(wn + j * 8 + g) ^ v];
 #pragma unroll
-                for (int j = 0; j < NJ; ++j) b[j] = Bs[slot][kk + q][(wn + j * 8 + g) ^ (kk >> 2)];
+                for (int i = 0; i < MI; ++i) {
+                    double a[2 * KV];
 #pragma unroll
-                for (int i = 0; i < MI; ++i)
+                    for (int v = 0; v < KV; ++v) {
+                        a[2 * v] = As[slot][q + 4 * v][(wm + i * 16 + g) ^ v];
+                        a[2 * v + 1] = As[slot][q + 4 * v][(wm + i * 16 + 8 + g) ^ v];
+                    }
 #pragma unroll
-                    for (int j = 0; j < NJ; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+                    for (int j = 0; j < NJ; ++j) {
+                        if constexpr (BK_ == 16)
+                            mma16x8x16(acc[i][j], a, b[j]);
+                        else
+                            mma16x8x8(acc[i][j], a, b[j]);
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int kk = 0; kk < BK_; kk += 4) {
+                    double a[MI], b[NJ];
+#pragma unroll
+                    for (int i = 0; i < MI; ++i) a[i] = As[slot][kk + q][(wm + i * 8 + g) ^ (kk >> 2)];
+#pragma unroll
+                    for (int j = 0; j < NJ; ++j) b[j] = Bs[slot][kk + q][(wn + j * 8 + g) ^ (kk >> 2)];
+#pragma unroll
+                    for (int i = 0; i < MI; ++i)
+#pragma unroll
+                        for (int j = 0; j < NJ; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+                }
             }
             __syncthreads();
             slot = (slot + 1) % STAGES;
@@ -200,19 +277,30 @@ __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb
         const DevProb pr = probs[tl.prob];
         bool empty = true;
         for (uint32_t sg = pr.seg_begin; sg < pr.seg_end; ++sg) empty = empty && segs[sg].K == 0;
+        const bool rowmode = pr.rows != DevProb::NO_ROWS;
         double* C = const_cast<double*>(op_base(bases, pr.C, tl.batch));
         const uint64_t ldc = pr.C.ld;
 #pragma unroll
-        for (int i = 0; i < MI; ++i)
+        for (int ih = 0; ih < MI * (AE / 2); ++ih) {
+            const int i = ih / (AE / 2), h = ih % (AE / 2);  // accumulator tile, row half
+            const uint32_t r = tl.m0 + wm + i * (8 * AE / 2) + 8 * h + g;
+            // the row's start and leading dimension: from the row table or the plain operand
+            double* crow = C + r;
+            uint64_t ld = ldc;
+            if (rowmode && r < pr.M) {
+                const DevRow rw = rowtab[pr.rows + r];
+                crow = reinterpret_cast<double*>(base_of(bases, pr.C.buf) + 8ull * (rw.c_off + tl.batch * rw.cbs));
+                ld = rw.ld;
+            }
 #pragma unroll
             for (int j = 0; j < NJ; ++j)
 #pragma unroll
                 for (int e = 0; e < 2; ++e) {
-                    uint32_t r = tl.m0 + wm + i * 8 + g;
                     uint32_t c = tl.n0 + wn + j * 8 + q * 2 + e;
-                    if (r < pr.M && c < pr.N) C[r + c * ldc] = empty ? 0.0 : acc[i][j][e];
-                    acc[i][j][e] = 0.0;
+                    if (r < pr.M && c < pr.N) crow[c * ld] = empty ? 0.0 : acc[i][j][2 * h + e];
+                    acc[i][j][2 * h + e] = 0.0;
                 }
+        }
     }
     cp_async_wait<0>();
 }
@@ -353,9 +441,61 @@ std::vector<uint64_t> s_offsets(FlatPlan const& p, uint64_t* total) {
     return off;
 }
 
+namespace {
+// Stage 1 of H psi / right step with the rows of all T tasks that share a
+// boundary cohort (same cohort, transposition and shape) stacked into one
+// row-table problem: A row r is row r' of task t's psi slice, C row r is row r'
+// of T_t (leading dimension = the task's row count), so one tile covers several
+// small psi blocks instead of padding each to a full tile.
+void stack_stage1(FlatPlan const& p, std::vector<uint64_t> const& stage1_bnd, std::vector<uint64_t> const& t_off,
+                  GemmList& g1) {
+    g1 = GemmList();
+    std::map<std::tuple<uint32_t, uint8_t, uint32_t, uint32_t, uint32_t>, std::vector<uint32_t>> groups;
+    for (uint32_t t = 0; t < p.n_t(); ++t)
+        groups[{p.t_ci[t], p.t_trans[t], p.t_brows[t], p.t_bcols[t], p.t_nb[t]}].push_back(t);
+    for (auto const& kv : groups) {
+        const uint32_t t0 = kv.second.front();
+        const uint32_t K = p.t_brows[t0], Nf = p.t_bcols[t0], nb = p.t_nb[t0];
+        const bool tr = p.t_trans[t0] != 0;
+        const uint64_t bnd = stage1_bnd.at(p.t_ci[t0]) / 8;
+        DevProb pr;
+        pr.rows = uint32_t(g1.rowtab.size());
+        uint32_t M = 0;
+        for (uint32_t t : kv.second) {
+            const uint32_t Mt = p.in_rows[p.t_lb[t]];
+            for (uint32_t r = 0; r < Mt; ++r)
+                g1.rowtab.push_back(DevRow{p.in_off[p.t_lb[t]] + uint64_t(p.t_col[t]) * Mt + r, t_off[t] + r,
+                                           tr ? uint64_t(Mt) * Nf : 0, Mt, 0});
+            M += Mt;
+        }
+        pr.M = M;
+        pr.C = op(BUF_T, 0, 0, false);
+        DevSeg sg{};
+        sg.A = op(BUF_IN, 0, 0, false);
+        sg.K = K;
+        uint32_t nbatch = 1;
+        if (!tr) {
+            // the nb stored blocks are adjacent K x Nf column blocks: one product of width nb * Nf
+            pr.N = Nf * nb;
+            sg.B = op(BUF_ABS, bnd, K, false, 0);
+        } else {
+            pr.N = Nf;
+            sg.B = op(BUF_ABS, bnd, Nf, true, uint64_t(K) * Nf);
+            nbatch = nb;
+        }
+        pr.seg_begin = uint32_t(g1.segs.size());
+        g1.segs.push_back(sg);
+        pr.seg_end = uint32_t(g1.segs.size());
+        g1.probs.push_back(pr);
+        add_tiles(g1, uint32_t(g1.probs.size() - 1), nbatch);
+    }
+    sort_tiles(g1);
+}
+}  // namespace
+
 void compile_program(FlatPlan const& p, std::vector<uint64_t> const& stage3_bnd,
                      std::vector<uint64_t> const& stage1_bnd, std::vector<uint64_t> const& outptr,
-                     DeviceProgram& prog) {
+                     DeviceProgram& prog, bool stack_rows) {
     prog = DeviceProgram();
     const uint32_t nt = p.n_t(), nc = p.n_cohorts();
     std::vector<uint64_t> t_off = t_offsets(p, &prog.t_elems);
@@ -400,6 +540,10 @@ void compile_program(FlatPlan const& p, std::vector<uint64_t> const& stage3_bnd,
         add_tiles(g1, uint32_t(g1.probs.size() - 1), p.t_nb[t]);
     }
     sort_tiles(g1);
+    if (stack_rows && p.kind != KIND_LEFT && p.n_t()) {
+        prog.stage1_tasks = std::move(prog.stage1);
+        stack_stage1(p, stage1_bnd, t_off, prog.stage1);
+    }
 
     // ---- stage 2 (S lines) ----
     std::vector<uint64_t> s_off = s_offsets(p, &prog.s_elems);
@@ -533,6 +677,7 @@ cudaError_t upload_program(DeviceProgram& prog) {
     if ((e = up(prog.stage3.probs, &prog.d_p3)) != cudaSuccess) return e;
     if ((e = up(prog.stage3.segs, &prog.d_s3)) != cudaSuccess) return e;
     if ((e = up(prog.stage3.tiles, &prog.d_t3)) != cudaSuccess) return e;
+    if ((e = up(prog.stage1.rowtab, &prog.d_r1)) != cudaSuccess) return e;
     for (int c = 1; c < N_TILE_CLASSES; ++c) {
         if ((e = up(prog.stage1.tiles_cls[c], &prog.x1.t[c])) != cudaSuccess) return e;
         if ((e = up(prog.stage3.tiles_cls[c], &prog.x3.t[c])) != cudaSuccess) return e;
@@ -554,6 +699,8 @@ void free_program(DeviceProgram& prog) {
     cudaFree(prog.d_p3);
     cudaFree(prog.d_s3);
     cudaFree(prog.d_t3);
+    cudaFree(prog.d_r1);
+    prog.d_r1 = nullptr;
     for (int c = 1; c < N_TILE_CLASSES; ++c) {
         cudaFree(prog.x1.t[c]);
         cudaFree(prog.x3.t[c]);
@@ -600,6 +747,7 @@ cudaError_t upload_gemm(GemmList const& gl, GemmDev& d) {
     if ((e = up(gl.probs, &d.p)) != cudaSuccess) return e;
     if ((e = up(gl.segs, &d.s)) != cudaSuccess) return e;
     if ((e = up(gl.tiles, &d.t)) != cudaSuccess) return e;
+    if ((e = up(gl.rowtab, &d.r)) != cudaSuccess) return e;
     for (int c = 1; c < N_TILE_CLASSES; ++c) {
         if ((e = up(gl.tiles_cls[c], &d.x.t[c])) != cudaSuccess) return e;
         d.x.n[c] = uint32_t(gl.tiles_cls[c].size());
@@ -614,11 +762,12 @@ void free_gemm(GemmDev& d) {
     cudaFree(d.s);
     cudaFree(d.t);
     for (int c = 1; c < N_TILE_CLASSES; ++c) cudaFree(d.x.t[c]);
+    cudaFree(d.r);
     d = GemmDev();
 }
 
 namespace {
-using GemmKernel = void (*)(const DevProb*, const DevSeg*, const DevTile*, uint32_t, Bases);
+using GemmKernel = void (*)(const DevProb*, const DevSeg*, const DevTile*, uint32_t, const DevRow*, Bases);
 
 // pipeline depth x CTAs per SM of the grouped GEMM, chosen per stage by the autotuner
 struct GemmVariant {
@@ -627,16 +776,21 @@ struct GemmVariant {
     int tile_class;  // which tile list it runs on
 };
 const GemmVariant kVariants[N_GEMM_VARIANTS] = {
-    {gemm_f64_grouped<32, 16, 2, 4>, "tile32x64_k16_stages2_ctas4", 0},
-    {gemm_f64_grouped<32, 16, 3, 4>, "tile32x64_k16_stages3_ctas4", 0},
-    {gemm_f64_grouped<32, 16, 2, 5>, "tile32x64_k16_stages2_ctas5", 0},
-    {gemm_f64_grouped<32, 16, 3, 5>, "tile32x64_k16_stages3_ctas5", 0},
-    {gemm_f64_grouped<16, 8, 3, 6>, "tile16x64_k8_stages3_ctas6", 1},
-    {gemm_f64_grouped<16, 8, 4, 6>, "tile16x64_k8_stages4_ctas6", 1},
-    {gemm_f64_grouped<16, 8, 3, 8>, "tile16x64_k8_stages3_ctas8", 1},
-    {gemm_f64_grouped<16, 8, 4, 8>, "tile16x64_k8_stages4_ctas8", 1},
-    {gemm_f64_grouped<64, 16, 2, 3>, "tile64x64_k16_stages2_ctas3", 2},
-    {gemm_f64_grouped<64, 16, 2, 2>, "tile64x64_k16_stages2_ctas2", 2},
+    {gemm_f64_grouped<32, 16, 2, 4, false>, "tile32x64_k16_stages2_ctas4", 0},
+    {gemm_f64_grouped<32, 16, 3, 4, false>, "tile32x64_k16_stages3_ctas4", 0},
+    {gemm_f64_grouped<32, 16, 2, 5, false>, "tile32x64_k16_stages2_ctas5", 0},
+    {gemm_f64_grouped<32, 16, 3, 5, false>, "tile32x64_k16_stages3_ctas5", 0},
+    {gemm_f64_grouped<16, 8, 3, 6, false>, "tile16x64_k8_stages3_ctas6", 1},
+    {gemm_f64_grouped<16, 8, 4, 6, false>, "tile16x64_k8_stages4_ctas6", 1},
+    {gemm_f64_grouped<16, 8, 3, 8, false>, "tile16x64_k8_stages3_ctas8", 1},
+    {gemm_f64_grouped<16, 8, 4, 8, false>, "tile16x64_k8_stages4_ctas8", 1},
+    {gemm_f64_grouped<64, 16, 2, 3, false>, "tile64x64_k16_stages2_ctas3", 2},
+    {gemm_f64_grouped<64, 16, 2, 2, false>, "tile64x64_k16_stages2_ctas2", 2},
+    {gemm_f64_grouped<32, 16, 2, 4, true>, "tile32x64_k16_stages2_ctas4_mma16", 0},
+    {gemm_f64_grouped<32, 16, 3, 4, true>, "tile32x64_k16_stages3_ctas4_mma16", 0},
+    {gemm_f64_grouped<16, 8, 3, 8, true>, "tile16x64_k8_stages3_ctas8_mma16", 1},
+    {gemm_f64_grouped<64, 16, 2, 3, true>, "tile64x64_k16_stages2_ctas3_mma16", 2},
+    {gemm_f64_grouped<64, 16, 2, 2, true>, "tile64x64_k16_stages2_ctas2_mma16", 2},
 };
 
 int variant_occupancy(int v) {
@@ -652,7 +806,7 @@ int variant_occupancy(int v) {
 // t / n: the tile list of class 0; x: the other classes (a variant whose list is
 // absent falls back to variant 0)
 cudaError_t launch_variant(int v, const DevProb* p, const DevSeg* sg, const DevTile* t, uint32_t n,
-                           TileLists const& x, Bases const& bs, cudaStream_t stream) {
+                           TileLists const& x, const DevRow* rows, Bases const& bs, cudaStream_t stream) {
     if (!n) return cudaSuccess;
     if (v < 0 || v >= N_GEMM_VARIANTS) v = 0;
     const int c = kVariants[v].tile_class;
@@ -662,7 +816,7 @@ cudaError_t launch_variant(int v, const DevProb* p, const DevSeg* sg, const DevT
         n = x.n[c];
     }
     uint32_t grid = std::min<uint32_t>(n, uint32_t(device_sm_count()) * variant_occupancy(v));
-    kVariants[v].fn<<<grid, NTHREADS, 0, stream>>>(p, sg, t, n, bs);
+    kVariants[v].fn<<<grid, NTHREADS, 0, stream>>>(p, sg, t, n, rows, bs);
     return cudaGetLastError();
 }
 }  // namespace
@@ -670,7 +824,7 @@ cudaError_t launch_variant(int v, const DevProb* p, const DevSeg* sg, const DevT
 const char* gemm_variant_name(int v) { return (v >= 0 && v < N_GEMM_VARIANTS) ? kVariants[v].name : "?"; }
 
 cudaError_t launch_gemm(GemmDev const& d, Bases const& bs, cudaStream_t stream) {
-    return launch_variant(d.var, d.p, d.s, d.t, d.n, d.x, bs, stream);
+    return launch_variant(d.var, d.p, d.s, d.t, d.n, d.x, d.r, bs, stream);
 }
 
 cudaError_t tune_program(DeviceProgram& prog, uint64_t in, uint64_t out, double* T, double* S, cudaStream_t stream) {
@@ -692,9 +846,10 @@ cudaError_t tune_program(DeviceProgram& prog, uint64_t in, uint64_t out, double*
         const DevTile* t;
         uint32_t n;
         TileLists x;
+        const DevRow* r;
         int* var;
-    } stages[2] = {{prog.d_p1, prog.d_s1, prog.d_t1, prog.n_t1, prog.x1, &prog.var1},
-                   {prog.d_p3, prog.d_s3, prog.d_t3, prog.n_t3, prog.x3, &prog.var3}};
+    } stages[2] = {{prog.d_p1, prog.d_s1, prog.d_t1, prog.n_t1, prog.x1, prog.d_r1, &prog.var1},
+                   {prog.d_p3, prog.d_s3, prog.d_t3, prog.n_t3, prog.x3, nullptr, &prog.var3}};
     // stage 1 writes T, read by nothing else here; stage 3 reads S: both are timed on the
     // plan's current scratch contents (the kernels' speed does not depend on the values)
     for (auto& st : stages) {
@@ -702,11 +857,11 @@ cudaError_t tune_program(DeviceProgram& prog, uint64_t in, uint64_t out, double*
         float best = 1e30f;
         int bv = 0;
         for (int v = 0; v < N_GEMM_VARIANTS && e == cudaSuccess; ++v) {
-            e = launch_variant(v, st.p, st.s, st.t, st.n, st.x, bs, stream);  // warm
+            e = launch_variant(v, st.p, st.s, st.t, st.n, st.x, st.r, bs, stream);  // warm
             float tot = 0.f;
             for (int r = 0; r < 2 && e == cudaSuccess; ++r) {
                 cudaEventRecord(e0, stream);
-                e = launch_variant(v, st.p, st.s, st.t, st.n, st.x, bs, stream);
+                e = launch_variant(v, st.p, st.s, st.t, st.n, st.x, st.r, bs, stream);
                 cudaEventRecord(e1, stream);
                 if (e == cudaSuccess) e = cudaEventSynchronize(e1);
                 float ms = 0.f;
@@ -761,14 +916,14 @@ cudaError_t run_program(DeviceProgram const& prog, uint64_t in, uint64_t out, do
     bs.b[BUF_ABS] = 0;
     const int sms = device_sm_count();
     if (ev) cudaEventRecord(ev[0], stream);
-    launch_variant(prog.var1, prog.d_p1, prog.d_s1, prog.d_t1, prog.n_t1, prog.x1, bs, stream);
+    launch_variant(prog.var1, prog.d_p1, prog.d_s1, prog.d_t1, prog.n_t1, prog.x1, prog.d_r1, bs, stream);
     if (ev) cudaEventRecord(ev[1], stream);
     if (prog.n_lines) {
         uint32_t grid = std::min<uint32_t>(prog.n_lines, uint32_t(sms) * 8);
         sbuild_lines<<<grid, 256, 0, stream>>>(prog.d_lines, prog.d_terms, prog.n_lines, S, T);
     }
     if (ev) cudaEventRecord(ev[2], stream);
-    launch_variant(prog.var3, prog.d_p3, prog.d_s3, prog.d_t3, prog.n_t3, prog.x3, bs, stream);
+    launch_variant(prog.var3, prog.d_p3, prog.d_s3, prog.d_t3, prog.n_t3, prog.x3, nullptr, bs, stream);
     if (ev) cudaEventRecord(ev[3], stream);
     return cudaGetLastError();
 }

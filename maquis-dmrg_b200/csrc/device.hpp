@@ -90,8 +90,9 @@ struct DevArray {
 };
 
 // tile classes of the grouped GEMM: 0 = 32 x 64 tiles with 16-deep K steps,
-// 1 = 16 x 64 with 8-deep steps, 2 = 64 x 64 with 16-deep steps
-constexpr int N_TILE_CLASSES = 3;
+// 1 = 16 x 64 with 8-deep steps, 2 = 64 x 64 with 16-deep steps, 3 = 16 x 64
+// with 16-deep steps
+constexpr int N_TILE_CLASSES = 4;
 
 struct GemmList {
     std::vector<DevProb> probs;

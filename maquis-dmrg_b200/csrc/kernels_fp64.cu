@@ -23,7 +23,7 @@ namespace dmrgb200 {
 
 namespace {
 
-constexpr int BN = 64, NTHREADS = 128;
+constexpr int BN = 64;
 constexpr int LDB_S = BN + 4;  // row strides = 8 words mod 32: conflict-free fragment loads
 
 __device__ __forceinline__ const double* op_base(Bases const& bs, DevOp const& op, uint32_t batch) {
@@ -80,7 +80,7 @@ __device__ __forceinline__ int swz(int k) { return (k >> 2) & 3; }
 // Issue the copies of one K tile (segment sg, rows k0..k0+BK_) into stage buffers.
 // arow (row-table problems): this thread's A row (its m is tid % BM_ in every
 // copy), NULL beyond the problem's rows; ald its leading dimension.
-template <int BM_, int BK_>
+template <int BM_, int BK_, int NTHREADS>
 __device__ __forceinline__ void load_tile(double (*As)[BM_ + 4], double (*Bs)[LDB_S], DevSeg const& sg,
                                           const double* A, const double* B, uint32_t m0, uint32_t n0, uint32_t M,
                                           uint32_t N, uint32_t k0, int tid, bool rowmode, const double* arow,
@@ -144,14 +144,14 @@ struct LoadCursor {
     uint32_t ald;
 };
 
-template <int BM_, int BK_, int STAGES, int MINB, bool BIG>
+template <int BM_, int BK_, int STAGES, int MINB, bool BIG, int NTHREADS>
 __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb* __restrict__ probs,
                                                                    const DevSeg* __restrict__ segs,
                                                                    const DevTile* __restrict__ tiles, uint32_t n_tiles,
                                                                    const DevRow* __restrict__ rowtab, Bases bases) {
     // warps: 2 x 2 for BM_ >= 32 (warp tiles BM_/2 x 32), 1 x 4 for BM_ = 16 (16 x 16)
     constexpr int WARPS_M = BM_ >= 32 ? 2 : 1, WM = BM_ / WARPS_M;
-    constexpr int WN = BN / (4 / WARPS_M), NJ = WN / 8;
+    constexpr int WN = BN / (NTHREADS / 32 / WARPS_M), NJ = WN / 8;
     // accumulator tiles: 16 x 8 (BIG: m16n8k16 / m16n8k8 MMAs) or 8 x 8 (m8n8k4)
     constexpr int MI = BIG ? WM / 16 : WM / 8, AE = BIG ? 4 : 2;
     __shared__ __align__(16) double As[STAGES][BK_][BM_ + 4];
@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb
             const DevTile tl = tiles[L.ti];
             const DevProb& pr = probs[tl.prob];
             const DevSeg sg = segs[L.seg];
-            load_tile<BM_, BK_>(As[slot], Bs[slot], sg, op_base(bases, sg.A, tl.batch),
+            load_tile<BM_, BK_, NTHREADS>(As[slot], Bs[slot], sg, op_base(bases, sg.A, tl.batch),
                                 op_base(bases, sg.B, tl.batch), tl.m0, tl.n0, pr.M, pr.N, L.k0, tid, L.rowmode,
                                 L.arow, L.ald);
             L.k0 += BK_;
@@ -328,6 +328,42 @@ __global__ void __launch_bounds__(256) sbuild_lines(const DevSLine* __restrict__
         }
         __syncthreads();
         const uint64_t n = uint64_t(L.rows) * L.cols;
+        if (staged && nt <= 4) {
+            // the common short lines: four elements per thread and pass, each a fixed
+            // four-term form with predicated loads, so up to sixteen loads are in flight
+            const double a0 = nt > 0 ? s_alpha[0] : 0.0, a1 = nt > 1 ? s_alpha[1] : 0.0;
+            const double a2 = nt > 2 ? s_alpha[2] : 0.0, a3 = nt > 3 ? s_alpha[3] : 0.0;
+            const uint64_t b0 = nt > 0 ? s_base[0] : 0, b1 = nt > 1 ? s_base[1] : 0;
+            const uint64_t b2 = nt > 2 ? s_base[2] : 0, b3 = nt > 3 ? s_base[3] : 0;
+            for (uint64_t base = threadIdx.x; base < n; base += 4ull * blockDim.x) {
+                double x[4][4];
+                uint64_t soff[4];
+                bool in[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const uint64_t idx = base + uint64_t(u) * blockDim.x;
+                    in[u] = idx < n;
+                    const uint32_t i = in[u] ? uint32_t(idx % L.rows) : 0, c = in[u] ? uint32_t(idx / L.rows) : 0;
+                    const uint64_t off = i + uint64_t(c) * L.ld_t;
+                    soff[u] = L.s_base + i + uint64_t(c) * L.ld_s;
+                    x[u][0] = (in[u] && nt > 0) ? T[b0 + off] : 0.0;
+                    x[u][1] = (in[u] && nt > 1) ? T[b1 + off] : 0.0;
+                    x[u][2] = (in[u] && nt > 2) ? T[b2 + off] : 0.0;
+                    x[u][3] = (in[u] && nt > 3) ? T[b3 + off] : 0.0;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    if (!in[u]) continue;
+                    double v = 0.0;  // the same term order as the general loop below
+                    if (nt > 0) v += a0 * x[u][0];
+                    if (nt > 1) v += a1 * x[u][1];
+                    if (nt > 2) v += a2 * x[u][2];
+                    if (nt > 3) v += a3 * x[u][3];
+                    S[soff[u]] = v;
+                }
+            }
+            continue;
+        }
         for (uint64_t idx = threadIdx.x; idx < n; idx += blockDim.x) {
             const uint32_t i = uint32_t(idx % L.rows), c = uint32_t(idx / L.rows);
             const uint64_t off = i + uint64_t(c) * L.ld_t;
@@ -373,7 +409,7 @@ __global__ void __launch_bounds__(128) dmma_rate_loop(int iters, double* sink) {
 // --- host-side lowering ---------------------------------------------------------
 
 // tile classes: 0 = 32 x 64 tiles with 16-deep K steps, 1 = 16 x 64 with 8-deep steps
-constexpr int CLASS_BM[N_TILE_CLASSES] = {32, 16, 64}, CLASS_BK[N_TILE_CLASSES] = {16, 8, 16};
+constexpr int CLASS_BM[N_TILE_CLASSES] = {32, 16, 64, 16}, CLASS_BK[N_TILE_CLASSES] = {16, 8, 16, 16};
 
 void add_tiles(GemmList& gl, uint32_t prob, uint32_t nbatch) {
     DevProb const& p = gl.probs[prob];
@@ -396,7 +432,7 @@ void sort_tiles(GemmList& gl) {
     std::vector<uint64_t> kwork(gl.probs.size(), 0);
     for (size_t p = 0; p < gl.probs.size(); ++p)
         for (uint32_t s = gl.probs[p].seg_begin; s < gl.probs[p].seg_end; ++s) kwork[p] += gl.segs[s].K;
-    for (auto* tl : {&gl.tiles, &gl.tiles_cls[1], &gl.tiles_cls[2]})
+    for (auto* tl : {&gl.tiles, &gl.tiles_cls[1], &gl.tiles_cls[2], &gl.tiles_cls[3]})
         std::stable_sort(tl->begin(), tl->end(),
                          [&](DevTile const& a, DevTile const& b) { return kwork[a.prob] > kwork[b.prob]; });
 }
@@ -774,30 +810,31 @@ struct GemmVariant {
     GemmKernel fn;
     const char* name;
     int tile_class;  // which tile list it runs on
+    int threads;     // CTA size
 };
 const GemmVariant kVariants[N_GEMM_VARIANTS] = {
-    {gemm_f64_grouped<32, 16, 2, 4, false>, "tile32x64_k16_stages2_ctas4", 0},
-    {gemm_f64_grouped<32, 16, 3, 4, false>, "tile32x64_k16_stages3_ctas4", 0},
-    {gemm_f64_grouped<32, 16, 2, 5, false>, "tile32x64_k16_stages2_ctas5", 0},
-    {gemm_f64_grouped<32, 16, 3, 5, false>, "tile32x64_k16_stages3_ctas5", 0},
-    {gemm_f64_grouped<16, 8, 3, 6, false>, "tile16x64_k8_stages3_ctas6", 1},
-    {gemm_f64_grouped<16, 8, 4, 6, false>, "tile16x64_k8_stages4_ctas6", 1},
-    {gemm_f64_grouped<16, 8, 3, 8, false>, "tile16x64_k8_stages3_ctas8", 1},
-    {gemm_f64_grouped<16, 8, 4, 8, false>, "tile16x64_k8_stages4_ctas8", 1},
-    {gemm_f64_grouped<64, 16, 2, 3, false>, "tile64x64_k16_stages2_ctas3", 2},
-    {gemm_f64_grouped<64, 16, 2, 2, false>, "tile64x64_k16_stages2_ctas2", 2},
-    {gemm_f64_grouped<32, 16, 2, 4, true>, "tile32x64_k16_stages2_ctas4_mma16", 0},
-    {gemm_f64_grouped<32, 16, 3, 4, true>, "tile32x64_k16_stages3_ctas4_mma16", 0},
-    {gemm_f64_grouped<16, 8, 3, 8, true>, "tile16x64_k8_stages3_ctas8_mma16", 1},
-    {gemm_f64_grouped<64, 16, 2, 3, true>, "tile64x64_k16_stages2_ctas3_mma16", 2},
-    {gemm_f64_grouped<64, 16, 2, 2, true>, "tile64x64_k16_stages2_ctas2_mma16", 2},
+    {gemm_f64_grouped<32, 16, 2, 4, false, 128>, "tile32x64_k16_stages2_ctas4", 0, 128},
+    {gemm_f64_grouped<32, 16, 3, 4, false, 128>, "tile32x64_k16_stages3_ctas4", 0, 128},
+    {gemm_f64_grouped<32, 16, 2, 5, false, 128>, "tile32x64_k16_stages2_ctas5", 0, 128},
+    {gemm_f64_grouped<32, 16, 3, 5, false, 128>, "tile32x64_k16_stages3_ctas5", 0, 128},
+    {gemm_f64_grouped<16, 8, 3, 6, false, 128>, "tile16x64_k8_stages3_ctas6", 1, 128},
+    {gemm_f64_grouped<16, 8, 4, 8, false, 128>, "tile16x64_k8_stages4_ctas8", 1, 128},
+    {gemm_f64_grouped<64, 16, 2, 3, false, 128>, "tile64x64_k16_stages2_ctas3", 2, 128},
+    {gemm_f64_grouped<64, 16, 2, 2, false, 128>, "tile64x64_k16_stages2_ctas2", 2, 128},
+    {gemm_f64_grouped<32, 16, 2, 4, true, 128>, "tile32x64_k16_stages2_ctas4_mma16", 0, 128},
+    {gemm_f64_grouped<64, 16, 2, 3, true, 128>, "tile64x64_k16_stages2_ctas3_mma16", 2, 128},
+    {gemm_f64_grouped<16, 16, 2, 8, false, 64>, "tile16x64_k16_warps2_stages2_ctas8", 3, 64},
+    {gemm_f64_grouped<16, 16, 3, 8, false, 64>, "tile16x64_k16_warps2_stages3_ctas8", 3, 64},
+    {gemm_f64_grouped<16, 16, 2, 10, false, 64>, "tile16x64_k16_warps2_stages2_ctas10", 3, 64},
+    {gemm_f64_grouped<16, 16, 3, 10, false, 64>, "tile16x64_k16_warps2_stages3_ctas10", 3, 64},
+    {gemm_f64_grouped<16, 16, 2, 8, true, 64>, "tile16x64_k16_warps2_stages2_ctas8_mma16", 3, 64},
 };
 
 int variant_occupancy(int v) {
     static int occ[N_GEMM_VARIANTS] = {0};
     if (!occ[v]) {
         int o = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kVariants[v].fn, NTHREADS, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kVariants[v].fn, kVariants[v].threads, 0);
         occ[v] = o > 0 ? o : 1;
     }
     return occ[v];
@@ -816,7 +853,7 @@ cudaError_t launch_variant(int v, const DevProb* p, const DevSeg* sg, const DevT
         n = x.n[c];
     }
     uint32_t grid = std::min<uint32_t>(n, uint32_t(device_sm_count()) * variant_occupancy(v));
-    kVariants[v].fn<<<grid, NTHREADS, 0, stream>>>(p, sg, t, n, rows, bs);
+    kVariants[v].fn<<<grid, kVariants[v].threads, 0, stream>>>(p, sg, t, n, rows, bs);
     return cudaGetLastError();
 }
 }  // namespace

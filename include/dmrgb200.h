@@ -197,7 +197,10 @@ dmrgb200_status dmrgb200_plan_scratch_bytes(dmrgb200_plan_t plan, uint64_t* byte
  * ietl::mult (ietl_interface_dv.h:112-118).  DMRGB200_PREC_FP64_EMULATED runs
  * the T and cohort contractions on the INT8 tensor cores (Ozaki split, see
  * dmrgb200_plan_set_slices) and the S build in FP64; it synchronises the
- * stream before returning. */
+ * stream before returning.  The digit planes of the boundaries are made on the
+ * first emulated call of a plan and reused by later calls (the boundaries of a
+ * site problem do not change while it is solved); dmrgb200_plan_set_slices
+ * with a new slice count makes them again. */
 dmrgb200_status dmrgb200_hpsi(dmrgb200_plan_t plan, const double* x, double* y, dmrgb200_precision prec,
                               void* cuda_stream);
 

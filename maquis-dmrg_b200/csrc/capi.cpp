@@ -67,8 +67,10 @@ struct dmrgb200_plan_s {
     int slices = 7;
     OzProgram* oz1 = nullptr;
     OzProgram* oz3 = nullptr;
-    void* oz_scratch = nullptr;
+    void* oz_scratch = nullptr;   // stage-1 digit planes (the constant ones persist between calls)
     uint64_t oz_scratch_size = 0;
+    void* oz_scratch3 = nullptr;  // stage-3 digit planes
+    uint64_t oz_scratch3_size = 0;
     // Jacobi-Davidson: solver mode and the cached solver graph
     int solver_mode = DMRGB200_SOLVER_GRAPH;
     void* jd = nullptr;
@@ -285,30 +287,41 @@ dmrgb200_status hpsi_emulated(dmrgb200_plan_s* plan, const double* x, double* y,
         plan->oz3 = oz_build(plan->prog.stage3);
         if (!plan->oz1 || !plan->oz3) return fail(DMRGB200_OUT_OF_MEMORY, "emulation tables");
     }
-    uint64_t need = std::max(oz_scratch_bytes(plan->oz1, plan->slices), oz_scratch_bytes(plan->oz3, plan->slices));
-    if (need > plan->oz_scratch_size) {
-        cudaFree(plan->oz_scratch);
-        plan->oz_scratch = nullptr;
-        plan->oz_scratch_size = 0;
-        cudaError_t e = cudaMalloc(&plan->oz_scratch, need);
-        if (e != cudaSuccess) return cuda_fail(e, "emulation scratch");
-        plan->oz_scratch_size = need;
-    }
+    // one scratch per stage: each keeps the digit planes of its constant (boundary) operand
+    auto ensure = [&](OzProgram* oz, void*& buf, uint64_t& size) -> cudaError_t {
+        const uint64_t need = oz_scratch_bytes(oz, plan->slices);
+        if (need <= size) return cudaSuccess;
+        cudaFree(buf);
+        buf = nullptr;
+        size = 0;
+        oz_invalidate(oz);
+        cudaError_t e = cudaMalloc(&buf, need);
+        if (e == cudaSuccess) size = need;
+        return e;
+    };
+    cudaError_t e = ensure(plan->oz1, plan->oz_scratch, plan->oz_scratch_size);
+    if (e == cudaSuccess) e = ensure(plan->oz3, plan->oz_scratch3, plan->oz_scratch3_size);
+    if (e != cudaSuccess) return cuda_fail(e, "emulation scratch");
     Bases bs{};
     bs.b[BUF_IN] = reinterpret_cast<uint64_t>(x);
     bs.b[BUF_OUT] = reinterpret_cast<uint64_t>(y);
     bs.b[BUF_T] = reinterpret_cast<uint64_t>(plan->T);
     bs.b[BUF_S] = reinterpret_cast<uint64_t>(plan->S);
-    cudaError_t e = oz_run(plan->oz1, bs, plan->slices, plan->oz_scratch, st);
+    e = oz_run(plan->oz1, bs, plan->slices, plan->oz_scratch, st);
     if (e != cudaSuccess) return cuda_fail(e, "emulated stage 1");
-    if (oz_timed_out(plan->oz1, plan->oz_scratch, plan->slices, st))
-        return fail(DMRGB200_TIMEOUT, "emulated stage 1: a pipeline wait timed out");
     e = run_sbuild(plan->prog, plan->T, plan->S, st);
     if (e != cudaSuccess) return cuda_fail(e, "S build");
-    e = oz_run(plan->oz3, bs, plan->slices, plan->oz_scratch, st);
+    e = oz_run(plan->oz3, bs, plan->slices, plan->oz_scratch3, st);
     if (e != cudaSuccess) return cuda_fail(e, "emulated stage 3");
-    if (oz_timed_out(plan->oz3, plan->oz_scratch, plan->slices, st))
-        return fail(DMRGB200_TIMEOUT, "emulated stage 3: a pipeline wait timed out");
+    // one synchronisation: both stages' wait-timeout flags
+    const int to1 = oz_timed_out(plan->oz1, plan->oz_scratch, plan->slices, st);
+    const int to3 = oz_timed_out(plan->oz3, plan->oz_scratch3, plan->slices, st);
+    if (to1 || to3) {
+        oz_invalidate(plan->oz1);
+        oz_invalidate(plan->oz3);
+        return fail(DMRGB200_TIMEOUT, to1 ? "emulated stage 1: a pipeline wait timed out"
+                                          : "emulated stage 3: a pipeline wait timed out");
+    }
     return DMRGB200_OK;
 }
 

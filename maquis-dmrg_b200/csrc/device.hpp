@@ -222,6 +222,8 @@ uint64_t max_k_total(GemmList const& gl);
 struct OzProgram;  // lowered grouped problem list
 OzProgram* oz_build(GemmList const& gl);
 void oz_free(OzProgram* oz);
+// forget the cached digit planes of constant operands (their scratch was replaced)
+void oz_invalidate(OzProgram* oz);
 // device bytes the program needs for s digit planes (digits, exponents, error flag)
 uint64_t oz_scratch_bytes(OzProgram const* oz, int s);
 // run on the stream with scratch of oz_scratch_bytes(oz, s); returns a CUDA error

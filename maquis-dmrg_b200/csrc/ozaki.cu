@@ -139,7 +139,7 @@ struct OzSplit {
     uint64_t out_base;  // byte offset inside a digit plane
     uint64_t e_off;     // exponent array offset of row 0
     uint32_t is_b;      // 0: A operand, 1: B operand (read transposed)
-    uint32_t pad;
+    uint32_t is_const;  // the operand and its exponents are constant between calls
 };
 
 __device__ __forceinline__ double op_elem(Bases const& bs, OzSplit const& j, uint32_t r, uint32_t k) {
@@ -373,12 +373,18 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_mma(OzArgs a) {
 
 size_t ozaki_smem_bytes(int s) { return size_t(OZ_STAGES) * s * (A_TILE + B_TILE) + 8 * (2 * OZ_STAGES + 1) + 16; }
 
+// Operands held in boundary memory (BUF_ABS) do not change between calls of a
+// plan: their digit planes and exponents are computed on the first run and kept
+// in the program's scratch; later runs split only the other operands.  The
+// exponents of constant operands occupy [0, n_exp_c) of the exponent array.
 struct OzProgram {
-    std::vector<OzSplit> jobs;
+    std::vector<OzSplit> jobs;      // every operand (constant ones first)
+    uint32_t n_const_jobs = 0;
     std::vector<OzPB> pbs;
     std::vector<OzSlab> slabs;
     std::vector<OzTile> tiles;
-    uint64_t a_plane = 0, b_plane = 0, n_exp = 0;
+    uint64_t a_plane = 0, b_plane = 0, n_exp = 0, n_exp_c = 0;
+    bool const_ready = false;       // constant digit planes present in the scratch
     OzSplit* d_jobs = nullptr;
     OzPB* d_pbs = nullptr;
     OzSlab* d_slabs = nullptr;
@@ -389,18 +395,30 @@ OzProgram* oz_build(GemmList const& gl) {
     auto* oz = new OzProgram;
     std::vector<uint32_t> nbatch(gl.probs.size(), 0);
     for (auto const& t : gl.tiles) nbatch[t.prob] = std::max(nbatch[t.prob], t.batch + 1);
+    // exponent offsets: constant operands count in n_exp_c, the others in n_exp
+    // (shifted behind the constant region below); var_e / var_f mark the latter
+    std::vector<uint8_t> var_e, var_f;
     for (uint32_t p = 0; p < gl.probs.size(); ++p) {
         DevProb const& pr = gl.probs[p];
+        bool a_const = true, b_const = true;
+        for (uint32_t sgi = pr.seg_begin; sgi < pr.seg_end; ++sgi) {
+            a_const = a_const && gl.segs[sgi].A.buf == BUF_ABS;
+            b_const = b_const && gl.segs[sgi].B.buf == BUF_ABS;
+        }
         for (uint32_t b = 0; b < nbatch[p]; ++b) {
             OzPB pb{};
             pb.M = pr.M;
             pb.N = pr.N;
             pb.MT = std::max<uint32_t>(1, (pr.M + OZ_BM - 1) / OZ_BM);
             pb.NT = std::max<uint32_t>(1, (pr.N + OZ_BN - 1) / OZ_BN);
-            pb.e_off = oz->n_exp;
-            oz->n_exp += uint64_t(pb.MT) * OZ_BM;
-            pb.f_off = oz->n_exp;
-            oz->n_exp += uint64_t(pb.NT) * OZ_BN;
+            uint64_t& ce = a_const ? oz->n_exp_c : oz->n_exp;
+            pb.e_off = ce;
+            ce += uint64_t(pb.MT) * OZ_BM;
+            uint64_t& cf = b_const ? oz->n_exp_c : oz->n_exp;
+            pb.f_off = cf;
+            cf += uint64_t(pb.NT) * OZ_BN;
+            var_e.push_back(!a_const);
+            var_f.push_back(!b_const);
             pb.C = pr.C;
             pb.C.off += uint64_t(b) * pr.C.bstride;
             pb.beta = 0;
@@ -419,6 +437,7 @@ OzProgram* oz_build(GemmList const& gl) {
                 ja.out_base = oz->a_plane;
                 ja.e_off = pb.e_off;
                 ja.is_b = 0;
+                ja.is_const = a_const ? 1 : 0;
                 oz->a_plane += uint64_t(pb.MT) * KS * A_TILE;
                 jb.op = sg.B;
                 jb.op.off += uint64_t(b) * sg.B.bstride;
@@ -429,6 +448,7 @@ OzProgram* oz_build(GemmList const& gl) {
                 jb.out_base = oz->b_plane;
                 jb.e_off = pb.f_off;
                 jb.is_b = 1;
+                jb.is_const = b_const ? 1 : 0;
                 oz->b_plane += uint64_t(pb.NT) * KS * B_TILE;
                 for (uint32_t ks = 0; ks < KS; ++ks)
                     oz->slabs.push_back(OzSlab{ja.out_base + uint64_t(ks) * A_TILE, jb.out_base + uint64_t(ks) * B_TILE,
@@ -443,6 +463,16 @@ OzProgram* oz_build(GemmList const& gl) {
                 for (uint32_t nt = 0; nt < pb.NT; ++nt) oz->tiles.push_back(OzTile{pbi, mt, nt, 0});
         }
     }
+    for (size_t i = 0; i < oz->pbs.size(); ++i) {
+        if (var_e[i]) oz->pbs[i].e_off += oz->n_exp_c;
+        if (var_f[i]) oz->pbs[i].f_off += oz->n_exp_c;
+    }
+    for (auto& j : oz->jobs)
+        if (!j.is_const) j.e_off += oz->n_exp_c;
+    oz->n_exp += oz->n_exp_c;
+    std::stable_partition(oz->jobs.begin(), oz->jobs.end(), [](OzSplit const& j) { return j.is_const != 0; });
+    oz->n_const_jobs =
+        uint32_t(std::count_if(oz->jobs.begin(), oz->jobs.end(), [](OzSplit const& j) { return j.is_const != 0; }));
     // longest K first for the static round-robin over the persistent grid
     std::stable_sort(oz->tiles.begin(), oz->tiles.end(), [&](OzTile const& x, OzTile const& y) {
         auto kx = oz->pbs[x.pb].slab_end - oz->pbs[x.pb].slab_begin;
@@ -462,6 +492,10 @@ OzProgram* oz_build(GemmList const& gl) {
         return nullptr;
     }
     return oz;
+}
+
+void oz_invalidate(OzProgram* oz) {
+    if (oz) oz->const_ready = false;
 }
 
 void oz_free(OzProgram* oz) {
@@ -504,14 +538,19 @@ cudaError_t oz_run(OzProgram* oz, Bases const& bs, int s, void* scratch, cudaStr
     OzScratch c = carve(oz, s, scratch);
     const int sms = device_sm_count();
     cudaMemsetAsync(c.err, 0, sizeof(int), st);
-    if (oz->n_exp)
-        fill_int<<<std::min<uint64_t>((oz->n_exp + 255) / 256, 4096), 256, 0, st>>>(c.e, oz->n_exp, -100000);
-    const uint32_t nj = uint32_t(oz->jobs.size());
+    // first run: every operand; later runs: only the operands that change between calls
+    const uint64_t e0 = oz->const_ready ? oz->n_exp_c : 0;
+    const uint32_t j0 = oz->const_ready ? oz->n_const_jobs : 0;
+    if (oz->n_exp > e0)
+        fill_int<<<std::min<uint64_t>((oz->n_exp - e0 + 255) / 256, 4096), 256, 0, st>>>(c.e + e0, oz->n_exp - e0,
+                                                                                        -100000);
+    const uint32_t nj = uint32_t(oz->jobs.size()) - j0;
     if (nj) {
-        oz_exponents<<<std::min<uint32_t>(nj, uint32_t(sms) * 8), 256, 0, st>>>(oz->d_jobs, nj, bs, c.e);
+        oz_exponents<<<std::min<uint32_t>(nj, uint32_t(sms) * 8), 256, 0, st>>>(oz->d_jobs + j0, nj, bs, c.e);
         dim3 grid(16, std::min<uint32_t>(nj, 65535u));
-        oz_split<<<grid, 256, 0, st>>>(oz->d_jobs, nj, bs, c.e, s, oz->a_plane, c.A8, oz->b_plane, c.B8);
+        oz_split<<<grid, 256, 0, st>>>(oz->d_jobs + j0, nj, bs, c.e, s, oz->a_plane, c.A8, oz->b_plane, c.B8);
     }
+    oz->const_ready = true;
     if (!oz->tiles.empty()) {
         static bool attr = false;
         if (!attr) {

@@ -328,42 +328,6 @@ __global__ void __launch_bounds__(256) sbuild_lines(const DevSLine* __restrict__
         }
         __syncthreads();
         const uint64_t n = uint64_t(L.rows) * L.cols;
-        if (staged && nt <= 4) {
-            // the common short lines: four elements per thread and pass, each a fixed
-            // four-term form with predicated loads, so up to sixteen loads are in flight
-            const double a0 = nt > 0 ? s_alpha[0] : 0.0, a1 = nt > 1 ? s_alpha[1] : 0.0;
-            const double a2 = nt > 2 ? s_alpha[2] : 0.0, a3 = nt > 3 ? s_alpha[3] : 0.0;
-            const uint64_t b0 = nt > 0 ? s_base[0] : 0, b1 = nt > 1 ? s_base[1] : 0;
-            const uint64_t b2 = nt > 2 ? s_base[2] : 0, b3 = nt > 3 ? s_base[3] : 0;
-            for (uint64_t base = threadIdx.x; base < n; base += 4ull * blockDim.x) {
-                double x[4][4];
-                uint64_t soff[4];
-                bool in[4];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const uint64_t idx = base + uint64_t(u) * blockDim.x;
-                    in[u] = idx < n;
-                    const uint32_t i = in[u] ? uint32_t(idx % L.rows) : 0, c = in[u] ? uint32_t(idx / L.rows) : 0;
-                    const uint64_t off = i + uint64_t(c) * L.ld_t;
-                    soff[u] = L.s_base + i + uint64_t(c) * L.ld_s;
-                    x[u][0] = (in[u] && nt > 0) ? T[b0 + off] : 0.0;
-                    x[u][1] = (in[u] && nt > 1) ? T[b1 + off] : 0.0;
-                    x[u][2] = (in[u] && nt > 2) ? T[b2 + off] : 0.0;
-                    x[u][3] = (in[u] && nt > 3) ? T[b3 + off] : 0.0;
-                }
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    if (!in[u]) continue;
-                    double v = 0.0;  // the same term order as the general loop below
-                    if (nt > 0) v += a0 * x[u][0];
-                    if (nt > 1) v += a1 * x[u][1];
-                    if (nt > 2) v += a2 * x[u][2];
-                    if (nt > 3) v += a3 * x[u][3];
-                    S[soff[u]] = v;
-                }
-            }
-            continue;
-        }
         for (uint64_t idx = threadIdx.x; idx < n; idx += blockDim.x) {
             const uint32_t i = uint32_t(idx % L.rows), c = uint32_t(idx / L.rows);
             const uint64_t off = i + uint64_t(c) * L.ld_t;

@@ -27,11 +27,20 @@ __global__ void __launch_bounds__(256) alpha_grad(const DevATerm* __restrict__ a
     const uint32_t lane = threadIdx.x & 31, warps = blockDim.x >> 5;
     for (uint32_t i = blockIdx.x * warps + (threadIdx.x >> 5); i < n; i += gridDim.x * warps) {
         const DevATerm a = at[i];
-        const uint64_t cnt = uint64_t(a.rows) * a.cols;
         double s = 0.0;
-        for (uint64_t idx = lane; idx < cnt; idx += 32) {
-            uint32_t r = uint32_t(idx % a.rows), c = uint32_t(idx / a.rows);
-            s = fma(G[a.g_base + r + uint64_t(c) * a.ld_g], T[a.t_base + r + uint64_t(c) * a.ld_t], s);
+        if (a.rows) {
+            // column-major walk in steps of 32 without per-element division
+            const uint32_t dr = 32u % a.rows, dc = 32u / a.rows;
+            uint32_t r = lane % a.rows, c = lane / a.rows;
+            while (c < a.cols) {
+                s = fma(G[a.g_base + r + uint64_t(c) * a.ld_g], T[a.t_base + r + uint64_t(c) * a.ld_t], s);
+                r += dr;
+                c += dc;
+                if (r >= a.rows) {
+                    r -= a.rows;
+                    ++c;
+                }
+            }
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
@@ -46,15 +55,23 @@ __global__ void __launch_bounds__(256) tgrad_cells(const DevSLine* __restrict__ 
                                                    double* __restrict__ gT, const double* __restrict__ G) {
     for (uint32_t li = blockIdx.x; li < n_lines; li += gridDim.x) {
         const DevSLine L = lines[li];
-        const uint64_t n = uint64_t(L.rows) * L.cols;
-        for (uint64_t idx = threadIdx.x; idx < n; idx += blockDim.x) {
-            uint32_t i = uint32_t(idx % L.rows), c = uint32_t(idx / L.rows);
+        if (!L.rows) continue;
+        // column-major walk in steps of blockDim.x without per-element division
+        const uint32_t di = blockDim.x % L.rows, dc = blockDim.x / L.rows;
+        uint32_t i = threadIdx.x % L.rows, c = threadIdx.x / L.rows;
+        while (c < L.cols) {
             double v = 0.0;
             for (uint32_t t = L.term_begin; t < L.term_end; ++t) {
                 const DevGTerm tm = terms[t];
                 v += tm.alpha * G[tm.g_base + i + uint64_t(c) * tm.ld];
             }
             gT[L.s_base + i + uint64_t(c) * L.ld_s] = v;
+            i += di;
+            c += dc;
+            if (i >= L.rows) {
+                i -= L.rows;
+                ++c;
+            }
         }
     }
 }

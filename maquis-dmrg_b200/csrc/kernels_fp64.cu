@@ -327,9 +327,12 @@ __global__ void __launch_bounds__(256) sbuild_lines(const DevSLine* __restrict__
             s_base[threadIdx.x] = tm.t_base;
         }
         __syncthreads();
-        const uint64_t n = uint64_t(L.rows) * L.cols;
-        for (uint64_t idx = threadIdx.x; idx < n; idx += blockDim.x) {
-            const uint32_t i = uint32_t(idx % L.rows), c = uint32_t(idx / L.rows);
+        // element (i, c) walks the line column-major in steps of blockDim.x without
+        // per-element division
+        if (!L.rows) continue;
+        const uint32_t di = blockDim.x % L.rows, dc = blockDim.x / L.rows;
+        uint32_t i = threadIdx.x % L.rows, c = threadIdx.x / L.rows;
+        while (c < L.cols) {
             const uint64_t off = i + uint64_t(c) * L.ld_t;
             double v = 0.0;
             if (staged) {
@@ -350,6 +353,12 @@ __global__ void __launch_bounds__(256) sbuild_lines(const DevSLine* __restrict__
                 }
             }
             S[L.s_base + i + uint64_t(c) * L.ld_s] = v;
+            i += di;
+            c += dc;
+            if (i >= L.rows) {
+                i -= L.rows;
+                ++c;
+            }
         }
     }
 }

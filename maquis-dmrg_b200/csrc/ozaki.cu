@@ -156,13 +156,14 @@ __global__ void fill_int(int* __restrict__ p, uint64_t n, int v) {
 }
 
 // exponent of every row of every job (max over segments by atomicMax):
-// |x 2^-e| < 1 for the whole row of the output matrix
+// |x 2^-e| < 1 for the whole row of the output matrix.  blockIdx.y walks the
+// jobs, blockIdx.x and the warps the rows, the lanes K.
 __global__ void __launch_bounds__(256) oz_exponents(const OzSplit* __restrict__ jobs, uint32_t njobs, Bases bs,
                                                     int* __restrict__ e) {
-    const uint32_t lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    for (uint32_t j = blockIdx.x; j < njobs; j += gridDim.x) {
+    const uint32_t lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+    for (uint32_t j = blockIdx.y; j < njobs; j += gridDim.y) {
         const OzSplit job = jobs[j];
-        for (uint32_t r = wib; r < job.rows; r += blockDim.x >> 5) {
+        for (uint32_t r = blockIdx.x * warps + (threadIdx.x >> 5); r < job.rows; r += gridDim.x * warps) {
             double m = 0.0;
             for (uint32_t k = lane; k < job.K; k += 32) m = fmax(m, fabs(op_elem(bs, job, r, k)));
             for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
@@ -171,6 +172,9 @@ __global__ void __launch_bounds__(256) oz_exponents(const OzSplit* __restrict__ 
     }
 }
 
+// Digit planes: every thread cuts four consecutive K elements of one row and
+// stores each plane's four digits as one 32-bit word (K-contiguous bytes of the
+// tile layout).  Rows outside the operand and K beyond it give zero digits.
 __global__ void __launch_bounds__(256) oz_split(const OzSplit* __restrict__ jobs, uint32_t njobs, Bases bs,
                                                 const int* __restrict__ e, int s, uint64_t a_plane,
                                                 int8_t* __restrict__ A8, uint64_t b_plane, int8_t* __restrict__ B8) {
@@ -180,26 +184,29 @@ __global__ void __launch_bounds__(256) oz_split(const OzSplit* __restrict__ jobs
         const uint64_t plane = job.is_b ? b_plane : a_plane;
         const uint32_t TR = job.is_b ? uint32_t(OZ_BN) : uint32_t(OZ_BM);
         const uint32_t tile_bytes = TR * OZ_BK;
-        const uint64_t total = uint64_t(job.RT) * TR * job.KS * OZ_BK;
-        for (uint64_t idx = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; idx < total;
-             idx += uint64_t(gridDim.x) * blockDim.x) {
-            uint32_t r, k;
-            if (!job.is_b && !job.op.trans) {  // walk rows: contiguous in a column-major A
-                r = uint32_t(idx % (uint64_t(job.RT) * TR));
-                k = uint32_t(idx / (uint64_t(job.RT) * TR));
-            } else {                             // walk K
-                k = uint32_t(idx % (uint64_t(job.KS) * OZ_BK));
-                r = uint32_t(idx / (uint64_t(job.KS) * OZ_BK));
-            }
-            double x = 0.0;
-            if (r < job.rows && k < job.K) x = ldexp(op_elem(bs, job, r, k), -e[job.e_off + r]);
-            const uint64_t off = job.out_base + (uint64_t(r / TR) * job.KS + k / OZ_BK) * tile_bytes +
-                                 tile_off(r % TR, k % OZ_BK);
+        const uint32_t nrows = job.RT * TR, ngroups = job.KS * (OZ_BK / 4);
+        const uint32_t total = nrows * ngroups;
+        const bool rows_fast = !job.is_b && !job.op.trans;  // column-major A: rows are contiguous
+        for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+            const uint32_t r = rows_fast ? idx % nrows : idx / ngroups;
+            const uint32_t k0 = 4 * (rows_fast ? idx / nrows : idx % ngroups);
+            double x[4];
+            const int ex = r < job.rows ? e[job.e_off + r] : 0;
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                x[u] = (r < job.rows && k0 + u < job.K) ? ldexp(op_elem(bs, job, r, k0 + u), -ex) : 0.0;
+            const uint64_t off = job.out_base + (uint64_t(r / TR) * job.KS + k0 / OZ_BK) * tile_bytes +
+                                 tile_off(r % TR, k0 % OZ_BK);
             for (int p = 0; p < s; ++p) {
-                const double t = x * 128.0;  // exact
-                const double d = trunc(t);   // |d| <= 127
-                x = t - d;                   // exact
-                out[p * plane + off] = static_cast<int8_t>(d);
+                uint32_t word = 0;
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const double t = x[u] * 128.0;  // exact
+                    const double d = trunc(t);      // |d| <= 127
+                    x[u] = t - d;                   // exact
+                    word |= (uint32_t(uint8_t(int8_t(d)))) << (8 * u);
+                }
+                *reinterpret_cast<uint32_t*>(out + p * plane + off) = word;
             }
         }
     }
@@ -546,7 +553,7 @@ cudaError_t oz_run(OzProgram* oz, Bases const& bs, int s, void* scratch, cudaStr
                                                                                         -100000);
     const uint32_t nj = uint32_t(oz->jobs.size()) - j0;
     if (nj) {
-        oz_exponents<<<std::min<uint32_t>(nj, uint32_t(sms) * 8), 256, 0, st>>>(oz->d_jobs + j0, nj, bs, c.e);
+        oz_exponents<<<dim3(8, std::min<uint32_t>(nj, 65535u)), 256, 0, st>>>(oz->d_jobs + j0, nj, bs, c.e);
         dim3 grid(16, std::min<uint32_t>(nj, 65535u));
         oz_split<<<grid, 256, 0, st>>>(oz->d_jobs + j0, nj, bs, c.e, s, oz->a_plane, c.A8, oz->b_plane, c.B8);
     }

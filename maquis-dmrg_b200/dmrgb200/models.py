@@ -259,40 +259,48 @@ def twosite_mpo(W1: MPOTensor, W2: MPOTensor, p1, p2, merge: bool = True) -> MPO
     assert W1.col_dim == W2.row_dim
     terms = {}
     sources = {}
-    for b1 in range(W1.row_dim):
-        for b3 in range(W2.col_dim):
-            summands = [b2 for b2 in range(W1.col_dim) if (b1, b2) in W1.terms and (b2, b3) in W2.terms]
-            if not summands:
-                continue
-            if not merge:
-                lst, src = [], []
-                for b2 in summands:
-                    for j1, (o1, s1) in enumerate(W1.terms[(b1, b2)]):
-                        for j2, (o2, s2) in enumerate(W2.terms[(b2, b3)]):
-                            lst.append((kron_op(o1, o2, p1, p2), s1 * s2))
-                            src.append(((b1, b2, j1), (b2, b3, j2)))
-                terms[(b1, b3)] = lst
-                sources[(b1, b3)] = src
-                continue
-            if len(summands) == 1 and len(W1.terms[(b1, summands[0])]) == 1 and len(W2.terms[(summands[0], b3)]) == 1:
-                (o1, s1), = W1.terms[(b1, summands[0])]
-                (o2, s2), = W2.terms[(summands[0], b3)]
-                terms[(b1, b3)] = [(kron_op(o1, o2, p1, p2), s1 * s2)]
-            else:
-                acc = None
-                for b2 in summands:
-                    for o1, s1 in W1.terms[(b1, b2)]:
-                        for o2, s2 in W2.terms[(b2, b3)]:
-                            k = kron_op(o1, o2, p1, p2)
-                            k = SiteOp({kk: vv * (s1 * s2) for kk, vv in k.blocks.items()}, name=k.name)
-                            if acc is None:
-                                acc = k
-                            else:
-                                for kk, vv in k.blocks.items():
-                                    acc.blocks[kk] = acc.blocks.get(kk, 0) + vv
-                acc.blocks = {k: v for k, v in acc.blocks.items() if np.any(v != 0)}
-                if acc.blocks:
-                    terms[(b1, b3)] = [(acc, 1.0)]
+    # summands of every (b1, b3) in increasing b2, from the sparse entry lists
+    out1, out2 = {}, {}
+    for (b1, b2) in W1.terms:
+        out1.setdefault(b1, []).append(b2)
+    for (b2, b3) in W2.terms:
+        out2.setdefault(b2, []).append(b3)
+    paths = {}
+    for b1 in sorted(out1):
+        for b2 in sorted(out1[b1]):
+            for b3 in out2.get(b2, ()):
+                paths.setdefault((b1, b3), []).append(b2)
+    for (b1, b3) in sorted(paths):
+        summands = sorted(paths[(b1, b3)])
+        if not merge:
+            lst, src = [], []
+            for b2 in summands:
+                for j1, (o1, s1) in enumerate(W1.terms[(b1, b2)]):
+                    for j2, (o2, s2) in enumerate(W2.terms[(b2, b3)]):
+                        lst.append((kron_op(o1, o2, p1, p2), s1 * s2))
+                        src.append(((b1, b2, j1), (b2, b3, j2)))
+            terms[(b1, b3)] = lst
+            sources[(b1, b3)] = src
+            continue
+        if len(summands) == 1 and len(W1.terms[(b1, summands[0])]) == 1 and len(W2.terms[(summands[0], b3)]) == 1:
+            (o1, s1), = W1.terms[(b1, summands[0])]
+            (o2, s2), = W2.terms[(summands[0], b3)]
+            terms[(b1, b3)] = [(kron_op(o1, o2, p1, p2), s1 * s2)]
+        else:
+            acc = None
+            for b2 in summands:
+                for o1, s1 in W1.terms[(b1, b2)]:
+                    for o2, s2 in W2.terms[(b2, b3)]:
+                        k = kron_op(o1, o2, p1, p2)
+                        k = SiteOp({kk: vv * (s1 * s2) for kk, vv in k.blocks.items()}, name=k.name)
+                        if acc is None:
+                            acc = k
+                        else:
+                            for kk, vv in k.blocks.items():
+                                acc.blocks[kk] = acc.blocks.get(kk, 0) + vv
+            acc.blocks = {k: v for k, v in acc.blocks.items() if np.any(v != 0)}
+            if acc.blocks:
+                terms[(b1, b3)] = [(acc, 1.0)]
     W = MPOTensor(W1.row_dim, W2.col_dim, terms, W1.left_herm, W1.left_phase, W2.right_herm, W2.right_phase,
                   W1.left_spin, W2.right_spin)
     if not merge:

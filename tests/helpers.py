@@ -54,9 +54,11 @@ class OracleChain:
 
 
 def make_chain(name, L, Mmax, seed=0, synthetic_m=None):
+    from dmrgb200 import qc
     model = {"heisenberg": lambda: M.heisenberg(L),
              "hubbard": lambda: M.fermi_hubbard(L),
-             "bose": lambda: M.bose_hubbard(L, N=L // 2)}[name]()
+             "bose": lambda: M.bose_hubbard(L, N=L // 2),
+             "qc": lambda: qc.quantum_chemistry(L, L // 2, L // 2)}[name]()
     rng = np.random.default_rng(seed)
     if synthetic_m is None:
         bonds = S.allowed_sectors(model.phys, L, model.total_charge, Mmax)

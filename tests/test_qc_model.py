@@ -39,3 +39,29 @@ def test_qc_heff_matches_dense(i):
     P = D.embedding(tensors[:i], tensors[i + 2:], model.phys, model.phys, ch.left, ch.right, ch.p12)
     yd = P.T @ (H @ (P @ psi.data))
     assert np.linalg.norm(y - yd) <= 1e-12 * np.linalg.norm(yd)
+
+
+# integrals whose every operator sits at or left of the centre pair (sites 1, 2 of
+# L = 5): their coefficient is placed in the centre MPO tensors, so the local
+# adjoint gives the whole derivative, a 1- or 2-RDM element of the embedded state
+LOCAL_INTEGRALS = [("h", (1, 2)), ("h", (1, 1)), ("h", (2, 2)), ("h", (0, 2)),
+                   ("eri", (1, 1, 2, 2)), ("eri", (1, 2, 1, 2)), ("eri", (0, 1, 2, 2)), ("eri", (2, 2, 2, 2))]
+
+
+@pytest.mark.parametrize("which,index", LOCAL_INTEGRALS)
+def test_qc_integral_derivative_is_local_rdm(which, index):
+    import dataclasses
+
+    import oracle as O
+    from helpers import qc_integral_derivative
+    L, i = 5, 1
+    model, bonds, tensors, rng = make_chain("qc", L, 16, seed=12)
+    ch = OracleChain(model, bonds, tensors, i)
+    psi = random_psi(ch.p12, ch.left, ch.right, rng).data
+    _, ga = O.hpsi_adjoint(ch.sched.plan, ch.Lval, ch.Lidx, ch.Rval, ch.Ridx, psi, psi)
+    grad, terms = qc_integral_derivative(model, L, i, ch, ga, which, index)
+    P = D.embedding(tensors[:i], tensors[i + 2:], model.phys, model.phys, ch.left, ch.right, ch.p12)
+    v = P @ psi
+    Op = D.sparse_hamiltonian(dataclasses.replace(model, dense_terms=terms), L)
+    expect = v @ (Op @ v)
+    assert abs(grad - expect) <= 1e-11 * max(1.0, abs(expect)), (which, index, grad, expect)

@@ -268,6 +268,62 @@ def gemm_workload(args):
                       "fp64_dmma_peak": peak.value}), flush=True)
 
 
+def qc_workload(args):
+    """Quantum-chemistry site problem (BASELINE config 3 in TwoU1 form; SU2U1 is not
+    built): synthetic integrals (h seed 3, ERI seed 4, 2 L auxiliary vectors), L
+    orbitals at half filling, bond dimension m, middle two-site H·psi with
+    device-built boundaries; FP64 and emulated FP64 (7 slices) timed with L2 flushes."""
+    import torch
+
+    from dmrgb200 import _capi as capi
+    from dmrgb200 import engine as E
+    from dmrgb200 import mps as S
+    from dmrgb200 import qc
+
+    L, m = args.qc_sites, args.qc_m
+    t0 = time.perf_counter()
+    model = qc.quantum_chemistry(L, L // 2, L // 2)
+    bonds = S.synthetic_bonds(model.phys, L, model.total_charge, m, RADIUS)
+    rng = np.random.default_rng(SEED)
+    tensors = S.random_mps(model.phys, bonds, rng)
+    ctx = E.Context(0)
+    i = L // 2 - 1
+    sp = E.SiteProblem(ctx, model, tensors, bonds, i)
+    setup_s = time.perf_counter() - t0
+    x = torch.rand(sp.size, dtype=torch.float64, device="cuda")
+    y = torch.zeros_like(x)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    res = {}
+    for name, prec in (("fp64", capi.PREC_FP64), ("emulated", capi.PREC_FP64_EMULATED)):
+        for _ in range(args.warmup):
+            sp.plan.hpsi(x.data_ptr(), y.data_ptr(), prec)
+        torch.cuda.synchronize()
+        ts = []
+        for k in range(min(args.steps, 10)):
+            flush.fill_(float(k))
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            sp.plan.hpsi(x.data_ptr(), y.data_ptr(), prec)
+            b.record()
+            b.synchronize()
+            ts.append(a.elapsed_time(b))
+        ms = statistics.mean(ts)
+        res[name] = {"ms_per_step": ms, "value": sp.plan.flops / (ms * 1e-3) / 1e9, "unit": "GFLOP/s"}
+        if name == "fp64":
+            y64 = y.clone()
+        else:
+            res[name]["rel_err_vs_fp64"] = float(torch.linalg.norm(y - y64) / torch.linalg.norm(y64))
+    W = sp.W12
+    line = {"metric": "QC H·psi GFLOP/s (FP64)", "value": res["fp64"]["value"], "unit": "GFLOP/s",
+            "higher_is_better": True, "n_gpus": 1, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"qc_L{L}_twou1_m{m}_twosite_hpsi_middle", "sites": L, "bond_dim": m,
+                       "symmetry": "TwoU1", "mpo_bond_dim_two_site": [W.row_dim, W.col_dim],
+                       "psi_elements": int(sp.size), "flops_per_step": int(sp.plan.flops),
+                       "setup_seconds": setup_s, "l2": "flushed (256 MiB write)"},
+            "fp64": res["fp64"], "emulated": res["emulated"]}
+    print(json.dumps(line), flush=True)
+
+
 def batched_workload(args):
     """64 independent site problems (32 Heisenberg U1, 32
     Fermi-Hubbard TwoU1, chains of 32 sites, middle two-site problem), bond
@@ -329,10 +385,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap.add_argument("--workload", default="hpsi", choices=["hpsi", "sweep", "batched", "solve", "gemm"],
+    ap.add_argument("--workload", default="hpsi", choices=["hpsi", "sweep", "batched", "solve", "gemm", "qc"],
                     help="hpsi: the headline H·psi line (default); sweep: config-1 sweeps; batched: config-5; "
                          "solve: Jacobi-Davidson solves of the config-2 site problem; gemm: the DMMA kernel on "
-                         "a regular 4096^3 GEMM")
+                         "a regular 4096^3 GEMM; qc: a quantum-chemistry site problem")
+    ap.add_argument("--qc-sites", type=int, default=24, help="orbitals of the qc workload")
+    ap.add_argument("--qc-m", type=int, default=2000, help="bond dimension of the qc workload")
     ap.add_argument("--prec", default="fp64", choices=["fp64", "emulated"],
                     help="precision of the --profile steps")
     ap.add_argument("--profile", action="store_true",
@@ -351,6 +409,9 @@ def main():
         os._exit(0)
     if args.workload == "gemm":
         gemm_workload(args)
+        os._exit(0)
+    if args.workload == "qc":
+        qc_workload(args)
         os._exit(0)
 
     rank = int(os.environ.get("RANK", "0"))

@@ -294,10 +294,13 @@ def qc_workload(args):
     y = torch.zeros_like(x)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     res = {}
+    import ctypes as C
     for name, prec in (("fp64", capi.PREC_FP64), ("emulated", capi.PREC_FP64_EMULATED)):
         for _ in range(args.warmup):
             sp.plan.hpsi(x.data_ptr(), y.data_ptr(), prec)
         torch.cuda.synchronize()
+        if name == "fp64":
+            capi.check(capi.lib.dmrgb200_plan_set_timing(sp.plan.handle, 1), "set_timing")
         ts = []
         for k in range(min(args.steps, 10)):
             flush.fill_(float(k))
@@ -311,6 +314,12 @@ def qc_workload(args):
         res[name] = {"ms_per_step": ms, "value": sp.plan.flops / (ms * 1e-3) / 1e9, "unit": "GFLOP/s"}
         if name == "fp64":
             y64 = y.clone()
+            ms3, fl3, calls = (C.c_double * 3)(), (C.c_uint64 * 3)(), C.c_uint64()
+            capi.check(capi.lib.dmrgb200_plan_stage_times(sp.plan.handle, ms3, fl3, C.byref(calls)), "stage_times")
+            capi.check(capi.lib.dmrgb200_plan_set_timing(sp.plan.handle, 0), "set_timing")
+            nc = max(int(calls.value), 1)
+            res[name]["stage_ms"] = [ms3[k] / nc for k in range(3)]
+            res[name]["stage_gflop"] = [fl3[k] / 1e9 for k in range(3)]
         else:
             res[name]["rel_err_vs_fp64"] = float(torch.linalg.norm(y - y64) / torch.linalg.norm(y64))
     W = sp.W12

@@ -308,9 +308,11 @@ __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb
 // S build: S is tiled by cells (one per unit and MPO row block); a cell with a
 // line writes the alpha-weighted sum of its T sources (summed in term order like
 // the reference's axpy sequence), a cell without one writes zeros, so S needs
-// no separate clearing.  A line's terms are staged in shared memory first, so
-// the T loads of one element do not wait on each other.
-constexpr int SB_TERMS = 64;
+// no separate clearing.  Every thread owns up to SB_EPT elements of a line (a
+// column-major walk in steps of blockDim.x, without per-element division) and
+// the line's terms pass through shared memory in chunks of SB_TERMS, so each
+// term costs SB_EPT independent loads per thread.
+constexpr int SB_TERMS = 256, SB_EPT = 4;
 __global__ void __launch_bounds__(256) sbuild_lines(const DevSLine* __restrict__ lines,
                                                     const DevSTerm* __restrict__ terms, uint32_t n_lines,
                                                     double* __restrict__ S, const double* __restrict__ T) {
@@ -318,47 +320,51 @@ __global__ void __launch_bounds__(256) sbuild_lines(const DevSLine* __restrict__
     __shared__ uint64_t s_base[SB_TERMS];
     for (uint32_t li = blockIdx.x; li < n_lines; li += gridDim.x) {
         const DevSLine L = lines[li];
-        const uint32_t nt = L.term_end - L.term_begin;
-        const bool staged = nt <= SB_TERMS;
-        __syncthreads();  // the previous line's readers are done
-        if (staged && threadIdx.x < nt) {
-            const DevSTerm tm = terms[L.term_begin + threadIdx.x];
-            s_alpha[threadIdx.x] = tm.alpha;
-            s_base[threadIdx.x] = tm.t_base;
-        }
-        __syncthreads();
-        // element (i, c) walks the line column-major in steps of blockDim.x without
-        // per-element division
-        if (!L.rows) continue;
+        if (!L.rows || !L.cols) continue;
+        const uint32_t n = L.rows * L.cols;
         const uint32_t di = blockDim.x % L.rows, dc = blockDim.x / L.rows;
-        uint32_t i = threadIdx.x % L.rows, c = threadIdx.x / L.rows;
-        while (c < L.cols) {
-            const uint64_t off = i + uint64_t(c) * L.ld_t;
-            double v = 0.0;
-            if (staged) {
-                uint32_t t = 0;
-                for (; t + 4 <= nt; t += 4) {
-                    const double x0 = T[s_base[t] + off], x1 = T[s_base[t + 1] + off];
-                    const double x2 = T[s_base[t + 2] + off], x3 = T[s_base[t + 3] + off];
-                    v += s_alpha[t] * x0;
-                    v += s_alpha[t + 1] * x1;
-                    v += s_alpha[t + 2] * x2;
-                    v += s_alpha[t + 3] * x3;
-                }
-                for (; t < nt; ++t) v += s_alpha[t] * T[s_base[t] + off];
-            } else {
-                for (uint32_t t = L.term_begin; t < L.term_end; ++t) {
-                    const DevSTerm tm = terms[t];
-                    v += tm.alpha * T[tm.t_base + off];
+        // this thread's first element of the line
+        uint32_t i0 = threadIdx.x % L.rows, c0 = threadIdx.x / L.rows;
+        for (uint32_t base = 0; base < n; base += SB_EPT * blockDim.x) {
+            uint64_t toff[SB_EPT], soff[SB_EPT];
+            bool in[SB_EPT];
+            double v[SB_EPT];
+            uint32_t i = i0, c = c0;
+#pragma unroll
+            for (int u = 0; u < SB_EPT; ++u) {
+                in[u] = c < L.cols;
+                toff[u] = i + uint64_t(c) * L.ld_t;
+                soff[u] = L.s_base + i + uint64_t(c) * L.ld_s;
+                v[u] = 0.0;
+                i += di;
+                c += dc;
+                if (i >= L.rows) {
+                    i -= L.rows;
+                    ++c;
                 }
             }
-            S[L.s_base + i + uint64_t(c) * L.ld_s] = v;
-            i += di;
-            c += dc;
-            if (i >= L.rows) {
-                i -= L.rows;
-                ++c;
+            i0 = i;
+            c0 = c;
+            for (uint32_t t0 = L.term_begin; t0 < L.term_end; t0 += SB_TERMS) {
+                const uint32_t nt = min(uint32_t(SB_TERMS), L.term_end - t0);
+                __syncthreads();  // readers of the previous chunk are done
+                if (threadIdx.x < nt) {
+                    const DevSTerm tm = terms[t0 + threadIdx.x];
+                    s_alpha[threadIdx.x] = tm.alpha;
+                    s_base[threadIdx.x] = tm.t_base;
+                }
+                __syncthreads();
+                for (uint32_t t = 0; t < nt; ++t) {
+                    const double a = s_alpha[t];
+                    const uint64_t b = s_base[t];
+#pragma unroll
+                    for (int u = 0; u < SB_EPT; ++u)
+                        if (in[u]) v[u] += a * T[b + toff[u]];
+                }
             }
+#pragma unroll
+            for (int u = 0; u < SB_EPT; ++u)
+                if (in[u]) S[soff[u]] = v[u];
         }
     }
 }

@@ -128,3 +128,23 @@ def test_stage_timing_reports(ctx):
     calls = C.c_uint64()
     capi.check(capi.lib.dmrgb200_plan_stage_times(plan.handle, ms, fl, C.byref(calls)), "stage_times")
     assert calls.value == 3 and all(v > 0 for v in ms) and sum(fl) == plan.flops
+
+
+def test_autotuned_variants_give_identical_results(ctx):
+    """Every grouped-GEMM variant sums in the same order: H·psi after an explicit
+    re-tune (whatever variants it picks) equals the default-variant result bitwise."""
+    import ctypes as C
+
+    from dmrgb200 import _capi as capi
+    model, bonds, tensors, rng = make_chain("hubbard", 16, 0, seed=17, synthetic_m=96)
+    ch = OracleChain(model, bonds, tensors, 7)
+    y0, keep = _gpu_hpsi(ctx, ch, random_psi(ch.p12, ch.left, ch.right, rng).data)
+    plan, Lb, Rb, xd, yd = keep
+    chosen = (C.c_int32 * 2)()
+    capi.check(capi.lib.dmrgb200_plan_autotune(plan.handle, xd.data_ptr(), yd.data_ptr(), None, chosen), "autotune")
+    assert all(0 <= v < 15 for v in chosen)
+    assert capi.lib.dmrgb200_gemm_variant_name(chosen[0]).startswith(b"tile")
+    yd.zero_()
+    plan.hpsi(xd.data_ptr(), yd.data_ptr())
+    torch.cuda.synchronize()
+    assert np.array_equal(y0, yd.cpu().numpy())

@@ -36,24 +36,6 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
                  : "d"(a), "d"(b));
 }
 
-// D += A B on 16 x 8 x 16 and 16 x 8 x 8 FP64 tensor-core tiles.  Fragments per
-// lane (g = lane / 4, q = lane % 4): a[v0 + 2 v1] = A(g + 8 v0, q + 4 v1),
-// b[v] = B(q + 4 v, g), d[e + 2 h] = D(g + 8 h, 2 q + e).
-__device__ __forceinline__ void mma16x8x16(double (&d)[4], const double (&a)[8], const double (&b)[4]) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
-        "{%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
-        : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
-        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]),
-          "d"(b[1]), "d"(b[2]), "d"(b[3]));
-}
-__device__ __forceinline__ void mma16x8x8(double (&d)[4], const double (&a)[4], const double (&b)[2]) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-        : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
-        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
-}
-
 // 8-byte asynchronous global->shared copy; src_bytes = 0 writes a zero (out-of-range element).
 __device__ __forceinline__ void cp_async8(double* smem, const double* gmem, bool valid) {
     unsigned saddr = static_cast<unsigned>(__cvta_generic_to_shared(smem));
@@ -134,8 +116,8 @@ __device__ __forceinline__ void load_tile(double (*As)[BM_ + 4], double (*Bs)[LD
 // tiles (BM_ x 64) and walks every K step (BK_ deep) of every segment of its
 // problem; the CTA's K steps over all its tiles form one stream, so the
 // cp.async pipeline (STAGES deep) keeps loading the next tile's operands while
-// the current tile finishes and stores.  4 warps: 2 x 2 of (BM_/2) x 32 (BM_ =
-// 32, 64) or 1 x 4 of 16 x 16 (BM_ = 16), DMMA m8n8k4.  A tile whose segments are all
+// the current tile finishes and stores.  Warps: 2 x 2 of (BM_/2) x 32 (BM_ = 32,
+// 64), or for BM_ = 16 a row of 16 x (64 / warps), DMMA m8n8k4.  A tile whose segments are all
 // empty (one step, no copies) stores zeros.
 struct LoadCursor {
     uint32_t ti, seg, seg_end, k0;
@@ -144,7 +126,7 @@ struct LoadCursor {
     uint32_t ald;
 };
 
-template <int BM_, int BK_, int STAGES, int MINB, bool BIG, int NTHREADS>
+template <int BM_, int BK_, int STAGES, int MINB, int NTHREADS>
 __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb* __restrict__ probs,
                                                                    const DevSeg* __restrict__ segs,
                                                                    const DevTile* __restrict__ tiles, uint32_t n_tiles,
@@ -152,8 +134,7 @@ __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb
     // warps: 2 x 2 for BM_ >= 32 (warp tiles BM_/2 x 32), 1 x 4 for BM_ = 16 (16 x 16)
     constexpr int WARPS_M = BM_ >= 32 ? 2 : 1, WM = BM_ / WARPS_M;
     constexpr int WN = BN / (NTHREADS / 32 / WARPS_M), NJ = WN / 8;
-    // accumulator tiles: 16 x 8 (BIG: m16n8k16 / m16n8k8 MMAs) or 8 x 8 (m8n8k4)
-    constexpr int MI = BIG ? WM / 16 : WM / 8, AE = BIG ? 4 : 2;
+    constexpr int MI = WM / 8;  // 8 x 8 accumulator tiles (m8n8k4)
     __shared__ __align__(16) double As[STAGES][BK_][BM_ + 4];
     __shared__ __align__(16) double Bs[STAGES][BK_][LDB_S];
 
@@ -211,13 +192,11 @@ __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb
         cp_async_commit();
     }
 
-    double acc[MI][NJ][AE];
+    double acc[MI][NJ][2];
 #pragma unroll
     for (int i = 0; i < MI; ++i)
 #pragma unroll
-        for (int j = 0; j < NJ; ++j)
-#pragma unroll
-            for (int e = 0; e < AE; ++e) acc[i][j][e] = 0.0;
+        for (int j = 0; j < NJ; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
     // ---- consumer: tiles in the same order, nsteps K steps each ----
     int slot = 0;
@@ -228,44 +207,17 @@ __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb
             cp_async_commit();
             cp_async_wait<STAGES - 1>();
             __syncthreads();
-            if constexpr (BIG) {
-                // one m16n8k(BK_) MMA per 16 x 8 accumulator tile; row k = q + 4 v of the
-                // K step sits behind swizzle constant v
-                constexpr int KV = BK_ / 4;
-                double b[NJ][KV];
 #pragma unroll
-                for (int j = 0; j < NJ; ++j)
+            for (int kk = 0; kk < BK_; kk += 4) {
+                double a[MI], b[NJ];
 #pragma unroll
-                    for (int v = 0; v < KV; ++v) b[j][v] = Bs[slot][q + 4 * v][(wn + j * 8 + g) ^ v];
+                for (int i = 0; i < MI; ++i) a[i] = As[slot][kk + q][(wm + i * 8 + g) ^ (kk >> 2)];
 #pragma unroll
-                for (int i = 0; i < MI; ++i) {
-                    double a[2 * KV];
+                for (int j = 0; j < NJ; ++j) b[j] = Bs[slot][kk + q][(wn + j * 8 + g) ^ (kk >> 2)];
 #pragma unroll
-                    for (int v = 0; v < KV; ++v) {
-                        a[2 * v] = As[slot][q + 4 * v][(wm + i * 16 + g) ^ v];
-                        a[2 * v + 1] = As[slot][q + 4 * v][(wm + i * 16 + 8 + g) ^ v];
-                    }
+                for (int i = 0; i < MI; ++i)
 #pragma unroll
-                    for (int j = 0; j < NJ; ++j) {
-                        if constexpr (BK_ == 16)
-                            mma16x8x16(acc[i][j], a, b[j]);
-                        else
-                            mma16x8x8(acc[i][j], a, b[j]);
-                    }
-                }
-            } else {
-#pragma unroll
-                for (int kk = 0; kk < BK_; kk += 4) {
-                    double a[MI], b[NJ];
-#pragma unroll
-                    for (int i = 0; i < MI; ++i) a[i] = As[slot][kk + q][(wm + i * 8 + g) ^ (kk >> 2)];
-#pragma unroll
-                    for (int j = 0; j < NJ; ++j) b[j] = Bs[slot][kk + q][(wn + j * 8 + g) ^ (kk >> 2)];
-#pragma unroll
-                    for (int i = 0; i < MI; ++i)
-#pragma unroll
-                        for (int j = 0; j < NJ; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
-                }
+                    for (int j = 0; j < NJ; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
             }
             __syncthreads();
             slot = (slot + 1) % STAGES;
@@ -281,9 +233,8 @@ __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb
         double* C = const_cast<double*>(op_base(bases, pr.C, tl.batch));
         const uint64_t ldc = pr.C.ld;
 #pragma unroll
-        for (int ih = 0; ih < MI * (AE / 2); ++ih) {
-            const int i = ih / (AE / 2), h = ih % (AE / 2);  // accumulator tile, row half
-            const uint32_t r = tl.m0 + wm + i * (8 * AE / 2) + 8 * h + g;
+        for (int i = 0; i < MI; ++i) {
+            const uint32_t r = tl.m0 + wm + i * 8 + g;
             // the row's start and leading dimension: from the row table or the plain operand
             double* crow = C + r;
             uint64_t ld = ldc;
@@ -297,8 +248,8 @@ __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb
 #pragma unroll
                 for (int e = 0; e < 2; ++e) {
                     uint32_t c = tl.n0 + wn + j * 8 + q * 2 + e;
-                    if (r < pr.M && c < pr.N) crow[c * ld] = empty ? 0.0 : acc[i][j][2 * h + e];
-                    acc[i][j][2 * h + e] = 0.0;
+                    if (r < pr.M && c < pr.N) crow[c * ld] = empty ? 0.0 : acc[i][j][e];
+                    acc[i][j][e] = 0.0;
                 }
         }
     }
@@ -792,21 +743,18 @@ struct GemmVariant {
     int threads;     // CTA size
 };
 const GemmVariant kVariants[N_GEMM_VARIANTS] = {
-    {gemm_f64_grouped<32, 16, 2, 4, false, 128>, "tile32x64_k16_stages2_ctas4", 0, 128},
-    {gemm_f64_grouped<32, 16, 3, 4, false, 128>, "tile32x64_k16_stages3_ctas4", 0, 128},
-    {gemm_f64_grouped<32, 16, 2, 5, false, 128>, "tile32x64_k16_stages2_ctas5", 0, 128},
-    {gemm_f64_grouped<32, 16, 3, 5, false, 128>, "tile32x64_k16_stages3_ctas5", 0, 128},
-    {gemm_f64_grouped<16, 8, 3, 6, false, 128>, "tile16x64_k8_stages3_ctas6", 1, 128},
-    {gemm_f64_grouped<16, 8, 4, 8, false, 128>, "tile16x64_k8_stages4_ctas8", 1, 128},
-    {gemm_f64_grouped<64, 16, 2, 3, false, 128>, "tile64x64_k16_stages2_ctas3", 2, 128},
-    {gemm_f64_grouped<64, 16, 2, 2, false, 128>, "tile64x64_k16_stages2_ctas2", 2, 128},
-    {gemm_f64_grouped<32, 16, 2, 4, true, 128>, "tile32x64_k16_stages2_ctas4_mma16", 0, 128},
-    {gemm_f64_grouped<64, 16, 2, 3, true, 128>, "tile64x64_k16_stages2_ctas3_mma16", 2, 128},
-    {gemm_f64_grouped<16, 16, 2, 8, false, 64>, "tile16x64_k16_warps2_stages2_ctas8", 3, 64},
-    {gemm_f64_grouped<16, 16, 3, 8, false, 64>, "tile16x64_k16_warps2_stages3_ctas8", 3, 64},
-    {gemm_f64_grouped<16, 16, 2, 10, false, 64>, "tile16x64_k16_warps2_stages2_ctas10", 3, 64},
-    {gemm_f64_grouped<16, 16, 3, 10, false, 64>, "tile16x64_k16_warps2_stages3_ctas10", 3, 64},
-    {gemm_f64_grouped<16, 16, 2, 8, true, 64>, "tile16x64_k16_warps2_stages2_ctas8_mma16", 3, 64},
+    {gemm_f64_grouped<32, 16, 2, 4, 128>, "tile32x64_k16_stages2_ctas4", 0, 128},
+    {gemm_f64_grouped<32, 16, 3, 4, 128>, "tile32x64_k16_stages3_ctas4", 0, 128},
+    {gemm_f64_grouped<32, 16, 2, 5, 128>, "tile32x64_k16_stages2_ctas5", 0, 128},
+    {gemm_f64_grouped<32, 16, 3, 5, 128>, "tile32x64_k16_stages3_ctas5", 0, 128},
+    {gemm_f64_grouped<16, 8, 3, 6, 128>, "tile16x64_k8_stages3_ctas6", 1, 128},
+    {gemm_f64_grouped<16, 8, 4, 8, 128>, "tile16x64_k8_stages4_ctas8", 1, 128},
+    {gemm_f64_grouped<64, 16, 2, 3, 128>, "tile64x64_k16_stages2_ctas3", 2, 128},
+    {gemm_f64_grouped<64, 16, 2, 2, 128>, "tile64x64_k16_stages2_ctas2", 2, 128},
+    {gemm_f64_grouped<16, 16, 2, 8, 64>, "tile16x64_k16_warps2_stages2_ctas8", 3, 64},
+    {gemm_f64_grouped<16, 16, 3, 8, 64>, "tile16x64_k16_warps2_stages3_ctas8", 3, 64},
+    {gemm_f64_grouped<16, 16, 2, 10, 64>, "tile16x64_k16_warps2_stages2_ctas10", 3, 64},
+    {gemm_f64_grouped<16, 16, 3, 10, 64>, "tile16x64_k16_warps2_stages3_ctas10", 3, 64},
 };
 
 int variant_occupancy(int v) {

@@ -296,8 +296,12 @@ def qc_workload(args):
     res = {}
     import ctypes as C
     for name, prec in (("fp64", capi.PREC_FP64), ("emulated", capi.PREC_FP64_EMULATED)):
-        for _ in range(args.warmup):
-            sp.plan.hpsi(x.data_ptr(), y.data_ptr(), prec)
+        try:
+            for _ in range(args.warmup):
+                sp.plan.hpsi(x.data_ptr(), y.data_ptr(), prec)
+        except capi.DmrgError as exc:  # reported, not hidden (e.g. a contraction beyond the INT32 range)
+            res[name] = {"unavailable": str(exc)}
+            continue
         torch.cuda.synchronize()
         if name == "fp64":
             capi.check(capi.lib.dmrgb200_plan_set_timing(sp.plan.handle, 1), "set_timing")

@@ -221,7 +221,7 @@ dmrgb200_status finish_plan(std::unique_ptr<dmrgb200_plan_s>& p, dmrgb200_plan_t
     if (!err.empty()) return fail(DMRGB200_INVALID_PLAN, err);
     cudaGetDevice(&p->device);
     if (p->flat.kind == KIND_HPSI) {
-        compile_program(p->flat, p->stage3_bnd, p->stage1_bnd, {}, p->prog, true);
+        compile_program(p->flat, p->stage3_bnd, p->stage1_bnd, {}, p->prog, true, true);
         cudaError_t e = upload_program(p->prog);
         if (e != cudaSuccess) {
             free_program(p->prog);
@@ -248,7 +248,7 @@ dmrgb200_status run_step(dmrgb200_plan_s* p, const double* ket, const double* br
         if (p->flat.c_out_ci[c] >= outp.size() || !outp[p->flat.c_out_ci[c]])
             return fail(DMRGB200_INVALID_ARGUMENT, "output boundary view misses a cohort");
     DeviceProgram prog;
-    compile_program(p->flat, {}, p->stage1_bnd, outp, prog);
+    compile_program(p->flat, {}, p->stage1_bnd, outp, prog, false, true);
     cudaError_t e = upload_program(prog);
     if (e != cudaSuccess) {
         free_program(prog);

@@ -63,6 +63,25 @@ struct DevSTerm {
     uint64_t t_base;
 };
 
+// S build of a unit in line groups: up to SG_LINES lines of consecutive MPO row
+// blocks b1 share one list of source cells (the union of their terms' T
+// slices), each with a column of SG_LINES alphas (zero where a line does not
+// read the cell, duplicate sources of a line summed).  Line j of the group
+// starts at s_base + j * line_stride; element (i, c) of a line sits at
+// i + c * ld_s, its source at t_base + i + c * rows.
+constexpr int SG_LINES = 8;
+struct DevSGroup {
+    uint64_t s_base;
+    uint32_t line_stride, ld_s, rows, cols;
+    uint32_t ent_begin, ent_end;
+    uint32_t mask;  // bit j: line j has terms (the others are written as zeros)
+    uint32_t nlines;
+};
+// one warp's work in the grouped S build: elements e0 .. e0 + 127 of a group
+struct DevSItem {
+    uint32_t group, e0;
+};
+
 enum BufId : uint16_t { BUF_IN = 0, BUF_OUT = 1, BUF_T = 2, BUF_S = 3, BUF_ABS = 4, BUF_W = 5, NBUF = 8 };
 
 struct Bases {
@@ -112,6 +131,11 @@ struct DeviceProgram {
     GemmList stage1, stage3;
     std::vector<DevSLine> lines;
     std::vector<DevSTerm> terms;
+    // units whose lines share sources run as line groups (see DevSGroup)
+    std::vector<DevSGroup> groups;
+    std::vector<uint64_t> gent_t;  // per group entry: source offset in T
+    std::vector<double> gent_a;    // per group entry: SG_LINES alphas
+    std::vector<DevSItem> gitems;  // warp work items, longest groups first
     uint64_t t_elems = 0, s_elems = 0;
 
     // device copies
@@ -123,7 +147,11 @@ struct DeviceProgram {
     DevTile* d_t3 = nullptr;
     DevSLine* d_lines = nullptr;
     DevSTerm* d_terms = nullptr;
-    uint32_t n_t1 = 0, n_t3 = 0, n_lines = 0;
+    DevSGroup* d_groups = nullptr;
+    uint64_t* d_gent_t = nullptr;
+    double* d_gent_a = nullptr;
+    DevSItem* d_gitems = nullptr;
+    uint32_t n_t1 = 0, n_t3 = 0, n_lines = 0, n_gitems = 0;
     TileLists x1, x3;  // tile lists of the other classes
     DevRow* d_r1 = nullptr;  // stage-1 row table (stacked T tasks)
     GemmList stage1_tasks;   // stage 1 as one problem per T task (when stage1 is stacked)
@@ -138,8 +166,13 @@ struct DeviceProgram {
 // stack_rows: stage 1 of H psi / right step as one row-table problem per set of
 // T tasks that share their boundary cohort (rows of all those tasks stacked);
 // the per-task list is kept in prog.stage1_tasks.
+// group_lines: a unit whose lines share enough sources runs its S build as line
+// groups (DevSGroup) when that issues at most twice the multiply-adds of the
+// per-line walk; DMRGB200_SBUILD=lines / groups in the environment forces one
+// form for every unit.
 void compile_program(FlatPlan const& p, std::vector<uint64_t> const& stage3_bnd, std::vector<uint64_t> const& stage1_bnd,
-                     std::vector<uint64_t> const& outptr, DeviceProgram& prog, bool stack_rows = false);
+                     std::vector<uint64_t> const& outptr, DeviceProgram& prog, bool stack_rows = false,
+                     bool group_lines = false);
 cudaError_t upload_program(DeviceProgram& prog);
 void free_program(DeviceProgram& prog);
 

@@ -11,10 +11,13 @@
 // mma.sync.m8n8k4.f64 (DMMA) on 64x64x16 CTA tiles, 4 warps of 32x32.
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
+#include <cstring>
 #include <map>
 #include <numeric>
 #include <tuple>
 #include <string>
+#include <unordered_map>
 
 #include "../../include/dmrgb200.h"
 #include "device.hpp"
@@ -48,10 +51,6 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
-struct TileCursor {
-    uint32_t seg, k0;
-};
-
 // Shared-memory column swizzle of the operand tiles: row k stores column c at
 // c ^ ((k >> 2) & 3).  With row pitches of 8 words mod 32, copies in which
 // consecutive threads take consecutive k (the coalesced order for K-contiguous
@@ -59,56 +58,76 @@ struct TileCursor {
 // step (one XOR constant) stay conflict-free.
 __device__ __forceinline__ int swz(int k) { return (k >> 2) & 3; }
 
-// Issue the copies of one K tile (segment sg, rows k0..k0+BK_) into stage buffers.
-// arow (row-table problems): this thread's A row (its m is tid % BM_ in every
-// copy), NULL beyond the problem's rows; ald its leading dimension.
-template <int BM_, int BK_, int NTHREADS>
-__device__ __forceinline__ void load_tile(double (*As)[BM_ + 4], double (*Bs)[LDB_S], DevSeg const& sg,
-                                          const double* A, const double* B, uint32_t m0, uint32_t n0, uint32_t M,
-                                          uint32_t N, uint32_t k0, int tid, bool rowmode, const double* arow,
-                                          uint32_t ald) {
-    const uint64_t lda = sg.A.ld, ldb = sg.B.ld;
-    const uint32_t K = sg.K;
-    if (rowmode) {
+// One thread's copies of one operand tile over the K steps of a segment.  The
+// operand tile is ROWS (m or n) x BK_ (k), stored in shared memory as
+// [k][ROWS + pad]; a thread issues NC = ROWS * BK_ / NTHREADS 8-byte copies per
+// K step.  When the operand's contiguous global dimension is m or n
+// ("row-major copies": A not transposed or read through the row table, B
+// transposed), the thread's copies share one row r = tid % ROWS and take
+// k = kt + j * (NTHREADS / ROWS); otherwise they share k = kt = tid % BK_ and
+// take rows r + j * (NTHREADS / BK_).  Copy j reads base + j * jstride; every
+// K step advances base by kstep.  All byte strides, fixed per segment.
+struct CopyStream {
+    const char* base;
+    const char* safe;  // a readable address for copies that fetch nothing
+    uint64_t jstride, kstep;
+    uint32_t mask;  // bit j: copy j's row lies inside the problem
+    uint32_t r, kt;
+    bool rowmajor;
+};
+
+template <int ROWS, int BK_, int NTHREADS, int LD>
+__device__ __forceinline__ void issue_copies(double* tile, CopyStream& cs, uint32_t krem) {
+    constexpr int NC = ROWS * BK_ / NTHREADS;
+    if (cs.rowmajor) {
+        constexpr int KJ = NTHREADS / ROWS;
 #pragma unroll
-        for (int j = 0; j < (BM_ * BK_) / NTHREADS; ++j) {
-            const int idx = tid + j * NTHREADS, m = idx % BM_, k = idx / BM_;
-            const uint32_t gk = k0 + k;
-            const bool ok = arow != nullptr && gk < K;
-            cp_async8(&As[k][m ^ swz(k)], ok ? arow + uint64_t(gk) * ald : B, ok);
+        for (int j = 0; j < NC; ++j) {
+            const uint32_t k = cs.kt + j * KJ;
+            const bool ok = ((cs.mask >> j) & 1u) && k < krem;
+            cp_async8(&tile[k * LD + (cs.r ^ swz(k))],
+                      reinterpret_cast<const double*>(ok ? cs.base + j * cs.jstride : cs.safe), ok);
         }
-    } else
+    } else {
+        constexpr int RJ = NTHREADS / BK_;
+        const bool kok = cs.kt < krem;
 #pragma unroll
-    for (int j = 0; j < (BM_ * BK_) / NTHREADS; ++j) {
-        int idx = tid + j * NTHREADS;
-        int m, k;
-        if (!sg.A.trans) {
-            m = idx % BM_;
-            k = idx / BM_;
-        } else {
-            k = idx % BK_;
-            m = idx / BK_;
+        for (int j = 0; j < NC; ++j) {
+            const bool ok = kok && ((cs.mask >> j) & 1u);
+            cp_async8(&tile[cs.kt * LD + ((cs.r + j * RJ) ^ swz(cs.kt))],
+                      reinterpret_cast<const double*>(ok ? cs.base + j * cs.jstride : cs.safe), ok);
         }
-        uint32_t gm = m0 + m, gk = k0 + k;
-        bool ok = gm < M && gk < K;
-        const double* src = ok ? (sg.A.trans ? A + gk + gm * lda : A + gm + gk * lda) : A;
-        cp_async8(&As[k][m ^ swz(k)], src, ok);
     }
+    cs.base += cs.kstep;
+}
+
+// Copy stream of an operand whose element (row, k) sits at elem + row * rs + k * ks
+// (element strides; rows from row0, nrows of them inside the problem).
+template <int ROWS, int BK_, int NTHREADS>
+__device__ __forceinline__ void setup_copies(CopyStream& cs, const double* elem, uint64_t rs, uint64_t ks,
+                                             uint32_t row0, uint32_t nrows, int tid) {
+    constexpr int NC = ROWS * BK_ / NTHREADS;
+    cs.safe = reinterpret_cast<const char*>(elem);
+    cs.rowmajor = rs == 1;
+    if (cs.rowmajor) {
+        constexpr int KJ = NTHREADS / ROWS;
+        cs.r = tid % ROWS;
+        cs.kt = tid / ROWS;
+        cs.base = reinterpret_cast<const char*>(elem + (row0 + cs.r) + cs.kt * ks);
+        cs.jstride = 8ull * KJ * ks;
+        cs.kstep = 8ull * BK_ * ks;
+        cs.mask = row0 + cs.r < nrows ? (1u << NC) - 1u : 0u;
+    } else {
+        constexpr int RJ = NTHREADS / BK_;
+        cs.kt = tid % BK_;
+        cs.r = tid / BK_;
+        cs.base = reinterpret_cast<const char*>(elem + (row0 + cs.r) * rs + cs.kt * ks);
+        cs.jstride = 8ull * RJ * rs;
+        cs.kstep = 8ull * BK_ * ks;
+        cs.mask = 0;
 #pragma unroll
-    for (int j = 0; j < (BN * BK_) / NTHREADS; ++j) {
-        int idx = tid + j * NTHREADS;
-        int n, k;
-        if (!sg.B.trans) {
-            k = idx % BK_;
-            n = idx / BK_;
-        } else {
-            n = idx % BN;
-            k = idx / BN;
-        }
-        uint32_t gn = n0 + n, gk = k0 + k;
-        bool ok = gn < N && gk < K;
-        const double* src = ok ? (sg.B.trans ? B + gn + gk * ldb : B + gk + gn * ldb) : B;
-        cp_async8(&Bs[k][n ^ swz(k)], src, ok);
+        for (int j = 0; j < NC; ++j)
+            if (row0 + cs.r + j * RJ < nrows) cs.mask |= 1u << j;
     }
 }
 
@@ -120,10 +139,8 @@ __device__ __forceinline__ void load_tile(double (*As)[BM_ + 4], double (*Bs)[LD
 // 64), or for BM_ = 16 a row of 16 x (64 / warps), DMMA m8n8k4.  A tile whose segments are all
 // empty (one step, no copies) stores zeros.
 struct LoadCursor {
-    uint32_t ti, seg, seg_end, k0;
-    bool valid, rowmode;
-    const double* arow;  // row-table problems: this thread's A row
-    uint32_t ald;
+    uint32_t ti, seg, seg_end, krem;
+    bool valid;
 };
 
 template <int BM_, int BK_, int STAGES, int MINB, int NTHREADS>
@@ -135,6 +152,7 @@ __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb
     constexpr int WARPS_M = BM_ >= 32 ? 2 : 1, WM = BM_ / WARPS_M;
     constexpr int WN = BN / (NTHREADS / 32 / WARPS_M), NJ = WN / 8;
     constexpr int MI = WM / 8;  // 8 x 8 accumulator tiles (m8n8k4)
+    constexpr int NCA = BM_ * BK_ / NTHREADS;
     __shared__ __align__(16) double As[STAGES][BK_][BM_ + 4];
     __shared__ __align__(16) double Bs[STAGES][BK_][LDB_S];
 
@@ -143,42 +161,65 @@ __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb
     const int wm = (warp % WARPS_M) * WM, wn = (warp / WARPS_M) * WN;
     const int g = lane >> 2, q = lane & 3;
 
-    // ---- producer: walks (tile, segment, k0) and issues one K step per call ----
-    LoadCursor L{blockIdx.x, 0, 0, 0, false, false, nullptr, 0};
+    // ---- producer: walks (tile, segment, K step) and issues one K step per call;
+    // the copy streams are set up once per segment ----
+    LoadCursor L{blockIdx.x, 0, 0, 0, false};
+    CopyStream ca, cb;
+    auto enter_segment = [&]() {
+        while (L.seg < L.seg_end && segs[L.seg].K == 0) ++L.seg;
+        if (L.seg >= L.seg_end) return;
+        const DevTile tl = tiles[L.ti];
+        const DevProb& pr = probs[tl.prob];
+        const DevSeg sg = segs[L.seg];
+        L.krem = sg.K;
+        const double* A = op_base(bases, sg.A, tl.batch);
+        const double* B = op_base(bases, sg.B, tl.batch);
+        if (pr.rows != DevProb::NO_ROWS) {
+            // row-table A: this thread's row (tid % BM_ in every copy) has its own start and stride
+            const uint32_t gm = tl.m0 + uint32_t(tid % BM_);
+            ca.safe = reinterpret_cast<const char*>(B);
+            ca.rowmajor = true;
+            ca.r = tid % BM_;
+            ca.kt = tid / BM_;
+            ca.mask = 0;
+            ca.base = ca.safe;
+            ca.jstride = ca.kstep = 0;
+            if (gm < pr.M) {
+                const DevRow rw = rowtab[pr.rows + gm];
+                ca.base = reinterpret_cast<const char*>(base_of(bases, sg.A.buf) + 8ull * (rw.a_off + uint64_t(ca.kt) * rw.ld));
+                ca.jstride = 8ull * (NTHREADS / BM_) * rw.ld;
+                ca.kstep = 8ull * BK_ * rw.ld;
+                ca.mask = (1u << NCA) - 1u;
+            }
+        } else if (!sg.A.trans) {
+            setup_copies<BM_, BK_, NTHREADS>(ca, A, 1, sg.A.ld, tl.m0, pr.M, tid);
+        } else {
+            setup_copies<BM_, BK_, NTHREADS>(ca, A, sg.A.ld, 1, tl.m0, pr.M, tid);
+        }
+        if (!sg.B.trans)
+            setup_copies<BN, BK_, NTHREADS>(cb, B, sg.B.ld, 1, tl.n0, pr.N, tid);
+        else
+            setup_copies<BN, BK_, NTHREADS>(cb, B, 1, sg.B.ld, tl.n0, pr.N, tid);
+    };
     auto enter_tile = [&]() {
         L.valid = L.ti < n_tiles;
         if (!L.valid) return;
-        const DevTile tl = tiles[L.ti];
-        const DevProb& pr = probs[tl.prob];
+        const DevProb& pr = probs[tiles[L.ti].prob];
         L.seg = pr.seg_begin;
         L.seg_end = pr.seg_end;
-        L.k0 = 0;
-        while (L.seg < L.seg_end && segs[L.seg].K == 0) ++L.seg;
-        L.rowmode = pr.rows != DevProb::NO_ROWS;
-        L.arow = nullptr;
-        if (L.rowmode && L.seg < L.seg_end) {
-            const uint32_t gm = tl.m0 + uint32_t(tid % BM_);
-            if (gm < pr.M) {
-                const DevRow rw = rowtab[pr.rows + gm];
-                L.arow = reinterpret_cast<const double*>(base_of(bases, segs[L.seg].A.buf) + 8ull * rw.a_off);
-                L.ald = rw.ld;
-            }
-        }
+        enter_segment();
     };
     auto issue = [&](int slot) {
         if (!L.valid) return;
         if (L.seg < L.seg_end) {  // an empty tile issues no copies
-            const DevTile tl = tiles[L.ti];
-            const DevProb& pr = probs[tl.prob];
-            const DevSeg sg = segs[L.seg];
-            load_tile<BM_, BK_, NTHREADS>(As[slot], Bs[slot], sg, op_base(bases, sg.A, tl.batch),
-                                op_base(bases, sg.B, tl.batch), tl.m0, tl.n0, pr.M, pr.N, L.k0, tid, L.rowmode,
-                                L.arow, L.ald);
-            L.k0 += BK_;
-            if (L.k0 < sg.K) return;
-            L.k0 = 0;
+            issue_copies<BM_, BK_, NTHREADS, BM_ + 4>(&As[slot][0][0], ca, L.krem);
+            issue_copies<BN, BK_, NTHREADS, LDB_S>(&Bs[slot][0][0], cb, L.krem);
+            if (L.krem > uint32_t(BK_)) {
+                L.krem -= BK_;
+                return;
+            }
             ++L.seg;
-            while (L.seg < L.seg_end && segs[L.seg].K == 0) ++L.seg;
+            enter_segment();
             if (L.seg < L.seg_end) return;
         }
         L.ti += gridDim.x;
@@ -316,6 +357,81 @@ __global__ void __launch_bounds__(256) sbuild_lines(const DevSLine* __restrict__
 #pragma unroll
             for (int u = 0; u < SB_EPT; ++u)
                 if (in[u]) S[soff[u]] = v[u];
+        }
+    }
+}
+
+// S build of line groups (DevSGroup): one warp per work item (a group and a
+// chunk of SG_CHUNK consecutive elements of its lines); every lane owns SG_EPT
+// elements and keeps SG_LINES x SG_EPT accumulators, so each source cell is
+// read once for all lines of the group (the alphas of a cell are one warp-wide
+// broadcast) and the loads of the next cells are in flight during the current
+// cell's multiply-adds (two cells ahead).  Each line sums its cells in the group's
+// entry order.
+constexpr int SG_EPT = 4, SG_CHUNK = 32 * SG_EPT;
+__global__ void __launch_bounds__(256, 2) sbuild_groups(const DevSGroup* __restrict__ groups,
+                                                     const DevSItem* __restrict__ items, uint32_t n_items,
+                                                     const uint64_t* __restrict__ ent_t,
+                                                     const double* __restrict__ ent_a, double* __restrict__ S,
+                                                     const double* __restrict__ T) {
+    const uint32_t lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    for (uint32_t it = blockIdx.x * wpb + (threadIdx.x >> 5); it < n_items; it += gridDim.x * wpb) {
+        const DevSItem I = items[it];
+        const DevSGroup G = groups[I.group];
+        const uint32_t n = G.rows * G.cols;
+        uint32_t e[SG_EPT];
+        bool in[SG_EPT];
+#pragma unroll
+        for (int u = 0; u < SG_EPT; ++u) {
+            e[u] = I.e0 + lane + 32u * u;
+            in[u] = e[u] < n;
+        }
+        double acc[SG_LINES][SG_EPT];
+#pragma unroll
+        for (int j = 0; j < SG_LINES; ++j)
+#pragma unroll
+            for (int u = 0; u < SG_EPT; ++u) acc[j][u] = 0.0;
+        // two cells of T values in flight ahead of the multiply-adds, the source
+        // offset of the cell after them one step earlier still
+        const uint32_t k0 = G.ent_begin, k1 = G.ent_end;
+        auto fetch = [&](uint32_t k, uint64_t tb, double (&v)[SG_EPT]) {
+#pragma unroll
+            for (int u = 0; u < SG_EPT; ++u) v[u] = (k < k1 && in[u]) ? T[tb + e[u]] : 0.0;
+        };
+        double v0[SG_EPT], v1[SG_EPT];
+        uint64_t tb2 = k0 + 2 < k1 ? ent_t[k0 + 2] : 0;
+        fetch(k0, k0 < k1 ? ent_t[k0] : 0, v0);
+        fetch(k0 + 1, k0 + 1 < k1 ? ent_t[k0 + 1] : 0, v1);
+        for (uint32_t k = k0; k < k1; ++k) {
+            double v2[SG_EPT];
+            fetch(k + 2, tb2, v2);
+            tb2 = k + 3 < k1 ? ent_t[k + 3] : 0;
+            const double2* a2 = reinterpret_cast<const double2*>(ent_a + uint64_t(k) * SG_LINES);
+            double a[SG_LINES];
+#pragma unroll
+            for (int h = 0; h < SG_LINES / 2; ++h) {
+                const double2 x = a2[h];
+                a[2 * h] = x.x;
+                a[2 * h + 1] = x.y;
+            }
+#pragma unroll
+            for (int j = 0; j < SG_LINES; ++j)
+#pragma unroll
+                for (int u = 0; u < SG_EPT; ++u) acc[j][u] = fma(a[j], v0[u], acc[j][u]);
+#pragma unroll
+            for (int u = 0; u < SG_EPT; ++u) {
+                v0[u] = v1[u];
+                v1[u] = v2[u];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < SG_EPT; ++u) {
+            if (!in[u]) continue;
+            const uint32_t col = e[u] / G.rows, i = e[u] - col * G.rows;
+            double* dst = S + G.s_base + i + uint64_t(col) * G.ld_s;
+#pragma unroll
+            for (int j = 0; j < SG_LINES; ++j)
+                if (uint32_t(j) < G.nlines) dst[uint64_t(j) * G.line_stride] = ((G.mask >> j) & 1u) ? acc[j][u] : 0.0;
         }
     }
 }
@@ -459,9 +575,82 @@ void stack_stage1(FlatPlan const& p, std::vector<uint64_t> const& stage1_bnd, st
 }
 }  // namespace
 
+namespace {
+// S build of one unit as line groups: groups of SG_LINES consecutive MPO row
+// blocks, each with the union of its lines' source cells in first-use order and
+// the summed alphas per (cell, line).  Returns the multiply-adds per element
+// this issues (entries x SG_LINES); `terms` receives the per-line walk's count.
+struct UnitGroups {
+    std::vector<DevSGroup> groups;
+    std::vector<uint64_t> ent_t;
+    std::vector<double> ent_a;
+};
+uint64_t group_unit(FlatPlan const& p, uint32_t c, uint32_t u, std::vector<int64_t> const& line_of,
+                    std::vector<uint64_t> const& t_off, std::vector<uint64_t> const& s_off, UnitGroups& out,
+                    uint64_t* terms) {
+    const bool left = p.kind == KIND_LEFT;
+    const uint32_t ns = p.c_nsrows[c], ls = p.c_ls[c], rs = p.c_rs[c];
+    std::unordered_map<uint64_t, uint32_t> slot;
+    uint64_t fmas = 0;
+    *terms = 0;
+    for (uint32_t g0 = 0; g0 < ns; g0 += SG_LINES) {
+        DevSGroup G{};
+        G.nlines = std::min<uint32_t>(SG_LINES, ns - g0);
+        if (left) {
+            G.rows = p.u_ms[u];
+            G.cols = rs;
+            G.ld_s = p.c_stripe[c];
+            G.line_stride = rs * p.c_stripe[c];
+            G.s_base = s_off[c] + p.u_offset[u] + uint64_t(g0) * rs * p.c_stripe[c];
+        } else {
+            G.rows = ls;
+            G.cols = p.u_ms[u];
+            G.ld_s = ns * ls;
+            G.line_stride = ls;
+            G.s_base = s_off[c] + uint64_t(g0) * ls + uint64_t(p.u_offset[u]) * G.ld_s;
+        }
+        G.ent_begin = uint32_t(out.ent_t.size());
+        slot.clear();
+        for (uint32_t j = 0; j < G.nlines; ++j) {
+            const int64_t l = line_of[g0 + j];
+            if (l < 0) continue;
+            for (uint32_t k = p.l_term[l]; k < p.l_term[l + 1]; ++k) {
+                const uint64_t src = t_off[p.term_t[k]] + uint64_t(p.term_col[k]) * (left ? rs : ls);
+                auto it = slot.find(src);
+                uint32_t e;
+                if (it == slot.end()) {
+                    e = uint32_t(out.ent_t.size());
+                    slot.emplace(src, e);
+                    out.ent_t.push_back(src);
+                    out.ent_a.insert(out.ent_a.end(), SG_LINES, 0.0);
+                } else {
+                    e = it->second;
+                }
+                out.ent_a[uint64_t(e) * SG_LINES + j] += p.term_alpha[k];
+                G.mask |= 1u << j;
+                ++*terms;
+            }
+        }
+        G.ent_end = uint32_t(out.ent_t.size());
+        fmas += uint64_t(G.ent_end - G.ent_begin) * SG_LINES;
+        out.groups.push_back(G);
+    }
+    return fmas;
+}
+
+// DMRGB200_SBUILD: "lines" or "groups" forces one S-build form; anything else chooses per unit
+int sbuild_mode() {
+    const char* v = std::getenv("DMRGB200_SBUILD");
+    if (!v) return 0;
+    if (!std::strcmp(v, "lines")) return 1;
+    if (!std::strcmp(v, "groups")) return 2;
+    return 0;
+}
+}  // namespace
+
 void compile_program(FlatPlan const& p, std::vector<uint64_t> const& stage3_bnd,
                      std::vector<uint64_t> const& stage1_bnd, std::vector<uint64_t> const& outptr,
-                     DeviceProgram& prog, bool stack_rows) {
+                     DeviceProgram& prog, bool stack_rows, bool group_lines) {
     prog = DeviceProgram();
     const uint32_t nt = p.n_t(), nc = p.n_cohorts();
     std::vector<uint64_t> t_off = t_offsets(p, &prog.t_elems);
@@ -515,10 +704,28 @@ void compile_program(FlatPlan const& p, std::vector<uint64_t> const& stage3_bnd,
     std::vector<uint64_t> s_off = s_offsets(p, &prog.s_elems);
     // units tile the S columns (rows for the left step) and b1 its row blocks, so
     // the cells (unit, b1) cover S exactly once
+    const int mode = group_lines ? sbuild_mode() : 1;
+    UnitGroups ug;
+    std::vector<std::pair<uint32_t, uint32_t>> ug_units;  // group range of every grouped unit
     for (uint32_t c = 0; c < nc; ++c) {
         for (uint32_t u = p.c_unit[c]; u < p.c_unit[c + 1]; ++u) {
             std::vector<int64_t> line_of(p.c_nsrows[c], -1);
             for (uint32_t l = p.u_line[u]; l < p.u_line[u + 1]; ++l) line_of[p.l_b1[l]] = l;
+            const uint64_t w = uint64_t(p.u_ms[u]) * (p.kind == KIND_LEFT ? p.c_rs[c] : p.c_ls[c]);
+            if (mode != 1 && w) {
+                // line groups when they issue at most twice the per-line walk's multiply-adds
+                // (a unit without terms is zero-filled by the line walk)
+                const size_t g0 = ug.groups.size(), e0 = ug.ent_t.size();
+                uint64_t nterms = 0;
+                const uint64_t fmas = group_unit(p, c, u, line_of, t_off, s_off, ug, &nterms);
+                if (mode == 2 || (nterms && fmas <= 2 * nterms)) {
+                    ug_units.emplace_back(uint32_t(g0), uint32_t(ug.groups.size()));
+                    continue;
+                }
+                ug.groups.resize(g0);
+                ug.ent_t.resize(e0);
+                ug.ent_a.resize(e0 * SG_LINES);
+            }
             for (uint32_t b1 = 0; b1 < p.c_nsrows[c]; ++b1) {
                 DevSLine L;
                 L.term_begin = uint32_t(prog.terms.size());
@@ -548,6 +755,30 @@ void compile_program(FlatPlan const& p, std::vector<uint64_t> const& stage3_bnd,
                 L.term_end = uint32_t(prog.terms.size());
                 if (uint64_t(L.rows) * L.cols) prog.lines.push_back(L);
             }
+        }
+    }
+    // warp items of the line groups: units by decreasing work; within a unit
+    // element chunk by chunk, every group of the unit per chunk, so the warps in
+    // flight read the same source cells' elements from L2
+    prog.groups = std::move(ug.groups);
+    prog.gent_t = std::move(ug.ent_t);
+    prog.gent_a = std::move(ug.ent_a);
+    {
+        std::vector<uint64_t> work(ug_units.size(), 0);
+        for (size_t x = 0; x < ug_units.size(); ++x)
+            for (uint32_t gi = ug_units[x].first; gi < ug_units[x].second; ++gi) {
+                DevSGroup const& G = prog.groups[gi];
+                work[x] += uint64_t(G.ent_end - G.ent_begin + 1) * G.rows * G.cols;
+            }
+        std::vector<uint32_t> order(ug_units.size());
+        std::iota(order.begin(), order.end(), 0u);
+        std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return work[a] > work[b]; });
+        for (uint32_t x : order) {
+            const uint32_t g0 = ug_units[x].first, g1 = ug_units[x].second;
+            if (g0 == g1) continue;
+            const uint64_t n = uint64_t(prog.groups[g0].rows) * prog.groups[g0].cols;
+            for (uint64_t e0 = 0; e0 < n; e0 += SG_CHUNK)
+                for (uint32_t gi = g0; gi < g1; ++gi) prog.gitems.push_back(DevSItem{gi, uint32_t(e0)});
         }
     }
 
@@ -652,9 +883,14 @@ cudaError_t upload_program(DeviceProgram& prog) {
     }
     if ((e = up(prog.lines, &prog.d_lines)) != cudaSuccess) return e;
     if ((e = up(prog.terms, &prog.d_terms)) != cudaSuccess) return e;
+    if ((e = up(prog.groups, &prog.d_groups)) != cudaSuccess) return e;
+    if ((e = up(prog.gent_t, &prog.d_gent_t)) != cudaSuccess) return e;
+    if ((e = up(prog.gent_a, &prog.d_gent_a)) != cudaSuccess) return e;
+    if ((e = up(prog.gitems, &prog.d_gitems)) != cudaSuccess) return e;
     prog.n_t1 = uint32_t(prog.stage1.tiles.size());
     prog.n_t3 = uint32_t(prog.stage3.tiles.size());
     prog.n_lines = uint32_t(prog.lines.size());
+    prog.n_gitems = uint32_t(prog.gitems.size());
     return cudaSuccess;
 }
 
@@ -683,6 +919,14 @@ void free_program(DeviceProgram& prog) {
     prog.d_t3 = nullptr;
     prog.d_lines = nullptr;
     prog.d_terms = nullptr;
+    cudaFree(prog.d_groups);
+    cudaFree(prog.d_gent_t);
+    cudaFree(prog.d_gent_a);
+    cudaFree(prog.d_gitems);
+    prog.d_groups = nullptr;
+    prog.d_gent_t = nullptr;
+    prog.d_gent_a = nullptr;
+    prog.d_gitems = nullptr;
 }
 
 double calibrate_fp64_tflops() {
@@ -848,9 +1092,16 @@ cudaError_t tune_program(DeviceProgram& prog, uint64_t in, uint64_t out, double*
 }
 
 cudaError_t run_sbuild(DeviceProgram const& prog, double* T, double* S, cudaStream_t stream) {
+    const uint32_t sms = uint32_t(device_sm_count());
     if (prog.n_lines) {
-        uint32_t grid = std::min<uint32_t>(prog.n_lines, uint32_t(device_sm_count()) * 8);
+        uint32_t grid = std::min<uint32_t>(prog.n_lines, sms * 8);
         sbuild_lines<<<grid, 256, 0, stream>>>(prog.d_lines, prog.d_terms, prog.n_lines, S, T);
+    }
+    if (prog.n_gitems) {
+        // 8 warps per CTA, up to two CTAs per SM resident
+        uint32_t grid = std::min<uint32_t>((prog.n_gitems + 7) / 8, sms * 2);
+        sbuild_groups<<<grid, 256, 0, stream>>>(prog.d_groups, prog.d_gitems, prog.n_gitems, prog.d_gent_t,
+                                                prog.d_gent_a, S, T);
     }
     return cudaGetLastError();
 }
@@ -880,14 +1131,10 @@ cudaError_t run_program(DeviceProgram const& prog, uint64_t in, uint64_t out, do
     bs.b[BUF_T] = reinterpret_cast<uint64_t>(T);
     bs.b[BUF_S] = reinterpret_cast<uint64_t>(S);
     bs.b[BUF_ABS] = 0;
-    const int sms = device_sm_count();
     if (ev) cudaEventRecord(ev[0], stream);
     launch_variant(prog.var1, prog.d_p1, prog.d_s1, prog.d_t1, prog.n_t1, prog.x1, prog.d_r1, bs, stream);
     if (ev) cudaEventRecord(ev[1], stream);
-    if (prog.n_lines) {
-        uint32_t grid = std::min<uint32_t>(prog.n_lines, uint32_t(sms) * 8);
-        sbuild_lines<<<grid, 256, 0, stream>>>(prog.d_lines, prog.d_terms, prog.n_lines, S, T);
-    }
+    run_sbuild(prog, T, S, stream);
     if (ev) cudaEventRecord(ev[2], stream);
     launch_variant(prog.var3, prog.d_p3, prog.d_s3, prog.d_t3, prog.n_t3, prog.x3, nullptr, bs, stream);
     if (ev) cudaEventRecord(ev[3], stream);

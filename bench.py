@@ -240,7 +240,7 @@ def gemm_workload(args):
     Cm = torch.empty(n, n, dtype=torch.float64, device="cuda")
     flops = 2.0 * n ** 3
     res = {}
-    for v in range(12):
+    for v in range(capi.lib.dmrgb200_gemm_variant_count()):
         name = capi.lib.dmrgb200_gemm_variant_name(v).decode()
         ts = []
         for k in range(args.warmup + 3):

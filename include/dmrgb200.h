@@ -214,6 +214,8 @@ dmrgb200_status dmrgb200_hpsi(dmrgb200_plan_t plan, const double* x, double* y, 
 dmrgb200_status dmrgb200_plan_autotune(dmrgb200_plan_t plan, const double* x, double* y, void* cuda_stream,
                                        int32_t variants[2]);
 const char* dmrgb200_gemm_variant_name(int variant);
+/* Number of grouped-GEMM variants (valid variant indices are 0 .. count - 1). */
+int dmrgb200_gemm_variant_count(void);
 
 /* Adjoint of H·psi (no counterpart in the reference, which has no derivative
  * code).  With the plan's terms y = sum_k alpha_k H_k x, one call gives
@@ -265,7 +267,8 @@ void dmrgb200_set_coupling(int a, int b, int c, int d, int e, int f, int g, int 
 
 /* ---- plain FP64 GEMM on the grouped DMMA kernel --------------------------- */
 /* C = A * B (column-major FP64, A M x K, B K x N) with grouped-GEMM variant
- * `variant` (0 .. 7, see dmrgb200_gemm_variant_name) as one problem; for
+ * `variant` (0 .. dmrgb200_gemm_variant_count() - 1, see
+ * dmrgb200_gemm_variant_name) as one problem; for
  * measuring the H·psi kernel on regular shapes.  No counterpart in the
  * reference (it calls BLAS).  Allocates its tile tables per call; returns
  * after completion. */

@@ -558,6 +558,7 @@ dmrgb200_status dmrgb200_plan_autotune(dmrgb200_plan_t plan, const double* x, do
 }
 
 const char* dmrgb200_gemm_variant_name(int variant) { return gemm_variant_name(variant); }
+int dmrgb200_gemm_variant_count(void) { return N_GEMM_VARIANTS; }
 
 dmrgb200_status dmrgb200_plan_set_solver(dmrgb200_plan_t plan, int mode) {
     if (!plan || (mode != DMRGB200_SOLVER_GRAPH && mode != DMRGB200_SOLVER_STEPWISE))

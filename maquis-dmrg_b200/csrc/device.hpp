@@ -111,7 +111,7 @@ struct DevArray {
 // tile classes of the grouped GEMM: 0 = 32 x 64 tiles with 16-deep K steps,
 // 1 = 16 x 64 with 8-deep steps, 2 = 64 x 64 with 16-deep steps, 3 = 16 x 64
 // with 16-deep steps
-constexpr int N_TILE_CLASSES = 4;
+constexpr int N_TILE_CLASSES = 6;
 
 struct GemmList {
     std::vector<DevProb> probs;
@@ -202,7 +202,7 @@ struct GemmDev {
 };
 // grouped-GEMM variants (tile shape x pipeline depth x CTAs per SM); all sum in the
 // same order, so the choice never changes a result bit
-constexpr int N_GEMM_VARIANTS = 12;
+constexpr int N_GEMM_VARIANTS = 16;
 const char* gemm_variant_name(int v);
 // Time every variant on the program's stage-1 and stage-3 tile lists (on the given
 // buffers, whose contents are overwritten as by an H psi) and keep the fastest per

@@ -26,8 +26,12 @@ namespace dmrgb200 {
 
 namespace {
 
-constexpr int BN = 64;
-constexpr int LDB_S = BN + 4;  // row strides = 8 words mod 32: conflict-free fragment loads
+// shared-memory row pitch of a tile of ROWS (m or n) columns: 8 words mod 32,
+// which makes the fragment loads conflict-free
+template <int ROWS>
+__host__ __device__ constexpr int pitch() {
+    return ROWS + 4;
+}
 
 __device__ __forceinline__ const double* op_base(Bases const& bs, DevOp const& op, uint32_t batch) {
     return reinterpret_cast<const double*>(base_of(bs, op.buf) + 8ull * (op.off + uint64_t(batch) * op.bstride));
@@ -143,18 +147,20 @@ struct LoadCursor {
     bool valid;
 };
 
-template <int BM_, int BK_, int STAGES, int MINB, int NTHREADS>
+template <int BM_, int BN_, int BK_, int STAGES, int MINB, int NTHREADS, int WARPS_M>
 __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb* __restrict__ probs,
                                                                    const DevSeg* __restrict__ segs,
                                                                    const DevTile* __restrict__ tiles, uint32_t n_tiles,
                                                                    const DevRow* __restrict__ rowtab, Bases bases) {
-    // warps: 2 x 2 for BM_ >= 32 (warp tiles BM_/2 x 32), 1 x 4 for BM_ = 16 (16 x 16)
-    constexpr int WARPS_M = BM_ >= 32 ? 2 : 1, WM = BM_ / WARPS_M;
-    constexpr int WN = BN / (NTHREADS / 32 / WARPS_M), NJ = WN / 8;
+    // warps: WARPS_M x (warps / WARPS_M), warp tiles WM x WN of 8 x 8 DMMA tiles
+    constexpr int WM = BM_ / WARPS_M;
+    constexpr int WN = BN_ / (NTHREADS / 32 / WARPS_M), NJ = WN / 8;
     constexpr int MI = WM / 8;  // 8 x 8 accumulator tiles (m8n8k4)
     constexpr int NCA = BM_ * BK_ / NTHREADS;
-    __shared__ __align__(16) double As[STAGES][BK_][BM_ + 4];
-    __shared__ __align__(16) double Bs[STAGES][BK_][LDB_S];
+    static_assert(MI >= 1 && NJ >= 1 && NTHREADS % BM_ == 0 && NTHREADS % BN_ == 0 && NTHREADS % BK_ == 0,
+                  "tile shape");
+    __shared__ __align__(16) double As[STAGES][BK_][pitch<BM_>()];
+    __shared__ __align__(16) double Bs[STAGES][BK_][pitch<BN_>()];
 
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
@@ -197,9 +203,9 @@ __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb
             setup_copies<BM_, BK_, NTHREADS>(ca, A, sg.A.ld, 1, tl.m0, pr.M, tid);
         }
         if (!sg.B.trans)
-            setup_copies<BN, BK_, NTHREADS>(cb, B, sg.B.ld, 1, tl.n0, pr.N, tid);
+            setup_copies<BN_, BK_, NTHREADS>(cb, B, sg.B.ld, 1, tl.n0, pr.N, tid);
         else
-            setup_copies<BN, BK_, NTHREADS>(cb, B, 1, sg.B.ld, tl.n0, pr.N, tid);
+            setup_copies<BN_, BK_, NTHREADS>(cb, B, 1, sg.B.ld, tl.n0, pr.N, tid);
     };
     auto enter_tile = [&]() {
         L.valid = L.ti < n_tiles;
@@ -212,8 +218,8 @@ __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb
     auto issue = [&](int slot) {
         if (!L.valid) return;
         if (L.seg < L.seg_end) {  // an empty tile issues no copies
-            issue_copies<BM_, BK_, NTHREADS, BM_ + 4>(&As[slot][0][0], ca, L.krem);
-            issue_copies<BN, BK_, NTHREADS, LDB_S>(&Bs[slot][0][0], cb, L.krem);
+            issue_copies<BM_, BK_, NTHREADS, pitch<BM_>()>(&As[slot][0][0], ca, L.krem);
+            issue_copies<BN_, BK_, NTHREADS, pitch<BN_>()>(&Bs[slot][0][0], cb, L.krem);
             if (L.krem > uint32_t(BK_)) {
                 L.krem -= BK_;
                 return;
@@ -454,20 +460,23 @@ __global__ void __launch_bounds__(128) dmma_rate_loop(int iters, double* sink) {
 
 // --- host-side lowering ---------------------------------------------------------
 
-// tile classes: 0 = 32 x 64 tiles with 16-deep K steps, 1 = 16 x 64 with 8-deep steps
-constexpr int CLASS_BM[N_TILE_CLASSES] = {32, 16, 64, 16}, CLASS_BK[N_TILE_CLASSES] = {16, 8, 16, 16};
+// tile classes (rows x columns, K step): 0 = 32 x 64 / 16, 1 = 16 x 64 / 8,
+// 2 = 64 x 64 / 16, 3 = 16 x 64 / 16 (two warps), 4 = 128 x 32 / 16, 5 = 64 x 32 / 8
+constexpr int CLASS_BM[N_TILE_CLASSES] = {32, 16, 64, 16, 128, 64};
+constexpr int CLASS_BN[N_TILE_CLASSES] = {64, 64, 64, 64, 32, 32};
+constexpr int CLASS_BK[N_TILE_CLASSES] = {16, 8, 16, 16, 16, 8};
 
 void add_tiles(GemmList& gl, uint32_t prob, uint32_t nbatch) {
     DevProb const& p = gl.probs[prob];
     for (int c = 0; c < N_TILE_CLASSES; ++c) {
-        const uint32_t bm = CLASS_BM[c], bk = CLASS_BK[c];
+        const uint32_t bm = CLASS_BM[c], bn = CLASS_BN[c], bk = CLASS_BK[c];
         uint32_t nsteps = 0;
         for (uint32_t s = p.seg_begin; s < p.seg_end; ++s) nsteps += (gl.segs[s].K + bk - 1) / bk;
         nsteps = std::max<uint32_t>(nsteps, 1);  // an empty problem: one step that issues no copies
         auto& out = c == 0 ? gl.tiles : gl.tiles_cls[c];
         for (uint32_t b = 0; b < nbatch; ++b)
             for (uint32_t m0 = 0; m0 < std::max<uint32_t>(p.M, 1); m0 += bm)
-                for (uint32_t n0 = 0; n0 < std::max<uint32_t>(p.N, 1); n0 += BN)
+                for (uint32_t n0 = 0; n0 < std::max<uint32_t>(p.N, 1); n0 += bn)
                     out.push_back(DevTile{prob, b, m0, n0, nsteps});
     }
 }
@@ -478,9 +487,11 @@ void sort_tiles(GemmList& gl) {
     std::vector<uint64_t> kwork(gl.probs.size(), 0);
     for (size_t p = 0; p < gl.probs.size(); ++p)
         for (uint32_t s = gl.probs[p].seg_begin; s < gl.probs[p].seg_end; ++s) kwork[p] += gl.segs[s].K;
-    for (auto* tl : {&gl.tiles, &gl.tiles_cls[1], &gl.tiles_cls[2], &gl.tiles_cls[3]})
-        std::stable_sort(tl->begin(), tl->end(),
+    for (int c = 0; c < N_TILE_CLASSES; ++c) {
+        auto& tl = c == 0 ? gl.tiles : gl.tiles_cls[c];
+        std::stable_sort(tl.begin(), tl.end(),
                          [&](DevTile const& a, DevTile const& b) { return kwork[a.prob] > kwork[b.prob]; });
+    }
 }
 
 DevOp op(uint16_t buf, uint64_t off, uint32_t ld, bool trans, uint64_t bstride = 0) {
@@ -577,7 +588,7 @@ void stack_stage1(FlatPlan const& p, std::vector<uint64_t> const& stage1_bnd, st
 
 namespace {
 // S build of one unit as line groups: groups of SG_LINES consecutive MPO row
-// blocks, each with the union of its lines' source cells in first-use order and
+// blocks, each with the union of its lines' source cells in address order and
 // the summed alphas per (cell, line).  Returns the multiply-adds per element
 // this issues (entries x SG_LINES); `terms` receives the per-line walk's count.
 struct UnitGroups {
@@ -632,6 +643,24 @@ uint64_t group_unit(FlatPlan const& p, uint32_t c, uint32_t u, std::vector<int64
             }
         }
         G.ent_end = uint32_t(out.ent_t.size());
+        // sources in address order: the warps on the groups of one unit then sweep
+        // the shared T slices together (L1 / L2 reuse)
+        {
+            const uint32_t n = G.ent_end - G.ent_begin;
+            std::vector<uint32_t> ord(n);
+            std::iota(ord.begin(), ord.end(), 0u);
+            std::sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) {
+                return out.ent_t[G.ent_begin + a] < out.ent_t[G.ent_begin + b];
+            });
+            std::vector<uint64_t> t(n);
+            std::vector<double> al(uint64_t(n) * SG_LINES);
+            for (uint32_t x = 0; x < n; ++x) {
+                t[x] = out.ent_t[G.ent_begin + ord[x]];
+                std::copy_n(&out.ent_a[uint64_t(G.ent_begin + ord[x]) * SG_LINES], SG_LINES, &al[uint64_t(x) * SG_LINES]);
+            }
+            std::copy(t.begin(), t.end(), out.ent_t.begin() + G.ent_begin);
+            std::copy(al.begin(), al.end(), out.ent_a.begin() + uint64_t(G.ent_begin) * SG_LINES);
+        }
         fmas += uint64_t(G.ent_end - G.ent_begin) * SG_LINES;
         out.groups.push_back(G);
     }
@@ -757,9 +786,10 @@ void compile_program(FlatPlan const& p, std::vector<uint64_t> const& stage3_bnd,
             }
         }
     }
-    // warp items of the line groups: units by decreasing work; within a unit
-    // element chunk by chunk, every group of the unit per chunk, so the warps in
-    // flight read the same source cells' elements from L2
+    // warp items of the line groups: units by decreasing work, then group by
+    // group, each group's element chunks consecutive (the warps of a CTA share the
+    // group's source list and read its T slices in long contiguous runs; the
+    // groups of a unit follow each other and reuse the unit's slices from L2)
     prog.groups = std::move(ug.groups);
     prog.gent_t = std::move(ug.ent_t);
     prog.gent_a = std::move(ug.ent_a);
@@ -777,8 +807,8 @@ void compile_program(FlatPlan const& p, std::vector<uint64_t> const& stage3_bnd,
             const uint32_t g0 = ug_units[x].first, g1 = ug_units[x].second;
             if (g0 == g1) continue;
             const uint64_t n = uint64_t(prog.groups[g0].rows) * prog.groups[g0].cols;
-            for (uint64_t e0 = 0; e0 < n; e0 += SG_CHUNK)
-                for (uint32_t gi = g0; gi < g1; ++gi) prog.gitems.push_back(DevSItem{gi, uint32_t(e0)});
+            for (uint32_t gi = g0; gi < g1; ++gi)
+                for (uint64_t e0 = 0; e0 < n; e0 += SG_CHUNK) prog.gitems.push_back(DevSItem{gi, uint32_t(e0)});
         }
     }
 
@@ -987,18 +1017,22 @@ struct GemmVariant {
     int threads;     // CTA size
 };
 const GemmVariant kVariants[N_GEMM_VARIANTS] = {
-    {gemm_f64_grouped<32, 16, 2, 4, 128>, "tile32x64_k16_stages2_ctas4", 0, 128},
-    {gemm_f64_grouped<32, 16, 3, 4, 128>, "tile32x64_k16_stages3_ctas4", 0, 128},
-    {gemm_f64_grouped<32, 16, 2, 5, 128>, "tile32x64_k16_stages2_ctas5", 0, 128},
-    {gemm_f64_grouped<32, 16, 3, 5, 128>, "tile32x64_k16_stages3_ctas5", 0, 128},
-    {gemm_f64_grouped<16, 8, 3, 6, 128>, "tile16x64_k8_stages3_ctas6", 1, 128},
-    {gemm_f64_grouped<16, 8, 4, 8, 128>, "tile16x64_k8_stages4_ctas8", 1, 128},
-    {gemm_f64_grouped<64, 16, 2, 3, 128>, "tile64x64_k16_stages2_ctas3", 2, 128},
-    {gemm_f64_grouped<64, 16, 2, 2, 128>, "tile64x64_k16_stages2_ctas2", 2, 128},
-    {gemm_f64_grouped<16, 16, 2, 8, 64>, "tile16x64_k16_warps2_stages2_ctas8", 3, 64},
-    {gemm_f64_grouped<16, 16, 3, 8, 64>, "tile16x64_k16_warps2_stages3_ctas8", 3, 64},
-    {gemm_f64_grouped<16, 16, 2, 10, 64>, "tile16x64_k16_warps2_stages2_ctas10", 3, 64},
-    {gemm_f64_grouped<16, 16, 3, 10, 64>, "tile16x64_k16_warps2_stages3_ctas10", 3, 64},
+    {gemm_f64_grouped<32, 64, 16, 2, 4, 128, 2>, "tile32x64_k16_stages2_ctas4", 0, 128},
+    {gemm_f64_grouped<32, 64, 16, 3, 4, 128, 2>, "tile32x64_k16_stages3_ctas4", 0, 128},
+    {gemm_f64_grouped<32, 64, 16, 2, 5, 128, 2>, "tile32x64_k16_stages2_ctas5", 0, 128},
+    {gemm_f64_grouped<32, 64, 16, 3, 5, 128, 2>, "tile32x64_k16_stages3_ctas5", 0, 128},
+    {gemm_f64_grouped<16, 64, 8, 3, 6, 128, 1>, "tile16x64_k8_stages3_ctas6", 1, 128},
+    {gemm_f64_grouped<16, 64, 8, 4, 8, 128, 1>, "tile16x64_k8_stages4_ctas8", 1, 128},
+    {gemm_f64_grouped<64, 64, 16, 2, 3, 128, 2>, "tile64x64_k16_stages2_ctas3", 2, 128},
+    {gemm_f64_grouped<64, 64, 16, 2, 2, 128, 2>, "tile64x64_k16_stages2_ctas2", 2, 128},
+    {gemm_f64_grouped<16, 64, 16, 2, 8, 64, 1>, "tile16x64_k16_warps2_stages2_ctas8", 3, 64},
+    {gemm_f64_grouped<16, 64, 16, 3, 8, 64, 1>, "tile16x64_k16_warps2_stages3_ctas8", 3, 64},
+    {gemm_f64_grouped<16, 64, 16, 2, 10, 64, 1>, "tile16x64_k16_warps2_stages2_ctas10", 3, 64},
+    {gemm_f64_grouped<16, 64, 16, 3, 10, 64, 1>, "tile16x64_k16_warps2_stages3_ctas10", 3, 64},
+    {gemm_f64_grouped<128, 32, 16, 2, 2, 128, 4>, "tile128x32_k16_stages2_ctas2", 4, 128},
+    {gemm_f64_grouped<128, 32, 16, 2, 3, 128, 4>, "tile128x32_k16_stages2_ctas3", 4, 128},
+    {gemm_f64_grouped<64, 32, 8, 3, 4, 128, 2>, "tile64x32_k8_stages3_ctas4", 5, 128},
+    {gemm_f64_grouped<64, 32, 8, 4, 5, 128, 2>, "tile64x32_k8_stages4_ctas5", 5, 128},
 };
 
 int variant_occupancy(int v) {

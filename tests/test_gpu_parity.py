@@ -142,7 +142,7 @@ def test_autotuned_variants_give_identical_results(ctx):
     plan, Lb, Rb, xd, yd = keep
     chosen = (C.c_int32 * 2)()
     capi.check(capi.lib.dmrgb200_plan_autotune(plan.handle, xd.data_ptr(), yd.data_ptr(), None, chosen), "autotune")
-    assert all(0 <= v < 12 for v in chosen)
+    assert all(0 <= v < capi.lib.dmrgb200_gemm_variant_count() for v in chosen)
     assert capi.lib.dmrgb200_gemm_variant_name(chosen[0]).startswith(b"tile")
     yd.zero_()
     plan.hpsi(xd.data_ptr(), yd.data_ptr())

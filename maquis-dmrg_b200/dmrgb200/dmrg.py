@@ -187,6 +187,47 @@ def right_canonicalize(tensors):
     return out
 
 
+def left_canonicalize(tensors, upto: int):
+    """Make sites 0..upto-1 left-normalised by per-charge SVDs of their
+    left-paired blocks, absorbing S V^T into the right neighbour (the mirror of
+    right_canonicalize); bond dimensions drop only where a block is rank
+    deficient.  Returns the new tensor list."""
+    out = list(tensors)
+    for j in range(upto):
+        t, nxt = out[j], out[j + 1]
+        lp = S.left_paired_layout(t.phys, t.left, t.right)
+        lpd = t.left_paired()
+        new_right, Us, absorb = [], {}, {}
+        for rb, (rc, mr) in enumerate(t.right):
+            blk = S.block_view(lpd, lp, rb)
+            if blk.size == 0:
+                continue
+            U, sv, Vt = np.linalg.svd(blk, full_matrices=False)
+            k = int(np.sum(sv > 1e-14 * max(sv[0], 1e-300))) if sv.size else 0
+            if k == 0:
+                continue
+            new_right.append((rc, k))
+            Us[rc] = U[:, :k]
+            absorb[rc] = sv[:k, None] * Vt[:k]
+        nt = S.SiteTensor(t.phys, t.left, new_right)
+        nlp = S.left_paired_layout(t.phys, t.left, new_right)
+        for (rb, s, ss), (r0, _, ml, k, lb) in nlp.sub.items():
+            rc = new_right[rb][0]
+            _, c0, _, _, _ = nt.rp.sub[(lb, s, ss)]
+            S.block_view(nt.data, nt.rp, lb)[:, c0:c0 + k] = Us[rc][r0:r0 + ml, :]
+        nn = S.SiteTensor(nxt.phys, new_right, nxt.right)
+        npos = {c: i for i, (c, _) in enumerate(new_right)}
+        for (lb, s, ss), (_, c0, ml, mr, rb) in nxt.rp.sub.items():
+            lc = nxt.left[lb][0]
+            if lc not in npos:
+                continue
+            nlb = npos[lc]
+            _, c1, _, _, _ = nn.rp.sub[(nlb, s, ss)]
+            S.block_view(nn.data, nn.rp, nlb)[:, c1:c1 + mr] = absorb[lc] @ S.block_view(nxt.data, nxt.rp, lb)[:, c0:c0 + mr]
+        out[j], out[j + 1] = nt, nn
+    return out
+
+
 @dataclass
 class SweepLog:
     energies: list = field(default_factory=list)      # (sweep, site, energy, iterations, truncated weight)

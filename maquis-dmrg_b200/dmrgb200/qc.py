@@ -229,3 +229,61 @@ def quantum_chemistry(L: int, n_up: int, n_down: int, h=None, eri=None, seed_h: 
     m = Model("quantum_chemistry", capi.TWOU1, PHYS, local, mpo, (n_up, n_down), terms, fermionic_ops=FERMIONIC)
     m.h, m.eri = h, eri
     return m
+
+
+# ---- integral derivatives ------------------------------------------------------------
+#
+# The MPO coefficients (and so the plan's term alphas) are linear in every
+# integral, and the bipartite construction's structure does not depend on the
+# integrals' values, so d(alpha)/d(integral) is the change of the alphas when the
+# integral is raised by one.  An integral stands for its symmetry orbit:
+# h_ab = h_ba, and (ab|cd) with its 8-fold symmetry.
+
+def integral_orbit(which: str, index) -> set:
+    """Index tuples that share the value of integral `which` ("h" or "eri") at `index`."""
+    if which == "h":
+        a, b = index
+        return {(a, b), (b, a)}
+    a, b, c, d = index
+    return {(a, b, c, d), (b, a, c, d), (a, b, d, c), (b, a, d, c),
+            (c, d, a, b), (d, c, a, b), (c, d, b, a), (d, c, b, a)}
+
+
+def raise_integral(h: np.ndarray, eri: np.ndarray, which: str, index, delta: float):
+    """Copies of (h, eri) with the integral's orbit raised by delta."""
+    h, eri = h.copy(), eri.copy()
+    for idx in integral_orbit(which, index):
+        if which == "h":
+            h[idx] += delta
+        else:
+            eri[idx] += delta
+    return h, eri
+
+
+def integral_operator_terms(which: str, index) -> list:
+    """dH/d(integral) as a term list [(coeff, [(site, op), ...])] (format of qc_terms)."""
+    terms = []
+    spins = ("up", "down")
+    for idx in integral_orbit(which, index):
+        if which == "h":
+            p, q = idx
+            for s in spins:
+                terms.append((1.0, [(p, "cdag_" + s), (q, "c_" + s)]))
+        else:
+            p, q, r, t = idx
+            for s in spins:
+                for u in spins:
+                    if (p == r and s == u) or (q == t and s == u):
+                        continue
+                    terms.append((0.5, [(p, "cdag_" + s), (r, "cdag_" + u), (t, "c_" + u), (q, "c_" + s)]))
+    return terms
+
+
+def operator_model(model: Model, terms: list) -> Model:
+    """The model's sites and symmetry with the MPO of another term list (an
+    observable such as dH/d(integral)), for expectation values through the same
+    boundary steps and H·psi."""
+    L = len(model.mpo)
+    mpo = build_mpo(terms, L, model.local, model.phys)
+    return Model(model.name + "_operator", model.symm, model.phys, model.local, mpo, model.total_charge, terms,
+                 fermionic_ops=model.fermionic_ops)

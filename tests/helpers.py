@@ -119,26 +119,8 @@ def qc_integral_derivative(model, L, i, ch, galpha, which, index):
     which = "h" (index (a, b), symmetric pair) or "eri" (index (a, b, c, d), its
     8-fold orbit).  Returns (derivative, dense term list of dH/d(integral))."""
     from dmrgb200 import qc
-    h, eri = model.h.copy(), model.eri.copy()
-    terms = []
-    if which == "h":
-        a, b = index
-        pairs = {(a, b), (b, a)}
-        for (p, q) in pairs:
-            h[p, q] += 1.0
-            for s in ("up", "down"):
-                terms.append((1.0, [(p, "cdag_" + s), (q, "c_" + s)]))
-    else:
-        a, b, c, d = index
-        orbit = {(a, b, c, d), (b, a, c, d), (a, b, d, c), (b, a, d, c),
-                 (c, d, a, b), (d, c, a, b), (c, d, b, a), (d, c, b, a)}
-        for (p, q, r, t) in orbit:
-            eri[p, q, r, t] += 1.0
-            for s in ("up", "down"):
-                for u in ("up", "down"):
-                    if (p == r and s == u) or (q == t and s == u):
-                        continue
-                    terms.append((0.5, [(p, "cdag_" + s), (r, "cdag_" + u), (t, "c_" + u), (q, "c_" + s)]))
+    h, eri = qc.raise_integral(model.h, model.eri, which, index, 1.0)
+    terms = qc.integral_operator_terms(which, index)
     m2 = qc.quantum_chemistry(L, model.total_charge[0], model.total_charge[1], h=h, eri=eri)
     W12 = M.MPOHandle(M.twosite_mpo(m2.mpo[i], m2.mpo[i + 1], m2.phys, m2.phys), m2.symm)
     s = E.schedule_hpsi(ch.p12, ch.left, ch.right, W12, ch.Lidx, ch.Ridx)

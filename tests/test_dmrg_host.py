@@ -47,6 +47,24 @@ def test_right_canonicalize_preserves_state_and_normalises():
         assert np.allclose(X @ X.T, np.eye(X.shape[0]), atol=1e-12)
 
 
+def test_left_canonicalize_preserves_state_and_normalises():
+    model = M.fermi_hubbard(6, t=1.0, U=4.0)
+    bonds = S.allowed_sectors(model.phys, 6, model.total_charge, 6)
+    A = G.right_canonicalize(S.random_mps(model.phys, bonds, np.random.default_rng(4)))
+    i = 3
+    B = G.left_canonicalize(A, i)
+    va, vb = D.mps_dense([t.dense() for t in A]), D.mps_dense([t.dense() for t in B])
+    assert np.linalg.norm(va - vb) <= 1e-12 * np.linalg.norm(va)
+    for t in B[:i]:
+        Td = t.dense()
+        X = Td.reshape(-1, Td.shape[2])
+        assert np.allclose(X.T @ X, np.eye(X.shape[1]), atol=1e-12)
+    for t in B[i + 1:]:
+        Td = t.dense()
+        X = Td.reshape(Td.shape[0], -1)
+        assert np.allclose(X @ X.T, np.eye(X.shape[0]), atol=1e-12)
+
+
 def test_truncation_keeps_largest_states():
     model = M.heisenberg(8)
     rng = np.random.default_rng(2)

@@ -65,3 +65,34 @@ def test_qc_integral_derivative_is_local_rdm(which, index):
     Op = D.sparse_hamiltonian(dataclasses.replace(model, dense_terms=terms), L)
     expect = v @ (Op @ v)
     assert abs(grad - expect) <= 1e-11 * max(1.0, abs(expect)), (which, index, grad, expect)
+
+
+@pytest.mark.parametrize("which,index", [("h", (0, 2)), ("eri", (0, 1, 2, 3)), ("eri", (1, 1, 2, 2))])
+def test_operator_model_mpo_reproduces_dense_operator(which, index):
+    """The MPO of dH/d(integral) (the observable of the RDM element) matches the
+    dense operator built from the same term list."""
+    import dataclasses
+    L = 4
+    model = qc.quantum_chemistry(L, 2, 2)
+    terms = qc.integral_operator_terms(which, index)
+    om = qc.operator_model(model, terms)
+    dense = D.dense_hamiltonian(dataclasses.replace(model, dense_terms=terms), L)
+    assert np.abs(D.mpo_dense(om, L) - dense).max() <= 1e-12 * max(1.0, np.abs(dense).max())
+
+
+@pytest.mark.parametrize("which,index", [("h", (0, 2)), ("eri", (0, 1, 2, 2))])
+def test_integral_derivative_equals_operator_expectation(which, index):
+    """The local adjoint derivative equals <psi|H_eff(dH/d(integral))|psi>, the RDM
+    element computed through the observable's own MPO, boundaries and schedule
+    (the check used at L = 16 on the device)."""
+    import oracle as O
+    from helpers import qc_integral_derivative
+    L, i = 5, 1
+    model, bonds, tensors, rng = make_chain("qc", L, 16, seed=12)
+    ch = OracleChain(model, bonds, tensors, i)
+    psi = random_psi(ch.p12, ch.left, ch.right, rng).data
+    _, ga = O.hpsi_adjoint(ch.sched.plan, ch.Lval, ch.Lidx, ch.Rval, ch.Ridx, psi, psi)
+    grad, terms = qc_integral_derivative(model, L, i, ch, ga, which, index)
+    oc = OracleChain(qc.operator_model(model, terms), bonds, tensors, i)
+    expect = float(psi @ oc.hpsi(psi))
+    assert abs(grad - expect) <= 1e-11 * max(1.0, abs(expect)), (grad, expect)

@@ -69,7 +69,7 @@ struct DevSTerm {
 // read the cell, duplicate sources of a line summed).  Line j of the group
 // starts at s_base + j * line_stride; element (i, c) of a line sits at
 // i + c * ld_s, its source at t_base + i + c * rows.
-constexpr int SG_LINES = 8;
+constexpr int SG_LINES = 8, SG_UNROLL = 4, SG_EPT = 4, SG_CHUNK = 32 * SG_EPT;
 struct DevSGroup {
     uint64_t s_base;
     uint32_t line_stride, ld_s, rows, cols;

@@ -369,12 +369,55 @@ __global__ void __launch_bounds__(256) sbuild_lines(const DevSLine* __restrict__
 
 // S build of line groups (DevSGroup): one warp per work item (a group and a
 // chunk of SG_CHUNK consecutive elements of its lines); every lane owns SG_EPT
-// elements and keeps SG_LINES x SG_EPT accumulators, so each source cell is
-// read once for all lines of the group (the alphas of a cell are one warp-wide
-// broadcast) and the loads of the next cells are in flight during the current
-// cell's multiply-adds (two cells ahead).  Each line sums its cells in the group's
-// entry order.
-constexpr int SG_EPT = 4, SG_CHUNK = 32 * SG_EPT;
+// elements (lane + 32 u) and keeps SG_LINES x SG_EPT accumulators, so each
+// source cell is read once for all lines of the group (the alphas of a cell are
+// one warp-wide broadcast).  Sources come SG_UNROLL at a time (the host pads each
+// group's list with zero-alpha sources): the T values of the next pair of
+// sources are loaded while the current pair is multiplied, every load addressed
+// from one per-lane pointer with constant offsets.  Each line sums its sources
+// in the group's entry order.
+template <bool FULL>
+__device__ __forceinline__ void sg_accumulate(double (&acc)[SG_LINES][SG_EPT], const double* __restrict__ T,
+                                              const uint64_t* __restrict__ ent_t, const double* __restrict__ ent_a,
+                                              uint32_t k0, uint32_t k1, uint32_t e0, uint32_t lane, uint32_t n) {
+    const double* Tl = T + e0 + lane;
+    bool in[SG_EPT];
+#pragma unroll
+    for (int u = 0; u < SG_EPT; ++u) in[u] = FULL || e0 + lane + 32u * u < n;
+    auto load = [&](uint64_t tb, double (&v)[SG_EPT]) {
+        const double* p = Tl + tb;
+#pragma unroll
+        for (int u = 0; u < SG_EPT; ++u) v[u] = in[u] ? __ldg(p + 32 * u) : 0.0;
+    };
+    auto madd = [&](uint32_t k, double const (&v)[SG_EPT]) {
+        const double2* a2 = reinterpret_cast<const double2*>(ent_a + uint64_t(k) * SG_LINES);
+#pragma unroll
+        for (int h = 0; h < SG_LINES / 2; ++h) {
+            const double2 x = __ldg(a2 + h);
+#pragma unroll
+            for (int u = 0; u < SG_EPT; ++u) {
+                acc[2 * h][u] = fma(x.x, v[u], acc[2 * h][u]);
+                acc[2 * h + 1][u] = fma(x.y, v[u], acc[2 * h + 1][u]);
+            }
+        }
+    };
+    double v0[SG_EPT], v1[SG_EPT], v2[SG_EPT], v3[SG_EPT];
+    load(ent_t[k0], v0);
+    load(ent_t[k0 + 1], v1);
+    for (uint32_t k = k0; k < k1; k += SG_UNROLL) {
+        load(ent_t[k + 2], v2);
+        load(ent_t[k + 3], v3);
+        madd(k, v0);
+        madd(k + 1, v1);
+        if (k + SG_UNROLL < k1) {
+            load(ent_t[k + 4], v0);
+            load(ent_t[k + 5], v1);
+        }
+        madd(k + 2, v2);
+        madd(k + 3, v3);
+    }
+}
+
 __global__ void __launch_bounds__(256, 2) sbuild_groups(const DevSGroup* __restrict__ groups,
                                                      const DevSItem* __restrict__ items, uint32_t n_items,
                                                      const uint64_t* __restrict__ ent_t,
@@ -385,55 +428,22 @@ __global__ void __launch_bounds__(256, 2) sbuild_groups(const DevSGroup* __restr
         const DevSItem I = items[it];
         const DevSGroup G = groups[I.group];
         const uint32_t n = G.rows * G.cols;
-        uint32_t e[SG_EPT];
-        bool in[SG_EPT];
-#pragma unroll
-        for (int u = 0; u < SG_EPT; ++u) {
-            e[u] = I.e0 + lane + 32u * u;
-            in[u] = e[u] < n;
-        }
         double acc[SG_LINES][SG_EPT];
 #pragma unroll
         for (int j = 0; j < SG_LINES; ++j)
 #pragma unroll
             for (int u = 0; u < SG_EPT; ++u) acc[j][u] = 0.0;
-        // two cells of T values in flight ahead of the multiply-adds, the source
-        // offset of the cell after them one step earlier still
-        const uint32_t k0 = G.ent_begin, k1 = G.ent_end;
-        auto fetch = [&](uint32_t k, uint64_t tb, double (&v)[SG_EPT]) {
-#pragma unroll
-            for (int u = 0; u < SG_EPT; ++u) v[u] = (k < k1 && in[u]) ? T[tb + e[u]] : 0.0;
-        };
-        double v0[SG_EPT], v1[SG_EPT];
-        uint64_t tb2 = k0 + 2 < k1 ? ent_t[k0 + 2] : 0;
-        fetch(k0, k0 < k1 ? ent_t[k0] : 0, v0);
-        fetch(k0 + 1, k0 + 1 < k1 ? ent_t[k0 + 1] : 0, v1);
-        for (uint32_t k = k0; k < k1; ++k) {
-            double v2[SG_EPT];
-            fetch(k + 2, tb2, v2);
-            tb2 = k + 3 < k1 ? ent_t[k + 3] : 0;
-            const double2* a2 = reinterpret_cast<const double2*>(ent_a + uint64_t(k) * SG_LINES);
-            double a[SG_LINES];
-#pragma unroll
-            for (int h = 0; h < SG_LINES / 2; ++h) {
-                const double2 x = a2[h];
-                a[2 * h] = x.x;
-                a[2 * h + 1] = x.y;
-            }
-#pragma unroll
-            for (int j = 0; j < SG_LINES; ++j)
-#pragma unroll
-                for (int u = 0; u < SG_EPT; ++u) acc[j][u] = fma(a[j], v0[u], acc[j][u]);
-#pragma unroll
-            for (int u = 0; u < SG_EPT; ++u) {
-                v0[u] = v1[u];
-                v1[u] = v2[u];
-            }
+        if (G.ent_begin < G.ent_end) {
+            if (I.e0 + SG_CHUNK <= n)
+                sg_accumulate<true>(acc, T, ent_t, ent_a, G.ent_begin, G.ent_end, I.e0, lane, n);
+            else
+                sg_accumulate<false>(acc, T, ent_t, ent_a, G.ent_begin, G.ent_end, I.e0, lane, n);
         }
 #pragma unroll
         for (int u = 0; u < SG_EPT; ++u) {
-            if (!in[u]) continue;
-            const uint32_t col = e[u] / G.rows, i = e[u] - col * G.rows;
+            const uint32_t e = I.e0 + lane + 32u * u;
+            if (e >= n) continue;
+            const uint32_t col = e / G.rows, i = e - col * G.rows;
             double* dst = S + G.s_base + i + uint64_t(col) * G.ld_s;
 #pragma unroll
             for (int j = 0; j < SG_LINES; ++j)
@@ -662,6 +672,13 @@ uint64_t group_unit(FlatPlan const& p, uint32_t c, uint32_t u, std::vector<int64
             std::copy(al.begin(), al.end(), out.ent_a.begin() + uint64_t(G.ent_begin) * SG_LINES);
         }
         fmas += uint64_t(G.ent_end - G.ent_begin) * SG_LINES;
+        // the kernel walks sources SG_UNROLL at a time: pad with zero-alpha sources at T
+        // offset 0 (their reads stay inside T: an element index is below the cell size)
+        while ((out.ent_t.size() - G.ent_begin) % SG_UNROLL) {
+            out.ent_t.push_back(0);
+            out.ent_a.insert(out.ent_a.end(), SG_LINES, 0.0);
+        }
+        G.ent_end = uint32_t(out.ent_t.size());
         out.groups.push_back(G);
     }
     return fmas;

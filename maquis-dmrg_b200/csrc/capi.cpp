@@ -268,9 +268,11 @@ dmrgb200_status run_step(dmrgb200_plan_s* p, const double* ket, const double* br
     cudaFreeAsync(T, stream);
     cudaFreeAsync(S, stream);
     cudaError_t e2 = cudaStreamSynchronize(stream);
+    const bool timed_out = e2 == cudaSuccess && sbuild_timed_out(prog);
     free_program(prog);
     if (e != cudaSuccess) return cuda_fail(e, "step launch");
     if (e2 != cudaSuccess) return cuda_fail(e2, "step execution");
+    if (timed_out) return fail(DMRGB200_TIMEOUT, "step S build: a bulk-copy wait timed out");
     return DMRGB200_OK;
 }
 
@@ -322,6 +324,7 @@ dmrgb200_status hpsi_emulated(dmrgb200_plan_s* plan, const double* x, double* y,
         return fail(DMRGB200_TIMEOUT, to1 ? "emulated stage 1: a pipeline wait timed out"
                                           : "emulated stage 3: a pipeline wait timed out");
     }
+    if (sbuild_timed_out(plan->prog)) return fail(DMRGB200_TIMEOUT, "S build: a bulk-copy wait timed out");
     return DMRGB200_OK;
 }
 
@@ -336,6 +339,7 @@ cudaError_t plan_hpsi_launch(dmrgb200_plan_t plan, const double* x, double* y, c
 }
 void noalloc_desc_to_flat(const dmrgb200_plan_desc* d, FlatPlan& f) { desc_to_flat(d, f); }
 int plan_solver_mode(dmrgb200_plan_t plan) { return plan->solver_mode; }
+bool plan_sbuild_timed_out(dmrgb200_plan_t plan) { return plan->compiled && sbuild_timed_out(plan->prog); }
 // Autotune the plan's grouped GEMMs once, outside any stream capture (DMRGB200_AUTOTUNE=0
 // keeps the default variant, and so do plans below 50 MFLOP per H psi).
 cudaError_t plan_ensure_tuned(dmrgb200_plan_t plan, const double* x, double* y, cudaStream_t stream) {

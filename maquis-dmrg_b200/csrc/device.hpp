@@ -151,6 +151,7 @@ struct DeviceProgram {
     uint64_t* d_gent_t = nullptr;
     double* d_gent_a = nullptr;
     DevSItem* d_gitems = nullptr;
+    int* d_err = nullptr;  // set by a grouped S build whose bulk-copy wait timed out
     uint32_t n_t1 = 0, n_t3 = 0, n_lines = 0, n_gitems = 0;
     TileLists x1, x3;  // tile lists of the other classes
     DevRow* d_r1 = nullptr;  // stage-1 row table (stacked T tasks)
@@ -249,6 +250,9 @@ cudaError_t run_adjoint(DeviceProgram const& fwd, AdjointProgram const& a, uint6
                         uint64_t gx_elems, double* galpha, double* T, double* S, cudaStream_t stream);
 // stage 2 only (S build), for the emulated path
 cudaError_t run_sbuild(DeviceProgram const& prog, double* T, double* S, cudaStream_t stream);
+// after the stream is synchronised: whether a grouped S build timed out since the
+// last call (the flag is cleared)
+bool sbuild_timed_out(DeviceProgram const& prog);
 // largest K of any output matrix of a GEMM list (emulation needs K * slices <= 2^17)
 uint64_t max_k_total(GemmList const& gl);
 

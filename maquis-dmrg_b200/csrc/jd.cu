@@ -189,10 +189,30 @@ struct Workspace {
 
 using namespace dmrgb200;
 
+namespace dmrgb200 {
+dmrgb200_status solve_stepwise(dmrgb200_plan_t plan, uint64_t n, const double* x0, const double* const* ortho,
+                               uint32_t n_ortho, double tol, uint32_t max_iter, double* energy, double* x_out,
+                               dmrgb200_solve_stats* stats, void* cuda_stream);
+bool plan_sbuild_timed_out(dmrgb200_plan_t plan);
+}  // namespace dmrgb200
+
+// Both solver forms end synchronised; a grouped S build whose wait timed out
+// during the solve turns the result into DMRGB200_TIMEOUT.
 extern "C" dmrgb200_status dmrgb200_solve(dmrgb200_plan_t plan, uint64_t n, const double* x0,
                                           const double* const* ortho, uint32_t n_ortho, double tol, uint32_t max_iter,
                                           double* energy, double* x_out, dmrgb200_solve_stats* stats,
                                           void* cuda_stream) {
+    dmrgb200_status s =
+        dmrgb200::solve_stepwise(plan, n, x0, ortho, n_ortho, tol, max_iter, energy, x_out, stats, cuda_stream);
+    if (s == DMRGB200_OK && plan && dmrgb200::plan_sbuild_timed_out(plan))
+        return noalloc_fail(DMRGB200_TIMEOUT, "S build: a bulk-copy wait timed out");
+    return s;
+}
+
+dmrgb200_status dmrgb200::solve_stepwise(dmrgb200_plan_t plan, uint64_t n, const double* x0,
+                                         const double* const* ortho, uint32_t n_ortho, double tol,
+                                         uint32_t max_iter, double* energy, double* x_out,
+                                         dmrgb200_solve_stats* stats, void* cuda_stream) {
     if (!plan || !x0 || !x_out || !energy || n == 0) return noalloc_fail(DMRGB200_INVALID_ARGUMENT, "null argument");
     if (max_iter < 1 || max_iter > 32) return noalloc_fail(DMRGB200_INVALID_ARGUMENT, "max_iter must be in 1..32");
     if (n_ortho > 8) return noalloc_fail(DMRGB200_INVALID_ARGUMENT, "at most 8 orthogonal vectors");

@@ -21,6 +21,7 @@
 
 #include "../../include/dmrgb200.h"
 #include "device.hpp"
+#include "async_copy.cuh"
 
 namespace dmrgb200 {
 
@@ -370,84 +371,130 @@ __global__ void __launch_bounds__(256) sbuild_lines(const DevSLine* __restrict__
 // S build of line groups (DevSGroup): one warp per work item (a group and a
 // chunk of SG_CHUNK consecutive elements of its lines); every lane owns SG_EPT
 // elements (lane + 32 u) and keeps SG_LINES x SG_EPT accumulators, so each
-// source cell is read once for all lines of the group (the alphas of a cell are
-// one warp-wide broadcast).  Sources come SG_UNROLL at a time (the host pads each
-// group's list with zero-alpha sources): the T values of the next pair of
-// sources are loaded while the current pair is multiplied, every load addressed
-// from one per-lane pointer with constant offsets.  Each line sums its sources
-// in the group's entry order.
-template <bool FULL>
-__device__ __forceinline__ void sg_accumulate(double (&acc)[SG_LINES][SG_EPT], const double* __restrict__ T,
-                                              const uint64_t* __restrict__ ent_t, const double* __restrict__ ent_a,
-                                              uint32_t k0, uint32_t k1, uint32_t e0, uint32_t lane, uint32_t n) {
-    const double* Tl = T + e0 + lane;
-    bool in[SG_EPT];
-#pragma unroll
-    for (int u = 0; u < SG_EPT; ++u) in[u] = FULL || e0 + lane + 32u * u < n;
-    auto load = [&](uint64_t tb, double (&v)[SG_EPT]) {
-        const double* p = Tl + tb;
-#pragma unroll
-        for (int u = 0; u < SG_EPT; ++u) v[u] = in[u] ? __ldg(p + 32 * u) : 0.0;
-    };
-    auto madd = [&](uint32_t k, double const (&v)[SG_EPT]) {
-        const double2* a2 = reinterpret_cast<const double2*>(ent_a + uint64_t(k) * SG_LINES);
-#pragma unroll
-        for (int h = 0; h < SG_LINES / 2; ++h) {
-            const double2 x = __ldg(a2 + h);
-#pragma unroll
-            for (int u = 0; u < SG_EPT; ++u) {
-                acc[2 * h][u] = fma(x.x, v[u], acc[2 * h][u]);
-                acc[2 * h + 1][u] = fma(x.y, v[u], acc[2 * h + 1][u]);
-            }
-        }
-    };
-    double v0[SG_EPT], v1[SG_EPT], v2[SG_EPT], v3[SG_EPT];
-    load(ent_t[k0], v0);
-    load(ent_t[k0 + 1], v1);
-    for (uint32_t k = k0; k < k1; k += SG_UNROLL) {
-        load(ent_t[k + 2], v2);
-        load(ent_t[k + 3], v3);
-        madd(k, v0);
-        madd(k + 1, v1);
-        if (k + SG_UNROLL < k1) {
-            load(ent_t[k + 4], v0);
-            load(ent_t[k + 5], v1);
-        }
-        madd(k + 2, v2);
-        madd(k + 3, v3);
-    }
-}
+// source cell is read once for all lines of the group.  The sources stream
+// through the warp's own shared-memory ring with bulk copies (TMA engine, no
+// multicast): a stage holds SGB_NC source rows of the chunk and their alpha
+// columns; lanes 0 .. SGB_NC - 1 each copy one row and lane SGB_NC the alphas,
+// every lane expecting its own bytes on the stage's mbarrier before lane 0
+// arrives, SGB_STAGES - 1 stages ahead of the multiply-adds.  The copies bypass
+// the L1 miss path, so a warp keeps kilobytes in flight without registers.  A
+// bulk copy starts on a 16-byte boundary, so a row whose first element is odd is
+// copied from one element earlier and read with that shift.  Every wait is
+// bounded (2 s; the thread is suspended while it waits): on a timeout the warp
+// records it in *err, lets its copies land (bounded) and stops.  Each line sums
+// its sources in the group's entry order.
+constexpr int SGB_WARPS = 8, SGB_STAGES = 3, SGB_NC = 4, SGB_ROW = SG_CHUNK + 2;
+struct alignas(16) SgbRing {
+    double rows[SGB_STAGES][SGB_NC][SGB_ROW];
+    double alpha[SGB_STAGES][SGB_NC][SG_LINES];
+    uint64_t full[SGB_STAGES];
+    uint32_t shift[SGB_STAGES][SGB_NC];
+};
+static_assert(sizeof(double) * SGB_ROW % 16 == 0 && sizeof(SgbRing) % 16 == 0, "bulk copy alignment");
+static_assert(SGB_NC < 32, "one lane per row plus one for the alphas");
+constexpr size_t SGB_SMEM = sizeof(SgbRing) * SGB_WARPS;
 
-__global__ void __launch_bounds__(256, 2) sbuild_groups(const DevSGroup* __restrict__ groups,
-                                                     const DevSItem* __restrict__ items, uint32_t n_items,
-                                                     const uint64_t* __restrict__ ent_t,
-                                                     const double* __restrict__ ent_a, double* __restrict__ S,
-                                                     const double* __restrict__ T) {
-    const uint32_t lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
-    for (uint32_t it = blockIdx.x * wpb + (threadIdx.x >> 5); it < n_items; it += gridDim.x * wpb) {
+__global__ void __launch_bounds__(32 * SGB_WARPS, 2) sbuild_groups(const DevSGroup* __restrict__ groups,
+                                                                  const DevSItem* __restrict__ items, uint32_t n_items,
+                                                                  const uint64_t* __restrict__ ent_t,
+                                                                  const double* __restrict__ ent_a,
+                                                                  double* __restrict__ S, const double* __restrict__ T,
+                                                                  int* err) {
+    using namespace async;
+    extern __shared__ __align__(16) unsigned char sgb_smem[];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    SgbRing& R = reinterpret_cast<SgbRing*>(sgb_smem)[warp];
+    if (lane == 0) {
+        for (int i = 0; i < SGB_STAGES; ++i) mbar_init(&R.full[i], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    uint32_t issued = 0, consumed = 0;  // stage fills of this warp, in order (the same in every lane)
+    bool failed = false;
+    for (uint32_t it = blockIdx.x * SGB_WARPS + warp; it < n_items && !failed; it += gridDim.x * SGB_WARPS) {
         const DevSItem I = items[it];
         const DevSGroup G = groups[I.group];
-        const uint32_t n = G.rows * G.cols;
+        const uint32_t n = G.rows * G.cols, e0 = I.e0, cnt = min(uint32_t(SG_CHUNK), n - e0);
+        const uint32_t k0 = G.ent_begin, k1 = G.ent_end;
         double acc[SG_LINES][SG_EPT];
 #pragma unroll
         for (int j = 0; j < SG_LINES; ++j)
 #pragma unroll
             for (int u = 0; u < SG_EPT; ++u) acc[j][u] = 0.0;
-        if (G.ent_begin < G.ent_end) {
-            if (I.e0 + SG_CHUNK <= n)
-                sg_accumulate<true>(acc, T, ent_t, ent_a, G.ent_begin, G.ent_end, I.e0, lane, n);
-            else
-                sg_accumulate<false>(acc, T, ent_t, ent_a, G.ent_begin, G.ent_end, I.e0, lane, n);
+        // every lane: the stage of sources kb .. kb + SGB_NC - 1 (those below k1)
+        auto fill = [&](uint32_t kb) {
+            const uint32_t slot = issued % SGB_STAGES, nc = min(uint32_t(SGB_NC), k1 - kb);
+            if (lane < nc) {
+                const uint64_t tb = ent_t[kb + lane];
+                const uint32_t sh = uint32_t((tb + e0) & 1u), sz = ((cnt + sh) * 8u + 15u) & ~15u;
+                R.shift[slot][lane] = sh;
+                mbar_expect_tx_only(&R.full[slot], sz);
+                bulk_load(R.rows[slot][lane], T + tb + e0 - sh, sz, &R.full[slot]);
+            } else if (lane == uint32_t(SGB_NC)) {
+                const uint32_t sz = nc * SG_LINES * uint32_t(sizeof(double));
+                mbar_expect_tx_only(&R.full[slot], sz);
+                bulk_load(R.alpha[slot], ent_a + uint64_t(kb) * SG_LINES, sz, &R.full[slot]);
+            }
+            __syncwarp();  // every expected byte count is in before the phase can complete
+            if (lane == 0) mbar_arrive(&R.full[slot]);
+            ++issued;
+        };
+        const uint32_t nst = (k1 - k0 + SGB_NC - 1) / SGB_NC;
+        for (uint32_t st = 0; st < min(nst, uint32_t(SGB_STAGES - 1)); ++st) fill(k0 + st * SGB_NC);
+        for (uint32_t st = 0; st < nst; ++st) {
+            const uint32_t slot = consumed % SGB_STAGES, kb = k0 + st * SGB_NC;
+            // the stage SGB_STAGES - 1 ahead goes into the slot freed in the previous step
+            const bool refill = st + SGB_STAGES - 1 < nst;
+            const uint32_t kf = k0 + (st + SGB_STAGES - 1) * SGB_NC;
+            if (refill) {
+                fence_proxy_async_smem();
+                fill(kf);
+            }
+            const bool ok = mbar_wait_suspend(&R.full[slot], (consumed / SGB_STAGES) & 1u, err);
+            if (__any_sync(0xffffffffu, !ok)) {
+                failed = true;
+                break;
+            }
+            const uint32_t nc = min(uint32_t(SGB_NC), k1 - kb);
+#pragma unroll 1
+            for (uint32_t c = 0; c < nc; ++c) {
+                const double* row = R.rows[slot][c] + R.shift[slot][c] + lane;
+                double v[SG_EPT];
+#pragma unroll
+                for (int u = 0; u < SG_EPT; ++u) v[u] = row[32 * u];
+                const double2* a2 = reinterpret_cast<const double2*>(R.alpha[slot][c]);
+#pragma unroll
+                for (int h = 0; h < SG_LINES / 2; ++h) {
+                    const double2 x = a2[h];
+#pragma unroll
+                    for (int u = 0; u < SG_EPT; ++u) {
+                        acc[2 * h][u] = fma(x.x, v[u], acc[2 * h][u]);
+                        acc[2 * h + 1][u] = fma(x.y, v[u], acc[2 * h + 1][u]);
+                    }
+                }
+            }
+            ++consumed;
+            __syncwarp();  // every lane's reads of this slot are done before it is refilled
         }
+        if (failed) break;
 #pragma unroll
         for (int u = 0; u < SG_EPT; ++u) {
-            const uint32_t e = I.e0 + lane + 32u * u;
+            const uint32_t e = e0 + lane + 32u * u;
             if (e >= n) continue;
             const uint32_t col = e / G.rows, i = e - col * G.rows;
             double* dst = S + G.s_base + i + uint64_t(col) * G.ld_s;
 #pragma unroll
             for (int j = 0; j < SG_LINES; ++j)
                 if (uint32_t(j) < G.nlines) dst[uint64_t(j) * G.line_stride] = ((G.mask >> j) & 1u) ? acc[j][u] : 0.0;
+        }
+    }
+    if (failed && lane == 0) {
+        // let the copies still in flight land before the warp's shared memory is released (bounded)
+        for (; consumed < issued; ++consumed) {
+            const unsigned long long t0 = global_ns();
+            while (!mbar_try(&R.full[consumed % SGB_STAGES], (consumed / SGB_STAGES) & 1u) &&
+                   global_ns() - t0 < WAIT_LIMIT_NS) {
+            }
         }
     }
 }
@@ -700,6 +747,9 @@ void compile_program(FlatPlan const& p, std::vector<uint64_t> const& stage3_bnd,
     prog = DeviceProgram();
     const uint32_t nt = p.n_t(), nc = p.n_cohorts();
     std::vector<uint64_t> t_off = t_offsets(p, &prog.t_elems);
+    // slack after the last T block: the grouped S build's bulk copies may read one
+    // element past a source row
+    prog.t_elems += 32;
 
     // ---- stage 1 ----
     GemmList& g1 = prog.stage1;
@@ -934,6 +984,10 @@ cudaError_t upload_program(DeviceProgram& prog) {
     if ((e = up(prog.gent_t, &prog.d_gent_t)) != cudaSuccess) return e;
     if ((e = up(prog.gent_a, &prog.d_gent_a)) != cudaSuccess) return e;
     if ((e = up(prog.gitems, &prog.d_gitems)) != cudaSuccess) return e;
+    if (!prog.gitems.empty()) {
+        if ((e = cudaMalloc(&prog.d_err, sizeof(int))) != cudaSuccess) return e;
+        if ((e = cudaMemset(prog.d_err, 0, sizeof(int))) != cudaSuccess) return e;
+    }
     prog.n_t1 = uint32_t(prog.stage1.tiles.size());
     prog.n_t3 = uint32_t(prog.stage3.tiles.size());
     prog.n_lines = uint32_t(prog.lines.size());
@@ -970,6 +1024,8 @@ void free_program(DeviceProgram& prog) {
     cudaFree(prog.d_gent_t);
     cudaFree(prog.d_gent_a);
     cudaFree(prog.d_gitems);
+    cudaFree(prog.d_err);
+    prog.d_err = nullptr;
     prog.d_groups = nullptr;
     prog.d_gent_t = nullptr;
     prog.d_gent_a = nullptr;
@@ -1149,12 +1205,24 @@ cudaError_t run_sbuild(DeviceProgram const& prog, double* T, double* S, cudaStre
         sbuild_lines<<<grid, 256, 0, stream>>>(prog.d_lines, prog.d_terms, prog.n_lines, S, T);
     }
     if (prog.n_gitems) {
-        // 8 warps per CTA, up to two CTAs per SM resident
-        uint32_t grid = std::min<uint32_t>((prog.n_gitems + 7) / 8, sms * 2);
-        sbuild_groups<<<grid, 256, 0, stream>>>(prog.d_groups, prog.d_gitems, prog.n_gitems, prog.d_gent_t,
-                                                prog.d_gent_a, S, T);
+        static const bool smem_ok =
+            cudaFuncSetAttribute(sbuild_groups, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SGB_SMEM)) ==
+            cudaSuccess;
+        if (!smem_ok) return cudaErrorInvalidConfiguration;
+        // SGB_WARPS warps per CTA, up to two CTAs per SM resident
+        uint32_t grid = std::min<uint32_t>((prog.n_gitems + SGB_WARPS - 1) / SGB_WARPS, sms * 2);
+        sbuild_groups<<<grid, 32 * SGB_WARPS, SGB_SMEM, stream>>>(prog.d_groups, prog.d_gitems, prog.n_gitems,
+                                                                  prog.d_gent_t, prog.d_gent_a, S, T, prog.d_err);
     }
     return cudaGetLastError();
+}
+
+bool sbuild_timed_out(DeviceProgram const& prog) {
+    if (!prog.d_err) return false;
+    int v = 0;
+    if (cudaMemcpy(&v, prog.d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return false;
+    if (v) cudaMemset(prog.d_err, 0, sizeof(int));
+    return v != 0;
 }
 
 uint64_t max_k_total(GemmList const& gl) {
@@ -1185,7 +1253,8 @@ cudaError_t run_program(DeviceProgram const& prog, uint64_t in, uint64_t out, do
     if (ev) cudaEventRecord(ev[0], stream);
     launch_variant(prog.var1, prog.d_p1, prog.d_s1, prog.d_t1, prog.n_t1, prog.x1, prog.d_r1, bs, stream);
     if (ev) cudaEventRecord(ev[1], stream);
-    run_sbuild(prog, T, S, stream);
+    cudaError_t e = run_sbuild(prog, T, S, stream);
+    if (e != cudaSuccess) return e;
     if (ev) cudaEventRecord(ev[2], stream);
     launch_variant(prog.var3, prog.d_p3, prog.d_s3, prog.d_t3, prog.n_t3, prog.x3, nullptr, bs, stream);
     if (ev) cudaEventRecord(ev[3], stream);

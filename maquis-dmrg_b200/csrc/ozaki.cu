@@ -27,6 +27,7 @@
 
 #include "../../include/dmrgb200.h"
 #include "device.hpp"
+#include "async_copy.cuh"
 
 namespace dmrgb200 {
 
@@ -37,16 +38,7 @@ namespace {
 constexpr int OZ_BM = 128, OZ_BN = 64, OZ_BK = 64;        // tile rows, tile columns, K bytes per slab
 constexpr int A_TILE = OZ_BM * OZ_BK, B_TILE = OZ_BN * OZ_BK;
 constexpr int OZ_THREADS = 128, OZ_STAGES = 2, OZ_MAX_SLICES = 8;
-constexpr unsigned long long WAIT_LIMIT_NS = 2000000000ull;  // 2 s
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ unsigned long long global_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
-    return t;
-}
+using namespace async;
 
 // byte offset of element (r, k) of a (rows x 64-byte) K-major tile in the
 // canonical no-swizzle layout: 8x16-byte core matrices, LBO = 128 B along K,
@@ -71,41 +63,6 @@ __host__ __device__ constexpr uint32_t idesc_i8(int M, int N) {
            | (uint32_t(M >> 4) << 24);     // M / 16   (both operands K-major, no negation)
 }
 
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// bounded wait; false (and *err set) when the phase does not complete in time
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
-    unsigned long long t0 = global_ns();
-    while (!mbar_try(bar, parity)) {
-        if (*reinterpret_cast<volatile int*>(err)) return false;
-        if (global_ns() - t0 > WAIT_LIMIT_NS) {
-            atomicExch(err, 1);
-            return false;
-        }
-    }
-    return true;
-}
-__device__ __forceinline__ void bulk_load(void* smem, const void* gmem, uint32_t bytes, uint64_t* bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(smem)),
-                 "l"(gmem), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
 __device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accum) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"

@@ -38,6 +38,12 @@ __device__ __forceinline__ const double* op_base(Bases const& bs, DevOp const& o
     return reinterpret_cast<const double*>(base_of(bs, op.buf) + 8ull * (op.off + uint64_t(batch) * op.bstride));
 }
 
+// Kernels launched with programmatic stream serialisation (launch_pdl) may be
+// scheduled while the previous kernel of the stream drains; each starts with this
+// wait, so none touches memory before its predecessor has completed and its
+// writes are visible.
+__device__ __forceinline__ void wait_for_predecessor() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
                  : "+d"(c0), "+d"(c1)
@@ -162,6 +168,7 @@ __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb
                   "tile shape");
     __shared__ __align__(16) double As[STAGES][BK_][pitch<BM_>()];
     __shared__ __align__(16) double Bs[STAGES][BK_][pitch<BN_>()];
+    wait_for_predecessor();
 
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
@@ -317,6 +324,7 @@ __global__ void __launch_bounds__(256) sbuild_lines(const DevSLine* __restrict__
                                                     double* __restrict__ S, const double* __restrict__ T) {
     __shared__ double s_alpha[SB_TERMS];
     __shared__ uint64_t s_base[SB_TERMS];
+    wait_for_predecessor();
     for (uint32_t li = blockIdx.x; li < n_lines; li += gridDim.x) {
         const DevSLine L = lines[li];
         if (!L.rows || !L.cols) continue;
@@ -383,7 +391,7 @@ __global__ void __launch_bounds__(256) sbuild_lines(const DevSLine* __restrict__
 // bounded (2 s; the thread is suspended while it waits): on a timeout the warp
 // records it in *err, lets its copies land (bounded) and stops.  Each line sums
 // its sources in the group's entry order.
-constexpr int SGB_WARPS = 8, SGB_STAGES = 3, SGB_NC = 4, SGB_ROW = SG_CHUNK + 2;
+constexpr int SGB_WARPS = 4, SGB_MINB = 3, SGB_STAGES = 2, SGB_NC = 8, SGB_ROW = SG_CHUNK + 2;
 struct alignas(16) SgbRing {
     double rows[SGB_STAGES][SGB_NC][SGB_ROW];
     double alpha[SGB_STAGES][SGB_NC][SG_LINES];
@@ -394,7 +402,7 @@ static_assert(sizeof(double) * SGB_ROW % 16 == 0 && sizeof(SgbRing) % 16 == 0, "
 static_assert(SGB_NC < 32, "one lane per row plus one for the alphas");
 constexpr size_t SGB_SMEM = sizeof(SgbRing) * SGB_WARPS;
 
-__global__ void __launch_bounds__(32 * SGB_WARPS, 2) sbuild_groups(const DevSGroup* __restrict__ groups,
+__global__ void __launch_bounds__(32 * SGB_WARPS, SGB_MINB) sbuild_groups(const DevSGroup* __restrict__ groups,
                                                                   const DevSItem* __restrict__ items, uint32_t n_items,
                                                                   const uint64_t* __restrict__ ent_t,
                                                                   const double* __restrict__ ent_a,
@@ -404,6 +412,7 @@ __global__ void __launch_bounds__(32 * SGB_WARPS, 2) sbuild_groups(const DevSGro
     extern __shared__ __align__(16) unsigned char sgb_smem[];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     SgbRing& R = reinterpret_cast<SgbRing*>(sgb_smem)[warp];
+    wait_for_predecessor();
     if (lane == 0) {
         for (int i = 0; i < SGB_STAGES; ++i) mbar_init(&R.full[i], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -1120,6 +1129,25 @@ int variant_occupancy(int v) {
 
 // t / n: the tile list of class 0; x: the other classes (a variant whose list is
 // absent falls back to variant 0)
+// Launch with programmatic stream serialisation (the kernel must begin with
+// wait_for_predecessor): its CTAs can be scheduled while the previous kernel's last
+// CTAs finish, which hides most of the launch gap between the H·psi stages.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), uint32_t grid, uint32_t block, size_t smem, cudaStream_t stream,
+                       Args... args) {
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 cudaError_t launch_variant(int v, const DevProb* p, const DevSeg* sg, const DevTile* t, uint32_t n,
                            TileLists const& x, const DevRow* rows, Bases const& bs, cudaStream_t stream) {
     if (!n) return cudaSuccess;
@@ -1131,8 +1159,7 @@ cudaError_t launch_variant(int v, const DevProb* p, const DevSeg* sg, const DevT
         n = x.n[c];
     }
     uint32_t grid = std::min<uint32_t>(n, uint32_t(device_sm_count()) * variant_occupancy(v));
-    kVariants[v].fn<<<grid, kVariants[v].threads, 0, stream>>>(p, sg, t, n, rows, bs);
-    return cudaGetLastError();
+    return launch_pdl(kVariants[v].fn, grid, uint32_t(kVariants[v].threads), 0, stream, p, sg, t, n, rows, bs);
 }
 }  // namespace
 
@@ -1202,17 +1229,23 @@ cudaError_t run_sbuild(DeviceProgram const& prog, double* T, double* S, cudaStre
     const uint32_t sms = uint32_t(device_sm_count());
     if (prog.n_lines) {
         uint32_t grid = std::min<uint32_t>(prog.n_lines, sms * 8);
-        sbuild_lines<<<grid, 256, 0, stream>>>(prog.d_lines, prog.d_terms, prog.n_lines, S, T);
+        cudaError_t e = launch_pdl(sbuild_lines, grid, 256, 0, stream, prog.d_lines, prog.d_terms, prog.n_lines, S,
+                                   static_cast<const double*>(T));
+        if (e != cudaSuccess) return e;
     }
     if (prog.n_gitems) {
         static const bool smem_ok =
             cudaFuncSetAttribute(sbuild_groups, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SGB_SMEM)) ==
             cudaSuccess;
         if (!smem_ok) return cudaErrorInvalidConfiguration;
-        // SGB_WARPS warps per CTA, up to two CTAs per SM resident
-        uint32_t grid = std::min<uint32_t>((prog.n_gitems + SGB_WARPS - 1) / SGB_WARPS, sms * 2);
-        sbuild_groups<<<grid, 32 * SGB_WARPS, SGB_SMEM, stream>>>(prog.d_groups, prog.d_gitems, prog.n_gitems,
-                                                                  prog.d_gent_t, prog.d_gent_a, S, T, prog.d_err);
+        // SGB_WARPS warps per CTA, SGB_MINB CTAs per SM resident
+        uint32_t grid = std::min<uint32_t>((prog.n_gitems + SGB_WARPS - 1) / SGB_WARPS, sms * SGB_MINB);
+        cudaError_t e = launch_pdl(sbuild_groups, grid, 32 * SGB_WARPS, SGB_SMEM, stream,
+                                   static_cast<const DevSGroup*>(prog.d_groups), static_cast<const DevSItem*>(prog.d_gitems),
+                                   prog.n_gitems, static_cast<const uint64_t*>(prog.d_gent_t),
+                                   static_cast<const double*>(prog.d_gent_a), S, static_cast<const double*>(T),
+                                   prog.d_err);
+        if (e != cudaSuccess) return e;
     }
     return cudaGetLastError();
 }

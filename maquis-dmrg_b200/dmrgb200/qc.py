@@ -287,3 +287,112 @@ def operator_model(model: Model, terms: list) -> Model:
     mpo = build_mpo(terms, L, model.local, model.phys)
     return Model(model.name + "_operator", model.symm, model.phys, model.local, mpo, model.total_charge, terms,
                  fermionic_ops=model.fermionic_ops)
+
+
+# ---- integral files -------------------------------------------------------------------
+#
+# The reference's integral text format (models/chem/parse_integrals.h:36-62, 134-146):
+# four header lines, then records "value i j k l" with 1-based orbital indices,
+# 0 for an absent index: (ij|kl) as "v i j k l", h_ij as "v i j 0 0", the core
+# energy as "v 0 0 0 0".  Only one representative of each symmetry orbit is listed.
+# The binary form (the `integrals` parameter, parse_integrals.h:64-80) is all
+# values as doubles followed by all indices as 32-bit ints, four per record.
+
+def integral_records(h: np.ndarray, eri: np.ndarray, core: float = 0.0, tol: float = 0.0):
+    """(values, indices[n, 4]) of the unique entries: (ij|kl) with i >= j, k >= l and
+    (i, j) >= (k, l) (pairs compared as i*(i+1)/2 + j), h_ij with i >= j, then the core
+    energy; 1-based indices, entries with |value| <= tol skipped (the core always kept)."""
+    L = h.shape[0]
+    vals, idx = [], []
+    for i in range(L):
+        for j in range(i + 1):
+            ij = i * (i + 1) // 2 + j
+            for k in range(L):
+                for l in range(k + 1):
+                    if k * (k + 1) // 2 + l > ij:
+                        continue
+                    v = float(eri[i, j, k, l])
+                    if abs(v) > tol:
+                        vals.append(v)
+                        idx.append((i + 1, j + 1, k + 1, l + 1))
+    for i in range(L):
+        for j in range(i + 1):
+            v = float(h[i, j])
+            if abs(v) > tol:
+                vals.append(v)
+                idx.append((i + 1, j + 1, 0, 0))
+    vals.append(float(core))
+    idx.append((0, 0, 0, 0))
+    return np.array(vals), np.array(idx, dtype=np.int32).reshape(-1, 4)
+
+
+def write_integrals(path, h: np.ndarray, eri: np.ndarray, core: float = 0.0, tol: float = 0.0,
+                    header=("synthetic integrals", "", "", "")) -> int:
+    """Write the text format (values to 17 significant digits, so they read back
+    exactly); returns the number of records."""
+    vals, idx = integral_records(h, eri, core, tol)
+    with open(path, "w") as f:
+        for line in list(header)[:4] + [""] * (4 - len(header)):
+            f.write(line + "\n")
+        for v, (i, j, k, l) in zip(vals, idx):
+            f.write(f"{v:.17g} {i} {j} {k} {l}\n")
+    return len(vals)
+
+
+def integrals_buffer(h: np.ndarray, eri: np.ndarray, core: float = 0.0, tol: float = 0.0) -> bytes:
+    """The binary form: all values (float64), then all indices (int32, four per record)."""
+    vals, idx = integral_records(h, eri, core, tol)
+    return vals.astype("<f8").tobytes() + idx.astype("<i4").tobytes()
+
+
+def _expand(vals, idx, L: int, order=None, cutoff: float = 0.0):
+    """h, eri (8-fold symmetric) and the core energy from records; `order` (1-based,
+    the orbital at each site, as the reference's orbital_order) maps orbitals to sites."""
+    if order is None:
+        site = np.arange(L)
+    else:
+        order = np.asarray(order) - 1
+        if sorted(order.tolist()) != list(range(L)):
+            raise ValueError("orbital_order must be a permutation of 1..L")
+        site = np.empty(L, dtype=int)
+        site[order] = np.arange(L)
+    h = np.zeros((L, L))
+    eri = np.zeros((L, L, L, L))
+    core = 0.0
+    for v, rec in zip(vals, idx):
+        if abs(v) <= cutoff and tuple(rec) != (0, 0, 0, 0):
+            continue
+        i, j, k, l = (int(x) for x in rec)
+        if (i, j, k, l) == (0, 0, 0, 0):
+            core += v
+        elif k == 0 and l == 0:
+            a, b = site[i - 1], site[j - 1]
+            h[a, b] = h[b, a] = v
+        else:
+            a, b, c, d = site[i - 1], site[j - 1], site[k - 1], site[l - 1]
+            for p in integral_orbit("eri", (a, b, c, d)):
+                eri[p] = v
+    return h, eri, core
+
+
+def read_integrals(path, L: int, order=None, cutoff: float = 0.0):
+    """Parse the text format: skip four header lines, read records of five numbers."""
+    with open(path) as f:
+        for _ in range(4):
+            f.readline()
+        raw = np.array(f.read().split(), dtype=np.float64)
+    if raw.size % 5:
+        raise ValueError("integral parsing failed: the record count is not a multiple of 5")
+    rec = raw.reshape(-1, 5)
+    return _expand(rec[:, 0], rec[:, 1:].astype(int), L, order, cutoff)
+
+
+def parse_integrals_buffer(buf: bytes, L: int, order=None, cutoff: float = 0.0):
+    """Parse the binary form."""
+    line = 8 + 4 * 4
+    if len(buf) % line:
+        raise ValueError("integral buffer parsing failed: size is not a multiple of one record")
+    n = len(buf) // line
+    vals = np.frombuffer(buf[:8 * n], dtype="<f8")
+    idx = np.frombuffer(buf[8 * n:], dtype="<i4").reshape(n, 4)
+    return _expand(vals, idx, L, order, cutoff)

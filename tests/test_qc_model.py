@@ -96,3 +96,50 @@ def test_integral_derivative_equals_operator_expectation(which, index):
     oc = OracleChain(qc.operator_model(model, terms), bonds, tensors, i)
     expect = float(psi @ oc.hpsi(psi))
     assert abs(grad - expect) <= 1e-11 * max(1.0, abs(expect)), (grad, expect)
+
+
+def test_integral_file_round_trip(tmp_path):
+    """The reference's integral text format (unique entries, 1-based, 0 for absent
+    indices) and its binary buffer both read back the synthetic integrals exactly."""
+    L = 5
+    h, eri = qc.synthetic_integrals(L)
+    path = tmp_path / "FCIDUMP"
+    n = qc.write_integrals(path, h, eri, core=1.25)
+    P = L * (L + 1) // 2
+    assert n == P * (P + 1) // 2 + P + 1
+    lines = path.read_text().splitlines()
+    assert len(lines) == 4 + n and lines[-1].split()[1:] == ["0", "0", "0", "0"]
+    h2, eri2, core = qc.read_integrals(path, L)
+    assert np.array_equal(h2, h) and np.array_equal(eri2, eri) and core == 1.25
+    h3, eri3, core3 = qc.parse_integrals_buffer(qc.integrals_buffer(h, eri, core=1.25), L)
+    assert np.array_equal(h3, h) and np.array_equal(eri3, eri) and core3 == 1.25
+
+
+def test_integral_file_orbital_order(tmp_path):
+    """orbital_order (1-based, the orbital placed at each site) permutes the integrals."""
+    L = 4
+    h, eri = qc.synthetic_integrals(L)
+    path = tmp_path / "FCIDUMP"
+    qc.write_integrals(path, h, eri)
+    order = [3, 1, 4, 2]
+    h2, eri2, _ = qc.read_integrals(path, L, order=order)
+    o = np.array(order) - 1
+    assert np.array_equal(h2, h[np.ix_(o, o)])
+    assert np.array_equal(eri2, eri[np.ix_(o, o, o, o)])
+
+
+def test_integral_file_cutoff_and_errors(tmp_path):
+    L = 3
+    h, eri = qc.synthetic_integrals(L)
+    path = tmp_path / "FCIDUMP"
+    qc.write_integrals(path, h, eri)
+    h2, eri2, _ = qc.read_integrals(path, L, cutoff=0.05)
+    keep = np.abs(eri) > 0.05
+    assert np.array_equal(eri2[keep], eri[keep]) and not np.any(eri2[~keep])
+    assert np.array_equal(h2[np.abs(h) > 0.05], h[np.abs(h) > 0.05])
+    bad = tmp_path / "bad"
+    bad.write_text("a\nb\nc\nd\n1.0 1 1 0\n")
+    with pytest.raises(ValueError):
+        qc.read_integrals(bad, L)
+    with pytest.raises(ValueError):
+        qc.parse_integrals_buffer(b"\0" * 23, L)

@@ -155,6 +155,84 @@ def cpu_reference(model, bonds, tensors, i, psi, seconds=15.0, threads=None):
                      if use_ref else "oracle restatement of the reference CPU path") + ", OpenMP + OpenBLAS"}
 
 
+def steps_workload(args):
+    """Boundary steps (overlap_mpo_left_step / overlap_mpo_right_step) at the middle of
+    the Hubbard L=64 m=1024 chain: the left step at site L/2-2 (building the left
+    boundary of the middle pair) and the right step at site L/2+1, each timed on the
+    device through the step plan's stage events (the host-side lowering excluded),
+    L2 flushed between calls.  Flop rate by the reference's formula; byte rate over
+    |L_in| + |A_ket| + |A_bra| + |L_out| (the boundary-step roofline bytes: T and S
+    intermediates excluded); one JSON line."""
+    import ctypes as C
+
+    import torch
+
+    from dmrgb200 import _capi as capi
+    from dmrgb200 import engine as E
+    from dmrgb200 import models as M
+
+    model, bonds, tensors, i, _ = build_workload()
+    ctx = E.Context(0)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    L = L_SITES
+    pl, pr = i - 1, i + 2
+    # left chain up to site pl, right chain down to site pr + 1 (untimed)
+    Lidx = E.edge_bindex(model.symm, bonds[0])
+    Lbuf = E.to_device(Lidx.edge_values())
+    for p in range(pl):
+        W = M.MPOHandle(model.mpo[p], model.symm)
+        t = tensors[p]
+        Lidx, Lbuf = E.device_left_step(ctx, model.phys, bonds[p], bonds[p + 1], W, Lidx, Lbuf,
+                                        E.to_device(t.data), E.to_device(t.left_paired()))
+    Ridx = E.edge_bindex(model.symm, bonds[L])
+    Rbuf = E.to_device(Ridx.edge_values())
+    for p in range(L - 1, pr, -1):
+        W = M.MPOHandle(model.mpo[p], model.symm)
+        td = E.to_device(tensors[p].data)
+        Ridx, Rbuf = E.device_right_step(ctx, model.phys, bonds[p], bonds[p + 1], W, Ridx, Rbuf, td, td)
+    res = {}
+    for side, p in (("left", pl), ("right", pr)):
+        W = M.MPOHandle(model.mpo[p], model.symm)
+        t = tensors[p]
+        ket = E.to_device(t.data)
+        if side == "left":
+            sched, nidx = E.schedule_left_step(model.phys, bonds[p], bonds[p + 1], W, Lidx, True)
+            plan = E.DevicePlan(ctx, sched.plan, left_addr=Lidx.cohort_addresses(Lbuf.data_ptr()))
+            bra = E.to_device(t.left_paired())
+            n_in = Lidx.n_elems
+        else:
+            sched, nidx = E.schedule_right_step(model.phys, bonds[p], bonds[p + 1], W, Ridx, True)
+            plan = E.DevicePlan(ctx, sched.plan, other_addr=Ridx.cohort_addresses(Rbuf.data_ptr()))
+            bra = ket
+            n_in = Ridx.n_elems
+        out = torch.zeros(max(nidx.n_elems, 1), dtype=torch.float64, device="cuda")
+        addr = nidx.cohort_addresses(out.data_ptr())
+        for _ in range(args.warmup):
+            plan.step(ket.data_ptr(), bra.data_ptr(), addr)
+        capi.check(capi.lib.dmrgb200_plan_set_timing(plan.handle, 1), "set_timing")
+        torch.cuda.profiler.start()  # the profiler range holds only the timed steps
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            plan.step(ket.data_ptr(), bra.data_ptr(), addr)
+        torch.cuda.profiler.stop()
+        ms3, fl3, calls = (C.c_double * 3)(), (C.c_uint64 * 3)(), C.c_uint64()
+        capi.check(capi.lib.dmrgb200_plan_stage_times(plan.handle, ms3, fl3, C.byref(calls)), "stage_times")
+        nc = max(int(calls.value), 1)
+        stage_ms = [ms3[k] / nc for k in range(3)]
+        ms = sum(stage_ms)
+        nbytes = 8 * (n_in + 2 * t.data.size + nidx.n_elems)
+        res[side] = {"site": p, "ms_per_step": ms, "stage_ms": stage_ms,
+                     "gflops": plan.flops / (ms * 1e-3) / 1e9, "flops_per_step": int(plan.flops),
+                     "roofline_bytes_per_step": int(nbytes), "gbs": nbytes / (ms * 1e-3) / 1e9,
+                     "hbm_frac_of_measured": nbytes / (ms * 1e-3) / 1e9 / hbm_peak()}
+    line = {"metric": "boundary step GFLOP/s (FP64)", "value": res["left"]["gflops"], "unit": "GFLOP/s",
+            "higher_is_better": True, "n_gpus": 1, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "fermi_hubbard_L64_twou1_m1024_boundary_steps_middle", "sites": L,
+                       "bond_dim": M_BOND, "steps": args.steps, "l2": "flushed (256 MiB write)"},
+            "left_step": res["left"], "right_step": res["right"]}
+    print(json.dumps(line), flush=True)
+
+
 def sweep_workload(args):
     """Heisenberg sweeps: L=32, J=1, U1 (Sz=0), two-site DMRG, m=128,
     4 sweeps, JD tol 1e-8 (max 8 iterations), seeded random initial MPS (every
@@ -525,12 +603,13 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--workload", default="hpsi",
-                    choices=["hpsi", "sweep", "batched", "solve", "gemm", "qc", "adjoint"],
+                    choices=["hpsi", "sweep", "batched", "solve", "gemm", "qc", "adjoint", "steps"],
                     help="hpsi: the headline H·psi line (default); sweep: Heisenberg L=32 sweeps; batched: 64 "
                          "instances in one plan; solve: Jacobi-Davidson solves of the Hubbard L=64 site problem; "
                          "gemm: the DMMA kernel on "
                          "a regular 4096^3 GEMM; qc: a quantum-chemistry site problem; adjoint: the adjoint "
-                         "checked by finite differences and RDM elements on a quantum-chemistry site problem")
+                         "checked by finite differences and RDM elements on a quantum-chemistry site problem; "
+                         "steps: the left and right boundary steps at the middle of the Hubbard chain")
     ap.add_argument("--qc-sites", type=int, default=24, help="orbitals of the qc workload")
     ap.add_argument("--qc-m", type=int, default=2000, help="bond dimension of the qc workload")
     ap.add_argument("--adj-sites", type=int, default=16, help="orbitals of the adjoint workload")
@@ -559,6 +638,9 @@ def main():
         os._exit(0)
     if args.workload == "adjoint":
         adjoint_workload(args)
+        os._exit(0)
+    if args.workload == "steps":
+        steps_workload(args)
         os._exit(0)
 
     rank = int(os.environ.get("RANK", "0"))

@@ -240,8 +240,10 @@ dmrgb200_status dmrgb200_hpsi_adjoint(dmrgb200_plan_t plan, const double* w, con
  * its row / column maxima (7: below 1e-13, 6: about 1e-11, 5: about 1e-9). */
 dmrgb200_status dmrgb200_plan_set_slices(dmrgb200_plan_t plan, int slices);
 
-/* Per-stage timing of H·psi executions: when enabled, every dmrgb200_hpsi call
- * records CUDA events around its stages on the call's stream.
+/* Per-stage timing of H·psi executions and boundary steps: when enabled, every
+ * dmrgb200_hpsi / dmrgb200_step_execute call records CUDA events around its
+ * stages on the call's stream (device time only, not the host-side lowering of
+ * a step plan).
  * dmrgb200_plan_stage_times synchronises the last recorded events and returns
  * the accumulated milliseconds and the number of timed calls; stage 0 = T
  * GEMMs (create_T), 1 = S build (create_s_r), 2 = cohort contraction

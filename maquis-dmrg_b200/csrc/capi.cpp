@@ -264,10 +264,15 @@ dmrgb200_status run_step(dmrgb200_plan_s* p, const double* ket, const double* br
         free_program(prog);
         return cuda_fail(e, "step S scratch");
     }
-    e = run_program(prog, reinterpret_cast<uint64_t>(ket), reinterpret_cast<uint64_t>(bra), T, S, stream);
+    e = run_program(prog, reinterpret_cast<uint64_t>(ket), reinterpret_cast<uint64_t>(bra), T, S, stream,
+                    p->timing ? p->ev : nullptr);
     cudaFreeAsync(T, stream);
     cudaFreeAsync(S, stream);
     cudaError_t e2 = cudaStreamSynchronize(stream);
+    if (p->timing && e == cudaSuccess && e2 == cudaSuccess) {
+        p->pending = true;  // the device time of the three stages, without the host-side lowering
+        p->collect();
+    }
     const bool timed_out = e2 == cudaSuccess && sbuild_timed_out(prog);
     free_program(prog);
     if (e != cudaSuccess) return cuda_fail(e, "step launch");

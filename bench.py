@@ -267,6 +267,7 @@ def sweep_workload(args):
             "sweep_seconds": dev.log.sweep_seconds, "final_energy": float(ed[-1]),
             "max_abs_energy_diff_vs_oracle": float(np.max(np.abs(ed - ec))),
             "hpsi_calls": dev.log.hpsi_calls, "solve_device_ms": dev.log.solve_ms,
+            "phase_seconds": dev.log.phase_seconds, "site_problem_phase_seconds": dev.be.phase_seconds,
             "cpu_oracle_sweep_seconds": cpu.log.sweep_seconds, "cpu_oracle_final_energy": float(ec[-1]),
             "note": "two-site formation and SVD truncation on the host (numpy); H·psi, JD and boundary steps on the device"}
     print(json.dumps(line), flush=True)

@@ -152,6 +152,7 @@ struct DeviceProgram {
     double* d_gent_a = nullptr;
     DevSItem* d_gitems = nullptr;
     int* d_err = nullptr;  // set by a grouped S build whose bulk-copy wait timed out
+    unsigned char* d_arena = nullptr;  // the one allocation holding every table above
     uint32_t n_t1 = 0, n_t3 = 0, n_lines = 0, n_gitems = 0;
     TileLists x1, x3;  // tile lists of the other classes
     DevRow* d_r1 = nullptr;  // stage-1 row table (stacked T tasks)

@@ -817,7 +817,12 @@ void compile_program(FlatPlan const& p, std::vector<uint64_t> const& stage3_bnd,
             std::vector<int64_t> line_of(p.c_nsrows[c], -1);
             for (uint32_t l = p.u_line[u]; l < p.u_line[u + 1]; ++l) line_of[p.l_b1[l]] = l;
             const uint64_t w = uint64_t(p.u_ms[u]) * (p.kind == KIND_LEFT ? p.c_rs[c] : p.c_ls[c]);
-            if (mode != 1 && w) {
+            // the group construction is tried only where lines average 4 or more terms: sparser
+            // units (Heisenberg, Hubbard: about two terms per line) keep the line walk without
+            // paying for the trial, which would cost more host time than it could save
+            const uint64_t unit_terms = p.l_term[p.u_line[u + 1]] - p.l_term[p.u_line[u]];
+            const bool dense_enough = unit_terms >= 4ull * (p.u_line[u + 1] - p.u_line[u]);
+            if (mode != 1 && w && (mode == 2 || dense_enough)) {
                 // line groups when they issue at most twice the per-line walk's multiply-adds
                 // (a unit without terms is zero-filled by the line walk)
                 const size_t g0 = ug.groups.size(), e0 = ug.ent_t.size();
@@ -972,31 +977,74 @@ cudaError_t up(std::vector<T> const& v, T** d) {
 }
 }  // namespace
 
+namespace {
+// All tables of a program in one device allocation: packed into one host buffer
+// (each table 256-byte aligned), copied with one transfer, freed with one call.
+struct TablePacker {
+    std::vector<unsigned char> host;
+    static constexpr size_t NONE = ~size_t(0);
+    template <class T>
+    size_t add(std::vector<T> const& v) {
+        if (v.empty()) return NONE;
+        const size_t off = (host.size() + 255) / 256 * 256;
+        host.resize(off + v.size() * sizeof(T));
+        std::memcpy(host.data() + off, v.data(), v.size() * sizeof(T));
+        return off;
+    }
+    size_t zeros(size_t bytes) {
+        const size_t off = (host.size() + 255) / 256 * 256;
+        host.resize(off + bytes, 0);
+        return off;
+    }
+};
+template <class T>
+T* at(unsigned char* base, size_t off) {
+    return off == TablePacker::NONE ? nullptr : reinterpret_cast<T*>(base + off);
+}
+}  // namespace
+
 cudaError_t upload_program(DeviceProgram& prog) {
-    cudaError_t e;
-    if ((e = up(prog.stage1.probs, &prog.d_p1)) != cudaSuccess) return e;
-    if ((e = up(prog.stage1.segs, &prog.d_s1)) != cudaSuccess) return e;
-    if ((e = up(prog.stage1.tiles, &prog.d_t1)) != cudaSuccess) return e;
-    if ((e = up(prog.stage3.probs, &prog.d_p3)) != cudaSuccess) return e;
-    if ((e = up(prog.stage3.segs, &prog.d_s3)) != cudaSuccess) return e;
-    if ((e = up(prog.stage3.tiles, &prog.d_t3)) != cudaSuccess) return e;
-    if ((e = up(prog.stage1.rowtab, &prog.d_r1)) != cudaSuccess) return e;
+    TablePacker pk;
+    const size_t o_p1 = pk.add(prog.stage1.probs), o_s1 = pk.add(prog.stage1.segs), o_t1 = pk.add(prog.stage1.tiles);
+    const size_t o_p3 = pk.add(prog.stage3.probs), o_s3 = pk.add(prog.stage3.segs), o_t3 = pk.add(prog.stage3.tiles);
+    const size_t o_r1 = pk.add(prog.stage1.rowtab);
+    size_t o_x1[N_TILE_CLASSES], o_x3[N_TILE_CLASSES];
     for (int c = 1; c < N_TILE_CLASSES; ++c) {
-        if ((e = up(prog.stage1.tiles_cls[c], &prog.x1.t[c])) != cudaSuccess) return e;
-        if ((e = up(prog.stage3.tiles_cls[c], &prog.x3.t[c])) != cudaSuccess) return e;
+        o_x1[c] = pk.add(prog.stage1.tiles_cls[c]);
+        o_x3[c] = pk.add(prog.stage3.tiles_cls[c]);
+    }
+    const size_t o_l = pk.add(prog.lines), o_k = pk.add(prog.terms);
+    const size_t o_g = pk.add(prog.groups), o_gt = pk.add(prog.gent_t), o_ga = pk.add(prog.gent_a);
+    const size_t o_gi = pk.add(prog.gitems);
+    const size_t o_err = prog.gitems.empty() ? TablePacker::NONE : pk.zeros(sizeof(int));
+    prog.d_arena = nullptr;
+    if (!pk.host.empty()) {
+        cudaError_t e = cudaMalloc(&prog.d_arena, pk.host.size());
+        if (e != cudaSuccess) return e;
+        if ((e = cudaMemcpy(prog.d_arena, pk.host.data(), pk.host.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+            return e;
+    }
+    unsigned char* b = prog.d_arena;
+    prog.d_p1 = at<DevProb>(b, o_p1);
+    prog.d_s1 = at<DevSeg>(b, o_s1);
+    prog.d_t1 = at<DevTile>(b, o_t1);
+    prog.d_p3 = at<DevProb>(b, o_p3);
+    prog.d_s3 = at<DevSeg>(b, o_s3);
+    prog.d_t3 = at<DevTile>(b, o_t3);
+    prog.d_r1 = at<DevRow>(b, o_r1);
+    for (int c = 1; c < N_TILE_CLASSES; ++c) {
+        prog.x1.t[c] = at<DevTile>(b, o_x1[c]);
+        prog.x3.t[c] = at<DevTile>(b, o_x3[c]);
         prog.x1.n[c] = uint32_t(prog.stage1.tiles_cls[c].size());
         prog.x3.n[c] = uint32_t(prog.stage3.tiles_cls[c].size());
     }
-    if ((e = up(prog.lines, &prog.d_lines)) != cudaSuccess) return e;
-    if ((e = up(prog.terms, &prog.d_terms)) != cudaSuccess) return e;
-    if ((e = up(prog.groups, &prog.d_groups)) != cudaSuccess) return e;
-    if ((e = up(prog.gent_t, &prog.d_gent_t)) != cudaSuccess) return e;
-    if ((e = up(prog.gent_a, &prog.d_gent_a)) != cudaSuccess) return e;
-    if ((e = up(prog.gitems, &prog.d_gitems)) != cudaSuccess) return e;
-    if (!prog.gitems.empty()) {
-        if ((e = cudaMalloc(&prog.d_err, sizeof(int))) != cudaSuccess) return e;
-        if ((e = cudaMemset(prog.d_err, 0, sizeof(int))) != cudaSuccess) return e;
-    }
+    prog.d_lines = at<DevSLine>(b, o_l);
+    prog.d_terms = at<DevSTerm>(b, o_k);
+    prog.d_groups = at<DevSGroup>(b, o_g);
+    prog.d_gent_t = at<uint64_t>(b, o_gt);
+    prog.d_gent_a = at<double>(b, o_ga);
+    prog.d_gitems = at<DevSItem>(b, o_gi);
+    prog.d_err = at<int>(b, o_err);
     prog.n_t1 = uint32_t(prog.stage1.tiles.size());
     prog.n_t3 = uint32_t(prog.stage3.tiles.size());
     prog.n_lines = uint32_t(prog.lines.size());
@@ -1005,40 +1053,24 @@ cudaError_t upload_program(DeviceProgram& prog) {
 }
 
 void free_program(DeviceProgram& prog) {
-    cudaFree(prog.d_p1);
-    cudaFree(prog.d_s1);
-    cudaFree(prog.d_t1);
-    cudaFree(prog.d_p3);
-    cudaFree(prog.d_s3);
-    cudaFree(prog.d_t3);
-    cudaFree(prog.d_r1);
-    prog.d_r1 = nullptr;
-    for (int c = 1; c < N_TILE_CLASSES; ++c) {
-        cudaFree(prog.x1.t[c]);
-        cudaFree(prog.x3.t[c]);
-    }
-    prog.x1 = TileLists();
-    prog.x3 = TileLists();
-    cudaFree(prog.d_lines);
-    cudaFree(prog.d_terms);
+    cudaFree(prog.d_arena);
+    prog.d_arena = nullptr;
     prog.d_p1 = nullptr;
     prog.d_s1 = nullptr;
     prog.d_t1 = nullptr;
     prog.d_p3 = nullptr;
     prog.d_s3 = nullptr;
     prog.d_t3 = nullptr;
+    prog.d_r1 = nullptr;
+    prog.x1 = TileLists();
+    prog.x3 = TileLists();
     prog.d_lines = nullptr;
     prog.d_terms = nullptr;
-    cudaFree(prog.d_groups);
-    cudaFree(prog.d_gent_t);
-    cudaFree(prog.d_gent_a);
-    cudaFree(prog.d_gitems);
-    cudaFree(prog.d_err);
-    prog.d_err = nullptr;
     prog.d_groups = nullptr;
     prog.d_gent_t = nullptr;
     prog.d_gent_a = nullptr;
     prog.d_gitems = nullptr;
+    prog.d_err = nullptr;
 }
 
 double calibrate_fp64_tflops() {

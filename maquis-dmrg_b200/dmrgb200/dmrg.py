@@ -234,6 +234,7 @@ class SweepLog:
     sweep_seconds: list = field(default_factory=list)
     hpsi_calls: int = 0
     solve_ms: float = 0.0   # device time of the eigen-solves
+    phase_seconds: dict = field(default_factory=dict)  # host wall time per phase of the site steps
 
 
 class DeviceBackend:
@@ -243,28 +244,61 @@ class DeviceBackend:
     def __init__(self, ctx: E.Context):
         import torch
         self.torch, self.ctx = torch, ctx
+        # host seconds per phase of the site problems (schedule building, plan lowering, solve)
+        self.phase_seconds = {"schedule": 0.0, "plan": 0.0, "solve": 0.0}
 
     def edge(self, symm, index):
         idx = E.edge_bindex(symm, index)
         return idx, E.to_device(idx.edge_values(), self.ctx.device)
 
-    def left_step(self, model, W, Lidx, Lbuf, t: S.SiteTensor):
+    def _step(self, left, model, W, idx, buf, t: S.SiteTensor):
         dev = self.ctx.device
-        return E.device_left_step(self.ctx, model.phys, t.left, t.right, W, Lidx, Lbuf, E.to_device(t.data, dev),
-                                  E.to_device(t.left_paired(), dev), True)
+        t0 = time.perf_counter()
+        if left:
+            sched, nidx = E.schedule_left_step(model.phys, t.left, t.right, W, idx, True)
+            plan = E.DevicePlan(self.ctx, sched.plan, left_addr=idx.cohort_addresses(buf.data_ptr()))
+            ket, bra = E.to_device(t.data, dev), E.to_device(t.left_paired(), dev)
+        else:
+            sched, nidx = E.schedule_right_step(model.phys, t.left, t.right, W, idx, True)
+            plan = E.DevicePlan(self.ctx, sched.plan, other_addr=idx.cohort_addresses(buf.data_ptr()))
+            ket = bra = E.to_device(t.data, dev)
+        out = self.torch.zeros(max(nidx.n_elems, 1), dtype=self.torch.float64, device=buf.device)
+        t1 = time.perf_counter()
+        plan.step(ket.data_ptr(), bra.data_ptr(), nidx.cohort_addresses(out.data_ptr()))
+        t2 = time.perf_counter()
+        del plan
+        t3 = time.perf_counter()
+        ph = self.phase_seconds
+        ph["step_schedule"] = ph.get("step_schedule", 0.0) + t1 - t0
+        ph["step_execute"] = ph.get("step_execute", 0.0) + t2 - t1
+        ph["step_destroy"] = ph.get("step_destroy", 0.0) + t3 - t2
+        return nidx, out
+
+    def left_step(self, model, W, Lidx, Lbuf, t: S.SiteTensor):
+        return self._step(True, model, W, Lidx, Lbuf, t)
 
     def right_step(self, model, W, Ridx, Rbuf, t: S.SiteTensor):
-        td = E.to_device(t.data, self.ctx.device)
-        return E.device_right_step(self.ctx, model.phys, t.left, t.right, W, Ridx, Rbuf, td, td, True)
+        return self._step(False, model, W, Ridx, Rbuf, t)
 
     def solve(self, p12, psi: S.SiteTensor, W12, Lidx, Lbuf, Ridx, Rbuf, tol, max_iter):
+        t0 = time.perf_counter()
         sched = E.schedule_hpsi(p12, psi.left, psi.right, W12, Lidx, Ridx)
+        t1 = time.perf_counter()
         plan = E.DevicePlan(self.ctx, sched.plan, left_addr=Lidx.cohort_addresses(Lbuf.data_ptr()),
                             other_addr=Ridx.cohort_addresses(Rbuf.data_ptr()))
+        t2 = time.perf_counter()
         xd = E.to_device(psi.data, self.ctx.device)
         xo = self.torch.zeros_like(xd)
         energy, st = plan.solve(xd.data_ptr(), xo.data_ptr(), xd.numel(), tol=tol, max_iter=max_iter)
-        return energy, xo.cpu().numpy(), st.iterations, st.solve_ms
+        out = xo.cpu().numpy()
+        t3 = time.perf_counter()
+        del plan
+        t4 = time.perf_counter()
+        self.phase_seconds["schedule"] += t1 - t0
+        self.phase_seconds["plan"] += t2 - t1
+        self.phase_seconds["solve"] += t3 - t2
+        self.phase_seconds["plan_destroy"] = self.phase_seconds.get("plan_destroy", 0.0) + t4 - t3
+        return energy, out, st.iterations, st.solve_ms
 
     def sync(self):
         self.torch.cuda.synchronize(self.ctx.device)
@@ -300,18 +334,28 @@ class TwoSiteDMRG:
                                                         self.A[j])
 
     def optimize_pair(self, i, left_to_right):
+        ph = self.log.phase_seconds
+        t0 = time.perf_counter()
         psi = twosite(self.A[i], self.A[i + 1], self.p12, self.offs)
+        t1 = time.perf_counter()
         energy, xo, iters, ms = self.be.solve(self.p12, psi, self.W12[i], self.Lidx[i], self.Lbuf[i],
                                               self.Ridx[i + 2], self.Rbuf[i + 2], self.jd_tol, self.jd_maxiter)
+        t2 = time.perf_counter()
         self.log.hpsi_calls += iters
         self.log.solve_ms += ms
         psi.data = xo
         res = split(psi, self.model.phys, self.model.phys, self.offs, self.m, self.cutoff, left_to_right)
         self.A[i], self.A[i + 1] = res.A, res.B
+        t3 = time.perf_counter()
         if left_to_right:
             self._left_step(i)
         else:
             self._right_step(i + 1)
+        t4 = time.perf_counter()
+        ph["twosite"] = ph.get("twosite", 0.0) + t1 - t0
+        ph["site_problem"] = ph.get("site_problem", 0.0) + t2 - t1
+        ph["split"] = ph.get("split", 0.0) + t3 - t2
+        ph["boundary_step"] = ph.get("boundary_step", 0.0) + t4 - t3
         return energy, iters, res.truncated_weight
 
     def sweep(self, sweep_index: int):

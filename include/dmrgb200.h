@@ -217,6 +217,17 @@ const char* dmrgb200_gemm_variant_name(int variant);
 /* Number of grouped-GEMM variants (valid variant indices are 0 .. count - 1). */
 int dmrgb200_gemm_variant_count(void);
 
+/* H·psi with host buffers, the counterpart of the reference's super_hamil_mv on
+ * host DavidsonVectors (solver/super_hamil_mv.hpp:100-155): x_host (the plan's in
+ * layout, in_size doubles) is copied to the device, y_host (out layout, out_size
+ * doubles) receives H·psi.  Stage 1 runs in four parts by input range and stage 3
+ * in four parts by output range, so the copies of one range overlap the products
+ * of another; the result is bitwise that of dmrgb200_hpsi.  Pin the host buffers
+ * (cudaHostAlloc / cudaHostRegister) for the copies to overlap.  Stream-ordered on
+ * cuda_stream: synchronise it before reading y_host.  The first call builds the
+ * split program and device copies of x and y (kept by the plan). */
+dmrgb200_status dmrgb200_hpsi_host(dmrgb200_plan_t plan, const double* x_host, double* y_host, void* cuda_stream);
+
 /* Adjoint of H·psi (no counterpart in the reference, which has no derivative
  * code).  With the plan's terms y = sum_k alpha_k H_k x, one call gives
  *   gx          = H^T w                      (the plan's in layout; may be NULL)

@@ -74,6 +74,15 @@ struct dmrgb200_plan_s {
     // Jacobi-Davidson: solver mode and the cached solver graph
     int solver_mode = DMRGB200_SOLVER_GRAPH;
     void* jd = nullptr;
+    // H psi with host buffers (built on first use): split program, device copies of x
+    // and y, a copy stream and its events
+    static constexpr uint32_t PIPE_PARTS = 4;
+    bool pipe_built = false;
+    PipelineProgram pipe;
+    double* hx = nullptr;
+    double* hy = nullptr;
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t pev[2 * PIPE_PARTS + 2] = {};
     // adjoint program (built on first use)
     bool adj_built = false;
     std::string adj_err;
@@ -483,6 +492,14 @@ dmrgb200_status dmrgb200_plan_destroy(dmrgb200_plan_t plan) {
     if (!plan) return DMRGB200_OK;
     if (plan->compiled) free_program(plan->prog);
     if (plan->adj_built) free_adjoint(plan->adj);
+    if (plan->pipe_built) {
+        free_pipeline(plan->pipe);
+        cudaFree(plan->hx);
+        cudaFree(plan->hy);
+        for (auto& e : plan->pev)
+            if (e) cudaEventDestroy(e);
+        if (plan->copy_stream) cudaStreamDestroy(plan->copy_stream);
+    }
     jd_graph_free(plan->jd);
     oz_free(plan->oz1);
     oz_free(plan->oz3);
@@ -523,6 +540,38 @@ dmrgb200_status dmrgb200_hpsi(dmrgb200_plan_t plan, const double* x, double* y, 
     if (e != cudaSuccess) return cuda_fail(e, "hpsi launch");
     if (plan->timing) plan->pending = true;
     return DMRGB200_OK;
+}
+
+dmrgb200_status dmrgb200_hpsi_host(dmrgb200_plan_t plan, const double* x_host, double* y_host, void* cuda_stream) {
+    DMRGB200_TRY
+    if (!plan || !x_host || !y_host) return fail(DMRGB200_INVALID_ARGUMENT, "null argument");
+    if (plan->flat.kind != KIND_HPSI || !plan->compiled) return fail(DMRGB200_INVALID_PLAN, "plan is not an H psi plan");
+    cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+    cudaError_t e;
+    if (!plan->pipe_built) {
+        plan->pipe_built = true;  // released by dmrgb200_plan_destroy, also after a failure here
+        if ((e = compile_pipeline(plan->flat, plan->stage3_bnd, plan->stage1_bnd, plan->PIPE_PARTS, plan->pipe)) !=
+            cudaSuccess)
+            return cuda_fail(e, "host-buffer program");
+        const size_t nx = std::max<uint64_t>(plan->flat.in_size, 1), ny = std::max<uint64_t>(plan->flat.out_size, 1);
+        if ((e = cudaMalloc(&plan->hx, nx * sizeof(double))) != cudaSuccess ||
+            (e = cudaMalloc(&plan->hy, ny * sizeof(double))) != cudaSuccess ||
+            // H psi writes only block elements: the padding copied back stays zero
+            (e = cudaMemset(plan->hy, 0, ny * sizeof(double))) != cudaSuccess ||
+            (e = cudaStreamCreateWithFlags(&plan->copy_stream, cudaStreamNonBlocking)) != cudaSuccess)
+            return cuda_fail(e, "host-buffer scratch");
+        for (auto& ev : plan->pev)
+            if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess)
+                return cuda_fail(e, "host-buffer events");
+    }
+    if (!plan->hx || !plan->copy_stream) return fail(DMRGB200_DEVICE_ERROR, "host-buffer program unavailable");
+    if ((e = plan_ensure_tuned(plan, plan->hx, plan->hy, st)) != cudaSuccess)
+        return cuda_fail(e, "grouped GEMM autotuning");
+    e = run_pipeline(plan->prog, plan->pipe, x_host, y_host, plan->hx, plan->hy, plan->T, plan->S, st,
+                     plan->copy_stream, plan->pev);
+    if (e != cudaSuccess) return cuda_fail(e, "host-buffer H psi");
+    return DMRGB200_OK;
+    DMRGB200_CATCH
 }
 
 dmrgb200_status dmrgb200_hpsi_adjoint(dmrgb200_plan_t plan, const double* w, const double* x, double* gx,

@@ -215,6 +215,24 @@ void free_gemm(GemmDev& d);
 // one persistent grouped-GEMM launch over the tile list
 cudaError_t launch_gemm(GemmDev const& d, Bases const& bs, cudaStream_t stream);
 
+// H psi with host buffers: stage 1 split by ranges of the input (the T tasks whose
+// psi block lies in a range, stacked per range) and stage 3 by ranges of the output,
+// so the host-device copies of one range overlap the products of another.  Every T
+// element and output element is computed by the same tile walk as in the whole-plan
+// program, so the results are bitwise the same.
+struct PipelineProgram {
+    uint32_t nparts = 0;
+    std::vector<uint64_t> in_cut, out_cut;  // nparts + 1 element offsets each
+    std::vector<GemmDev> s1, s3;            // device tile lists per range
+};
+cudaError_t compile_pipeline(FlatPlan const& p, std::vector<uint64_t> const& stage3_bnd,
+                             std::vector<uint64_t> const& stage1_bnd, uint32_t nparts, PipelineProgram& pp);
+void free_pipeline(PipelineProgram& pp);
+// ev: 2 * nparts + 2 events; c: a second stream for the copies
+cudaError_t run_pipeline(DeviceProgram const& prog, PipelineProgram const& pp, const double* x_host, double* y_host,
+                         double* xd, double* yd, double* T, double* S, cudaStream_t s, cudaStream_t c,
+                         cudaEvent_t const* ev);
+
 // ---- adjoint of H psi (adjoint.cu) ----
 // galpha term: <G cell, T cell> for plan term k
 struct DevATerm {

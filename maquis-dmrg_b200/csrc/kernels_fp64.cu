@@ -465,7 +465,7 @@ __global__ void __launch_bounds__(32 * SGB_WARPS, SGB_MINB) sbuild_groups(const 
                 break;
             }
             const uint32_t nc = min(uint32_t(SGB_NC), k1 - kb);
-#pragma unroll 1
+#pragma unroll 2
             for (uint32_t c = 0; c < nc; ++c) {
                 const double* row = R.rows[slot][c] + R.shift[slot][c] + lane;
                 double v[SG_EPT];
@@ -607,11 +607,11 @@ namespace {
 // of T_t (leading dimension = the task's row count), so one tile covers several
 // small psi blocks instead of padding each to a full tile.
 void stack_stage1(FlatPlan const& p, std::vector<uint64_t> const& stage1_bnd, std::vector<uint64_t> const& t_off,
-                  GemmList& g1) {
+                  GemmList& g1, std::vector<char> const* keep = nullptr) {
     g1 = GemmList();
     std::map<std::tuple<uint32_t, uint8_t, uint32_t, uint32_t, uint32_t>, std::vector<uint32_t>> groups;
     for (uint32_t t = 0; t < p.n_t(); ++t)
-        groups[{p.t_ci[t], p.t_trans[t], p.t_brows[t], p.t_bcols[t], p.t_nb[t]}].push_back(t);
+        if (!keep || (*keep)[t]) groups[{p.t_ci[t], p.t_trans[t], p.t_brows[t], p.t_bcols[t], p.t_nb[t]}].push_back(t);
     for (auto const& kv : groups) {
         const uint32_t t0 = kv.second.front();
         const uint32_t K = p.t_brows[t0], Nf = p.t_bcols[t0], nb = p.t_nb[t0];
@@ -747,6 +747,48 @@ int sbuild_mode() {
     if (!std::strcmp(v, "lines")) return 1;
     if (!std::strcmp(v, "groups")) return 2;
     return 0;
+}
+}  // namespace
+
+namespace {
+// Stage 3 of H psi: one problem per output block (every cohort writing the block is
+// a K segment of it); keep (optional) selects output blocks.
+void build_stage3_hpsi(FlatPlan const& p, std::vector<uint64_t> const& stage3_bnd, std::vector<uint64_t> const& s_off,
+                       GemmList& g3, std::vector<char> const* keep) {
+    const uint32_t nc = p.n_cohorts();
+    std::vector<std::vector<uint32_t>> by_out(p.out_rows.size());
+    for (uint32_t c = 0; c < nc; ++c) by_out[p.c_rb[c]].push_back(c);
+    for (uint32_t ob = 0; ob < p.out_rows.size(); ++ob) {
+        if (keep && !(*keep)[ob]) continue;
+        DevProb pr;
+        pr.M = p.out_rows[ob];
+        pr.N = p.out_cols[ob];
+        pr.C = op(BUF_OUT, p.out_off[ob], pr.M, false, 0);
+        pr.seg_begin = uint32_t(g3.segs.size());
+        for (uint32_t c : by_out[ob]) {
+            uint32_t ls = p.c_ls[c], rs = p.c_rs[c], ns = p.c_nsrows[c];
+            uint64_t lbase = stage3_bnd.at(p.c_ci[c]) / 8;
+            if (!p.c_trans[c]) {
+                DevSeg sg{};
+                sg.A = op(BUF_ABS, lbase, rs, false);
+                sg.B = op(BUF_S, s_off[c], ns * ls, false);
+                sg.K = ns * ls;
+                g3.segs.push_back(sg);
+            } else {
+                // each stored block (ls x rs) is read transposed: one segment per MPO row block
+                for (uint32_t b = 0; b < ns; ++b) {
+                    DevSeg sg{};
+                    sg.A = op(BUF_ABS, lbase + uint64_t(b) * ls * rs, ls, true);
+                    sg.B = op(BUF_S, s_off[c] + uint64_t(b) * ls, ns * ls, false);
+                    sg.K = ls;
+                    g3.segs.push_back(sg);
+                }
+            }
+        }
+        pr.seg_end = uint32_t(g3.segs.size());
+        g3.probs.push_back(pr);
+        add_tiles(g3, uint32_t(g3.probs.size() - 1), 1);
+    }
 }
 }  // namespace
 
@@ -896,38 +938,7 @@ void compile_program(FlatPlan const& p, std::vector<uint64_t> const& stage3_bnd,
     // ---- stage 3 ----
     GemmList& g3 = prog.stage3;
     if (p.kind == KIND_HPSI) {
-        std::vector<std::vector<uint32_t>> by_out(p.out_rows.size());
-        for (uint32_t c = 0; c < nc; ++c) by_out[p.c_rb[c]].push_back(c);
-        for (uint32_t ob = 0; ob < p.out_rows.size(); ++ob) {
-            DevProb pr;
-            pr.M = p.out_rows[ob];
-            pr.N = p.out_cols[ob];
-            pr.C = op(BUF_OUT, p.out_off[ob], pr.M, false, 0);
-            pr.seg_begin = uint32_t(g3.segs.size());
-            for (uint32_t c : by_out[ob]) {
-                uint32_t ls = p.c_ls[c], rs = p.c_rs[c], ns = p.c_nsrows[c];
-                uint64_t lbase = stage3_bnd.at(p.c_ci[c]) / 8;
-                if (!p.c_trans[c]) {
-                    DevSeg sg{};
-                    sg.A = op(BUF_ABS, lbase, rs, false);
-                    sg.B = op(BUF_S, s_off[c], ns * ls, false);
-                    sg.K = ns * ls;
-                    g3.segs.push_back(sg);
-                } else {
-                    // each stored block (ls x rs) is read transposed: one segment per MPO row block
-                    for (uint32_t b = 0; b < ns; ++b) {
-                        DevSeg sg{};
-                        sg.A = op(BUF_ABS, lbase + uint64_t(b) * ls * rs, ls, true);
-                        sg.B = op(BUF_S, s_off[c] + uint64_t(b) * ls, ns * ls, false);
-                        sg.K = ls;
-                        g3.segs.push_back(sg);
-                    }
-                }
-            }
-            pr.seg_end = uint32_t(g3.segs.size());
-            g3.probs.push_back(pr);
-            add_tiles(g3, uint32_t(g3.probs.size() - 1), 1);
-        }
+        build_stage3_hpsi(p, stage3_bnd, s_off, g3, nullptr);
     } else if (p.kind == KIND_RIGHT) {
         for (uint32_t c = 0; c < nc; ++c) {
             uint32_t ls = p.c_ls[c], rs = p.c_rs[c], ns = p.c_nsrows[c];
@@ -1071,6 +1082,100 @@ void free_program(DeviceProgram& prog) {
     prog.d_gent_a = nullptr;
     prog.d_gitems = nullptr;
     prog.d_err = nullptr;
+}
+
+namespace {
+// cut points at block boundaries near equal shares of [0, total)
+std::vector<uint64_t> cut_ranges(std::vector<uint64_t> const& block_off, uint64_t total, uint32_t nparts) {
+    std::vector<uint64_t> starts(block_off);
+    std::sort(starts.begin(), starts.end());
+    std::vector<uint64_t> cut{0};
+    for (uint32_t q = 1; q < nparts; ++q) {
+        const uint64_t want = total * q / nparts;
+        auto it = std::lower_bound(starts.begin(), starts.end(), want);
+        uint64_t c = it == starts.end() ? total : *it;
+        cut.push_back(std::max(c, cut.back()));
+    }
+    cut.push_back(total);
+    return cut;
+}
+}  // namespace
+
+cudaError_t compile_pipeline(FlatPlan const& p, std::vector<uint64_t> const& stage3_bnd,
+                             std::vector<uint64_t> const& stage1_bnd, uint32_t nparts, PipelineProgram& pp) {
+    pp = PipelineProgram();
+    pp.nparts = nparts;
+    std::vector<uint64_t> in_off(p.in_off.begin(), p.in_off.end()), out_off(p.out_off.begin(), p.out_off.end());
+    pp.in_cut = cut_ranges(in_off, p.in_size, nparts);
+    pp.out_cut = cut_ranges(out_off, p.out_size, nparts);
+    const std::vector<uint64_t> t_off = t_offsets(p, nullptr), s_off = s_offsets(p, nullptr);
+    pp.s1.resize(nparts);
+    pp.s3.resize(nparts);
+    for (uint32_t q = 0; q < nparts; ++q) {
+        std::vector<char> keep_t(p.n_t()), keep_o(p.out_rows.size());
+        for (uint32_t t = 0; t < p.n_t(); ++t) {
+            const uint64_t o = p.in_off[p.t_lb[t]];
+            keep_t[t] = o >= pp.in_cut[q] && o < pp.in_cut[q + 1];
+        }
+        for (uint32_t ob = 0; ob < p.out_rows.size(); ++ob)
+            keep_o[ob] = p.out_off[ob] >= pp.out_cut[q] && p.out_off[ob] < pp.out_cut[q + 1];
+        GemmList g1, g3;
+        stack_stage1(p, stage1_bnd, t_off, g1, &keep_t);
+        build_stage3_hpsi(p, stage3_bnd, s_off, g3, &keep_o);
+        sort_tiles(g3);
+        cudaError_t e;
+        if ((e = upload_gemm(g1, pp.s1[q])) != cudaSuccess) return e;
+        if ((e = upload_gemm(g3, pp.s3[q])) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+void free_pipeline(PipelineProgram& pp) {
+    for (auto& g : pp.s1) free_gemm(g);
+    for (auto& g : pp.s3) free_gemm(g);
+    pp = PipelineProgram();
+}
+
+cudaError_t run_pipeline(DeviceProgram const& prog, PipelineProgram const& pp, const double* x_host, double* y_host,
+                         double* xd, double* yd, double* T, double* S, cudaStream_t s, cudaStream_t c,
+                         cudaEvent_t const* ev) {
+    const uint32_t np = pp.nparts;
+    Bases bs{};
+    bs.b[BUF_IN] = reinterpret_cast<uint64_t>(xd);
+    bs.b[BUF_OUT] = reinterpret_cast<uint64_t>(yd);
+    bs.b[BUF_T] = reinterpret_cast<uint64_t>(T);
+    bs.b[BUF_S] = reinterpret_cast<uint64_t>(S);
+    cudaError_t e;
+    // the copies start after the work already queued on the caller's stream
+    if ((e = cudaEventRecord(ev[0], s)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(c, ev[0], 0)) != cudaSuccess) return e;
+    for (uint32_t q = 0; q < np; ++q) {
+        const uint64_t n = pp.in_cut[q + 1] - pp.in_cut[q];
+        if (n && (e = cudaMemcpyAsync(xd + pp.in_cut[q], x_host + pp.in_cut[q], n * sizeof(double),
+                                      cudaMemcpyHostToDevice, c)) != cudaSuccess)
+            return e;
+        if ((e = cudaEventRecord(ev[1 + q], c)) != cudaSuccess) return e;
+    }
+    for (uint32_t q = 0; q < np; ++q) {
+        if ((e = cudaStreamWaitEvent(s, ev[1 + q], 0)) != cudaSuccess) return e;
+        GemmDev g = pp.s1[q];
+        g.var = prog.var1;
+        if ((e = launch_gemm(g, bs, s)) != cudaSuccess) return e;
+    }
+    if ((e = run_sbuild(prog, T, S, s)) != cudaSuccess) return e;
+    for (uint32_t q = 0; q < np; ++q) {
+        GemmDev g = pp.s3[q];
+        g.var = prog.var3;
+        if ((e = launch_gemm(g, bs, s)) != cudaSuccess) return e;
+        if ((e = cudaEventRecord(ev[1 + np + q], s)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(c, ev[1 + np + q], 0)) != cudaSuccess) return e;
+        const uint64_t n = pp.out_cut[q + 1] - pp.out_cut[q];
+        if (n && (e = cudaMemcpyAsync(y_host + pp.out_cut[q], yd + pp.out_cut[q], n * sizeof(double),
+                                      cudaMemcpyDeviceToHost, c)) != cudaSuccess)
+            return e;
+    }
+    if ((e = cudaEventRecord(ev[1 + 2 * np], c)) != cudaSuccess) return e;
+    return cudaStreamWaitEvent(s, ev[1 + 2 * np], 0);
 }
 
 double calibrate_fp64_tflops() {

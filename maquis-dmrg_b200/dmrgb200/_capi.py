@@ -110,6 +110,7 @@ _sigs = {
     "dmrgb200_plan_flops": ([vp, u64p], C.c_int),
     "dmrgb200_plan_scratch_bytes": ([vp, u64p], C.c_int),
     "dmrgb200_hpsi": ([vp, vp, vp, C.c_int, vp], C.c_int),
+    "dmrgb200_hpsi_host": ([vp, vp, vp, vp], C.c_int),
     "dmrgb200_hpsi_adjoint": ([vp, vp, vp, vp, vp, vp], C.c_int),
     "dmrgb200_plan_set_timing": ([vp, C.c_int], C.c_int),
     "dmrgb200_plan_set_slices": ([vp, C.c_int], C.c_int),

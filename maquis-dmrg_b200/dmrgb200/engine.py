@@ -201,6 +201,12 @@ class DevicePlan:
     def hpsi(self, x_ptr: int, y_ptr: int, prec: int = capi.PREC_FP64, stream: int = 0) -> None:
         capi.check(capi.lib.dmrgb200_hpsi(self.handle, x_ptr, y_ptr, prec, stream or None), "dmrgb200_hpsi")
 
+    def hpsi_host(self, x_host_ptr: int, y_host_ptr: int, stream: int = 0) -> None:
+        """H·psi from and into host buffers (dmrgb200_hpsi_host: copies overlapped with the
+        products; pinned buffers for the overlap; synchronise the stream before reading)."""
+        capi.check(capi.lib.dmrgb200_hpsi_host(self.handle, x_host_ptr, y_host_ptr, stream or None),
+                   "dmrgb200_hpsi_host")
+
     def adjoint(self, w_ptr: int, x_ptr: int, gx_ptr: int, galpha_ptr: int, stream: int = 0) -> None:
         """gx = H^T w and galpha[k] = <w|H_k x> (dmrgb200_hpsi_adjoint; 0 skips an output)."""
         capi.check(capi.lib.dmrgb200_hpsi_adjoint(self.handle, w_ptr, x_ptr or None, gx_ptr or None,

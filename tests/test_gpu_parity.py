@@ -148,3 +148,21 @@ def test_autotuned_variants_give_identical_results(ctx):
     plan.hpsi(xd.data_ptr(), yd.data_ptr())
     torch.cuda.synchronize()
     assert np.array_equal(y0, yd.cpu().numpy())
+
+
+@pytest.mark.parametrize("name,L,m", [("hubbard", 16, 96), ("qc", 8, 64)])
+def test_hpsi_host_buffers_bitwise_equal(ctx, name, L, m):
+    """dmrgb200_hpsi_host (pinned host x and y, copies overlapped with the split
+    stages) gives bitwise the device H·psi, repeatedly."""
+    model, bonds, tensors, rng = make_chain(name, L, 0, seed=8, synthetic_m=m)
+    ch = OracleChain(model, bonds, tensors, L // 2 - 1)
+    x = random_psi(ch.p12, ch.left, ch.right, rng).data
+    y_dev, keep = _gpu_hpsi(ctx, ch, x)
+    plan = keep[0]
+    xh = torch.from_numpy(x.copy()).pin_memory()
+    for _ in range(2):
+        yh = torch.full((len(x),), float("nan"), dtype=torch.float64).pin_memory()
+        plan.hpsi_host(xh.data_ptr(), yh.data_ptr())
+        torch.cuda.synchronize()
+        assert np.array_equal(yh.numpy(), y_dev)
+    assert _rel(y_dev, ch.hpsi(x)) <= TOL

@@ -225,7 +225,9 @@ int dmrgb200_gemm_variant_count(void);
  * of another; the result is bitwise that of dmrgb200_hpsi.  Pin the host buffers
  * (cudaHostAlloc / cudaHostRegister) for the copies to overlap.  Stream-ordered on
  * cuda_stream: synchronise it before reading y_host.  The first call builds the
- * split program and device copies of x and y (kept by the plan). */
+ * split program and device copies of x and y (kept by the plan); the sequence is
+ * captured as one CUDA graph per (x_host, y_host) pair, so reusing the same host
+ * buffers costs one graph launch per call. */
 dmrgb200_status dmrgb200_hpsi_host(dmrgb200_plan_t plan, const double* x_host, double* y_host, void* cuda_stream);
 
 /* Adjoint of H·psi (no counterpart in the reference, which has no derivative

@@ -81,8 +81,13 @@ struct dmrgb200_plan_s {
     PipelineProgram pipe;
     double* hx = nullptr;
     double* hy = nullptr;
-    cudaStream_t copy_stream = nullptr;
+    cudaStream_t copy_stream = nullptr, capture_stream = nullptr;
     cudaEvent_t pev[2 * PIPE_PARTS + 2] = {};
+    // the whole host-buffer sequence as one CUDA graph, captured for one (x_host, y_host)
+    // pair: 26 API calls per H psi cost more host time than the device takes
+    cudaGraphExec_t pipe_exec = nullptr;
+    const double* pipe_x = nullptr;
+    double* pipe_y = nullptr;
     // adjoint program (built on first use)
     bool adj_built = false;
     std::string adj_err;
@@ -496,9 +501,11 @@ dmrgb200_status dmrgb200_plan_destroy(dmrgb200_plan_t plan) {
         free_pipeline(plan->pipe);
         cudaFree(plan->hx);
         cudaFree(plan->hy);
+        if (plan->pipe_exec) cudaGraphExecDestroy(plan->pipe_exec);
         for (auto& e : plan->pev)
             if (e) cudaEventDestroy(e);
         if (plan->copy_stream) cudaStreamDestroy(plan->copy_stream);
+        if (plan->capture_stream) cudaStreamDestroy(plan->capture_stream);
     }
     jd_graph_free(plan->jd);
     oz_free(plan->oz1);
@@ -558,7 +565,8 @@ dmrgb200_status dmrgb200_hpsi_host(dmrgb200_plan_t plan, const double* x_host, d
             (e = cudaMalloc(&plan->hy, ny * sizeof(double))) != cudaSuccess ||
             // H psi writes only block elements: the padding copied back stays zero
             (e = cudaMemset(plan->hy, 0, ny * sizeof(double))) != cudaSuccess ||
-            (e = cudaStreamCreateWithFlags(&plan->copy_stream, cudaStreamNonBlocking)) != cudaSuccess)
+            (e = cudaStreamCreateWithFlags(&plan->copy_stream, cudaStreamNonBlocking)) != cudaSuccess ||
+            (e = cudaStreamCreateWithFlags(&plan->capture_stream, cudaStreamNonBlocking)) != cudaSuccess)
             return cuda_fail(e, "host-buffer scratch");
         for (auto& ev : plan->pev)
             if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess)
@@ -567,9 +575,35 @@ dmrgb200_status dmrgb200_hpsi_host(dmrgb200_plan_t plan, const double* x_host, d
     if (!plan->hx || !plan->copy_stream) return fail(DMRGB200_DEVICE_ERROR, "host-buffer program unavailable");
     if ((e = plan_ensure_tuned(plan, plan->hx, plan->hy, st)) != cudaSuccess)
         return cuda_fail(e, "grouped GEMM autotuning");
-    e = run_pipeline(plan->prog, plan->pipe, x_host, y_host, plan->hx, plan->hy, plan->T, plan->S, st,
-                     plan->copy_stream, plan->pev);
-    if (e != cudaSuccess) return cuda_fail(e, "host-buffer H psi");
+    if (!plan->pipe_exec || plan->pipe_x != x_host || plan->pipe_y != y_host) {
+        // (re)capture for these host buffers on the plan's own stream
+        if (plan->pipe_exec) cudaGraphExecDestroy(plan->pipe_exec);
+        plan->pipe_exec = nullptr;
+        cudaGraph_t g = nullptr;
+        cudaStream_t cs = plan->capture_stream;
+        if ((e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+            return cuda_fail(e, "host-buffer capture");
+        cudaError_t er = run_pipeline(plan->prog, plan->pipe, x_host, y_host, plan->hx, plan->hy, plan->T, plan->S, cs,
+                                      plan->copy_stream, plan->pev);
+        e = cudaStreamEndCapture(cs, &g);
+        if (er != cudaSuccess || e != cudaSuccess) {
+            // not capturable (pageable host buffers, for one): run the sequence directly
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            e = run_pipeline(plan->prog, plan->pipe, x_host, y_host, plan->hx, plan->hy, plan->T, plan->S, st,
+                             plan->copy_stream, plan->pev);
+            return e == cudaSuccess ? DMRGB200_OK : cuda_fail(e, "host-buffer H psi");
+        }
+        e = cudaGraphInstantiate(&plan->pipe_exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            plan->pipe_exec = nullptr;
+            return cuda_fail(e, "host-buffer graph");
+        }
+        plan->pipe_x = x_host;
+        plan->pipe_y = y_host;
+    }
+    if ((e = cudaGraphLaunch(plan->pipe_exec, st)) != cudaSuccess) return cuda_fail(e, "host-buffer H psi");
     return DMRGB200_OK;
     DMRGB200_CATCH
 }

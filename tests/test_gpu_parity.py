@@ -166,3 +166,16 @@ def test_hpsi_host_buffers_bitwise_equal(ctx, name, L, m):
         torch.cuda.synchronize()
         assert np.array_equal(yh.numpy(), y_dev)
     assert _rel(y_dev, ch.hpsi(x)) <= TOL
+
+
+def test_hpsi_host_pageable_buffers(ctx):
+    """dmrgb200_hpsi_host also takes pageable host memory (no overlap then)."""
+    model, bonds, tensors, rng = make_chain("hubbard", 12, 0, seed=9, synthetic_m=64)
+    ch = OracleChain(model, bonds, tensors, 5)
+    x = random_psi(ch.p12, ch.left, ch.right, rng).data
+    y_dev, keep = _gpu_hpsi(ctx, ch, x)
+    xh = np.ascontiguousarray(x)
+    yh = np.full(len(x), np.nan)
+    keep[0].hpsi_host(xh.ctypes.data, yh.ctypes.data)
+    torch.cuda.synchronize()
+    assert np.array_equal(yh, y_dev)

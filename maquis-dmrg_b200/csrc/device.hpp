@@ -77,7 +77,7 @@ struct DevSGroup {
     uint32_t mask;  // bit j: line j has terms (the others are written as zeros)
     uint32_t nlines;
 };
-// one warp's work in the grouped S build: elements e0 .. e0 + 127 of a group
+// one warp's work in the S build: elements e0 .. e0 + 127 of a group (or of a line)
 struct DevSItem {
     uint32_t group, e0;
 };
@@ -135,7 +135,8 @@ struct DeviceProgram {
     std::vector<DevSGroup> groups;
     std::vector<uint64_t> gent_t;  // per group entry: source offset in T
     std::vector<double> gent_a;    // per group entry: SG_LINES alphas
-    std::vector<DevSItem> gitems;  // warp work items, longest groups first
+    std::vector<DevSItem> gitems;  // warp items of the groups
+    std::vector<DevSItem> litems;  // warp items of the lines (DevSItem.group = line index)
     uint64_t t_elems = 0, s_elems = 0;
 
     // device copies
@@ -151,9 +152,10 @@ struct DeviceProgram {
     uint64_t* d_gent_t = nullptr;
     double* d_gent_a = nullptr;
     DevSItem* d_gitems = nullptr;
+    DevSItem* d_litems = nullptr;
     int* d_err = nullptr;  // set by a grouped S build whose bulk-copy wait timed out
     unsigned char* d_arena = nullptr;  // the one allocation holding every table above
-    uint32_t n_t1 = 0, n_t3 = 0, n_lines = 0, n_gitems = 0;
+    uint32_t n_t1 = 0, n_t3 = 0, n_lines = 0, n_litems = 0, n_gitems = 0;
     TileLists x1, x3;  // tile lists of the other classes
     DevRow* d_r1 = nullptr;  // stage-1 row table (stacked T tasks)
     GemmList stage1_tasks;   // stage 1 as one problem per T task (when stage1 is stacked)

@@ -314,65 +314,54 @@ __global__ void __launch_bounds__(NTHREADS, MINB) gemm_f64_grouped(const DevProb
 // S build: S is tiled by cells (one per unit and MPO row block); a cell with a
 // line writes the alpha-weighted sum of its T sources (summed in term order like
 // the reference's axpy sequence), a cell without one writes zeros, so S needs
-// no separate clearing.  Every thread owns up to SB_EPT elements of a line (a
-// column-major walk in steps of blockDim.x, without per-element division) and
-// the line's terms pass through shared memory in chunks of SB_TERMS, so each
-// term costs SB_EPT independent loads per thread.
-constexpr int SB_TERMS = 256, SB_EPT = 4;
+// no separate clearing.  One warp per work item (a line and a chunk of SB_CHUNK
+// consecutive elements of its column-major walk): every lane owns SB_EPT elements
+// (lane + 32 u); the line's terms are read 32 at a time, one per lane, and handed
+// round by shuffles, so no block barrier is needed and the warps of a CTA, on
+// neighbouring chunks of one line, share its term list through L1.
+constexpr int SB_EPT = 4, SB_CHUNK = 32 * SB_EPT;
 __global__ void __launch_bounds__(256) sbuild_lines(const DevSLine* __restrict__ lines,
-                                                    const DevSTerm* __restrict__ terms, uint32_t n_lines,
+                                                    const DevSTerm* __restrict__ terms,
+                                                    const DevSItem* __restrict__ items, uint32_t n_items,
                                                     double* __restrict__ S, const double* __restrict__ T) {
-    __shared__ double s_alpha[SB_TERMS];
-    __shared__ uint64_t s_base[SB_TERMS];
     wait_for_predecessor();
-    for (uint32_t li = blockIdx.x; li < n_lines; li += gridDim.x) {
-        const DevSLine L = lines[li];
-        if (!L.rows || !L.cols) continue;
+    const uint32_t lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    for (uint32_t it = blockIdx.x * wpb + (threadIdx.x >> 5); it < n_items; it += gridDim.x * wpb) {
+        const DevSItem I = items[it];
+        const DevSLine L = lines[I.group];
         const uint32_t n = L.rows * L.cols;
-        const uint32_t di = blockDim.x % L.rows, dc = blockDim.x / L.rows;
-        // this thread's first element of the line
-        uint32_t i0 = threadIdx.x % L.rows, c0 = threadIdx.x / L.rows;
-        for (uint32_t base = 0; base < n; base += SB_EPT * blockDim.x) {
-            uint64_t toff[SB_EPT], soff[SB_EPT];
-            bool in[SB_EPT];
-            double v[SB_EPT];
-            uint32_t i = i0, c = c0;
+        uint64_t toff[SB_EPT], soff[SB_EPT];
+        bool in[SB_EPT];
+        double v[SB_EPT];
 #pragma unroll
-            for (int u = 0; u < SB_EPT; ++u) {
-                in[u] = c < L.cols;
-                toff[u] = i + uint64_t(c) * L.ld_t;
-                soff[u] = L.s_base + i + uint64_t(c) * L.ld_s;
-                v[u] = 0.0;
-                i += di;
-                c += dc;
-                if (i >= L.rows) {
-                    i -= L.rows;
-                    ++c;
-                }
-            }
-            i0 = i;
-            c0 = c;
-            for (uint32_t t0 = L.term_begin; t0 < L.term_end; t0 += SB_TERMS) {
-                const uint32_t nt = min(uint32_t(SB_TERMS), L.term_end - t0);
-                __syncthreads();  // readers of the previous chunk are done
-                if (threadIdx.x < nt) {
-                    const DevSTerm tm = terms[t0 + threadIdx.x];
-                    s_alpha[threadIdx.x] = tm.alpha;
-                    s_base[threadIdx.x] = tm.t_base;
-                }
-                __syncthreads();
-                for (uint32_t t = 0; t < nt; ++t) {
-                    const double a = s_alpha[t];
-                    const uint64_t b = s_base[t];
-#pragma unroll
-                    for (int u = 0; u < SB_EPT; ++u)
-                        if (in[u]) v[u] += a * T[b + toff[u]];
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < SB_EPT; ++u)
-                if (in[u]) S[soff[u]] = v[u];
+        for (int u = 0; u < SB_EPT; ++u) {
+            const uint32_t e = I.e0 + lane + 32u * u;
+            in[u] = e < n;
+            const uint32_t c = in[u] ? e / L.rows : 0, i = in[u] ? e - c * L.rows : 0;
+            toff[u] = i + uint64_t(c) * L.ld_t;
+            soff[u] = L.s_base + i + uint64_t(c) * L.ld_s;
+            v[u] = 0.0;
         }
+        for (uint32_t t0 = L.term_begin; t0 < L.term_end; t0 += 32) {
+            const uint32_t nt = min(32u, L.term_end - t0);
+            double my_a = 0.0;
+            uint64_t my_b = 0;
+            if (lane < nt) {
+                const DevSTerm tm = terms[t0 + lane];
+                my_a = tm.alpha;
+                my_b = tm.t_base;
+            }
+            for (uint32_t t = 0; t < nt; ++t) {
+                const double a = __shfl_sync(0xffffffffu, my_a, t);
+                const uint64_t b = __shfl_sync(0xffffffffu, my_b, t);
+#pragma unroll
+                for (int u = 0; u < SB_EPT; ++u)
+                    if (in[u]) v[u] += a * T[b + toff[u]];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < SB_EPT; ++u)
+            if (in[u]) S[soff[u]] = v[u];
     }
 }
 
@@ -909,6 +898,11 @@ void compile_program(FlatPlan const& p, std::vector<uint64_t> const& stage3_bnd,
             }
         }
     }
+    // warp items of the lines: every line in chunks of SB_CHUNK elements, in line order
+    for (uint32_t li = 0; li < prog.lines.size(); ++li) {
+        const uint64_t n = uint64_t(prog.lines[li].rows) * prog.lines[li].cols;
+        for (uint64_t e0 = 0; e0 < n; e0 += SB_CHUNK) prog.litems.push_back(DevSItem{li, uint32_t(e0)});
+    }
     // warp items of the line groups: units by decreasing work, then group by
     // group, each group's element chunks consecutive (the warps of a CTA share the
     // group's source list and read its T slices in long contiguous runs; the
@@ -1024,7 +1018,7 @@ cudaError_t upload_program(DeviceProgram& prog) {
         o_x1[c] = pk.add(prog.stage1.tiles_cls[c]);
         o_x3[c] = pk.add(prog.stage3.tiles_cls[c]);
     }
-    const size_t o_l = pk.add(prog.lines), o_k = pk.add(prog.terms);
+    const size_t o_l = pk.add(prog.lines), o_k = pk.add(prog.terms), o_li = pk.add(prog.litems);
     const size_t o_g = pk.add(prog.groups), o_gt = pk.add(prog.gent_t), o_ga = pk.add(prog.gent_a);
     const size_t o_gi = pk.add(prog.gitems);
     const size_t o_err = prog.gitems.empty() ? TablePacker::NONE : pk.zeros(sizeof(int));
@@ -1051,6 +1045,7 @@ cudaError_t upload_program(DeviceProgram& prog) {
     }
     prog.d_lines = at<DevSLine>(b, o_l);
     prog.d_terms = at<DevSTerm>(b, o_k);
+    prog.d_litems = at<DevSItem>(b, o_li);
     prog.d_groups = at<DevSGroup>(b, o_g);
     prog.d_gent_t = at<uint64_t>(b, o_gt);
     prog.d_gent_a = at<double>(b, o_ga);
@@ -1059,6 +1054,7 @@ cudaError_t upload_program(DeviceProgram& prog) {
     prog.n_t1 = uint32_t(prog.stage1.tiles.size());
     prog.n_t3 = uint32_t(prog.stage3.tiles.size());
     prog.n_lines = uint32_t(prog.lines.size());
+    prog.n_litems = uint32_t(prog.litems.size());
     prog.n_gitems = uint32_t(prog.gitems.size());
     return cudaSuccess;
 }
@@ -1077,6 +1073,7 @@ void free_program(DeviceProgram& prog) {
     prog.x3 = TileLists();
     prog.d_lines = nullptr;
     prog.d_terms = nullptr;
+    prog.d_litems = nullptr;
     prog.d_groups = nullptr;
     prog.d_gent_t = nullptr;
     prog.d_gent_a = nullptr;
@@ -1364,9 +1361,12 @@ cudaError_t tune_program(DeviceProgram& prog, uint64_t in, uint64_t out, double*
 
 cudaError_t run_sbuild(DeviceProgram const& prog, double* T, double* S, cudaStream_t stream) {
     const uint32_t sms = uint32_t(device_sm_count());
-    if (prog.n_lines) {
-        uint32_t grid = std::min<uint32_t>(prog.n_lines, sms * 8);
-        cudaError_t e = launch_pdl(sbuild_lines, grid, 256, 0, stream, prog.d_lines, prog.d_terms, prog.n_lines, S,
+    if (prog.n_litems) {
+        // 8 warps per CTA, up to 8 CTAs per SM resident
+        uint32_t grid = std::min<uint32_t>((prog.n_litems + 7) / 8, sms * 8);
+        cudaError_t e = launch_pdl(sbuild_lines, grid, 256, 0, stream, static_cast<const DevSLine*>(prog.d_lines),
+                                   static_cast<const DevSTerm*>(prog.d_terms),
+                                   static_cast<const DevSItem*>(prog.d_litems), prog.n_litems, S,
                                    static_cast<const double*>(T));
         if (e != cudaSuccess) return e;
     }

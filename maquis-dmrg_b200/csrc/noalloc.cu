@@ -94,7 +94,7 @@ extern "C" dmrgb200_status dmrgb200_hpsi_noalloc(const dmrgb200_plan_desc* desc,
         size_t o_p1 = place(cur, prog.stage1.probs), o_s1 = place(cur, prog.stage1.segs),
                o_t1 = place(cur, prog.stage1.tiles), o_p3 = place(cur, prog.stage3.probs),
                o_s3 = place(cur, prog.stage3.segs), o_t3 = place(cur, prog.stage3.tiles), o_l = place(cur, prog.lines),
-               o_k = place(cur, prog.terms);
+               o_k = place(cur, prog.terms), o_li = place(cur, prog.litems);
         size_t o_T = (cur + 255) / 256 * 256;
         size_t o_S = (o_T + prog.t_elems * sizeof(double) + 255) / 256 * 256;
         size_t need = o_S + prog.s_elems * sizeof(double);
@@ -121,6 +121,7 @@ extern "C" dmrgb200_status dmrgb200_hpsi_noalloc(const dmrgb200_plan_desc* desc,
         e = e == cudaSuccess ? put(o_t3, prog.stage3.tiles.data(), prog.stage3.tiles.size() * sizeof(DevTile)) : e;
         e = e == cudaSuccess ? put(o_l, prog.lines.data(), prog.lines.size() * sizeof(DevSLine)) : e;
         e = e == cudaSuccess ? put(o_k, prog.terms.data(), prog.terms.size() * sizeof(DevSTerm)) : e;
+        e = e == cudaSuccess ? put(o_li, prog.litems.data(), prog.litems.size() * sizeof(DevSItem)) : e;
         if (e != cudaSuccess)
             return noalloc_fail(DMRGB200_DEVICE_ERROR, std::string("table upload: ") + cudaGetErrorString(e));
         prog.d_p1 = reinterpret_cast<DevProb*>(b + o_p1);
@@ -131,9 +132,11 @@ extern "C" dmrgb200_status dmrgb200_hpsi_noalloc(const dmrgb200_plan_desc* desc,
         prog.d_t3 = reinterpret_cast<DevTile*>(b + o_t3);
         prog.d_lines = reinterpret_cast<DevSLine*>(b + o_l);
         prog.d_terms = reinterpret_cast<DevSTerm*>(b + o_k);
+        prog.d_litems = reinterpret_cast<DevSItem*>(b + o_li);
         prog.n_t1 = uint32_t(prog.stage1.tiles.size());
         prog.n_t3 = uint32_t(prog.stage3.tiles.size());
         prog.n_lines = uint32_t(prog.lines.size());
+        prog.n_litems = uint32_t(prog.litems.size());
         e = run_program(prog, reinterpret_cast<uint64_t>(x), reinterpret_cast<uint64_t>(y),
                         reinterpret_cast<double*>(b + o_T), reinterpret_cast<double*>(b + o_S), stream);
         if (e != cudaSuccess) return noalloc_fail(DMRGB200_DEVICE_ERROR, std::string("launch: ") + cudaGetErrorString(e));

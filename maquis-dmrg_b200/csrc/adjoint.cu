@@ -76,6 +76,91 @@ __global__ void __launch_bounds__(256) tgrad_cells(const DevSLine* __restrict__ 
     }
 }
 
+// galpha of the terms of grouped units (DevSGroup, built for the forward S build):
+// gram[entry * SG_LINES + j] = <G line j of the group, T source of the entry>, one
+// warp per (group, batch of AG_BATCH entries).  Per 128-element chunk every lane
+// holds the 8 lines' G values of its 4 elements; per entry it forms 8 partial
+// products, which a reduce-scatter butterfly (9 shuffles) sums over the warp so that
+// lanes 4j .. 4j+3 end with line j's total; the chunks add up in order, so the
+// result is bitwise reproducible.  A term's galpha is then its (entry, line) slot.
+constexpr int AG_BATCH = 16;
+__device__ __forceinline__ double sum8_scatter(double const (&p)[SG_LINES], uint32_t lane) {
+    const bool h1 = (lane >> 4) & 1u, h2 = (lane >> 3) & 1u, h3 = (lane >> 2) & 1u;
+    double q[4], r[2];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const double send = h1 ? p[k] : p[4 + k];
+        q[k] = (h1 ? p[4 + k] : p[k]) + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const double send = h2 ? q[k] : q[2 + k];
+        r[k] = (h2 ? q[2 + k] : q[k]) + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+    double v = (h3 ? r[1] : r[0]) + __shfl_xor_sync(0xffffffffu, h3 ? r[0] : r[1], 4);
+    v += __shfl_xor_sync(0xffffffffu, v, 2);
+    v += __shfl_xor_sync(0xffffffffu, v, 1);
+    return v;  // the line (lane >> 2) & 7
+}
+
+__global__ void __launch_bounds__(128) gram_groups(const DevSGroup* __restrict__ groups,
+                                                   const DevSItem* __restrict__ items, uint32_t n_items,
+                                                   const uint64_t* __restrict__ ent_t, const double* __restrict__ G,
+                                                   const double* __restrict__ T, double* __restrict__ gram) {
+    const uint32_t lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    for (uint32_t it = blockIdx.x * wpb + (threadIdx.x >> 5); it < n_items; it += gridDim.x * wpb) {
+        const DevSItem I = items[it];
+        const DevSGroup Gr = groups[I.group];
+        const uint32_t n = Gr.rows * Gr.cols, nb = min(uint32_t(AG_BATCH), Gr.ent_end - I.e0);
+        const uint64_t my_tb = lane < nb ? ent_t[I.e0 + lane] : 0;
+        double acc[AG_BATCH];
+#pragma unroll
+        for (int b = 0; b < AG_BATCH; ++b) acc[b] = 0.0;
+        for (uint32_t c0 = 0; c0 < n; c0 += 32 * SG_EPT) {
+            double g[SG_LINES][SG_EPT];
+            uint32_t el[SG_EPT];
+            bool in[SG_EPT];
+#pragma unroll
+            for (int u = 0; u < SG_EPT; ++u) {
+                el[u] = c0 + lane + 32u * u;
+                in[u] = el[u] < n;
+                const uint32_t col = in[u] ? el[u] / Gr.rows : 0, i = in[u] ? el[u] - col * Gr.rows : 0;
+                const double* src = G + Gr.s_base + i + uint64_t(col) * Gr.ld_s;
+#pragma unroll
+                for (int j = 0; j < SG_LINES; ++j)
+                    g[j][u] = (in[u] && uint32_t(j) < Gr.nlines) ? src[uint64_t(j) * Gr.line_stride] : 0.0;
+            }
+#pragma unroll
+            for (int b = 0; b < AG_BATCH; ++b) {
+                if (uint32_t(b) >= nb) break;
+                const uint64_t tb = __shfl_sync(0xffffffffu, my_tb, b);
+                double t[SG_EPT];
+#pragma unroll
+                for (int u = 0; u < SG_EPT; ++u) t[u] = in[u] ? T[tb + el[u]] : 0.0;
+                double p[SG_LINES];
+#pragma unroll
+                for (int j = 0; j < SG_LINES; ++j) {
+                    double a = 0.0;
+#pragma unroll
+                    for (int u = 0; u < SG_EPT; ++u) a = fma(g[j][u], t[u], a);
+                    p[j] = a;
+                }
+                acc[b] += sum8_scatter(p, lane);
+            }
+        }
+#pragma unroll
+        for (int b = 0; b < AG_BATCH; ++b)
+            if (uint32_t(b) < nb && (lane & 3u) == 0) gram[uint64_t(I.e0 + b) * SG_LINES + (lane >> 2)] = acc[b];
+    }
+}
+
+__global__ void __launch_bounds__(256) gram_scatter(const uint32_t* __restrict__ k, const uint32_t* __restrict__ slot,
+                                                    uint32_t n, const double* __restrict__ gram,
+                                                    double* __restrict__ galpha) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        galpha[k[i]] = gram[slot[i]];
+}
+
 template <class T>
 cudaError_t up(std::vector<T> const& v, T** d) {
     *d = nullptr;
@@ -88,7 +173,7 @@ cudaError_t up(std::vector<T> const& v, T** d) {
 }  // namespace
 
 std::string compile_adjoint(FlatPlan const& p, std::vector<uint64_t> const& stage3_bnd,
-                            std::vector<uint64_t> const& stage1_bnd, AdjointProgram& a) {
+                            std::vector<uint64_t> const& stage1_bnd, DeviceProgram const& fwd, AdjointProgram& a) {
     a = AdjointProgram();
     if (p.kind != KIND_HPSI) return "the adjoint exists for H psi plans only";
     const uint32_t nt = p.n_t(), nc = p.n_cohorts();
@@ -218,6 +303,18 @@ std::string compile_adjoint(FlatPlan const& p, std::vector<uint64_t> const& stag
         gemm_add_tiles(a.g1, uint32_t(a.g1.probs.size() - 1), 1);
     }
     gemm_sort_tiles(a.g1);
+
+    // ---- galpha of grouped units from the groups' Gram blocks; the rest term by term ----
+    std::vector<char> grouped(p.n_terms(), 0);
+    for (uint32_t k : fwd.gterm_k) grouped[k] = 1;
+    for (DevATerm const& at : a.aterms)
+        if (!grouped[at.k]) a.aterms_walk.push_back(at);
+    for (uint32_t gi = 0; gi < fwd.groups.size(); ++gi)
+        for (uint32_t e = fwd.groups[gi].ent_begin; e < fwd.groups[gi].ent_end; e += AG_BATCH)
+            a.gram_items.push_back(DevSItem{gi, e});
+    a.gram_k = fwd.gterm_k;
+    a.gram_slot = fwd.gterm_slot;
+    a.gram_elems = uint64_t(fwd.gent_t.size()) * SG_LINES;
     return std::string();
 }
 
@@ -225,10 +322,16 @@ cudaError_t upload_adjoint(AdjointProgram& a) {
     cudaError_t e;
     if ((e = upload_gemm(a.g3, a.d3)) != cudaSuccess) return e;
     if ((e = upload_gemm(a.g1, a.d1)) != cudaSuccess) return e;
-    if ((e = up(a.aterms, &a.d_aterms)) != cudaSuccess) return e;
+    if ((e = up(a.aterms_walk, &a.d_aterms)) != cudaSuccess) return e;
+    if ((e = up(a.gram_items, &a.d_gram_items)) != cudaSuccess) return e;
+    if ((e = up(a.gram_k, &a.d_gram_k)) != cudaSuccess) return e;
+    if ((e = up(a.gram_slot, &a.d_gram_slot)) != cudaSuccess) return e;
+    if (a.gram_elems && (e = cudaMalloc(&a.d_gram, a.gram_elems * sizeof(double))) != cudaSuccess) return e;
+    a.n_gram_items = uint32_t(a.gram_items.size());
+    a.n_gram_terms = uint32_t(a.gram_k.size());
     if ((e = up(a.tlines, &a.d_tlines)) != cudaSuccess) return e;
     if ((e = up(a.gterms, &a.d_gterms)) != cudaSuccess) return e;
-    a.n_aterms = uint32_t(a.aterms.size());
+    a.n_aterms = uint32_t(a.aterms_walk.size());
     a.n_tlines = uint32_t(a.tlines.size());
     return cudaSuccess;
 }
@@ -239,6 +342,14 @@ void free_adjoint(AdjointProgram& a) {
     cudaFree(a.d_aterms);
     cudaFree(a.d_tlines);
     cudaFree(a.d_gterms);
+    cudaFree(a.d_gram_items);
+    cudaFree(a.d_gram_k);
+    cudaFree(a.d_gram_slot);
+    cudaFree(a.d_gram);
+    a.d_gram_items = nullptr;
+    a.d_gram_k = nullptr;
+    a.d_gram_slot = nullptr;
+    a.d_gram = nullptr;
     a.d_aterms = nullptr;
     a.d_tlines = nullptr;
     a.d_gterms = nullptr;
@@ -272,6 +383,15 @@ cudaError_t run_adjoint(DeviceProgram const& fwd, AdjointProgram const& a, uint6
         if (a.n_aterms) {
             uint32_t grid = std::min<uint32_t>((a.n_aterms + 7) / 8, sms * 8);
             alpha_grad<<<grid, 256, 0, stream>>>(a.d_aterms, a.n_aterms, S, T, galpha);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        }
+        if (a.n_gram_items) {
+            uint32_t grid = std::min<uint32_t>((a.n_gram_items + 3) / 4, sms * 8);
+            gram_groups<<<grid, 128, 0, stream>>>(fwd.d_groups, a.d_gram_items, a.n_gram_items, fwd.d_gent_t, S, T,
+                                                  a.d_gram);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+            grid = std::min<uint32_t>((a.n_gram_terms + 255) / 256, sms * 8);
+            gram_scatter<<<grid, 256, 0, stream>>>(a.d_gram_k, a.d_gram_slot, a.n_gram_terms, a.d_gram, galpha);
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
     }

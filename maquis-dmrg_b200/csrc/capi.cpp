@@ -614,7 +614,7 @@ dmrgb200_status dmrgb200_hpsi_adjoint(dmrgb200_plan_t plan, const double* w, con
     if (!plan || !w || (galpha && !x)) return fail(DMRGB200_INVALID_ARGUMENT, "null argument");
     if (plan->flat.kind != KIND_HPSI) return fail(DMRGB200_INVALID_PLAN, "plan is not an H psi plan");
     if (!plan->adj_built) {
-        plan->adj_err = compile_adjoint(plan->flat, plan->stage3_bnd, plan->stage1_bnd, plan->adj);
+        plan->adj_err = compile_adjoint(plan->flat, plan->stage3_bnd, plan->stage1_bnd, plan->prog, plan->adj);
         if (plan->adj_err.empty()) {
             cudaError_t e = upload_adjoint(plan->adj);
             if (e != cudaSuccess) {

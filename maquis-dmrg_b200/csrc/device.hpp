@@ -137,6 +137,9 @@ struct DeviceProgram {
     std::vector<double> gent_a;    // per group entry: SG_LINES alphas
     std::vector<DevSItem> gitems;  // warp items of the groups
     std::vector<DevSItem> litems;  // warp items of the lines (DevSItem.group = line index)
+    // host only: the plan terms of grouped units and their slot (entry * SG_LINES + line)
+    // in the groups' entry tables (the adjoint reads <G line, T source> from there)
+    std::vector<uint32_t> gterm_k, gterm_slot;
     uint64_t t_elems = 0, s_elems = 0;
 
     // device copies
@@ -251,19 +254,28 @@ struct DevGTerm {
 struct AdjointProgram {
     GemmList g3;                    // G = L^T w per cohort (into the S scratch)
     GemmList g1;                    // gx slice = sum over its T tasks of gT * R^T
-    std::vector<DevATerm> aterms;   // one per plan term
-    std::vector<DevSLine> tlines;   // one per T block: gT cell = sum of its sources
+    std::vector<DevATerm> aterms;       // one per plan term
+    std::vector<DevATerm> aterms_walk;  // the terms of ungrouped units (galpha term by term)
+    std::vector<DevSLine> tlines;       // one per T block: gT cell = sum of its sources
     std::vector<DevGTerm> gterms;
+    // galpha of grouped units: Gram blocks per (group, entry batch), then one slot per term
+    std::vector<DevSItem> gram_items;
+    std::vector<uint32_t> gram_k, gram_slot;
+    uint64_t gram_elems = 0;
     GemmDev d3, d1;
     DevATerm* d_aterms = nullptr;
     DevSLine* d_tlines = nullptr;
     DevGTerm* d_gterms = nullptr;
-    uint32_t n_aterms = 0, n_tlines = 0;
+    DevSItem* d_gram_items = nullptr;
+    uint32_t* d_gram_k = nullptr;
+    uint32_t* d_gram_slot = nullptr;
+    double* d_gram = nullptr;
+    uint32_t n_aterms = 0, n_tlines = 0, n_gram_items = 0, n_gram_terms = 0;
 };
 // Lower the adjoint of an H psi plan; returns an empty string, or why the plan
 // has none (overlapping T slices, a term that is not one whole T block).
 std::string compile_adjoint(FlatPlan const& p, std::vector<uint64_t> const& stage3_bnd,
-                            std::vector<uint64_t> const& stage1_bnd, AdjointProgram& a);
+                            std::vector<uint64_t> const& stage1_bnd, DeviceProgram const& fwd, AdjointProgram& a);
 cudaError_t upload_adjoint(AdjointProgram& a);
 void free_adjoint(AdjointProgram& a);
 // gx = H^T w (NULL: skipped), galpha[k] = <w|H_k x> (NULL: skipped)

@@ -650,6 +650,7 @@ struct UnitGroups {
     std::vector<DevSGroup> groups;
     std::vector<uint64_t> ent_t;
     std::vector<double> ent_a;
+    std::vector<uint32_t> term_k, term_slot;  // plan term -> entry * SG_LINES + line
 };
 uint64_t group_unit(FlatPlan const& p, uint32_t c, uint32_t u, std::vector<int64_t> const& line_of,
                     std::vector<uint64_t> const& t_off, std::vector<uint64_t> const& s_off, UnitGroups& out,
@@ -677,6 +678,7 @@ uint64_t group_unit(FlatPlan const& p, uint32_t c, uint32_t u, std::vector<int64
         }
         G.ent_begin = uint32_t(out.ent_t.size());
         slot.clear();
+        const size_t map0 = out.term_k.size();
         for (uint32_t j = 0; j < G.nlines; ++j) {
             const int64_t l = line_of[g0 + j];
             if (l < 0) continue;
@@ -693,6 +695,8 @@ uint64_t group_unit(FlatPlan const& p, uint32_t c, uint32_t u, std::vector<int64
                     e = it->second;
                 }
                 out.ent_a[uint64_t(e) * SG_LINES + j] += p.term_alpha[k];
+                out.term_k.push_back(k);
+                out.term_slot.push_back((e - G.ent_begin) * SG_LINES + j);  // group-local until sorted
                 G.mask |= 1u << j;
                 ++*terms;
             }
@@ -715,6 +719,13 @@ uint64_t group_unit(FlatPlan const& p, uint32_t c, uint32_t u, std::vector<int64
             }
             std::copy(t.begin(), t.end(), out.ent_t.begin() + G.ent_begin);
             std::copy(al.begin(), al.end(), out.ent_a.begin() + uint64_t(G.ent_begin) * SG_LINES);
+            // the terms' slots follow their entries to the sorted positions
+            std::vector<uint32_t> pos(n);
+            for (uint32_t x = 0; x < n; ++x) pos[ord[x]] = x;
+            for (size_t q = map0; q < out.term_slot.size(); ++q) {
+                const uint32_t le = out.term_slot[q] / SG_LINES, j = out.term_slot[q] % SG_LINES;
+                out.term_slot[q] = (G.ent_begin + pos[le]) * SG_LINES + j;
+            }
         }
         fmas += uint64_t(G.ent_end - G.ent_begin) * SG_LINES;
         // the kernel walks sources SG_UNROLL at a time: pad with zero-alpha sources at T
@@ -856,7 +867,7 @@ void compile_program(FlatPlan const& p, std::vector<uint64_t> const& stage3_bnd,
             if (mode != 1 && w && (mode == 2 || dense_enough)) {
                 // line groups when they issue at most twice the per-line walk's multiply-adds
                 // (a unit without terms is zero-filled by the line walk)
-                const size_t g0 = ug.groups.size(), e0 = ug.ent_t.size();
+                const size_t g0 = ug.groups.size(), e0 = ug.ent_t.size(), m0 = ug.term_k.size();
                 uint64_t nterms = 0;
                 const uint64_t fmas = group_unit(p, c, u, line_of, t_off, s_off, ug, &nterms);
                 if (mode == 2 || (nterms && fmas <= 2 * nterms)) {
@@ -866,6 +877,8 @@ void compile_program(FlatPlan const& p, std::vector<uint64_t> const& stage3_bnd,
                 ug.groups.resize(g0);
                 ug.ent_t.resize(e0);
                 ug.ent_a.resize(e0 * SG_LINES);
+                ug.term_k.resize(m0);
+                ug.term_slot.resize(m0);
             }
             for (uint32_t b1 = 0; b1 < p.c_nsrows[c]; ++b1) {
                 DevSLine L;
@@ -910,6 +923,8 @@ void compile_program(FlatPlan const& p, std::vector<uint64_t> const& stage3_bnd,
     prog.groups = std::move(ug.groups);
     prog.gent_t = std::move(ug.ent_t);
     prog.gent_a = std::move(ug.ent_a);
+    prog.gterm_k = std::move(ug.term_k);
+    prog.gterm_slot = std::move(ug.term_slot);
     {
         std::vector<uint64_t> work(ug_units.size(), 0);
         for (size_t x = 0; x < ug_units.size(); ++x)

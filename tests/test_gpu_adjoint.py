@@ -103,6 +103,25 @@ def test_adjoint_matches_oracle(ctx, name, L, m, i):
     assert np.array_equal(gx, gx2) and np.array_equal(ga, ga2)
 
 
+@pytest.mark.parametrize("mode", ["lines", "groups", "auto"])
+def test_adjoint_qc_each_sbuild_form(ctx, monkeypatch, mode):
+    """Quantum chemistry: galpha from the line groups' Gram blocks (grouped units) and
+    term by term (the others) against the oracle, and bitwise repeatable."""
+    monkeypatch.setenv("DMRGB200_SBUILD", mode)
+    model, bonds, tensors, rng = make_chain("qc", 8, 0, seed=33, synthetic_m=64)
+    ch = OracleChain(model, bonds, tensors, 3)
+    dc = DeviceChain(ctx, ch)
+    w = random_psi(ch.p12, ch.left, ch.right, rng).data
+    x = random_psi(ch.p12, ch.left, ch.right, rng).data
+    gx, ga = dc.adjoint(w, x)
+    gx_o, ga_o = O.hpsi_adjoint(ch.sched.plan, ch.Lval, ch.Lidx, ch.Rval, ch.Ridx, w, x)
+    assert _rel(gx, gx_o) <= TOL
+    assert _rel(ga, ga_o) <= TOL
+    assert np.max(np.abs(ga - ga_o)) <= 1e-12 * np.max(np.abs(ga_o))
+    _, ga2 = dc.adjoint(w, x, want_gx=False)
+    assert np.array_equal(ga, ga2)
+
+
 def test_adjoint_identities_at_size(ctx):
     """Hubbard L=16, centre sites (7, 8), synthetic m=512: transpose and
     term-linearity identities on the device (no oracle at this size)."""

@@ -154,6 +154,63 @@ __global__ void __launch_bounds__(128) gram_groups(const DevSGroup* __restrict__
     }
 }
 
+// gT of T blocks taken as cell groups (DevTGroup): one warp per 128 elements of a
+// group; each lane keeps SG_LINES x SG_EPT accumulators (one per cell) and reads
+// every G line of the group once for all its cells; cells sum their lines in the
+// group's entry order.
+__global__ void __launch_bounds__(256) tgrad_groups(const DevTGroup* __restrict__ groups,
+                                                    const DevSItem* __restrict__ items, uint32_t n_items,
+                                                    const uint64_t* __restrict__ ent_g,
+                                                    const uint32_t* __restrict__ ent_ld,
+                                                    const double* __restrict__ ent_a, const double* __restrict__ G,
+                                                    double* __restrict__ gT) {
+    const uint32_t lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    for (uint32_t it = blockIdx.x * wpb + (threadIdx.x >> 5); it < n_items; it += gridDim.x * wpb) {
+        const DevSItem I = items[it];
+        const DevTGroup Gr = groups[I.group];
+        const uint32_t n = Gr.rows * Gr.cols;
+        uint32_t el[SG_EPT], ri[SG_EPT], ci[SG_EPT];
+        bool in[SG_EPT];
+#pragma unroll
+        for (int u = 0; u < SG_EPT; ++u) {
+            el[u] = I.e0 + lane + 32u * u;
+            in[u] = el[u] < n;
+            ci[u] = in[u] ? el[u] / Gr.rows : 0;
+            ri[u] = in[u] ? el[u] - ci[u] * Gr.rows : 0;
+        }
+        double acc[SG_LINES][SG_EPT];
+#pragma unroll
+        for (int j = 0; j < SG_LINES; ++j)
+#pragma unroll
+            for (int u = 0; u < SG_EPT; ++u) acc[j][u] = 0.0;
+        for (uint32_t k = Gr.ent_begin; k < Gr.ent_end; ++k) {
+            const double* g = G + ent_g[k];
+            const uint64_t ld = ent_ld[k];
+            double v[SG_EPT];
+#pragma unroll
+            for (int u = 0; u < SG_EPT; ++u) v[u] = in[u] ? g[ri[u] + ci[u] * ld] : 0.0;
+            const double2* a2 = reinterpret_cast<const double2*>(ent_a + uint64_t(k) * SG_LINES);
+#pragma unroll
+            for (int h = 0; h < SG_LINES / 2; ++h) {
+                const double2 x = a2[h];
+#pragma unroll
+                for (int u = 0; u < SG_EPT; ++u) {
+                    acc[2 * h][u] = fma(x.x, v[u], acc[2 * h][u]);
+                    acc[2 * h + 1][u] = fma(x.y, v[u], acc[2 * h + 1][u]);
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < SG_EPT; ++u) {
+            if (!in[u]) continue;
+#pragma unroll
+            for (int c = 0; c < SG_LINES; ++c)
+                if (uint32_t(c) < Gr.ncells)
+                    gT[Gr.out_base + uint64_t(c) * n + el[u]] = ((Gr.mask >> c) & 1u) ? acc[c][u] : 0.0;
+        }
+    }
+}
+
 __global__ void __launch_bounds__(256) gram_scatter(const uint32_t* __restrict__ k, const uint32_t* __restrict__ slot,
                                                     uint32_t n, const double* __restrict__ gram,
                                                     double* __restrict__ galpha) {
@@ -242,7 +299,49 @@ std::string compile_adjoint(FlatPlan const& p, std::vector<uint64_t> const& stag
     }
     for (uint32_t t = 0; t < nt; ++t) {
         const uint32_t M = p.in_rows[p.t_lb[t]], N = p.t_bcols[t];
+        // up to 8 consecutive blocks of the task as one cell group over the union of
+        // their G lines, where that issues at most twice the term walk's multiply-adds
+        // (and the blocks average 4 or more terms); the other blocks keep the walk
+        std::vector<char> grouped_b(p.t_nb[t], 0);
+        if (uint64_t(M) * N)
+            for (uint32_t b0 = 0; b0 < p.t_nb[t]; b0 += SG_LINES) {
+                const uint32_t ncell = std::min<uint32_t>(SG_LINES, p.t_nb[t] - b0);
+                uint64_t nterms = 0;
+                for (uint32_t c = 0; c < ncell; ++c) nterms += block_terms[tb_base[t] + b0 + c].size();
+                if (nterms < 4ull * ncell) continue;
+                std::map<std::pair<uint64_t, uint32_t>, uint32_t> slot;  // (g_base, ld_g) in address order
+                for (uint32_t c = 0; c < ncell; ++c)
+                    for (uint32_t i : block_terms[tb_base[t] + b0 + c])
+                        slot.emplace(std::make_pair(a.aterms[i].g_base, a.aterms[i].ld_g), 0u);
+                if (uint64_t(slot.size()) * SG_LINES > 2 * nterms) continue;
+                DevTGroup G{};
+                G.out_base = t_off[t] + uint64_t(b0) * M * N;
+                G.rows = M;
+                G.cols = N;
+                G.ncells = ncell;
+                G.ent_begin = uint32_t(a.tg_g.size());
+                uint32_t e = G.ent_begin;
+                for (auto& kv : slot) {
+                    kv.second = e++;
+                    a.tg_g.push_back(kv.first.first);
+                    a.tg_ld.push_back(kv.first.second);
+                    a.tg_a.insert(a.tg_a.end(), SG_LINES, 0.0);
+                }
+                G.ent_end = e;
+                for (uint32_t c = 0; c < ncell; ++c)
+                    for (uint32_t i : block_terms[tb_base[t] + b0 + c]) {
+                        DevATerm const& at = a.aterms[i];
+                        a.tg_a[uint64_t(slot[{at.g_base, at.ld_g}]) * SG_LINES + c] += p.term_alpha[at.k];
+                        G.mask |= 1u << c;
+                    }
+                const uint32_t gi = uint32_t(a.tgroups.size());
+                a.tgroups.push_back(G);
+                for (uint64_t e0 = 0; e0 < uint64_t(M) * N; e0 += 32 * SG_EPT)
+                    a.tg_items.push_back(DevSItem{gi, uint32_t(e0)});
+                for (uint32_t c = 0; c < ncell; ++c) grouped_b[b0 + c] = 1;
+            }
         for (uint32_t b = 0; b < p.t_nb[t]; ++b) {
+            if (grouped_b[b]) continue;
             DevSLine L{};
             L.s_base = t_off[t] + uint64_t(b) * M * N;
             L.ld_s = M;
@@ -324,6 +423,12 @@ cudaError_t upload_adjoint(AdjointProgram& a) {
     if ((e = upload_gemm(a.g1, a.d1)) != cudaSuccess) return e;
     if ((e = up(a.aterms_walk, &a.d_aterms)) != cudaSuccess) return e;
     if ((e = up(a.gram_items, &a.d_gram_items)) != cudaSuccess) return e;
+    if ((e = up(a.tgroups, &a.d_tgroups)) != cudaSuccess) return e;
+    if ((e = up(a.tg_items, &a.d_tg_items)) != cudaSuccess) return e;
+    if ((e = up(a.tg_g, &a.d_tg_g)) != cudaSuccess) return e;
+    if ((e = up(a.tg_ld, &a.d_tg_ld)) != cudaSuccess) return e;
+    if ((e = up(a.tg_a, &a.d_tg_a)) != cudaSuccess) return e;
+    a.n_tg_items = uint32_t(a.tg_items.size());
     if ((e = up(a.gram_k, &a.d_gram_k)) != cudaSuccess) return e;
     if ((e = up(a.gram_slot, &a.d_gram_slot)) != cudaSuccess) return e;
     if (a.gram_elems && (e = cudaMalloc(&a.d_gram, a.gram_elems * sizeof(double))) != cudaSuccess) return e;
@@ -343,6 +448,16 @@ void free_adjoint(AdjointProgram& a) {
     cudaFree(a.d_tlines);
     cudaFree(a.d_gterms);
     cudaFree(a.d_gram_items);
+    cudaFree(a.d_tgroups);
+    cudaFree(a.d_tg_items);
+    cudaFree(a.d_tg_g);
+    cudaFree(a.d_tg_ld);
+    cudaFree(a.d_tg_a);
+    a.d_tgroups = nullptr;
+    a.d_tg_items = nullptr;
+    a.d_tg_g = nullptr;
+    a.d_tg_ld = nullptr;
+    a.d_tg_a = nullptr;
     cudaFree(a.d_gram_k);
     cudaFree(a.d_gram_slot);
     cudaFree(a.d_gram);
@@ -399,6 +514,12 @@ cudaError_t run_adjoint(DeviceProgram const& fwd, AdjointProgram const& a, uint6
         if (a.n_tlines) {
             uint32_t grid = std::min<uint32_t>(a.n_tlines, sms * 8);
             tgrad_cells<<<grid, 256, 0, stream>>>(a.d_tlines, a.d_gterms, a.n_tlines, T, S);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        }
+        if (a.n_tg_items) {
+            uint32_t grid = std::min<uint32_t>((a.n_tg_items + 7) / 8, sms * 4);
+            tgrad_groups<<<grid, 256, 0, stream>>>(a.d_tgroups, a.d_tg_items, a.n_tg_items, a.d_tg_g, a.d_tg_ld,
+                                                   a.d_tg_a, S, T);
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
         if ((e = cudaMemsetAsync(gx, 0, gx_elems * sizeof(double), stream)) != cudaSuccess) return e;

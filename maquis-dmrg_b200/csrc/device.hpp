@@ -245,6 +245,14 @@ struct DevATerm {
     uint32_t rows, cols, ld_g, ld_t;
     uint32_t k, pad;
 };
+// adjoint gT of up to SG_LINES consecutive T blocks (cells) of one T task over the union
+// of their G lines: cell c is rows x cols at out_base + c * rows * cols
+struct DevTGroup {
+    uint64_t out_base;
+    uint32_t rows, cols, ncells;
+    uint32_t ent_begin, ent_end;
+    uint32_t mask;  // bit c: cell c has sources (the others are written as zeros)
+};
 // gT source: alpha * G cell at g_base with leading dimension ld
 struct DevGTerm {
     double alpha;
@@ -262,6 +270,13 @@ struct AdjointProgram {
     std::vector<DevSItem> gram_items;
     std::vector<uint32_t> gram_k, gram_slot;
     uint64_t gram_elems = 0;
+    // gT of T blocks in cell groups: groups, warp items, and per entry the G line
+    // (start, leading dimension) with SG_LINES alphas
+    std::vector<DevTGroup> tgroups;
+    std::vector<DevSItem> tg_items;
+    std::vector<uint64_t> tg_g;
+    std::vector<uint32_t> tg_ld;
+    std::vector<double> tg_a;
     GemmDev d3, d1;
     DevATerm* d_aterms = nullptr;
     DevSLine* d_tlines = nullptr;
@@ -270,7 +285,12 @@ struct AdjointProgram {
     uint32_t* d_gram_k = nullptr;
     uint32_t* d_gram_slot = nullptr;
     double* d_gram = nullptr;
-    uint32_t n_aterms = 0, n_tlines = 0, n_gram_items = 0, n_gram_terms = 0;
+    DevTGroup* d_tgroups = nullptr;
+    DevSItem* d_tg_items = nullptr;
+    uint64_t* d_tg_g = nullptr;
+    uint32_t* d_tg_ld = nullptr;
+    double* d_tg_a = nullptr;
+    uint32_t n_aterms = 0, n_tlines = 0, n_gram_items = 0, n_gram_terms = 0, n_tg_items = 0;
 };
 // Lower the adjoint of an H psi plan; returns an empty string, or why the plan
 // has none (overlapping T slices, a term that is not one whole T block).

@@ -295,8 +295,9 @@ dmrgb200_status dmrgb200_dgemm_f64(uint32_t M, uint32_t N, uint32_t K, const dou
 /* C = A * B (column-major FP64, A M x K, B K x N) computed with `slices`
  * (2..8) signed 7-bit digit planes per operand on tcgen05 INT8 MMAs with exact
  * INT32 accumulation and FP64 recombination (Ozaki scheme, integer variant);
- * relative accuracy about 2^(-7 slices) of the row/column maxima.  Requires
- * K * slices <= 2^17.  Stream-ordered; returns after completion. */
+ * relative accuracy about 2^(-7 slices) of the row/column maxima.  K beyond
+ * 2^17 / slices accumulates in exact INT32 chunks of that length, summed in
+ * FP64.  Stream-ordered; returns after completion. */
 dmrgb200_status dmrgb200_dgemm_emulated(uint32_t M, uint32_t N, uint32_t K, const double* A, uint64_t lda,
                                         const double* B, uint64_t ldb, double* C, uint64_t ldc, int slices,
                                         void* cuda_stream);

@@ -299,11 +299,8 @@ dmrgb200_status run_step(dmrgb200_plan_s* p, const double* ket, const double* br
 // digit planes), the S build in FP64 between them.  Synchronises the stream to
 // report pipeline timeouts.
 dmrgb200_status hpsi_emulated(dmrgb200_plan_s* plan, const double* x, double* y, cudaStream_t st) {
-    const uint64_t klim = (1ull << 17) / uint64_t(plan->slices);
     if (!plan->oz1) {
         GemmList const& s1 = plan->prog.stage1_tasks.probs.empty() ? plan->prog.stage1 : plan->prog.stage1_tasks;
-        if (max_k_total(s1) > klim || max_k_total(plan->prog.stage3) > klim)
-            return fail(DMRGB200_NOT_SUPPORTED, "a contraction is longer than the exact INT32 range of the emulation");
         plan->oz1 = oz_build(s1);
         plan->oz3 = oz_build(plan->prog.stage3);
         if (!plan->oz1 || !plan->oz3) return fail(DMRGB200_OUT_OF_MEMORY, "emulation tables");

@@ -307,7 +307,6 @@ cudaError_t run_sbuild(DeviceProgram const& prog, double* T, double* S, cudaStre
 // last call (the flag is cleared)
 bool sbuild_timed_out(DeviceProgram const& prog);
 // largest K of any output matrix of a GEMM list (emulation needs K * slices <= 2^17)
-uint64_t max_k_total(GemmList const& gl);
 
 // ---- FP64 emulated on the INT8 tensor cores (ozaki.cu) ----
 struct OzProgram;  // lowered grouped problem list

@@ -1410,16 +1410,6 @@ bool sbuild_timed_out(DeviceProgram const& prog) {
     return v != 0;
 }
 
-uint64_t max_k_total(GemmList const& gl) {
-    uint64_t m = 0;
-    for (auto const& p : gl.probs) {
-        uint64_t k = 0;
-        for (uint32_t s = p.seg_begin; s < p.seg_end; ++s) k += gl.segs[s].K;
-        m = std::max(m, k);
-    }
-    return m;
-}
-
 int device_sm_count() {
     int dev = 0, n = 0;
     cudaGetDevice(&dev);

@@ -7,8 +7,9 @@
 //   * every row i of A is scaled by 2^-e_i so that |A_ij 2^-e_i| < 1 and cut into
 //     s signed 7-bit digits a_p (p = 0..s-1): A_ij 2^-e_i = sum_p a_p 2^-7(p+1) + r,
 //     |r| < 2^-7s; every column j of B likewise with 2^-f_j;
-//   * products of digit matrices are exact in INT32 (|a b| <= 127^2, K <= 2^17/s);
-//     digit pairs with p + q = g share one accumulator D_g, pairs with p + q >= s
+//   * products of digit matrices are exact in INT32 (|a b| <= 127^2) over up to
+//     2^17/s K elements; longer contractions accumulate in chunks of that length,
+//     each chunk's partial product added into C in FP64; digit pairs with p + q = g share one accumulator D_g, pairs with p + q >= s
 //     are dropped (their weight is below the truncation error);
 //   * C_ij = 2^(e_i + f_j) sum_g 2^-7(g+2) D_g[i][j], combined in FP64 from the
 //     smallest group up.
@@ -39,6 +40,10 @@ constexpr int OZ_BM = 128, OZ_BN = 64, OZ_BK = 64;        // tile rows, tile col
 constexpr int A_TILE = OZ_BM * OZ_BK, B_TILE = OZ_BN * OZ_BK;
 constexpr int OZ_THREADS = 128, OZ_STAGES = 2, OZ_MAX_SLICES = 8;
 using namespace async;
+
+// K slabs per exact INT32 accumulation: accumulator D_g sums (g + 1) <= s digit
+// products of |a b| <= 127^2 per K element, and 127^2 * 2^17 < 2^31
+constexpr uint32_t oz_chunk_slabs(int s) { return std::max<uint32_t>(1u, (1u << 17) / uint32_t(s * OZ_BK)); }
 
 // byte offset of element (r, k) of a (rows x 64-byte) K-major tile in the
 // canonical no-swizzle layout: 8x16-byte core matrices, LBO = 128 B along K,
@@ -195,6 +200,7 @@ struct OzArgs {
     const OzSlab* slabs;
     const OzTile* tiles;
     uint32_t n_tiles;
+    uint32_t chunk;  // K slabs accumulated in TMEM before a partial epilogue (>= 1)
     int s;
     Bases bases;
     int* err;
@@ -231,92 +237,100 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_mma(OzArgs a) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
 
-    // running slab / tile counters: every arrival on every barrier is waited for exactly once, in order
-    uint32_t slab0 = 0, tiles = 0, issued = 0, consumed = 0;
+    // running slab / round counters: every arrival on every barrier is waited for exactly once, in order.
+    // A tile's slabs are accumulated in chunks of a.chunk slabs (the exact INT32 range); each chunk
+    // ends with one epilogue round that adds its partial product into C.
+    uint32_t slab0 = 0, rounds = 0, issued = 0, consumed = 0;
     bool failed = false;
     for (uint32_t tile = blockIdx.x; tile < a.n_tiles && !failed; tile += gridDim.x) {
         const OzTile tl = a.tiles[tile];
         const OzPB pb = a.pbs[tl.pb];
         const uint32_t mt = tl.mt, nt = tl.nt;
         const uint32_t KT = pb.slab_end - pb.slab_begin;
-        if (threadIdx.x == 0) {
-            auto load = [&](uint32_t kt) -> bool {
-                const uint32_t gs = slab0 + kt, st = gs % OZ_STAGES;
-                if (gs >= OZ_STAGES && !mbar_wait(&empty[st], ((gs - OZ_STAGES) / OZ_STAGES) & 1u, a.err)) return false;
-                const OzSlab sl = a.slabs[pb.slab_begin + kt];
-                unsigned char* base = smem + st * stage_bytes;
-                mbar_expect_tx(&full[st], stage_bytes);
-                for (int p = 0; p < s; ++p) {
-                    bulk_load(base + p * A_TILE, a.A8 + p * a.a_plane + sl.a_off + uint64_t(mt) * sl.a_ts, A_TILE,
-                              &full[st]);
-                    bulk_load(base + s * A_TILE + p * B_TILE, a.B8 + p * a.b_plane + sl.b_off + uint64_t(nt) * sl.b_ts,
-                              B_TILE, &full[st]);
-                }
-                ++issued;
-                return true;
-            };
-            bool ok = true;
-            for (uint32_t kt = 0; kt < KT && kt < OZ_STAGES && ok; ++kt) ok = load(kt);
-            for (uint32_t kt = 0; kt < KT && ok; ++kt) {
-                const uint32_t gs = slab0 + kt, st = gs % OZ_STAGES;
-                ok = mbar_wait(&full[st], (gs / OZ_STAGES) & 1u, a.err);
-                if (!ok) break;
-                ++consumed;
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t abase = smem_u32(smem + st * stage_bytes);
-                const uint32_t bbase = abase + s * A_TILE;
-                for (int ks = 0; ks < OZ_BK / 32; ++ks)
-                    for (int g = 0; g < s; ++g)
-                        for (int p = 0; p <= g; ++p) {
-                            const uint64_t da = umma_desc(abase + p * A_TILE + ks * 256);
-                            const uint64_t db = umma_desc(bbase + (g - p) * B_TILE + ks * 256);
-                            const uint32_t accum = (kt > 0 || ks > 0 || p > 0) ? 1u : 0u;
-                            umma_i8(tmem + uint32_t(g * OZ_BN), da, db, idesc, accum);
-                        }
-                umma_commit(&empty[st]);
-                if (kt + OZ_STAGES < KT) ok = load(kt + OZ_STAGES);
+        const uint32_t nch = KT ? (KT + a.chunk - 1) / a.chunk : 1;
+        bool ok = true;  // thread 0's pipeline state over the tile's chunks
+        auto load = [&](uint32_t kt) -> bool {
+            const uint32_t gs = slab0 + kt, st = gs % OZ_STAGES;
+            if (gs >= OZ_STAGES && !mbar_wait(&empty[st], ((gs - OZ_STAGES) / OZ_STAGES) & 1u, a.err)) return false;
+            const OzSlab sl = a.slabs[pb.slab_begin + kt];
+            unsigned char* base = smem + st * stage_bytes;
+            mbar_expect_tx(&full[st], stage_bytes);
+            for (int p = 0; p < s; ++p) {
+                bulk_load(base + p * A_TILE, a.A8 + p * a.a_plane + sl.a_off + uint64_t(mt) * sl.a_ts, A_TILE,
+                          &full[st]);
+                bulk_load(base + s * A_TILE + p * B_TILE, a.B8 + p * a.b_plane + sl.b_off + uint64_t(nt) * sl.b_ts,
+                          B_TILE, &full[st]);
             }
-            if (!ok) atomicExch(a.err, 1);
-            umma_commit(done);  // arrives once every MMA issued so far has completed
-        }
-        slab0 += KT;
-        __syncwarp();
-        const bool ready = mbar_wait(done, tiles & 1u, a.err);
-        ++tiles;
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const bool go = __all_sync(0xffffffffu, ready && *verr == 0);
-        if (go) {
-            const uint32_t row = mt * OZ_BM + warp * 32 + lane;
-            const int erow = (row < pb.M) ? a.e[pb.e_off + row] : 0;
-            double* Cb = reinterpret_cast<double*>(base_of(a.bases, pb.C.buf) + 8ull * pb.C.off);
-            for (int c0 = 0; c0 < OZ_BN; c0 += 16) {
-                double acc[16];
-#pragma unroll
-                for (int j = 0; j < 16; ++j) acc[j] = 0.0;
-                for (int g = s - 1; g >= 0 && KT > 0; --g) {
-                    int32_t v[16];
-                    tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + uint32_t(g * OZ_BN + c0), v);
-                    const double w = ldexp(1.0, -7 * (g + 2));
-#pragma unroll
-                    for (int j = 0; j < 16; ++j) acc[j] += double(v[j]) * w;
+            ++issued;
+            return true;
+        };
+        for (uint32_t ch = 0; ch < nch && !failed; ++ch) {
+            const uint32_t k_begin = ch * a.chunk, k_end = min(KT, k_begin + a.chunk);
+            if (threadIdx.x == 0) {
+                if (ch == 0)
+                    for (uint32_t kt = 0; kt < KT && kt < OZ_STAGES && ok; ++kt) ok = load(kt);
+                for (uint32_t kt = k_begin; kt < k_end && ok; ++kt) {
+                    const uint32_t gs = slab0 + kt, st = gs % OZ_STAGES;
+                    ok = mbar_wait(&full[st], (gs / OZ_STAGES) & 1u, a.err);
+                    if (!ok) break;
+                    ++consumed;
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t abase = smem_u32(smem + st * stage_bytes);
+                    const uint32_t bbase = abase + s * A_TILE;
+                    for (int ks = 0; ks < OZ_BK / 32; ++ks)
+                        for (int g = 0; g < s; ++g)
+                            for (int p = 0; p <= g; ++p) {
+                                const uint64_t da = umma_desc(abase + p * A_TILE + ks * 256);
+                                const uint64_t db = umma_desc(bbase + (g - p) * B_TILE + ks * 256);
+                                const uint32_t accum = (kt > k_begin || ks > 0 || p > 0) ? 1u : 0u;
+                                umma_i8(tmem + uint32_t(g * OZ_BN), da, db, idesc, accum);
+                            }
+                    umma_commit(&empty[st]);
+                    if (kt + OZ_STAGES < KT) ok = load(kt + OZ_STAGES);
                 }
-                if (row < pb.M) {
+                if (!ok) atomicExch(a.err, 1);
+                umma_commit(done);  // arrives once every MMA issued so far has completed
+            }
+            __syncwarp();
+            const bool ready = mbar_wait(done, rounds & 1u, a.err);
+            ++rounds;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const bool go = __all_sync(0xffffffffu, ready && *verr == 0);
+            if (go) {
+                const uint32_t row = mt * OZ_BM + warp * 32 + lane;
+                const int erow = (row < pb.M) ? a.e[pb.e_off + row] : 0;
+                const bool add = pb.beta || ch > 0;
+                double* Cb = reinterpret_cast<double*>(base_of(a.bases, pb.C.buf) + 8ull * pb.C.off);
+                for (int c0 = 0; c0 < OZ_BN; c0 += 16) {
+                    double acc[16];
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) {
-                        const uint32_t col = nt * OZ_BN + c0 + j;
-                        if (col < pb.N) {
-                            const double val = ldexp(acc[j], erow + a.e[pb.f_off + col]);
-                            double* dst = Cb + row + uint64_t(col) * pb.C.ld;
-                            *dst = pb.beta ? *dst + val : val;
+                    for (int j = 0; j < 16; ++j) acc[j] = 0.0;
+                    for (int g = s - 1; g >= 0 && KT > 0; --g) {
+                        int32_t v[16];
+                        tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + uint32_t(g * OZ_BN + c0), v);
+                        const double w = ldexp(1.0, -7 * (g + 2));
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) acc[j] += double(v[j]) * w;
+                    }
+                    if (row < pb.M) {
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) {
+                            const uint32_t col = nt * OZ_BN + c0 + j;
+                            if (col < pb.N) {
+                                const double val = ldexp(acc[j], erow + a.e[pb.f_off + col]);
+                                double* dst = Cb + row + uint64_t(col) * pb.C.ld;
+                                *dst = add ? *dst + val : val;
+                            }
                         }
                     }
                 }
             }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncthreads();
+            failed = (*verr != 0);
+            __syncthreads();
         }
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();
-        failed = (*verr != 0);
-        __syncthreads();
+        slab0 += KT;
     }
     if (threadIdx.x == 0) {
         // after a timeout: let the bulk copies still in flight land before the CTA leaves (bounded);
@@ -523,7 +537,7 @@ cudaError_t oz_run(OzProgram* oz, Bases const& bs, int s, void* scratch, cudaStr
             attr = true;
         }
         OzArgs args{c.A8, c.B8, oz->a_plane, oz->b_plane, c.e, oz->d_pbs, oz->d_slabs, oz->d_tiles,
-                    uint32_t(oz->tiles.size()), s, bs, c.err};
+                    uint32_t(oz->tiles.size()), oz_chunk_slabs(s), s, bs, c.err};
         ozaki_mma<<<std::min<uint32_t>(uint32_t(oz->tiles.size()), uint32_t(sms)), OZ_THREADS, ozaki_smem_bytes(s),
                     st>>>(args);
     }
@@ -547,8 +561,6 @@ extern "C" dmrgb200_status dmrgb200_dgemm_emulated(uint32_t M, uint32_t N, uint3
                                                    int slices, void* cuda_stream) {
     if (!A || !B || !C) return noalloc_fail(DMRGB200_INVALID_ARGUMENT, "null argument");
     if (slices < 2 || slices > OZ_MAX_SLICES) return noalloc_fail(DMRGB200_INVALID_ARGUMENT, "slices must be 2..8");
-    if (uint64_t(K) * uint64_t(slices) > (1ull << 17))
-        return noalloc_fail(DMRGB200_INVALID_ARGUMENT, "K * slices exceeds the exact INT32 accumulation range");
     if (lda < M || ldb < K || ldc < M) return noalloc_fail(DMRGB200_INVALID_ARGUMENT, "leading dimension too small");
     cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
     GemmList gl;

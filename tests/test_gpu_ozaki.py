@@ -43,5 +43,21 @@ def test_emulated_gemm_rejects_bad_arguments():
     d = torch.zeros(16, dtype=torch.float64, device="cuda")
     assert capi.lib.dmrgb200_dgemm_emulated(4, 4, 4, d.data_ptr(), 4, d.data_ptr(), 4, d.data_ptr(), 4, 9,
                                             None) == 1
-    assert capi.lib.dmrgb200_dgemm_emulated(4, 4, 1 << 17, d.data_ptr(), 4, d.data_ptr(), 1 << 17, d.data_ptr(),
-                                            4, 7, None) == 1
+    assert capi.lib.dmrgb200_dgemm_emulated(4, 4, 4, d.data_ptr(), 3, d.data_ptr(), 4, d.data_ptr(), 4, 7,
+                                            None) == 1
+
+
+@pytest.mark.parametrize("s,K", [(7, 40000), (8, 16384 + 64), (3, 2 * 43648 + 5)])
+def test_emulated_gemm_long_k_in_chunks(s, K):
+    """K beyond 2^17 / slices: the tile accumulates exact INT32 chunks of
+    floor(2^17 / (64 s)) slabs of 64 and adds each chunk's FP64 partial product
+    into C; the error bound stays that of the split."""
+    M, N = 130, 70
+    rng = np.random.default_rng(K + s)
+    A = rng.standard_normal((M, K))
+    B = rng.standard_normal((K, N))
+    ref = A @ B
+    scale = np.abs(A).max(axis=1)[:, None] * np.abs(B).max(axis=0)[None, :] * K
+    tol = {7: 1e-14, 8: 1e-14, 3: 1e-5}[s]
+    err = np.max(np.abs(_emulated(A, B, s) - ref) / scale)
+    assert err <= tol, err

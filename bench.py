@@ -251,7 +251,8 @@ def sweep_workload(args):
     rng = np.random.default_rng(1)
     A = S.random_mps(model.phys, S.allowed_sectors(model.phys, L, model.total_charge, 5), rng)
     ctx = E.Context(0)
-    dev = G.TwoSiteDMRG(G.DeviceBackend(ctx), model, list(A), m, jd_tol=1e-8, jd_maxiter=8)
+    dsplit = args.split == "device"
+    dev = G.TwoSiteDMRG(G.DeviceBackend(ctx), model, list(A), m, jd_tol=1e-8, jd_maxiter=8, device_split=dsplit)
     for sw in range(nsweeps):
         dev.sweep(sw)
     cpu_t0 = time.perf_counter()
@@ -263,13 +264,17 @@ def sweep_workload(args):
     ec = np.array([e[2] for e in cpu.log.energies])
     line = {"metric": "two-site sweep time (s)", "value": float(np.mean(dev.log.sweep_seconds)), "unit": "s",
             "higher_is_better": False, "n_gpus": 1, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "heisenberg_L32_u1_m128_4sweeps", "sites": L, "bond_dim": m, "sweeps": nsweeps},
+            "config": {"workload": "heisenberg_L32_u1_m128_4sweeps", "sites": L, "bond_dim": m, "sweeps": nsweeps,
+                       "split": args.split},
             "sweep_seconds": dev.log.sweep_seconds, "final_energy": float(ed[-1]),
             "max_abs_energy_diff_vs_oracle": float(np.max(np.abs(ed - ec))),
             "hpsi_calls": dev.log.hpsi_calls, "solve_device_ms": dev.log.solve_ms,
             "phase_seconds": dev.log.phase_seconds, "site_problem_phase_seconds": dev.be.phase_seconds,
             "cpu_oracle_sweep_seconds": cpu.log.sweep_seconds, "cpu_oracle_final_energy": float(ec[-1]),
-            "note": "two-site formation and SVD truncation on the host (numpy); H·psi, JD and boundary steps on the device"}
+            "note": ("two-site formation on the host; the split on the device (block Jacobi SVD, truncation choice "
+                     "on the host from the singular values)" if dsplit else
+                     "two-site formation and SVD truncation on the host (numpy)") +
+                    "; H·psi, JD and boundary steps on the device"}
     print(json.dumps(line), flush=True)
 
 
@@ -613,6 +618,8 @@ def main():
                          "a regular 4096^3 GEMM; qc: a quantum-chemistry site problem; adjoint: the adjoint "
                          "checked by finite differences and RDM elements on a quantum-chemistry site problem; "
                          "steps: the left and right boundary steps at the middle of the Hubbard chain")
+    ap.add_argument("--split", default="host", choices=["host", "device"],
+                    help="where the sweep workload splits the two-site tensor")
     ap.add_argument("--qc-sites", type=int, default=24, help="orbitals of the qc workload")
     ap.add_argument("--qc-m", type=int, default=2000, help="bond dimension of the qc workload")
     ap.add_argument("--adj-sites", type=int, default=16, help="orbitals of the adjoint workload")

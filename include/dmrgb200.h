@@ -302,6 +302,40 @@ dmrgb200_status dmrgb200_dgemm_emulated(uint32_t M, uint32_t N, uint32_t K, cons
                                         const double* B, uint64_t ldb, double* C, uint64_t ldc, int slices,
                                         void* cuda_stream);
 
+/* ---- two-site split on the device ----------------------------------------- */
+/* Thin SVD of every block of a block matrix: for block i (column-major,
+ * rows[i] x cols[i], ld rows[i], device memory) writes U (rows x k, ld rows),
+ * the singular values s (k, descending) and V^T (k x cols, ld k), k =
+ * min(rows, cols); replaces the per-block loop of svd(block_matrix)
+ * (dmrg/framework/dmrg/block_matrix/block_matrix_algorithms.h:95-113).  The
+ * pointer arrays are host arrays of device pointers.  One-sided Jacobi in FP64:
+ * singular values to high relative accuracy; the U columns of zero singular
+ * values are zero.  Blocks with a zero extent are skipped.  Stream-ordered;
+ * returns after completion (DMRGB200_NUMERIC if the sweeps do not converge). */
+dmrgb200_status dmrgb200_block_svd(uint32_t n_blocks, const uint32_t* rows, const uint32_t* cols,
+                                   const double* const* a, double* const* u, double* const* s,
+                                   double* const* vt, void* cuda_stream);
+
+typedef enum { DMRGB200_SCALE_NONE = 0, DMRGB200_SCALE_ROWS = 1, DMRGB200_SCALE_COLS = 2 } dmrgb200_scale_mode;
+
+/* dst[dst_off + i + j dst_ld] = src[src_off + i + j src_ld] (times
+ * scale[scale_off + i] for DMRGB200_SCALE_ROWS, scale[scale_off + j] for
+ * DMRGB200_SCALE_COLS), 0 <= i < rows, 0 <= j < cols; offsets in elements. */
+typedef struct {
+    uint64_t src_off, dst_off, scale_off;
+    uint32_t src_ld, dst_ld;
+    uint32_t rows, cols;
+    uint32_t scale_mode, reserved;
+} dmrgb200_block_copy;
+
+/* Block copies between device buffers: the gather of the two-site matrix
+ * Theta and the scatter of U, S V^T (or U S, V^T) into the site tensors
+ * (TwoSiteTensor::split_mps_l2r / split_mps_r2l,
+ * dmrg/framework/dmrg/mp_tensors/twositetensor.hpp:153-200).  `copies` is a host
+ * array; destinations must not overlap.  Stream-ordered, asynchronous. */
+dmrgb200_status dmrgb200_copy_blocks(uint32_t n, const dmrgb200_block_copy* copies, const double* src, double* dst,
+                                     const double* scale, void* cuda_stream);
+
 /* ---- eigensolver ---------------------------------------------------------- */
 /* Lowest eigenpair of H_eff by Jacobi-Davidson in FP64 on the device
  * (solve<double>, dmrg/framework/dmrg/solver/solver.cpp:13-28 ->

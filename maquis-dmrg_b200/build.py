@@ -19,9 +19,9 @@ INCLUDE = HERE.parent / "include"
 CUDA = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 
 CXX_SOURCES = ["coupling.cpp", "schedule.cpp", "plan.cpp", "capi.cpp"]
-CU_SOURCES = ["kernels_fp64.cu", "noalloc.cu", "jd.cu", "jd_graph.cu", "ozaki.cu", "adjoint.cu"]
+CU_SOURCES = ["kernels_fp64.cu", "noalloc.cu", "jd.cu", "jd_graph.cu", "ozaki.cu", "adjoint.cu", "block_svd.cu"]
 HEADERS = ["symm.hpp", "mpo.hpp", "coupling.hpp", "boundary_index.hpp", "schedule.hpp", "plan.hpp",
-           "device.hpp"]
+           "device.hpp", "async_copy.cuh"]
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-Xptxas", "-v"]

@@ -90,6 +90,16 @@ class BoundaryView(C.Structure):
     _fields_ = [("n_cohorts", C.c_uint32), ("cohort_ptr", C.POINTER(C.c_void_p))]
 
 
+class BlockCopy(C.Structure):
+    """dmrgb200_block_copy: one column-major block copy, optionally scaled per row or column."""
+    _fields_ = [("src_off", C.c_uint64), ("dst_off", C.c_uint64), ("scale_off", C.c_uint64),
+                ("src_ld", C.c_uint32), ("dst_ld", C.c_uint32), ("rows", C.c_uint32), ("cols", C.c_uint32),
+                ("scale_mode", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+SCALE_NONE, SCALE_ROWS, SCALE_COLS = 0, 1, 2
+
+
 vp = C.c_void_p
 _sigs = {
     "dmrgb200_status_string": ([C.c_int], C.c_char_p),
@@ -123,6 +133,9 @@ _sigs = {
                             C.c_int, vp], C.c_int),
     "dmrgb200_dgemm_emulated": ([C.c_uint32, C.c_uint32, C.c_uint32, vp, C.c_uint64, vp, C.c_uint64, vp,
                                  C.c_uint64, C.c_int, vp], C.c_int),
+    "dmrgb200_block_svd": ([C.c_uint32, u32p, u32p, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), C.POINTER(vp),
+                            vp], C.c_int),
+    "dmrgb200_copy_blocks": ([C.c_uint32, C.POINTER(BlockCopy), vp, vp, vp, vp], C.c_int),
     "dmrgb200_solve": ([vp, C.c_uint64, vp, C.POINTER(vp), C.c_uint32, C.c_double, C.c_uint32, f64p, vp,
                         C.POINTER(SolveStats), vp], C.c_int),
     "dmrgb200_hpsi_noalloc": ([C.POINTER(PlanDesc), C.POINTER(BoundaryView), C.POINTER(BoundaryView), vp, vp, vp],

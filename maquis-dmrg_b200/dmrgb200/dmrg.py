@@ -16,6 +16,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
+from . import _capi as capi
 from . import engine as E
 from . import models as M
 from . import mps as S
@@ -59,18 +60,21 @@ class SplitResult:
     B: S.SiteTensor
     truncated_weight: float
     bond: list
+    # device copies written by split_device: A right-paired, A left-paired, B right-paired
+    dev_A: object = None
+    dev_A_lp: object = None
+    dev_B: object = None
 
 
-def split(psi: S.SiteTensor, phys1, phys2, offs, m: int, cutoff: float, left_to_right: bool) -> SplitResult:
-    """SVD split of a two-site tensor with truncation to m states and relative
-    cutoff (svd_truncate, block_matrix/block_matrix_algorithms.h:185-298):
-    left-to-right keeps U left-normalised and moves S V^T right, right-to-left
-    keeps V^T right-normalised and moves U S left."""
+def _mid_blocks(psi: S.SiteTensor, phys1, phys2, offs):
+    """Rows (s1, i1, lc, ml) and columns (s2, i2, rc, mr) of the matrix Theta of
+    every middle charge, and the psi sub-blocks that fill it as (row offset,
+    column offset, ml, mr, psi block, column in that block) (the reshape of
+    TwoSiteTensor to a left-paired matrix, mp_tensors/twositetensor.hpp:153-200)."""
     left, right = psi.left, psi.right
     lpos = {c: i for i, (c, _) in enumerate(left)}
     rpos = {c: i for i, (c, _) in enumerate(right)}
     p12pos = {c: k for k, (c, _) in enumerate(psi.phys)}
-    # rows (s1, i1, lc) and columns (s2, i2, rc) of every middle charge
     mids = {}
     for s1, (c1, d1) in enumerate(phys1):
         for lc, ml in left:
@@ -85,12 +89,12 @@ def split(psi: S.SiteTensor, phys1, phys2, offs, m: int, cutoff: float, left_to_
             for i2 in range(d2):
                 mids[mc][1].append((s2, i2, rc, right[rpos[rc]][1]))
     d2s = dict(phys2)
-    svds = {}
+    out = {}
     for mc, (rows, cols) in mids.items():
         nr, nc = sum(r[3] for r in rows), sum(c[3] for c in cols)
         if nr == 0 or nc == 0:
             continue
-        Th = np.zeros((nr, nc))
+        fills = []
         ro = 0
         for (s1, i1, lc, ml) in rows:
             co = 0
@@ -100,28 +104,52 @@ def split(psi: S.SiteTensor, phys1, phys2, offs, m: int, cutoff: float, left_to_
                 f = (c1[0] + c2[0], c1[1] + c2[1])
                 k = (lpos[lc], p12pos[f], offs[(c1, c2)] + i1 * d2s[c2] + i2)
                 if k in psi.rp.sub:
-                    _, c0, _, _, _ = psi.rp.sub[k]
-                    Th[ro:ro + ml, co:co + mr] = S.block_view(psi.data, psi.rp, lpos[lc])[:, c0:c0 + mr]
+                    fills.append((ro, co, ml, mr, lpos[lc], psi.rp.sub[k][1]))
                 co += mr
             ro += ml
-        U, sv, Vt = np.linalg.svd(Th, full_matrices=False)
-        svds[mc] = (U, sv, Vt, rows, cols)
-    allsv = np.concatenate([v[1] for v in svds.values()]) if svds else np.zeros(0)
+        out[mc] = (rows, cols, nr, nc, fills)
+    return out
+
+
+def _truncate(svals: dict, m: int, cutoff: float):
+    """Kept states per middle charge: the m largest singular values over all
+    blocks above cutoff times the largest (svd_truncate,
+    block_matrix/block_matrix_algorithms.h:185-298).  Returns (kept, bond,
+    truncated weight)."""
+    allsv = np.concatenate([v for v in svals.values()]) if svals else np.zeros(0)
     total = float(np.sum(allsv ** 2))
     order = np.sort(allsv)[::-1]
     keep_n = min(m, int(np.sum(order > cutoff * (order[0] if order.size else 0))))
     thresh = order[keep_n - 1] if keep_n > 0 else np.inf
-    kept, bond = {}, []
+    kept = {}
     count = 0
-    for mc in sorted(svds):
-        sv = svds[mc][1]
+    for mc in sorted(svals):
+        sv = svals[mc]
         k = int(np.sum(sv >= thresh))
         k = min(k, keep_n - count)
         if k > 0:
             kept[mc] = k
             count += k
     bond = [(mc, kept[mc]) for mc in sorted(kept)]
-    tw = 1.0 - float(sum(np.sum(svds[mc][1][:kept[mc]] ** 2) for mc in kept)) / total if total > 0 else 0.0
+    tw = 1.0 - float(sum(np.sum(svals[mc][:kept[mc]] ** 2) for mc in kept)) / total if total > 0 else 0.0
+    return kept, bond, tw
+
+
+def split(psi: S.SiteTensor, phys1, phys2, offs, m: int, cutoff: float, left_to_right: bool) -> SplitResult:
+    """SVD split of a two-site tensor with truncation to m states and relative
+    cutoff (svd_truncate, block_matrix/block_matrix_algorithms.h:185-298):
+    left-to-right keeps U left-normalised and moves S V^T right, right-to-left
+    keeps V^T right-normalised and moves U S left.  Host (numpy) SVDs."""
+    left, right = psi.left, psi.right
+    lpos = {c: i for i, (c, _) in enumerate(left)}
+    svds = {}
+    for mc, (rows, cols, nr, nc, fills) in _mid_blocks(psi, phys1, phys2, offs).items():
+        Th = np.zeros((nr, nc))
+        for (ro, co, ml, mr, lb, c0) in fills:
+            Th[ro:ro + ml, co:co + mr] = S.block_view(psi.data, psi.rp, lb)[:, c0:c0 + mr]
+        U, sv, Vt = np.linalg.svd(Th, full_matrices=False)
+        svds[mc] = (U, sv, Vt, rows, cols)
+    kept, bond, tw = _truncate({mc: v[1] for mc, v in svds.items()}, m, cutoff)
     A = S.SiteTensor(phys1, left, bond)
     B = S.SiteTensor(phys2, bond, right)
     bpos = {c: i for i, (c, _) in enumerate(bond)}
@@ -146,6 +174,114 @@ def split(psi: S.SiteTensor, phys1, phys2, offs, m: int, cutoff: float, left_to_
             S.block_view(B.data, B.rp, bpos[mc])[:, c0:c0 + mr] = Vk[:, co:co + mr]
             co += mr
     return SplitResult(A, B, tw, bond)
+
+
+class DeviceSplitPlan:
+    """Host-side part of the device split: the layout of Theta, U, s and V^T in
+    device workspaces and the gather copies from psi (no device work here)."""
+
+    def __init__(self, psi: S.SiteTensor, phys1, phys2, offs):
+        self.psi, self.phys1, self.phys2 = psi, phys1, phys2
+        self.blocks = _mid_blocks(psi, phys1, phys2, offs)
+        self.order = sorted(self.blocks)
+        self.th_off, self.u_off, self.s_off, self.vt_off = {}, {}, {}, {}
+        th = u = sv = vt = 0
+        for mc in self.order:
+            _, _, nr, nc, _ = self.blocks[mc]
+            k = min(nr, nc)
+            self.th_off[mc], self.u_off[mc], self.s_off[mc], self.vt_off[mc] = th, u, sv, vt
+            th += nr * nc
+            u += nr * k
+            sv += k
+            vt += k * nc
+        self.th_elems = th
+        # one workspace for U | V^T | s
+        self.vt_base, self.s_base = u, u + vt
+        self.usv_elems = u + vt + sv
+        rp = psi.rp
+        rec = []
+        for mc in self.order:
+            _, _, nr, nc, fills = self.blocks[mc]
+            for (ro, co, ml, mr, lb, c0) in fills:
+                rec.append((rp.offs[lb] + c0 * rp.rows[lb], rp.rows[lb], self.th_off[mc] + ro + co * nr, nr, ml, mr,
+                            0, 0))
+        self.gather = E.copy_records(rec)
+
+    def svals(self, s_host: np.ndarray) -> dict:
+        out = {}
+        for mc in self.order:
+            _, _, nr, nc, _ = self.blocks[mc]
+            o = self.s_off[mc]
+            out[mc] = s_host[o:o + min(nr, nc)]
+        return out
+
+    def scatter(self, kept: dict, bond, right, left_to_right: bool):
+        """Site tensors of the new bond and the copies that fill them from the
+        U | V^T | s workspace: A right-paired at 0, A left-paired at a_lp, B
+        right-paired at b0 of one output buffer."""
+        psi, phys1, phys2 = self.psi, self.phys1, self.phys2
+        A = S.SiteTensor(phys1, psi.left, bond)
+        B = S.SiteTensor(phys2, bond, right)
+        lp = S.left_paired_layout(phys1, psi.left, bond)
+        a_lp, b0 = A.rp.total, A.rp.total + lp.total
+        lpos = {c: i for i, (c, _) in enumerate(psi.left)}
+        bpos = {c: i for i, (c, _) in enumerate(bond)}
+        u_mode = capi.SCALE_NONE if left_to_right else capi.SCALE_COLS
+        vt_mode = capi.SCALE_ROWS if left_to_right else capi.SCALE_NONE
+        rec = []
+        for mc, k in kept.items():
+            rows, cols, nr, nc, _ = self.blocks[mc]
+            k0 = min(nr, nc)
+            uo, so, vo = self.u_off[mc], self.s_base + self.s_off[mc], self.vt_base + self.vt_off[mc]
+            rb = bpos[mc]
+            ro = 0
+            for (s1, i1, lc, ml) in rows:
+                key = (lpos[lc], s1, i1)
+                if key in A.rp.sub:
+                    lb = lpos[lc]
+                    c0 = A.rp.sub[key][1]
+                    rec.append((uo + ro, nr, A.rp.offs[lb] + c0 * A.rp.rows[lb], A.rp.rows[lb], ml, k, u_mode, so))
+                    r0 = lp.sub[(rb, s1, i1)][0]
+                    rec.append((uo + ro, nr, a_lp + lp.offs[rb] + r0, lp.rows[rb], ml, k, u_mode, so))
+                ro += ml
+            co = 0
+            for (s2, i2, rc, mr) in cols:
+                c0 = B.rp.sub[(rb, s2, i2)][1]
+                rec.append((vo + co * k0, k0, b0 + B.rp.offs[rb] + c0 * B.rp.rows[rb], B.rp.rows[rb], k, mr, vt_mode,
+                            so))
+                co += mr
+        return A, B, lp, (a_lp, b0, b0 + B.rp.total), E.copy_records(rec)
+
+
+def split_device(psi_dev, psi: S.SiteTensor, phys1, phys2, offs, m: int, cutoff: float, left_to_right: bool,
+                 device: int = 0) -> SplitResult:
+    """The split of `split` with the two-site tensor on the device: Theta is
+    gathered from psi_dev, every block is decomposed by dmrgb200_block_svd, the
+    singular values alone come to the host for the truncation choice, and U,
+    S V^T (or U S, V^T) are scattered into the new site tensors on the device.
+    The site tensors are also copied to the host (SplitResult.A / .B)."""
+    import torch
+    plan = DeviceSplitPlan(psi, phys1, phys2, offs)
+    dev = psi_dev.device
+    theta = torch.zeros(max(plan.th_elems, 1), dtype=torch.float64, device=dev)
+    E.copy_blocks(plan.gather, psi_dev, theta)
+    usv = torch.empty(max(plan.usv_elems, 1), dtype=torch.float64, device=dev)
+    blocks = []
+    for mc in plan.order:
+        _, _, nr, nc, _ = plan.blocks[mc]
+        k = min(nr, nc)
+        t0, u0, s0, v0 = plan.th_off[mc], plan.u_off[mc], plan.s_base + plan.s_off[mc], plan.vt_base + plan.vt_off[mc]
+        blocks.append((nr, nc, theta[t0:t0 + nr * nc], usv[u0:u0 + nr * k], usv[s0:s0 + k], usv[v0:v0 + k * nc]))
+    E.block_svd(blocks, torch.cuda.current_stream(dev).cuda_stream)
+    s_host = usv[plan.s_base:plan.s_base + (plan.usv_elems - plan.s_base)].cpu().numpy()
+    kept, bond, tw = _truncate(plan.svals(s_host), m, cutoff)
+    A, B, lp, (a_lp, b0, end), copies = plan.scatter(kept, bond, psi.right, left_to_right)
+    out = torch.zeros(max(end, 1), dtype=torch.float64, device=dev)
+    E.copy_blocks(copies, usv, out, usv)
+    host = out.cpu().numpy()
+    A.data = host[:a_lp].copy()
+    B.data = host[b0:end].copy()
+    return SplitResult(A, B, tw, bond, dev_A=out[:a_lp], dev_A_lp=out[a_lp:b0], dev_B=out[b0:end])
 
 
 def right_canonicalize(tensors):
@@ -251,17 +387,20 @@ class DeviceBackend:
         idx = E.edge_bindex(symm, index)
         return idx, E.to_device(idx.edge_values(), self.ctx.device)
 
-    def _step(self, left, model, W, idx, buf, t: S.SiteTensor):
+    def _step(self, left, model, W, idx, buf, t: S.SiteTensor, dev_rp=None, dev_lp=None):
+        """One boundary step; dev_rp / dev_lp are device copies of t (right- and
+        left-paired) when the split left them on the device."""
         dev = self.ctx.device
         t0 = time.perf_counter()
         if left:
             sched, nidx = E.schedule_left_step(model.phys, t.left, t.right, W, idx, True)
             plan = E.DevicePlan(self.ctx, sched.plan, left_addr=idx.cohort_addresses(buf.data_ptr()))
-            ket, bra = E.to_device(t.data, dev), E.to_device(t.left_paired(), dev)
+            ket = dev_rp if dev_rp is not None else E.to_device(t.data, dev)
+            bra = dev_lp if dev_lp is not None else E.to_device(t.left_paired(), dev)
         else:
             sched, nidx = E.schedule_right_step(model.phys, t.left, t.right, W, idx, True)
             plan = E.DevicePlan(self.ctx, sched.plan, other_addr=idx.cohort_addresses(buf.data_ptr()))
-            ket = bra = E.to_device(t.data, dev)
+            ket = bra = dev_rp if dev_rp is not None else E.to_device(t.data, dev)
         out = self.torch.zeros(max(nidx.n_elems, 1), dtype=self.torch.float64, device=buf.device)
         t1 = time.perf_counter()
         plan.step(ket.data_ptr(), bra.data_ptr(), nidx.cohort_addresses(out.data_ptr()))
@@ -274,13 +413,15 @@ class DeviceBackend:
         ph["step_destroy"] = ph.get("step_destroy", 0.0) + t3 - t2
         return nidx, out
 
-    def left_step(self, model, W, Lidx, Lbuf, t: S.SiteTensor):
-        return self._step(True, model, W, Lidx, Lbuf, t)
+    def left_step(self, model, W, Lidx, Lbuf, t: S.SiteTensor, dev_rp=None, dev_lp=None):
+        return self._step(True, model, W, Lidx, Lbuf, t, dev_rp, dev_lp)
 
-    def right_step(self, model, W, Ridx, Rbuf, t: S.SiteTensor):
-        return self._step(False, model, W, Ridx, Rbuf, t)
+    def right_step(self, model, W, Ridx, Rbuf, t: S.SiteTensor, dev_rp=None):
+        return self._step(False, model, W, Ridx, Rbuf, t, dev_rp)
 
-    def solve(self, p12, psi: S.SiteTensor, W12, Lidx, Lbuf, Ridx, Rbuf, tol, max_iter):
+    def solve(self, p12, psi: S.SiteTensor, W12, Lidx, Lbuf, Ridx, Rbuf, tol, max_iter, keep_on_device=False):
+        """Lowest eigenpair of the site problem; the eigenvector comes back as a
+        host array, or as the device tensor with keep_on_device."""
         t0 = time.perf_counter()
         sched = E.schedule_hpsi(p12, psi.left, psi.right, W12, Lidx, Ridx)
         t1 = time.perf_counter()
@@ -290,7 +431,7 @@ class DeviceBackend:
         xd = E.to_device(psi.data, self.ctx.device)
         xo = self.torch.zeros_like(xd)
         energy, st = plan.solve(xd.data_ptr(), xo.data_ptr(), xd.numel(), tol=tol, max_iter=max_iter)
-        out = xo.cpu().numpy()
+        out = xo if keep_on_device else xo.cpu().numpy()
         t3 = time.perf_counter()
         del plan
         t4 = time.perf_counter()
@@ -306,8 +447,11 @@ class DeviceBackend:
 
 class TwoSiteDMRG:
     def __init__(self, backend, model: M.Model, tensors, m: int, cutoff: float = 1e-16, jd_tol: float = 1e-8,
-                 jd_maxiter: int = 8):
+                 jd_maxiter: int = 8, device_split: bool = False):
+        """device_split: split the optimised two-site tensor on the device
+        (split_device; needs a DeviceBackend) instead of by host SVDs."""
         self.be, self.model, self.m, self.cutoff = backend, model, m, cutoff
+        self.device_split = device_split
         self.jd_tol, self.jd_maxiter = jd_tol, jd_maxiter
         self.L = len(tensors)
         self.A = right_canonicalize(tensors)
@@ -325,32 +469,38 @@ class TwoSiteDMRG:
             self._right_step(j)
         self.log = SweepLog()
 
-    def _left_step(self, j):
+    def _left_step(self, j, dev=None):
         self.Lidx[j + 1], self.Lbuf[j + 1] = self.be.left_step(self.model, self.W[j], self.Lidx[j], self.Lbuf[j],
-                                                               self.A[j])
+                                                               self.A[j], *(dev or ()))
 
-    def _right_step(self, j):
+    def _right_step(self, j, dev=None):
         self.Ridx[j], self.Rbuf[j] = self.be.right_step(self.model, self.W[j], self.Ridx[j + 1], self.Rbuf[j + 1],
-                                                        self.A[j])
+                                                        self.A[j], *(dev or ()))
 
     def optimize_pair(self, i, left_to_right):
         ph = self.log.phase_seconds
         t0 = time.perf_counter()
         psi = twosite(self.A[i], self.A[i + 1], self.p12, self.offs)
         t1 = time.perf_counter()
+        extra = {"keep_on_device": True} if self.device_split else {}
         energy, xo, iters, ms = self.be.solve(self.p12, psi, self.W12[i], self.Lidx[i], self.Lbuf[i],
-                                              self.Ridx[i + 2], self.Rbuf[i + 2], self.jd_tol, self.jd_maxiter)
+                                              self.Ridx[i + 2], self.Rbuf[i + 2], self.jd_tol, self.jd_maxiter,
+                                              **extra)
         t2 = time.perf_counter()
         self.log.hpsi_calls += iters
         self.log.solve_ms += ms
-        psi.data = xo
-        res = split(psi, self.model.phys, self.model.phys, self.offs, self.m, self.cutoff, left_to_right)
+        if self.device_split:
+            res = split_device(xo, psi, self.model.phys, self.model.phys, self.offs, self.m, self.cutoff,
+                               left_to_right)
+        else:
+            psi.data = xo
+            res = split(psi, self.model.phys, self.model.phys, self.offs, self.m, self.cutoff, left_to_right)
         self.A[i], self.A[i + 1] = res.A, res.B
         t3 = time.perf_counter()
         if left_to_right:
-            self._left_step(i)
+            self._left_step(i, (res.dev_A, res.dev_A_lp) if res.dev_A is not None else None)
         else:
-            self._right_step(i + 1)
+            self._right_step(i + 1, (res.dev_B,) if res.dev_B is not None else None)
         t4 = time.perf_counter()
         ph["twosite"] = ph.get("twosite", 0.0) + t1 - t0
         ph["site_problem"] = ph.get("site_problem", 0.0) + t2 - t1

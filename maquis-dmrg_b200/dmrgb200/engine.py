@@ -349,3 +349,64 @@ class BatchedPlan(DevicePlan):
         capi.check(capi.lib.dmrgb200_plan_scratch_bytes(h, C.byref(s)), "plan_scratch_bytes")
         self.flops, self.scratch_bytes = f.value, s.value
         self.plan = None
+
+
+def block_svd(blocks, stream=None):
+    """Thin SVD of device blocks on the device (dmrgb200_block_svd).
+
+    `blocks` is a list of (rows, cols, a, u, s, vt): a the column-major rows x
+    cols input, u (rows x k), s (k) and vt (k x cols) the outputs, k =
+    min(rows, cols), all CUDA float64 tensors (plain device buffers; only their
+    data pointers are used).  Returns after completion."""
+    n = len(blocks)
+    rows = np.ascontiguousarray([b[0] for b in blocks], dtype=np.uint32)
+    cols = np.ascontiguousarray([b[1] for b in blocks], dtype=np.uint32)
+    arr = [(C.c_void_p * max(n, 1))(*[b[j].data_ptr() if b[j] is not None else None for b in blocks])
+           for j in range(2, 6)]
+    st = capi.lib.dmrgb200_block_svd(n, capi.ptr(rows, C.c_uint32), capi.ptr(cols, C.c_uint32), *arr,
+                                     None if stream is None else C.c_void_p(stream))
+    capi.check(st, "dmrgb200_block_svd")
+
+
+def copy_blocks(copies: np.ndarray, src, dst, scale=None, stream=None):
+    """Column-major block copies between device buffers (dmrgb200_copy_blocks).
+    `copies` is a structured array of capi.BlockCopy records (see copy_records)."""
+    n = len(copies)
+    if n == 0:
+        return
+    arr = (capi.BlockCopy * n).from_buffer_copy(np.ascontiguousarray(copies).tobytes())
+    st = capi.lib.dmrgb200_copy_blocks(n, arr, src.data_ptr(), dst.data_ptr(),
+                                       None if scale is None else scale.data_ptr(),
+                                       None if stream is None else C.c_void_p(stream))
+    capi.check(st, "dmrgb200_copy_blocks")
+
+
+COPY_DTYPE = np.dtype([("src_off", np.uint64), ("dst_off", np.uint64), ("scale_off", np.uint64),
+                       ("src_ld", np.uint32), ("dst_ld", np.uint32), ("rows", np.uint32), ("cols", np.uint32),
+                       ("scale_mode", np.uint32), ("reserved", np.uint32)])
+
+
+def copy_records(rows):
+    """Structured array of block copies from (src_off, src_ld, dst_off, dst_ld,
+    nrows, ncols, scale_mode, scale_off) tuples."""
+    out = np.zeros(len(rows), dtype=COPY_DTYPE)
+    for k, (so, sl, do, dl, r, c, mode, sco) in enumerate(rows):
+        out[k] = (so, do, sco, sl, dl, r, c, mode, 0)
+    return out
+
+
+def apply_copies(copies: np.ndarray, src: np.ndarray, dst: np.ndarray, scale: np.ndarray | None = None):
+    """The same copies on host arrays (the definition the device copies follow;
+    used to check the host-side split logic without a GPU)."""
+    for c in copies:
+        r, n = int(c["rows"]), int(c["cols"])
+        if r == 0 or n == 0:
+            continue
+        so, sl, do, dl = int(c["src_off"]), int(c["src_ld"]), int(c["dst_off"]), int(c["dst_ld"])
+        blk = np.stack([src[so + j * sl: so + j * sl + r] for j in range(n)], axis=1)
+        if c["scale_mode"] == capi.SCALE_ROWS:
+            blk = blk * scale[int(c["scale_off"]): int(c["scale_off"]) + r, None]
+        elif c["scale_mode"] == capi.SCALE_COLS:
+            blk = blk * scale[None, int(c["scale_off"]): int(c["scale_off"]) + n]
+        for j in range(n):
+            dst[do + j * dl: do + j * dl + r] = blk[:, j]

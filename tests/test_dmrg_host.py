@@ -75,3 +75,48 @@ def test_truncation_keeps_largest_states():
     res = G.split(psi, model.phys, model.phys, offs, 5, 0.0, True)
     assert sum(k for _, k in res.bond) == 5
     assert 0.0 < res.truncated_weight < 1.0
+
+
+def _device_split_on_host(psi, phys, offs, m, cutoff, l2r):
+    """The device split's host logic (DeviceSplitPlan) with the device work
+    replaced by its host definitions: block copies by engine.apply_copies and the
+    block SVDs by numpy, in the workspaces the device path uses."""
+    from dmrgb200 import engine as E
+    plan = G.DeviceSplitPlan(psi, phys, phys, offs)
+    theta = np.zeros(max(plan.th_elems, 1))
+    E.apply_copies(plan.gather, psi.data, theta)
+    usv = np.zeros(max(plan.usv_elems, 1))
+    for mc in plan.order:
+        _, _, nr, nc, _ = plan.blocks[mc]
+        k = min(nr, nc)
+        t0 = plan.th_off[mc]
+        U, sv, Vt = np.linalg.svd(theta[t0:t0 + nr * nc].reshape(nc, nr).T, full_matrices=False)
+        usv[plan.u_off[mc]:plan.u_off[mc] + nr * k] = U.T.reshape(-1)
+        usv[plan.vt_base + plan.vt_off[mc]:plan.vt_base + plan.vt_off[mc] + k * nc] = Vt.T.reshape(-1)
+        usv[plan.s_base + plan.s_off[mc]:plan.s_base + plan.s_off[mc] + k] = sv
+    kept, bond, tw = G._truncate(plan.svals(usv[plan.s_base:]), m, cutoff)
+    A, B, lp, (a_lp, b0, end), copies = plan.scatter(kept, bond, psi.right, l2r)
+    out = np.zeros(max(end, 1))
+    E.apply_copies(copies, usv, out, usv)
+    return A, B, out[:a_lp], out[a_lp:b0], out[b0:end], tw, bond
+
+
+@pytest.mark.parametrize("name,m", [("heisenberg", 10 ** 6), ("hubbard", 10 ** 6), ("hubbard", 7), ("bose", 3)])
+def test_device_split_plan_matches_host_split(name, m):
+    """Gather, truncation and scatter of the device split reproduce the host
+    split bitwise when the block SVDs agree (both numpy here)."""
+    L = 5
+    model = {"heisenberg": M.heisenberg(L), "hubbard": M.fermi_hubbard(L, n_up=2, n_down=2),
+             "bose": M.bose_hubbard(L, N=2)}[name]
+    rng = np.random.default_rng(3)
+    bonds = S.allowed_sectors(model.phys, L, model.total_charge, 6)
+    A = S.random_mps(model.phys, bonds, rng)
+    p12, offs = M.fuse_phys(model.phys, model.phys)
+    psi = G.twosite(A[1], A[2], p12, offs)
+    for l2r in (True, False):
+        ref = G.split(psi, model.phys, model.phys, offs, m, 1e-16, l2r)
+        a, b, a_rp, a_lp, b_rp, tw, bond = _device_split_on_host(psi, model.phys, offs, m, 1e-16, l2r)
+        assert bond == ref.bond and tw == ref.truncated_weight
+        assert np.array_equal(a_rp, ref.A.data)
+        assert np.array_equal(a_lp, ref.A.left_paired())
+        assert np.array_equal(b_rp, ref.B.data)

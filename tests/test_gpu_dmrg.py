@@ -61,3 +61,23 @@ def test_device_sweep_matches_oracle_sweep():
     ed = np.array([e[2] for e in dev.log.energies])
     ec = np.array([e[2] for e in cpu.log.energies])
     assert np.max(np.abs(ed - ec)) <= 1e-9
+
+
+def test_device_split_sweeps():
+    """Sweeps whose splits run on the device (split_device): the Bose-Hubbard
+    known answer with truncation to m=200, and the same energies as the sweeps
+    with host SVDs within 1e-8."""
+    model = M.bose_hubbard(10, t=1.0, U=8.0, Nmax=2, N=5)
+    res = {}
+    for dsplit in (False, True):
+        rng = np.random.default_rng(1)
+        bonds = S.allowed_sectors(model.phys, 10, model.total_charge, 5)
+        A = S.random_mps(model.phys, bonds, rng)
+        opt = G.TwoSiteDMRG(G.DeviceBackend(E.Context(0)), model, A, 200, cutoff=1e-16, jd_tol=1e-10, jd_maxiter=16,
+                            device_split=dsplit)
+        for s in range(5):
+            e = opt.sweep(s)
+        res[dsplit] = e
+    assert abs(res[True] - E_BH_REFERENCE) <= 1e-3
+    assert abs(res[True] - res[False]) <= 1e-8
+    assert abs(res[True] - D.ground_energy(model, 10)) <= 1e-8

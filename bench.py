@@ -278,6 +278,71 @@ def sweep_workload(args):
     print(json.dumps(line), flush=True)
 
 
+def split_workload(args):
+    """Two-site split of the middle Hubbard L=64 m=1024 two-site tensor (TwoSiteTensor::
+    split_mps_l2r, truncation to m=1024, cutoff 1e-16): the device split (gather, block
+    Jacobi SVD, singular values to the host, truncation choice, scatter, site tensors
+    back to the host) against the host split (numpy LAPACK SVDs, one thread per the
+    numpy build's defaults), wall time per split; one JSON line."""
+    import torch
+    from dmrgb200 import dmrg as G
+    from dmrgb200 import engine as E
+    from dmrgb200 import models as M
+
+    model, bonds, tensors, i, psi = build_workload()
+    p12, offs = M.fuse_phys(model.phys, model.phys)
+    ctx = E.Context(0)
+    xd = E.to_device(psi.data, ctx.device)
+    plan = G.DeviceSplitPlan(psi, model.phys, model.phys, offs)
+    shapes = [(plan.blocks[mc][2], plan.blocks[mc][3]) for mc in plan.order]
+    for _ in range(2):
+        G.split_device(xd, psi, model.phys, model.phys, offs, M_BOND, 1e-16, True)
+    torch.cuda.synchronize()
+    dev_s = []
+    for _ in range(max(1, min(args.steps, 10))):
+        t0 = time.perf_counter()
+        got = G.split_device(xd, psi, model.phys, model.phys, offs, M_BOND, 1e-16, True)
+        dev_s.append(time.perf_counter() - t0)
+    # the block SVD launch alone (CUDA events; includes its table upload and the synchronisation)
+    theta = torch.zeros(max(plan.th_elems, 1), dtype=torch.float64, device=xd.device)
+    E.copy_blocks(plan.gather, xd, theta)
+    usv = torch.empty(max(plan.usv_elems, 1), dtype=torch.float64, device=xd.device)
+    blocks = []
+    for mc in plan.order:
+        _, _, nr, nc, _ = plan.blocks[mc]
+        k = min(nr, nc)
+        t0_, u0, s0, v0 = plan.th_off[mc], plan.u_off[mc], plan.s_base + plan.s_off[mc], plan.vt_base + plan.vt_off[mc]
+        blocks.append((nr, nc, theta[t0_:t0_ + nr * nc], usv[u0:u0 + nr * k], usv[s0:s0 + k], usv[v0:v0 + k * nc]))
+    svd_ms = []
+    stream = torch.cuda.current_stream()
+    for _ in range(3):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        E.block_svd(blocks, stream.cuda_stream)
+        b.record(stream)
+        b.synchronize()
+        svd_ms.append(a.elapsed_time(b))
+    host_s = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        ref = G.split(psi, model.phys, model.phys, offs, M_BOND, 1e-16, True)
+        host_s.append(time.perf_counter() - t0)
+    t_ref = G.twosite(ref.A, ref.B, p12, offs).data
+    t_got = G.twosite(got.A, got.B, p12, offs).data
+    line = {"metric": "two-site split time (ms)", "value": 1e3 * statistics.mean(dev_s), "unit": "ms",
+            "higher_is_better": False, "n_gpus": 1, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "hubbard_L64_twou1_m1024_twosite_split_middle", "sites": L_SITES, "bond_dim": M_BOND,
+                       "psi_elements": int(psi.data.size), "blocks": len(shapes),
+                       "largest_block": list(max(shapes, key=lambda t: t[0] * t[1])) if shapes else None},
+            "device_split_ms": [1e3 * t for t in dev_s], "block_svd_kernel_ms": svd_ms,
+            "host_split_ms": [1e3 * t for t in host_s],
+            "kept_states": sum(k for _, k in got.bond), "bond_equal": got.bond == ref.bond,
+            "truncated_weight": got.truncated_weight,
+            "truncated_weight_diff": abs(got.truncated_weight - ref.truncated_weight),
+            "rel_diff_kept_twosite_vs_host": float(np.linalg.norm(t_got - t_ref) / np.linalg.norm(t_ref))}
+    print(json.dumps(line), flush=True)
+
+
 def solve_workload(args):
     """Jacobi-Davidson solves of the Hubbard L=64 m=1024 site problem (8 iterations each, tol 0 so
     that every iteration runs), graph-captured and stepwise; one JSON line."""
@@ -611,13 +676,14 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--workload", default="hpsi",
-                    choices=["hpsi", "sweep", "batched", "solve", "gemm", "qc", "adjoint", "steps"],
+                    choices=["hpsi", "sweep", "batched", "solve", "gemm", "qc", "adjoint", "steps", "split"],
                     help="hpsi: the headline H·psi line (default); sweep: Heisenberg L=32 sweeps; batched: 64 "
                          "instances in one plan; solve: Jacobi-Davidson solves of the Hubbard L=64 site problem; "
                          "gemm: the DMMA kernel on "
                          "a regular 4096^3 GEMM; qc: a quantum-chemistry site problem; adjoint: the adjoint "
                          "checked by finite differences and RDM elements on a quantum-chemistry site problem; "
-                         "steps: the left and right boundary steps at the middle of the Hubbard chain")
+                         "steps: the left and right boundary steps at the middle of the Hubbard chain; split: the "
+                         "two-site split of the middle Hubbard tensor on the device and on the host")
     ap.add_argument("--split", default="host", choices=["host", "device"],
                     help="where the sweep workload splits the two-site tensor")
     ap.add_argument("--qc-sites", type=int, default=24, help="orbitals of the qc workload")
@@ -633,6 +699,9 @@ def main():
 
     if args.workload == "sweep":
         sweep_workload(args)
+        os._exit(0)
+    if args.workload == "split":
+        split_workload(args)
         os._exit(0)
     if args.workload == "batched":
         batched_workload(args)

@@ -7,7 +7,7 @@
 // 95-113; svd_truncate: :185-298; TwoSiteTensor::split_mps_l2r / r2l:
 // mp_tensors/twositetensor.hpp:153-200).
 //
-// block_svd_jacobi: one CTA of 32 warps per block, one-sided (Hestenes) Jacobi.  The block is
+// block_svd_jacobi: one CTA of 16 warps per block, one-sided (Hestenes) Jacobi.  The block is
 // taken as m x n columns with n = min(rows, cols) (the transpose when rows < cols).
 // Column pairs are orthogonalised in round-robin order, n/2 disjoint pairs per
 // round spread over the warps; a pair rotates when |g_p . g_q| > tol |g_p| |g_q|
@@ -38,7 +38,8 @@ dmrgb200_status noalloc_fail(dmrgb200_status s, std::string const& msg);
 
 namespace {
 
-constexpr int SVD_THREADS = 1024, SVD_WARPS = SVD_THREADS / 32, SVD_MAX_SWEEPS = 60;
+constexpr int SVD_THREADS = 512, SVD_WARPS = SVD_THREADS / 32, SVD_MAX_SWEEPS = 60;
+constexpr int SVD_REG = 8;  // register path for columns of up to 32 * SVD_REG elements
 constexpr size_t SVD_SMEM_LIMIT = 200 * 1024;
 
 struct SvdBlock {
@@ -60,6 +61,98 @@ __device__ inline double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
+}
+
+// Rutishauser's rotation of columns p, q from their squared norms al, be and
+// inner product ga: t the smaller root of t^2 + 2 zeta t - 1 = 0.  Returns false
+// when the pair is already orthogonal to tol.
+__device__ inline bool jacobi_cs(double al, double be, double ga, double tol, double& c, double& s) {
+    if (ga == 0.0 || !(fabs(ga) > tol * sqrt(al) * sqrt(be))) return false;
+    const double zeta = (be - al) / (2.0 * ga);
+    const double az = fabs(zeta);
+    const double t = (az > 1e150) ? 0.5 / zeta : copysign(1.0, zeta) / (az + sqrt(1.0 + zeta * zeta));
+    c = 1.0 / sqrt(1.0 + t * t);
+    s = c * t;
+    return true;
+}
+
+// One pair, columns of up to 32 * SVD_REG elements: every lane loads its
+// elements of both columns in one unrolled batch (one memory latency instead of
+// one per element), and the same for V when the pair rotates.
+__device__ inline bool pair_rotate_regs(double* gp, double* gq, uint32_t m, double* vp, double* vq, uint32_t n,
+                                        double tol) {
+    const uint32_t lane = threadIdx.x & 31u;
+    double x[SVD_REG], y[SVD_REG];
+#pragma unroll
+    for (int r = 0; r < SVD_REG; ++r) {
+        const uint32_t i = lane + 32u * r;
+        x[r] = i < m ? gp[i] : 0.0;
+        y[r] = i < m ? gq[i] : 0.0;
+    }
+    double al = 0.0, be = 0.0, ga = 0.0;
+#pragma unroll
+    for (int r = 0; r < SVD_REG; ++r) {
+        al = fma(x[r], x[r], al);
+        be = fma(y[r], y[r], be);
+        ga = fma(x[r], y[r], ga);
+    }
+    al = warp_sum(al);
+    be = warp_sum(be);
+    ga = warp_sum(ga);
+    double c, s;
+    if (!jacobi_cs(al, be, ga, tol, c, s)) return false;
+#pragma unroll
+    for (int r = 0; r < SVD_REG; ++r) {
+        const uint32_t i = lane + 32u * r;
+        if (i < m) {
+            gp[i] = c * x[r] - s * y[r];
+            gq[i] = s * x[r] + c * y[r];
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < SVD_REG; ++r) {
+        const uint32_t i = lane + 32u * r;
+        x[r] = i < n ? vp[i] : 0.0;
+        y[r] = i < n ? vq[i] : 0.0;
+    }
+#pragma unroll
+    for (int r = 0; r < SVD_REG; ++r) {
+        const uint32_t i = lane + 32u * r;
+        if (i < n) {
+            vp[i] = c * x[r] - s * y[r];
+            vq[i] = s * x[r] + c * y[r];
+        }
+    }
+    return true;
+}
+
+// The same for longer columns, element by element.
+__device__ inline bool pair_rotate_loop(double* gp, double* gq, uint32_t m, double* vp, double* vq, uint32_t n,
+                                        double tol) {
+    const uint32_t lane = threadIdx.x & 31u;
+    double al = 0.0, be = 0.0, ga = 0.0;
+    for (uint32_t i = lane; i < m; i += 32) {
+        const double x = gp[i], y = gq[i];
+        al = fma(x, x, al);
+        be = fma(y, y, be);
+        ga = fma(x, y, ga);
+    }
+    al = warp_sum(al);
+    be = warp_sum(be);
+    ga = warp_sum(ga);
+    double c, s;
+    if (!jacobi_cs(al, be, ga, tol, c, s)) return false;
+    for (uint32_t i = lane; i < m; i += 32) {
+        const double x = gp[i], y = gq[i];
+        gp[i] = c * x - s * y;
+        gq[i] = s * x + c * y;
+    }
+    for (uint32_t i = lane; i < n; i += 32) {
+        const double x = vp[i], y = vq[i];
+        vp[i] = c * x - s * y;
+        vq[i] = s * x + c * y;
+    }
+    return true;
 }
 
 __global__ void __launch_bounds__(SVD_THREADS) block_svd_jacobi(const SvdBlock* blocks, int* err) {
@@ -120,35 +213,11 @@ __global__ void __launch_bounds__(SVD_THREADS) block_svd_jacobi(const SvdBlock* 
                 }
                 double* gp = G + size_t(p) * m;
                 double* gq = G + size_t(q) * m;
-                double al = 0.0, be = 0.0, ga = 0.0;
-                for (uint32_t i = lane; i < m; i += 32) {
-                    const double x = gp[i], y = gq[i];
-                    al = fma(x, x, al);
-                    be = fma(y, y, be);
-                    ga = fma(x, y, ga);
-                }
-                al = warp_sum(al);
-                be = warp_sum(be);
-                ga = warp_sum(ga);
-                if (ga == 0.0 || !(fabs(ga) > tol * sqrt(al) * sqrt(be))) continue;
-                // Rutishauser's rotation: t the smaller root of t^2 + 2 zeta t - 1 = 0
-                const double zeta = (be - al) / (2.0 * ga);
-                const double az = fabs(zeta);
-                const double t = (az > 1e150) ? 0.5 / zeta : copysign(1.0, zeta) / (az + sqrt(1.0 + zeta * zeta));
-                const double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
-                for (uint32_t i = lane; i < m; i += 32) {
-                    const double x = gp[i], y = gq[i];
-                    gp[i] = c * x - s * y;
-                    gq[i] = s * x + c * y;
-                }
                 double* vp = V + size_t(p) * n;
                 double* vq = V + size_t(q) * n;
-                for (uint32_t i = lane; i < n; i += 32) {
-                    const double x = vp[i], y = vq[i];
-                    vp[i] = c * x - s * y;
-                    vq[i] = s * x + c * y;
-                }
-                rotated = 1;
+                const bool rot = (m <= 32u * SVD_REG) ? pair_rotate_regs(gp, gq, m, vp, vq, n, tol)
+                                                     : pair_rotate_loop(gp, gq, m, vp, vq, n, tol);
+                if (rot) rotated = 1;
             }
             __syncthreads();
         }

@@ -109,10 +109,12 @@ def clocks_summary(path, device):
             "samples": len(sm)}
 
 
-def cpu_reference(model, bonds, tensors, i, psi, seconds=15.0, threads=None):
+def cpu_reference(model, bonds, tensors, i, psi, seconds=15.0, threads=None, steps=None, warmup=1):
     """The reference's CPU execution of the same H·psi: the reference's own
     solver core (oracle/_ref, compiled from its sources) when present, else the
-    oracle's restatement of it; OpenMP over all host cores, OpenBLAS."""
+    oracle's restatement of it; OpenMP over all host cores, OpenBLAS.  With
+    `steps`, exactly that many H·psi are timed after `warmup` untimed ones;
+    otherwise H·psi repeat for about `seconds` (at most 2000)."""
     import oracle as O
     import ref as REF
     from dmrgb200 import engine as E
@@ -141,13 +143,14 @@ def cpu_reference(model, bonds, tensors, i, psi, seconds=15.0, threads=None):
     p12, _ = M.fuse_phys(model.phys, model.phys)
     W12 = M.MPOHandle(M.twosite_mpo(model.mpo[i], model.mpo[i + 1], model.phys, model.phys), model.symm)
     sch = E.schedule_hpsi(p12, bonds[i], bonds[i + 2], W12, Lidx, Ridx)
-    run(sch.plan, Lval, Lidx, Rval, Ridx, psi.data)  # warm-up
+    for _ in range(max(1, warmup)):
+        run(sch.plan, Lval, Lidx, Rval, Ridx, psi.data)
     n, t0 = 0, time.perf_counter()
     while True:
         y = run(sch.plan, Lval, Lidx, Rval, Ridx, psi.data)
         n += 1
         el = time.perf_counter() - t0
-        if el >= seconds or n >= 2000:
+        if (steps is not None and n >= steps) or (steps is None and (el >= seconds or n >= 2000)):
             break
     return {"gflops": sch.flops * n / el / 1e9, "calls": n, "seconds": el, "threads": threads,
             "flops": sch.flops, "y": y, "kind": kind,
@@ -730,18 +733,19 @@ def main():
         if rank != 0:
             return
         model, bonds, tensors, i, psi = build_workload()
-        res = cpu_reference(model, bonds, tensors, i, psi, seconds=max(2.0, args.cpu_seconds))
+        # a step is one H·psi of the whole workload on the host cores (about 2.5 ms on 16 threads)
+        res = cpu_reference(model, bonds, tensors, i, psi, steps=args.steps, warmup=args.warmup)
         per = res["seconds"] / res["calls"]
         line = {"metric": METRIC, "value": res["gflops"], "unit": "GFLOP/s", "n_gpus": args.gpus,
-                "steps": res["calls"], "warmup": 1, "ms_per_step": per * 1e3, "higher_is_better": True,
+                "steps": res["calls"], "warmup": args.warmup, "ms_per_step": per * 1e3, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "impl": "reference",
                 "config": {"workload": WORKLOAD, "sites": L_SITES, "bond_dim": M_BOND, "symmetry": "TwoU1",
                            "parallelism": "cpu"},
                 "cpu_baseline": {"value": res["gflops"], "unit": "GFLOP/s", "cores": res["threads"],
                                  "kind": res["kind"],
-                                 "sample": f"{res['calls']} H·psi of the full workload in {res['seconds']:.1f} s "
-                                           f"({res['what']})"},
+                                 "sample": f"{res['calls']} H·psi of the full workload in {res['seconds']:.2f} s "
+                                           f"after {args.warmup} untimed ({res['what']})"},
                 "e2e": {"value": res["gflops"], "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         # the reference library's static timers print at exit; keep stdout to the one JSON line

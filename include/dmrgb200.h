@@ -332,7 +332,9 @@ typedef struct {
  * Theta and the scatter of U, S V^T (or U S, V^T) into the site tensors
  * (TwoSiteTensor::split_mps_l2r / split_mps_r2l,
  * dmrg/framework/dmrg/mp_tensors/twositetensor.hpp:153-200).  `copies` is a host
- * array; destinations must not overlap.  Stream-ordered, asynchronous. */
+ * array that may be released on return; destinations must not overlap; the
+ * offsets are not checked against the buffers.  Stream-ordered; the upload of
+ * the descriptors from pageable memory may first wait for the stream. */
 dmrgb200_status dmrgb200_copy_blocks(uint32_t n, const dmrgb200_block_copy* copies, const double* src, double* dst,
                                      const double* scale, void* cuda_stream);
 

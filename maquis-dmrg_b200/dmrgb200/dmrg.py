@@ -263,8 +263,9 @@ def split_device(psi_dev, psi: S.SiteTensor, phys1, phys2, offs, m: int, cutoff:
     import torch
     plan = DeviceSplitPlan(psi, phys1, phys2, offs)
     dev = psi_dev.device
+    sh = torch.cuda.current_stream(dev).cuda_stream  # every step of the split on torch's current stream
     theta = torch.zeros(max(plan.th_elems, 1), dtype=torch.float64, device=dev)
-    E.copy_blocks(plan.gather, psi_dev, theta)
+    E.copy_blocks(plan.gather, psi_dev, theta, stream=sh)
     usv = torch.empty(max(plan.usv_elems, 1), dtype=torch.float64, device=dev)
     blocks = []
     for mc in plan.order:
@@ -272,12 +273,12 @@ def split_device(psi_dev, psi: S.SiteTensor, phys1, phys2, offs, m: int, cutoff:
         k = min(nr, nc)
         t0, u0, s0, v0 = plan.th_off[mc], plan.u_off[mc], plan.s_base + plan.s_off[mc], plan.vt_base + plan.vt_off[mc]
         blocks.append((nr, nc, theta[t0:t0 + nr * nc], usv[u0:u0 + nr * k], usv[s0:s0 + k], usv[v0:v0 + k * nc]))
-    E.block_svd(blocks, torch.cuda.current_stream(dev).cuda_stream)
+    E.block_svd(blocks, sh)
     s_host = usv[plan.s_base:plan.s_base + (plan.usv_elems - plan.s_base)].cpu().numpy()
     kept, bond, tw = _truncate(plan.svals(s_host), m, cutoff)
     A, B, lp, (a_lp, b0, end), copies = plan.scatter(kept, bond, psi.right, left_to_right)
     out = torch.zeros(max(end, 1), dtype=torch.float64, device=dev)
-    E.copy_blocks(copies, usv, out, usv)
+    E.copy_blocks(copies, usv, out, usv, stream=sh)
     host = out.cpu().numpy()
     A.data = host[:a_lp].copy()
     B.data = host[b0:end].copy()

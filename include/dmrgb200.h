@@ -17,7 +17,7 @@
  *  (1) dmrgb200_plan_create(): the caller flattens its own schedule
  *      (the reference's ScheduleNew / MPSBlock / Cohort) into
  *      dmrgb200_plan_desc.  This is the drop-in seam for the reference's
- *      C++ host code; see INTEGRATION.md.
+ *      C++ host code.
  *  (2) dmrgb200_*_plan_build(): the library's own schedule builder (a C++
  *      restatement of the reference's create_contraction_schedule and the
  *      lshtm_* / rshtm_* builders) from index, MPO and boundary descriptions.
@@ -379,11 +379,16 @@ dmrgb200_status dmrgb200_plan_set_solver(dmrgb200_plan_t plan, int mode);
  * the library holds until the process exits.  The call allocates no device
  * memory.  Plans needing more than that return DMRGB200_OUT_OF_MEMORY with a
  * message giving the required size.  The first call on a device looks up the
- * array's device address (cudaGetSymbolAddress) with that device current; make
- * that first call before any stream capture.  All calls share the one array
- * (it keeps the last call's contents; nothing in it needs to start at zero), so
- * calls whose executions overlap on the GPU race: serialise them, e.g. on one
- * stream.  The call returns after its work on `cuda_stream` has finished. */
+ * array's device address (cudaGetSymbolAddress) with that device current; under
+ * CUDA's lazy module loading (the default since CUDA 12.2) that lookup is also
+ * when the array is placed in device memory, so the first call on a device
+ * needs DMRGB200_NOALLOC_BYTES of free device memory (DMRGB200_OUT_OF_MEMORY
+ * otherwise): make it before a pool or allocator takes the memory.  All calls
+ * share the one array (it keeps the last call's contents; nothing in it needs
+ * to start at zero), so calls whose executions overlap on the GPU race:
+ * serialise them, e.g. on one stream.  The call copies its tables from host
+ * memory and synchronises `cuda_stream` before returning, so it must not be
+ * made while that stream is being captured. */
 #define DMRGB200_NOALLOC_BYTES (64ull << 20)
 dmrgb200_status dmrgb200_hpsi_noalloc(const dmrgb200_plan_desc* desc, const dmrgb200_boundary_view* left,
                                       const dmrgb200_boundary_view* right, const double* x, double* y,

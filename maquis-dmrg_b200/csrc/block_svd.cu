@@ -31,6 +31,7 @@
 #include <vector>
 
 #include "../../include/dmrgb200.h"
+#include "device.hpp"
 
 namespace dmrgb200 {
 
@@ -320,10 +321,10 @@ extern "C" dmrgb200_status dmrgb200_block_svd(uint32_t n_blocks, const uint32_t*
     double* scratch = reinterpret_cast<double*>(mem + tab + 256);
     for (size_t i = 0; i < bl.size(); ++i)
         if (work_off[i] != SIZE_MAX) bl[i].work = scratch + work_off[i];
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(block_svd_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SVD_SMEM_LIMIT));
-        attr = true;
+    e = ensure_smem_limit(reinterpret_cast<const void*>(block_svd_jacobi), int(SVD_SMEM_LIMIT));
+    if (e != cudaSuccess) {
+        cudaFreeAsync(mem, st);
+        return noalloc_fail(DMRGB200_DEVICE_ERROR, std::string("block SVD shared memory: ") + cudaGetErrorString(e));
     }
     cudaMemcpyAsync(mem, bl.data(), bl.size() * sizeof(SvdBlock), cudaMemcpyHostToDevice, st);
     cudaMemsetAsync(d_err, 0, sizeof(int), st);
@@ -355,7 +356,10 @@ extern "C" dmrgb200_status dmrgb200_copy_blocks(uint32_t n, const dmrgb200_block
     void* d = nullptr;
     cudaError_t e = cudaMallocAsync(&d, size_t(n) * sizeof(dmrgb200_block_copy), st);
     if (e != cudaSuccess) return noalloc_fail(DMRGB200_OUT_OF_MEMORY, std::string("block copy: ") + cudaGetErrorString(e));
-    cudaMemcpyAsync(d, copies, size_t(n) * sizeof(dmrgb200_block_copy), cudaMemcpyHostToDevice, st);
+    // upload from a pageable copy: a pageable source is staged before cudaMemcpyAsync
+    // returns, so the caller's array (pinned or not) may be released on return
+    std::vector<dmrgb200_block_copy> staged(copies, copies + n);
+    cudaMemcpyAsync(d, staged.data(), size_t(n) * sizeof(dmrgb200_block_copy), cudaMemcpyHostToDevice, st);
     copy_blocks<<<std::min<uint32_t>(n, 148u * 8u), 256, 0, st>>>(static_cast<const dmrgb200_block_copy*>(d), n, src,
                                                                    dst, scale);
     e = cudaGetLastError();

@@ -5,7 +5,10 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
+#include <set>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "plan.hpp"
@@ -323,5 +326,21 @@ int oz_timed_out(OzProgram const* oz, void* scratch, int s, cudaStream_t st);
 double calibrate_fp64_tflops();
 // solver graph cache of a plan (jd_graph.cu)
 void jd_graph_free(void* g);
+
+// Raise a kernel's dynamic shared-memory limit once per (device, kernel): the
+// attribute belongs to the kernel on the current device, so a process-wide flag
+// would skip it on a second device.  Thread-safe.
+inline cudaError_t ensure_smem_limit(const void* kernel, int bytes) {
+    static std::mutex mu;
+    static std::set<std::pair<int, const void*>> done;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    if (done.count({dev, kernel})) return cudaSuccess;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) done.insert({dev, kernel});
+    return e;
+}
 
 }  // namespace dmrgb200

@@ -1386,10 +1386,8 @@ cudaError_t run_sbuild(DeviceProgram const& prog, double* T, double* S, cudaStre
         if (e != cudaSuccess) return e;
     }
     if (prog.n_gitems) {
-        static const bool smem_ok =
-            cudaFuncSetAttribute(sbuild_groups, cudaFuncAttributeMaxDynamicSharedMemorySize, int(SGB_SMEM)) ==
-            cudaSuccess;
-        if (!smem_ok) return cudaErrorInvalidConfiguration;
+        cudaError_t ea = ensure_smem_limit(reinterpret_cast<const void*>(sbuild_groups), int(SGB_SMEM));
+        if (ea != cudaSuccess) return ea;
         // SGB_WARPS warps per CTA, SGB_MINB CTAs per SM resident
         uint32_t grid = std::min<uint32_t>((prog.n_gitems + SGB_WARPS - 1) / SGB_WARPS, sms * SGB_MINB);
         cudaError_t e = launch_pdl(sbuild_groups, grid, 32 * SGB_WARPS, SGB_SMEM, stream,

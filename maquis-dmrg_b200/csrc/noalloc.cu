@@ -10,6 +10,13 @@
 // and line tables and the T / S intermediates -- in one file-scope device array
 // of fixed size, DMRGB200_NOALLOC_BYTES, that every GPU loading the library
 // holds until the process exits.
+//
+// With CUDA's lazy module loading (the default since CUDA 12.2) the array is
+// placed in device memory when its module is loaded on a device, which happens
+// at the first cudaGetSymbolAddress below, i.e. on the first call on that
+// device.  That first call therefore needs DMRGB200_NOALLOC_BYTES of free
+// device memory: make it (with any plan that fits) before a pool or allocator
+// takes the memory.  A failed placement is reported as DMRGB200_OUT_OF_MEMORY.
 #include <cuda_runtime.h>
 
 #include <cstring>
@@ -48,6 +55,12 @@ dmrgb200_status scratch_address(void** out) {
     if (!g_scratch_ptr[dev]) {
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e == cudaErrorMemoryAllocation) {
+            cudaGetLastError();  // reset the runtime's last-error state
+            return noalloc_fail(DMRGB200_OUT_OF_MEMORY,
+                                "placing the static scratch of dmrgb200_hpsi_noalloc (" +
+                                    std::to_string(kScratchBytes) + " bytes) on this device failed: out of memory");
+        }
         if (e != cudaSuccess || !p)
             return noalloc_fail(DMRGB200_DEVICE_ERROR,
                                 std::string("cudaGetSymbolAddress of the static scratch: ") + cudaGetErrorString(e));

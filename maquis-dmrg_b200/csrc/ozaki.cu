@@ -530,12 +530,8 @@ cudaError_t oz_run(OzProgram* oz, Bases const& bs, int s, void* scratch, cudaStr
     }
     oz->const_ready = true;
     if (!oz->tiles.empty()) {
-        static bool attr = false;
-        if (!attr) {
-            cudaFuncSetAttribute(ozaki_mma, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(ozaki_smem_bytes(OZ_MAX_SLICES)));
-            attr = true;
-        }
+        cudaError_t ea = ensure_smem_limit(reinterpret_cast<const void*>(ozaki_mma), int(ozaki_smem_bytes(OZ_MAX_SLICES)));
+        if (ea != cudaSuccess) return ea;
         OzArgs args{c.A8, c.B8, oz->a_plane, oz->b_plane, c.e, oz->d_pbs, oz->d_slabs, oz->d_tiles,
                     uint32_t(oz->tiles.size()), oz_chunk_slabs(s), s, bs, c.err};
         ozaki_mma<<<std::min<uint32_t>(uint32_t(oz->tiles.size()), uint32_t(sms)), OZ_THREADS, ozaki_smem_bytes(s),

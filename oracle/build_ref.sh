@@ -6,7 +6,11 @@
 # compiled too because tasks.cpp references them; they are never called.
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
-REF="${MAQUIS_REFERENCE:-/root/reference}/dmrg/framework"
+if [ -z "${MAQUIS_REFERENCE:-}" ]; then
+  MAQUIS_REFERENCE="$(python -c 'import json, sys; print(json.load(open(sys.argv[1])).get("reference_path", ""))' "$HERE/../BASELINE.json" 2>/dev/null || true)"
+fi
+[ -n "$MAQUIS_REFERENCE" ] || { echo "set MAQUIS_REFERENCE to the reference source tree" >&2; exit 1; }
+REF="$MAQUIS_REFERENCE/dmrg/framework"
 OUT="$HERE/_ref"
 [ -d "$REF/dmrg/solver" ] || { echo "reference sources not found at $REF" >&2; exit 1; }
 mkdir -p "$OUT"

@@ -29,6 +29,10 @@ def lib():
         _lib.ref_hpsi.argtypes = [PD, C.c_uint32, u32, u32, u32, pp, C.c_uint32, pp, C.c_void_p, C.c_void_p]
         _lib.ref_left_step.argtypes = [PD, C.c_uint32, u32, u32, u32, pp, C.c_void_p, C.c_void_p, pp]
         _lib.ref_right_step.argtypes = [PD, C.c_uint32, u32, u32, u32, pp, C.c_void_p, C.c_void_p, pp]
+        _lib.ref_hpsi_create.argtypes = [PD, C.c_uint32, u32, u32, u32, pp, C.c_uint32, pp]
+        _lib.ref_hpsi_create.restype = C.c_void_p
+        _lib.ref_hpsi_run.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.ref_hpsi_destroy.argtypes = [C.c_void_p]
     return _lib
 
 
@@ -50,6 +54,33 @@ def hpsi(plan, L, Lidx, R, Ridx, x):
                         _ptrs(R, Ridx), np.ascontiguousarray(x).ctypes.data, y.ctypes.data)
     assert rc == 0
     return y
+
+
+class Hpsi:
+    """The reference's ScheduleNew for one H psi plan, built once (as the reference
+    builds one schedule per site problem) and run on many x: `run(x)` executes
+    only create_T and contract on the host cores."""
+
+    def __init__(self, plan, L, Lidx, R, Ridx):
+        self._desc, self._keep = capi.numpy_to_desc(plan)
+        self._L, self._R = L, R
+        self._ls, self._rs, self._nb = _u32(Ridx.lsize), _u32(Ridx.rsize), _u32(Ridx.nblocks)
+        self._lp, self._rp = _ptrs(L, Lidx), _ptrs(R, Ridx)
+        u = lambda a: a.ctypes.data_as(C.POINTER(C.c_uint32))
+        self.out_size = int(plan["out_size"])
+        self._h = lib().ref_hpsi_create(C.byref(self._desc), Ridx.n_cohorts, u(self._ls), u(self._rs), u(self._nb),
+                                        self._lp, Lidx.n_cohorts, self._rp)
+        assert self._h
+
+    def run(self, x, y=None):
+        y = np.zeros(self.out_size) if y is None else y
+        assert lib().ref_hpsi_run(self._h, np.ascontiguousarray(x).ctypes.data, y.ctypes.data) == 0
+        return y
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().ref_hpsi_destroy(self._h)
+            self._h = None
 
 
 def left_step(plan, L, Lidx, ket_rp, bra_lp, new_idx):

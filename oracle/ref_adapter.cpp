@@ -108,6 +108,59 @@ int ref_hpsi(const dmrgb200_plan_desc* dp, uint32_t nR, const uint32_t* R_lsz, c
     return 0;
 }
 
+// A ScheduleNew built once from a flat H psi plan and kept with its boundary
+// views, as the reference builds one schedule per site problem and reuses it
+// for every Davidson iteration (site_hamil_schedule.hpp:40-93,
+// solver_interface.hpp:30-77); ref_hpsi_run then times only create_T and
+// contract (super_hamil_mv.hpp:121-132).
+struct RefHpsi {
+    std::vector<uint32_t> in_rows;
+    std::vector<uint64_t> in_off, out_off;
+    std::vector<uint32_t> out_rows, out_cols;
+    BoundaryIndexRT rrt, lrt;
+    std::unique_ptr<ScheduleNew<double>> tasks;
+    std::vector<const double*> lv, rv;
+    std::vector<std::mutex> mutexes;
+};
+
+void* ref_hpsi_create(const dmrgb200_plan_desc* dp, uint32_t nR, const uint32_t* R_lsz, const uint32_t* R_rsz,
+                      const uint32_t* R_nb, const double* const* L, uint32_t nL, const double* const* R) {
+    dmrgb200_plan_desc const& d = *dp;
+    if (d.kind != DMRGB200_PLAN_HPSI) return nullptr;
+    auto* h = new RefHpsi;
+    h->in_off.assign(d.in_off, d.in_off + d.n_in_blocks);
+    h->out_off.assign(d.out_off, d.out_off + d.n_out_blocks);
+    h->out_rows.assign(d.out_rows, d.out_rows + d.n_out_blocks);
+    h->out_cols.assign(d.out_cols, d.out_cols + d.n_out_blocks);
+    h->rrt = make_rt(nR, R_lsz, R_rsz, R_nb);
+    std::vector<std::size_t> lr(d.in_rows, d.in_rows + d.n_in_blocks), mpsbs(d.n_in_blocks, 0);
+    h->tasks.reset(new ScheduleNew<double>(mpsbs, lr, h->lrt, h->rrt));
+    for (uint32_t g = 0; g < d.n_groups; ++g) fill_group(d, g, nR, (*h->tasks)[g], false, false, true);
+    h->lv.assign(L, L + nL);
+    h->rv.assign(R, R + nR);
+    h->mutexes = std::vector<std::mutex>(d.n_out_blocks);
+    return h;
+}
+
+int ref_hpsi_run(void* handle, const double* x, double* y) {
+    auto* h = static_cast<RefHpsi*>(handle);
+    if (!h) return 1;
+    auto xv = block_views(x, h->in_off.data(), uint32_t(h->in_off.size()));
+    for (size_t b = 0; b < h->out_off.size(); ++b)
+        std::memset(y + h->out_off[b], 0, sizeof(double) * size_t(h->out_rows[b]) * h->out_cols[b]);
+    ScheduleNew<double>& tasks = *h->tasks;
+    int ng = int(tasks.size());
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int g = 0; g < ng; ++g) {
+        auto T = tasks[g].create_T(h->rv, xv);
+        for (auto it = tasks[g].begin(); it != tasks[g].end(); ++it)
+            it->contract(h->lv, T, y + h->out_off[it->get_rb()], h->mutexes[it->get_rb()]);
+    }
+    return 0;
+}
+
+void ref_hpsi_destroy(void* handle) { delete static_cast<RefHpsi*>(handle); }
+
 int ref_left_step(const dmrgb200_plan_desc* dp, uint32_t nL, const uint32_t* L_lsz, const uint32_t* L_rsz,
                   const uint32_t* L_nb, const double* const* L, const double* ket, const double* bra,
                   double* const* out) {

@@ -458,8 +458,13 @@ class TwoSiteDMRG:
         self.A = right_canonicalize(tensors)
         self.p12, self.offs = M.fuse_phys(model.phys, model.phys)
         self.W = [M.MPOHandle(w, model.symm) for w in model.mpo]
-        self.W12 = [M.MPOHandle(M.twosite_mpo(model.mpo[i], model.mpo[i + 1], model.phys, model.phys), model.symm)
-                    for i in range(self.L - 1)]
+        self.W12 = [M.MPOHandle(M.twosite_for(model, i), model.symm) for i in range(self.L - 1)]
+        # SU2U1: H_eff acts on the spin-reduced two-site tensor (ts_reduction.h; TwoSiteTensor::make_mps,
+        # twositetensor.hpp:130-151); the split works on the product-basis tensor
+        self.su2 = model.symm == capi.SU2U1
+        self.core_energy = getattr(model, "core_energy", 0.0)
+        if self.su2 and device_split:
+            raise ValueError("the device split takes product-basis two-site tensors; SU2U1 sweeps split on the host")
         self.Lidx = [None] * (self.L + 1)
         self.Lbuf = [None] * (self.L + 1)
         self.Ridx = [None] * (self.L + 1)
@@ -482,6 +487,9 @@ class TwoSiteDMRG:
         ph = self.log.phase_seconds
         t0 = time.perf_counter()
         psi = twosite(self.A[i], self.A[i + 1], self.p12, self.offs)
+        if self.su2:
+            from . import su2u1
+            psi = su2u1.reduce_twosite(psi, self.model.phys, self.model.phys, self.offs)
         t1 = time.perf_counter()
         extra = {"keep_on_device": True} if self.device_split else {}
         energy, xo, iters, ms = self.be.solve(self.p12, psi, self.W12[i], self.Lidx[i], self.Lbuf[i],
@@ -495,6 +503,9 @@ class TwoSiteDMRG:
                                left_to_right)
         else:
             psi.data = xo
+            if self.su2:
+                from . import su2u1
+                psi = su2u1.unreduce_twosite(psi, self.model.phys, self.model.phys, self.offs)
             res = split(psi, self.model.phys, self.model.phys, self.offs, self.m, self.cutoff, left_to_right)
         self.A[i], self.A[i + 1] = res.A, res.B
         t3 = time.perf_counter()
@@ -507,7 +518,7 @@ class TwoSiteDMRG:
         ph["site_problem"] = ph.get("site_problem", 0.0) + t2 - t1
         ph["split"] = ph.get("split", 0.0) + t3 - t2
         ph["boundary_step"] = ph.get("boundary_step", 0.0) + t4 - t3
-        return energy, iters, res.truncated_weight
+        return energy + self.core_energy, iters, res.truncated_weight
 
     def sweep(self, sweep_index: int):
         t0 = time.perf_counter()

@@ -303,7 +303,7 @@ class SiteProblem:
                                            symmetric, stream)
         self.Lidx, self.Lbuf, self.Ridx, self.Rbuf = Lidx, Lbuf, Ridx, Rbuf
         self.p12, _ = M.fuse_phys(model.phys, model.phys)
-        self.W12 = M.MPOHandle(M.twosite_mpo(model.mpo[i], model.mpo[i + 1], model.phys, model.phys), model.symm)
+        self.W12 = M.MPOHandle(M.twosite_for(model, i), model.symm)
         self.left, self.right = bonds[i], bonds[i + 2]
         self.schedule = schedule_hpsi(self.p12, self.left, self.right, self.W12, Lidx, Ridx)
         self.plan = DevicePlan(ctx, self.schedule.plan, left_addr=Lidx.cohort_addresses(Lbuf.data_ptr()),

@@ -30,6 +30,7 @@ class SiteOp:
     blocks: dict  # (cin, cout) -> np.ndarray (d_in x d_out), entry <out|O|in>
     spin: int = 0
     name: str = ""
+    spins: dict = None  # SU2 only: (cin, cout) -> (row spins, column spins) of the block's entries
 
 
 @dataclass
@@ -308,6 +309,15 @@ def twosite_mpo(W1: MPOTensor, W2: MPOTensor, p1, p2, merge: bool = True) -> MPO
     return W
 
 
+def twosite_for(model: Model, i: int, merge: bool = True) -> MPOTensor:
+    """The two-site MPO of sites (i, i+1) of a model: the spin-coupled product for SU2U1
+    (su2u1.twosite_mpo), the Kronecker product otherwise."""
+    if model.symm == capi.SU2U1:
+        from . import su2u1
+        return su2u1.twosite_mpo(model.mpo[i], model.mpo[i + 1], model.phys, model.phys)
+    return twosite_mpo(model.mpo[i], model.mpo[i + 1], model.phys, model.phys, merge=merge)
+
+
 # ---- C description ------------------------------------------------------------------
 
 class MPOHandle:
@@ -329,17 +339,24 @@ class MPOHandle:
                 tsc.append(sc)
         op_block, blk_in, blk_out, blk_entry = [0], [], [], [0]
         e_row, e_col, e_rs, e_cs, e_coeff = [], [], [], [], []
+        su2 = symm == capi.SU2U1
         for op in ops:
             for (cin, cout), B in op.blocks.items():
                 blk_in += list(cin)
                 blk_out += list(cout)
+                if su2 and op.spins is not None:
+                    rsp, csp = op.spins[(cin, cout)]
+                elif su2:  # site operator: the entries' spins are those of the block's charges
+                    rsp, csp = [abs(cin[1])] * B.shape[0], [abs(cout[1])] * B.shape[1]
+                else:
+                    rsp, csp = [0] * B.shape[0], [0] * B.shape[1]
                 for i in range(B.shape[0]):
                     for j in range(B.shape[1]):
                         if B[i, j] != 0:
                             e_row.append(i)
                             e_col.append(j)
-                            e_rs.append(0)
-                            e_cs.append(0)
+                            e_rs.append(rsp[i])
+                            e_cs.append(csp[j])
                             e_coeff.append(B[i, j])
                 blk_entry.append(len(e_row))
             op_block.append(len(blk_entry) - 1)

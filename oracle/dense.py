@@ -156,3 +156,112 @@ def mpo_dense(model: M.Model, L: int) -> np.ndarray:
             new[b2] = new.get(b2, 0) + np.kron(env[b1], O)
         env = new
     return env[0]
+
+
+def spin_sector_spectrum_jw(h: np.ndarray, eri: np.ndarray, n_elec: int, two_s: int) -> np.ndarray:
+    """Exact (FCI) eigenvalues of the ab-initio Hamiltonian with integrals (h, eri) in the
+    sector of n_elec electrons and total spin two_s / 2, ascending: H in the spin-orbital
+    basis (TwoU1 model, Sz = S), restricted to the eigenspace S^2 = S(S+1) of the dense
+    S^2 = sum_ab (S+_a S-_b + S-_a S+_b) / 2 + Sz_a Sz_b.  The reference for SU2U1 results
+    (whose H_eff acts on spin multiplets)."""
+    from dmrgb200 import qc
+    L = h.shape[0]
+    nu, nd = (n_elec + two_s) // 2, (n_elec - two_s) // 2
+    m = qc.quantum_chemistry(L, nu, nd, h=h, eri=eri)
+    mask = sector_mask(m, L, (nu, nd))
+    H = sparse_hamiltonian(m, L)[mask][:, mask].toarray()
+    loc = dict(m.local)
+    splus = loc["cdag_up"] @ loc["c_down"]
+    loc.update(splus=splus, sminus=splus.T.copy(), sz=np.diag([0.0, 0.5, -0.5, 0.0]))
+    spin_terms = []
+    for a in range(L):
+        for b in range(L):
+            spin_terms += [(0.5, [(a, "splus"), (b, "sminus")]), (0.5, [(a, "sminus"), (b, "splus")]),
+                           (1.0, [(a, "sz"), (b, "sz")])]
+    ms = M.Model("spin_squared", m.symm, m.phys, loc, [], m.total_charge, spin_terms, fermionic_ops=m.fermionic_ops)
+    S2 = sparse_hamiltonian(ms, L)[mask][:, mask].toarray()
+    w, V = np.linalg.eigh(S2)
+    s = two_s / 2
+    Q = V[:, np.abs(w - s * (s + 1)) < 1e-8]
+    return np.sort(np.linalg.eigvalsh(Q.T @ H @ Q))
+
+
+def _strings(L: int, n: int):
+    from itertools import combinations
+    return [sum(1 << p for p in c) for c in combinations(range(L), n)]
+
+
+def _excitation(strings, L):
+    """e[p][q]: sparse matrix of a+_p a_q on one spin's occupation strings (sign from the
+    occupied orbitals between p and q)."""
+    pos = {s: k for k, s in enumerate(strings)}
+    n = len(strings)
+    out = [[None] * L for _ in range(L)]
+    for p in range(L):
+        for q in range(L):
+            rows, cols, vals = [], [], []
+            for k, st in enumerate(strings):
+                if not (st >> q) & 1:
+                    continue
+                t = st & ~(1 << q)
+                if (t >> p) & 1:
+                    continue
+                sign = (-1) ** bin(st & ((1 << q) - 1)).count("1") * (-1) ** bin(t & ((1 << p) - 1)).count("1")
+                rows.append(pos[t | (1 << p)])
+                cols.append(k)
+                vals.append(sign)
+            out[p][q] = sp.csr_matrix((vals, (rows, cols)), shape=(n, n))
+    return out
+
+
+def spin_sector_spectrum(h: np.ndarray, eri: np.ndarray, n_elec: int, two_s: int) -> np.ndarray:
+    """Exact (FCI) eigenvalues of H = sum h_pq E_pq + 1/2 sum (pq|rs) (E_pq E_rs - d_qr E_ps)
+    (E_pq = sum over spin of a+_p a_q) on the spin multiplets of n_elec electrons and total
+    spin two_s / 2, ascending.  The determinants of the sector Sz = S are alpha x beta
+    occupation strings; the states with total spin S are those annihilated by
+    S+ = sum_p a+_(p alpha) a_(p beta) (the highest-weight states of each multiplet)."""
+    L = h.shape[0]
+    nu, nd = (n_elec + two_s) // 2, (n_elec - two_s) // 2
+    sa, sb = _strings(L, nu), _strings(L, nd)
+    ea, eb = _excitation(sa, L), _excitation(sb, L)
+    Ia, Ib = sp.identity(len(sa), format="csr"), sp.identity(len(sb), format="csr")
+    E = [[sp.kron(ea[p][q], Ib, format="csr") + sp.kron(Ia, eb[p][q], format="csr") for q in range(L)]
+         for p in range(L)]
+    H = sp.csr_matrix((len(sa) * len(sb),) * 2)
+    for p in range(L):
+        for q in range(L):
+            F = sp.csr_matrix(H.shape)
+            for r in range(L):
+                for s_ in range(L):
+                    if eri[p, q, r, s_] != 0.0:
+                        F = F + eri[p, q, r, s_] * E[r][s_]
+            H = H + h[p, q] * E[p][q] + 0.5 * (E[p][q] @ F)
+            for s_ in range(L):
+                H = H - 0.5 * eri[p, q, q, s_] * E[p][s_]
+    H = H.toarray()
+    if two_s < nd + nu:
+        # S+ from (nu, nd) to (nu + 1, nd - 1): a+_(p alpha) a_(p beta), alpha orbitals ordered first
+        if nd == 0:
+            Q = np.eye(H.shape[0])
+        else:
+            ta, tb = _strings(L, nu + 1), _strings(L, nd - 1)
+            pa, pb = {x: k for k, x in enumerate(ta)}, {x: k for k, x in enumerate(tb)}
+            rows, cols, vals = [], [], []
+            for ia, a in enumerate(sa):
+                for ib, b in enumerate(sb):
+                    for p in range(L):
+                        if not (b >> p) & 1 or (a >> p) & 1:
+                            continue
+                        b2, a2 = b & ~(1 << p), a | (1 << p)
+                        sign = (-1) ** (nu + bin(b & ((1 << p) - 1)).count("1")) * \
+                            (-1) ** bin(a & ((1 << p) - 1)).count("1")
+                        rows.append(pa[a2] * len(tb) + pb[b2])
+                        cols.append(ia * len(sb) + ib)
+                        vals.append(sign)
+            Sp = sp.csr_matrix((vals, (rows, cols)), shape=(len(ta) * len(tb), H.shape[0])).toarray()
+            _, sv, Vt = np.linalg.svd(Sp)
+            rank = int(np.sum(sv > 1e-10))
+            Q = Vt[rank:].T
+    else:
+        Q = np.eye(H.shape[0])
+    return np.sort(np.linalg.eigvalsh(Q.T @ H @ Q))

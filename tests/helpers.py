@@ -44,7 +44,7 @@ class OracleChain:
             Ridx = nidx
         self.Lidx, self.Lval, self.Ridx, self.Rval = Lidx, Lval, Ridx, Rval
         self.p12, _ = M.fuse_phys(model.phys, model.phys)
-        self.W12mpo = M.twosite_mpo(model.mpo[i], model.mpo[i + 1], model.phys, model.phys, merge=merge)
+        self.W12mpo = M.twosite_for(model, i, merge=merge)
         self.W12 = M.MPOHandle(self.W12mpo, model.symm)
         self.left, self.right = bonds[i], bonds[i + 2]
         self.sched = E.schedule_hpsi(self.p12, self.left, self.right, self.W12, Lidx, Ridx)

@@ -426,50 +426,62 @@ def gemm_workload(args):
 
 
 def qc_workload(args):
-    """Quantum-chemistry site problem (the ab-initio workload in TwoU1 form; SU2U1 is not
-    built): synthetic integrals (h seed 3, ERI seed 4, 2 L auxiliary vectors), L
-    orbitals at half filling, bond dimension m, middle two-site H·psi with
-    device-built boundaries; FP64 and emulated FP64 (7 slices) timed with L2 flushes."""
+    """Quantum-chemistry site problem (config 3 of the reference's ab-initio workload):
+    synthetic integrals (h seed 3, ERI seed 4, 2 L auxiliary vectors) written to and read
+    back from the reference's integral text format, L orbitals, L electrons, S = 0, in
+    SU2U1 (spin-adapted, default) or TwoU1 (spin-orbital) symmetry, bond dimension m
+    (SU2U1: spin multiplets), seeded random MPS made mixed-canonical around the middle
+    pair, boundaries built by device steps.  The middle two-site H·psi is timed in FP64
+    and in emulated FP64 (L2 flushed between steps); one JSON line."""
+    import ctypes as C
+
     import torch
 
     from dmrgb200 import _capi as capi
+    from dmrgb200 import dmrg as G
     from dmrgb200 import engine as E
     from dmrgb200 import mps as S
     from dmrgb200 import qc
+    from dmrgb200 import su2u1 as SU
 
-    L, m = args.qc_sites, args.qc_m
+    L, m, su2 = args.qc_sites, args.qc_m, args.qc_symmetry == "su2u1"
     t0 = time.perf_counter()
-    # the integrals go through the reference's integral text format and back
     fcidump = Path(tempfile.mkdtemp()) / "FCIDUMP"
     n_records = qc.write_integrals(fcidump, *qc.synthetic_integrals(L))
     h, eri, _ = qc.read_integrals(fcidump, L)
-    model = qc.quantum_chemistry(L, L // 2, L // 2, h=h, eri=eri)
-    bonds = S.synthetic_bonds(model.phys, L, model.total_charge, m, RADIUS)
+    if su2:
+        model = SU.quantum_chemistry(L, L, 0, h=h, eri=eri)
+        bonds = SU.synthetic_bonds(L, (L, 0), m, RADIUS)
+        phys = SU.PHYS
+    else:
+        model = qc.quantum_chemistry(L, L // 2, L // 2, h=h, eri=eri)
+        bonds = S.synthetic_bonds(model.phys, L, model.total_charge, m, RADIUS)
+        phys = model.phys
+    t_model = time.perf_counter() - t0
     rng = np.random.default_rng(SEED)
-    tensors = S.random_mps(model.phys, bonds, rng)
-    ctx = E.Context(0)
     i = L // 2 - 1
+    tensors = G.left_canonicalize(G.right_canonicalize(S.random_mps(phys, bonds, rng)), i)
+    bonds = [t.left for t in tensors] + [tensors[-1].right]
+    ctx = E.Context(0)
     sp = E.SiteProblem(ctx, model, tensors, bonds, i)
     setup_s = time.perf_counter() - t0
-    x = torch.rand(sp.size, dtype=torch.float64, device="cuda")
+    x = torch.tensor(rng.standard_normal(sp.size), dtype=torch.float64, device="cuda")
+    x /= torch.linalg.norm(x)
     y = torch.zeros_like(x)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     res = {}
-    import ctypes as C
     for name, prec in (("fp64", capi.PREC_FP64), ("emulated", capi.PREC_FP64_EMULATED)):
         try:
             for _ in range(args.warmup):
                 sp.plan.hpsi(x.data_ptr(), y.data_ptr(), prec)
-        except capi.DmrgError as exc:  # reported, not hidden (e.g. a contraction beyond the INT32 range)
+            torch.cuda.synchronize()
+        except capi.DmrgError as exc:  # reported, not hidden
             res[name] = {"unavailable": str(exc)}
             continue
-        torch.cuda.synchronize()
         if name == "fp64":
             capi.check(capi.lib.dmrgb200_plan_set_timing(sp.plan.handle, 1), "set_timing")
+            torch.cuda.profiler.start()  # the profiler range holds only the timed FP64 steps
         ts = []
-        if name == "fp64":
-            # the profiler range holds only the timed FP64 steps (ncu --profile-from-start off)
-            torch.cuda.profiler.start()
         for k in range(min(args.steps, 10)):
             flush.fill_(float(k))
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -493,12 +505,15 @@ def qc_workload(args):
         else:
             res[name]["rel_err_vs_fp64"] = float(torch.linalg.norm(y - y64) / torch.linalg.norm(y64))
     W = sp.W12
+    sym = "SU2U1" if su2 else "TwoU1"
     line = {"metric": "QC H·psi GFLOP/s (FP64)", "value": res["fp64"]["value"], "unit": "GFLOP/s",
             "higher_is_better": True, "n_gpus": 1, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"qc_L{L}_twou1_m{m}_twosite_hpsi_middle", "sites": L, "bond_dim": m,
-                       "symmetry": "TwoU1", "mpo_bond_dim_two_site": [W.row_dim, W.col_dim],
+            "config": {"workload": f"qc_L{L}_{sym.lower()}_m{m}_twosite_hpsi_middle", "sites": L, "bond_dim": m,
+                       "electrons": L, "two_s": 0, "symmetry": sym,
+                       "mpo_bond_dim_two_site": [W.row_dim, W.col_dim],
                        "psi_elements": int(sp.size), "flops_per_step": int(sp.plan.flops),
-                       "integral_records": n_records, "setup_seconds": setup_s,
+                       "terms": int(len(sp.schedule.plan["term_alpha"])),
+                       "integral_records": n_records, "model_seconds": t_model, "setup_seconds": setup_s,
                        "l2": "flushed (256 MiB write)"},
             "fp64": res["fp64"], "emulated": res["emulated"]}
     print(json.dumps(line), flush=True)
@@ -696,6 +711,8 @@ def main():
                     help="where the sweep workload splits the two-site tensor")
     ap.add_argument("--qc-sites", type=int, default=24, help="orbitals of the qc workload")
     ap.add_argument("--qc-m", type=int, default=2000, help="bond dimension of the qc workload")
+    ap.add_argument("--qc-symmetry", default="su2u1", choices=["su2u1", "twou1"],
+                    help="symmetry of the qc workload (SU2U1: spin-adapted, bond dimension in multiplets)")
     ap.add_argument("--adj-sites", type=int, default=16, help="orbitals of the adjoint workload")
     ap.add_argument("--adj-m", type=int, default=512, help="bond dimension of the adjoint workload")
     ap.add_argument("--prec", default="fp64", choices=["fp64", "emulated"],

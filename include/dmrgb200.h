@@ -196,11 +196,14 @@ dmrgb200_status dmrgb200_plan_scratch_bytes(dmrgb200_plan_t plan, uint64_t* byte
  * is left untouched.  Replaces super_hamil_mv (super_hamil_mv.hpp:100-155) and
  * ietl::mult (ietl_interface_dv.h:112-118).  DMRGB200_PREC_FP64_EMULATED runs
  * the T and cohort contractions on the INT8 tensor cores (Ozaki split, see
- * dmrgb200_plan_set_slices) and the S build in FP64; it synchronises the
- * stream before returning.  The digit planes of the boundaries are made on the
- * first emulated call of a plan and reused by later calls (the boundaries of a
- * site problem do not change while it is solved); dmrgb200_plan_set_slices
- * with a new slice count makes them again. */
+ * dmrgb200_plan_set_slices) and the S build in FP64, stream-ordered like the
+ * FP64 path.  The first emulated call of a plan allocates its digit-plane
+ * scratch (make it before capturing the stream; DMRGB200_NOT_SUPPORTED
+ * otherwise) and makes the digit planes of the boundaries, which later calls
+ * reuse (the boundaries of a site problem do not change while it is solved);
+ * dmrgb200_plan_set_slices with a new slice count makes them again.  Kernel
+ * waits that run out are recorded on the device and reported by the next
+ * dmrgb200_plan_check or dmrgb200_solve. */
 dmrgb200_status dmrgb200_hpsi(dmrgb200_plan_t plan, const double* x, double* y, dmrgb200_precision prec,
                               void* cuda_stream);
 
@@ -247,6 +250,31 @@ dmrgb200_status dmrgb200_hpsi_host(dmrgb200_plan_t plan, const double* x_host, d
  * slices of one input block overlap (no such plan comes from the builders). */
 dmrgb200_status dmrgb200_hpsi_adjoint(dmrgb200_plan_t plan, const double* w, const double* x, double* gx,
                                       double* galpha, void* cuda_stream);
+
+/* Synchronise `cuda_stream` and report the device-side error words of the plan's
+ * kernels since the last check (bounded waits of the grouped S build and of the
+ * emulated stages that ran out): DMRGB200_TIMEOUT if any did (the results of
+ * those calls are not valid; the words are cleared and the plan stays usable),
+ * DMRGB200_OK otherwise.  The asynchronous dmrgb200_hpsi calls report such
+ * failures only here.  No counterpart in the reference, whose kernels do not
+ * wait on the device. */
+dmrgb200_status dmrgb200_plan_check(dmrgb200_plan_t plan, void* cuda_stream);
+
+/* Precision of the H·psi inside dmrgb200_solve (default DMRGB200_PREC_FP64):
+ * with DMRGB200_PREC_FP64_EMULATED the contractions of every H·psi run emulated
+ * on the INT8 tensor cores while orthogonalisation, Rayleigh-Ritz, residuals and
+ * energies stay in native FP64.  Changing it drops the plan's cached solver
+ * graph. */
+dmrgb200_status dmrgb200_plan_set_precision(dmrgb200_plan_t plan, int prec);
+
+/* Slice count from an error target: H·psi of x (the plan's in layout) in FP64
+ * against emulated H·psi with 3, 4, ... 8 digit planes; the smallest count whose
+ * relative error ||y_emu - y_fp64|| / ||y_fp64|| is at most `target` is kept
+ * (as by dmrgb200_plan_set_slices) and returned with its error.
+ * DMRGB200_NUMERIC if 8 planes miss the target (8 is kept).  Synchronises the
+ * stream. */
+dmrgb200_status dmrgb200_plan_tune_slices(dmrgb200_plan_t plan, const double* x, double target, void* cuda_stream,
+                                          int* slices, double* rel_err);
 
 /* Digit planes per operand (2..8, default 7) used by DMRGB200_PREC_FP64_EMULATED:
  * the relative error of each emulated contraction is about 2^(-7 slices) of

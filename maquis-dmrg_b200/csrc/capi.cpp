@@ -65,6 +65,7 @@ struct dmrgb200_plan_s {
     uint64_t timed_calls = 0;
     // FP64 emulated on the INT8 tensor cores (built on first use)
     int slices = 7;
+    int solve_prec = DMRGB200_PREC_FP64;  // precision of the H psi inside dmrgb200_solve
     OzProgram* oz1 = nullptr;
     OzProgram* oz3 = nullptr;
     void* oz_scratch = nullptr;   // stage-1 digit planes (the constant ones persist between calls)
@@ -295,17 +296,18 @@ dmrgb200_status run_step(dmrgb200_plan_s* p, const double* ket, const double* br
     return DMRGB200_OK;
 }
 
-// Stage 1 and stage 3 on the INT8 tensor cores (Ozaki split with plan->slices
-// digit planes), the S build in FP64 between them.  Synchronises the stream to
-// report pipeline timeouts.
-dmrgb200_status hpsi_emulated(dmrgb200_plan_s* plan, const double* x, double* y, cudaStream_t st) {
+// Emulation tables and digit-plane scratch of a plan (host work and allocations:
+// outside any stream capture).  A new scratch drops the cached constant digit
+// planes; the calls that change the slice count (and so the scratch a captured
+// solver graph used) drop that graph themselves.
+cudaError_t emu_prepare(dmrgb200_plan_s* plan) {
     if (!plan->oz1) {
-        GemmList const& s1 = plan->prog.stage1_tasks.probs.empty() ? plan->prog.stage1 : plan->prog.stage1_tasks;
-        plan->oz1 = oz_build(s1);
+        // stage 1 on the stacked row-table problems when the plan has them (one problem per
+        // boundary cohort instead of one per T task)
+        plan->oz1 = oz_build(plan->prog.stage1);
         plan->oz3 = oz_build(plan->prog.stage3);
-        if (!plan->oz1 || !plan->oz3) return fail(DMRGB200_OUT_OF_MEMORY, "emulation tables");
+        if (!plan->oz1 || !plan->oz3) return cudaErrorMemoryAllocation;
     }
-    // one scratch per stage: each keeps the digit planes of its constant (boundary) operand
     auto ensure = [&](OzProgram* oz, void*& buf, uint64_t& size) -> cudaError_t {
         const uint64_t need = oz_scratch_bytes(oz, plan->slices);
         if (need <= size) return cudaSuccess;
@@ -314,34 +316,74 @@ dmrgb200_status hpsi_emulated(dmrgb200_plan_s* plan, const double* x, double* y,
         size = 0;
         oz_invalidate(oz);
         cudaError_t e = cudaMalloc(&buf, need);
-        if (e == cudaSuccess) size = need;
-        return e;
+        if (e != cudaSuccess) return e;
+        size = need;
+        return cudaMemset(oz_error_word(oz, buf, plan->slices), 0, sizeof(int));
     };
     cudaError_t e = ensure(plan->oz1, plan->oz_scratch, plan->oz_scratch_size);
     if (e == cudaSuccess) e = ensure(plan->oz3, plan->oz_scratch3, plan->oz_scratch3_size);
-    if (e != cudaSuccess) return cuda_fail(e, "emulation scratch");
+    return e;
+}
+
+// Stage 1 and stage 3 on the INT8 tensor cores (Ozaki split with plan->slices digit
+// planes), the S build in FP64 between them.  Stream-ordered: a pipeline wait that
+// timed out is recorded in the device error words and reported by the next
+// dmrgb200_plan_check or dmrgb200_solve.
+cudaError_t emu_launch(dmrgb200_plan_s* plan, const double* x, double* y, cudaStream_t st) {
     Bases bs{};
     bs.b[BUF_IN] = reinterpret_cast<uint64_t>(x);
     bs.b[BUF_OUT] = reinterpret_cast<uint64_t>(y);
     bs.b[BUF_T] = reinterpret_cast<uint64_t>(plan->T);
     bs.b[BUF_S] = reinterpret_cast<uint64_t>(plan->S);
-    e = oz_run(plan->oz1, bs, plan->slices, plan->oz_scratch, st);
-    if (e != cudaSuccess) return cuda_fail(e, "emulated stage 1");
-    e = run_sbuild(plan->prog, plan->T, plan->S, st);
-    if (e != cudaSuccess) return cuda_fail(e, "S build");
-    e = oz_run(plan->oz3, bs, plan->slices, plan->oz_scratch3, st);
-    if (e != cudaSuccess) return cuda_fail(e, "emulated stage 3");
-    // one synchronisation: both stages' wait-timeout flags
-    const int to1 = oz_timed_out(plan->oz1, plan->oz_scratch, plan->slices, st);
-    const int to3 = oz_timed_out(plan->oz3, plan->oz_scratch3, plan->slices, st);
-    if (to1 || to3) {
-        oz_invalidate(plan->oz1);
-        oz_invalidate(plan->oz3);
-        return fail(DMRGB200_TIMEOUT, to1 ? "emulated stage 1: a pipeline wait timed out"
-                                          : "emulated stage 3: a pipeline wait timed out");
-    }
-    if (sbuild_timed_out(plan->prog)) return fail(DMRGB200_TIMEOUT, "S build: a bulk-copy wait timed out");
+    cudaError_t e = oz_run(plan->oz1, bs, plan->slices, plan->oz_scratch, st);
+    if (e == cudaSuccess) e = run_sbuild(plan->prog, plan->T, plan->S, st);
+    if (e == cudaSuccess) e = oz_run(plan->oz3, bs, plan->slices, plan->oz_scratch3, st);
+    return e;
+}
+
+bool capturing(cudaStream_t st) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    return cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone;
+}
+
+dmrgb200_status hpsi_emulated(dmrgb200_plan_s* plan, const double* x, double* y, cudaStream_t st) {
+    const bool ready = plan->oz1 && plan->oz_scratch && plan->oz_scratch3;
+    if (!ready && capturing(st))
+        return fail(DMRGB200_NOT_SUPPORTED, "the first emulated H psi of a plan allocates its digit planes: make it "
+                                            "before capturing the stream");
+    cudaError_t e = ready ? cudaSuccess : emu_prepare(plan);
+    if (e != cudaSuccess) return cuda_fail(e, "emulation tables and scratch");
+    e = emu_launch(plan, x, y, st);
+    if (e != cudaSuccess) return cuda_fail(e, "emulated H psi");
     return DMRGB200_OK;
+}
+
+// Wait-timeout words of a plan's kernels, read after the stream is synchronised and
+// cleared: bit 0 the S build, bit 1 emulated stage 1, bit 2 emulated stage 3.
+int read_error_words(dmrgb200_plan_s* plan) {
+    int bits = 0;
+    if (plan->compiled && sbuild_timed_out(plan->prog)) bits |= 1;
+    auto oz_word = [&](OzProgram* oz, void* scratch) -> int {
+        if (!oz || !scratch) return 0;
+        int* w = oz_error_word(oz, scratch, plan->slices);
+        int v = 0;
+        if (cudaMemcpy(&v, w, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return 0;
+        if (v) {
+            cudaMemset(w, 0, sizeof(int));
+            oz_invalidate(oz);  // the digit planes of a stopped run may be incomplete
+        }
+        return v != 0;
+    };
+    if (oz_word(plan->oz1, plan->oz_scratch)) bits |= 2;
+    if (oz_word(plan->oz3, plan->oz_scratch3)) bits |= 4;
+    return bits;
+}
+
+dmrgb200_status timeout_status(int bits) {
+    if (!bits) return DMRGB200_OK;
+    std::string where = (bits & 1) ? "S build (bulk-copy ring)" : (bits & 2) ? "emulated stage 1" : "emulated stage 3";
+    return fail(DMRGB200_TIMEOUT, where + ": a bounded wait ran out; the results of the calls since the last check "
+                                          "are not valid");
 }
 
 }  // namespace
@@ -350,16 +392,35 @@ namespace dmrgb200 {
 dmrgb200_status noalloc_fail(dmrgb200_status s, std::string const& msg) { return fail(s, msg); }
 cudaError_t plan_hpsi_launch(dmrgb200_plan_t plan, const double* x, double* y, cudaStream_t stream) {
     if (plan->flat.kind != KIND_HPSI || !plan->compiled) return cudaErrorInvalidValue;
+    if (plan->solve_prec == DMRGB200_PREC_FP64_EMULATED) {
+        if (!plan->oz_scratch3) {
+            if (capturing(stream)) return cudaErrorStreamCaptureUnsupported;
+            cudaError_t e = emu_prepare(plan);
+            if (e != cudaSuccess) return e;
+        }
+        return emu_launch(plan, x, y, stream);
+    }
     return run_program(plan->prog, reinterpret_cast<uint64_t>(x), reinterpret_cast<uint64_t>(y), plan->T, plan->S,
                        stream);
 }
 void noalloc_desc_to_flat(const dmrgb200_plan_desc* d, FlatPlan& f) { desc_to_flat(d, f); }
 int plan_solver_mode(dmrgb200_plan_t plan) { return plan->solver_mode; }
-bool plan_sbuild_timed_out(dmrgb200_plan_t plan) { return plan->compiled && sbuild_timed_out(plan->prog); }
+int plan_error_words(dmrgb200_plan_t plan) { return read_error_words(plan); }
 // Autotune the plan's grouped GEMMs once, outside any stream capture (DMRGB200_AUTOTUNE=0
 // keeps the default variant, and so do plans below 50 MFLOP per H psi).
 cudaError_t plan_ensure_tuned(dmrgb200_plan_t plan, const double* x, double* y, cudaStream_t stream) {
-    if (plan->prog.tuned || !plan->compiled) return cudaSuccess;
+    if (!plan->compiled) return cudaSuccess;
+    if (plan->solve_prec == DMRGB200_PREC_FP64_EMULATED) {
+        // tables, scratch and the constant (boundary) digit planes before any capture: one
+        // emulated H psi splits the boundaries, later ones (captured or not) only psi and S
+        const bool fresh = !plan->oz_scratch3;
+        cudaError_t e = emu_prepare(plan);
+        if (e == cudaSuccess && (fresh || !oz_constants_ready(plan->oz1) || !oz_constants_ready(plan->oz3)) &&
+            !capturing(stream))
+            e = emu_launch(plan, x, y, stream);
+        return e;
+    }
+    if (plan->prog.tuned) return cudaSuccess;
     static const bool enabled = [] {
         const char* v = std::getenv("DMRGB200_AUTOTUNE");
         return !(v && v[0] == '0');
@@ -663,8 +724,87 @@ dmrgb200_status dmrgb200_plan_set_slices(dmrgb200_plan_t plan, int slices) {
         oz_free(plan->oz1);
         oz_free(plan->oz3);
         plan->oz1 = plan->oz3 = nullptr;
+        jd_graph_free(plan->jd);  // a captured emulated solve used the old digit planes
+        plan->jd = nullptr;
     }
     return DMRGB200_OK;
+}
+
+dmrgb200_status dmrgb200_plan_set_precision(dmrgb200_plan_t plan, int prec) {
+    if (!plan) return fail(DMRGB200_INVALID_ARGUMENT, "null plan");
+    if (prec != DMRGB200_PREC_FP64 && prec != DMRGB200_PREC_FP64_EMULATED)
+        return fail(DMRGB200_INVALID_ARGUMENT, "unknown precision");
+    if (prec != plan->solve_prec) {
+        plan->solve_prec = prec;
+        jd_graph_free(plan->jd);  // the cached solver graph captured the other H psi
+        plan->jd = nullptr;
+    }
+    return DMRGB200_OK;
+}
+
+dmrgb200_status dmrgb200_plan_check(dmrgb200_plan_t plan, void* cuda_stream) {
+    if (!plan) return fail(DMRGB200_INVALID_ARGUMENT, "null plan");
+    cudaError_t e = cudaStreamSynchronize(static_cast<cudaStream_t>(cuda_stream));
+    if (e != cudaSuccess) return cuda_fail(e, "plan check");
+    return timeout_status(read_error_words(plan));
+}
+
+dmrgb200_status dmrgb200_plan_tune_slices(dmrgb200_plan_t plan, const double* x, double target, void* cuda_stream,
+                                          int* slices, double* rel_err) {
+    DMRGB200_TRY
+    if (!plan || !x || !(target > 0.0)) return fail(DMRGB200_INVALID_ARGUMENT, "null argument or target <= 0");
+    if (plan->flat.kind != KIND_HPSI || !plan->compiled) return fail(DMRGB200_INVALID_PLAN, "plan is not an H psi plan");
+    cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+    const uint64_t n = std::max<uint64_t>(plan->flat.out_size, 1);
+    double *y64 = nullptr, *ye = nullptr, *dot = nullptr;
+    cudaError_t e = cudaMalloc(&y64, 2 * n * sizeof(double) + 2 * sizeof(double));
+    if (e != cudaSuccess) return cuda_fail(e, "slice tuning buffers");
+    ye = y64 + n;
+    dot = ye + n;
+    struct Free {
+        double* p;
+        ~Free() { cudaFree(p); }
+    } guard{y64};
+    if ((e = cudaMemsetAsync(y64, 0, 2 * n * sizeof(double), st)) != cudaSuccess) return cuda_fail(e, "slice tuning");
+    if ((e = run_program(plan->prog, reinterpret_cast<uint64_t>(x), reinterpret_cast<uint64_t>(y64), plan->T, plan->S,
+                         st)) != cudaSuccess)
+        return cuda_fail(e, "slice tuning: FP64 H psi");
+    const int s0 = plan->slices;
+    int chosen = 8;
+    double chosen_err = -1.0;
+    for (int sl = 3; sl <= 8; ++sl) {
+        plan->slices = sl;
+        oz_free(plan->oz1);
+        oz_free(plan->oz3);
+        plan->oz1 = plan->oz3 = nullptr;
+        if ((e = emu_prepare(plan)) != cudaSuccess) return cuda_fail(e, "slice tuning: emulation scratch");
+        if ((e = emu_launch(plan, x, ye, st)) != cudaSuccess) return cuda_fail(e, "slice tuning: emulated H psi");
+        if ((e = diff_norms(ye, y64, n, dot, st)) != cudaSuccess) return cuda_fail(e, "slice tuning: norms");
+        double h[2] = {0, 0};
+        if ((e = cudaMemcpyAsync(h, dot, 2 * sizeof(double), cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(st)) != cudaSuccess)
+            return cuda_fail(e, "slice tuning");
+        dmrgb200_status ts = timeout_status(read_error_words(plan));
+        if (ts != DMRGB200_OK) {
+            plan->slices = s0;
+            return ts;
+        }
+        const double err = h[1] > 0 ? std::sqrt(h[0] / h[1]) : std::sqrt(h[0]);
+        if (err <= target || sl == 8) {
+            chosen = sl;
+            chosen_err = err;
+            break;
+        }
+    }
+    // keep the chosen slice count (its digit planes are the ones now in the scratch)
+    plan->slices = chosen;
+    jd_graph_free(plan->jd);
+    plan->jd = nullptr;
+    if (slices) *slices = chosen;
+    if (rel_err) *rel_err = chosen_err;
+    if (chosen_err > target) return fail(DMRGB200_NUMERIC, "no slice count up to 8 meets the target error");
+    return DMRGB200_OK;
+    DMRGB200_CATCH
 }
 
 dmrgb200_status dmrgb200_plan_set_timing(dmrgb200_plan_t plan, int enable) {

@@ -321,8 +321,13 @@ void oz_invalidate(OzProgram* oz);
 uint64_t oz_scratch_bytes(OzProgram const* oz, int s);
 // run on the stream with scratch of oz_scratch_bytes(oz, s); returns a CUDA error
 cudaError_t oz_run(OzProgram* oz, Bases const& bs, int s, void* scratch, cudaStream_t st);
-// non-zero when a pipeline wait of the last run timed out (synchronises the stream)
-int oz_timed_out(OzProgram const* oz, void* scratch, int s, cudaStream_t st);
+// device word that records pipeline-wait timeouts of the program's runs (not cleared by
+// oz_run; the reader clears it)
+int* oz_error_word(OzProgram const* oz, void* scratch, int s);
+// the digit planes of the constant (boundary) operands are in the scratch
+bool oz_constants_ready(OzProgram const* oz);
+// out[0] = sum (a - b)^2, out[1] = sum b^2 over n elements (device scalars)
+cudaError_t diff_norms(const double* a, const double* b, uint64_t n, double* out, cudaStream_t st);
 double calibrate_fp64_tflops();
 // solver graph cache of a plan (jd_graph.cu)
 void jd_graph_free(void* g);

@@ -193,19 +193,22 @@ namespace dmrgb200 {
 dmrgb200_status solve_stepwise(dmrgb200_plan_t plan, uint64_t n, const double* x0, const double* const* ortho,
                                uint32_t n_ortho, double tol, uint32_t max_iter, double* energy, double* x_out,
                                dmrgb200_solve_stats* stats, void* cuda_stream);
-bool plan_sbuild_timed_out(dmrgb200_plan_t plan);
+int plan_error_words(dmrgb200_plan_t plan);
 }  // namespace dmrgb200
 
-// Both solver forms end synchronised; a grouped S build whose wait timed out
-// during the solve turns the result into DMRGB200_TIMEOUT.
+// Both solver forms end synchronised; a kernel whose bounded wait ran out during
+// the solve (grouped S build, emulated stages) turns the result into
+// DMRGB200_TIMEOUT.
 extern "C" dmrgb200_status dmrgb200_solve(dmrgb200_plan_t plan, uint64_t n, const double* x0,
                                           const double* const* ortho, uint32_t n_ortho, double tol, uint32_t max_iter,
                                           double* energy, double* x_out, dmrgb200_solve_stats* stats,
                                           void* cuda_stream) {
     dmrgb200_status s =
         dmrgb200::solve_stepwise(plan, n, x0, ortho, n_ortho, tol, max_iter, energy, x_out, stats, cuda_stream);
-    if (s == DMRGB200_OK && plan && dmrgb200::plan_sbuild_timed_out(plan))
-        return noalloc_fail(DMRGB200_TIMEOUT, "S build: a bulk-copy wait timed out");
+    const int bits = plan ? dmrgb200::plan_error_words(plan) : 0;
+    if (s == DMRGB200_OK && bits)
+        return noalloc_fail(DMRGB200_TIMEOUT, (bits & 1) ? "S build: a bulk-copy wait timed out"
+                                                         : "emulated H psi: a pipeline wait timed out");
     return s;
 }
 

@@ -102,9 +102,16 @@ struct OzSplit {
     uint64_t e_off;     // exponent array offset of row 0
     uint32_t is_b;      // 0: A operand, 1: B operand (read transposed)
     uint32_t is_const;  // the operand and its exponents are constant between calls
+    uint32_t rowtab;    // A of a row-table problem: row r at rowtab[rowtab + r]; DevProb::NO_ROWS otherwise
+    uint32_t pad;
 };
 
-__device__ __forceinline__ double op_elem(Bases const& bs, OzSplit const& j, uint32_t r, uint32_t k) {
+__device__ __forceinline__ double op_elem(Bases const& bs, OzSplit const& j, uint32_t r, uint32_t k,
+                                          const DevRow* __restrict__ rowtab) {
+    if (!j.is_b && j.rowtab != DevProb::NO_ROWS) {
+        const DevRow rw = rowtab[j.rowtab + r];
+        return reinterpret_cast<const double*>(base_of(bs, j.op.buf))[rw.a_off + uint64_t(k) * rw.ld];
+    }
     const double* base = reinterpret_cast<const double*>(base_of(bs, j.op.buf) + 8ull * j.op.off);
     const uint64_t ld = j.op.ld;
     if (!j.is_b) return j.op.trans ? base[k + uint64_t(r) * ld] : base[r + uint64_t(k) * ld];
@@ -121,13 +128,13 @@ __global__ void fill_int(int* __restrict__ p, uint64_t n, int v) {
 // |x 2^-e| < 1 for the whole row of the output matrix.  blockIdx.y walks the
 // jobs, blockIdx.x and the warps the rows, the lanes K.
 __global__ void __launch_bounds__(256) oz_exponents(const OzSplit* __restrict__ jobs, uint32_t njobs, Bases bs,
-                                                    int* __restrict__ e) {
+                                                    int* __restrict__ e, const DevRow* __restrict__ rowtab) {
     const uint32_t lane = threadIdx.x & 31, warps = blockDim.x >> 5;
     for (uint32_t j = blockIdx.y; j < njobs; j += gridDim.y) {
         const OzSplit job = jobs[j];
         for (uint32_t r = blockIdx.x * warps + (threadIdx.x >> 5); r < job.rows; r += gridDim.x * warps) {
             double m = 0.0;
-            for (uint32_t k = lane; k < job.K; k += 32) m = fmax(m, fabs(op_elem(bs, job, r, k)));
+            for (uint32_t k = lane; k < job.K; k += 32) m = fmax(m, fabs(op_elem(bs, job, r, k, rowtab)));
             for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
             if (lane == 0 && m > 0.0) atomicMax(&e[job.e_off + r], ilogb(m) + 1);
         }
@@ -139,7 +146,8 @@ __global__ void __launch_bounds__(256) oz_exponents(const OzSplit* __restrict__ 
 // tile layout).  Rows outside the operand and K beyond it give zero digits.
 __global__ void __launch_bounds__(256) oz_split(const OzSplit* __restrict__ jobs, uint32_t njobs, Bases bs,
                                                 const int* __restrict__ e, int s, uint64_t a_plane,
-                                                int8_t* __restrict__ A8, uint64_t b_plane, int8_t* __restrict__ B8) {
+                                                int8_t* __restrict__ A8, uint64_t b_plane, int8_t* __restrict__ B8,
+                                                const DevRow* __restrict__ rowtab) {
     for (uint32_t j = blockIdx.y; j < njobs; j += gridDim.y) {
         const OzSplit job = jobs[j];
         int8_t* out = job.is_b ? B8 : A8;
@@ -148,7 +156,8 @@ __global__ void __launch_bounds__(256) oz_split(const OzSplit* __restrict__ jobs
         const uint32_t tile_bytes = TR * OZ_BK;
         const uint32_t nrows = job.RT * TR, ngroups = job.KS * (OZ_BK / 4);
         const uint32_t total = nrows * ngroups;
-        const bool rows_fast = !job.is_b && !job.op.trans;  // column-major A: rows are contiguous
+        // column-major A: rows are contiguous (row-table rows are separate slices: K-major order)
+        const bool rows_fast = !job.is_b && !job.op.trans && job.rowtab == DevProb::NO_ROWS;
         for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
             const uint32_t r = rows_fast ? idx % nrows : idx / ngroups;
             const uint32_t k0 = 4 * (rows_fast ? idx / nrows : idx % ngroups);
@@ -156,7 +165,7 @@ __global__ void __launch_bounds__(256) oz_split(const OzSplit* __restrict__ jobs
             const int ex = r < job.rows ? e[job.e_off + r] : 0;
 #pragma unroll
             for (int u = 0; u < 4; ++u)
-                x[u] = (r < job.rows && k0 + u < job.K) ? ldexp(op_elem(bs, job, r, k0 + u), -ex) : 0.0;
+                x[u] = (r < job.rows && k0 + u < job.K) ? ldexp(op_elem(bs, job, r, k0 + u, rowtab), -ex) : 0.0;
             const uint64_t off = job.out_base + (uint64_t(r / TR) * job.KS + k0 / OZ_BK) * tile_bytes +
                                  tile_off(r % TR, k0 % OZ_BK);
             for (int p = 0; p < s; ++p) {
@@ -182,6 +191,7 @@ struct OzPB {  // one output matrix (a GEMM problem of one batch index)
     uint64_t e_off, f_off;          // exponents of its rows / columns
     DevOp C;                        // destination (batch folded into C.off)
     uint32_t beta, pad;
+    uint32_t rowtab, batch;         // row-table problems: C row r at rowtab[rowtab + r] (batch `batch`)
 };
 struct OzSlab {  // K slab: A tile of row tile mt at a_off + mt * a_ts, B tile of nt at b_off + nt * b_ts
     uint64_t a_off, b_off;
@@ -204,6 +214,7 @@ struct OzArgs {
     int s;
     Bases bases;
     int* err;
+    const DevRow* rowtab;
 };
 
 __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_mma(OzArgs a) {
@@ -313,12 +324,21 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_mma(OzArgs a) {
                         for (int j = 0; j < 16; ++j) acc[j] += double(v[j]) * w;
                     }
                     if (row < pb.M) {
+                        // the row's start and leading dimension: from the row table or the plain operand
+                        double* crow = Cb + row;
+                        uint64_t ldc = pb.C.ld;
+                        if (pb.rowtab != DevProb::NO_ROWS) {
+                            const DevRow rw = a.rowtab[pb.rowtab + row];
+                            crow = reinterpret_cast<double*>(base_of(a.bases, pb.C.buf)) + rw.c_off +
+                                   uint64_t(pb.batch) * rw.cbs;
+                            ldc = rw.ld;
+                        }
 #pragma unroll
                         for (int j = 0; j < 16; ++j) {
                             const uint32_t col = nt * OZ_BN + c0 + j;
                             if (col < pb.N) {
                                 const double val = ldexp(acc[j], erow + a.e[pb.f_off + col]);
-                                double* dst = Cb + row + uint64_t(col) * pb.C.ld;
+                                double* dst = crow + uint64_t(col) * ldc;
                                 *dst = add ? *dst + val : val;
                             }
                         }
@@ -363,10 +383,12 @@ struct OzProgram {
     std::vector<OzTile> tiles;
     uint64_t a_plane = 0, b_plane = 0, n_exp = 0, n_exp_c = 0;
     bool const_ready = false;       // constant digit planes present in the scratch
+    std::vector<DevRow> rowtab;     // rows of row-table problems (the GEMM list's table)
     OzSplit* d_jobs = nullptr;
     OzPB* d_pbs = nullptr;
     OzSlab* d_slabs = nullptr;
     OzTile* d_tiles = nullptr;
+    DevRow* d_rowtab = nullptr;
 };
 
 OzProgram* oz_build(GemmList const& gl) {
@@ -400,6 +422,8 @@ OzProgram* oz_build(GemmList const& gl) {
             pb.C = pr.C;
             pb.C.off += uint64_t(b) * pr.C.bstride;
             pb.beta = 0;
+            pb.rowtab = pr.rows;
+            pb.batch = b;
             pb.slab_begin = uint32_t(oz->slabs.size());
             for (uint32_t sgi = pr.seg_begin; sgi < pr.seg_end; ++sgi) {
                 DevSeg const& sg = gl.segs[sgi];
@@ -416,6 +440,7 @@ OzProgram* oz_build(GemmList const& gl) {
                 ja.e_off = pb.e_off;
                 ja.is_b = 0;
                 ja.is_const = a_const ? 1 : 0;
+                ja.rowtab = pr.rows;
                 oz->a_plane += uint64_t(pb.MT) * KS * A_TILE;
                 jb.op = sg.B;
                 jb.op.off += uint64_t(b) * sg.B.bstride;
@@ -427,6 +452,7 @@ OzProgram* oz_build(GemmList const& gl) {
                 jb.e_off = pb.f_off;
                 jb.is_b = 1;
                 jb.is_const = b_const ? 1 : 0;
+                jb.rowtab = DevProb::NO_ROWS;
                 oz->b_plane += uint64_t(pb.NT) * KS * B_TILE;
                 for (uint32_t ks = 0; ks < KS; ++ks)
                     oz->slabs.push_back(OzSlab{ja.out_base + uint64_t(ks) * A_TILE, jb.out_base + uint64_t(ks) * B_TILE,
@@ -464,8 +490,10 @@ OzProgram* oz_build(GemmList const& gl) {
         if (e != cudaSuccess) return e;
         return cudaMemcpy(*d, v.data(), v.size() * sizeof(v[0]), cudaMemcpyHostToDevice);
     };
+    oz->rowtab = gl.rowtab;
     if (up(oz->jobs, &oz->d_jobs) != cudaSuccess || up(oz->pbs, &oz->d_pbs) != cudaSuccess ||
-        up(oz->slabs, &oz->d_slabs) != cudaSuccess || up(oz->tiles, &oz->d_tiles) != cudaSuccess) {
+        up(oz->slabs, &oz->d_slabs) != cudaSuccess || up(oz->tiles, &oz->d_tiles) != cudaSuccess ||
+        up(oz->rowtab, &oz->d_rowtab) != cudaSuccess) {
         oz_free(oz);
         return nullptr;
     }
@@ -482,6 +510,7 @@ void oz_free(OzProgram* oz) {
     cudaFree(oz->d_pbs);
     cudaFree(oz->d_slabs);
     cudaFree(oz->d_tiles);
+    cudaFree(oz->d_rowtab);
     delete oz;
 }
 
@@ -515,7 +544,7 @@ cudaError_t oz_run(OzProgram* oz, Bases const& bs, int s, void* scratch, cudaStr
     if (s < 2 || s > OZ_MAX_SLICES) return cudaErrorInvalidValue;
     OzScratch c = carve(oz, s, scratch);
     const int sms = device_sm_count();
-    cudaMemsetAsync(c.err, 0, sizeof(int), st);
+    // the error word is not cleared here: it collects timeouts until the caller reads it
     // first run: every operand; later runs: only the operands that change between calls
     const uint64_t e0 = oz->const_ready ? oz->n_exp_c : 0;
     const uint32_t j0 = oz->const_ready ? oz->n_const_jobs : 0;
@@ -524,28 +553,59 @@ cudaError_t oz_run(OzProgram* oz, Bases const& bs, int s, void* scratch, cudaStr
                                                                                         -100000);
     const uint32_t nj = uint32_t(oz->jobs.size()) - j0;
     if (nj) {
-        oz_exponents<<<dim3(8, std::min<uint32_t>(nj, 65535u)), 256, 0, st>>>(oz->d_jobs + j0, nj, bs, c.e);
+        oz_exponents<<<dim3(8, std::min<uint32_t>(nj, 65535u)), 256, 0, st>>>(oz->d_jobs + j0, nj, bs, c.e,
+                                                                             oz->d_rowtab);
         dim3 grid(16, std::min<uint32_t>(nj, 65535u));
-        oz_split<<<grid, 256, 0, st>>>(oz->d_jobs + j0, nj, bs, c.e, s, oz->a_plane, c.A8, oz->b_plane, c.B8);
+        oz_split<<<grid, 256, 0, st>>>(oz->d_jobs + j0, nj, bs, c.e, s, oz->a_plane, c.A8, oz->b_plane, c.B8,
+                                       oz->d_rowtab);
     }
     oz->const_ready = true;
     if (!oz->tiles.empty()) {
         cudaError_t ea = ensure_smem_limit(reinterpret_cast<const void*>(ozaki_mma), int(ozaki_smem_bytes(OZ_MAX_SLICES)));
         if (ea != cudaSuccess) return ea;
         OzArgs args{c.A8, c.B8, oz->a_plane, oz->b_plane, c.e, oz->d_pbs, oz->d_slabs, oz->d_tiles,
-                    uint32_t(oz->tiles.size()), oz_chunk_slabs(s), s, bs, c.err};
+                    uint32_t(oz->tiles.size()), oz_chunk_slabs(s), s, bs, c.err, oz->d_rowtab};
         ozaki_mma<<<std::min<uint32_t>(uint32_t(oz->tiles.size()), uint32_t(sms)), OZ_THREADS, ozaki_smem_bytes(s),
                     st>>>(args);
     }
     return cudaGetLastError();
 }
 
-int oz_timed_out(OzProgram const* oz, void* scratch, int s, cudaStream_t st) {
-    OzScratch c = carve(oz, s, scratch);
-    int h = 0;
-    cudaMemcpyAsync(&h, c.err, sizeof(int), cudaMemcpyDeviceToHost, st);
-    cudaStreamSynchronize(st);
-    return h;
+int* oz_error_word(OzProgram const* oz, void* scratch, int s) { return carve(oz, s, scratch).err; }
+
+bool oz_constants_ready(OzProgram const* oz) { return oz && oz->const_ready; }
+
+namespace {
+// out[0] = sum (a - b)^2, out[1] = sum b^2 (one block, FP64)
+__global__ void __launch_bounds__(256) diff_norms_kernel(const double* __restrict__ a, const double* __restrict__ b,
+                                                         uint64_t n, double* __restrict__ out) {
+    __shared__ double sd[256], sb[256];
+    double d = 0.0, q = 0.0;
+    for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const double x = a[i] - b[i];
+        d += x * x;
+        q += b[i] * b[i];
+    }
+    sd[threadIdx.x] = d;
+    sb[threadIdx.x] = q;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            sd[threadIdx.x] += sd[threadIdx.x + o];
+            sb[threadIdx.x] += sb[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[0] = sd[0];
+        out[1] = sb[0];
+    }
+}
+}  // namespace
+
+cudaError_t diff_norms(const double* a, const double* b, uint64_t n, double* out, cudaStream_t st) {
+    diff_norms_kernel<<<1, 256, 0, st>>>(a, b, n, out);
+    return cudaGetLastError();
 }
 
 }  // namespace dmrgb200
@@ -582,8 +642,10 @@ extern "C" dmrgb200_status dmrgb200_dgemm_emulated(uint32_t M, uint32_t N, uint3
         return noalloc_fail(DMRGB200_OUT_OF_MEMORY, cudaGetErrorString(r));
     }
     Bases bs{};
+    int to = 0;
+    cudaMemsetAsync(oz_error_word(oz, scratch, slices), 0, sizeof(int), st);
     r = oz_run(oz, bs, slices, scratch, st);
-    int to = oz_timed_out(oz, scratch, slices, st);
+    cudaMemcpyAsync(&to, oz_error_word(oz, scratch, slices), sizeof(int), cudaMemcpyDeviceToHost, st);
     cudaError_t r2 = cudaStreamSynchronize(st);
     cudaFreeAsync(scratch, st);
     cudaStreamSynchronize(st);

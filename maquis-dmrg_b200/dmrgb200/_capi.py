@@ -105,6 +105,9 @@ _sigs = {
     "dmrgb200_status_string": ([C.c_int], C.c_char_p),
     "dmrgb200_last_error": ([], C.c_char_p),
     "dmrgb200_abi_version": ([], C.c_int),
+    "dmrgb200_plan_check": ([vp, vp], C.c_int),
+    "dmrgb200_plan_set_precision": ([vp, C.c_int], C.c_int),
+    "dmrgb200_plan_tune_slices": ([vp, vp, C.c_double, vp, i32p, f64p], C.c_int),
     "dmrgb200_wigner6j": ([C.c_int] * 6, C.c_double),
     "dmrgb200_wigner9j": ([C.c_int] * 9, C.c_double),
     "dmrgb200_set_coupling": ([C.c_int] * 9 + [C.c_double, f64p], None),

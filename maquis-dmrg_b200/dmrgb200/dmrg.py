@@ -285,9 +285,13 @@ def split_device(psi_dev, psi: S.SiteTensor, phys1, phys2, offs, m: int, cutoff:
     return SplitResult(A, B, tw, bond, dev_A=out[:a_lp], dev_A_lp=out[a_lp:b0], dev_B=out[b0:end])
 
 
-def right_canonicalize(tensors):
+def right_canonicalize(tensors, cutoff: float = 1e-14):
     """Make sites 1..L-1 right-normalised by per-charge SVDs, absorbing the
-    remainder into the left neighbour."""
+    remainder into the left neighbour.  Singular vectors whose singular value is at
+    most `cutoff` times the block's largest are dropped; cutoff = 0 keeps every
+    block at full rank (the singular vectors stay orthonormal however small their
+    weight), so the bond dimensions of a synthetic environment survive the products
+    of positive random blocks, whose spectra decay by orders of magnitude per site."""
     out = list(tensors)
     for j in range(len(out) - 1, 0, -1):
         t = out[j]
@@ -297,7 +301,7 @@ def right_canonicalize(tensors):
             if blk.size == 0:
                 continue
             U, sv, Vt = np.linalg.svd(blk, full_matrices=False)
-            k = int(np.sum(sv > 1e-14 * max(sv[0], 1e-300))) if sv.size else 0
+            k = int(np.sum(sv > cutoff * max(sv[0], 1e-300))) if sv.size else 0
             if k == 0:
                 continue
             new_left.append((lc, k))
@@ -324,11 +328,11 @@ def right_canonicalize(tensors):
     return out
 
 
-def left_canonicalize(tensors, upto: int):
+def left_canonicalize(tensors, upto: int, cutoff: float = 1e-14):
     """Make sites 0..upto-1 left-normalised by per-charge SVDs of their
     left-paired blocks, absorbing S V^T into the right neighbour (the mirror of
     right_canonicalize); bond dimensions drop only where a block is rank
-    deficient.  Returns the new tensor list."""
+    deficient (by `cutoff`, as in right_canonicalize).  Returns the new tensor list."""
     out = list(tensors)
     for j in range(upto):
         t, nxt = out[j], out[j + 1]
@@ -340,7 +344,7 @@ def left_canonicalize(tensors, upto: int):
             if blk.size == 0:
                 continue
             U, sv, Vt = np.linalg.svd(blk, full_matrices=False)
-            k = int(np.sum(sv > 1e-14 * max(sv[0], 1e-300))) if sv.size else 0
+            k = int(np.sum(sv > cutoff * max(sv[0], 1e-300))) if sv.size else 0
             if k == 0:
                 continue
             new_right.append((rc, k))
@@ -378,9 +382,17 @@ class DeviceBackend:
     """Hot-path operations on the device through libdmrgb200: boundary steps,
     H·psi plans and the Jacobi-Davidson solver (dmrgb200_solve)."""
 
-    def __init__(self, ctx: E.Context):
+    def __init__(self, ctx: E.Context, precision: int = capi.PREC_FP64, slices: int | None = None,
+                 slice_target: float = 1e-10):
+        """precision: of the H·psi inside every solve (capi.PREC_FP64 or capi.PREC_FP64_EMULATED:
+        contractions on the INT8 tensor cores, orthogonalisation, Rayleigh-Ritz and energies in
+        FP64).  Emulated solves use `slices` digit planes, or, with slices None, the smallest
+        count whose H·psi of the start vector is within slice_target of FP64 (tuned per site
+        problem, dmrgb200_plan_tune_slices)."""
         import torch
         self.torch, self.ctx = torch, ctx
+        self.precision, self.slices, self.slice_target = precision, slices, slice_target
+        self.slices_used = []  # (digit planes, relative H·psi error of the start vector) per emulated solve
         # host seconds per phase of the site problems (schedule building, plan lowering, solve)
         self.phase_seconds = {"schedule": 0.0, "plan": 0.0, "solve": 0.0}
 
@@ -431,6 +443,12 @@ class DeviceBackend:
         t2 = time.perf_counter()
         xd = E.to_device(psi.data, self.ctx.device)
         xo = self.torch.zeros_like(xd)
+        if self.precision == capi.PREC_FP64_EMULATED:
+            if self.slices is None:
+                self.slices_used.append(plan.tune_slices(xd.data_ptr(), self.slice_target))
+            else:
+                plan.set_slices(self.slices)
+            plan.set_precision(capi.PREC_FP64_EMULATED)
         energy, st = plan.solve(xd.data_ptr(), xo.data_ptr(), xd.numel(), tol=tol, max_iter=max_iter)
         out = xo if keep_on_device else xo.cpu().numpy()
         t3 = time.perf_counter()

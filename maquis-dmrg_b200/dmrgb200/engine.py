@@ -212,6 +212,25 @@ class DevicePlan:
         capi.check(capi.lib.dmrgb200_hpsi_adjoint(self.handle, w_ptr, x_ptr or None, gx_ptr or None,
                                                   galpha_ptr or None, stream or None), "dmrgb200_hpsi_adjoint")
 
+    def set_precision(self, prec: int) -> None:
+        """Precision of the H·psi inside solve (dmrgb200_plan_set_precision)."""
+        capi.check(capi.lib.dmrgb200_plan_set_precision(self.handle, prec), "dmrgb200_plan_set_precision")
+
+    def set_slices(self, slices: int) -> None:
+        capi.check(capi.lib.dmrgb200_plan_set_slices(self.handle, slices), "dmrgb200_plan_set_slices")
+
+    def tune_slices(self, x_ptr: int, target: float = 1e-10, stream: int = 0):
+        """Smallest digit-plane count whose emulated H·psi of x is within `target` (relative)
+        of the FP64 one (dmrgb200_plan_tune_slices); returns (slices, relative error)."""
+        sl, err = C.c_int32(), C.c_double()
+        capi.check(capi.lib.dmrgb200_plan_tune_slices(self.handle, x_ptr, target, stream or None, C.byref(sl),
+                                                      C.byref(err)), "dmrgb200_plan_tune_slices")
+        return sl.value, err.value
+
+    def check(self, stream: int = 0) -> None:
+        """Synchronise and raise if a kernel's bounded wait ran out (dmrgb200_plan_check)."""
+        capi.check(capi.lib.dmrgb200_plan_check(self.handle, stream or None), "dmrgb200_plan_check")
+
     def set_solver(self, mode: int) -> None:
         """capi.SOLVER_GRAPH (default: one CUDA graph per solve) or capi.SOLVER_STEPWISE."""
         capi.check(capi.lib.dmrgb200_plan_set_solver(self.handle, mode), "dmrgb200_plan_set_solver")

@@ -260,6 +260,17 @@ dmrgb200_status dmrgb200_hpsi_adjoint(dmrgb200_plan_t plan, const double* w, con
  * wait on the device. */
 dmrgb200_status dmrgb200_plan_check(dmrgb200_plan_t plan, void* cuda_stream);
 
+/* Limit, in nanoseconds, of the device-side waits for pipeline data in the
+ * grouped S build and the emulated stages (bulk copies completing on shared-memory
+ * barriers); 0 restores the default of 2 s.  A wait that runs out sets the plan's
+ * error word, the kernel lets the copies and MMAs it has in flight complete (with a
+ * fixed 2 s limit), releases its tensor memory and returns; dmrgb200_plan_check or
+ * dmrgb200_solve then reports DMRGB200_TIMEOUT and the plan stays usable.
+ * Process-wide; read at every launch (a captured solver graph keeps the value of
+ * its capture).  No counterpart in the reference, whose kernels do not wait on the
+ * device. */
+dmrgb200_status dmrgb200_set_wait_limit(uint64_t ns);
+
 /* Precision of the H·psi inside dmrgb200_solve (default DMRGB200_PREC_FP64):
  * with DMRGB200_PREC_FP64_EMULATED the contractions of every H·psi run emulated
  * on the INT8 tensor cores while orthogonalisation, Rayleigh-Ritz, residuals and

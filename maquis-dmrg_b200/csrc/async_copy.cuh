@@ -7,7 +7,11 @@
 namespace dmrgb200 {
 namespace async {
 
-constexpr unsigned long long WAIT_LIMIT_NS = 2000000000ull;  // 2 s
+// Limit of the waits for events that always happen once work is in flight (the
+// completion of issued MMAs, the landing of issued copies before a CTA leaves after
+// a timeout): 2 s.  Waits for the data a pipeline stage needs take their limit as
+// an argument (dmrgb200_set_wait_limit, default the same 2 s).
+constexpr unsigned long long WAIT_LIMIT_NS = 2000000000ull;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -35,12 +39,13 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// bounded wait; false (and *err set) when the phase does not complete in time
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
+// bounded wait; false (and *err set) when the phase does not complete within limit_ns
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err,
+                                          unsigned long long limit_ns = WAIT_LIMIT_NS) {
     unsigned long long t0 = global_ns();
     while (!mbar_try(bar, parity)) {
         if (*reinterpret_cast<volatile int*>(err)) return false;
-        if (global_ns() - t0 > WAIT_LIMIT_NS) {
+        if (global_ns() - t0 > limit_ns) {
             atomicExch(err, 1);
             return false;
         }
@@ -61,24 +66,27 @@ __device__ __forceinline__ void mbar_expect_tx_only(uint64_t* bar, uint32_t byte
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
-// one bounded wait whose try_wait may suspend the thread up to SUSPEND_NS per
-// attempt, so a waiting warp does not spin on the issue slots
-__device__ __forceinline__ bool mbar_try_suspend(uint64_t* bar, uint32_t parity) {
+// one bounded wait whose try_wait may suspend the thread up to hint_ns per attempt,
+// so a waiting warp does not spin on the issue slots
+__device__ __forceinline__ bool mbar_try_suspend(uint64_t* bar, uint32_t parity, uint32_t hint_ns) {
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity), "r"(20000u)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
         : "memory");
     return ok != 0;
 }
-__device__ __forceinline__ bool mbar_wait_suspend(uint64_t* bar, uint32_t parity, int* err) {
+// the suspend hint is 20 us, or the limit when that is shorter
+__device__ __forceinline__ bool mbar_wait_suspend(uint64_t* bar, uint32_t parity, int* err,
+                                                  unsigned long long limit_ns = WAIT_LIMIT_NS) {
+    const uint32_t hint = limit_ns < 20000ull ? uint32_t(limit_ns) : 20000u;
     unsigned long long t0 = global_ns();
-    while (!mbar_try_suspend(bar, parity)) {
+    while (!mbar_try_suspend(bar, parity, hint)) {
         if (*reinterpret_cast<volatile int*>(err)) return false;
-        if (global_ns() - t0 > WAIT_LIMIT_NS) {
+        if (global_ns() - t0 > limit_ns) {
             atomicExch(err, 1);
             return false;
         }

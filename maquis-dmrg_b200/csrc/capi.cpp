@@ -72,6 +72,7 @@ struct dmrgb200_plan_s {
     uint64_t oz_scratch_size = 0;
     void* oz_scratch3 = nullptr;  // stage-3 digit planes
     uint64_t oz_scratch3_size = 0;
+    int* oz_err = nullptr;        // wait-timeout words of emulated stage 1 and stage 3
     // Jacobi-Davidson: solver mode and the cached solver graph
     int solver_mode = DMRGB200_SOLVER_GRAPH;
     void* jd = nullptr;
@@ -308,6 +309,11 @@ cudaError_t emu_prepare(dmrgb200_plan_s* plan) {
         plan->oz3 = oz_build(plan->prog.stage3);
         if (!plan->oz1 || !plan->oz3) return cudaErrorMemoryAllocation;
     }
+    if (!plan->oz_err) {
+        cudaError_t e = cudaMalloc(&plan->oz_err, 2 * sizeof(int));
+        if (e == cudaSuccess) e = cudaMemset(plan->oz_err, 0, 2 * sizeof(int));
+        if (e != cudaSuccess) return e;
+    }
     auto ensure = [&](OzProgram* oz, void*& buf, uint64_t& size) -> cudaError_t {
         const uint64_t need = oz_scratch_bytes(oz, plan->slices);
         if (need <= size) return cudaSuccess;
@@ -318,7 +324,7 @@ cudaError_t emu_prepare(dmrgb200_plan_s* plan) {
         cudaError_t e = cudaMalloc(&buf, need);
         if (e != cudaSuccess) return e;
         size = need;
-        return cudaMemset(oz_error_word(oz, buf, plan->slices), 0, sizeof(int));
+        return cudaSuccess;
     };
     cudaError_t e = ensure(plan->oz1, plan->oz_scratch, plan->oz_scratch_size);
     if (e == cudaSuccess) e = ensure(plan->oz3, plan->oz_scratch3, plan->oz_scratch3_size);
@@ -335,9 +341,9 @@ cudaError_t emu_launch(dmrgb200_plan_s* plan, const double* x, double* y, cudaSt
     bs.b[BUF_OUT] = reinterpret_cast<uint64_t>(y);
     bs.b[BUF_T] = reinterpret_cast<uint64_t>(plan->T);
     bs.b[BUF_S] = reinterpret_cast<uint64_t>(plan->S);
-    cudaError_t e = oz_run(plan->oz1, bs, plan->slices, plan->oz_scratch, st);
+    cudaError_t e = oz_run(plan->oz1, bs, plan->slices, plan->oz_scratch, plan->oz_err, st);
     if (e == cudaSuccess) e = run_sbuild(plan->prog, plan->T, plan->S, st);
-    if (e == cudaSuccess) e = oz_run(plan->oz3, bs, plan->slices, plan->oz_scratch3, st);
+    if (e == cudaSuccess) e = oz_run(plan->oz3, bs, plan->slices, plan->oz_scratch3, plan->oz_err + 1, st);
     return e;
 }
 
@@ -363,9 +369,8 @@ dmrgb200_status hpsi_emulated(dmrgb200_plan_s* plan, const double* x, double* y,
 int read_error_words(dmrgb200_plan_s* plan) {
     int bits = 0;
     if (plan->compiled && sbuild_timed_out(plan->prog)) bits |= 1;
-    auto oz_word = [&](OzProgram* oz, void* scratch) -> int {
-        if (!oz || !scratch) return 0;
-        int* w = oz_error_word(oz, scratch, plan->slices);
+    auto oz_word = [&](OzProgram* oz, int* w) -> int {
+        if (!oz || !w) return 0;
         int v = 0;
         if (cudaMemcpy(&v, w, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return 0;
         if (v) {
@@ -374,8 +379,8 @@ int read_error_words(dmrgb200_plan_s* plan) {
         }
         return v != 0;
     };
-    if (oz_word(plan->oz1, plan->oz_scratch)) bits |= 2;
-    if (oz_word(plan->oz3, plan->oz_scratch3)) bits |= 4;
+    if (plan->oz_err && oz_word(plan->oz1, plan->oz_err)) bits |= 2;
+    if (plan->oz_err && oz_word(plan->oz3, plan->oz_err + 1)) bits |= 4;
     return bits;
 }
 
@@ -569,6 +574,8 @@ dmrgb200_status dmrgb200_plan_destroy(dmrgb200_plan_t plan) {
     oz_free(plan->oz1);
     oz_free(plan->oz3);
     cudaFree(plan->oz_scratch);
+    cudaFree(plan->oz_scratch3);
+    cudaFree(plan->oz_err);
     for (auto& e : plan->ev)
         if (e) cudaEventDestroy(e);
     cudaFree(plan->T);
@@ -727,6 +734,11 @@ dmrgb200_status dmrgb200_plan_set_slices(dmrgb200_plan_t plan, int slices) {
         jd_graph_free(plan->jd);  // a captured emulated solve used the old digit planes
         plan->jd = nullptr;
     }
+    return DMRGB200_OK;
+}
+
+dmrgb200_status dmrgb200_set_wait_limit(uint64_t ns) {
+    g_wait_limit_ns.store(ns ? ns : 2000000000ull, std::memory_order_relaxed);
     return DMRGB200_OK;
 }
 

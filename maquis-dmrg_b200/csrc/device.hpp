@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <mutex>
 #include <set>
@@ -319,11 +320,10 @@ void oz_free(OzProgram* oz);
 void oz_invalidate(OzProgram* oz);
 // device bytes the program needs for s digit planes (digits, exponents, error flag)
 uint64_t oz_scratch_bytes(OzProgram const* oz, int s);
-// run on the stream with scratch of oz_scratch_bytes(oz, s); returns a CUDA error
-cudaError_t oz_run(OzProgram* oz, Bases const& bs, int s, void* scratch, cudaStream_t st);
-// device word that records pipeline-wait timeouts of the program's runs (not cleared by
-// oz_run; the reader clears it)
-int* oz_error_word(OzProgram const* oz, void* scratch, int s);
+// run on the stream with scratch of oz_scratch_bytes(oz, s); `err` is a device word that
+// records pipeline-wait timeouts (not cleared by oz_run; the reader clears it); returns a
+// CUDA error
+cudaError_t oz_run(OzProgram* oz, Bases const& bs, int s, void* scratch, int* err, cudaStream_t st);
 // the digit planes of the constant (boundary) operands are in the scratch
 bool oz_constants_ready(OzProgram const* oz);
 // out[0] = sum (a - b)^2, out[1] = sum b^2 over n elements (device scalars)
@@ -331,6 +331,11 @@ cudaError_t diff_norms(const double* a, const double* b, uint64_t n, double* out
 double calibrate_fp64_tflops();
 // solver graph cache of a plan (jd_graph.cu)
 void jd_graph_free(void* g);
+
+// Limit of the bounded waits for pipeline data (grouped S build, emulated stages), in
+// nanoseconds, read at every launch (dmrgb200_set_wait_limit).
+inline std::atomic<unsigned long long> g_wait_limit_ns{2000000000ull};
+inline unsigned long long wait_limit_ns() { return g_wait_limit_ns.load(std::memory_order_relaxed); }
 
 // Raise a kernel's dynamic shared-memory limit once per (device, kernel): the
 // attribute belongs to the kernel on the current device, so a process-wide flag

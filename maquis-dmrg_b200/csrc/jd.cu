@@ -205,8 +205,10 @@ extern "C" dmrgb200_status dmrgb200_solve(dmrgb200_plan_t plan, uint64_t n, cons
                                           void* cuda_stream) {
     dmrgb200_status s =
         dmrgb200::solve_stepwise(plan, n, x0, ortho, n_ortho, tol, max_iter, energy, x_out, stats, cuda_stream);
+    // a wait that ran out is the cause of whatever else went wrong in the solve (garbage H psi
+    // products can stop the iteration with a numeric error): it is reported first
     const int bits = plan ? dmrgb200::plan_error_words(plan) : 0;
-    if (s == DMRGB200_OK && bits)
+    if (bits)
         return noalloc_fail(DMRGB200_TIMEOUT, (bits & 1) ? "S build: a bulk-copy wait timed out"
                                                          : "emulated H psi: a pipeline wait timed out");
     return s;

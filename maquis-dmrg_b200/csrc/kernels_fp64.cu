@@ -396,7 +396,7 @@ __global__ void __launch_bounds__(32 * SGB_WARPS, SGB_MINB) sbuild_groups(const 
                                                                   const uint64_t* __restrict__ ent_t,
                                                                   const double* __restrict__ ent_a,
                                                                   double* __restrict__ S, const double* __restrict__ T,
-                                                                  int* err) {
+                                                                  int* err, unsigned long long wait_ns) {
     using namespace async;
     extern __shared__ __align__(16) unsigned char sgb_smem[];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -448,7 +448,7 @@ __global__ void __launch_bounds__(32 * SGB_WARPS, SGB_MINB) sbuild_groups(const 
                 fence_proxy_async_smem();
                 fill(kf);
             }
-            const bool ok = mbar_wait_suspend(&R.full[slot], (consumed / SGB_STAGES) & 1u, err);
+            const bool ok = mbar_wait_suspend(&R.full[slot], (consumed / SGB_STAGES) & 1u, err, wait_ns);
             if (__any_sync(0xffffffffu, !ok)) {
                 failed = true;
                 break;
@@ -1394,7 +1394,7 @@ cudaError_t run_sbuild(DeviceProgram const& prog, double* T, double* S, cudaStre
                                    static_cast<const DevSGroup*>(prog.d_groups), static_cast<const DevSItem*>(prog.d_gitems),
                                    prog.n_gitems, static_cast<const uint64_t*>(prog.d_gent_t),
                                    static_cast<const double*>(prog.d_gent_a), S, static_cast<const double*>(T),
-                                   prog.d_err);
+                                   prog.d_err, wait_limit_ns());
         if (e != cudaSuccess) return e;
     }
     return cudaGetLastError();

@@ -215,6 +215,7 @@ struct OzArgs {
     Bases bases;
     int* err;
     const DevRow* rowtab;
+    unsigned long long wait_ns;  // limit of the waits for operand slabs
 };
 
 __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_mma(OzArgs a) {
@@ -262,7 +263,8 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_mma(OzArgs a) {
         bool ok = true;  // thread 0's pipeline state over the tile's chunks
         auto load = [&](uint32_t kt) -> bool {
             const uint32_t gs = slab0 + kt, st = gs % OZ_STAGES;
-            if (gs >= OZ_STAGES && !mbar_wait(&empty[st], ((gs - OZ_STAGES) / OZ_STAGES) & 1u, a.err)) return false;
+            if (gs >= OZ_STAGES && !mbar_wait(&empty[st], ((gs - OZ_STAGES) / OZ_STAGES) & 1u, a.err, a.wait_ns))
+                return false;
             const OzSlab sl = a.slabs[pb.slab_begin + kt];
             unsigned char* base = smem + st * stage_bytes;
             mbar_expect_tx(&full[st], stage_bytes);
@@ -282,7 +284,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_mma(OzArgs a) {
                     for (uint32_t kt = 0; kt < KT && kt < OZ_STAGES && ok; ++kt) ok = load(kt);
                 for (uint32_t kt = k_begin; kt < k_end && ok; ++kt) {
                     const uint32_t gs = slab0 + kt, st = gs % OZ_STAGES;
-                    ok = mbar_wait(&full[st], (gs / OZ_STAGES) & 1u, a.err);
+                    ok = mbar_wait(&full[st], (gs / OZ_STAGES) & 1u, a.err, a.wait_ns);
                     if (!ok) break;
                     ++consumed;
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -303,7 +305,18 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_mma(OzArgs a) {
                 umma_commit(done);  // arrives once every MMA issued so far has completed
             }
             __syncwarp();
-            const bool ready = mbar_wait(done, rounds & 1u, a.err);
+            // the MMAs issued so far always complete: their wait keeps the fixed limit even when
+            // the error word is set, so TMEM is never released under a running MMA
+            bool ready = true;
+            {
+                const unsigned long long t0 = global_ns();
+                while (!mbar_try(done, rounds & 1u))
+                    if (global_ns() - t0 > WAIT_LIMIT_NS) {
+                        atomicExch(a.err, 1);
+                        ready = false;
+                        break;
+                    }
+            }
             ++rounds;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const bool go = __all_sync(0xffffffffu, ready && *verr == 0);
@@ -519,7 +532,6 @@ struct OzScratch {
     int8_t* A8;
     int8_t* B8;
     int* e;
-    int* err;
 };
 OzScratch carve(OzProgram const* oz, int s, void* scratch) {
     auto* p = static_cast<unsigned char*>(scratch);
@@ -529,18 +541,16 @@ OzScratch carve(OzProgram const* oz, int s, void* scratch) {
     c.B8 = reinterpret_cast<int8_t*>(p);
     p += round_up(uint64_t(s) * oz->b_plane, 256);
     c.e = reinterpret_cast<int*>(p);
-    p += round_up(oz->n_exp * sizeof(int), 256);
-    c.err = reinterpret_cast<int*>(p);
     return c;
 }
 }  // namespace
 
 uint64_t oz_scratch_bytes(OzProgram const* oz, int s) {
     return round_up(uint64_t(s) * oz->a_plane, 256) + round_up(uint64_t(s) * oz->b_plane, 256) +
-           round_up(oz->n_exp * sizeof(int), 256) + 256;
+           round_up(oz->n_exp * sizeof(int), 256);
 }
 
-cudaError_t oz_run(OzProgram* oz, Bases const& bs, int s, void* scratch, cudaStream_t st) {
+cudaError_t oz_run(OzProgram* oz, Bases const& bs, int s, void* scratch, int* err, cudaStream_t st) {
     if (s < 2 || s > OZ_MAX_SLICES) return cudaErrorInvalidValue;
     OzScratch c = carve(oz, s, scratch);
     const int sms = device_sm_count();
@@ -564,14 +574,12 @@ cudaError_t oz_run(OzProgram* oz, Bases const& bs, int s, void* scratch, cudaStr
         cudaError_t ea = ensure_smem_limit(reinterpret_cast<const void*>(ozaki_mma), int(ozaki_smem_bytes(OZ_MAX_SLICES)));
         if (ea != cudaSuccess) return ea;
         OzArgs args{c.A8, c.B8, oz->a_plane, oz->b_plane, c.e, oz->d_pbs, oz->d_slabs, oz->d_tiles,
-                    uint32_t(oz->tiles.size()), oz_chunk_slabs(s), s, bs, c.err, oz->d_rowtab};
+                    uint32_t(oz->tiles.size()), oz_chunk_slabs(s), s, bs, err, oz->d_rowtab, wait_limit_ns()};
         ozaki_mma<<<std::min<uint32_t>(uint32_t(oz->tiles.size()), uint32_t(sms)), OZ_THREADS, ozaki_smem_bytes(s),
                     st>>>(args);
     }
     return cudaGetLastError();
 }
-
-int* oz_error_word(OzProgram const* oz, void* scratch, int s) { return carve(oz, s, scratch).err; }
 
 bool oz_constants_ready(OzProgram const* oz) { return oz && oz->const_ready; }
 
@@ -636,16 +644,18 @@ extern "C" dmrgb200_status dmrgb200_dgemm_emulated(uint32_t M, uint32_t N, uint3
     OzProgram* oz = oz_build(gl);
     if (!oz) return noalloc_fail(DMRGB200_OUT_OF_MEMORY, "emulated GEMM tables");
     void* scratch = nullptr;
-    cudaError_t r = cudaMallocAsync(&scratch, oz_scratch_bytes(oz, slices), st);
+    const uint64_t sbytes = oz_scratch_bytes(oz, slices);
+    cudaError_t r = cudaMallocAsync(&scratch, sbytes + 256, st);
     if (r != cudaSuccess) {
         oz_free(oz);
         return noalloc_fail(DMRGB200_OUT_OF_MEMORY, cudaGetErrorString(r));
     }
+    int* err = reinterpret_cast<int*>(static_cast<unsigned char*>(scratch) + sbytes);
     Bases bs{};
     int to = 0;
-    cudaMemsetAsync(oz_error_word(oz, scratch, slices), 0, sizeof(int), st);
-    r = oz_run(oz, bs, slices, scratch, st);
-    cudaMemcpyAsync(&to, oz_error_word(oz, scratch, slices), sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaMemsetAsync(err, 0, sizeof(int), st);
+    r = oz_run(oz, bs, slices, scratch, err, st);
+    cudaMemcpyAsync(&to, err, sizeof(int), cudaMemcpyDeviceToHost, st);
     cudaError_t r2 = cudaStreamSynchronize(st);
     cudaFreeAsync(scratch, st);
     cudaStreamSynchronize(st);

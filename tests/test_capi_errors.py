@@ -78,3 +78,20 @@ def test_noalloc_rejects_plans_beyond_its_static_area():
     assert st == 3, (st, msg)  # DMRGB200_OUT_OF_MEMORY
     assert "bytes of scratch" in msg and str(64 << 20) in msg, msg
     del keep
+
+
+def test_library_exports_every_declared_entry_point():
+    """Every function include/dmrgb200.h declares is exported by libdmrgb200.so and has
+    a ctypes signature in the binding (loading needs no GPU)."""
+    import ctypes
+    import re
+    from pathlib import Path
+
+    header = (Path(__file__).resolve().parent.parent / "include" / "dmrgb200.h").read_text()
+    names = set(re.findall(r"^\s*(?:const\s+)?\w+\*?\s+\*?(dmrgb200_\w+)\s*\(", header, re.M))
+    assert len(names) > 40, names
+    lib = ctypes.CDLL(str(capi.LIB_PATH))
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+    unbound = [n for n in sorted(names) if n not in capi.EXPORTED]
+    assert not unbound, unbound

@@ -39,11 +39,28 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
+// non-blocking test of the phase (try_wait may block for a hardware-chosen time, longer
+// than a short limit)
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// limits below this are honoured with non-blocking tests instead of try_wait
+constexpr unsigned long long SHORT_LIMIT_NS = 20000ull;
+
 // bounded wait; false (and *err set) when the phase does not complete within limit_ns
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err,
                                           unsigned long long limit_ns = WAIT_LIMIT_NS) {
     unsigned long long t0 = global_ns();
-    while (!mbar_try(bar, parity)) {
+    const bool poll = limit_ns < SHORT_LIMIT_NS;
+    while (!(poll ? mbar_test(bar, parity) : mbar_try(bar, parity))) {
         if (*reinterpret_cast<volatile int*>(err)) return false;
         if (global_ns() - t0 > limit_ns) {
             atomicExch(err, 1);
@@ -79,12 +96,12 @@ __device__ __forceinline__ bool mbar_try_suspend(uint64_t* bar, uint32_t parity,
         : "memory");
     return ok != 0;
 }
-// the suspend hint is 20 us, or the limit when that is shorter
+// try_wait suspends the warp up to 20 us per attempt; short limits poll instead
 __device__ __forceinline__ bool mbar_wait_suspend(uint64_t* bar, uint32_t parity, int* err,
                                                   unsigned long long limit_ns = WAIT_LIMIT_NS) {
-    const uint32_t hint = limit_ns < 20000ull ? uint32_t(limit_ns) : 20000u;
+    const bool poll = limit_ns < SHORT_LIMIT_NS;
     unsigned long long t0 = global_ns();
-    while (!mbar_try_suspend(bar, parity, hint)) {
+    while (!(poll ? mbar_test(bar, parity) : mbar_try_suspend(bar, parity, 20000u))) {
         if (*reinterpret_cast<volatile int*>(err)) return false;
         if (global_ns() - t0 > limit_ns) {
             atomicExch(err, 1);

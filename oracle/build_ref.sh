@@ -25,6 +25,7 @@ for f in gpu_dgemm_ddot gpu_vgemm; do
       -I"$HERE/shim" -I"$REF" -c "$REF/dmrg/solver/numeric/$f.cu" -o "$OUT/$f.o"
 done
 $CXX -c "$HERE/ref_adapter.cpp" -o "$OUT/ref_adapter.o"
+$CXX -c "$HERE/ref_flatten.cpp" -o "$OUT/ref_flatten.o"
 g++ -shared -fopenmp -o "$OUT/libmaquis_ref.so" "$OUT"/*.o -L"$BLAS_DIR" -l:"$BLAS_LIB" -Wl,-rpath,"$BLAS_DIR" \
     -L/usr/local/cuda/lib64 -lcudart -lcublas -Wl,-rpath,/usr/local/cuda/lib64
 rm -f "$OUT"/*.o

@@ -33,6 +33,8 @@ def lib():
         _lib.ref_hpsi_create.restype = C.c_void_p
         _lib.ref_hpsi_run.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         _lib.ref_hpsi_destroy.argtypes = [C.c_void_p]
+        _lib.ref_hpsi_flatten.argtypes = [C.c_void_p]
+        _lib.ref_hpsi_flatten.restype = C.POINTER(capi.PlanDesc)
     return _lib
 
 
@@ -76,6 +78,13 @@ class Hpsi:
         y = np.zeros(self.out_size) if y is None else y
         assert lib().ref_hpsi_run(self._h, np.ascontiguousarray(x).ctypes.data, y.ctypes.data) == 0
         return y
+
+    def flatten(self) -> dict:
+        """The reference's ScheduleNew flattened back into a plan description (ref_flatten.cpp),
+        copied into numpy arrays."""
+        d = lib().ref_hpsi_flatten(self._h)
+        assert d
+        return capi.desc_to_numpy(d.contents)
 
     def __del__(self):
         if getattr(self, "_h", None):

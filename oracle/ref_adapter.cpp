@@ -113,10 +113,22 @@ int ref_hpsi(const dmrgb200_plan_desc* dp, uint32_t nR, const uint32_t* R_lsz, c
 // for every Davidson iteration (site_hamil_schedule.hpp:40-93,
 // solver_interface.hpp:30-77); ref_hpsi_run then times only create_T and
 // contract (super_hamil_mv.hpp:121-132).
+struct RefFlat;
+void ref_flatten_hpsi(ScheduleNew<double> const& sched, BoundaryIndexRT const& right_rt,
+                      std::vector<uint32_t> const& in_rows, std::vector<uint32_t> const& in_cols,
+                      std::vector<uint64_t> const& in_off, uint64_t in_size, std::vector<uint32_t> const& out_rows,
+                      std::vector<uint32_t> const& out_cols, std::vector<uint64_t> const& out_off, uint64_t out_size,
+                      RefFlat& f);
+RefFlat* ref_flat_new();
+void ref_flat_delete(RefFlat* f);
+const dmrgb200_plan_desc* ref_flat_desc(RefFlat* f);
+
 struct RefHpsi {
-    std::vector<uint32_t> in_rows;
+    std::vector<uint32_t> in_rows, in_cols;
     std::vector<uint64_t> in_off, out_off;
     std::vector<uint32_t> out_rows, out_cols;
+    uint64_t in_size = 0, out_size = 0;
+    RefFlat* flat = nullptr;
     BoundaryIndexRT rrt, lrt;
     std::unique_ptr<ScheduleNew<double>> tasks;
     std::vector<const double*> lv, rv;
@@ -129,6 +141,10 @@ void* ref_hpsi_create(const dmrgb200_plan_desc* dp, uint32_t nR, const uint32_t*
     if (d.kind != DMRGB200_PLAN_HPSI) return nullptr;
     auto* h = new RefHpsi;
     h->in_off.assign(d.in_off, d.in_off + d.n_in_blocks);
+    h->in_rows.assign(d.in_rows, d.in_rows + d.n_in_blocks);
+    h->in_cols.assign(d.in_cols, d.in_cols + d.n_in_blocks);
+    h->in_size = d.in_size;
+    h->out_size = d.out_size;
     h->out_off.assign(d.out_off, d.out_off + d.n_out_blocks);
     h->out_rows.assign(d.out_rows, d.out_rows + d.n_out_blocks);
     h->out_cols.assign(d.out_cols, d.out_cols + d.n_out_blocks);
@@ -159,7 +175,22 @@ int ref_hpsi_run(void* handle, const double* x, double* y) {
     return 0;
 }
 
-void ref_hpsi_destroy(void* handle) { delete static_cast<RefHpsi*>(handle); }
+void ref_hpsi_destroy(void* handle) {
+    auto* h = static_cast<RefHpsi*>(handle);
+    if (h) ref_flat_delete(h->flat);
+    delete h;
+}
+
+// The handle's ScheduleNew flattened back into a plan description (ref_flatten.cpp);
+// the arrays live until the handle is destroyed.
+const dmrgb200_plan_desc* ref_hpsi_flatten(void* handle) {
+    auto* h = static_cast<RefHpsi*>(handle);
+    if (!h) return nullptr;
+    if (!h->flat) h->flat = ref_flat_new();
+    ref_flatten_hpsi(*h->tasks, h->rrt, h->in_rows, h->in_cols, h->in_off, h->in_size, h->out_rows, h->out_cols,
+                     h->out_off, h->out_size, *h->flat);
+    return ref_flat_desc(h->flat);
+}
 
 int ref_left_step(const dmrgb200_plan_desc* dp, uint32_t nL, const uint32_t* L_lsz, const uint32_t* L_rsz,
                   const uint32_t* L_nb, const double* const* L, const double* ket, const double* bra,

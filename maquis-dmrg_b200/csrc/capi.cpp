@@ -90,6 +90,21 @@ struct dmrgb200_plan_s {
     cudaGraphExec_t pipe_exec = nullptr;
     const double* pipe_x = nullptr;
     double* pipe_y = nullptr;
+    // boundary step: the lowered program of the last output binding, its T / S scratch
+    // (reused while a caller keeps writing the same output boundary buffer)
+    bool step_valid = false;
+    std::vector<uint64_t> step_outp;
+    DeviceProgram step_prog;
+    double* step_T = nullptr;
+    double* step_S = nullptr;
+    void drop_step() {
+        if (step_valid) free_program(step_prog);
+        cudaFree(step_T);
+        cudaFree(step_S);
+        step_T = step_S = nullptr;
+        step_valid = false;
+        step_outp.clear();
+    }
     // adjoint program (built on first use)
     bool adj_built = false;
     std::string adj_err;
@@ -256,41 +271,57 @@ dmrgb200_status finish_plan(std::unique_ptr<dmrgb200_plan_s>& p, dmrgb200_plan_t
     return DMRGB200_OK;
 }
 
-// Execute a step plan whose output cohort pointers are `outp`; scratch and the
-// lowered program live only for this call.
+// Execute a step plan whose output cohort pointers are `outp`.  The lowered program
+// (row-stacked stage 1 for right steps, grouped S build) and its T / S scratch are
+// kept with the plan and reused while the output binding stays the same, so a sweep
+// that rewrites one boundary buffer per bond lowers each step once; the grouped GEMMs
+// of a program of at least 50 MFLOP are autotuned once.  Synchronises the stream.
+bool capturing(cudaStream_t st);
+
 dmrgb200_status run_step(dmrgb200_plan_s* p, const double* ket, const double* bra, std::vector<uint64_t> const& outp,
                          cudaStream_t stream) {
     for (uint32_t c = 0; c < p->flat.n_cohorts(); ++c)
         if (p->flat.c_out_ci[c] >= outp.size() || !outp[p->flat.c_out_ci[c]])
             return fail(DMRGB200_INVALID_ARGUMENT, "output boundary view misses a cohort");
-    DeviceProgram prog;
-    compile_program(p->flat, {}, p->stage1_bnd, outp, prog, false, true);
-    cudaError_t e = upload_program(prog);
-    if (e != cudaSuccess) {
-        free_program(prog);
-        return cuda_fail(e, "step plan upload");
+    cudaError_t e;
+    if (!p->step_valid || p->step_outp != outp) {
+        p->drop_step();
+        compile_program(p->flat, {}, p->stage1_bnd, outp, p->step_prog, true, true);
+        if ((e = upload_program(p->step_prog)) != cudaSuccess) {
+            free_program(p->step_prog);
+            return cuda_fail(e, "step plan upload");
+        }
+        p->step_valid = true;
+        p->step_outp = outp;
+        if (p->step_prog.t_elems && (e = cudaMalloc(&p->step_T, p->step_prog.t_elems * sizeof(double))) != cudaSuccess) {
+            p->drop_step();
+            return cuda_fail(e, "step T scratch");
+        }
+        if (p->step_prog.s_elems && (e = cudaMalloc(&p->step_S, p->step_prog.s_elems * sizeof(double))) != cudaSuccess) {
+            p->drop_step();
+            return cuda_fail(e, "step S scratch");
+        }
+        static const bool tune = [] {
+            const char* v = std::getenv("DMRGB200_AUTOTUNE");
+            return !(v && v[0] == '0');
+        }();
+        if (tune && p->flat.flops() >= 50000000ull && !capturing(stream)) {
+            // the variants run the whole step (outputs included): the run below rewrites them
+            if ((e = tune_program(p->step_prog, reinterpret_cast<uint64_t>(ket), reinterpret_cast<uint64_t>(bra),
+                                  p->step_T, p->step_S, stream)) != cudaSuccess) {
+                p->drop_step();
+                return cuda_fail(e, "step autotuning");
+            }
+        }
     }
-    double *T = nullptr, *S = nullptr;
-    if (prog.t_elems && (e = cudaMallocAsync(&T, prog.t_elems * sizeof(double), stream)) != cudaSuccess) {
-        free_program(prog);
-        return cuda_fail(e, "step T scratch");
-    }
-    if (prog.s_elems && (e = cudaMallocAsync(&S, prog.s_elems * sizeof(double), stream)) != cudaSuccess) {
-        cudaFreeAsync(T, stream);
-        free_program(prog);
-        return cuda_fail(e, "step S scratch");
-    }
-    e = run_program(prog, reinterpret_cast<uint64_t>(ket), reinterpret_cast<uint64_t>(bra), T, S, stream,
-                    p->timing ? p->ev : nullptr);
-    cudaFreeAsync(T, stream);
-    cudaFreeAsync(S, stream);
+    e = run_program(p->step_prog, reinterpret_cast<uint64_t>(ket), reinterpret_cast<uint64_t>(bra), p->step_T,
+                    p->step_S, stream, p->timing ? p->ev : nullptr);
     cudaError_t e2 = cudaStreamSynchronize(stream);
     if (p->timing && e == cudaSuccess && e2 == cudaSuccess) {
         p->pending = true;  // the device time of the three stages, without the host-side lowering
         p->collect();
     }
-    const bool timed_out = e2 == cudaSuccess && sbuild_timed_out(prog);
-    free_program(prog);
+    const bool timed_out = e2 == cudaSuccess && sbuild_timed_out(p->step_prog);
     if (e != cudaSuccess) return cuda_fail(e, "step launch");
     if (e2 != cudaSuccess) return cuda_fail(e2, "step execution");
     if (timed_out) return fail(DMRGB200_TIMEOUT, "step S build: a bulk-copy wait timed out");
@@ -571,6 +602,7 @@ dmrgb200_status dmrgb200_plan_destroy(dmrgb200_plan_t plan) {
         if (plan->capture_stream) cudaStreamDestroy(plan->capture_stream);
     }
     jd_graph_free(plan->jd);
+    plan->drop_step();
     oz_free(plan->oz1);
     oz_free(plan->oz3);
     cudaFree(plan->oz_scratch);

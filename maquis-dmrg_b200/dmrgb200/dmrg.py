@@ -383,7 +383,7 @@ class DeviceBackend:
     H·psi plans and the Jacobi-Davidson solver (dmrgb200_solve)."""
 
     def __init__(self, ctx: E.Context, precision: int = capi.PREC_FP64, slices: int | None = None,
-                 slice_target: float = 1e-10):
+                 slice_target: float = 1e-10, reuse_plans: bool = True):
         """precision: of the H·psi inside every solve (capi.PREC_FP64 or capi.PREC_FP64_EMULATED:
         contractions on the INT8 tensor cores, orthogonalisation, Rayleigh-Ritz and energies in
         FP64).  Emulated solves use `slices` digit planes, or, with slices None, the smallest
@@ -392,6 +392,15 @@ class DeviceBackend:
         import torch
         self.torch, self.ctx = torch, ctx
         self.precision, self.slices, self.slice_target = precision, slices, slice_target
+        # reuse_plans: one cached (schedule, device plan, output buffer) per site and kind,
+        # reused while the site's bond sectors and input boundary stay the same -- in the
+        # sweeps after the bond dimensions have settled every schedule, lowered step
+        # program and captured solver graph is reused (the reference rebuilds its
+        # schedules at every site of every sweep, site_hamil_schedule.hpp:40-93)
+        self.reuse_plans = reuse_plans
+        self.cache = {}
+        self.cache_hits = 0
+        self.cache_misses = 0
         self.slices_used = []  # (digit planes, relative H·psi error of the start vector) per emulated solve
         # host seconds per phase of the site problems (schedule building, plan lowering, solve)
         self.phase_seconds = {"schedule": 0.0, "plan": 0.0, "solve": 0.0}
@@ -405,20 +414,34 @@ class DeviceBackend:
         left-paired) when the split left them on the device."""
         dev = self.ctx.device
         t0 = time.perf_counter()
+        site_key = ("L" if left else "R", id(W))
+        full_key = (id(idx), buf.data_ptr(), tuple(t.left), tuple(t.right))
+        hit = self.cache.get(site_key) if self.reuse_plans else None
+        if hit is not None and hit[0] == full_key:
+            _, idx_keep, nidx, plan, out = hit
+            self.cache_hits += 1
+        else:
+            if left:
+                sched, nidx = E.schedule_left_step(model.phys, t.left, t.right, W, idx, True)
+                plan = E.DevicePlan(self.ctx, sched.plan, left_addr=idx.cohort_addresses(buf.data_ptr()))
+            else:
+                sched, nidx = E.schedule_right_step(model.phys, t.left, t.right, W, idx, True)
+                plan = E.DevicePlan(self.ctx, sched.plan, other_addr=idx.cohort_addresses(buf.data_ptr()))
+            out = self.torch.zeros(max(nidx.n_elems, 1), dtype=self.torch.float64, device=buf.device)
+            self.cache_misses += 1
+            if self.reuse_plans:
+                # idx is kept alive with the entry, so its id cannot be reused by another index
+                self.cache[site_key] = (full_key, idx, nidx, plan, out)
         if left:
-            sched, nidx = E.schedule_left_step(model.phys, t.left, t.right, W, idx, True)
-            plan = E.DevicePlan(self.ctx, sched.plan, left_addr=idx.cohort_addresses(buf.data_ptr()))
             ket = dev_rp if dev_rp is not None else E.to_device(t.data, dev)
             bra = dev_lp if dev_lp is not None else E.to_device(t.left_paired(), dev)
         else:
-            sched, nidx = E.schedule_right_step(model.phys, t.left, t.right, W, idx, True)
-            plan = E.DevicePlan(self.ctx, sched.plan, other_addr=idx.cohort_addresses(buf.data_ptr()))
             ket = bra = dev_rp if dev_rp is not None else E.to_device(t.data, dev)
-        out = self.torch.zeros(max(nidx.n_elems, 1), dtype=self.torch.float64, device=buf.device)
         t1 = time.perf_counter()
         plan.step(ket.data_ptr(), bra.data_ptr(), nidx.cohort_addresses(out.data_ptr()))
         t2 = time.perf_counter()
-        del plan
+        if not self.reuse_plans:
+            del plan
         t3 = time.perf_counter()
         ph = self.phase_seconds
         ph["step_schedule"] = ph.get("step_schedule", 0.0) + t1 - t0
@@ -436,23 +459,37 @@ class DeviceBackend:
         """Lowest eigenpair of the site problem; the eigenvector comes back as a
         host array, or as the device tensor with keep_on_device."""
         t0 = time.perf_counter()
-        sched = E.schedule_hpsi(p12, psi.left, psi.right, W12, Lidx, Ridx)
-        t1 = time.perf_counter()
-        plan = E.DevicePlan(self.ctx, sched.plan, left_addr=Lidx.cohort_addresses(Lbuf.data_ptr()),
-                            other_addr=Ridx.cohort_addresses(Rbuf.data_ptr()))
-        t2 = time.perf_counter()
+        site_key = ("H", id(W12))
+        full_key = (id(Lidx), id(Ridx), Lbuf.data_ptr(), Rbuf.data_ptr(), tuple(psi.left), tuple(psi.right))
+        hit = self.cache.get(site_key) if self.reuse_plans else None
+        if hit is not None and hit[0] == full_key:
+            plan = hit[3]
+            self.cache_hits += 1
+            t1 = t2 = time.perf_counter()
+        else:
+            sched = E.schedule_hpsi(p12, psi.left, psi.right, W12, Lidx, Ridx)
+            t1 = time.perf_counter()
+            plan = E.DevicePlan(self.ctx, sched.plan, left_addr=Lidx.cohort_addresses(Lbuf.data_ptr()),
+                                other_addr=Ridx.cohort_addresses(Rbuf.data_ptr()))
+            t2 = time.perf_counter()
+            self.cache_misses += 1
+            if self.reuse_plans:
+                self.cache[site_key] = (full_key, Lidx, Ridx, plan)
         xd = E.to_device(psi.data, self.ctx.device)
         xo = self.torch.zeros_like(xd)
-        if self.precision == capi.PREC_FP64_EMULATED:
+        if self.precision == capi.PREC_FP64_EMULATED and not getattr(plan, "emulation_set", False):
+            # once per plan: a reused plan keeps its slice count (and its captured solver graph)
             if self.slices is None:
                 self.slices_used.append(plan.tune_slices(xd.data_ptr(), self.slice_target))
             else:
                 plan.set_slices(self.slices)
             plan.set_precision(capi.PREC_FP64_EMULATED)
+            plan.emulation_set = True
         energy, st = plan.solve(xd.data_ptr(), xo.data_ptr(), xd.numel(), tol=tol, max_iter=max_iter)
         out = xo if keep_on_device else xo.cpu().numpy()
         t3 = time.perf_counter()
-        del plan
+        if not self.reuse_plans:
+            del plan
         t4 = time.perf_counter()
         self.phase_seconds["schedule"] += t1 - t0
         self.phase_seconds["plan"] += t2 - t1

@@ -885,6 +885,34 @@ def main():
         emu_err = str(exc)
     yd.copy_(y64)
 
+    # the reference's launch pattern on the same plan (one library DGEMM per T task and per
+    # cohort, dmrgb200_hpsi_per_block): what batching every block product into one launch
+    # per stage gains
+    per_block = {}
+    try:
+        nl = C.c_uint64()
+        for _ in range(2):
+            capi.check(capi.lib.dmrgb200_hpsi_per_block(sp.plan.handle, xd.data_ptr(), yd.data_ptr(), sh,
+                                                        C.byref(nl)), "hpsi_per_block")
+        pb_ms = []
+        for k in range(min(args.steps, 10)):
+            flush.fill_(float(k))
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            capi.check(capi.lib.dmrgb200_hpsi_per_block(sp.plan.handle, xd.data_ptr(), yd.data_ptr(), sh,
+                                                        C.byref(nl)), "hpsi_per_block")
+            b.record(stream)
+            b.synchronize()
+            pb_ms.append(a.elapsed_time(b))
+        per_block = {"ms_per_step": statistics.mean(pb_ms), "value": flops / (statistics.mean(pb_ms) * 1e-3) / 1e9,
+                     "unit": "GFLOP/s", "launches_per_step": int(nl.value),
+                     "rel_err_vs_grouped": float(torch.linalg.norm(yd - y64) / torch.linalg.norm(y64)),
+                     "note": "one cuBLAS DGEMM per T task and per cohort (the reference's create_T_gpu / "
+                             "contract_gpu pattern) and the library's S build, one stream"}
+    except capi.DmrgError as exc:  # reported, not hidden
+        per_block = {"unavailable": str(exc)}
+    yd.copy_(y64)
+
     # Jacobi-Davidson solve of this site problem, 8 iterations (the reference's
     # ietl_jcd_maxiter; tol 0 so that every iteration runs): the graph-captured solver
     # against the stepwise one (host reads the scalars each iteration)
@@ -1014,6 +1042,7 @@ def main():
                          "stage_ms": stage_ms, "stage_flops": [int(f) for f in fl3],
                          "fp64_dmma_peak_tflops": fp64_peak.value},
             "jd_solve": jd,
+            "per_block_launches": per_block,
             "autotune": autotune,
             "cpu_baseline": cpu,
             "max_rel_err_vs_cpu": err,

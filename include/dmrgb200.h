@@ -207,6 +207,17 @@ dmrgb200_status dmrgb200_plan_scratch_bytes(dmrgb200_plan_t plan, uint64_t* byte
 dmrgb200_status dmrgb200_hpsi(dmrgb200_plan_t plan, const double* x, double* y, dmrgb200_precision prec,
                               void* cuda_stream);
 
+/* H·psi with the reference's launch pattern, for comparison with the grouped
+ * kernels: one cuBLAS DGEMM per T task (per stored block for transposed cohorts)
+ * as MPSBlock::create_T_gpu (dmrg/framework/dmrg/solver/tasks.cpp:707-752), the
+ * library's S build, and one cuBLAS DGEMM per cohort into its output block as
+ * Cohort::contract_gpu (tasks.cpp:315-344), all on cuda_stream.  y's block
+ * elements are overwritten.  *launches (may be NULL) receives the number of
+ * launches made.  Same sums as dmrgb200_hpsi up to the addition order inside
+ * the library GEMMs. */
+dmrgb200_status dmrgb200_hpsi_per_block(dmrgb200_plan_t plan, const double* x, double* y, void* cuda_stream,
+                                        uint64_t* launches);
+
 /* Autotuning of the grouped FP64 GEMMs: every variant (pipeline depth x CTAs
  * per SM) is timed on the plan's stage-1 and stage-3 tile lists and the
  * fastest is kept per stage.  The first FP64 dmrgb200_hpsi / dmrgb200_solve of

@@ -18,7 +18,7 @@ OUT = HERE / "dmrgb200" / "libdmrgb200.so"
 INCLUDE = HERE.parent / "include"
 CUDA = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 
-CXX_SOURCES = ["coupling.cpp", "schedule.cpp", "plan.cpp", "capi.cpp"]
+CXX_SOURCES = ["coupling.cpp", "schedule.cpp", "plan.cpp", "capi.cpp", "per_block.cpp"]
 CU_SOURCES = ["kernels_fp64.cu", "noalloc.cu", "jd.cu", "jd_graph.cu", "ozaki.cu", "adjoint.cu", "block_svd.cu"]
 HEADERS = ["symm.hpp", "mpo.hpp", "coupling.hpp", "boundary_index.hpp", "schedule.hpp", "plan.hpp",
            "device.hpp", "async_copy.cuh"]
@@ -60,7 +60,7 @@ def build(force: bool = False) -> Path:
                  log=BUILD / (src + ".ptxas.txt"))
         objs.append(obj)
     if force or _stale(OUT, objs):
-        _run(["g++", "-shared", "-o", str(OUT), *map(str, objs), f"-L{CUDA}/lib64", "-lcudart", "-fopenmp",
+        _run(["g++", "-shared", "-o", str(OUT), *map(str, objs), f"-L{CUDA}/lib64", "-lcudart", "-lcublas", "-fopenmp",
               f"-Wl,-rpath,{CUDA}/lib64"])
     return OUT
 

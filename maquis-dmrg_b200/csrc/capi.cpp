@@ -105,6 +105,8 @@ struct dmrgb200_plan_s {
         step_valid = false;
         step_outp.clear();
     }
+    // cuBLAS handle of the per-block comparison path (dmrgb200_hpsi_per_block)
+    void* blas = nullptr;
     // adjoint program (built on first use)
     bool adj_built = false;
     std::string adj_err;
@@ -472,6 +474,13 @@ cudaError_t plan_ensure_tuned(dmrgb200_plan_t plan, const double* x, double* y, 
                         stream);
 }
 void** plan_jd_cache(dmrgb200_plan_t plan) { return &plan->jd; }
+FlatPlan const& plan_flat(dmrgb200_plan_t plan) { return plan->flat; }
+DeviceProgram const& plan_program(dmrgb200_plan_t plan) { return plan->prog; }
+std::vector<uint64_t> const& plan_stage1_bnd(dmrgb200_plan_t plan) { return plan->stage1_bnd; }
+std::vector<uint64_t> const& plan_stage3_bnd(dmrgb200_plan_t plan) { return plan->stage3_bnd; }
+double* plan_T(dmrgb200_plan_t plan) { return plan->compiled ? plan->T : nullptr; }
+double* plan_S(dmrgb200_plan_t plan) { return plan->S; }
+void*& plan_blas_handle(dmrgb200_plan_t plan) { return plan->blas; }
 }  // namespace dmrgb200
 
 extern "C" {
@@ -602,6 +611,7 @@ dmrgb200_status dmrgb200_plan_destroy(dmrgb200_plan_t plan) {
         if (plan->capture_stream) cudaStreamDestroy(plan->capture_stream);
     }
     jd_graph_free(plan->jd);
+    blas_handle_free(plan->blas);
     plan->drop_step();
     oz_free(plan->oz1);
     oz_free(plan->oz3);

@@ -331,6 +331,8 @@ cudaError_t diff_norms(const double* a, const double* b, uint64_t n, double* out
 double calibrate_fp64_tflops();
 // solver graph cache of a plan (jd_graph.cu)
 void jd_graph_free(void* g);
+// cuBLAS handle of the per-block comparison path (per_block.cpp)
+void blas_handle_free(void* h);
 
 // Limit of the bounded waits for pipeline data (grouped S build, emulated stages), in
 // nanoseconds, read at every launch (dmrgb200_set_wait_limit).

@@ -282,6 +282,13 @@ dmrgb200_status dmrgb200_plan_check(dmrgb200_plan_t plan, void* cuda_stream);
  * device. */
 dmrgb200_status dmrgb200_set_wait_limit(uint64_t ns);
 
+/* The boundary buffers bound to the plan were rewritten in place (a sweep that
+ * keeps one buffer per bond and reuses the plan): the emulated path drops the digit
+ * planes it keeps of the boundaries and makes them again on its next call (FP64
+ * execution keeps nothing derived from the boundary values).  No counterpart in
+ * the reference, which rebuilds its schedules at every site. */
+dmrgb200_status dmrgb200_plan_boundaries_changed(dmrgb200_plan_t plan);
+
 /* Precision of the H·psi inside dmrgb200_solve (default DMRGB200_PREC_FP64):
  * with DMRGB200_PREC_FP64_EMULATED the contractions of every H·psi run emulated
  * on the INT8 tensor cores while orthogonalisation, Rayleigh-Ritz, residuals and

@@ -444,6 +444,15 @@ cudaError_t plan_hpsi_launch(dmrgb200_plan_t plan, const double* x, double* y, c
 void noalloc_desc_to_flat(const dmrgb200_plan_desc* d, FlatPlan& f) { desc_to_flat(d, f); }
 int plan_solver_mode(dmrgb200_plan_t plan) { return plan->solver_mode; }
 int plan_error_words(dmrgb200_plan_t plan) { return read_error_words(plan); }
+// Before a solve: an emulated plan whose boundary digit planes were dropped (new boundary
+// values) makes them again eagerly, outside the solver graph (which only splits psi and S);
+// x is read and y written as scratch.
+cudaError_t plan_refresh_constants(dmrgb200_plan_t plan, const double* x, double* y, cudaStream_t stream) {
+    if (plan->solve_prec != DMRGB200_PREC_FP64_EMULATED || !plan->oz1 || !plan->oz_scratch3) return cudaSuccess;
+    if (oz_constants_ready(plan->oz1) && oz_constants_ready(plan->oz3)) return cudaSuccess;
+    if (capturing(stream)) return cudaErrorStreamCaptureUnsupported;
+    return emu_launch(plan, x, y, stream);
+}
 // Autotune the plan's grouped GEMMs once, outside any stream capture (DMRGB200_AUTOTUNE=0
 // keeps the default variant, and so do plans below 50 MFLOP per H psi).
 cudaError_t plan_ensure_tuned(dmrgb200_plan_t plan, const double* x, double* y, cudaStream_t stream) {
@@ -793,6 +802,13 @@ dmrgb200_status dmrgb200_plan_set_precision(dmrgb200_plan_t plan, int prec) {
         jd_graph_free(plan->jd);  // the cached solver graph captured the other H psi
         plan->jd = nullptr;
     }
+    return DMRGB200_OK;
+}
+
+dmrgb200_status dmrgb200_plan_boundaries_changed(dmrgb200_plan_t plan) {
+    if (!plan) return fail(DMRGB200_INVALID_ARGUMENT, "null plan");
+    oz_invalidate(plan->oz1);
+    oz_invalidate(plan->oz3);
     return DMRGB200_OK;
 }
 

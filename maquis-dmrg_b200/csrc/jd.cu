@@ -194,6 +194,7 @@ dmrgb200_status solve_stepwise(dmrgb200_plan_t plan, uint64_t n, const double* x
                                uint32_t n_ortho, double tol, uint32_t max_iter, double* energy, double* x_out,
                                dmrgb200_solve_stats* stats, void* cuda_stream);
 int plan_error_words(dmrgb200_plan_t plan);
+cudaError_t plan_refresh_constants(dmrgb200_plan_t plan, const double* x, double* y, cudaStream_t stream);
 }  // namespace dmrgb200
 
 // Both solver forms end synchronised; a kernel whose bounded wait ran out during
@@ -203,6 +204,12 @@ extern "C" dmrgb200_status dmrgb200_solve(dmrgb200_plan_t plan, uint64_t n, cons
                                           const double* const* ortho, uint32_t n_ortho, double tol, uint32_t max_iter,
                                           double* energy, double* x_out, dmrgb200_solve_stats* stats,
                                           void* cuda_stream) {
+    if (plan && x0 && x_out) {
+        cudaError_t e = dmrgb200::plan_refresh_constants(plan, x0, x_out, static_cast<cudaStream_t>(cuda_stream));
+        if (e != cudaSuccess)
+            return noalloc_fail(DMRGB200_DEVICE_ERROR, std::string("emulated boundary digit planes: ") +
+                                                           cudaGetErrorString(e));
+    }
     dmrgb200_status s =
         dmrgb200::solve_stepwise(plan, n, x0, ortho, n_ortho, tol, max_iter, energy, x_out, stats, cuda_stream);
     // a wait that ran out is the cause of whatever else went wrong in the solve (garbage H psi

@@ -106,6 +106,7 @@ _sigs = {
     "dmrgb200_last_error": ([], C.c_char_p),
     "dmrgb200_abi_version": ([], C.c_int),
     "dmrgb200_plan_check": ([vp, vp], C.c_int),
+    "dmrgb200_plan_boundaries_changed": ([vp], C.c_int),
     "dmrgb200_hpsi_per_block": ([vp, vp, vp, vp, u64p], C.c_int),
     "dmrgb200_set_wait_limit": ([C.c_uint64], C.c_int),
     "dmrgb200_plan_set_precision": ([vp, C.c_int], C.c_int),

@@ -464,6 +464,7 @@ class DeviceBackend:
         hit = self.cache.get(site_key) if self.reuse_plans else None
         if hit is not None and hit[0] == full_key:
             plan = hit[3]
+            plan.boundaries_changed()  # the bound boundary buffers were rewritten since its last solve
             self.cache_hits += 1
             t1 = t2 = time.perf_counter()
         else:

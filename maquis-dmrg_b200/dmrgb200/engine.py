@@ -227,6 +227,10 @@ class DevicePlan:
                                                       C.byref(err)), "dmrgb200_plan_tune_slices")
         return sl.value, err.value
 
+    def boundaries_changed(self) -> None:
+        """The bound boundary buffers were rewritten in place (dmrgb200_plan_boundaries_changed)."""
+        capi.check(capi.lib.dmrgb200_plan_boundaries_changed(self.handle), "dmrgb200_plan_boundaries_changed")
+
     def check(self, stream: int = 0) -> None:
         """Synchronise and raise if a kernel's bounded wait ran out (dmrgb200_plan_check)."""
         capi.check(capi.lib.dmrgb200_plan_check(self.handle, stream or None), "dmrgb200_plan_check")

@@ -485,9 +485,11 @@ def qc_workload(args):
         except capi.DmrgError as exc:  # reported, not hidden
             res[name] = {"unavailable": str(exc)}
             continue
+        profiled = name == args.prec  # the profiler range holds only the timed steps of --prec
         if name == "fp64":
             capi.check(capi.lib.dmrgb200_plan_set_timing(sp.plan.handle, 1), "set_timing")
-            torch.cuda.profiler.start()  # the profiler range holds only the timed FP64 steps
+        if profiled:
+            torch.cuda.profiler.start()
         ts = []
         for k in range(min(args.steps, 10)):
             flush.fill_(float(k))
@@ -497,7 +499,7 @@ def qc_workload(args):
             b.record()
             b.synchronize()
             ts.append(a.elapsed_time(b))
-        if name == "fp64":
+        if profiled:
             torch.cuda.profiler.stop()
         ms = statistics.mean(ts)
         res[name] = {"ms_per_step": ms, "value": sp.plan.flops / (ms * 1e-3) / 1e9, "unit": "GFLOP/s"}
@@ -663,33 +665,53 @@ def adjoint_workload(args):
 
 
 def batched_workload(args):
-    """Batched instances: 64 independent site problems (32 Heisenberg U1, 32
-    Fermi-Hubbard TwoU1, chains of 32 sites, middle two-site problem), bond
-    dimensions log-uniform in [64, 1024] (seed 6), merged into one batched plan:
-    every H·psi stage is a single launch over all instances.  20 H·psi steps
-    (the Davidson iterations' products) are timed in FP64 and emulated FP64."""
+    """Batched instances (config 5): 64 independent site problems (32 Heisenberg U1, 32
+    Fermi-Hubbard TwoU1, chains of 32 sites, middle two-site problem, environments made
+    mixed-canonical), bond dimensions log-uniform in [64, 1024] (seed 6), merged into one
+    batched plan: every H·psi stage is a single launch over all instances.  Timed: the
+    batched H·psi in FP64 and emulated FP64, and 20 Jacobi-Davidson iterations of every
+    instance (dmrgb200.batched.BatchedJD: one batched H·psi per iteration) in FP64 and
+    with the H·psi emulated (slices tuned to 1e-10); reported per instance: the emulated
+    energy's difference from the FP64 one and the FP64 H·psi's error against the CPU
+    oracle on the same inputs."""
     import torch
+    import oracle as O
     from dmrgb200 import _capi as capi
+    from dmrgb200 import batched as BJ
+    from dmrgb200 import dmrg as G
     from dmrgb200 import engine as E
     from dmrgb200 import models as M
     from dmrgb200 import mps as S
 
     rng = np.random.default_rng(6)
     ctx = E.Context(0)
-    items, keep, xs = [], [], []
+    t0 = time.perf_counter()
+    items, keep, ms_ = [], [], []
     for k in range(64):
         L = 32
         model = M.heisenberg(L) if k % 2 == 0 else M.fermi_hubbard(L)
         m = int(round(np.exp(rng.uniform(np.log(64), np.log(1024)))))
         radius = 10.0 if k % 2 == 0 else 3.5
         bonds = S.synthetic_bonds(model.phys, L, model.total_charge, m, radius)
-        tensors = S.random_mps(model.phys, bonds, rng)
-        sp = E.SiteProblem(ctx, model, tensors, bonds, L // 2 - 1)
+        i = L // 2 - 1
+        tensors = G.left_canonicalize(G.right_canonicalize(S.random_mps(model.phys, bonds, rng), 0.0), i, 0.0)
+        bonds = [t.left for t in tensors] + [tensors[-1].right]
+        sp = E.SiteProblem(ctx, model, tensors, bonds, i)
         items.append((sp.schedule.plan, sp.Lidx.cohort_addresses(sp.Lbuf.data_ptr()),
                       sp.Ridx.cohort_addresses(sp.Rbuf.data_ptr())))
         keep.append(sp)
+        ms_.append(m)
     bp = E.BatchedPlan(ctx, items)
-    x = torch.rand(bp.total_size, dtype=torch.float64, device="cuda")
+    setup_s = time.perf_counter() - t0
+    # start vectors: normalised random blocks per instance, zero padding
+    x0h = np.zeros(bp.total_size)
+    for sp, b in zip(keep, bp.in_base):
+        pl = sp.schedule.plan
+        for off, r, c in zip(pl["in_off"], pl["in_rows"], pl["in_cols"]):
+            o = b + int(off)
+            x0h[o:o + int(r) * int(c)] = rng.standard_normal(int(r) * int(c))
+        x0h[b:b + sp.size] /= np.linalg.norm(x0h[b:b + sp.size])
+    x = torch.from_numpy(x0h).cuda()
     y = torch.zeros_like(x)
     res = {}
     for name, prec in (("fp64", capi.PREC_FP64), ("emulated", capi.PREC_FP64_EMULATED)):
@@ -702,17 +724,49 @@ def batched_workload(args):
             bp.hpsi(x.data_ptr(), y.data_ptr(), prec)
         b.record()
         b.synchronize()
+        bp.check()
         ms = a.elapsed_time(b) / 20
         res[name] = {"ms_per_step": ms, "value": bp.flops / (ms * 1e-3) / 1e9, "unit": "GFLOP/s"}
         if name == "fp64":
             y64 = y.clone()
         else:
             res[name]["rel_err_vs_fp64"] = float(torch.linalg.norm(y - y64) / torch.linalg.norm(y64))
+    # per-instance FP64 H·psi against the CPU oracle on the same boundaries and vector
+    y64h = y64.cpu().numpy()
+    ora = []
+    for sp, b in zip(keep, bp.in_base):
+        yo = O.hpsi(sp.schedule.plan, sp.Lbuf.cpu().numpy(), sp.Lidx, sp.Rbuf.cpu().numpy(), sp.Ridx,
+                    x0h[b:b + sp.size])
+        yd = y64h[b:b + sp.size]
+        ora.append(float(np.linalg.norm(yd - yo) / np.linalg.norm(yo)))
+    # 20 Jacobi-Davidson iterations per instance
+    solver = BJ.BatchedJD(bp)
+    jd = {}
+    s_t, e_t = bp.tune_slices(x.data_ptr(), 1e-10)
+    for name, prec in (("fp64", capi.PREC_FP64), ("emulated", capi.PREC_FP64_EMULATED)):
+        solver.solve(x, max_iter=3, prec=prec)  # warm-up
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        th, u, its, rn = solver.solve(x, max_iter=20, prec=prec)
+        b.record()
+        b.synchronize()
+        bp.check()
+        jd[name] = {"ms": a.elapsed_time(b), "energies": th.cpu().numpy().tolist(),
+                    "iterations": int(its.min().item())}
+    de = np.abs(np.array(jd["emulated"]["energies"]) - np.array(jd["fp64"]["energies"]))
     line = {"metric": "batched H·psi GFLOP/s (FP64)", "value": res["fp64"]["value"], "unit": "GFLOP/s",
             "higher_is_better": True, "n_gpus": 1, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "64_instances_heisenberg_u1_hubbard_twou1_L32_m_loguniform_64_1024",
-                       "instances": 64, "flops_per_step": int(bp.flops), "psi_elements": int(bp.total_size)},
-            "fp64": res["fp64"], "emulated": res["emulated"]}
+                       "instances": 64, "bond_dims": ms_, "flops_per_step": int(bp.flops),
+                       "psi_elements": int(bp.total_size), "setup_seconds": setup_s},
+            "fp64": res["fp64"], "emulated": res["emulated"],
+            "oracle_hpsi_rel_err": {"max": max(ora), "median": float(np.median(ora)), "per_instance": ora},
+            "jd_20_iterations": {"fp64_ms": jd["fp64"]["ms"], "emulated_ms": jd["emulated"]["ms"],
+                                 "iterations": jd["fp64"]["iterations"], "slices": s_t,
+                                 "hpsi_rel_err_at_x0": e_t, "max_abs_delta_e": float(de.max()),
+                                 "per_instance_delta_e": de.tolist(),
+                                 "fp64_energies": jd["fp64"]["energies"]}}
     print(json.dumps(line), flush=True)
 
 

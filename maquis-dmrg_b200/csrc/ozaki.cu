@@ -36,27 +36,38 @@ dmrgb200_status noalloc_fail(dmrgb200_status s, std::string const& msg);
 
 namespace {
 
-constexpr int OZ_BM = 128, OZ_BN = 64, OZ_BK = 64;        // tile rows, tile columns, K bytes per slab
+constexpr int OZ_BM = 128, OZ_BN = 64, OZ_BK = 32;        // tile rows, tile columns, K bytes per slab
 constexpr int A_TILE = OZ_BM * OZ_BK, B_TILE = OZ_BN * OZ_BK;
-constexpr int OZ_THREADS = 128, OZ_STAGES = 2, OZ_MAX_SLICES = 8;
+constexpr int OZ_MAX_SLICES = 8, OZ_MAX_STAGES = 8;
+// warps 0-3 drain the accumulators (TMEM lane quarter = warp), warp 4 loads the slabs,
+// warp 5 issues the MMAs
+constexpr int OZ_EPI_WARPS = 4, OZ_LOAD_WARP = 4, OZ_MMA_WARP = 5, OZ_THREADS = 32 * 6;
+constexpr uint32_t OZ_SMEM_CAP = 227u * 1024u;  // dynamic shared memory of one CTA
+constexpr uint32_t OZ_BAR_BYTES = 256;          // barriers and slots behind the stages
+// pipeline depth for s digit planes: as many stages of s (A + B) tiles as fit
+__host__ __device__ constexpr uint32_t oz_stages(int s) {
+    return (OZ_SMEM_CAP - OZ_BAR_BYTES) / (uint32_t(s) * (A_TILE + B_TILE)) < uint32_t(OZ_MAX_STAGES)
+               ? (OZ_SMEM_CAP - OZ_BAR_BYTES) / (uint32_t(s) * (A_TILE + B_TILE))
+               : uint32_t(OZ_MAX_STAGES);
+}
 using namespace async;
 
 // K slabs per exact INT32 accumulation: accumulator D_g sums (g + 1) <= s digit
 // products of |a b| <= 127^2 per K element, and 127^2 * 2^17 < 2^31
 constexpr uint32_t oz_chunk_slabs(int s) { return std::max<uint32_t>(1u, (1u << 17) / uint32_t(s * OZ_BK)); }
 
-// byte offset of element (r, k) of a (rows x 64-byte) K-major tile in the
+// byte offset of element (r, k) of a (rows x 32-byte) K-major tile in the
 // canonical no-swizzle layout: 8x16-byte core matrices, LBO = 128 B along K,
-// SBO = 512 B between 8-row groups
+// SBO = 256 B between 8-row groups
 __device__ __forceinline__ uint32_t tile_off(uint32_t r, uint32_t k) {
-    return (r >> 3) * 512u + (k >> 4) * 128u + (r & 7u) * 16u + (k & 15u);
+    return (r >> 3) * 256u + (k >> 4) * 128u + (r & 7u) * 16u + (k & 15u);
 }
 
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
     uint64_t d = 0;
     d |= uint64_t((saddr >> 4) & 0x3FFFu);
     d |= uint64_t((128u >> 4) & 0x3FFFu) << 16;  // leading (K) byte offset
-    d |= uint64_t((512u >> 4) & 0x3FFFu) << 32;  // stride (row-group) byte offset
+    d |= uint64_t((256u >> 4) & 0x3FFFu) << 32;  // stride (row-group) byte offset
     d |= uint64_t(1) << 46;                       // descriptor version (sm_100)
     return d;                                      // base offset 0, no swizzle
 }
@@ -92,8 +103,11 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, int32_t (&v)[16]) {
 
 // One operand of one segment to be cut into digit planes.  For an A operand the
 // digit matrix is A itself (row r, column k); for a B operand it is B^T (row n,
-// column k), both stored K-major in 8 KB (A, 128 rows) or 4 KB (B, 64 rows)
-// tiles: tile (rt, ks) at out_base + (rt * KS + ks) * tile_bytes.
+// column k), both stored K-major in 4 KB (A, 128 rows) or 2 KB (B, 64 rows) tiles.
+// Tile (rt, ks) has the index t = out_base / tile_bytes + rt * KS + ks, and its s
+// digit planes lie side by side: plane p at (t * s + p) * tile_bytes, so that one
+// bulk copy moves every plane of a slab.  Offsets and sizes that count one plane
+// (out_base, a_plane, the slab offsets) are scaled by s where memory is addressed.
 struct OzSplit {
     DevOp op;           // batch already folded into op.off
     uint32_t rows, K;   // logical rows (M or N) and K of the segment
@@ -106,78 +120,227 @@ struct OzSplit {
     uint32_t pad;
 };
 
-__device__ __forceinline__ double op_elem(Bases const& bs, OzSplit const& j, uint32_t r, uint32_t k,
-                                          const DevRow* __restrict__ rowtab) {
-    if (!j.is_b && j.rowtab != DevProb::NO_ROWS) {
-        const DevRow rw = rowtab[j.rowtab + r];
-        return reinterpret_cast<const double*>(base_of(bs, j.op.buf))[rw.a_off + uint64_t(k) * rw.ld];
-    }
-    const double* base = reinterpret_cast<const double*>(base_of(bs, j.op.buf) + 8ull * j.op.off);
-    const uint64_t ld = j.op.ld;
-    if (!j.is_b) return j.op.trans ? base[k + uint64_t(r) * ld] : base[r + uint64_t(k) * ld];
-    // B(k, r): non-transposed B[k + r * ld], transposed B[r + k * ld]
-    return j.op.trans ? base[r + uint64_t(k) * ld] : base[k + uint64_t(r) * ld];
-}
-
 __global__ void fill_int(int* __restrict__ p, uint64_t n, int v) {
     for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x)
         p[i] = v;
 }
 
-// exponent of every row of every job (max over segments by atomicMax):
-// |x 2^-e| < 1 for the whole row of the output matrix.  blockIdx.y walks the
-// jobs, blockIdx.x and the warps the rows, the lanes K.
-__global__ void __launch_bounds__(256) oz_exponents(const OzSplit* __restrict__ jobs, uint32_t njobs, Bases bs,
-                                                    int* __restrict__ e, const DevRow* __restrict__ rowtab) {
-    const uint32_t lane = threadIdx.x & 31, warps = blockDim.x >> 5;
-    for (uint32_t j = blockIdx.y; j < njobs; j += gridDim.y) {
-        const OzSplit job = jobs[j];
-        for (uint32_t r = blockIdx.x * warps + (threadIdx.x >> 5); r < job.rows; r += gridDim.x * warps) {
-            double m = 0.0;
-            for (uint32_t k = lane; k < job.K; k += 32) m = fmax(m, fabs(op_elem(bs, job, r, k, rowtab)));
+// Addressing of a split job: element (r, k) of a plain operand is base[r * sr + k * sk];
+// a row-table A row r starts at rowtab[rowtab + r].a_off with K stride rowtab[..].ld.
+struct OzAddr {
+    const double* base;
+    uint64_t sr, sk;
+};
+__device__ __forceinline__ OzAddr oz_addr(Bases const& bs, OzSplit const& j) {
+    OzAddr a;
+    a.base = reinterpret_cast<const double*>(base_of(bs, j.op.buf) + 8ull * j.op.off);
+    const uint64_t ld = j.op.ld;
+    const bool rows_contig = j.is_b ? (j.op.trans != 0) : (j.op.trans == 0);
+    a.sr = rows_contig ? 1 : ld;
+    a.sk = rows_contig ? ld : 1;
+    return a;
+}
+// k-major jobs (K contiguous for a row, no row table): a warp walks one row
+__host__ __device__ __forceinline__ bool oz_kmajor(OzSplit const& j) {
+    const bool rows_contig = j.is_b ? (j.op.trans != 0) : (j.op.trans == 0);
+    return !rows_contig && (j.is_b || j.rowtab == DevProb::NO_ROWS);
+}
+constexpr uint32_t OZ_EXP_KCH = 1024;  // K elements of a k-major exponent item (one warp)
+constexpr uint32_t OZ_EXP_RCH = 256;   // K elements of a row-major exponent item (32 rows, one per lane)
+
+// Warp items of the exponent pass:
+//   k-major:   (row, K chunk of OZ_EXP_KCH): the lanes read the chunk contiguously
+//   row-major: (32 consecutive rows, K chunk of OZ_EXP_RCH): one row per lane, the
+//              lanes read consecutive rows of one K column (contiguous)
+__host__ __device__ __forceinline__ uint64_t oz_exp_items(OzSplit const& j) {
+    if (oz_kmajor(j)) return uint64_t(j.rows) * ((j.K + OZ_EXP_KCH - 1) / OZ_EXP_KCH);
+    return uint64_t((j.rows + 31) / 32) * ((j.K + OZ_EXP_RCH - 1) / OZ_EXP_RCH);
+}
+// Warp items of the split pass (every padded row and K slab of the digit tiles):
+//   k-major:   (16-row group, 32-element slab): lane t takes row (t & 15) and the 16
+//              K elements (t >> 4) * 16 .. + 15, so the warp writes two contiguous
+//              256-byte core-matrix groups (512 bytes) per digit plane
+//   row-major: (32 consecutive rows, 16-element K group): one row per lane, the lanes
+//              read one K column of 32 rows at a time and write 16 bytes each
+__host__ __device__ __forceinline__ uint64_t oz_split_items(OzSplit const& j, uint32_t TR) {
+    if (oz_kmajor(j)) return uint64_t(j.RT) * (TR / 16) * j.KS;
+    return uint64_t(j.RT) * (TR / 32) * j.KS * (OZ_BK / 16);
+}
+
+// job of a warp item: the job j with first[j] <= it < first[j + 1] (jobs without items
+// have first[j] == first[j + 1] and are never chosen)
+__device__ __forceinline__ uint32_t oz_job_of(const uint64_t* __restrict__ first, uint32_t njobs, uint64_t it) {
+    uint32_t lo = 0, hi = njobs;  // first[lo] <= it < first[hi]
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (first[mid] <= it) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// exponent of every row of every job (max over segments and chunks by atomicMax):
+// |x 2^-e| < 1 for the whole row of the output matrix.  `first` holds the first warp
+// item of every job and the end (njobs + 1 entries; the items of the launched jobs are
+// first[0] .. first[njobs] - 1).
+__global__ void __launch_bounds__(256) oz_exponents(const OzSplit* __restrict__ jobs, const uint64_t* __restrict__ first,
+                                                    uint32_t njobs, Bases bs, int* __restrict__ e,
+                                                    const DevRow* __restrict__ rowtab) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t total = first[njobs];
+    const uint64_t nwarps = uint64_t(gridDim.x) * (blockDim.x >> 5);
+    for (uint64_t it = first[0] + uint64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); it < total;
+         it += nwarps) {
+        const uint32_t jn = oz_job_of(first, njobs, it);
+        const OzSplit job = jobs[jn];
+        const uint64_t local = it - first[jn];
+        if (oz_kmajor(job)) {
+            const uint32_t nch = (job.K + OZ_EXP_KCH - 1) / OZ_EXP_KCH;
+            const uint32_t r = uint32_t(local / nch), k0 = uint32_t(local % nch) * OZ_EXP_KCH;
+            const OzAddr a = oz_addr(bs, job);
+            const double* row = a.base + uint64_t(r) * a.sr;
+            const uint32_t k1 = min(job.K, k0 + OZ_EXP_KCH);
+            double m0 = 0.0, m1 = 0.0, m2 = 0.0, m3 = 0.0;
+            uint32_t k = k0 + lane;
+            for (; k + 96 < k1; k += 128) {
+                m0 = fmax(m0, fabs(row[k]));
+                m1 = fmax(m1, fabs(row[k + 32]));
+                m2 = fmax(m2, fabs(row[k + 64]));
+                m3 = fmax(m3, fabs(row[k + 96]));
+            }
+            for (; k < k1; k += 32) m0 = fmax(m0, fabs(row[k]));
+            double m = fmax(fmax(m0, m1), fmax(m2, m3));
             for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
             if (lane == 0 && m > 0.0) atomicMax(&e[job.e_off + r], ilogb(m) + 1);
+        } else {
+            const uint32_t nch = (job.K + OZ_EXP_RCH - 1) / OZ_EXP_RCH;
+            const uint32_t r = uint32_t(local / nch) * 32 + lane, k0 = uint32_t(local % nch) * OZ_EXP_RCH;
+            if (r >= job.rows) continue;
+            const double* row;
+            uint64_t sk;
+            if (!job.is_b && job.rowtab != DevProb::NO_ROWS) {
+                const DevRow rw = rowtab[job.rowtab + r];
+                row = reinterpret_cast<const double*>(base_of(bs, job.op.buf)) + rw.a_off;
+                sk = rw.ld;
+            } else {
+                const OzAddr a = oz_addr(bs, job);
+                row = a.base + r;  // rows contiguous: sr = 1
+                sk = a.sk;
+            }
+            const uint32_t k1 = min(job.K, k0 + OZ_EXP_RCH);
+            double m0 = 0.0, m1 = 0.0;
+            uint32_t k = k0;
+            for (; k + 1 < k1; k += 2) {
+                m0 = fmax(m0, fabs(row[uint64_t(k) * sk]));
+                m1 = fmax(m1, fabs(row[uint64_t(k + 1) * sk]));
+            }
+            if (k < k1) m0 = fmax(m0, fabs(row[uint64_t(k) * sk]));
+            const double m = fmax(m0, m1);
+            if (m > 0.0) atomicMax(&e[job.e_off + r], ilogb(m) + 1);
         }
     }
 }
 
-// Digit planes: every thread cuts four consecutive K elements of one row and
-// stores each plane's four digits as one 32-bit word (K-contiguous bytes of the
-// tile layout).  Rows outside the operand and K beyond it give zero digits.
-__global__ void __launch_bounds__(256) oz_split(const OzSplit* __restrict__ jobs, uint32_t njobs, Bases bs,
-                                                const int* __restrict__ e, int s, uint64_t a_plane,
-                                                int8_t* __restrict__ A8, uint64_t b_plane, int8_t* __restrict__ B8,
+// The digits of y = x 2^-ex (|y| < 1) are those of the repeated step d = trunc(128 y),
+// y <- 128 y - d: digit p is sign(x) times bits 49 - 7p .. 55 - 7p of the integer
+// trunc(|x| 2^(56 - ex)), p = 0 .. 7.  That integer is formed from the bits of x
+// alone (mantissa shifted by the exponent difference; exact, no rounding), so the
+// split needs no floating-point conversions.
+__device__ __forceinline__ uint64_t oz_fixed(double x, int ex, uint32_t& neg) {
+    const uint64_t b = static_cast<uint64_t>(__double_as_longlong(x));
+    neg = uint32_t(b >> 63);
+    int E = int((b >> 52) & 0x7ffu);
+    uint64_t m = b & ((1ull << 52) - 1ull);
+    if (E) m |= 1ull << 52;  // normal: implicit bit
+    else E = 1;              // subnormal: m units of 2^-1074
+    const int sh = E - 1075 + 56 - ex;  // |x| 2^(56 - ex) = m 2^sh < 2^56 when |y| < 1
+    if (sh >= 0) return sh < 64 ? (m << sh) : 0ull;
+    return sh > -64 ? (m >> -sh) : 0ull;
+}
+// digit p of a fixed-point value as a byte (two's complement)
+__device__ __forceinline__ uint32_t oz_digit(uint64_t X, uint32_t neg, int p) {
+    const uint32_t d = uint32_t(X >> (49 - 7 * p)) & 127u;
+    return (neg ? 0u - d : d) & 255u;
+}
+
+// Digit planes of every job: the s signed 7-bit digits of every element scaled by its
+// row's exponent, in the K-major core-matrix layout of the MMA tiles (rows beyond the
+// operand and K beyond it give zero digits).  `first` as for oz_exponents.
+__global__ void __launch_bounds__(256) oz_split(const OzSplit* __restrict__ jobs, const uint64_t* __restrict__ first,
+                                                uint32_t njobs, Bases bs, const int* __restrict__ e, int s,
+                                                int8_t* __restrict__ A8, int8_t* __restrict__ B8,
                                                 const DevRow* __restrict__ rowtab) {
-    for (uint32_t j = blockIdx.y; j < njobs; j += gridDim.y) {
-        const OzSplit job = jobs[j];
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t total = first[njobs];
+    const uint64_t nwarps = uint64_t(gridDim.x) * (blockDim.x >> 5);
+    for (uint64_t it = first[0] + uint64_t(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); it < total;
+         it += nwarps) {
+        const uint32_t jn = oz_job_of(first, njobs, it);
+        const OzSplit job = jobs[jn];
+        const uint64_t local = it - first[jn];
         int8_t* out = job.is_b ? B8 : A8;
-        const uint64_t plane = job.is_b ? b_plane : a_plane;
         const uint32_t TR = job.is_b ? uint32_t(OZ_BN) : uint32_t(OZ_BM);
         const uint32_t tile_bytes = TR * OZ_BK;
-        const uint32_t nrows = job.RT * TR, ngroups = job.KS * (OZ_BK / 4);
-        const uint32_t total = nrows * ngroups;
-        // column-major A: rows are contiguous (row-table rows are separate slices: K-major order)
-        const bool rows_fast = !job.is_b && !job.op.trans && job.rowtab == DevProb::NO_ROWS;
-        for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
-            const uint32_t r = rows_fast ? idx % nrows : idx / ngroups;
-            const uint32_t k0 = 4 * (rows_fast ? idx / nrows : idx % ngroups);
-            double x[4];
-            const int ex = r < job.rows ? e[job.e_off + r] : 0;
+        if (oz_kmajor(job)) {
+            // item = (16-row group g, slab ks); lane: row g * 16 + (lane & 15), K 16 (lane >> 4) .. + 15
+            const uint32_t ks = uint32_t(local % job.KS);
+            const uint32_t g = uint32_t(local / job.KS);
+            const uint32_t r = g * 16 + (lane & 15);
+            const uint32_t kk = (lane >> 4) * 16;  // within the slab
+            const uint32_t k0 = ks * OZ_BK + kk;
+            const bool live = r < job.rows;
+            const int ex = live ? e[job.e_off + r] : 0;
+            const OzAddr a = oz_addr(bs, job);
+            const double* row = a.base + uint64_t(r) * a.sr;
+            uint64_t X[16];
+            uint32_t neg[16];
 #pragma unroll
-            for (int u = 0; u < 4; ++u)
-                x[u] = (r < job.rows && k0 + u < job.K) ? ldexp(op_elem(bs, job, r, k0 + u, rowtab), -ex) : 0.0;
-            const uint64_t off = job.out_base + (uint64_t(r / TR) * job.KS + k0 / OZ_BK) * tile_bytes +
+            for (int u = 0; u < 16; ++u) X[u] = oz_fixed((live && k0 + u < job.K) ? row[k0 + u] : 0.0, ex, neg[u]);
+            const uint64_t off = (job.out_base + (uint64_t(r / TR) * job.KS + ks) * tile_bytes) * s + tile_off(r % TR, kk);
+            for (int p = 0; p < s; ++p) {
+                uint32_t w[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    w[q] = oz_digit(X[4 * q], neg[4 * q], p) | (oz_digit(X[4 * q + 1], neg[4 * q + 1], p) << 8) |
+                           (oz_digit(X[4 * q + 2], neg[4 * q + 2], p) << 16) |
+                           (oz_digit(X[4 * q + 3], neg[4 * q + 3], p) << 24);
+                *reinterpret_cast<uint4*>(out + off + p * tile_bytes) = make_uint4(w[0], w[1], w[2], w[3]);
+            }
+        } else {
+            // item = (32-row group, 16-element K group); lane: one row
+            const uint32_t ngroups = job.KS * (OZ_BK / 16);
+            const uint32_t r = uint32_t(local / ngroups) * 32 + lane;
+            const uint32_t k0 = 16 * uint32_t(local % ngroups);
+            const bool live = r < job.rows;
+            const int ex = live ? e[job.e_off + r] : 0;
+            const double* row = nullptr;
+            uint64_t sk = 0;
+            if (live) {
+                if (!job.is_b && job.rowtab != DevProb::NO_ROWS) {
+                    const DevRow rw = rowtab[job.rowtab + r];
+                    row = reinterpret_cast<const double*>(base_of(bs, job.op.buf)) + rw.a_off;
+                    sk = rw.ld;
+                } else {
+                    const OzAddr a = oz_addr(bs, job);
+                    row = a.base + r;  // rows contiguous: sr = 1
+                    sk = a.sk;
+                }
+            }
+            uint64_t X[16];
+            uint32_t neg[16];
+#pragma unroll
+            for (int u = 0; u < 16; ++u)
+                X[u] = oz_fixed((live && k0 + u < job.K) ? row[uint64_t(k0 + u) * sk] : 0.0, ex, neg[u]);
+            const uint64_t off = (job.out_base + (uint64_t(r / TR) * job.KS + k0 / OZ_BK) * tile_bytes) * s +
                                  tile_off(r % TR, k0 % OZ_BK);
             for (int p = 0; p < s; ++p) {
-                uint32_t word = 0;
+                uint32_t w[4];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const double t = x[u] * 128.0;  // exact
-                    const double d = trunc(t);      // |d| <= 127
-                    x[u] = t - d;                   // exact
-                    word |= (uint32_t(uint8_t(int8_t(d)))) << (8 * u);
-                }
-                *reinterpret_cast<uint32_t*>(out + p * plane + off) = word;
+                for (int q = 0; q < 4; ++q)
+                    w[q] = oz_digit(X[4 * q], neg[4 * q], p) | (oz_digit(X[4 * q + 1], neg[4 * q + 1], p) << 8) |
+                           (oz_digit(X[4 * q + 2], neg[4 * q + 2], p) << 16) |
+                           (oz_digit(X[4 * q + 3], neg[4 * q + 3], p) << 24);
+                *reinterpret_cast<uint4*>(out + off + p * tile_bytes) = make_uint4(w[0], w[1], w[2], w[3]);
             }
         }
     }
@@ -204,13 +367,13 @@ struct OzTile {
 struct OzArgs {
     const int8_t* A8;
     const int8_t* B8;
-    uint64_t a_plane, b_plane;  // bytes per digit plane
     const int* e;
     const OzPB* pbs;
     const OzSlab* slabs;
     const OzTile* tiles;
     uint32_t n_tiles;
-    uint32_t chunk;  // K slabs accumulated in TMEM before a partial epilogue (>= 1)
+    uint32_t chunk;   // K slabs accumulated in TMEM before a partial epilogue (>= 1)
+    uint32_t stages;  // pipeline stages of s (A + B) tiles
     int s;
     Bases bases;
     int* err;
@@ -218,25 +381,64 @@ struct OzArgs {
     unsigned long long wait_ns;  // limit of the waits for operand slabs
 };
 
+// exact int32 -> double on the integer and FP64 pipes: the bit pattern of 2^52 + 2^51
+// plus v is the double 2^52 + 2^51 + v (unit spacing there, |v| < 2^51)
+__device__ __forceinline__ double i2d_exact(int32_t v) {
+    return __longlong_as_double(0x4338000000000000ll + static_cast<long long>(v)) - 6755399441055744.0;
+}
+// 2^e for -1022 <= e <= 1023
+__device__ __forceinline__ double pow2_normal(int e) { return __longlong_as_double(static_cast<long long>(e + 1023) << 52); }
+
+// bounded wait that ignores the error word: for events that always happen once work is
+// in flight (issued MMAs completing, issued copies landing before the CTA leaves)
+__device__ __forceinline__ void oz_settle(uint64_t* bar, uint32_t parity, int* err) {
+    const unsigned long long t0 = global_ns();
+    while (!mbar_try(bar, parity))
+        if (global_ns() - t0 > WAIT_LIMIT_NS) {
+            atomicExch(err, 1);
+            return;
+        }
+}
+
+// Persistent grouped INT8 GEMM over the digit planes, one 128 x 64 output tile at a
+// time, with warp roles:
+//   load warp (lane 0): one bulk copy of the s A-planes and one of the s B-planes of
+//     each K slab into a ring of `stages` stages (full barriers), refilling a stage
+//     once the MMAs that read it have completed (empty barriers, MMA commits);
+//   MMA warp (lane 0): for each slab, the s(s+1)/2 digit products p + q = g < s into
+//     accumulator g (TMEM columns g * 64 ..), one 128x64x32 tcgen05.mma each; after a
+//     chunk of slabs it commits to `tfull`;
+//   epilogue warps 0-3: wait `tfull`, read their 32 TMEM lanes of every accumulator,
+//     sum them scaled by 2^-7(g+2) in FP64 (smallest weight first), release the
+//     accumulators (`tempty`, which the MMA warp waits for before the next chunk) and
+//     add 2^(e_row + e_col) times the sum into C.
+// The load warp runs ahead across tiles and chunks, so copies overlap the epilogue.
+// Every wait is bounded; on a timeout or a set error word each role stops, the issued
+// MMAs and copies are waited for (fixed limit), TMEM is released and the CTA returns.
 __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_mma(OzArgs a) {
     extern __shared__ __align__(1024) unsigned char smem[];
     const int s = a.s;
-    const uint32_t stage_bytes = uint32_t(s) * (A_TILE + B_TILE);
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem + OZ_STAGES * stage_bytes);
-    uint64_t* empty = full + OZ_STAGES;
-    uint64_t* done = empty + OZ_STAGES;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    const uint32_t nst = a.stages;
+    const uint32_t a_bytes = uint32_t(s) * A_TILE, stage_bytes = uint32_t(s) * (A_TILE + B_TILE);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + nst * stage_bytes);
+    uint64_t* empty = full + nst;
+    uint64_t* tfull = empty + nst;
+    uint64_t* tempty = tfull + 1;
+    uint64_t* fin = tempty + 1;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(fin + 1);
+    uint32_t* consumed_slot = tmem_slot + 1;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t ncols = (s * OZ_BN <= 256) ? ((s * OZ_BN <= 128) ? 128u : 256u) : 512u;
-    const uint32_t idesc = idesc_i8(OZ_BM, OZ_BN);
-    volatile int* verr = a.err;
 
     if (threadIdx.x == 0) {
-        for (int i = 0; i < OZ_STAGES; ++i) {
+        for (uint32_t i = 0; i < nst; ++i) {
             mbar_init(&full[i], 1);
             mbar_init(&empty[i], 1);
         }
-        mbar_init(done, 1);
+        mbar_init(tfull, 1);
+        mbar_init(tempty, OZ_EPI_WARPS);
+        mbar_init(fin, 1);
+        *consumed_slot = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -248,141 +450,154 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_mma(OzArgs a) {
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
+    uint32_t issued = 0;  // load warp lane 0: slabs whose copies were issued
 
-    // running slab / round counters: every arrival on every barrier is waited for exactly once, in order.
-    // A tile's slabs are accumulated in chunks of a.chunk slabs (the exact INT32 range); each chunk
-    // ends with one epilogue round that adds its partial product into C.
-    uint32_t slab0 = 0, rounds = 0, issued = 0, consumed = 0;
-    bool failed = false;
-    for (uint32_t tile = blockIdx.x; tile < a.n_tiles && !failed; tile += gridDim.x) {
-        const OzTile tl = a.tiles[tile];
-        const OzPB pb = a.pbs[tl.pb];
-        const uint32_t mt = tl.mt, nt = tl.nt;
-        const uint32_t KT = pb.slab_end - pb.slab_begin;
-        const uint32_t nch = KT ? (KT + a.chunk - 1) / a.chunk : 1;
-        bool ok = true;  // thread 0's pipeline state over the tile's chunks
-        auto load = [&](uint32_t kt) -> bool {
-            const uint32_t gs = slab0 + kt, st = gs % OZ_STAGES;
-            if (gs >= OZ_STAGES && !mbar_wait(&empty[st], ((gs - OZ_STAGES) / OZ_STAGES) & 1u, a.err, a.wait_ns))
-                return false;
-            const OzSlab sl = a.slabs[pb.slab_begin + kt];
-            unsigned char* base = smem + st * stage_bytes;
-            mbar_expect_tx(&full[st], stage_bytes);
-            for (int p = 0; p < s; ++p) {
-                bulk_load(base + p * A_TILE, a.A8 + p * a.a_plane + sl.a_off + uint64_t(mt) * sl.a_ts, A_TILE,
-                          &full[st]);
-                bulk_load(base + s * A_TILE + p * B_TILE, a.B8 + p * a.b_plane + sl.b_off + uint64_t(nt) * sl.b_ts,
-                          B_TILE, &full[st]);
-            }
-            ++issued;
-            return true;
-        };
-        for (uint32_t ch = 0; ch < nch && !failed; ++ch) {
-            const uint32_t k_begin = ch * a.chunk, k_end = min(KT, k_begin + a.chunk);
-            if (threadIdx.x == 0) {
-                if (ch == 0)
-                    for (uint32_t kt = 0; kt < KT && kt < OZ_STAGES && ok; ++kt) ok = load(kt);
-                for (uint32_t kt = k_begin; kt < k_end && ok; ++kt) {
-                    const uint32_t gs = slab0 + kt, st = gs % OZ_STAGES;
-                    ok = mbar_wait(&full[st], (gs / OZ_STAGES) & 1u, a.err, a.wait_ns);
-                    if (!ok) break;
-                    ++consumed;
-                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                    const uint32_t abase = smem_u32(smem + st * stage_bytes);
-                    const uint32_t bbase = abase + s * A_TILE;
-                    for (int ks = 0; ks < OZ_BK / 32; ++ks)
-                        for (int g = 0; g < s; ++g)
-                            for (int p = 0; p <= g; ++p) {
-                                const uint64_t da = umma_desc(abase + p * A_TILE + ks * 256);
-                                const uint64_t db = umma_desc(bbase + (g - p) * B_TILE + ks * 256);
-                                const uint32_t accum = (kt > k_begin || ks > 0 || p > 0) ? 1u : 0u;
-                                umma_i8(tmem + uint32_t(g * OZ_BN), da, db, idesc, accum);
-                            }
-                    umma_commit(&empty[st]);
-                    if (kt + OZ_STAGES < KT) ok = load(kt + OZ_STAGES);
-                }
-                if (!ok) atomicExch(a.err, 1);
-                umma_commit(done);  // arrives once every MMA issued so far has completed
-            }
-            __syncwarp();
-            // the MMAs issued so far always complete: their wait keeps the fixed limit even when
-            // the error word is set, so TMEM is never released under a running MMA
-            bool ready = true;
-            {
-                const unsigned long long t0 = global_ns();
-                while (!mbar_try(done, rounds & 1u))
-                    if (global_ns() - t0 > WAIT_LIMIT_NS) {
-                        atomicExch(a.err, 1);
-                        ready = false;
+    if (warp == OZ_LOAD_WARP) {
+        if (lane == 0) {
+            uint32_t gs = 0;
+            bool ok = true;
+            for (uint32_t tile = blockIdx.x; tile < a.n_tiles && ok; tile += gridDim.x) {
+                const OzTile tl = a.tiles[tile];
+                const OzPB pb = a.pbs[tl.pb];
+                for (uint32_t kt = pb.slab_begin; kt < pb.slab_end; ++kt, ++gs) {
+                    const uint32_t st = gs % nst;
+                    if (gs >= nst && !mbar_wait(&empty[st], ((gs / nst) - 1) & 1u, a.err, a.wait_ns)) {
+                        ok = false;
                         break;
                     }
+                    const OzSlab sl = a.slabs[kt];
+                    unsigned char* base = smem + st * stage_bytes;
+                    mbar_expect_tx(&full[st], stage_bytes);
+                    bulk_load(base, a.A8 + (sl.a_off + uint64_t(tl.mt) * sl.a_ts) * s, a_bytes, &full[st]);
+                    bulk_load(base + a_bytes, a.B8 + (sl.b_off + uint64_t(tl.nt) * sl.b_ts) * s,
+                              uint32_t(s) * B_TILE, &full[st]);
+                }
             }
-            ++rounds;
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const bool go = __all_sync(0xffffffffu, ready && *verr == 0);
-            if (go) {
-                const uint32_t row = mt * OZ_BM + warp * 32 + lane;
-                const int erow = (row < pb.M) ? a.e[pb.e_off + row] : 0;
-                const bool add = pb.beta || ch > 0;
-                double* Cb = reinterpret_cast<double*>(base_of(a.bases, pb.C.buf) + 8ull * pb.C.off);
-                for (int c0 = 0; c0 < OZ_BN; c0 += 16) {
-                    double acc[16];
+            issued = gs;
+        }
+        __syncwarp();
+    } else if (warp == OZ_MMA_WARP) {
+        if (lane == 0) {
+            const uint32_t idesc = idesc_i8(OZ_BM, OZ_BN);
+            uint32_t gs = 0, rounds = 0;
+            bool ok = true;
+            for (uint32_t tile = blockIdx.x; tile < a.n_tiles && ok; tile += gridDim.x) {
+                const OzPB pb = a.pbs[a.tiles[tile].pb];
+                const uint32_t KT = pb.slab_end - pb.slab_begin;
+                const uint32_t nch = KT ? (KT + a.chunk - 1) / a.chunk : 1;
+                for (uint32_t ch = 0; ch < nch && ok; ++ch) {
+                    // the accumulators are free once the epilogue of the previous round has read them
+                    if (rounds > 0 && !mbar_wait_suspend(tempty, (rounds - 1) & 1u, a.err)) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t k_begin = ch * a.chunk, k_end = min(KT, k_begin + a.chunk);
+                    for (uint32_t kt = k_begin; kt < k_end; ++kt, ++gs) {
+                        const uint32_t st = gs % nst;
+                        if (!mbar_wait(&full[st], (gs / nst) & 1u, a.err, a.wait_ns)) {
+                            ok = false;
+                            break;
+                        }
+                        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                        const uint32_t abase = smem_u32(smem + st * stage_bytes);
+                        const uint32_t bbase = abase + a_bytes;
+                        for (int g = 0; g < s; ++g)
+                            for (int p = 0; p <= g; ++p)
+                                umma_i8(tmem + uint32_t(g * OZ_BN), umma_desc(abase + p * A_TILE),
+                                        umma_desc(bbase + (g - p) * B_TILE), idesc, (kt > k_begin || p > 0) ? 1u : 0u);
+                        umma_commit(&empty[st]);  // the stage is free once these MMAs complete
+                    }
+                    if (!ok) break;
+                    umma_commit(tfull);  // the chunk's sums are complete once every MMA issued so far is
+                    ++rounds;
+                }
+            }
+            *consumed_slot = gs;
+            umma_commit(fin);  // every MMA this thread issued
+        }
+        __syncwarp();
+    } else {
+        // epilogue warps: TMEM lanes warp * 32 .. + 31 are rows warp * 32 .. of the tile
+        uint32_t rounds = 0;
+        bool ok = true;
+        for (uint32_t tile = blockIdx.x; tile < a.n_tiles && ok; tile += gridDim.x) {
+            const OzTile tl = a.tiles[tile];
+            const OzPB pb = a.pbs[tl.pb];
+            const uint32_t KT = pb.slab_end - pb.slab_begin;
+            const uint32_t nch = KT ? (KT + a.chunk - 1) / a.chunk : 1;
+            const uint32_t row = tl.mt * OZ_BM + warp * 32 + lane;
+            const int erow = (row < pb.M) ? a.e[pb.e_off + row] : 0;
+            double* crow = nullptr;
+            uint64_t ldc = pb.C.ld;
+            if (row < pb.M) {
+                // the row's start and leading dimension: from the row table or the plain operand
+                if (pb.rowtab != DevProb::NO_ROWS) {
+                    const DevRow rw = a.rowtab[pb.rowtab + row];
+                    crow = reinterpret_cast<double*>(base_of(a.bases, pb.C.buf)) + rw.c_off +
+                           uint64_t(pb.batch) * rw.cbs;
+                    ldc = rw.ld;
+                } else {
+                    crow = reinterpret_cast<double*>(base_of(a.bases, pb.C.buf) + 8ull * pb.C.off) + row;
+                }
+            }
+            for (uint32_t ch = 0; ch < nch; ++ch) {
+                if (!mbar_wait_suspend(tfull, rounds & 1u, a.err)) {
+                    ok = false;
+                    break;
+                }
+                ++rounds;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                double acc[OZ_BN];
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) acc[j] = 0.0;
-                    for (int g = s - 1; g >= 0 && KT > 0; --g) {
+                for (int j = 0; j < OZ_BN; ++j) acc[j] = 0.0;
+                for (int g = s - 1; g >= 0 && KT > 0; --g) {
+                    const double w = pow2_normal(-7 * (g + 2));
+#pragma unroll
+                    for (int c0 = 0; c0 < OZ_BN; c0 += 16) {
                         int32_t v[16];
                         tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + uint32_t(g * OZ_BN + c0), v);
-                        const double w = ldexp(1.0, -7 * (g + 2));
 #pragma unroll
-                        for (int j = 0; j < 16; ++j) acc[j] += double(v[j]) * w;
+                        for (int j = 0; j < 16; ++j) acc[c0 + j] += i2d_exact(v[j]) * w;
                     }
-                    if (row < pb.M) {
-                        // the row's start and leading dimension: from the row table or the plain operand
-                        double* crow = Cb + row;
-                        uint64_t ldc = pb.C.ld;
-                        if (pb.rowtab != DevProb::NO_ROWS) {
-                            const DevRow rw = a.rowtab[pb.rowtab + row];
-                            crow = reinterpret_cast<double*>(base_of(a.bases, pb.C.buf)) + rw.c_off +
-                                   uint64_t(pb.batch) * rw.cbs;
-                            ldc = rw.ld;
-                        }
+                }
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                __syncwarp();
+                if (lane == 0) mbar_arrive(tempty);
+                if (crow) {
+                    const bool add = pb.beta || ch > 0;
 #pragma unroll
-                        for (int j = 0; j < 16; ++j) {
-                            const uint32_t col = nt * OZ_BN + c0 + j;
-                            if (col < pb.N) {
-                                const double val = ldexp(acc[j], erow + a.e[pb.f_off + col]);
-                                double* dst = crow + uint64_t(col) * ldc;
-                                *dst = add ? *dst + val : val;
-                            }
+                    for (int j = 0; j < OZ_BN; ++j) {
+                        const uint32_t col = tl.nt * OZ_BN + j;
+                        if (col < pb.N) {
+                            // x 2^(e_row + e_col): one multiplication by the exact power where it is
+                            // normal (the value ldexp gives), ldexp otherwise
+                            const int ex = erow + a.e[pb.f_off + col];
+                            const double val = (ex >= -1022 && ex <= 1023) ? acc[j] * pow2_normal(ex) : ldexp(acc[j], ex);
+                            double* dst = crow + uint64_t(col) * ldc;
+                            *dst = add ? *dst + val : val;
                         }
                     }
                 }
             }
-            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-            __syncthreads();
-            failed = (*verr != 0);
-            __syncthreads();
         }
-        slab0 += KT;
     }
-    if (threadIdx.x == 0) {
-        // after a timeout: let the bulk copies still in flight land before the CTA leaves (bounded);
-        // slabs are issued and consumed in global order, so `consumed` is the next slab's index
-        for (; consumed < issued; ++consumed) {
-            unsigned long long t0 = global_ns();
-            while (!mbar_try(&full[consumed % OZ_STAGES], (consumed / OZ_STAGES) & 1u) &&
-                   global_ns() - t0 < WAIT_LIMIT_NS) {
-            }
-        }
+    __syncthreads();
+    if (warp == OZ_MMA_WARP && lane == 0) oz_settle(fin, 0, a.err);
+    if (warp == OZ_LOAD_WARP && lane == 0) {
+        // copies still in flight after a stop land before the CTA leaves; slabs are issued
+        // and consumed in order, so they are the slabs consumed .. issued - 1
+        for (uint32_t g = *consumed_slot; g < issued; ++g) oz_settle(&full[g % nst], (g / nst) & 1u, a.err);
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
 }
 
 }  // namespace
 
-size_t ozaki_smem_bytes(int s) { return size_t(OZ_STAGES) * s * (A_TILE + B_TILE) + 8 * (2 * OZ_STAGES + 1) + 16; }
+size_t ozaki_smem_bytes(int s) { return size_t(oz_stages(s)) * s * (A_TILE + B_TILE) + OZ_BAR_BYTES; }
 
 // Operands held in boundary memory (BUF_ABS) do not change between calls of a
 // plan: their digit planes and exponents are computed on the first run and kept
@@ -397,7 +612,11 @@ struct OzProgram {
     uint64_t a_plane = 0, b_plane = 0, n_exp = 0, n_exp_c = 0;
     bool const_ready = false;       // constant digit planes present in the scratch
     std::vector<DevRow> rowtab;     // rows of row-table problems (the GEMM list's table)
+    // first warp item of every job in the exponent and split passes (jobs + 1 entries)
+    std::vector<uint64_t> exp_first, split_first;
     OzSplit* d_jobs = nullptr;
+    uint64_t* d_exp_first = nullptr;
+    uint64_t* d_split_first = nullptr;
     OzPB* d_pbs = nullptr;
     OzSlab* d_slabs = nullptr;
     OzTile* d_tiles = nullptr;
@@ -504,7 +723,14 @@ OzProgram* oz_build(GemmList const& gl) {
         return cudaMemcpy(*d, v.data(), v.size() * sizeof(v[0]), cudaMemcpyHostToDevice);
     };
     oz->rowtab = gl.rowtab;
-    if (up(oz->jobs, &oz->d_jobs) != cudaSuccess || up(oz->pbs, &oz->d_pbs) != cudaSuccess ||
+    oz->exp_first.assign(1, 0);
+    oz->split_first.assign(1, 0);
+    for (auto const& j : oz->jobs) {
+        oz->exp_first.push_back(oz->exp_first.back() + oz_exp_items(j));
+        oz->split_first.push_back(oz->split_first.back() + oz_split_items(j, j.is_b ? OZ_BN : OZ_BM));
+    }
+    if (up(oz->jobs, &oz->d_jobs) != cudaSuccess || up(oz->exp_first, &oz->d_exp_first) != cudaSuccess ||
+        up(oz->split_first, &oz->d_split_first) != cudaSuccess || up(oz->pbs, &oz->d_pbs) != cudaSuccess ||
         up(oz->slabs, &oz->d_slabs) != cudaSuccess || up(oz->tiles, &oz->d_tiles) != cudaSuccess ||
         up(oz->rowtab, &oz->d_rowtab) != cudaSuccess) {
         oz_free(oz);
@@ -520,6 +746,8 @@ void oz_invalidate(OzProgram* oz) {
 void oz_free(OzProgram* oz) {
     if (!oz) return;
     cudaFree(oz->d_jobs);
+    cudaFree(oz->d_exp_first);
+    cudaFree(oz->d_split_first);
     cudaFree(oz->d_pbs);
     cudaFree(oz->d_slabs);
     cudaFree(oz->d_tiles);
@@ -563,18 +791,24 @@ cudaError_t oz_run(OzProgram* oz, Bases const& bs, int s, void* scratch, int* er
                                                                                         -100000);
     const uint32_t nj = uint32_t(oz->jobs.size()) - j0;
     if (nj) {
-        oz_exponents<<<dim3(8, std::min<uint32_t>(nj, 65535u)), 256, 0, st>>>(oz->d_jobs + j0, nj, bs, c.e,
-                                                                             oz->d_rowtab);
-        dim3 grid(16, std::min<uint32_t>(nj, 65535u));
-        oz_split<<<grid, 256, 0, st>>>(oz->d_jobs + j0, nj, bs, c.e, s, oz->a_plane, c.A8, oz->b_plane, c.B8,
-                                       oz->d_rowtab);
+        // 8 warps a block; at most 8 blocks an SM, the warps stride over the items
+        auto blocks = [&](std::vector<uint64_t> const& first) {
+            const uint64_t items = first[j0 + nj] - first[j0];
+            return uint32_t(std::max<uint64_t>(1, std::min<uint64_t>((items + 7) / 8, uint64_t(sms) * 8)));
+        };
+        oz_exponents<<<blocks(oz->exp_first), 256, 0, st>>>(oz->d_jobs + j0, oz->d_exp_first + j0, nj, bs, c.e,
+                                                            oz->d_rowtab);
+        oz_split<<<blocks(oz->split_first), 256, 0, st>>>(oz->d_jobs + j0, oz->d_split_first + j0, nj, bs, c.e, s,
+                                                          c.A8, c.B8, oz->d_rowtab);
     }
     oz->const_ready = true;
     if (!oz->tiles.empty()) {
-        cudaError_t ea = ensure_smem_limit(reinterpret_cast<const void*>(ozaki_mma), int(ozaki_smem_bytes(OZ_MAX_SLICES)));
+        size_t smem_max = 0;
+        for (int sl = 2; sl <= OZ_MAX_SLICES; ++sl) smem_max = std::max(smem_max, ozaki_smem_bytes(sl));
+        cudaError_t ea = ensure_smem_limit(reinterpret_cast<const void*>(ozaki_mma), int(smem_max));
         if (ea != cudaSuccess) return ea;
-        OzArgs args{c.A8, c.B8, oz->a_plane, oz->b_plane, c.e, oz->d_pbs, oz->d_slabs, oz->d_tiles,
-                    uint32_t(oz->tiles.size()), oz_chunk_slabs(s), s, bs, err, oz->d_rowtab, wait_limit_ns()};
+        OzArgs args{c.A8,        c.B8, c.e, oz->d_pbs, oz->d_slabs, oz->d_tiles, uint32_t(oz->tiles.size()),
+                    oz_chunk_slabs(s), oz_stages(s), s, bs, err, oz->d_rowtab, wait_limit_ns()};
         ozaki_mma<<<std::min<uint32_t>(uint32_t(oz->tiles.size()), uint32_t(sms)), OZ_THREADS, ozaki_smem_bytes(s),
                     st>>>(args);
     }

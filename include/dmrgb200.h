@@ -462,6 +462,25 @@ dmrgb200_status dmrgb200_hpsi_noalloc(const dmrgb200_plan_desc* desc, const dmrg
 dmrgb200_status dmrgb200_step_execute(dmrgb200_plan_t plan, const double* ket, const double* bra,
                                       const dmrgb200_boundary_view* out, void* cuda_stream);
 
+/* Density matrix of a two-site split with the state prediction (perturbation) on a
+ * LEFT_STEP / RIGHT_STEP plan built for the two-site tensor Theta viewed as one site
+ * (ket = bra = Theta; left step: site 1 with the middle index as its right bond,
+ * right step: site 2 with the middle index as its left bond; boundary skipping off):
+ *   left step:  dm[b] = Theta_b Theta_b^T + alpha sum_{c: c_lb = b} S_c S_c^T
+ *   right step: dm[b] = Theta_b^T Theta_b + alpha sum_{c: c_rb = b} S_c^T S_c
+ * for every bra block b (left-paired blocks for the left step, right-paired for the
+ * right step); S_c is the cohort's S of the step.  ket and bra are Theta in the
+ * layouts dmrgb200_step_execute takes (ket right-paired; bra left-paired for the left
+ * step, right-paired for the right step).  dm->cohort_ptr[b] is a device
+ * stripe_b x stripe_b column-major block (stripe_b = out_rows[b] for the left step,
+ * out_cols[b] for the right step), overwritten; alpha >= 0.  Stream-ordered (the
+ * host-side lowering happens on the first call with a given dm binding).
+ * Replaces the GPU side of alpha_dm / alpha_dm_right with alpha_dm_direct and
+ * Cohort::lbtm / rbtm (prediction.hpp:41-69, move_boundary.hpp:38-143,
+ * tasks.cpp:346-380), used by predict_split_l2r / r2l (prediction.hpp:152-240). */
+dmrgb200_status dmrgb200_step_alpha_dm(dmrgb200_plan_t plan, const double* ket, const double* bra,
+                                       const dmrgb200_boundary_view* dm, double alpha, void* cuda_stream);
+
 /* ---- library-side schedule builder (host only) -------------------------- */
 /* Index description: n sectors, charges[2*i+0..1] (U1 uses component 0),
  * sizes[i]. */

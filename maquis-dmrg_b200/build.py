@@ -19,7 +19,8 @@ INCLUDE = HERE.parent / "include"
 CUDA = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
 
 CXX_SOURCES = ["coupling.cpp", "schedule.cpp", "plan.cpp", "capi.cpp", "per_block.cpp"]
-CU_SOURCES = ["kernels_fp64.cu", "noalloc.cu", "jd.cu", "jd_graph.cu", "ozaki.cu", "adjoint.cu", "block_svd.cu"]
+CU_SOURCES = ["kernels_fp64.cu", "noalloc.cu", "jd.cu", "jd_graph.cu", "ozaki.cu", "adjoint.cu", "block_svd.cu",
+              "alpha_dm.cu"]
 HEADERS = ["symm.hpp", "mpo.hpp", "coupling.hpp", "boundary_index.hpp", "schedule.hpp", "plan.hpp",
            "device.hpp", "async_copy.cuh"]
 

@@ -78,13 +78,15 @@ __global__ void __launch_bounds__(256) tgrad_cells(const DevSLine* __restrict__ 
 
 // galpha of the terms of grouped units (DevSGroup, built for the forward S build):
 // gram[entry * SG_LINES + j] = <G line j of the group, T source of the entry>, one
-// warp per (group, batch of AG_BATCH entries).  Per 128-element chunk every lane
-// holds the 8 lines' G values of its 4 elements; per entry it forms 8 partial
-// products, which a reduce-scatter butterfly (9 shuffles) sums over the warp so that
-// lanes 4j .. 4j+3 end with line j's total; the chunks add up in order, so the
-// result is bitwise reproducible.  A term's galpha is then its (entry, line) slot.
-constexpr int AG_BATCH = 16;
-__device__ __forceinline__ double sum8_scatter(double const (&p)[SG_LINES], uint32_t lane) {
+// warp per (group, batch of AG_BATCH entries, half of the group's lines).  Per
+// 128-element chunk every lane holds the half's 8 lines' G values of its 4 elements;
+// per entry it forms 8 partial products, which a reduce-scatter butterfly (9
+// shuffles) sums over the warp so that lanes 4j .. 4j+3 end with line j's total;
+// the chunks add up in order, so the result is bitwise reproducible.  A term's
+// galpha is then its (entry, line) slot.
+constexpr int AG_BATCH = 16, AG_LINES = 8, AG_HALVES = SG_LINES / AG_LINES;
+static_assert(SG_LINES % AG_LINES == 0, "line groups in halves of 8");
+__device__ __forceinline__ double sum8_scatter(double const (&p)[AG_LINES], uint32_t lane) {
     const bool h1 = (lane >> 4) & 1u, h2 = (lane >> 3) & 1u, h3 = (lane >> 2) & 1u;
     double q[4], r[2];
 #pragma unroll
@@ -100,16 +102,19 @@ __device__ __forceinline__ double sum8_scatter(double const (&p)[SG_LINES], uint
     double v = (h3 ? r[1] : r[0]) + __shfl_xor_sync(0xffffffffu, h3 ? r[0] : r[1], 4);
     v += __shfl_xor_sync(0xffffffffu, v, 2);
     v += __shfl_xor_sync(0xffffffffu, v, 1);
-    return v;  // the line (lane >> 2) & 7
+    return v;  // the line (lane >> 2) & 7 of the half
 }
 
+// items: DevSItem{group, entry} per batch; the warp item it covers half it % AG_HALVES
 __global__ void __launch_bounds__(128) gram_groups(const DevSGroup* __restrict__ groups,
                                                    const DevSItem* __restrict__ items, uint32_t n_items,
                                                    const uint64_t* __restrict__ ent_t, const double* __restrict__ G,
                                                    const double* __restrict__ T, double* __restrict__ gram) {
     const uint32_t lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
-    for (uint32_t it = blockIdx.x * wpb + (threadIdx.x >> 5); it < n_items; it += gridDim.x * wpb) {
-        const DevSItem I = items[it];
+    const uint32_t n_work = n_items * AG_HALVES;
+    for (uint32_t w = blockIdx.x * wpb + (threadIdx.x >> 5); w < n_work; w += gridDim.x * wpb) {
+        const DevSItem I = items[w / AG_HALVES];
+        const uint32_t j0 = (w % AG_HALVES) * AG_LINES;
         const DevSGroup Gr = groups[I.group];
         const uint32_t n = Gr.rows * Gr.cols, nb = min(uint32_t(AG_BATCH), Gr.ent_end - I.e0);
         const uint64_t my_tb = lane < nb ? ent_t[I.e0 + lane] : 0;
@@ -117,7 +122,7 @@ __global__ void __launch_bounds__(128) gram_groups(const DevSGroup* __restrict__
 #pragma unroll
         for (int b = 0; b < AG_BATCH; ++b) acc[b] = 0.0;
         for (uint32_t c0 = 0; c0 < n; c0 += 32 * SG_EPT) {
-            double g[SG_LINES][SG_EPT];
+            double g[AG_LINES][SG_EPT];
             uint32_t el[SG_EPT];
             bool in[SG_EPT];
 #pragma unroll
@@ -127,8 +132,8 @@ __global__ void __launch_bounds__(128) gram_groups(const DevSGroup* __restrict__
                 const uint32_t col = in[u] ? el[u] / Gr.rows : 0, i = in[u] ? el[u] - col * Gr.rows : 0;
                 const double* src = G + Gr.s_base + i + uint64_t(col) * Gr.ld_s;
 #pragma unroll
-                for (int j = 0; j < SG_LINES; ++j)
-                    g[j][u] = (in[u] && uint32_t(j) < Gr.nlines) ? src[uint64_t(j) * Gr.line_stride] : 0.0;
+                for (int j = 0; j < AG_LINES; ++j)
+                    g[j][u] = (in[u] && j0 + j < Gr.nlines) ? src[uint64_t(j0 + j) * Gr.line_stride] : 0.0;
             }
 #pragma unroll
             for (int b = 0; b < AG_BATCH; ++b) {
@@ -137,9 +142,9 @@ __global__ void __launch_bounds__(128) gram_groups(const DevSGroup* __restrict__
                 double t[SG_EPT];
 #pragma unroll
                 for (int u = 0; u < SG_EPT; ++u) t[u] = in[u] ? T[tb + el[u]] : 0.0;
-                double p[SG_LINES];
+                double p[AG_LINES];
 #pragma unroll
-                for (int j = 0; j < SG_LINES; ++j) {
+                for (int j = 0; j < AG_LINES; ++j) {
                     double a = 0.0;
 #pragma unroll
                     for (int u = 0; u < SG_EPT; ++u) a = fma(g[j][u], t[u], a);
@@ -150,12 +155,13 @@ __global__ void __launch_bounds__(128) gram_groups(const DevSGroup* __restrict__
         }
 #pragma unroll
         for (int b = 0; b < AG_BATCH; ++b)
-            if (uint32_t(b) < nb && (lane & 3u) == 0) gram[uint64_t(I.e0 + b) * SG_LINES + (lane >> 2)] = acc[b];
+            if (uint32_t(b) < nb && (lane & 3u) == 0)
+                gram[uint64_t(I.e0 + b) * SG_LINES + j0 + (lane >> 2)] = acc[b];
     }
 }
 
 // gT of T blocks taken as cell groups (DevTGroup): one warp per 128 elements of a
-// group; each lane keeps SG_LINES x SG_EPT accumulators (one per cell) and reads
+// group; each lane keeps TG_CELLS x SG_EPT accumulators (one per cell) and reads
 // every G line of the group once for all its cells; cells sum their lines in the
 // group's entry order.
 __global__ void __launch_bounds__(256) tgrad_groups(const DevTGroup* __restrict__ groups,
@@ -178,9 +184,9 @@ __global__ void __launch_bounds__(256) tgrad_groups(const DevTGroup* __restrict_
             ci[u] = in[u] ? el[u] / Gr.rows : 0;
             ri[u] = in[u] ? el[u] - ci[u] * Gr.rows : 0;
         }
-        double acc[SG_LINES][SG_EPT];
+        double acc[TG_CELLS][SG_EPT];
 #pragma unroll
-        for (int j = 0; j < SG_LINES; ++j)
+        for (int j = 0; j < TG_CELLS; ++j)
 #pragma unroll
             for (int u = 0; u < SG_EPT; ++u) acc[j][u] = 0.0;
         for (uint32_t k = Gr.ent_begin; k < Gr.ent_end; ++k) {
@@ -189,9 +195,9 @@ __global__ void __launch_bounds__(256) tgrad_groups(const DevTGroup* __restrict_
             double v[SG_EPT];
 #pragma unroll
             for (int u = 0; u < SG_EPT; ++u) v[u] = in[u] ? g[ri[u] + ci[u] * ld] : 0.0;
-            const double2* a2 = reinterpret_cast<const double2*>(ent_a + uint64_t(k) * SG_LINES);
+            const double2* a2 = reinterpret_cast<const double2*>(ent_a + uint64_t(k) * TG_CELLS);
 #pragma unroll
-            for (int h = 0; h < SG_LINES / 2; ++h) {
+            for (int h = 0; h < TG_CELLS / 2; ++h) {
                 const double2 x = a2[h];
 #pragma unroll
                 for (int u = 0; u < SG_EPT; ++u) {
@@ -204,7 +210,7 @@ __global__ void __launch_bounds__(256) tgrad_groups(const DevTGroup* __restrict_
         for (int u = 0; u < SG_EPT; ++u) {
             if (!in[u]) continue;
 #pragma unroll
-            for (int c = 0; c < SG_LINES; ++c)
+            for (int c = 0; c < TG_CELLS; ++c)
                 if (uint32_t(c) < Gr.ncells)
                     gT[Gr.out_base + uint64_t(c) * n + el[u]] = ((Gr.mask >> c) & 1u) ? acc[c][u] : 0.0;
         }
@@ -304,8 +310,8 @@ std::string compile_adjoint(FlatPlan const& p, std::vector<uint64_t> const& stag
         // (and the blocks average 4 or more terms); the other blocks keep the walk
         std::vector<char> grouped_b(p.t_nb[t], 0);
         if (uint64_t(M) * N)
-            for (uint32_t b0 = 0; b0 < p.t_nb[t]; b0 += SG_LINES) {
-                const uint32_t ncell = std::min<uint32_t>(SG_LINES, p.t_nb[t] - b0);
+            for (uint32_t b0 = 0; b0 < p.t_nb[t]; b0 += TG_CELLS) {
+                const uint32_t ncell = std::min<uint32_t>(TG_CELLS, p.t_nb[t] - b0);
                 uint64_t nterms = 0;
                 for (uint32_t c = 0; c < ncell; ++c) nterms += block_terms[tb_base[t] + b0 + c].size();
                 if (nterms < 4ull * ncell) continue;
@@ -313,7 +319,7 @@ std::string compile_adjoint(FlatPlan const& p, std::vector<uint64_t> const& stag
                 for (uint32_t c = 0; c < ncell; ++c)
                     for (uint32_t i : block_terms[tb_base[t] + b0 + c])
                         slot.emplace(std::make_pair(a.aterms[i].g_base, a.aterms[i].ld_g), 0u);
-                if (uint64_t(slot.size()) * SG_LINES > 2 * nterms) continue;
+                if (uint64_t(slot.size()) * TG_CELLS > 2 * nterms) continue;
                 DevTGroup G{};
                 G.out_base = t_off[t] + uint64_t(b0) * M * N;
                 G.rows = M;
@@ -325,13 +331,13 @@ std::string compile_adjoint(FlatPlan const& p, std::vector<uint64_t> const& stag
                     kv.second = e++;
                     a.tg_g.push_back(kv.first.first);
                     a.tg_ld.push_back(kv.first.second);
-                    a.tg_a.insert(a.tg_a.end(), SG_LINES, 0.0);
+                    a.tg_a.insert(a.tg_a.end(), TG_CELLS, 0.0);
                 }
                 G.ent_end = e;
                 for (uint32_t c = 0; c < ncell; ++c)
                     for (uint32_t i : block_terms[tb_base[t] + b0 + c]) {
                         DevATerm const& at = a.aterms[i];
-                        a.tg_a[uint64_t(slot[{at.g_base, at.ld_g}]) * SG_LINES + c] += p.term_alpha[at.k];
+                        a.tg_a[uint64_t(slot[{at.g_base, at.ld_g}]) * TG_CELLS + c] += p.term_alpha[at.k];
                         G.mask |= 1u << c;
                     }
                 const uint32_t gi = uint32_t(a.tgroups.size());
@@ -501,7 +507,7 @@ cudaError_t run_adjoint(DeviceProgram const& fwd, AdjointProgram const& a, uint6
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
         if (a.n_gram_items) {
-            uint32_t grid = std::min<uint32_t>((a.n_gram_items + 3) / 4, sms * 8);
+            uint32_t grid = std::min<uint32_t>((a.n_gram_items * AG_HALVES + 3) / 4, sms * 8);
             gram_groups<<<grid, 128, 0, stream>>>(fwd.d_groups, a.d_gram_items, a.n_gram_items, fwd.d_gent_t, S, T,
                                                   a.d_gram);
             if ((e = cudaGetLastError()) != cudaSuccess) return e;

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <exception>
@@ -104,6 +105,16 @@ struct dmrgb200_plan_s {
         step_T = step_S = nullptr;
         step_valid = false;
         step_outp.clear();
+    }
+    // density matrix with the perturbation (dmrgb200_step_alpha_dm): the grouped GEMM
+    // of the last dm binding
+    bool dm_valid = false;
+    std::vector<uint64_t> dm_ptrs;
+    GemmDev dm_gemm;
+    void drop_dm() {
+        if (dm_valid) free_gemm(dm_gemm);
+        dm_valid = false;
+        dm_ptrs.clear();
     }
     // cuBLAS handle of the per-block comparison path (dmrgb200_hpsi_per_block)
     void* blas = nullptr;
@@ -622,6 +633,7 @@ dmrgb200_status dmrgb200_plan_destroy(dmrgb200_plan_t plan) {
     jd_graph_free(plan->jd);
     blas_handle_free(plan->blas);
     plan->drop_step();
+    plan->drop_dm();
     oz_free(plan->oz1);
     oz_free(plan->oz3);
     cudaFree(plan->oz_scratch);
@@ -899,6 +911,73 @@ dmrgb200_status dmrgb200_plan_stage_times(dmrgb200_plan_t plan, double ms[3], ui
     if (flops) plan->flat.stage_flops(flops);
     if (calls) *calls = plan->timed_calls;
     return DMRGB200_OK;
+}
+
+dmrgb200_status dmrgb200_step_alpha_dm(dmrgb200_plan_t plan, const double* ket, const double* bra,
+                                       const dmrgb200_boundary_view* dm, double alpha, void* cuda_stream) {
+    DMRGB200_TRY
+    if (!plan || !ket || !bra || !dm) return fail(DMRGB200_INVALID_ARGUMENT, "null argument");
+    if (!(alpha >= 0.0)) return fail(DMRGB200_INVALID_ARGUMENT, "alpha must be >= 0");
+    FlatPlan const& p = plan->flat;
+    const bool left = p.kind == KIND_LEFT;
+    if (!left && p.kind != KIND_RIGHT) return fail(DMRGB200_INVALID_PLAN, "alpha_dm needs a left or right step plan");
+    const uint32_t nb = uint32_t(p.out_rows.size());
+    std::vector<uint64_t> ptrs = view_ptrs(dm);
+    if (ptrs.size() < nb) return fail(DMRGB200_INVALID_ARGUMENT, "dm view has fewer blocks than the bra");
+    ptrs.resize(nb);
+    for (uint32_t b = 0; b < nb; ++b)
+        if (!ptrs[b] && (left ? p.out_rows[b] : p.out_cols[b]))
+            return fail(DMRGB200_INVALID_ARGUMENT, "dm view misses a block");
+    for (uint32_t c = 0; c < p.n_cohorts(); ++c) {
+        const uint32_t b = left ? p.c_lb[c] : p.c_rb[c];
+        if (b >= nb || p.c_stripe[c] != (left ? p.out_rows[b] : p.out_cols[b]))
+            return fail(DMRGB200_INVALID_PLAN, "cohort stripe differs from its bra block");
+    }
+    cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
+    cudaError_t e;
+    if (!plan->step_valid) {
+        // stages 1 and 2 of the step program; its stage 3 (never launched here) gets
+        // placeholder output addresses, so a later dmrgb200_step_execute lowers it again
+        uint32_t nout = 0;
+        for (uint32_t c = 0; c < p.n_cohorts(); ++c) nout = std::max(nout, p.c_out_ci[c] + 1);
+        std::vector<uint64_t> placeholder(nout, 8);
+        compile_program(p, {}, plan->stage1_bnd, placeholder, plan->step_prog, true, true);
+        if ((e = upload_program(plan->step_prog)) != cudaSuccess) {
+            free_program(plan->step_prog);
+            return cuda_fail(e, "alpha_dm step upload");
+        }
+        plan->step_valid = true;
+        plan->step_outp = placeholder;
+        if (plan->step_prog.t_elems &&
+            (e = cudaMalloc(&plan->step_T, plan->step_prog.t_elems * sizeof(double))) != cudaSuccess) {
+            plan->drop_step();
+            return cuda_fail(e, "alpha_dm T scratch");
+        }
+        if (plan->step_prog.s_elems &&
+            (e = cudaMalloc(&plan->step_S, plan->step_prog.s_elems * sizeof(double))) != cudaSuccess) {
+            plan->drop_step();
+            return cuda_fail(e, "alpha_dm S scratch");
+        }
+    }
+    if (!plan->dm_valid || plan->dm_ptrs != ptrs) {
+        plan->drop_dm();
+        GemmList gl;
+        build_alpha_dm(p, ptrs, gl);
+        if ((e = upload_gemm(gl, plan->dm_gemm)) != cudaSuccess) return cuda_fail(e, "alpha_dm tables");
+        plan->dm_valid = true;
+        plan->dm_ptrs = ptrs;
+    }
+    const uint64_t ki = reinterpret_cast<uint64_t>(ket), bo = reinterpret_cast<uint64_t>(bra);
+    if ((e = run_stages12(plan->step_prog, ki, bo, plan->step_T, plan->step_S, stream)) != cudaSuccess)
+        return cuda_fail(e, "alpha_dm S build");
+    if ((e = scale_buffer(plan->step_S, plan->step_prog.s_elems, std::sqrt(alpha), stream)) != cudaSuccess)
+        return cuda_fail(e, "alpha_dm scale");
+    Bases bs{};
+    bs.b[BUF_OUT] = bo;
+    bs.b[BUF_S] = reinterpret_cast<uint64_t>(plan->step_S);
+    if ((e = launch_gemm(plan->dm_gemm, bs, stream)) != cudaSuccess) return cuda_fail(e, "alpha_dm GEMM");
+    return DMRGB200_OK;
+    DMRGB200_CATCH
 }
 
 dmrgb200_status dmrgb200_step_execute(dmrgb200_plan_t plan, const double* ket, const double* bra,

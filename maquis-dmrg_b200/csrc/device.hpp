@@ -73,7 +73,9 @@ struct DevSTerm {
 // read the cell, duplicate sources of a line summed).  Line j of the group
 // starts at s_base + j * line_stride; element (i, c) of a line sits at
 // i + c * ld_s, its source at t_base + i + c * rows.
-constexpr int SG_LINES = 8, SG_UNROLL = 4, SG_EPT = 4, SG_CHUNK = 32 * SG_EPT;
+constexpr int SG_LINES = 16, SG_UNROLL = 4, SG_EPT = 4, SG_CHUNK = 32 * SG_EPT;
+// cells of an adjoint T group (DevTGroup)
+constexpr int TG_CELLS = 8;
 struct DevSGroup {
     uint64_t s_base;
     uint32_t line_stride, ld_s, rows, cols;
@@ -163,6 +165,7 @@ struct DeviceProgram {
     int* d_err = nullptr;  // set by a grouped S build whose bulk-copy wait timed out
     unsigned char* d_arena = nullptr;  // the one allocation holding every table above
     uint32_t n_t1 = 0, n_t3 = 0, n_lines = 0, n_litems = 0, n_gitems = 0;
+    uint32_t n_gitems8 = 0;  // gitems[0, n_gitems8): groups of up to 8 lines (the narrow launch)
     TileLists x1, x3;  // tile lists of the other classes
     DevRow* d_r1 = nullptr;  // stage-1 row table (stacked T tasks)
     GemmList stage1_tasks;   // stage 1 as one problem per T task (when stage1 is stacked)
@@ -193,6 +196,17 @@ cudaError_t run_program(DeviceProgram const& prog, uint64_t in, uint64_t out, do
                         cudaStream_t stream, cudaEvent_t const* ev = nullptr);
 
 int device_sm_count();
+// stages 1 and 2 only (T and the S build), as run_program launches them
+cudaError_t run_stages12(DeviceProgram const& prog, uint64_t in, uint64_t out, double* T, double* S,
+                         cudaStream_t stream);
+
+// ---- density matrix of a split with the perturbation (alpha_dm.cu) ----
+// One grouped-GEMM problem per bra block b of a step plan, written at dm[b]
+// (stripe x stripe, column-major): Theta_b Theta_b^T + sum_c S_c S_c^T (left step) or
+// Theta_b^T Theta_b + sum_c S_c^T S_c (right step), over the cohorts c of block b with
+// S as the step's S build leaves it (scaled by sqrt(alpha) beforehand) and Theta the bra.
+void build_alpha_dm(FlatPlan const& p, std::vector<uint64_t> const& dm, GemmList& gl);
+cudaError_t scale_buffer(double* x, uint64_t n, double a, cudaStream_t st);
 
 // ---- lowering helpers shared by the forward and adjoint programs ----
 DevOp dev_op(uint16_t buf, uint64_t off, uint32_t ld, bool trans, uint64_t bstride = 0);
@@ -249,7 +263,7 @@ struct DevATerm {
     uint32_t rows, cols, ld_g, ld_t;
     uint32_t k, pad;
 };
-// adjoint gT of up to SG_LINES consecutive T blocks (cells) of one T task over the union
+// adjoint gT of up to TG_CELLS consecutive T blocks (cells) of one T task over the union
 // of their G lines: cell c is rows x cols at out_base + c * rows * cols
 struct DevTGroup {
     uint64_t out_base;

@@ -380,27 +380,125 @@ __global__ void __launch_bounds__(256) sbuild_lines(const DevSLine* __restrict__
 // bounded (2 s; the thread is suspended while it waits): on a timeout the warp
 // records it in *err, lets its copies land (bounded) and stops.  Each line sums
 // its sources in the group's entry order.
-constexpr int SGB_WARPS = 4, SGB_MINB = 3, SGB_STAGES = 2, SGB_NC = 8, SGB_ROW = SG_CHUNK + 2;
+// Groups of up to 8 lines run as one launch (8 accumulated lines, 2 stages, 3 CTAs per
+// SM), larger groups as another (SG_LINES lines, 3 stages, 2 CTAs per SM, for their
+// larger register file).
+constexpr int SGB_WARPS = 4, SGB_NC = 8, SGB_ROW = SG_CHUNK + 2;
+template <int STAGES>
 struct alignas(16) SgbRing {
-    double rows[SGB_STAGES][SGB_NC][SGB_ROW];
-    double alpha[SGB_STAGES][SGB_NC][SG_LINES];
-    uint64_t full[SGB_STAGES];
-    uint32_t shift[SGB_STAGES][SGB_NC];
+    double rows[STAGES][SGB_NC][SGB_ROW];
+    double alpha[STAGES][SGB_NC][SG_LINES];
+    uint64_t full[STAGES];
+    uint32_t shift[STAGES][SGB_NC];
 };
-static_assert(sizeof(double) * SGB_ROW % 16 == 0 && sizeof(SgbRing) % 16 == 0, "bulk copy alignment");
+static_assert(sizeof(double) * SGB_ROW % 16 == 0 && sizeof(SgbRing<2>) % 16 == 0 && sizeof(SgbRing<3>) % 16 == 0,
+              "bulk copy alignment");
 static_assert(SGB_NC < 32, "one lane per row plus one for the alphas");
-constexpr size_t SGB_SMEM = sizeof(SgbRing) * SGB_WARPS;
+template <int NL>
+struct SgbShape;
+template <>
+struct SgbShape<8> {
+    static constexpr int STAGES = 2, MINB = 3;
+};
+template <>
+struct SgbShape<SG_LINES> {
+    static constexpr int STAGES = 3, MINB = 2;
+};
+template <int NL>
+constexpr size_t sgb_smem() {
+    return sizeof(SgbRing<SgbShape<NL>::STAGES>) * SGB_WARPS;
+}
 
-__global__ void __launch_bounds__(32 * SGB_WARPS, SGB_MINB) sbuild_groups(const DevSGroup* __restrict__ groups,
-                                                                  const DevSItem* __restrict__ items, uint32_t n_items,
-                                                                  const uint64_t* __restrict__ ent_t,
-                                                                  const double* __restrict__ ent_a,
-                                                                  double* __restrict__ S, const double* __restrict__ T,
-                                                                  int* err, unsigned long long wait_ns) {
+// One work item of the grouped S build with NL accumulated lines (NL = 8 for groups of
+// at most 8 lines, SG_LINES otherwise; the alpha columns always hold SG_LINES entries).
+// Returns false when a wait failed (the warp then stops).
+template <int NL, int SGB_STAGES>
+__device__ __forceinline__ bool sgb_item(SgbRing<SGB_STAGES>& R, DevSGroup const& G, uint32_t e0,
+                                         const uint64_t* __restrict__ ent_t,
+                                         const double* __restrict__ ent_a, double* __restrict__ S,
+                                         const double* __restrict__ T, int* err, unsigned long long wait_ns,
+                                         uint32_t lane, uint32_t& issued, uint32_t& consumed) {
     using namespace async;
-    extern __shared__ __align__(16) unsigned char sgb_smem[];
+    const uint32_t n = G.rows * G.cols, cnt = min(uint32_t(SG_CHUNK), n - e0);
+    const uint32_t k0 = G.ent_begin, k1 = G.ent_end;
+    double acc[NL][SG_EPT];
+#pragma unroll
+    for (int j = 0; j < NL; ++j)
+#pragma unroll
+        for (int u = 0; u < SG_EPT; ++u) acc[j][u] = 0.0;
+    // every lane: the stage of sources kb .. kb + SGB_NC - 1 (those below k1)
+    auto fill = [&](uint32_t kb) {
+        const uint32_t slot = issued % SGB_STAGES, nc = min(uint32_t(SGB_NC), k1 - kb);
+        if (lane < nc) {
+            const uint64_t tb = ent_t[kb + lane];
+            const uint32_t sh = uint32_t((tb + e0) & 1u), sz = ((cnt + sh) * 8u + 15u) & ~15u;
+            R.shift[slot][lane] = sh;
+            mbar_expect_tx_only(&R.full[slot], sz);
+            bulk_load(R.rows[slot][lane], T + tb + e0 - sh, sz, &R.full[slot]);
+        } else if (lane == uint32_t(SGB_NC)) {
+            const uint32_t sz = nc * SG_LINES * uint32_t(sizeof(double));
+            mbar_expect_tx_only(&R.full[slot], sz);
+            bulk_load(R.alpha[slot], ent_a + uint64_t(kb) * SG_LINES, sz, &R.full[slot]);
+        }
+        __syncwarp();  // every expected byte count is in before the phase can complete
+        if (lane == 0) mbar_arrive(&R.full[slot]);
+        ++issued;
+    };
+    const uint32_t nst = (k1 - k0 + SGB_NC - 1) / SGB_NC;
+    for (uint32_t st = 0; st < min(nst, uint32_t(SGB_STAGES - 1)); ++st) fill(k0 + st * SGB_NC);
+    for (uint32_t st = 0; st < nst; ++st) {
+        const uint32_t slot = consumed % SGB_STAGES, kb = k0 + st * SGB_NC;
+        // the stage SGB_STAGES - 1 ahead goes into the slot freed in the previous step
+        if (st + SGB_STAGES - 1 < nst) {
+            fence_proxy_async_smem();
+            fill(k0 + (st + SGB_STAGES - 1) * SGB_NC);
+        }
+        const bool ok = mbar_wait_suspend(&R.full[slot], (consumed / SGB_STAGES) & 1u, err, wait_ns);
+        if (__any_sync(0xffffffffu, !ok)) return false;
+        const uint32_t nc = min(uint32_t(SGB_NC), k1 - kb);
+#pragma unroll 2
+        for (uint32_t c = 0; c < nc; ++c) {
+            const double* row = R.rows[slot][c] + R.shift[slot][c] + lane;
+            double v[SG_EPT];
+#pragma unroll
+            for (int u = 0; u < SG_EPT; ++u) v[u] = row[32 * u];
+            const double2* a2 = reinterpret_cast<const double2*>(R.alpha[slot][c]);
+#pragma unroll
+            for (int h = 0; h < NL / 2; ++h) {
+                const double2 x = a2[h];
+#pragma unroll
+                for (int u = 0; u < SG_EPT; ++u) {
+                    acc[2 * h][u] = fma(x.x, v[u], acc[2 * h][u]);
+                    acc[2 * h + 1][u] = fma(x.y, v[u], acc[2 * h + 1][u]);
+                }
+            }
+        }
+        ++consumed;
+        __syncwarp();  // every lane's reads of this slot are done before it is refilled
+    }
+#pragma unroll
+    for (int u = 0; u < SG_EPT; ++u) {
+        const uint32_t e = e0 + lane + 32u * u;
+        if (e >= n) continue;
+        const uint32_t col = e / G.rows, i = e - col * G.rows;
+        double* dst = S + G.s_base + i + uint64_t(col) * G.ld_s;
+#pragma unroll
+        for (int j = 0; j < NL; ++j)
+            if (uint32_t(j) < G.nlines) dst[uint64_t(j) * G.line_stride] = ((G.mask >> j) & 1u) ? acc[j][u] : 0.0;
+    }
+    return true;
+}
+
+template <int NL>
+__global__ void __launch_bounds__(32 * SGB_WARPS, SgbShape<NL>::MINB)
+    sbuild_groups(const DevSGroup* __restrict__ groups, const DevSItem* __restrict__ items, uint32_t n_items,
+                  const uint64_t* __restrict__ ent_t, const double* __restrict__ ent_a, double* __restrict__ S,
+                  const double* __restrict__ T, int* err, unsigned long long wait_ns) {
+    using namespace async;
+    constexpr int SGB_STAGES = SgbShape<NL>::STAGES;
+    extern __shared__ __align__(16) unsigned char sgb_smem_raw[];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    SgbRing& R = reinterpret_cast<SgbRing*>(sgb_smem)[warp];
+    SgbRing<SGB_STAGES>& R = reinterpret_cast<SgbRing<SGB_STAGES>*>(sgb_smem_raw)[warp];
     wait_for_predecessor();
     if (lane == 0) {
         for (int i = 0; i < SGB_STAGES; ++i) mbar_init(&R.full[i], 1);
@@ -411,80 +509,8 @@ __global__ void __launch_bounds__(32 * SGB_WARPS, SGB_MINB) sbuild_groups(const 
     bool failed = false;
     for (uint32_t it = blockIdx.x * SGB_WARPS + warp; it < n_items && !failed; it += gridDim.x * SGB_WARPS) {
         const DevSItem I = items[it];
-        const DevSGroup G = groups[I.group];
-        const uint32_t n = G.rows * G.cols, e0 = I.e0, cnt = min(uint32_t(SG_CHUNK), n - e0);
-        const uint32_t k0 = G.ent_begin, k1 = G.ent_end;
-        double acc[SG_LINES][SG_EPT];
-#pragma unroll
-        for (int j = 0; j < SG_LINES; ++j)
-#pragma unroll
-            for (int u = 0; u < SG_EPT; ++u) acc[j][u] = 0.0;
-        // every lane: the stage of sources kb .. kb + SGB_NC - 1 (those below k1)
-        auto fill = [&](uint32_t kb) {
-            const uint32_t slot = issued % SGB_STAGES, nc = min(uint32_t(SGB_NC), k1 - kb);
-            if (lane < nc) {
-                const uint64_t tb = ent_t[kb + lane];
-                const uint32_t sh = uint32_t((tb + e0) & 1u), sz = ((cnt + sh) * 8u + 15u) & ~15u;
-                R.shift[slot][lane] = sh;
-                mbar_expect_tx_only(&R.full[slot], sz);
-                bulk_load(R.rows[slot][lane], T + tb + e0 - sh, sz, &R.full[slot]);
-            } else if (lane == uint32_t(SGB_NC)) {
-                const uint32_t sz = nc * SG_LINES * uint32_t(sizeof(double));
-                mbar_expect_tx_only(&R.full[slot], sz);
-                bulk_load(R.alpha[slot], ent_a + uint64_t(kb) * SG_LINES, sz, &R.full[slot]);
-            }
-            __syncwarp();  // every expected byte count is in before the phase can complete
-            if (lane == 0) mbar_arrive(&R.full[slot]);
-            ++issued;
-        };
-        const uint32_t nst = (k1 - k0 + SGB_NC - 1) / SGB_NC;
-        for (uint32_t st = 0; st < min(nst, uint32_t(SGB_STAGES - 1)); ++st) fill(k0 + st * SGB_NC);
-        for (uint32_t st = 0; st < nst; ++st) {
-            const uint32_t slot = consumed % SGB_STAGES, kb = k0 + st * SGB_NC;
-            // the stage SGB_STAGES - 1 ahead goes into the slot freed in the previous step
-            const bool refill = st + SGB_STAGES - 1 < nst;
-            const uint32_t kf = k0 + (st + SGB_STAGES - 1) * SGB_NC;
-            if (refill) {
-                fence_proxy_async_smem();
-                fill(kf);
-            }
-            const bool ok = mbar_wait_suspend(&R.full[slot], (consumed / SGB_STAGES) & 1u, err, wait_ns);
-            if (__any_sync(0xffffffffu, !ok)) {
-                failed = true;
-                break;
-            }
-            const uint32_t nc = min(uint32_t(SGB_NC), k1 - kb);
-#pragma unroll 2
-            for (uint32_t c = 0; c < nc; ++c) {
-                const double* row = R.rows[slot][c] + R.shift[slot][c] + lane;
-                double v[SG_EPT];
-#pragma unroll
-                for (int u = 0; u < SG_EPT; ++u) v[u] = row[32 * u];
-                const double2* a2 = reinterpret_cast<const double2*>(R.alpha[slot][c]);
-#pragma unroll
-                for (int h = 0; h < SG_LINES / 2; ++h) {
-                    const double2 x = a2[h];
-#pragma unroll
-                    for (int u = 0; u < SG_EPT; ++u) {
-                        acc[2 * h][u] = fma(x.x, v[u], acc[2 * h][u]);
-                        acc[2 * h + 1][u] = fma(x.y, v[u], acc[2 * h + 1][u]);
-                    }
-                }
-            }
-            ++consumed;
-            __syncwarp();  // every lane's reads of this slot are done before it is refilled
-        }
-        if (failed) break;
-#pragma unroll
-        for (int u = 0; u < SG_EPT; ++u) {
-            const uint32_t e = e0 + lane + 32u * u;
-            if (e >= n) continue;
-            const uint32_t col = e / G.rows, i = e - col * G.rows;
-            double* dst = S + G.s_base + i + uint64_t(col) * G.ld_s;
-#pragma unroll
-            for (int j = 0; j < SG_LINES; ++j)
-                if (uint32_t(j) < G.nlines) dst[uint64_t(j) * G.line_stride] = ((G.mask >> j) & 1u) ? acc[j][u] : 0.0;
-        }
+        failed = !sgb_item<NL, SGB_STAGES>(R, groups[I.group], I.e0, ent_t, ent_a, S, T, err, wait_ns, lane, issued,
+                                           consumed);
     }
     if (failed && lane == 0) {
         // let the copies still in flight land before the warp's shared memory is released (bounded)
@@ -642,10 +668,11 @@ void stack_stage1(FlatPlan const& p, std::vector<uint64_t> const& stage1_bnd, st
 }  // namespace
 
 namespace {
-// S build of one unit as line groups: groups of SG_LINES consecutive MPO row
-// blocks, each with the union of its lines' source cells in address order and
-// the summed alphas per (cell, line).  Returns the multiply-adds per element
-// this issues (entries x SG_LINES); `terms` receives the per-line walk's count.
+// S build of one unit as line groups: groups of `width` (8 or SG_LINES) consecutive
+// MPO row blocks, each with the union of its lines' source cells in address order
+// and the summed alphas per (cell, line) (SG_LINES alpha slots per entry either
+// way).  Returns the multiply-adds per element this issues (entries x the lines the
+// kernel accumulates); `terms` receives the per-line walk's count.
 struct UnitGroups {
     std::vector<DevSGroup> groups;
     std::vector<uint64_t> ent_t;
@@ -654,15 +681,15 @@ struct UnitGroups {
 };
 uint64_t group_unit(FlatPlan const& p, uint32_t c, uint32_t u, std::vector<int64_t> const& line_of,
                     std::vector<uint64_t> const& t_off, std::vector<uint64_t> const& s_off, UnitGroups& out,
-                    uint64_t* terms) {
+                    uint64_t* terms, uint32_t width) {
     const bool left = p.kind == KIND_LEFT;
     const uint32_t ns = p.c_nsrows[c], ls = p.c_ls[c], rs = p.c_rs[c];
     std::unordered_map<uint64_t, uint32_t> slot;
     uint64_t fmas = 0;
     *terms = 0;
-    for (uint32_t g0 = 0; g0 < ns; g0 += SG_LINES) {
+    for (uint32_t g0 = 0; g0 < ns; g0 += width) {
         DevSGroup G{};
-        G.nlines = std::min<uint32_t>(SG_LINES, ns - g0);
+        G.nlines = std::min<uint32_t>(width, ns - g0);
         if (left) {
             G.rows = p.u_ms[u];
             G.cols = rs;
@@ -727,7 +754,8 @@ uint64_t group_unit(FlatPlan const& p, uint32_t c, uint32_t u, std::vector<int64
                 out.term_slot[q] = (G.ent_begin + pos[le]) * SG_LINES + j;
             }
         }
-        fmas += uint64_t(G.ent_end - G.ent_begin) * SG_LINES;
+        // the kernel accumulates 8 lines for groups of up to 8, SG_LINES otherwise
+        fmas += uint64_t(G.ent_end - G.ent_begin) * (G.nlines <= 8 ? 8u : uint32_t(SG_LINES));
         // the kernel walks sources SG_UNROLL at a time: pad with zero-alpha sources at T
         // offset 0 (their reads stay inside T: an element index is below the cell size)
         while ((out.ent_t.size() - G.ent_begin) % SG_UNROLL) {
@@ -867,18 +895,25 @@ void compile_program(FlatPlan const& p, std::vector<uint64_t> const& stage3_bnd,
             if (mode != 1 && w && (mode == 2 || dense_enough)) {
                 // line groups when they issue at most twice the per-line walk's multiply-adds
                 // (a unit without terms is zero-filled by the line walk)
+                // wide groups read each shared source once for more lines; narrow ones waste
+                // fewer multiply-adds on lines that do not read a source
                 const size_t g0 = ug.groups.size(), e0 = ug.ent_t.size(), m0 = ug.term_k.size();
-                uint64_t nterms = 0;
-                const uint64_t fmas = group_unit(p, c, u, line_of, t_off, s_off, ug, &nterms);
-                if (mode == 2 || (nterms && fmas <= 2 * nterms)) {
-                    ug_units.emplace_back(uint32_t(g0), uint32_t(ug.groups.size()));
-                    continue;
+                bool grouped = false;
+                for (uint32_t width : {uint32_t(SG_LINES), 8u}) {
+                    uint64_t nterms = 0;
+                    const uint64_t fmas = group_unit(p, c, u, line_of, t_off, s_off, ug, &nterms, width);
+                    if (mode == 2 || (nterms && fmas <= 2 * nterms)) {
+                        ug_units.emplace_back(uint32_t(g0), uint32_t(ug.groups.size()));
+                        grouped = true;
+                        break;
+                    }
+                    ug.groups.resize(g0);
+                    ug.ent_t.resize(e0);
+                    ug.ent_a.resize(e0 * SG_LINES);
+                    ug.term_k.resize(m0);
+                    ug.term_slot.resize(m0);
                 }
-                ug.groups.resize(g0);
-                ug.ent_t.resize(e0);
-                ug.ent_a.resize(e0 * SG_LINES);
-                ug.term_k.resize(m0);
-                ug.term_slot.resize(m0);
+                if (grouped) continue;
             }
             for (uint32_t b1 = 0; b1 < p.c_nsrows[c]; ++b1) {
                 DevSLine L;
@@ -935,12 +970,18 @@ void compile_program(FlatPlan const& p, std::vector<uint64_t> const& stage3_bnd,
         std::vector<uint32_t> order(ug_units.size());
         std::iota(order.begin(), order.end(), 0u);
         std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return work[a] > work[b]; });
-        for (uint32_t x : order) {
-            const uint32_t g0 = ug_units[x].first, g1 = ug_units[x].second;
-            if (g0 == g1) continue;
-            const uint64_t n = uint64_t(prog.groups[g0].rows) * prog.groups[g0].cols;
-            for (uint32_t gi = g0; gi < g1; ++gi)
-                for (uint64_t e0 = 0; e0 < n; e0 += SG_CHUNK) prog.gitems.push_back(DevSItem{gi, uint32_t(e0)});
+        // groups of up to 8 lines first (their own launch), then the wide ones
+        for (int wide = 0; wide < 2; ++wide) {
+            for (uint32_t x : order) {
+                const uint32_t g0 = ug_units[x].first, g1 = ug_units[x].second;
+                if (g0 == g1) continue;
+                const uint64_t n = uint64_t(prog.groups[g0].rows) * prog.groups[g0].cols;
+                for (uint32_t gi = g0; gi < g1; ++gi) {
+                    if ((prog.groups[gi].nlines > 8) != (wide == 1)) continue;
+                    for (uint64_t e0 = 0; e0 < n; e0 += SG_CHUNK) prog.gitems.push_back(DevSItem{gi, uint32_t(e0)});
+                }
+            }
+            if (!wide) prog.n_gitems8 = uint32_t(prog.gitems.size());
         }
     }
 
@@ -1385,16 +1426,24 @@ cudaError_t run_sbuild(DeviceProgram const& prog, double* T, double* S, cudaStre
                                    static_cast<const double*>(T));
         if (e != cudaSuccess) return e;
     }
-    if (prog.n_gitems) {
-        cudaError_t ea = ensure_smem_limit(reinterpret_cast<const void*>(sbuild_groups), int(SGB_SMEM));
+    // the items of groups of up to 8 lines come first (prog.n_gitems8 of them)
+    auto groups_launch = [&](auto kernel, size_t smem, int minb, const DevSItem* items, uint32_t n) -> cudaError_t {
+        if (!n) return cudaSuccess;
+        cudaError_t ea = ensure_smem_limit(reinterpret_cast<const void*>(kernel), int(smem));
         if (ea != cudaSuccess) return ea;
-        // SGB_WARPS warps per CTA, SGB_MINB CTAs per SM resident
-        uint32_t grid = std::min<uint32_t>((prog.n_gitems + SGB_WARPS - 1) / SGB_WARPS, sms * SGB_MINB);
-        cudaError_t e = launch_pdl(sbuild_groups, grid, 32 * SGB_WARPS, SGB_SMEM, stream,
-                                   static_cast<const DevSGroup*>(prog.d_groups), static_cast<const DevSItem*>(prog.d_gitems),
-                                   prog.n_gitems, static_cast<const uint64_t*>(prog.d_gent_t),
-                                   static_cast<const double*>(prog.d_gent_a), S, static_cast<const double*>(T),
-                                   prog.d_err, wait_limit_ns());
+        // SGB_WARPS warps per CTA, minb CTAs per SM resident
+        const uint32_t grid = std::min<uint32_t>((n + SGB_WARPS - 1) / SGB_WARPS, sms * uint32_t(minb));
+        return launch_pdl(kernel, grid, 32 * SGB_WARPS, smem, stream, static_cast<const DevSGroup*>(prog.d_groups),
+                          items, n, static_cast<const uint64_t*>(prog.d_gent_t),
+                          static_cast<const double*>(prog.d_gent_a), S, static_cast<const double*>(T), prog.d_err,
+                          wait_limit_ns());
+    };
+    if (prog.n_gitems) {
+        const DevSItem* items = static_cast<const DevSItem*>(prog.d_gitems);
+        cudaError_t e = groups_launch(sbuild_groups<8>, sgb_smem<8>(), SgbShape<8>::MINB, items, prog.n_gitems8);
+        if (e != cudaSuccess) return e;
+        e = groups_launch(sbuild_groups<SG_LINES>, sgb_smem<SG_LINES>(), SgbShape<SG_LINES>::MINB,
+                          items + prog.n_gitems8, prog.n_gitems - prog.n_gitems8);
         if (e != cudaSuccess) return e;
     }
     return cudaGetLastError();
@@ -1413,6 +1462,20 @@ int device_sm_count() {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
     return n > 0 ? n : 148;
+}
+
+cudaError_t run_stages12(DeviceProgram const& prog, uint64_t in, uint64_t out, double* T, double* S,
+                         cudaStream_t stream) {
+    Bases bs{};
+    bs.b[BUF_IN] = in;
+    bs.b[BUF_OUT] = out;
+    bs.b[BUF_T] = reinterpret_cast<uint64_t>(T);
+    bs.b[BUF_S] = reinterpret_cast<uint64_t>(S);
+    bs.b[BUF_ABS] = 0;
+    launch_variant(prog.var1, prog.d_p1, prog.d_s1, prog.d_t1, prog.n_t1, prog.x1, prog.d_r1, bs, stream);
+    cudaError_t e = run_sbuild(prog, T, S, stream);
+    if (e != cudaSuccess) return e;
+    return cudaGetLastError();
 }
 
 cudaError_t run_program(DeviceProgram const& prog, uint64_t in, uint64_t out, double* T, double* S,

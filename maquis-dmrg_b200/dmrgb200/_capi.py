@@ -147,6 +147,7 @@ _sigs = {
     "dmrgb200_hpsi_noalloc": ([C.POINTER(PlanDesc), C.POINTER(BoundaryView), C.POINTER(BoundaryView), vp, vp, vp],
                               C.c_int),
     "dmrgb200_step_execute": ([vp, vp, vp, C.POINTER(BoundaryView), vp], C.c_int),
+    "dmrgb200_step_alpha_dm": ([vp, vp, vp, C.POINTER(BoundaryView), C.c_double, vp], C.c_int),
     "dmrgb200_mpo_create": ([C.POINTER(MpoDesc), C.POINTER(vp)], C.c_int),
     "dmrgb200_mpo_destroy": ([vp], C.c_int),
     "dmrgb200_bindex_create_edge": ([C.c_int, C.POINTER(IndexDesc), C.c_uint32, C.POINTER(vp)], C.c_int),

@@ -176,6 +176,90 @@ def split(psi: S.SiteTensor, phys1, phys2, offs, m: int, cutoff: float, left_to_
     return SplitResult(A, B, tw, bond)
 
 
+def theta_site(psi: S.SiteTensor, phys1, phys2, offs, left_to_right: bool):
+    """The two-site tensor viewed as one site tensor, as the state prediction of the
+    reference does (prediction.hpp:152-171 / 193-212): left-to-right, the tensor at
+    site 1 whose right bond is the middle index (one block per middle charge, the
+    columns of Theta); right-to-left, the tensor at site 2 whose left bond is the
+    middle index (the rows of Theta).  Its left-paired (right-paired) block of a
+    middle charge is Theta of that charge.  Returns (tensor, middle blocks)."""
+    mids = _mid_blocks(psi, phys1, phys2, offs)
+    order = sorted(mids)
+    if left_to_right:
+        t = S.SiteTensor(phys1, psi.left, [(mc, mids[mc][3]) for mc in order])
+    else:
+        t = S.SiteTensor(phys2, [(mc, mids[mc][2]) for mc in order], psi.right)
+    lpos = {c: i for i, (c, _) in enumerate(psi.left)}
+    for b, mc in enumerate(order):
+        rows, cols, nr, nc, fills = mids[mc]
+        Th = np.zeros((nr, nc))
+        for (ro, co, ml, mr, lb, c0) in fills:
+            Th[ro:ro + ml, co:co + mr] = S.block_view(psi.data, psi.rp, lb)[:, c0:c0 + mr]
+        if left_to_right:
+            ro = 0
+            for (s1, i1, lc, ml) in rows:
+                key = (lpos[lc], s1, i1)
+                if key in t.rp.sub:
+                    _, c0, _, mr, rb = t.rp.sub[key]
+                    S.block_view(t.data, t.rp, lpos[lc])[:, c0:c0 + mr] = Th[ro:ro + ml, :]
+                ro += ml
+        else:
+            co = 0
+            for (s2, i2, rc, mr) in cols:
+                _, c0, _, _, _ = t.rp.sub[(b, s2, i2)]
+                S.block_view(t.data, t.rp, b)[:, c0:c0 + mr] = Th[:, co:co + mr]
+                co += mr
+    return t, mids
+
+
+def predict_split(psi: S.SiteTensor, phys1, phys2, offs, m: int, cutoff: float, left_to_right: bool, dm_blocks):
+    """Two-site split with the reference's state prediction (predict_split_l2r / r2l,
+    prediction.hpp:152-240): the density matrix of every middle charge is
+    Theta Theta^T (left-to-right; Theta^T Theta right-to-left) plus alpha times the
+    perturbation terms, as dm_blocks (the backend's alpha_dm on theta_site) returns
+    them in middle-charge order; it is diagonalised on the host (eigh), truncated like
+    heev_truncate (block_matrix_algorithms.h:298-346: the square roots of the
+    eigenvalues as singular values, svd truncation rules), and left-to-right keeps the
+    eigenvectors U as site 1 and U^T Theta as site 2, right-to-left U^T as site 2 and
+    Theta U as site 1."""
+    mids = _mid_blocks(psi, phys1, phys2, offs)
+    order = sorted(mids)
+    eig = {}
+    for b, mc in enumerate(order):
+        w, U = np.linalg.eigh(0.5 * (dm_blocks[b] + dm_blocks[b].T))
+        w, U = w[::-1], U[:, ::-1]
+        eig[mc] = (np.sqrt(np.maximum(w, 0.0)), U)
+    kept, bond, tw = _truncate({mc: v[0] for mc, v in eig.items()}, m, cutoff)
+    left, right = psi.left, psi.right
+    lpos = {c: i for i, (c, _) in enumerate(left)}
+    A = S.SiteTensor(phys1, left, bond)
+    B = S.SiteTensor(phys2, bond, right)
+    bpos = {c: i for i, (c, _) in enumerate(bond)}
+    for mc, k in kept.items():
+        rows, cols, nr, nc, fills = mids[mc]
+        Th = np.zeros((nr, nc))
+        for (ro, co, ml, mr, lb, c0) in fills:
+            Th[ro:ro + ml, co:co + mr] = S.block_view(psi.data, psi.rp, lb)[:, c0:c0 + mr]
+        Uk = eig[mc][1][:, :k]
+        if left_to_right:
+            Ak, Bk = Uk, Uk.T @ Th
+        else:
+            Ak, Bk = Th @ Uk, Uk.T
+        ro = 0
+        for (s1, i1, lc, ml) in rows:
+            key = (lpos[lc], s1, i1)
+            if key in A.rp.sub:
+                _, c0, _, mr, rb = A.rp.sub[key]
+                S.block_view(A.data, A.rp, lpos[lc])[:, c0:c0 + mr] = Ak[ro:ro + ml, :]
+            ro += ml
+        co = 0
+        for (s2, i2, rc, mr) in cols:
+            _, c0, _, _, _ = B.rp.sub[(bpos[mc], s2, i2)]
+            S.block_view(B.data, B.rp, bpos[mc])[:, c0:c0 + mr] = Bk[:, co:co + mr]
+            co += mr
+    return SplitResult(A, B, tw, bond)
+
+
 class DeviceSplitPlan:
     """Host-side part of the device split: the layout of Theta, U, s and V^T in
     device workspaces and the gather copies from psi (no device work here)."""
@@ -455,6 +539,29 @@ class DeviceBackend:
     def right_step(self, model, W, Ridx, Rbuf, t: S.SiteTensor, dev_rp=None):
         return self._step(False, model, W, Ridx, Rbuf, t, dev_rp)
 
+    def alpha_dm(self, phys, W, idx, buf, t: S.SiteTensor, alpha: float, left: bool):
+        """Density-matrix blocks (host, per bra block of the step) of the split with the
+        perturbation, for t = theta_site(...): dmrgb200_step_alpha_dm on a step plan
+        without boundary skipping (alpha_dm_direct builds its schedule with skip off,
+        move_boundary.hpp:72-75 / 126-129)."""
+        dev = self.ctx.device
+        if left:
+            sched, _ = E.schedule_left_step(phys, t.left, t.right, W, idx, False)
+            plan = E.DevicePlan(self.ctx, sched.plan, left_addr=idx.cohort_addresses(buf.data_ptr()))
+            ket, bra = E.to_device(t.data, dev), E.to_device(t.left_paired(), dev)
+            dims = [int(r) for r in sched.plan["out_rows"]]
+        else:
+            sched, _ = E.schedule_right_step(phys, t.left, t.right, W, idx, False)
+            plan = E.DevicePlan(self.ctx, sched.plan, other_addr=idx.cohort_addresses(buf.data_ptr()))
+            ket = bra = E.to_device(t.data, dev)
+            dims = [int(c) for c in sched.plan["out_cols"]]
+        offs = np.concatenate([[0], np.cumsum([d * d for d in dims])]).astype(np.int64)
+        store = self.torch.zeros(max(int(offs[-1]), 1), dtype=self.torch.float64, device=buf.device)
+        addr = np.array([store.data_ptr() + 8 * int(o) for o in offs[:-1]], dtype=np.uint64)
+        plan.alpha_dm(ket.data_ptr(), bra.data_ptr(), addr, alpha)
+        flat = store.cpu().numpy()
+        return [flat[offs[b]:offs[b + 1]].reshape(d, d, order="F") for b, d in enumerate(dims)]
+
     def solve(self, p12, psi: S.SiteTensor, W12, Lidx, Lbuf, Ridx, Rbuf, tol, max_iter, keep_on_device=False):
         """Lowest eigenpair of the site problem; the eigenvector comes back as a
         host array, or as the device tensor with keep_on_device."""
@@ -504,11 +611,18 @@ class DeviceBackend:
 
 class TwoSiteDMRG:
     def __init__(self, backend, model: M.Model, tensors, m: int, cutoff: float = 1e-16, jd_tol: float = 1e-8,
-                 jd_maxiter: int = 8, device_split: bool = False):
+                 jd_maxiter: int = 8, device_split: bool = False, alpha=0.0):
         """device_split: split the optimised two-site tensor on the device
-        (split_device; needs a DeviceBackend) instead of by host SVDs."""
+        (split_device; needs a DeviceBackend) instead of by host SVDs.
+        alpha: the perturbation strength of the state prediction, a number or a function
+        of the sweep index (the reference's alpha_initial / alpha_main / alpha_final by
+        sweep, ts_optimize.hpp:274-282); nonzero alpha splits by predict_split."""
         self.be, self.model, self.m, self.cutoff = backend, model, m, cutoff
         self.device_split = device_split
+        self.alpha = alpha
+        self._sweep = 0
+        if device_split and (callable(alpha) or alpha != 0.0):
+            raise ValueError("the perturbed split runs on the host (dm blocks from the device)")
         self.jd_tol, self.jd_maxiter = jd_tol, jd_maxiter
         self.L = len(tensors)
         self.A = right_canonicalize(tensors)
@@ -562,7 +676,20 @@ class TwoSiteDMRG:
             if self.su2:
                 from . import su2u1
                 psi = su2u1.unreduce_twosite(psi, self.model.phys, self.model.phys, self.offs)
-            res = split(psi, self.model.phys, self.model.phys, self.offs, self.m, self.cutoff, left_to_right)
+            alpha = self.alpha(self._sweep) if callable(self.alpha) else self.alpha
+            if alpha != 0.0:
+                ph_t = time.perf_counter()
+                t, _ = theta_site(psi, self.model.phys, self.model.phys, self.offs, left_to_right)
+                if left_to_right:
+                    dm = self.be.alpha_dm(self.model.phys, self.W[i], self.Lidx[i], self.Lbuf[i], t, alpha, True)
+                else:
+                    dm = self.be.alpha_dm(self.model.phys, self.W[i + 1], self.Ridx[i + 2], self.Rbuf[i + 2], t,
+                                          alpha, False)
+                ph["alpha_dm"] = ph.get("alpha_dm", 0.0) + time.perf_counter() - ph_t
+                res = predict_split(psi, self.model.phys, self.model.phys, self.offs, self.m, self.cutoff,
+                                    left_to_right, dm)
+            else:
+                res = split(psi, self.model.phys, self.model.phys, self.offs, self.m, self.cutoff, left_to_right)
         self.A[i], self.A[i + 1] = res.A, res.B
         t3 = time.perf_counter()
         if left_to_right:
@@ -578,6 +705,7 @@ class TwoSiteDMRG:
 
     def sweep(self, sweep_index: int):
         t0 = time.perf_counter()
+        self._sweep = sweep_index
         for i in range(0, self.L - 1):
             e, it, tw = self.optimize_pair(i, True)
             self.log.energies.append((sweep_index, i, e, it, tw))

@@ -256,6 +256,14 @@ class DevicePlan:
                    "dmrgb200_step_execute")
         del arr
 
+    def alpha_dm(self, ket_ptr: int, bra_ptr: int, dm_addr: np.ndarray, alpha: float, stream: int = 0) -> None:
+        """Density matrix of the split with the perturbation into the blocks at dm_addr
+        (dmrgb200_step_alpha_dm; a step plan of the two-site tensor as one site)."""
+        v, arr = _view(dm_addr)
+        capi.check(capi.lib.dmrgb200_step_alpha_dm(self.handle, ket_ptr, bra_ptr, C.byref(v), float(alpha),
+                                                   stream or None), "dmrgb200_step_alpha_dm")
+        del arr
+
     def __del__(self):
         if getattr(self, "handle", None):
             capi.lib.dmrgb200_plan_destroy(self.handle)

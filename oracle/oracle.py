@@ -47,6 +47,7 @@ def lib():
         _lib.oracle_left_step.argtypes = [PD, pp, C.c_void_p, C.c_void_p, pp]
         _lib.oracle_right_step.argtypes = [PD, pp, C.c_void_p, C.c_void_p, pp]
         _lib.oracle_hpsi_adjoint.argtypes = [PD, pp, pp, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.oracle_alpha_dm.argtypes = [PD, pp, C.c_void_p, C.c_void_p, C.c_double, C.c_int, pp]
         _lib.oracle_set_threads.argtypes = [C.c_int]
         _lib.oracle_set_threads(int(os.environ.get("ORACLE_THREADS", os.cpu_count() or 1)))
     return _lib
@@ -113,3 +114,29 @@ def right_step(plan: dict, R: np.ndarray, Ridx: engine.BIndex, ket_rp: np.ndarra
     assert rc == 0
     del keep
     return out
+
+
+def dm_storage(plan: dict):
+    """Zeroed square column-major blocks of a step plan's density matrix, one per bra
+    block (left step: out_rows; right step: out_cols), as views of one flat array,
+    with the block pointer array for the C calls."""
+    left = int(plan["kind"]) == capi.PLAN_LEFT
+    dims = [int(r) if left else int(c) for r, c in zip(plan["out_rows"], plan["out_cols"])]
+    offs = np.concatenate([[0], np.cumsum([d * d for d in dims])]).astype(np.int64)
+    flat = np.zeros(max(int(offs[-1]), 1))
+    blocks = [flat[offs[b]:offs[b + 1]].reshape(d, d, order="F") for b, d in enumerate(dims)]
+    ptrs = (C.c_void_p * max(len(dims), 1))(*[flat.ctypes.data + 8 * int(offs[b]) for b in range(len(dims))])
+    return blocks, flat, ptrs
+
+
+def alpha_dm(plan: dict, B: np.ndarray, Bidx: engine.BIndex, ket: np.ndarray, bra: np.ndarray, alpha: float,
+             with_theta: bool = True):
+    """Density matrix of the split with the perturbation, per bra block (plan_exec.cpp
+    oracle_alpha_dm): a list of square column-major blocks."""
+    desc, keep = capi.numpy_to_desc(plan)
+    blocks, flat, ptrs = dm_storage(plan)
+    rc = lib().oracle_alpha_dm(C.byref(desc), _ptrs(B, Bidx), np.ascontiguousarray(ket).ctypes.data,
+                               np.ascontiguousarray(bra).ctypes.data, float(alpha), int(with_theta), ptrs)
+    assert rc == 0
+    del keep
+    return blocks

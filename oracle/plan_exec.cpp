@@ -16,6 +16,8 @@
 //   right step  move_boundary.hpp:385-401
 //     create_T, create_s_r                   (as above)
 //     prop_r                                 solver/tasks.cpp:243-260
+//   alpha_dm    prediction.hpp:41-69, move_boundary.hpp:38-143
+//     lbtm, rbtm                             solver/tasks.cpp:346-380
 // Output accumulation of H psi is serialised per output block with a mutex,
 // as in the reference (tasks.cpp:310-312).
 #include <cstdint>
@@ -220,6 +222,60 @@ int oracle_right_step(const dmrgb200_plan_desc* dp, const double* const* R, cons
                 for (int col = 0; col < rs; ++col)
                     std::memcpy(o + (size_t(b) * rs + col) * ls, &buf[size_t(ls) * b + size_t(col) * M],
                                 ls * sizeof(double));
+        }
+    }
+    return 0;
+}
+
+// Density matrix of a two-site split with the perturbation (state prediction) of the
+// reference, on a step plan whose ket and bra are the same tensor Theta (the two-site
+// tensor viewed as one site; prediction.hpp:41-69 alpha_dm / alpha_dm_right):
+//   left step:  dm_b = Theta_b Theta_b^T + alpha sum_{c: c_lb = b} S_c S_c^T
+//               (Theta_b the left-paired bra block b, S_c = create_s; Cohort::lbtm,
+//                tasks.cpp:346-362, driven by alpha_dm_direct, move_boundary.hpp:38-91)
+//   right step: dm_b = Theta_b^T Theta_b + alpha sum_{c: c_rb = b} S_c^T S_c
+//               (Theta_b the right-paired bra block b, S_c = create_s_r; Cohort::rbtm,
+//                tasks.cpp:364-380, driven by alpha_dm_direct_right, :93-143)
+// dm[b] is stripe_b x stripe_b; with_theta = 0 leaves the Theta term out (the
+// reference's alpha_dm_direct alone, accumulated into dm, which is not cleared then).
+int oracle_alpha_dm(const dmrgb200_plan_desc* dp, const double* const* B, const double* ket, const double* bra,
+                    double alpha, int with_theta, double* const* dm) {
+    dmrgb200_plan_desc const& d = *dp;
+    const bool left = d.kind == DMRGB200_PLAN_LEFT_STEP;
+    if (!left && d.kind != DMRGB200_PLAN_RIGHT_STEP) return 1;
+    if (with_theta)
+        for (uint32_t b = 0; b < d.n_out_blocks; ++b) {
+            const int r = int(d.out_rows[b]), c = int(d.out_cols[b]);
+            const double* th = bra + d.out_off[b];
+            if (left)
+                gemm('N', 'T', r, r, c, 1.0, th, r, th, r, 0.0, dm[b], r);
+            else
+                gemm('T', 'N', c, c, r, 1.0, th, r, th, r, 0.0, dm[b], c);
+        }
+    std::vector<std::mutex> mutexes(d.n_out_blocks);
+    int ng = int(d.n_groups);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int gi = 0; gi < ng; ++gi) {
+        std::vector<std::vector<double>> T;
+        for (uint32_t t = d.g_t[gi]; t < d.g_t[gi + 1]; ++t)
+            T.push_back(left ? create_T_left(d, t, B, ket) : create_T(d, t, B, ket));
+        for (uint32_t c = d.g_c[gi]; c < d.g_c[gi + 1]; ++c) {
+            const int M = int(d.c_stripe[c]);
+            std::vector<double> tmp(size_t(M) * M, 0.0);
+            uint32_t b;
+            if (left) {
+                std::vector<double> S = create_s(d, c, T, d.g_t[gi]);
+                const int K = int(S.size() / size_t(M));
+                gemm('N', 'T', M, M, K, alpha, S.data(), M, S.data(), M, 1.0, tmp.data(), M);
+                b = d.c_lb[c];
+            } else {
+                std::vector<double> S = create_s_r(d, c, T, d.g_t[gi]);
+                const int K = int(d.c_nsrows[c] * d.c_ls[c]);
+                gemm('T', 'N', M, M, K, alpha, S.data(), K, S.data(), K, 1.0, tmp.data(), M);
+                b = d.c_rb[c];
+            }
+            std::lock_guard<std::mutex> lk(mutexes[b]);
+            axpy(size_t(M) * M, 1.0, tmp.data(), dm[b]);
         }
     }
     return 0;

@@ -33,6 +33,7 @@ def lib():
         _lib.ref_hpsi_create.restype = C.c_void_p
         _lib.ref_hpsi_run.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         _lib.ref_hpsi_destroy.argtypes = [C.c_void_p]
+        _lib.ref_alpha_dm.argtypes = [PD, C.c_uint32, u32, u32, u32, pp, C.c_void_p, C.c_double, pp]
         _lib.ref_hpsi_flatten.argtypes = [C.c_void_p]
         _lib.ref_hpsi_flatten.restype = C.POINTER(capi.PlanDesc)
     return _lib
@@ -114,3 +115,19 @@ def right_step(plan, R, Ridx, ket_rp, bra_rp, new_idx):
                               _ptrs(out, new_idx))
     assert rc == 0
     return out
+
+
+def alpha_dm(plan, B, Bidx, ket, alpha):
+    """The reference's perturbation terms alpha sum S S^T (left step) or alpha sum S^T S
+    (right step) per bra block, from its own Cohort::lbtm / rbtm; a list of square
+    column-major blocks (see oracle.alpha_dm)."""
+    import oracle as O
+    desc, keep = capi.numpy_to_desc(plan)
+    blocks, flat, ptrs = O.dm_storage(plan)
+    ls, rs, nb = _u32(Bidx.lsize), _u32(Bidx.rsize), _u32(Bidx.nblocks)
+    u = lambda a: a.ctypes.data_as(C.POINTER(C.c_uint32))
+    rc = lib().ref_alpha_dm(C.byref(desc), Bidx.n_cohorts, u(ls), u(rs), u(nb), _ptrs(B, Bidx),
+                            np.ascontiguousarray(ket).ctypes.data, float(alpha), ptrs)
+    assert rc == 0
+    del keep
+    return blocks

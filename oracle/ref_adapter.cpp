@@ -240,4 +240,45 @@ int ref_right_step(const dmrgb200_plan_desc* dp, uint32_t nR, const uint32_t* R_
     return 0;
 }
 
+// The reference's perturbation terms on a step plan (bra = ket = the tensor viewed
+// as one site): Cohort::lbtm / rbtm (tasks.cpp:346-380) of every cohort added into
+// dm[lb] (left) or dm[rb] (right), as alpha_dm_direct / alpha_dm_direct_right do
+// (move_boundary.hpp:38-143).  dm is not cleared.
+int ref_alpha_dm(const dmrgb200_plan_desc* dp, uint32_t nB, const uint32_t* B_lsz, const uint32_t* B_rsz,
+                 const uint32_t* B_nb, const double* const* B, const double* ket, double alpha, double* const* dm) {
+    dmrgb200_plan_desc const& d = *dp;
+    const bool left = d.kind == DMRGB200_PLAN_LEFT_STEP;
+    if (!left && d.kind != DMRGB200_PLAN_RIGHT_STEP) return 1;
+    BoundaryIndexRT rt = make_rt(nB, B_lsz, B_rsz, B_nb);
+    std::vector<std::size_t> mpsbs(d.n_in_blocks, 0), sizes;
+    if (left) {
+        sizes.assign(d.n_groups, 0);
+        for (uint32_t g = 0; g < d.n_groups; ++g) {
+            if (d.g_t[g] < d.g_t[g + 1]) sizes[g] = d.t_width[d.g_t[g]];
+            else if (d.g_c[g] < d.g_c[g + 1]) sizes[g] = d.c_rs[d.g_c[g]];
+        }
+    } else {
+        sizes.assign(d.in_rows, d.in_rows + d.n_in_blocks);
+    }
+    ScheduleNew<double> tasks(mpsbs, sizes, rt, rt);
+    for (uint32_t g = 0; g < d.n_groups; ++g) fill_group(d, g, nB, tasks[g], left, true, false);
+    std::vector<const double*> bv(B, B + nB);
+    auto kv = block_views(ket, d.in_off, d.n_in_blocks);
+    std::vector<std::mutex> mutexes(d.n_out_blocks);
+    int ng = int(d.n_groups);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int g = 0; g < ng; ++g) {
+        auto T = left ? tasks[g].create_T_left(bv, kv) : tasks[g].create_T(bv, kv);
+        for (auto it = tasks[g].begin(); it != tasks[g].end(); ++it) {
+            const unsigned b = left ? it->get_lb() : it->get_rb();
+            std::lock_guard<std::mutex> lk(mutexes[b]);
+            if (left)
+                it->lbtm(T, dm[b], alpha);
+            else
+                it->rbtm(T, dm[b], alpha);
+        }
+    }
+    return 0;
+}
+
 }  // extern "C"

@@ -23,6 +23,13 @@ class OracleBackend:
         sch, nidx = E.schedule_right_step(model.phys, t.left, t.right, W, Ridx, True)
         return nidx, O.right_step(sch.plan, Rval, Ridx, t.data, t.data, nidx)
 
+    def alpha_dm(self, phys, W, idx, val, t, alpha, left):
+        if left:
+            sch, _ = E.schedule_left_step(phys, t.left, t.right, W, idx, False)
+            return O.alpha_dm(sch.plan, val, idx, t.data, t.left_paired(), alpha)
+        sch, _ = E.schedule_right_step(phys, t.left, t.right, W, idx, False)
+        return O.alpha_dm(sch.plan, val, idx, t.data, t.data, alpha)
+
     def solve(self, p12, psi, W12, Lidx, Lval, Ridx, Rval, tol, max_iter):
         sch = E.schedule_hpsi(p12, psi.left, psi.right, W12, Lidx, Ridx)
         theta, u, it, conv, rn = JD.jcd(lambda v: O.hpsi(sch.plan, Lval, Lidx, Rval, Ridx, v), psi.data, tol=tol,

@@ -36,18 +36,24 @@ dmrgb200_status noalloc_fail(dmrgb200_status s, std::string const& msg);
 
 namespace {
 
-constexpr int OZ_BM = 128, OZ_BN = 64, OZ_BK = 32;        // tile rows, tile columns, K bytes per slab
-constexpr int A_TILE = OZ_BM * OZ_BK, B_TILE = OZ_BN * OZ_BK;
+// Output tiles are 128 rows by BN = 64 or 128 columns (chosen per program, oz_build).
+// TMEM holds 512 int32 columns: 512 / BN accumulators at a time, so with BN = 128 the
+// digit groups g = 0 .. s-1 of a tile run as passes of up to 4 groups over its K slabs
+// (BN = 64: one pass for s <= 8).
+constexpr int OZ_BM = 128, OZ_BK = 32;  // tile rows, K bytes per slab
+constexpr int A_TILE = OZ_BM * OZ_BK;
 constexpr int OZ_MAX_SLICES = 8, OZ_MAX_STAGES = 8;
+__host__ __device__ constexpr int oz_pass_groups(int bn) { return 512 / bn; }
+__host__ __device__ constexpr int oz_passes(int s, int bn) { return (s + oz_pass_groups(bn) - 1) / oz_pass_groups(bn); }
 // warps 0-3 drain the accumulators (TMEM lane quarter = warp), warp 4 loads the slabs,
 // warp 5 issues the MMAs
 constexpr int OZ_EPI_WARPS = 4, OZ_LOAD_WARP = 4, OZ_MMA_WARP = 5, OZ_THREADS = 32 * 6;
 constexpr uint32_t OZ_SMEM_CAP = 227u * 1024u;  // dynamic shared memory of one CTA
 constexpr uint32_t OZ_BAR_BYTES = 256;          // barriers and slots behind the stages
 // pipeline depth for s digit planes: as many stages of s (A + B) tiles as fit
-__host__ __device__ constexpr uint32_t oz_stages(int s) {
-    return (OZ_SMEM_CAP - OZ_BAR_BYTES) / (uint32_t(s) * (A_TILE + B_TILE)) < uint32_t(OZ_MAX_STAGES)
-               ? (OZ_SMEM_CAP - OZ_BAR_BYTES) / (uint32_t(s) * (A_TILE + B_TILE))
+__host__ __device__ constexpr uint32_t oz_stages(int s, int bn) {
+    return (OZ_SMEM_CAP - OZ_BAR_BYTES) / (uint32_t(s) * uint32_t(A_TILE + bn * OZ_BK)) < uint32_t(OZ_MAX_STAGES)
+               ? (OZ_SMEM_CAP - OZ_BAR_BYTES) / (uint32_t(s) * uint32_t(A_TILE + bn * OZ_BK))
                : uint32_t(OZ_MAX_STAGES);
 }
 using namespace async;
@@ -90,14 +96,15 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                  : "memory");
 }
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, int32_t (&v)[16]) {
+// 16 consecutive TMEM columns of this warp's 32 lanes; the values are valid after tmem_wait_ld
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, int32_t* v) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
           "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
         : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 // ---- digit extraction --------------------------------------------------------------
 
@@ -117,7 +124,7 @@ struct OzSplit {
     uint32_t is_b;      // 0: A operand, 1: B operand (read transposed)
     uint32_t is_const;  // the operand and its exponents are constant between calls
     uint32_t rowtab;    // A of a row-table problem: row r at rowtab[rowtab + r]; DevProb::NO_ROWS otherwise
-    uint32_t pad;
+    uint32_t tr;        // rows of a digit tile: OZ_BM (A) or the program's BN (B)
 };
 
 __global__ void fill_int(int* __restrict__ p, uint64_t n, int v) {
@@ -279,7 +286,7 @@ __global__ void __launch_bounds__(256) oz_split(const OzSplit* __restrict__ jobs
         const OzSplit job = jobs[jn];
         const uint64_t local = it - first[jn];
         int8_t* out = job.is_b ? B8 : A8;
-        const uint32_t TR = job.is_b ? uint32_t(OZ_BN) : uint32_t(OZ_BM);
+        const uint32_t TR = job.tr;
         const uint32_t tile_bytes = TR * OZ_BK;
         if (oz_kmajor(job)) {
             // item = (16-row group g, slab ks); lane: row g * 16 + (lane & 15), K 16 (lane >> 4) .. + 15
@@ -400,35 +407,48 @@ __device__ __forceinline__ void oz_settle(uint64_t* bar, uint32_t parity, int* e
         }
 }
 
-// Persistent grouped INT8 GEMM over the digit planes, one 128 x 64 output tile at a
-// time, with warp roles:
-//   load warp (lane 0): one bulk copy of the s A-planes and one of the s B-planes of
-//     each K slab into a ring of `stages` stages (full barriers), refilling a stage
-//     once the MMAs that read it have completed (empty barriers, MMA commits);
-//   MMA warp (lane 0): for each slab, the s(s+1)/2 digit products p + q = g < s into
-//     accumulator g (TMEM columns g * 64 ..), one 128x64x32 tcgen05.mma each; after a
-//     chunk of slabs it commits to `tfull`;
-//   epilogue warps 0-3: wait `tfull`, read their 32 TMEM lanes of every accumulator,
-//     sum them scaled by 2^-7(g+2) in FP64 (smallest weight first), release the
-//     accumulators (`tempty`, which the MMA warp waits for before the next chunk) and
-//     add 2^(e_row + e_col) times the sum into C.
-// The load warp runs ahead across tiles and chunks, so copies overlap the epilogue.
+// Persistent grouped INT8 GEMM over the digit planes, one 128 x OZ_BN output tile at a
+// time.  The digit groups g = p + q < s of a tile run as passes of up to 512 / OZ_BN
+// groups (the accumulators of one pass fill at most the 512 TMEM columns), smallest
+// weights first; a pass needs the digit planes 0 .. (its last group).  Warp roles:
+//   load warp (lane 0): per (tile, pass, K slab) one bulk copy of the pass's A planes
+//     and one of its B planes into a ring of `stages` stages (full barriers), refilling
+//     a stage once the MMAs that read it have completed (empty barriers, MMA commits);
+//   MMA warp (lane 0): for each slab, the digit products of the pass's groups into
+//     accumulator g - g0 (TMEM columns (g - g0) * OZ_BN ..), one 128 x OZ_BN x 32
+//     tcgen05.mma each; after a chunk of slabs it commits to `tfull`;
+//   epilogue warps 0-3: wait `tfull`, read their 32 TMEM lanes of the pass's
+//     accumulators 32 columns at a time, sum them scaled by 2^-7(g+2) in FP64
+//     (smallest weight first), add 2^(e_row + e_col) times the sum into C, and release
+//     the accumulators (`tempty`, which the MMA warp waits for before the next chunk).
+// The load warp runs ahead across passes and tiles, so copies overlap the epilogue.
 // Every wait is bounded; on a timeout or a set error word each role stops, the issued
 // MMAs and copies are waited for (fixed limit), TMEM is released and the CTA returns.
+template <int OZ_BN>
 __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_mma(OzArgs a) {
+    constexpr int B_TILE = OZ_BN * OZ_BK, OZ_PASS_GROUPS = oz_pass_groups(OZ_BN);
     extern __shared__ __align__(1024) unsigned char smem[];
     const int s = a.s;
+    const int npass = oz_passes(s, OZ_BN);
     const uint32_t nst = a.stages;
-    const uint32_t a_bytes = uint32_t(s) * A_TILE, stage_bytes = uint32_t(s) * (A_TILE + B_TILE);
+    const uint32_t a_room = uint32_t(s) * A_TILE, stage_bytes = uint32_t(s) * (A_TILE + B_TILE);
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + nst * stage_bytes);
     uint64_t* empty = full + nst;
     uint64_t* tfull = empty + nst;
+    // accumulator releases: one per group of the pass with 64-column tiles (the MMA warp
+    // reuses a group as soon as the epilogue has read it), one for the pass otherwise
+    constexpr int NREL = OZ_BN == 64 ? OZ_PASS_GROUPS : 1;
     uint64_t* tempty = tfull + 1;
-    uint64_t* fin = tempty + 1;
+    uint64_t* fin = tempty + NREL;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(fin + 1);
     uint32_t* consumed_slot = tmem_slot + 1;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t ncols = (s * OZ_BN <= 256) ? ((s * OZ_BN <= 128) ? 128u : 256u) : 512u;
+    const uint32_t ncols = min(s, OZ_PASS_GROUPS) * OZ_BN <= 128 ? 128u : (min(s, OZ_PASS_GROUPS) * OZ_BN <= 256 ? 256u : 512u);
+    // groups [g0, g1) of pass q (passes run q = npass - 1 .. 0) and the planes it reads
+    auto pass_groups = [&](int q, int& g0, int& g1) {
+        g0 = q * OZ_PASS_GROUPS;
+        g1 = min(s, g0 + OZ_PASS_GROUPS);
+    };
 
     if (threadIdx.x == 0) {
         for (uint32_t i = 0; i < nst; ++i) {
@@ -436,7 +456,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_mma(OzArgs a) {
             mbar_init(&empty[i], 1);
         }
         mbar_init(tfull, 1);
-        mbar_init(tempty, OZ_EPI_WARPS);
+        for (int i = 0; i < NREL; ++i) mbar_init(&tempty[i], OZ_EPI_WARPS);
         mbar_init(fin, 1);
         *consumed_slot = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -459,18 +479,24 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_mma(OzArgs a) {
             for (uint32_t tile = blockIdx.x; tile < a.n_tiles && ok; tile += gridDim.x) {
                 const OzTile tl = a.tiles[tile];
                 const OzPB pb = a.pbs[tl.pb];
-                for (uint32_t kt = pb.slab_begin; kt < pb.slab_end; ++kt, ++gs) {
-                    const uint32_t st = gs % nst;
-                    if (gs >= nst && !mbar_wait(&empty[st], ((gs / nst) - 1) & 1u, a.err, a.wait_ns)) {
-                        ok = false;
-                        break;
+                for (int q = npass - 1; q >= 0 && ok; --q) {
+                    int g0, g1;
+                    pass_groups(q, g0, g1);
+                    const uint32_t planes = uint32_t(g1);  // planes 0 .. g1 - 1
+                    for (uint32_t kt = pb.slab_begin; kt < pb.slab_end; ++kt, ++gs) {
+                        const uint32_t st = gs % nst;
+                        if (gs >= nst && !mbar_wait(&empty[st], ((gs / nst) - 1) & 1u, a.err, a.wait_ns)) {
+                            ok = false;
+                            break;
+                        }
+                        const OzSlab sl = a.slabs[kt];
+                        unsigned char* base = smem + st * stage_bytes;
+                        mbar_expect_tx(&full[st], planes * (A_TILE + B_TILE));
+                        bulk_load(base, a.A8 + (sl.a_off + uint64_t(tl.mt) * sl.a_ts) * s, planes * A_TILE,
+                                  &full[st]);
+                        bulk_load(base + a_room, a.B8 + (sl.b_off + uint64_t(tl.nt) * sl.b_ts) * s, planes * B_TILE,
+                                  &full[st]);
                     }
-                    const OzSlab sl = a.slabs[kt];
-                    unsigned char* base = smem + st * stage_bytes;
-                    mbar_expect_tx(&full[st], stage_bytes);
-                    bulk_load(base, a.A8 + (sl.a_off + uint64_t(tl.mt) * sl.a_ts) * s, a_bytes, &full[st]);
-                    bulk_load(base + a_bytes, a.B8 + (sl.b_off + uint64_t(tl.nt) * sl.b_ts) * s,
-                              uint32_t(s) * B_TILE, &full[st]);
                 }
             }
             issued = gs;
@@ -485,32 +511,48 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_mma(OzArgs a) {
                 const OzPB pb = a.pbs[a.tiles[tile].pb];
                 const uint32_t KT = pb.slab_end - pb.slab_begin;
                 const uint32_t nch = KT ? (KT + a.chunk - 1) / a.chunk : 1;
-                for (uint32_t ch = 0; ch < nch && ok; ++ch) {
-                    // the accumulators are free once the epilogue of the previous round has read them
-                    if (rounds > 0 && !mbar_wait_suspend(tempty, (rounds - 1) & 1u, a.err)) {
-                        ok = false;
-                        break;
-                    }
-                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                    const uint32_t k_begin = ch * a.chunk, k_end = min(KT, k_begin + a.chunk);
-                    for (uint32_t kt = k_begin; kt < k_end; ++kt, ++gs) {
-                        const uint32_t st = gs % nst;
-                        if (!mbar_wait(&full[st], (gs / nst) & 1u, a.err, a.wait_ns)) {
+                for (int q = npass - 1; q >= 0 && ok; --q) {
+                    int g0, g1;
+                    pass_groups(q, g0, g1);
+                    for (uint32_t ch = 0; ch < nch && ok; ++ch) {
+                        // the accumulators are free once the epilogue of the previous round has
+                        // read them: the whole pass (128-column tiles) before the chunk, each group
+                        // (64-column tiles) before its first product, largest g first as the
+                        // epilogue releases them
+                        if (NREL == 1 && rounds > 0 && !mbar_wait_suspend(tempty, (rounds - 1) & 1u, a.err)) {
                             ok = false;
                             break;
                         }
                         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                        const uint32_t abase = smem_u32(smem + st * stage_bytes);
-                        const uint32_t bbase = abase + a_bytes;
-                        for (int g = 0; g < s; ++g)
-                            for (int p = 0; p <= g; ++p)
-                                umma_i8(tmem + uint32_t(g * OZ_BN), umma_desc(abase + p * A_TILE),
-                                        umma_desc(bbase + (g - p) * B_TILE), idesc, (kt > k_begin || p > 0) ? 1u : 0u);
-                        umma_commit(&empty[st]);  // the stage is free once these MMAs complete
+                        const uint32_t k_begin = ch * a.chunk, k_end = min(KT, k_begin + a.chunk);
+                        for (uint32_t kt = k_begin; kt < k_end && ok; ++kt, ++gs) {
+                            const uint32_t st = gs % nst;
+                            if (!mbar_wait(&full[st], (gs / nst) & 1u, a.err, a.wait_ns)) {
+                                ok = false;
+                                break;
+                            }
+                            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                            const uint32_t abase = smem_u32(smem + st * stage_bytes);
+                            const uint32_t bbase = abase + a_room;
+                            for (int g = g1 - 1; g >= g0; --g) {
+                                if (NREL > 1 && kt == k_begin && rounds > 0) {
+                                    if (!mbar_wait_suspend(&tempty[g - g0], (rounds - 1) & 1u, a.err)) {
+                                        ok = false;
+                                        break;
+                                    }
+                                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                                }
+                                for (int pl = 0; pl <= g; ++pl)
+                                    umma_i8(tmem + uint32_t((g - g0) * OZ_BN), umma_desc(abase + pl * A_TILE),
+                                            umma_desc(bbase + (g - pl) * B_TILE), idesc,
+                                            (kt > k_begin || pl > 0) ? 1u : 0u);
+                            }
+                            umma_commit(&empty[st]);  // the stage is free once these MMAs complete
+                        }
+                        if (!ok) break;
+                        umma_commit(tfull);  // the chunk's sums are complete once every MMA issued so far is
+                        ++rounds;
                     }
-                    if (!ok) break;
-                    umma_commit(tfull);  // the chunk's sums are complete once every MMA issued so far is
-                    ++rounds;
                 }
             }
             *consumed_slot = gs;
@@ -541,42 +583,92 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_mma(OzArgs a) {
                     crow = reinterpret_cast<double*>(base_of(a.bases, pb.C.buf) + 8ull * pb.C.off) + row;
                 }
             }
-            for (uint32_t ch = 0; ch < nch; ++ch) {
-                if (!mbar_wait_suspend(tfull, rounds & 1u, a.err)) {
-                    ok = false;
-                    break;
-                }
-                ++rounds;
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                double acc[OZ_BN];
-#pragma unroll
-                for (int j = 0; j < OZ_BN; ++j) acc[j] = 0.0;
-                for (int g = s - 1; g >= 0 && KT > 0; --g) {
-                    const double w = pow2_normal(-7 * (g + 2));
-#pragma unroll
-                    for (int c0 = 0; c0 < OZ_BN; c0 += 16) {
-                        int32_t v[16];
-                        tmem_ld16(tmem + (uint32_t(warp * 32) << 16) + uint32_t(g * OZ_BN + c0), v);
-#pragma unroll
-                        for (int j = 0; j < 16; ++j) acc[c0 + j] += i2d_exact(v[j]) * w;
+            bool first = true;  // the tile's first round writes C (adds when the problem has beta)
+            for (int q = npass - 1; q >= 0 && ok; --q) {
+                int g0, g1;
+                pass_groups(q, g0, g1);
+                for (uint32_t ch = 0; ch < nch; ++ch) {
+                    if (!mbar_wait_suspend(tfull, rounds & 1u, a.err)) {
+                        ok = false;
+                        break;
                     }
-                }
-                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-                __syncwarp();
-                if (lane == 0) mbar_arrive(tempty);
-                if (crow) {
-                    const bool add = pb.beta || ch > 0;
+                    ++rounds;
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const bool add = pb.beta || !first;
+                    first = false;
+                    if constexpr (OZ_BN == 64) {
+                        // read the groups largest g first, releasing each as soon as all four
+                        // warps have read it, then scale and store the 64 sums
+                        double acc[OZ_BN];
 #pragma unroll
-                    for (int j = 0; j < OZ_BN; ++j) {
-                        const uint32_t col = tl.nt * OZ_BN + j;
-                        if (col < pb.N) {
-                            // x 2^(e_row + e_col): one multiplication by the exact power where it is
-                            // normal (the value ldexp gives), ldexp otherwise
-                            const int ex = erow + a.e[pb.f_off + col];
-                            const double val = (ex >= -1022 && ex <= 1023) ? acc[j] * pow2_normal(ex) : ldexp(acc[j], ex);
-                            double* dst = crow + uint64_t(col) * ldc;
-                            *dst = add ? *dst + val : val;
+                        for (int j = 0; j < OZ_BN; ++j) acc[j] = 0.0;
+                        for (int g = g1 - 1; g >= g0; --g) {
+                            if (KT > 0) {
+                                const double w = pow2_normal(-7 * (g + 2));
+                                const uint32_t taddr = tmem + (uint32_t(warp * 32) << 16) + uint32_t((g - g0) * OZ_BN);
+#pragma unroll
+                                for (int c0 = 0; c0 < OZ_BN; c0 += 32) {
+                                    int32_t v[32];
+                                    tmem_ld16(taddr + c0, v);
+                                    tmem_ld16(taddr + c0 + 16, v + 16);
+                                    tmem_wait_ld();
+#pragma unroll
+                                    for (int j = 0; j < 32; ++j) acc[c0 + j] += i2d_exact(v[j]) * w;
+                                }
+                            }
+                            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                            __syncwarp();
+                            if (lane == 0) mbar_arrive(&tempty[g - g0]);
                         }
+                        if (crow) {
+#pragma unroll
+                            for (int j = 0; j < OZ_BN; ++j) {
+                                const uint32_t col = tl.nt * OZ_BN + j;
+                                if (col < pb.N) {
+                                    // x 2^(e_row + e_col): one multiplication by the exact power
+                                    // where it is normal (the value ldexp gives), ldexp otherwise
+                                    const int ex = erow + a.e[pb.f_off + col];
+                                    const double val =
+                                        (ex >= -1022 && ex <= 1023) ? acc[j] * pow2_normal(ex) : ldexp(acc[j], ex);
+                                    double* dst = crow + uint64_t(col) * ldc;
+                                    *dst = add ? *dst + val : val;
+                                }
+                            }
+                        }
+                    } else {
+                    for (int c0 = 0; c0 < OZ_BN; c0 += 32) {
+                        double acc[32];
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) acc[j] = 0.0;
+                        for (int g = g1 - 1; g >= g0 && KT > 0; --g) {
+                            const double w = pow2_normal(-7 * (g + 2));
+                            int32_t v[32];
+                            const uint32_t taddr = tmem + (uint32_t(warp * 32) << 16) + uint32_t((g - g0) * OZ_BN + c0);
+                            tmem_ld16(taddr, v);
+                            tmem_ld16(taddr + 16, v + 16);
+                            tmem_wait_ld();
+#pragma unroll
+                            for (int j = 0; j < 32; ++j) acc[j] += i2d_exact(v[j]) * w;
+                        }
+                        if (crow) {
+#pragma unroll
+                            for (int j = 0; j < 32; ++j) {
+                                const uint32_t col = tl.nt * OZ_BN + c0 + j;
+                                if (col < pb.N) {
+                                    // x 2^(e_row + e_col): one multiplication by the exact power
+                                    // where it is normal (the value ldexp gives), ldexp otherwise
+                                    const int ex = erow + a.e[pb.f_off + col];
+                                    const double val =
+                                        (ex >= -1022 && ex <= 1023) ? acc[j] * pow2_normal(ex) : ldexp(acc[j], ex);
+                                    double* dst = crow + uint64_t(col) * ldc;
+                                    *dst = add ? *dst + val : val;
+                                }
+                            }
+                        }
+                    }
+                    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(tempty);
                     }
                 }
             }
@@ -597,7 +689,9 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_mma(OzArgs a) {
 
 }  // namespace
 
-size_t ozaki_smem_bytes(int s) { return size_t(oz_stages(s)) * s * (A_TILE + B_TILE) + OZ_BAR_BYTES; }
+size_t ozaki_smem_bytes(int s, int bn) {
+    return size_t(oz_stages(s, bn)) * s * (A_TILE + bn * OZ_BK) + OZ_BAR_BYTES;
+}
 
 // Operands held in boundary memory (BUF_ABS) do not change between calls of a
 // plan: their digit planes and exponents are computed on the first run and kept
@@ -610,6 +704,7 @@ struct OzProgram {
     std::vector<OzSlab> slabs;
     std::vector<OzTile> tiles;
     uint64_t a_plane = 0, b_plane = 0, n_exp = 0, n_exp_c = 0;
+    int bn = 64;                    // output tile columns (64 or 128)
     bool const_ready = false;       // constant digit planes present in the scratch
     std::vector<DevRow> rowtab;     // rows of row-table problems (the GEMM list's table)
     // first warp item of every job in the exponent and split passes (jobs + 1 entries)
@@ -627,6 +722,26 @@ OzProgram* oz_build(GemmList const& gl) {
     auto* oz = new OzProgram;
     std::vector<uint32_t> nbatch(gl.probs.size(), 0);
     for (auto const& t : gl.tiles) nbatch[t.prob] = std::max(nbatch[t.prob], t.batch + 1);
+    // Tile width: 128-column tiles run the tensor pipe at twice the rate of 64-column
+    // ones but need two passes over K for more than 4 digit groups (reading the digit
+    // planes 11/7 times as often at s = 7) and twice the epilogue per tile; they pay where
+    // the tiles' K walks are long (>= 32 slabs on average) and the columns fill them.
+    {
+        uint64_t tiles64 = 0, slabs64 = 0, area64 = 0, area128 = 0;
+        for (uint32_t p = 0; p < gl.probs.size(); ++p) {
+            DevProb const& pr = gl.probs[p];
+            uint64_t kt = 0;
+            for (uint32_t sgi = pr.seg_begin; sgi < pr.seg_end; ++sgi) kt += (gl.segs[sgi].K + OZ_BK - 1) / OZ_BK;
+            const uint64_t mt = std::max<uint32_t>(1, (pr.M + OZ_BM - 1) / OZ_BM) * uint64_t(nbatch[p]);
+            const uint64_t n64 = std::max<uint32_t>(1, (pr.N + 63) / 64), n128 = std::max<uint32_t>(1, (pr.N + 127) / 128);
+            tiles64 += mt * n64;
+            slabs64 += mt * n64 * kt;
+            area64 += mt * n64 * 64 * kt;
+            area128 += mt * n128 * 128 * kt;
+        }
+        oz->bn = (tiles64 && slabs64 >= 32 * tiles64 && area128 * 100 <= area64 * 115) ? 128 : 64;
+    }
+    const uint32_t OZ_BN = uint32_t(oz->bn), B_TILE = OZ_BN * OZ_BK;
     // exponent offsets: constant operands count in n_exp_c, the others in n_exp
     // (shifted behind the constant region below); var_e / var_f mark the latter
     std::vector<uint8_t> var_e, var_f;
@@ -673,6 +788,7 @@ OzProgram* oz_build(GemmList const& gl) {
                 ja.is_b = 0;
                 ja.is_const = a_const ? 1 : 0;
                 ja.rowtab = pr.rows;
+                ja.tr = OZ_BM;
                 oz->a_plane += uint64_t(pb.MT) * KS * A_TILE;
                 jb.op = sg.B;
                 jb.op.off += uint64_t(b) * sg.B.bstride;
@@ -685,6 +801,7 @@ OzProgram* oz_build(GemmList const& gl) {
                 jb.is_b = 1;
                 jb.is_const = b_const ? 1 : 0;
                 jb.rowtab = DevProb::NO_ROWS;
+                jb.tr = OZ_BN;
                 oz->b_plane += uint64_t(pb.NT) * KS * B_TILE;
                 for (uint32_t ks = 0; ks < KS; ++ks)
                     oz->slabs.push_back(OzSlab{ja.out_base + uint64_t(ks) * A_TILE, jb.out_base + uint64_t(ks) * B_TILE,
@@ -727,7 +844,7 @@ OzProgram* oz_build(GemmList const& gl) {
     oz->split_first.assign(1, 0);
     for (auto const& j : oz->jobs) {
         oz->exp_first.push_back(oz->exp_first.back() + oz_exp_items(j));
-        oz->split_first.push_back(oz->split_first.back() + oz_split_items(j, j.is_b ? OZ_BN : OZ_BM));
+        oz->split_first.push_back(oz->split_first.back() + oz_split_items(j, j.tr));
     }
     if (up(oz->jobs, &oz->d_jobs) != cudaSuccess || up(oz->exp_first, &oz->d_exp_first) != cudaSuccess ||
         up(oz->split_first, &oz->d_split_first) != cudaSuccess || up(oz->pbs, &oz->d_pbs) != cudaSuccess ||
@@ -803,14 +920,20 @@ cudaError_t oz_run(OzProgram* oz, Bases const& bs, int s, void* scratch, int* er
     }
     oz->const_ready = true;
     if (!oz->tiles.empty()) {
-        size_t smem_max = 0;
-        for (int sl = 2; sl <= OZ_MAX_SLICES; ++sl) smem_max = std::max(smem_max, ozaki_smem_bytes(sl));
-        cudaError_t ea = ensure_smem_limit(reinterpret_cast<const void*>(ozaki_mma), int(smem_max));
-        if (ea != cudaSuccess) return ea;
-        OzArgs args{c.A8,        c.B8, c.e, oz->d_pbs, oz->d_slabs, oz->d_tiles, uint32_t(oz->tiles.size()),
-                    oz_chunk_slabs(s), oz_stages(s), s, bs, err, oz->d_rowtab, wait_limit_ns()};
-        ozaki_mma<<<std::min<uint32_t>(uint32_t(oz->tiles.size()), uint32_t(sms)), OZ_THREADS, ozaki_smem_bytes(s),
-                    st>>>(args);
+        // the kernel of the program's tile width, its shared-memory limit raised once for all slice counts
+        auto launch = [&](auto kernel, int bn) -> cudaError_t {
+            size_t smem_max = 0;
+            for (int sl = 2; sl <= OZ_MAX_SLICES; ++sl) smem_max = std::max(smem_max, ozaki_smem_bytes(sl, bn));
+            cudaError_t ea = ensure_smem_limit(reinterpret_cast<const void*>(kernel), int(smem_max));
+            if (ea != cudaSuccess) return ea;
+            OzArgs args{c.A8, c.B8, c.e, oz->d_pbs, oz->d_slabs, oz->d_tiles, uint32_t(oz->tiles.size()),
+                        oz_chunk_slabs(s), oz_stages(s, bn), s, bs, err, oz->d_rowtab, wait_limit_ns()};
+            kernel<<<std::min<uint32_t>(uint32_t(oz->tiles.size()), uint32_t(sms)), OZ_THREADS, ozaki_smem_bytes(s, bn),
+                     st>>>(args);
+            return cudaSuccess;
+        };
+        cudaError_t el = oz->bn == 128 ? launch(ozaki_mma<128>, 128) : launch(ozaki_mma<64>, 64);
+        if (el != cudaSuccess) return el;
     }
     return cudaGetLastError();
 }

@@ -266,11 +266,15 @@ def sweep_workload(args):
     A = S.random_mps(model.phys, S.allowed_sectors(model.phys, L, model.total_charge, 5), rng)
     ctx = E.Context(0)
     dsplit = args.split == "device"
-    dev = G.TwoSiteDMRG(G.DeviceBackend(ctx), model, list(A), m, jd_tol=1e-8, jd_maxiter=8, device_split=dsplit)
+    # state prediction (perturbation) in the first two sweeps, as the reference's alpha_initial
+    # for its grow sweeps (ts_optimize.hpp:274-282); host split only
+    alpha = (lambda sweep: args.alpha if sweep < 2 else 0.0) if args.alpha else 0.0
+    dev = G.TwoSiteDMRG(G.DeviceBackend(ctx), model, list(A), m, jd_tol=1e-8, jd_maxiter=8, device_split=dsplit,
+                        alpha=alpha)
     for sw in range(nsweeps):
         dev.sweep(sw)
     cpu_t0 = time.perf_counter()
-    cpu = G.TwoSiteDMRG(OracleBackend(), model, list(A), m, jd_tol=1e-8, jd_maxiter=8)
+    cpu = G.TwoSiteDMRG(OracleBackend(), model, list(A), m, jd_tol=1e-8, jd_maxiter=8, alpha=alpha)
     for sw in range(nsweeps):
         cpu.sweep(sw)
     cpu_s = time.perf_counter() - cpu_t0
@@ -279,9 +283,12 @@ def sweep_workload(args):
     line = {"metric": "two-site sweep time (s)", "value": float(np.mean(dev.log.sweep_seconds)), "unit": "s",
             "higher_is_better": False, "n_gpus": 1, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "heisenberg_L32_u1_m128_4sweeps", "sites": L, "bond_dim": m, "sweeps": nsweeps,
-                       "split": args.split},
+                       "split": args.split, "alpha_first_two_sweeps": args.alpha},
             "sweep_seconds": dev.log.sweep_seconds, "final_energy": float(ed[-1]),
             "max_abs_energy_diff_vs_oracle": float(np.max(np.abs(ed - ec))),
+            # per-site energies of the last sweep (no perturbation there): with alpha, the earlier
+            # sweeps' truncations may keep different states of a degenerate density-matrix spectrum
+            "last_sweep_max_abs_energy_diff_vs_oracle": float(np.max(np.abs(ed[-(2 * L - 2):] - ec[-(2 * L - 2):]))),
             "hpsi_calls": dev.log.hpsi_calls, "solve_device_ms": dev.log.solve_ms,
             "phase_seconds": dev.log.phase_seconds, "site_problem_phase_seconds": dev.be.phase_seconds,
             "cpu_oracle_sweep_seconds": cpu.log.sweep_seconds, "cpu_oracle_final_energy": float(ec[-1]),
@@ -788,6 +795,8 @@ def main():
                          "two-site split of the middle Hubbard tensor on the device and on the host")
     ap.add_argument("--split", default="host", choices=["host", "device"],
                     help="where the sweep workload splits the two-site tensor")
+    ap.add_argument("--alpha", type=float, default=0.0,
+                    help="perturbation strength of the sweep workload's first two sweeps (host split)")
     ap.add_argument("--qc-sites", type=int, default=24, help="orbitals of the qc workload")
     ap.add_argument("--qc-m", type=int, default=2000, help="bond dimension of the qc workload")
     ap.add_argument("--qc-symmetry", default="su2u1", choices=["su2u1", "twou1"],

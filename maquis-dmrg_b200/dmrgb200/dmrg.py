@@ -539,6 +539,15 @@ class DeviceBackend:
     def right_step(self, model, W, Ridx, Rbuf, t: S.SiteTensor, dev_rp=None):
         return self._step(False, model, W, Ridx, Rbuf, t, dev_rp)
 
+    def galpha(self, plan: dict, Lidx, Lbuf, Ridx, Rbuf, x: np.ndarray) -> np.ndarray:
+        """d<x|H_eff x>/d alpha per plan term (dmrgb200_hpsi_adjoint on the device)."""
+        dp = E.DevicePlan(self.ctx, plan, left_addr=Lidx.cohort_addresses(Lbuf.data_ptr()),
+                          other_addr=Ridx.cohort_addresses(Rbuf.data_ptr()))
+        xd = E.to_device(x, self.ctx.device)
+        ga = self.torch.empty(max(len(plan["term_alpha"]), 1), dtype=self.torch.float64, device=xd.device)
+        dp.adjoint(xd.data_ptr(), xd.data_ptr(), 0, ga.data_ptr())
+        return ga.cpu().numpy()[:len(plan["term_alpha"])]
+
     def alpha_dm(self, phys, W, idx, buf, t: S.SiteTensor, alpha: float, left: bool):
         """Density-matrix blocks (host, per bra block of the step) of the split with the
         perturbation, for t = theta_site(...): dmrgb200_step_alpha_dm on a step plan

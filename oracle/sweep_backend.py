@@ -30,6 +30,9 @@ class OracleBackend:
         sch, _ = E.schedule_right_step(phys, t.left, t.right, W, idx, False)
         return O.alpha_dm(sch.plan, val, idx, t.data, t.data, alpha)
 
+    def galpha(self, plan, Lidx, Lval, Ridx, Rval, x):
+        return O.hpsi_adjoint(plan, Lval, Lidx, Rval, Ridx, x, x)[1]
+
     def solve(self, p12, psi, W12, Lidx, Lval, Ridx, Rval, tol, max_iter):
         sch = E.schedule_hpsi(p12, psi.left, psi.right, W12, Lidx, Ridx)
         theta, u, it, conv, rn = JD.jcd(lambda v: O.hpsi(sch.plan, Lval, Lidx, Rval, Ridx, v), psi.data, tol=tol,

@@ -1,0 +1,37 @@
+"""Integral derivatives (1-/2-RDM elements) of a whole MPS by moving the two-site
+centre over every site pair (dmrgb200.rdm) on the CPU oracle, against the dense
+expectation value <psi|dH/dc|psi> of the normalised state -- including integrals
+whose coefficients sit far from any one centre pair."""
+import dataclasses
+
+import numpy as np
+
+import dense as D
+from dmrgb200 import mps as S
+from dmrgb200 import qc
+from dmrgb200 import rdm
+from sweep_backend import OracleBackend
+
+INTEGRALS = [("h", (0, 1)), ("h", (3, 4)), ("h", (0, 4)), ("h", (2, 2)), ("eri", (0, 0, 4, 4)),
+             ("eri", (0, 1, 3, 4)), ("eri", (1, 2, 2, 3)), ("eri", (0, 3, 1, 4))]
+
+
+def dense_derivatives(model, tensors, L):
+    v = D.mps_dense([t.dense() for t in tensors])
+    v = v / np.linalg.norm(v)
+    out = {}
+    for key in INTEGRALS:
+        Op = D.sparse_hamiltonian(dataclasses.replace(model, dense_terms=qc.integral_operator_terms(*key)), L)
+        out[key] = float(v @ (Op @ v))
+    return out
+
+
+def test_integral_derivatives_over_the_chain_match_dense_rdm_elements():
+    L = 5
+    model = qc.quantum_chemistry(L, 2, 2)
+    tensors = S.random_mps(model.phys, S.allowed_sectors(model.phys, L, model.total_charge, 16),
+                           np.random.default_rng(7))
+    got = rdm.integral_derivatives(OracleBackend(), model, tensors, INTEGRALS)
+    want = dense_derivatives(model, tensors, L)
+    for key in INTEGRALS:
+        assert abs(got[key] - want[key]) <= 1e-11 * max(1.0, abs(want[key])), (key, got[key], want[key])

@@ -725,9 +725,9 @@ OzProgram* oz_build(GemmList const& gl) {
     // Tile width: 128-column tiles run the tensor pipe at twice the rate of 64-column
     // ones but need two passes over K for more than 4 digit groups (reading the digit
     // planes 11/7 times as often at s = 7) and twice the epilogue per tile; they pay where
-    // the tiles' K walks are long (>= 32 slabs on average) and the columns fill them.
+    // the tiles' K walks are long (>= 32 slabs on average) and the columns fill them
     {
-        uint64_t tiles64 = 0, slabs64 = 0, area64 = 0, area128 = 0;
+        uint64_t tiles64 = 0, tiles128 = 0, slabs64 = 0, area64 = 0, area128 = 0;
         for (uint32_t p = 0; p < gl.probs.size(); ++p) {
             DevProb const& pr = gl.probs[p];
             uint64_t kt = 0;
@@ -735,11 +735,16 @@ OzProgram* oz_build(GemmList const& gl) {
             const uint64_t mt = std::max<uint32_t>(1, (pr.M + OZ_BM - 1) / OZ_BM) * uint64_t(nbatch[p]);
             const uint64_t n64 = std::max<uint32_t>(1, (pr.N + 63) / 64), n128 = std::max<uint32_t>(1, (pr.N + 127) / 128);
             tiles64 += mt * n64;
+            tiles128 += mt * n128;
             slabs64 += mt * n64 * kt;
             area64 += mt * n64 * 64 * kt;
             area128 += mt * n128 * 128 * kt;
         }
-        oz->bn = (tiles64 && slabs64 >= 32 * tiles64 && area128 * 100 <= area64 * 115) ? 128 : 64;
+        // ... and where the wider tiles still give every SM two of them
+        oz->bn = (tiles64 && slabs64 >= 32 * tiles64 && area128 * 100 <= area64 * 115 &&
+                  tiles128 >= 2 * uint64_t(device_sm_count()))
+                     ? 128
+                     : 64;
     }
     const uint32_t OZ_BN = uint32_t(oz->bn), B_TILE = OZ_BN * OZ_BK;
     // exponent offsets: constant operands count in n_exp_c, the others in n_exp

@@ -554,9 +554,10 @@ def qc_workload(args):
 
 
 def adjoint_workload(args):
-    """Adjoint check on the ab-initio Hamiltonian (TwoU1) at L orbitals, L electrons,
-    bond dimension m, middle two-site problem with device-built boundaries and a
-    seeded random normalised psi, E = <psi|H_eff|psi> / <psi|psi>:
+    """Adjoint check on the ab-initio Hamiltonian (SU2U1 by default, TwoU1 with
+    --adj-symmetry twou1) at L orbitals, L electrons, bond dimension m, middle two-site
+    problem with device-built boundaries and a seeded random normalised psi (the
+    spin-reduced two-site tensor for SU2U1), E = <psi|H_eff|psi> / <psi|psi>:
       * dE/dpsi from one adjoint call (gx = H^T psi) against central finite
         differences (step 1e-6) along seeded random unit directions;
       * dE/d(integral) for integrals whose operators all sit at or left of the
@@ -564,7 +565,8 @@ def adjoint_workload(args):
         against central finite differences of E (alphas moved by +-1e-6 d alpha,
         exact because alpha is linear in the integral) and against the RDM
         element <psi|H_eff(dH/d integral)|psi> / <psi|psi> computed through the
-        observable's own MPO, boundary steps and H·psi.
+        observable's own MPO (the model whose only integral is the raised one: H is
+        linear in the integrals), boundary steps and H·psi.
     The environment is mixed-canonical (sites left of the pair left-normalised,
     right of it right-normalised), so E is the energy of the MPS state.  One JSON
     line: the adjoint and forward times and every relative error."""
@@ -574,13 +576,21 @@ def adjoint_workload(args):
     from dmrgb200 import models as M
     from dmrgb200 import mps as S
     from dmrgb200 import qc
+    from dmrgb200 import rdm as RD
+    from dmrgb200 import su2u1 as SU
 
     from dmrgb200 import dmrg as G
 
     L, m = args.adj_sites, args.adj_m
+    su2 = args.adj_symmetry == "su2u1"
     t0 = time.perf_counter()
-    model = qc.quantum_chemistry(L, L // 2, L // 2)
-    bonds = S.synthetic_bonds(model.phys, L, model.total_charge, m, RADIUS)
+    if su2:
+        h, eri = qc.synthetic_integrals(L)
+        model = SU.quantum_chemistry(L, L, 0, h=h, eri=eri)
+        bonds = SU.synthetic_bonds(L, (L, 0), m, RADIUS)
+    else:
+        model = qc.quantum_chemistry(L, L // 2, L // 2)
+        bonds = S.synthetic_bonds(model.phys, L, model.total_charge, m, RADIUS)
     rng = np.random.default_rng(SEED)
     i = L // 2 - 1
     # mixed-canonical environment (left-normalised left of the pair, right-normalised
@@ -630,12 +640,17 @@ def adjoint_workload(args):
         psi_err.append(abs(an - fd) / max(abs(fd), 1e-300))
     ga_np = ga.cpu().numpy()
     c = i + 1
-    integrals = [("h", (i, c)), ("h", (2, c)), ("eri", (i, c, i, c)), ("eri", (3, i, c, c))]
+    # integrals whose coefficients sit in the centre tensors (the centre-pair derivative is then
+    # the whole derivative; dmrgb200.rdm moves the centre for the others)
+    if su2:
+        integrals = [("h", (i, c)), ("h", (c, c)), ("eri", (i, c, i, c)), ("eri", (i - 1, i, c, c))]
+    else:
+        integrals = [("h", (i, c)), ("h", (2, c)), ("eri", (i, c, i, c)), ("eri", (3, i, c, c))]
     checks = []
     for which, index in integrals:
         h2, eri2 = qc.raise_integral(model.h, model.eri, which, index, 1.0)
-        m2 = qc.quantum_chemistry(L, L // 2, L // 2, h=h2, eri=eri2)
-        W12 = M.MPOHandle(M.twosite_mpo(m2.mpo[i], m2.mpo[i + 1], m2.phys, m2.phys), m2.symm)
+        m2 = RD.with_integrals(model, h2, eri2)
+        W12 = M.MPOHandle(M.twosite_for(m2, i), m2.symm)
         s2 = E.schedule_hpsi(sp.p12, sp.left, sp.right, W12, sp.Lidx, sp.Ridx).plan
         for key in ("term_t", "term_col", "l_term", "l_b1"):
             assert np.array_equal(base[key], s2[key]), "MPO structure changed with the integral"
@@ -650,7 +665,11 @@ def adjoint_workload(args):
             es.append(energy(p2, x))
             del p2
         fd = (es[0] - es[1]) / (2 * eps)
-        om = qc.operator_model(model, qc.integral_operator_terms(which, index))
+        if su2:
+            om = RD.with_integrals(model, *qc.raise_integral(np.zeros_like(model.h), np.zeros_like(model.eri),
+                                                             which, index, 1.0))
+        else:
+            om = qc.operator_model(model, qc.integral_operator_terms(which, index))
         so = E.SiteProblem(ctx, om, tensors, bonds, i)
         assert so.size == n
         rdm = energy(so.plan, x)
@@ -660,8 +679,9 @@ def adjoint_workload(args):
                        "rel_err_rdm": abs(adj - rdm) / max(abs(rdm), 1e-300)})
     line = {"metric": "H·psi adjoint check (FP64)", "value": adj_ms, "unit": "ms", "higher_is_better": False,
             "n_gpus": 1, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"qc_L{L}_twou1_m{m}_adjoint_middle", "sites": L, "bond_dim": m,
-                       "symmetry": "TwoU1", "psi_elements": int(n), "terms": int(len(base["term_alpha"])),
+            "config": {"workload": f"qc_L{L}_{args.adj_symmetry}_m{m}_adjoint_middle", "sites": L, "bond_dim": m,
+                       "symmetry": "SU2U1" if su2 else "TwoU1", "psi_elements": int(n),
+                       "terms": int(len(base["term_alpha"])),
                        "setup_seconds": time.perf_counter() - t0, "fd_step": eps},
             "forward_ms": fwd_ms, "adjoint_ms": adj_ms, "energy": e0,
             "psi_gradient": {"directions": 3, "max_rel_err_fd": max(psi_err)},
@@ -803,6 +823,8 @@ def main():
                     help="symmetry of the qc workload (SU2U1: spin-adapted, bond dimension in multiplets)")
     ap.add_argument("--adj-sites", type=int, default=16, help="orbitals of the adjoint workload")
     ap.add_argument("--adj-m", type=int, default=512, help="bond dimension of the adjoint workload")
+    ap.add_argument("--adj-symmetry", default="su2u1", choices=["su2u1", "twou1"],
+                    help="symmetry of the adjoint workload")
     ap.add_argument("--prec", default="fp64", choices=["fp64", "emulated"],
                     help="precision of the --profile steps")
     ap.add_argument("--profile", action="store_true",

@@ -22,26 +22,47 @@ from __future__ import annotations
 
 import numpy as np
 
+from . import _capi as capi
 from . import dmrg as G
 from . import engine as E
 from . import models as M
 from . import qc
 
 
+def _twosite(W1, W2, model):
+    """Two-site MPO whose term scales are linear in each site's scales: the spin-coupled
+    product for SU2U1, the unmerged Kronecker product otherwise."""
+    if model.symm == capi.SU2U1:
+        from . import su2u1
+        return su2u1.twosite_mpo(W1, W2, model.phys, model.phys)
+    return M.twosite_mpo(W1, W2, model.phys, model.phys, merge=False)
+
+
 def _alpha(p12, left, right, W1, W2, model, Lidx, Ridx):
-    W12 = M.MPOHandle(M.twosite_mpo(W1, W2, model.phys, model.phys, merge=False), model.symm)
+    W12 = M.MPOHandle(_twosite(W1, W2, model), model.symm)
     return E.schedule_hpsi(p12, left, right, W12, Lidx, Ridx).plan
+
+
+def with_integrals(model, h, eri):
+    """The quantum-chemistry model of `model`'s kind (TwoU1 or SU2U1), sites and electrons
+    with other integrals."""
+    L = len(model.mpo)
+    if model.symm == capi.SU2U1:
+        from . import su2u1
+        return su2u1.quantum_chemistry(L, model.total_charge[0], model.total_charge[1], h=h, eri=eri)
+    return qc.quantum_chemistry(L, model.total_charge[0], model.total_charge[1], h=h, eri=eri)
 
 
 def integral_derivatives(backend, model, tensors, integrals) -> dict:
     """dE/dc for every c in `integrals` (("h", (a, b)) or ("eri", (a, b, c, d)); the
-    orbit of the index as qc.raise_integral raises it) of the TwoU1 quantum-chemistry
-    model for the normalised state of `tensors`.  backend: an object with edge,
-    left_step, right_step (as dmrg.DeviceBackend / the oracle backend) and
-    galpha(plan, Lidx, Lbuf, Ridx, Rbuf, x) returning d<x|H x>/d alpha per plan term."""
+    orbit of the index as qc.raise_integral raises it) of the quantum-chemistry model
+    (TwoU1, or SU2U1 where H_eff acts on the spin-reduced two-site tensor) for the
+    normalised state of `tensors`.  backend: an object with edge, left_step, right_step
+    (as dmrg.DeviceBackend / the oracle backend) and galpha(plan, Lidx, Lbuf, Ridx, Rbuf,
+    x) returning d<x|H x>/d alpha per plan term."""
     L = len(tensors)
-    raised = {key: qc.quantum_chemistry(L, model.total_charge[0], model.total_charge[1],
-                                        *qc.raise_integral(model.h, model.eri, key[0], key[1], 1.0))
+    su2 = model.symm == capi.SU2U1
+    raised = {key: with_integrals(model, *qc.raise_integral(model.h, model.eri, key[0], key[1], 1.0))
               for key in integrals}
     A = G.right_canonicalize(list(tensors), 0.0)
     p12, offs = M.fuse_phys(model.phys, model.phys)
@@ -60,7 +81,13 @@ def integral_derivatives(backend, model, tensors, integrals) -> dict:
         psi.data = psi.data / norm
         Ridx, Rbuf = R[i + 2]
         base = _alpha(p12, psi.left, psi.right, model.mpo[i], model.mpo[i + 1], model, Lidx, Ridx)
-        ga = backend.galpha(base, Lidx, Lbuf, Ridx, Rbuf, psi.data)
+        if su2:
+            # H_eff acts on the spin-reduced two-site tensor (the 6j recoupling is orthogonal)
+            from . import su2u1
+            x = su2u1.reduce_twosite(psi, model.phys, model.phys, offs).data
+        else:
+            x = psi.data
+        ga = backend.galpha(base, Lidx, Lbuf, Ridx, Rbuf, x)
         sites = (i, i + 1) if i == L - 2 else (i,)
         for key, m2 in raised.items():
             for j in sites:

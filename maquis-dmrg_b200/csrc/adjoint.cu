@@ -78,43 +78,43 @@ __global__ void __launch_bounds__(256) tgrad_cells(const DevSLine* __restrict__ 
 
 // galpha of the terms of grouped units (DevSGroup, built for the forward S build):
 // gram[entry * SG_LINES + j] = <G line j of the group, T source of the entry>, one
-// warp per (group, batch of AG_BATCH entries, half of the group's lines).  Per
-// 128-element chunk every lane holds the half's 8 lines' G values of its 4 elements;
-// per entry it forms 8 partial products, which a reduce-scatter butterfly (9
-// shuffles) sums over the warp so that lanes 4j .. 4j+3 end with line j's total;
-// the chunks add up in order, so the result is bitwise reproducible.  A term's
-// galpha is then its (entry, line) slot.
-constexpr int AG_BATCH = 16, AG_LINES = 8, AG_HALVES = SG_LINES / AG_LINES;
-static_assert(SG_LINES % AG_LINES == 0, "line groups in halves of 8");
-__device__ __forceinline__ double sum8_scatter(double const (&p)[AG_LINES], uint32_t lane) {
-    const bool h1 = (lane >> 4) & 1u, h2 = (lane >> 3) & 1u, h3 = (lane >> 2) & 1u;
-    double q[4], r[2];
+// warp per (group, batch of AG_BATCH entries).  Per 128-element chunk every lane holds
+// the group's 16 lines' G values of its 4 elements; per entry it forms 16 partial
+// products, which a reduce-scatter butterfly (16 shuffles) sums over the warp so that
+// lanes 2j, 2j+1 end with line j's total; the chunks add up in order, so the result is
+// bitwise reproducible.  A term's galpha is then its (entry, line) slot.
+constexpr int AG_BATCH = 16;
+static_assert(SG_LINES == 16, "the butterfly below scatters 16 lines over the warp");
+__device__ __forceinline__ double sum16_scatter(double const (&p)[SG_LINES], uint32_t lane) {
+    const bool h1 = (lane >> 4) & 1u, h2 = (lane >> 3) & 1u, h3 = (lane >> 2) & 1u, h4 = (lane >> 1) & 1u;
+    double q[8], r[4], t[2];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const double send = h1 ? p[k] : p[8 + k];
+        q[k] = (h1 ? p[8 + k] : p[k]) + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        const double send = h1 ? p[k] : p[4 + k];
-        q[k] = (h1 ? p[4 + k] : p[k]) + __shfl_xor_sync(0xffffffffu, send, 16);
+        const double send = h2 ? q[k] : q[4 + k];
+        r[k] = (h2 ? q[4 + k] : q[k]) + __shfl_xor_sync(0xffffffffu, send, 8);
     }
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
-        const double send = h2 ? q[k] : q[2 + k];
-        r[k] = (h2 ? q[2 + k] : q[k]) + __shfl_xor_sync(0xffffffffu, send, 8);
+        const double send = h3 ? r[k] : r[2 + k];
+        t[k] = (h3 ? r[2 + k] : r[k]) + __shfl_xor_sync(0xffffffffu, send, 4);
     }
-    double v = (h3 ? r[1] : r[0]) + __shfl_xor_sync(0xffffffffu, h3 ? r[0] : r[1], 4);
-    v += __shfl_xor_sync(0xffffffffu, v, 2);
+    double v = (h4 ? t[1] : t[0]) + __shfl_xor_sync(0xffffffffu, h4 ? t[0] : t[1], 2);
     v += __shfl_xor_sync(0xffffffffu, v, 1);
-    return v;  // the line (lane >> 2) & 7 of the half
+    return v;  // the line (lane >> 1) & 15
 }
 
-// items: DevSItem{group, entry} per batch; the warp item it covers half it % AG_HALVES
 __global__ void __launch_bounds__(128) gram_groups(const DevSGroup* __restrict__ groups,
                                                    const DevSItem* __restrict__ items, uint32_t n_items,
                                                    const uint64_t* __restrict__ ent_t, const double* __restrict__ G,
                                                    const double* __restrict__ T, double* __restrict__ gram) {
     const uint32_t lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
-    const uint32_t n_work = n_items * AG_HALVES;
-    for (uint32_t w = blockIdx.x * wpb + (threadIdx.x >> 5); w < n_work; w += gridDim.x * wpb) {
-        const DevSItem I = items[w / AG_HALVES];
-        const uint32_t j0 = (w % AG_HALVES) * AG_LINES;
+    for (uint32_t it = blockIdx.x * wpb + (threadIdx.x >> 5); it < n_items; it += gridDim.x * wpb) {
+        const DevSItem I = items[it];
         const DevSGroup Gr = groups[I.group];
         const uint32_t n = Gr.rows * Gr.cols, nb = min(uint32_t(AG_BATCH), Gr.ent_end - I.e0);
         const uint64_t my_tb = lane < nb ? ent_t[I.e0 + lane] : 0;
@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(128) gram_groups(const DevSGroup* __restrict__
 #pragma unroll
         for (int b = 0; b < AG_BATCH; ++b) acc[b] = 0.0;
         for (uint32_t c0 = 0; c0 < n; c0 += 32 * SG_EPT) {
-            double g[AG_LINES][SG_EPT];
+            double g[SG_LINES][SG_EPT];
             uint32_t el[SG_EPT];
             bool in[SG_EPT];
 #pragma unroll
@@ -132,8 +132,8 @@ __global__ void __launch_bounds__(128) gram_groups(const DevSGroup* __restrict__
                 const uint32_t col = in[u] ? el[u] / Gr.rows : 0, i = in[u] ? el[u] - col * Gr.rows : 0;
                 const double* src = G + Gr.s_base + i + uint64_t(col) * Gr.ld_s;
 #pragma unroll
-                for (int j = 0; j < AG_LINES; ++j)
-                    g[j][u] = (in[u] && j0 + j < Gr.nlines) ? src[uint64_t(j0 + j) * Gr.line_stride] : 0.0;
+                for (int j = 0; j < SG_LINES; ++j)
+                    g[j][u] = (in[u] && uint32_t(j) < Gr.nlines) ? src[uint64_t(j) * Gr.line_stride] : 0.0;
             }
 #pragma unroll
             for (int b = 0; b < AG_BATCH; ++b) {
@@ -142,21 +142,20 @@ __global__ void __launch_bounds__(128) gram_groups(const DevSGroup* __restrict__
                 double t[SG_EPT];
 #pragma unroll
                 for (int u = 0; u < SG_EPT; ++u) t[u] = in[u] ? T[tb + el[u]] : 0.0;
-                double p[AG_LINES];
+                double p[SG_LINES];
 #pragma unroll
-                for (int j = 0; j < AG_LINES; ++j) {
+                for (int j = 0; j < SG_LINES; ++j) {
                     double a = 0.0;
 #pragma unroll
                     for (int u = 0; u < SG_EPT; ++u) a = fma(g[j][u], t[u], a);
                     p[j] = a;
                 }
-                acc[b] += sum8_scatter(p, lane);
+                acc[b] += sum16_scatter(p, lane);
             }
         }
 #pragma unroll
         for (int b = 0; b < AG_BATCH; ++b)
-            if (uint32_t(b) < nb && (lane & 3u) == 0)
-                gram[uint64_t(I.e0 + b) * SG_LINES + j0 + (lane >> 2)] = acc[b];
+            if (uint32_t(b) < nb && (lane & 1u) == 0) gram[uint64_t(I.e0 + b) * SG_LINES + (lane >> 1)] = acc[b];
     }
 }
 
@@ -507,7 +506,7 @@ cudaError_t run_adjoint(DeviceProgram const& fwd, AdjointProgram const& a, uint6
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
         if (a.n_gram_items) {
-            uint32_t grid = std::min<uint32_t>((a.n_gram_items * AG_HALVES + 3) / 4, sms * 8);
+            uint32_t grid = std::min<uint32_t>((a.n_gram_items + 3) / 4, sms * 8);
             gram_groups<<<grid, 128, 0, stream>>>(fwd.d_groups, a.d_gram_items, a.n_gram_items, fwd.d_gent_t, S, T,
                                                   a.d_gram);
             if ((e = cudaGetLastError()) != cudaSuccess) return e;

@@ -291,6 +291,8 @@ def sweep_workload(args):
             "last_sweep_max_abs_energy_diff_vs_oracle": float(np.max(np.abs(ed[-(2 * L - 2):] - ec[-(2 * L - 2):]))),
             "hpsi_calls": dev.log.hpsi_calls, "solve_device_ms": dev.log.solve_ms,
             "phase_seconds": dev.log.phase_seconds, "site_problem_phase_seconds": dev.be.phase_seconds,
+            "plan_cache": {"hits": dev.be.cache_hits, "misses": dev.be.cache_misses,
+                           "schedule_hits": dev.be.schedule_hits},
             "cpu_oracle_sweep_seconds": cpu.log.sweep_seconds, "cpu_oracle_final_energy": float(ec[-1]),
             "note": ("two-site formation on the host; the split on the device (block Jacobi SVD, truncation choice "
                      "on the host from the singular values)" if dsplit else

@@ -483,6 +483,11 @@ class DeviceBackend:
         # schedules at every site of every sweep, site_hamil_schedule.hpp:40-93)
         self.reuse_plans = reuse_plans
         self.cache = {}
+        # schedules by structure: (kind, MPO tensor, bond sectors, boundary index signatures); a
+        # schedule depends on nothing else, so after the bond sectors settle every later sweep
+        # finds its schedules here even though its boundary buffers and index objects are new
+        self.schedules = {}
+        self.schedule_hits = 0
         self.cache_hits = 0
         self.cache_misses = 0
         self.slices_used = []  # (digit planes, relative H·psi error of the start vector) per emulated solve
@@ -505,11 +510,20 @@ class DeviceBackend:
             _, idx_keep, nidx, plan, out = hit
             self.cache_hits += 1
         else:
-            if left:
+            skey = (site_key, tuple(t.left), tuple(t.right), idx.signature())
+            cached = self.schedules.get(skey) if self.reuse_plans else None
+            if cached is not None:
+                sched, nidx = cached[1], cached[2]
+                self.schedule_hits += 1
+            elif left:
                 sched, nidx = E.schedule_left_step(model.phys, t.left, t.right, W, idx, True)
-                plan = E.DevicePlan(self.ctx, sched.plan, left_addr=idx.cohort_addresses(buf.data_ptr()))
             else:
                 sched, nidx = E.schedule_right_step(model.phys, t.left, t.right, W, idx, True)
+            if self.reuse_plans and cached is None:
+                self.schedules[skey] = (W, sched, nidx)  # W kept alive: its id is part of the key
+            if left:
+                plan = E.DevicePlan(self.ctx, sched.plan, left_addr=idx.cohort_addresses(buf.data_ptr()))
+            else:
                 plan = E.DevicePlan(self.ctx, sched.plan, other_addr=idx.cohort_addresses(buf.data_ptr()))
             out = self.torch.zeros(max(nidx.n_elems, 1), dtype=self.torch.float64, device=buf.device)
             self.cache_misses += 1
@@ -584,7 +598,15 @@ class DeviceBackend:
             self.cache_hits += 1
             t1 = t2 = time.perf_counter()
         else:
-            sched = E.schedule_hpsi(p12, psi.left, psi.right, W12, Lidx, Ridx)
+            skey = (site_key, tuple(psi.left), tuple(psi.right), Lidx.signature(), Ridx.signature())
+            cached = self.schedules.get(skey) if self.reuse_plans else None
+            if cached is not None:
+                sched = cached[1]
+                self.schedule_hits += 1
+            else:
+                sched = E.schedule_hpsi(p12, psi.left, psi.right, W12, Lidx, Ridx)
+                if self.reuse_plans:
+                    self.schedules[skey] = (W12, sched)
             t1 = time.perf_counter()
             plan = E.DevicePlan(self.ctx, sched.plan, left_addr=Lidx.cohort_addresses(Lbuf.data_ptr()),
                                 other_addr=Ridx.cohort_addresses(Rbuf.data_ptr()))

@@ -60,6 +60,19 @@ class BIndex:
         self.conj = self.conj.reshape(n, a)
         self.trans = self.trans.reshape(n, a)
 
+    def signature(self) -> int:
+        """Hash of the index structure (cohorts, sizes, storage layout, conjugation and
+        transposition tables): equal for indices that schedules cannot tell apart."""
+        if getattr(self, "_sig", None) is None:
+            import hashlib
+            hsh = hashlib.blake2b(digest_size=16)
+            for a in (self.lb, self.rb, self.tr, self.storage_off, self.lsize, self.rsize, self.nblocks, self.offsets,
+                      self.conj, self.trans):
+                hsh.update(np.ascontiguousarray(a).tobytes())
+            hsh.update(np.array([self.n_cohorts, self.aux, self.n_elems], dtype=np.uint64).tobytes())
+            self._sig = int.from_bytes(hsh.digest(), "little")
+        return self._sig
+
     def has_storage(self, ci):
         return self.storage_off[ci] != np.uint64(0xFFFFFFFFFFFFFFFF)
 

@@ -110,3 +110,18 @@ def test_perturbed_sweeps_reach_exact_ground_energy():
         e = dm.sweep(sw)
     assert dm.log.phase_seconds.get("alpha_dm", 0.0) > 0.0
     assert abs(e - dense.ground_energy(model, L)) <= 1e-9
+
+
+def test_perturbed_su2u1_sweeps_reach_fci():
+    """SU2U1 quantum chemistry L=6 from a bond-dimension-3 start with the perturbation in
+    the first two sweeps: the sweeps still reach the FCI singlet ground energy."""
+    L, n = 6, 6
+    h, eri = qc.synthetic_integrals(L)
+    model = SU.quantum_chemistry(L, n, 0, h=h, eri=eri)
+    A = S.random_mps(SU.PHYS, SU.allowed_sectors(L, (n, 0), 3), np.random.default_rng(2))
+    dm = G.TwoSiteDMRG(OracleBackend(), model, list(A), 100, jd_tol=1e-10, jd_maxiter=12,
+                       alpha=lambda sweep: 1e-3 if sweep < 2 else 0.0)
+    for sw in range(4):
+        e = dm.sweep(sw)
+    assert dm.log.phase_seconds.get("alpha_dm", 0.0) > 0.0
+    assert abs(e - dense.spin_sector_spectrum(h, eri, n, 0)[0]) <= 1e-9

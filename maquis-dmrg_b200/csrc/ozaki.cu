@@ -45,9 +45,9 @@ constexpr int A_TILE = OZ_BM * OZ_BK;
 constexpr int OZ_MAX_SLICES = 8, OZ_MAX_STAGES = 8;
 __host__ __device__ constexpr int oz_pass_groups(int bn) { return 512 / bn; }
 __host__ __device__ constexpr int oz_passes(int s, int bn) { return (s + oz_pass_groups(bn) - 1) / oz_pass_groups(bn); }
-// warps 0-3 drain the accumulators (TMEM lane quarter = warp), warp 4 loads the slabs,
-// warp 5 issues the MMAs
-constexpr int OZ_EPI_WARPS = 4, OZ_LOAD_WARP = 4, OZ_MMA_WARP = 5, OZ_THREADS = 32 * 6;
+// warps 0-7 drain the accumulators (TMEM lane quarter = warp % 4, column half = warp / 4),
+// warp 8 loads the slabs, warp 9 issues the MMAs
+constexpr int OZ_EPI_WARPS = 8, OZ_LOAD_WARP = 8, OZ_MMA_WARP = 9, OZ_THREADS = 32 * 10;
 constexpr uint32_t OZ_SMEM_CAP = 227u * 1024u;  // dynamic shared memory of one CTA
 constexpr uint32_t OZ_BAR_BYTES = 256;          // barriers and slots behind the stages
 // pipeline depth for s digit planes: as many stages of s (A + B) tiles as fit
@@ -560,7 +560,10 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_mma(OzArgs a) {
         }
         __syncwarp();
     } else {
-        // epilogue warps: TMEM lanes warp * 32 .. + 31 are rows warp * 32 .. of the tile
+        // epilogue warps: TMEM lanes (warp % 4) * 32 .. + 31 are rows (warp % 4) * 32 .. of the
+        // tile; the warp drains the columns half * OZ_BN / 2 .. of them
+        const int quarter = warp & 3, half = warp >> 2;
+        constexpr int HALF = OZ_BN / 2;
         uint32_t rounds = 0;
         bool ok = true;
         for (uint32_t tile = blockIdx.x; tile < a.n_tiles && ok; tile += gridDim.x) {
@@ -568,7 +571,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_mma(OzArgs a) {
             const OzPB pb = a.pbs[tl.pb];
             const uint32_t KT = pb.slab_end - pb.slab_begin;
             const uint32_t nch = KT ? (KT + a.chunk - 1) / a.chunk : 1;
-            const uint32_t row = tl.mt * OZ_BM + warp * 32 + lane;
+            const uint32_t row = tl.mt * OZ_BM + quarter * 32 + lane;
             const int erow = (row < pb.M) ? a.e[pb.e_off + row] : 0;
             double* crow = nullptr;
             uint64_t ldc = pb.C.ld;
@@ -597,24 +600,22 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_mma(OzArgs a) {
                     const bool add = pb.beta || !first;
                     first = false;
                     if constexpr (OZ_BN == 64) {
-                        // read the groups largest g first, releasing each as soon as all four
-                        // warps have read it, then scale and store the 64 sums
-                        double acc[OZ_BN];
+                        // read the groups largest g first, releasing each as soon as all eight
+                        // warps have read it, then scale and store the warp's 32 sums
+                        double acc[HALF];
 #pragma unroll
-                        for (int j = 0; j < OZ_BN; ++j) acc[j] = 0.0;
+                        for (int j = 0; j < HALF; ++j) acc[j] = 0.0;
                         for (int g = g1 - 1; g >= g0; --g) {
                             if (KT > 0) {
                                 const double w = pow2_normal(-7 * (g + 2));
-                                const uint32_t taddr = tmem + (uint32_t(warp * 32) << 16) + uint32_t((g - g0) * OZ_BN);
+                                const uint32_t taddr =
+                                    tmem + (uint32_t(quarter * 32) << 16) + uint32_t((g - g0) * OZ_BN + half * HALF);
+                                int32_t v[32];
+                                tmem_ld16(taddr, v);
+                                tmem_ld16(taddr + 16, v + 16);
+                                tmem_wait_ld();
 #pragma unroll
-                                for (int c0 = 0; c0 < OZ_BN; c0 += 32) {
-                                    int32_t v[32];
-                                    tmem_ld16(taddr + c0, v);
-                                    tmem_ld16(taddr + c0 + 16, v + 16);
-                                    tmem_wait_ld();
-#pragma unroll
-                                    for (int j = 0; j < 32; ++j) acc[c0 + j] += i2d_exact(v[j]) * w;
-                                }
+                                for (int j = 0; j < 32; ++j) acc[j] += i2d_exact(v[j]) * w;
                             }
                             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
                             __syncwarp();
@@ -622,8 +623,8 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_mma(OzArgs a) {
                         }
                         if (crow) {
 #pragma unroll
-                            for (int j = 0; j < OZ_BN; ++j) {
-                                const uint32_t col = tl.nt * OZ_BN + j;
+                            for (int j = 0; j < HALF; ++j) {
+                                const uint32_t col = tl.nt * OZ_BN + half * HALF + j;
                                 if (col < pb.N) {
                                     // x 2^(e_row + e_col): one multiplication by the exact power
                                     // where it is normal (the value ldexp gives), ldexp otherwise
@@ -636,14 +637,14 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) ozaki_mma(OzArgs a) {
                             }
                         }
                     } else {
-                    for (int c0 = 0; c0 < OZ_BN; c0 += 32) {
+                    for (int c0 = half * HALF; c0 < (half + 1) * HALF; c0 += 32) {
                         double acc[32];
 #pragma unroll
                         for (int j = 0; j < 32; ++j) acc[j] = 0.0;
                         for (int g = g1 - 1; g >= g0 && KT > 0; --g) {
                             const double w = pow2_normal(-7 * (g + 2));
                             int32_t v[32];
-                            const uint32_t taddr = tmem + (uint32_t(warp * 32) << 16) + uint32_t((g - g0) * OZ_BN + c0);
+                            const uint32_t taddr = tmem + (uint32_t(quarter * 32) << 16) + uint32_t((g - g0) * OZ_BN + c0);
                             tmem_ld16(taddr, v);
                             tmem_ld16(taddr + 16, v + 16);
                             tmem_wait_ld();
@@ -817,8 +818,16 @@ OzProgram* oz_build(GemmList const& gl) {
             pb.slab_end = uint32_t(oz->slabs.size());
             uint32_t pbi = uint32_t(oz->pbs.size());
             oz->pbs.push_back(pb);
-            for (uint32_t mt = 0; mt < pb.MT; ++mt)
-                for (uint32_t nt = 0; nt < pb.NT; ++nt) oz->tiles.push_back(OzTile{pbi, mt, nt, 0});
+            // the tiles that share the larger operand's digit tile next to each other: CTAs that
+            // start together read the same tile of it, so it comes from DRAM once and from L2 for
+            // the others (the smaller operand is re-read, from L2)
+            if (pb.N > pb.M) {
+                for (uint32_t nt = 0; nt < pb.NT; ++nt)
+                    for (uint32_t mt = 0; mt < pb.MT; ++mt) oz->tiles.push_back(OzTile{pbi, mt, nt, 0});
+            } else {
+                for (uint32_t mt = 0; mt < pb.MT; ++mt)
+                    for (uint32_t nt = 0; nt < pb.NT; ++nt) oz->tiles.push_back(OzTile{pbi, mt, nt, 0});
+            }
         }
     }
     for (size_t i = 0; i < oz->pbs.size(); ++i) {

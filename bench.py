@@ -747,12 +747,17 @@ def batched_workload(args):
         for _ in range(3):
             bp.hpsi(x.data_ptr(), y.data_ptr(), prec)
         torch.cuda.synchronize()
+        profiled = name == args.prec  # the profiler range holds only the timed steps of --prec
+        if profiled:
+            torch.cuda.profiler.start()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
         for _ in range(20):
             bp.hpsi(x.data_ptr(), y.data_ptr(), prec)
         b.record()
         b.synchronize()
+        if profiled:
+            torch.cuda.profiler.stop()
         bp.check()
         ms = a.elapsed_time(b) / 20
         res[name] = {"ms_per_step": ms, "value": bp.flops / (ms * 1e-3) / 1e9, "unit": "GFLOP/s"}

@@ -28,6 +28,7 @@ u8p = C.POINTER(C.c_uint8)
 f64p = C.POINTER(C.c_double)
 
 OK = 0
+INVALID_ARGUMENT, INVALID_PLAN, OUT_OF_MEMORY, DEVICE_ERROR, TIMEOUT, NUMERIC, NOT_SUPPORTED = 1, 2, 3, 4, 5, 6, 7
 STATUS = {0: "ok", 1: "invalid argument", 2: "invalid plan", 3: "out of memory", 4: "device error",
           5: "timeout", 6: "numeric error", 7: "not supported"}
 

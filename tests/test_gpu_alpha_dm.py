@@ -58,3 +58,36 @@ def test_perturbed_device_sweeps_match_oracle_sweeps(ctx):
     ec = np.array([x[2] for x in cpu.log.energies])
     assert np.abs(ed - ec).max() <= 1e-9
     assert abs(ed[-1] - dense.ground_energy(model, L)) <= 1e-9
+
+
+def test_alpha_dm_rejects_bad_arguments(ctx):
+    """dmrgb200_step_alpha_dm checks its arguments before any device work: alpha < 0, an
+    H·psi plan, and a dm view with a missing block are rejected with their status."""
+    from dmrgb200 import _capi as capi
+    model, ch, psi, i = site_pair("heisenberg", L=8, m=16)
+    p12, offs = M.fuse_phys(model.phys, model.phys)
+    t, _ = G.theta_site(psi, model.phys, model.phys, offs, True)
+    W = M.MPOHandle(model.mpo[i], model.symm)
+    sch, _ = E.schedule_left_step(model.phys, t.left, t.right, W, ch.Lidx, False)
+    Lb = E.to_device(ch.Lval)
+    plan = E.DevicePlan(ctx, sch.plan, left_addr=ch.Lidx.cohort_addresses(Lb.data_ptr()))
+    ket, bra = E.to_device(t.data), E.to_device(t.left_paired())
+    dims = [int(r) for r in sch.plan["out_rows"]]
+    store = torch.zeros(sum(d * d for d in dims) + 1, dtype=torch.float64, device="cuda")
+    offs_ = np.concatenate([[0], np.cumsum([d * d for d in dims])])
+    addr = np.array([store.data_ptr() + 8 * int(o) for o in offs_[:-1]], dtype=np.uint64)
+    with pytest.raises(capi.DmrgError) as e1:
+        plan.alpha_dm(ket.data_ptr(), bra.data_ptr(), addr, -1.0)
+    assert e1.value.status == capi.INVALID_ARGUMENT
+    bad = addr.copy()
+    bad[int(np.argmax(dims))] = 0
+    with pytest.raises(capi.DmrgError) as e2:
+        plan.alpha_dm(ket.data_ptr(), bra.data_ptr(), bad, 0.5)
+    assert e2.value.status == capi.INVALID_ARGUMENT
+    hp = E.DevicePlan(ctx, ch.sched.plan, left_addr=ch.Lidx.cohort_addresses(Lb.data_ptr()),
+                      other_addr=ch.Ridx.cohort_addresses(E.to_device(ch.Rval).data_ptr()))
+    with pytest.raises(capi.DmrgError) as e3:
+        hp.alpha_dm(ket.data_ptr(), bra.data_ptr(), addr, 0.5)
+    assert e3.value.status == capi.INVALID_PLAN
+    plan.alpha_dm(ket.data_ptr(), bra.data_ptr(), addr, 0.5)  # the plan still works
+    torch.cuda.synchronize()

@@ -366,9 +366,11 @@ __global__ void __launch_bounds__(256) sbuild_lines(const DevSLine* __restrict__
 }
 
 // S build of line groups (DevSGroup): one warp per work item (a group and a
-// chunk of SG_CHUNK consecutive elements of its lines); every lane owns SG_EPT
-// elements (lane + 32 u) and keeps SG_LINES x SG_EPT accumulators, so each
-// source cell is read once for all lines of the group.  The sources stream
+// chunk of SG_CHUNK consecutive elements of its lines).  The chunk of every line is
+// one product (elements x sources) * (sources x lines) on the FP64 tensor cores
+// (DMMA m8n8k4: 8 elements x 8 lines x 4 sources per instruction, the warp holding
+// SG_CHUNK x lines accumulators), so each source cell is read once for all lines of
+// the group and one warp instruction does 256 multiply-adds.  The sources stream
 // through the warp's own shared-memory ring with bulk copies (TMA engine, no
 // multicast): a stage holds SGB_NC source rows of the chunk and their alpha
 // columns; lanes 0 .. SGB_NC - 1 each copy one row and lane SGB_NC the alphas,
@@ -379,11 +381,13 @@ __global__ void __launch_bounds__(256) sbuild_lines(const DevSLine* __restrict__
 // copied from one element earlier and read with that shift.  Every wait is
 // bounded (2 s; the thread is suspended while it waits): on a timeout the warp
 // records it in *err, lets its copies land (bounded) and stops.  Each line sums
-// its sources in the group's entry order.
+// its sources in the group's entry order, four per DMMA.  The row pitch of a stage
+// (SG_CHUNK + 4 doubles, 4 mod 16) puts the four sources of a K step in different
+// banks for the fragment loads.
 // Groups of up to 8 lines run as one launch (8 accumulated lines, 2 stages, 3 CTAs per
 // SM), larger groups as another (SG_LINES lines, 3 stages, 2 CTAs per SM, for their
 // larger register file).
-constexpr int SGB_WARPS = 4, SGB_NC = 8, SGB_ROW = SG_CHUNK + 2;
+constexpr int SGB_WARPS = 4, SGB_NC = 8, SGB_ROW = SG_CHUNK + 4;
 template <int STAGES>
 struct alignas(16) SgbRing {
     double rows[STAGES][SGB_NC][SGB_ROW];
@@ -393,7 +397,7 @@ struct alignas(16) SgbRing {
 };
 static_assert(sizeof(double) * SGB_ROW % 16 == 0 && sizeof(SgbRing<2>) % 16 == 0 && sizeof(SgbRing<3>) % 16 == 0,
               "bulk copy alignment");
-static_assert(SGB_NC < 32, "one lane per row plus one for the alphas");
+static_assert(SGB_NC < 32 && SGB_NC % 4 == 0, "one lane per row plus one for the alphas; whole DMMA K steps");
 template <int NL>
 struct SgbShape;
 template <>
@@ -421,11 +425,13 @@ __device__ __forceinline__ bool sgb_item(SgbRing<SGB_STAGES>& R, DevSGroup const
     using namespace async;
     const uint32_t n = G.rows * G.cols, cnt = min(uint32_t(SG_CHUNK), n - e0);
     const uint32_t k0 = G.ent_begin, k1 = G.ent_end;
-    double acc[NL][SG_EPT];
+    constexpr int MT = SG_CHUNK / 8, NT = NL / 8;  // m8n8k4 tiles: elements x lines
+    const uint32_t g = lane >> 2, q = lane & 3;
+    double acc[MT][NT][2];
 #pragma unroll
-    for (int j = 0; j < NL; ++j)
+    for (int i = 0; i < MT; ++i)
 #pragma unroll
-        for (int u = 0; u < SG_EPT; ++u) acc[j][u] = 0.0;
+        for (int j = 0; j < NT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
     // every lane: the stage of sources kb .. kb + SGB_NC - 1 (those below k1)
     auto fill = [&](uint32_t kb) {
         const uint32_t slot = issued % SGB_STAGES, nc = min(uint32_t(SGB_NC), k1 - kb);
@@ -456,35 +462,47 @@ __device__ __forceinline__ bool sgb_item(SgbRing<SGB_STAGES>& R, DevSGroup const
         const bool ok = mbar_wait_suspend(&R.full[slot], (consumed / SGB_STAGES) & 1u, err, wait_ns);
         if (__any_sync(0xffffffffu, !ok)) return false;
         const uint32_t nc = min(uint32_t(SGB_NC), k1 - kb);
-#pragma unroll 2
-        for (uint32_t c = 0; c < nc; ++c) {
-            const double* row = R.rows[slot][c] + R.shift[slot][c] + lane;
-            double v[SG_EPT];
+        // D (elements x lines) += T (elements x 4 sources) * alpha (4 sources x lines) per
+        // K step of four sources; sources past nc enter as zeros on both sides, and a
+        // line tile whose 4 x 8 alphas are all zero skips its DMMAs (warp-uniform)
 #pragma unroll
-            for (int u = 0; u < SG_EPT; ++u) v[u] = row[32 * u];
-            const double2* a2 = reinterpret_cast<const double2*>(R.alpha[slot][c]);
+        for (int ks = 0; ks < SGB_NC / 4; ++ks) {
+            if (uint32_t(ks * 4) >= nc) break;
+            const uint32_t c = uint32_t(ks * 4) + q;
+            const bool live = c < nc;
+            const double* row = R.rows[slot][c] + R.shift[slot][c] + g;
+            double b[NT];
+            bool nz[NT];
 #pragma unroll
-            for (int h = 0; h < NL / 2; ++h) {
-                const double2 x = a2[h];
+            for (int j = 0; j < NT; ++j) {
+                b[j] = live ? R.alpha[slot][c][j * 8 + g] : 0.0;
+                nz[j] = __any_sync(0xffffffffu, b[j] != 0.0);
+            }
 #pragma unroll
-                for (int u = 0; u < SG_EPT; ++u) {
-                    acc[2 * h][u] = fma(x.x, v[u], acc[2 * h][u]);
-                    acc[2 * h + 1][u] = fma(x.y, v[u], acc[2 * h + 1][u]);
-                }
+            for (int i = 0; i < MT; ++i) {
+                const double a = live ? row[i * 8] : 0.0;
+#pragma unroll
+                for (int j = 0; j < NT; ++j)
+                    if (nz[j]) dmma(acc[i][j][0], acc[i][j][1], a, b[j]);
             }
         }
         ++consumed;
         __syncwarp();  // every lane's reads of this slot are done before it is refilled
     }
 #pragma unroll
-    for (int u = 0; u < SG_EPT; ++u) {
-        const uint32_t e = e0 + lane + 32u * u;
+    for (int i = 0; i < MT; ++i) {
+        const uint32_t e = e0 + uint32_t(i * 8) + g;
         if (e >= n) continue;
-        const uint32_t col = e / G.rows, i = e - col * G.rows;
-        double* dst = S + G.s_base + i + uint64_t(col) * G.ld_s;
+        const uint32_t col = e / G.rows, r = e - col * G.rows;
+        double* dst = S + G.s_base + r + uint64_t(col) * G.ld_s;
 #pragma unroll
-        for (int j = 0; j < NL; ++j)
-            if (uint32_t(j) < G.nlines) dst[uint64_t(j) * G.line_stride] = ((G.mask >> j) & 1u) ? acc[j][u] : 0.0;
+        for (int j = 0; j < NT; ++j)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const uint32_t line = uint32_t(j * 8) + 2u * q + uint32_t(h);
+                if (line < G.nlines)
+                    dst[uint64_t(line) * G.line_stride] = ((G.mask >> line) & 1u) ? acc[i][j][h] : 0.0;
+            }
     }
     return true;
 }

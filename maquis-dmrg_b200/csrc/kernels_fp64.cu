@@ -384,9 +384,9 @@ __global__ void __launch_bounds__(256) sbuild_lines(const DevSLine* __restrict__
 // its sources in the group's entry order, four per DMMA.  The row pitch of a stage
 // (SG_CHUNK + 4 doubles, 4 mod 16) puts the four sources of a K step in different
 // banks for the fragment loads.
-// Groups of up to 8 lines run as one launch (8 accumulated lines, 2 stages, 3 CTAs per
-// SM), larger groups as another (SG_LINES lines, 3 stages, 2 CTAs per SM, for their
-// larger register file).
+// Groups of up to 8 lines run as one launch (8 accumulated lines), larger groups as
+// another (SG_LINES lines); both with 2 stages and 3 CTAs (12 warps) per SM, the wide
+// launch's accumulators held in 168 registers.
 constexpr int SGB_WARPS = 4, SGB_NC = 8, SGB_ROW = SG_CHUNK + 4;
 template <int STAGES>
 struct alignas(16) SgbRing {
@@ -406,7 +406,7 @@ struct SgbShape<8> {
 };
 template <>
 struct SgbShape<SG_LINES> {
-    static constexpr int STAGES = 3, MINB = 2;
+    static constexpr int STAGES = 2, MINB = 3;
 };
 template <int NL>
 constexpr size_t sgb_smem() {

@@ -23,6 +23,8 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstdlib>
+#include <cstring>
 #include <string>
 #include <vector>
 
@@ -746,6 +748,11 @@ OzProgram* oz_build(GemmList const& gl) {
                   tiles128 >= 2 * uint64_t(device_sm_count()))
                      ? 128
                      : 64;
+        // DMRGB200_OZ_BN=64 or 128 forces the width for programs built while it is set
+        if (const char* v = std::getenv("DMRGB200_OZ_BN")) {
+            if (!std::strcmp(v, "64")) oz->bn = 64;
+            if (!std::strcmp(v, "128")) oz->bn = 128;
+        }
     }
     const uint32_t OZ_BN = uint32_t(oz->bn), B_TILE = OZ_BN * OZ_BK;
     // exponent offsets: constant operands count in n_exp_c, the others in n_exp

@@ -486,6 +486,10 @@ def qc_workload(args):
     y = torch.zeros_like(x)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     res = {}
+    chosen = (C.c_int32 * 2)()
+    capi.check(capi.lib.dmrgb200_plan_autotune(sp.plan.handle, x.data_ptr(), y.data_ptr(), None, chosen), "autotune")
+    autotune = {"stage1_gemm": capi.lib.dmrgb200_gemm_variant_name(chosen[0]).decode(),
+                "stage3_gemm": capi.lib.dmrgb200_gemm_variant_name(chosen[1]).decode()}
     for name, prec in (("fp64", capi.PREC_FP64), ("emulated", capi.PREC_FP64_EMULATED)):
         try:
             for _ in range(args.warmup):
@@ -551,7 +555,7 @@ def qc_workload(args):
                        "terms": int(len(sp.schedule.plan["term_alpha"])),
                        "integral_records": n_records, "model_seconds": t_model, "setup_seconds": setup_s,
                        "l2": "flushed (256 MiB write)"},
-            "fp64": res["fp64"], "emulated": res["emulated"], "jd_solve": solve}
+            "fp64": res["fp64"], "autotune": autotune, "emulated": res["emulated"], "jd_solve": solve}
     print(json.dumps(line), flush=True)
 
 

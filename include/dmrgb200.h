@@ -230,6 +230,11 @@ dmrgb200_status dmrgb200_plan_autotune(dmrgb200_plan_t plan, const double* x, do
 const char* dmrgb200_gemm_variant_name(int variant);
 /* Number of grouped-GEMM variants (valid variant indices are 0 .. count - 1). */
 int dmrgb200_gemm_variant_count(void);
+/* Pin the grouped-GEMM variant of stage 1 and of stage 3 of an H·psi plan (each 0 ..
+ * dmrgb200_gemm_variant_count() - 1) instead of the autotuner's choice: later calls use
+ * them and do not tune the plan (dmrgb200_plan_autotune re-tunes).  The sums are the same
+ * for every variant up to the order of the K steps.  No counterpart in the reference. */
+dmrgb200_status dmrgb200_plan_set_gemm_variants(dmrgb200_plan_t plan, int32_t stage1, int32_t stage3);
 
 /* H·psi with host buffers, the counterpart of the reference's super_hamil_mv on
  * host DavidsonVectors (solver/super_hamil_mv.hpp:100-155): x_host (the plan's in

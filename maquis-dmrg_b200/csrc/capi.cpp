@@ -761,6 +761,17 @@ dmrgb200_status dmrgb200_hpsi_adjoint(dmrgb200_plan_t plan, const double* w, con
     DMRGB200_CATCH
 }
 
+// The captured graphs of a plan (the solver graph, the host-buffer H psi) launch the GEMM
+// variants chosen when they were captured: a new choice drops them (captured again on use).
+static void drop_variant_graphs(dmrgb200_plan_t plan) {
+    jd_graph_free(plan->jd);
+    plan->jd = nullptr;
+    if (plan->pipe_exec) cudaGraphExecDestroy(plan->pipe_exec);
+    plan->pipe_exec = nullptr;
+    plan->pipe_x = nullptr;
+    plan->pipe_y = nullptr;
+}
+
 dmrgb200_status dmrgb200_plan_autotune(dmrgb200_plan_t plan, const double* x, double* y, void* cuda_stream,
                                        int32_t variants[2]) {
     if (!plan || !x || !y) return fail(DMRGB200_INVALID_ARGUMENT, "null argument");
@@ -769,11 +780,24 @@ dmrgb200_status dmrgb200_plan_autotune(dmrgb200_plan_t plan, const double* x, do
     cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
     cudaError_t e = tune_program(plan->prog, reinterpret_cast<uint64_t>(x), reinterpret_cast<uint64_t>(y), plan->T,
                                  plan->S, st);
+    drop_variant_graphs(plan);
     if (e != cudaSuccess) return cuda_fail(e, "grouped GEMM autotuning");
     if (variants) {
         variants[0] = plan->prog.var1;
         variants[1] = plan->prog.var3;
     }
+    return DMRGB200_OK;
+}
+
+dmrgb200_status dmrgb200_plan_set_gemm_variants(dmrgb200_plan_t plan, int32_t stage1, int32_t stage3) {
+    if (!plan) return fail(DMRGB200_INVALID_ARGUMENT, "null plan");
+    if (stage1 < 0 || stage1 >= N_GEMM_VARIANTS || stage3 < 0 || stage3 >= N_GEMM_VARIANTS)
+        return fail(DMRGB200_INVALID_ARGUMENT, "variant index out of range");
+    if (plan->flat.kind != KIND_HPSI || !plan->compiled) return fail(DMRGB200_INVALID_PLAN, "plan is not an H psi plan");
+    plan->prog.var1 = stage1;
+    plan->prog.var3 = stage3;
+    plan->prog.tuned = true;
+    drop_variant_graphs(plan);
     return DMRGB200_OK;
 }
 

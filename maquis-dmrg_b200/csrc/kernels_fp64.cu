@@ -1405,8 +1405,9 @@ cudaError_t tune_program(DeviceProgram& prog, uint64_t in, uint64_t out, double*
     // the clocks settle on a short run of the default variant first; then every
     // variant is timed once per round, round-robin, and keeps its best round, so a
     // clock ramp or a stray slow launch favours no variant; a variant must beat the
-    // default by 3% to replace it
-    constexpr int ROUNDS = 3;
+    // default by 1.5% to replace it (at QC L=24 m=2000 the 64x64 stage-3 variants run 4%
+    // faster than the default inside H psi, which a 3% margin missed in some runs)
+    constexpr int ROUNDS = 4;
     for (auto& st : stages) {
         if (!st.n) continue;
         for (int w = 0; w < 8 && e == cudaSuccess; ++w) e = launch_variant(0, st.p, st.s, st.t, st.n, st.x, st.r, bs, stream);
@@ -1424,7 +1425,7 @@ cudaError_t tune_program(DeviceProgram& prog, uint64_t in, uint64_t out, double*
             }
         int bv = 0;
         for (int v = 1; v < N_GEMM_VARIANTS; ++v)
-            if (best_v[v] < best_v[bv] * (bv == 0 ? 0.97f : 1.0f)) bv = v;
+            if (best_v[v] < best_v[bv] * (bv == 0 ? 0.985f : 1.0f)) bv = v;
         *st.var = bv;
     }
     cudaEventDestroy(e0);

@@ -135,6 +135,7 @@ _sigs = {
     "dmrgb200_plan_autotune": ([vp, vp, vp, vp, C.POINTER(C.c_int32)], C.c_int),
     "dmrgb200_gemm_variant_name": ([C.c_int], C.c_char_p),
     "dmrgb200_gemm_variant_count": ([], C.c_int),
+    "dmrgb200_plan_set_gemm_variants": ([vp, C.c_int32, C.c_int32], C.c_int),
     "dmrgb200_plan_stage_times": ([vp, f64p, u64p, u64p], C.c_int),
     "dmrgb200_dgemm_f64": ([C.c_uint32, C.c_uint32, C.c_uint32, vp, C.c_uint64, vp, C.c_uint64, vp, C.c_uint64,
                             C.c_int, vp], C.c_int),

@@ -232,6 +232,11 @@ class DevicePlan:
     def set_slices(self, slices: int) -> None:
         capi.check(capi.lib.dmrgb200_plan_set_slices(self.handle, slices), "dmrgb200_plan_set_slices")
 
+    def set_gemm_variants(self, stage1: int, stage3: int) -> None:
+        """Pin the grouped-GEMM variants of stages 1 and 3 (dmrgb200_plan_set_gemm_variants)."""
+        capi.check(capi.lib.dmrgb200_plan_set_gemm_variants(self.handle, stage1, stage3),
+                   "dmrgb200_plan_set_gemm_variants")
+
     def tune_slices(self, x_ptr: int, target: float = 1e-10, stream: int = 0):
         """Smallest digit-plane count whose emulated H·psi of x is within `target` (relative)
         of the FP64 one (dmrgb200_plan_tune_slices); returns (slices, relative error)."""

@@ -33,3 +33,37 @@ def test_dgemm_f64_matches_torch(variant, M, N, K, pad):
     # the padding rows of C are not written
     if pad:
         assert torch.isnan(Cm.view(N, ldc)[:, M:]).all()
+
+
+def test_pinned_plan_variants_match_oracle():
+    """dmrgb200_plan_set_gemm_variants: every variant pinned on both stages of an H·psi plan
+    gives the oracle's H·psi (FP64, 1e-12), on the device and through the host-buffer graph
+    (which is captured again after a new choice); an index out of range is rejected."""
+    import numpy as np
+
+    from dmrgb200 import engine as E
+    from helpers import OracleChain, make_chain, random_psi
+
+    model, bonds, tensors, rng = make_chain("qc", 8, 0, seed=5, synthetic_m=64)
+    ch = OracleChain(model, bonds, tensors, 3)
+    x = random_psi(ch.p12, ch.left, ch.right, rng).data
+    want = ch.hpsi(x)
+    ctx = E.Context(0)
+    Lb, Rb = E.to_device(ch.Lval), E.to_device(ch.Rval)
+    plan = E.DevicePlan(ctx, ch.sched.plan, left_addr=ch.Lidx.cohort_addresses(Lb.data_ptr()),
+                        other_addr=ch.Ridx.cohort_addresses(Rb.data_ptr()))
+    xd = E.to_device(x)
+    xh = torch.tensor(x, dtype=torch.float64).pin_memory()
+    yh = torch.zeros(len(want), dtype=torch.float64).pin_memory()
+    n = capi.lib.dmrgb200_gemm_variant_count()
+    for v in range(n):
+        plan.set_gemm_variants(v, (v + 3) % n)
+        yd = torch.zeros_like(xd)
+        plan.hpsi(xd.data_ptr(), yd.data_ptr())
+        plan.hpsi_host(xh.data_ptr(), yh.data_ptr())
+        torch.cuda.synchronize()
+        for got in (yd.cpu().numpy(), yh.numpy()):
+            assert np.linalg.norm(got - want) <= 1e-12 * np.linalg.norm(want), v
+    with pytest.raises(capi.DmrgError) as e:
+        plan.set_gemm_variants(n, 0)
+    assert e.value.status == capi.INVALID_ARGUMENT

@@ -48,64 +48,65 @@ __global__ void __launch_bounds__(256) alpha_grad(const DevATerm* __restrict__ a
     }
 }
 
-// gT: one block per T block; every element is the alpha-weighted sum of its
-// G sources in plan term order (a block without sources becomes zero)
+// gT of the T blocks outside cell groups: one warp per 128 elements of a block (a
+// block without sources becomes zero).  Each lane owns four elements (lane + 32 u) and
+// sums the block's terms in plan term order; the terms (alpha, G cell, leading dimension)
+// are read 32 at a time, one per lane, and handed round by shuffles, so a lane keeps four
+// independent G loads in flight per term and no block barrier is needed.
 __global__ void __launch_bounds__(256) tgrad_cells(const DevSLine* __restrict__ lines,
-                                                   const DevGTerm* __restrict__ terms, uint32_t n_lines,
+                                                   const DevGTerm* __restrict__ terms,
+                                                   const DevSItem* __restrict__ items, uint32_t n_items,
                                                    double* __restrict__ gT, const double* __restrict__ G) {
-    for (uint32_t li = blockIdx.x; li < n_lines; li += gridDim.x) {
-        const DevSLine L = lines[li];
-        if (!L.rows) continue;
-        // column-major walk in steps of blockDim.x without per-element division
-        const uint32_t di = blockDim.x % L.rows, dc = blockDim.x / L.rows;
-        uint32_t i = threadIdx.x % L.rows, c = threadIdx.x / L.rows;
-        while (c < L.cols) {
-            double v = 0.0;
-            for (uint32_t t = L.term_begin; t < L.term_end; ++t) {
-                const DevGTerm tm = terms[t];
-                v += tm.alpha * G[tm.g_base + i + uint64_t(c) * tm.ld];
-            }
-            gT[L.s_base + i + uint64_t(c) * L.ld_s] = v;
-            i += di;
-            c += dc;
-            if (i >= L.rows) {
-                i -= L.rows;
-                ++c;
+    const uint32_t lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    for (uint32_t it = blockIdx.x * wpb + (threadIdx.x >> 5); it < n_items; it += gridDim.x * wpb) {
+        const DevSItem I = items[it];
+        const DevSLine L = lines[I.group];
+        const uint32_t n = L.rows * L.cols;
+        uint32_t ri[SG_EPT], ci[SG_EPT];
+        bool in[SG_EPT];
+        double v[SG_EPT];
+#pragma unroll
+        for (int u = 0; u < SG_EPT; ++u) {
+            const uint32_t e = I.e0 + lane + 32u * u;
+            in[u] = e < n;
+            ci[u] = in[u] ? e / L.rows : 0;
+            ri[u] = in[u] ? e - ci[u] * L.rows : 0;
+            v[u] = 0.0;
+        }
+        for (uint32_t t0 = L.term_begin; t0 < L.term_end; t0 += 32) {
+            const uint32_t nt = min(32u, L.term_end - t0);
+            DevGTerm my{0.0, 0, 0, 0};
+            if (lane < nt) my = terms[t0 + lane];
+            for (uint32_t t = 0; t < nt; ++t) {
+                const double a = __shfl_sync(0xffffffffu, my.alpha, t);
+                const uint64_t gb = __shfl_sync(0xffffffffu, my.g_base, t);
+                const uint32_t ld = __shfl_sync(0xffffffffu, my.ld, t);
+#pragma unroll
+                for (int u = 0; u < SG_EPT; ++u)
+                    if (in[u]) v[u] += a * G[gb + ri[u] + uint64_t(ci[u]) * ld];
             }
         }
+#pragma unroll
+        for (int u = 0; u < SG_EPT; ++u)
+            if (in[u]) gT[L.s_base + ri[u] + uint64_t(ci[u]) * L.ld_s] = v[u];
     }
 }
 
 // galpha of the terms of grouped units (DevSGroup, built for the forward S build):
 // gram[entry * SG_LINES + j] = <G line j of the group, T source of the entry>, one
-// warp per (group, batch of AG_BATCH entries).  Per 128-element chunk every lane holds
-// the group's 16 lines' G values of its 4 elements; per entry it forms 16 partial
-// products, which a reduce-scatter butterfly (16 shuffles) sums over the warp so that
-// lanes 2j, 2j+1 end with line j's total; the chunks add up in order, so the result is
-// bitwise reproducible.  A term's galpha is then its (entry, line) slot.
+// warp per (group, batch of AG_BATCH entries).  The Gram block of the batch, 16 lines x
+// 16 entries, is a product (lines x elements) * (elements x entries) on the FP64 tensor
+// cores: DMMA m8n8k4 over 8 lines x 8 entries per tile, four elements per K step, each
+// lane loading its line's and its entry's element (lane & 3) of the step from global
+// memory (8 rows x 32 bytes per warp load).  Two accumulator sets take alternate K steps
+// and are added at the end, in a fixed order, so the result is bitwise reproducible.  A
+// term's galpha is then its (entry, line) slot.
 constexpr int AG_BATCH = 16;
-static_assert(SG_LINES == 16, "the butterfly below scatters 16 lines over the warp");
-__device__ __forceinline__ double sum16_scatter(double const (&p)[SG_LINES], uint32_t lane) {
-    const bool h1 = (lane >> 4) & 1u, h2 = (lane >> 3) & 1u, h3 = (lane >> 2) & 1u, h4 = (lane >> 1) & 1u;
-    double q[8], r[4], t[2];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        const double send = h1 ? p[k] : p[8 + k];
-        q[k] = (h1 ? p[8 + k] : p[k]) + __shfl_xor_sync(0xffffffffu, send, 16);
-    }
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const double send = h2 ? q[k] : q[4 + k];
-        r[k] = (h2 ? q[4 + k] : q[k]) + __shfl_xor_sync(0xffffffffu, send, 8);
-    }
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-        const double send = h3 ? r[k] : r[2 + k];
-        t[k] = (h3 ? r[2 + k] : r[k]) + __shfl_xor_sync(0xffffffffu, send, 4);
-    }
-    double v = (h4 ? t[1] : t[0]) + __shfl_xor_sync(0xffffffffu, h4 ? t[0] : t[1], 2);
-    v += __shfl_xor_sync(0xffffffffu, v, 1);
-    return v;  // the line (lane >> 1) & 15
+static_assert(SG_LINES == 16 && AG_BATCH == 16, "2 x 2 DMMA tiles of 8 lines x 8 entries");
+__device__ __forceinline__ void gram_dmma(double& c0, double& c1, double a, double b) {
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+        : "+d"(c0), "+d"(c1)
+        : "d"(a), "d"(b));
 }
 
 __global__ void __launch_bounds__(128) gram_groups(const DevSGroup* __restrict__ groups,
@@ -113,105 +114,132 @@ __global__ void __launch_bounds__(128) gram_groups(const DevSGroup* __restrict__
                                                    const uint64_t* __restrict__ ent_t, const double* __restrict__ G,
                                                    const double* __restrict__ T, double* __restrict__ gram) {
     const uint32_t lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    const uint32_t g = lane >> 2, q = lane & 3;
     for (uint32_t it = blockIdx.x * wpb + (threadIdx.x >> 5); it < n_items; it += gridDim.x * wpb) {
         const DevSItem I = items[it];
         const DevSGroup Gr = groups[I.group];
         const uint32_t n = Gr.rows * Gr.cols, nb = min(uint32_t(AG_BATCH), Gr.ent_end - I.e0);
-        const uint64_t my_tb = lane < nb ? ent_t[I.e0 + lane] : 0;
-        double acc[AG_BATCH];
+        // this lane's rows of the A (lines g, 8 + g) and B (entries g, 8 + g) fragments
+        const bool l0 = g < Gr.nlines, l1 = 8 + g < Gr.nlines, b0 = g < nb, b1 = 8 + g < nb;
+        const double* G0 = G + Gr.s_base + uint64_t(g) * Gr.line_stride;
+        const double* G1 = G0 + 8ull * Gr.line_stride;
+        const double* T0 = T + (b0 ? ent_t[I.e0 + g] : 0);
+        const double* T1 = T + (b1 ? ent_t[I.e0 + 8 + g] : 0);
+        double acc[2][2][2][2];  // [set][line tile][entry tile][pair]
 #pragma unroll
-        for (int b = 0; b < AG_BATCH; ++b) acc[b] = 0.0;
-        for (uint32_t c0 = 0; c0 < n; c0 += 32 * SG_EPT) {
-            double g[SG_LINES][SG_EPT];
-            uint32_t el[SG_EPT];
-            bool in[SG_EPT];
+        for (int s = 0; s < 2; ++s)
 #pragma unroll
-            for (int u = 0; u < SG_EPT; ++u) {
-                el[u] = c0 + lane + 32u * u;
-                in[u] = el[u] < n;
-                const uint32_t col = in[u] ? el[u] / Gr.rows : 0, i = in[u] ? el[u] - col * Gr.rows : 0;
-                const double* src = G + Gr.s_base + i + uint64_t(col) * Gr.ld_s;
+            for (int i = 0; i < 2; ++i)
 #pragma unroll
-                for (int j = 0; j < SG_LINES; ++j)
-                    g[j][u] = (in[u] && uint32_t(j) < Gr.nlines) ? src[uint64_t(j) * Gr.line_stride] : 0.0;
-            }
+                for (int j = 0; j < 2; ++j) acc[s][i][j][0] = acc[s][i][j][1] = 0.0;
+        // element e = 4 step + q of the lane, at (row r, column c) of the lines' cells
+        uint32_t e = q, c = q / max(Gr.rows, 1u), r = q - c * Gr.rows;
+        const uint32_t dc = 4u / max(Gr.rows, 1u), dr = 4u - dc * Gr.rows;
+        for (uint32_t st = 0; st * 4 < n; st += 2) {
 #pragma unroll
-            for (int b = 0; b < AG_BATCH; ++b) {
-                if (uint32_t(b) >= nb) break;
-                const uint64_t tb = __shfl_sync(0xffffffffu, my_tb, b);
-                double t[SG_EPT];
-#pragma unroll
-                for (int u = 0; u < SG_EPT; ++u) t[u] = in[u] ? T[tb + el[u]] : 0.0;
-                double p[SG_LINES];
-#pragma unroll
-                for (int j = 0; j < SG_LINES; ++j) {
-                    double a = 0.0;
-#pragma unroll
-                    for (int u = 0; u < SG_EPT; ++u) a = fma(g[j][u], t[u], a);
-                    p[j] = a;
+            for (int s = 0; s < 2; ++s) {
+                const bool in = e < n;
+                const uint64_t go = r + uint64_t(c) * Gr.ld_s;
+                const double a0 = (in && l0) ? G0[go] : 0.0, a1 = (in && l1) ? G1[go] : 0.0;
+                const double t0 = (in && b0) ? T0[e] : 0.0, t1 = (in && b1) ? T1[e] : 0.0;
+                gram_dmma(acc[s][0][0][0], acc[s][0][0][1], a0, t0);
+                gram_dmma(acc[s][0][1][0], acc[s][0][1][1], a0, t1);
+                gram_dmma(acc[s][1][0][0], acc[s][1][0][1], a1, t0);
+                gram_dmma(acc[s][1][1][0], acc[s][1][1][1], a1, t1);
+                e += 4;
+                r += dr;
+                c += dc;
+                if (r >= Gr.rows) {
+                    r -= Gr.rows;
+                    ++c;
                 }
-                acc[b] += sum16_scatter(p, lane);
             }
         }
+        // D tile (line tile i, entry tile j): line 8 i + g, entries 8 j + 2 q + h
 #pragma unroll
-        for (int b = 0; b < AG_BATCH; ++b)
-            if (uint32_t(b) < nb && (lane & 1u) == 0) gram[uint64_t(I.e0 + b) * SG_LINES + (lane >> 1)] = acc[b];
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < 2; ++j)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const uint32_t ent = uint32_t(8 * j) + 2u * q + uint32_t(h);
+                    if (ent < nb)
+                        gram[uint64_t(I.e0 + ent) * SG_LINES + uint32_t(8 * i) + g] = acc[0][i][j][h] + acc[1][i][j][h];
+                }
     }
 }
 
 // gT of T blocks taken as cell groups (DevTGroup): one warp per 128 elements of a
-// group; each lane keeps TG_CELLS x SG_EPT accumulators (one per cell) and reads
-// every G line of the group once for all its cells; cells sum their lines in the
-// group's entry order.
+// group.  The chunk of every cell is one product (elements x G lines) * (G lines x
+// cells) on the FP64 tensor cores (DMMA m8n8k4: 8 elements x 8 cells x 4 lines per
+// instruction; the chunk in two passes of 8 element tiles), so every G line of the group
+// is read once per pass for all its cells; the lines enter four per K step in the group's
+// entry order (lines past the end as zeros).
 __global__ void __launch_bounds__(256) tgrad_groups(const DevTGroup* __restrict__ groups,
                                                     const DevSItem* __restrict__ items, uint32_t n_items,
                                                     const uint64_t* __restrict__ ent_g,
                                                     const uint32_t* __restrict__ ent_ld,
                                                     const double* __restrict__ ent_a, const double* __restrict__ G,
                                                     double* __restrict__ gT) {
+    static_assert(TG_CELLS == 8, "one DMMA tile of cells");
+    constexpr int MT = 8;  // element tiles per pass: a 128-element chunk in two passes of 64
     const uint32_t lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    const uint32_t g = lane >> 2, q = lane & 3;
     for (uint32_t it = blockIdx.x * wpb + (threadIdx.x >> 5); it < n_items; it += gridDim.x * wpb) {
         const DevSItem I = items[it];
         const DevTGroup Gr = groups[I.group];
         const uint32_t n = Gr.rows * Gr.cols;
-        uint32_t el[SG_EPT], ri[SG_EPT], ci[SG_EPT];
-        bool in[SG_EPT];
+        for (uint32_t half = 0; half < 32u * SG_EPT; half += 8u * MT) {
+            const uint32_t eb = I.e0 + half;
+            if (eb >= n) break;
+            // this lane's elements eb + 8 i + g: row and column in the G lines' cells
+            uint32_t ri[MT], ci[MT];
 #pragma unroll
-        for (int u = 0; u < SG_EPT; ++u) {
-            el[u] = I.e0 + lane + 32u * u;
-            in[u] = el[u] < n;
-            ci[u] = in[u] ? el[u] / Gr.rows : 0;
-            ri[u] = in[u] ? el[u] - ci[u] * Gr.rows : 0;
-        }
-        double acc[TG_CELLS][SG_EPT];
+            for (int i = 0; i < MT; ++i) {
+                const uint32_t e = eb + uint32_t(8 * i) + g;
+                ci[i] = e < n ? e / Gr.rows : 0xffffffffu;  // beyond the block: no load
+                ri[i] = e < n ? e - ci[i] * Gr.rows : 0;
+            }
+            double acc[MT][2];
 #pragma unroll
-        for (int j = 0; j < TG_CELLS; ++j)
+            for (int i = 0; i < MT; ++i) acc[i][0] = acc[i][1] = 0.0;
+            // the line of K step k0 + 4 (its address, leading dimension and alpha) is read
+            // while step k0 multiplies, so the two dependent loads of a step overlap the last
+            auto line = [&](uint32_t k0, const double*& gk, uint64_t& ld, double& b) {
+                const uint32_t k = k0 + q;
+                const bool live = k < Gr.ent_end;
+                gk = live ? G + ent_g[k] : nullptr;
+                ld = live ? ent_ld[k] : 0;
+                b = live ? ent_a[uint64_t(k) * TG_CELLS + g] : 0.0;
+            };
+            const double* gk;
+            uint64_t ld;
+            double b;
+            line(Gr.ent_begin, gk, ld, b);
+            for (uint32_t k0 = Gr.ent_begin; k0 < Gr.ent_end; k0 += 4) {
+                double a[MT];
 #pragma unroll
-            for (int u = 0; u < SG_EPT; ++u) acc[j][u] = 0.0;
-        for (uint32_t k = Gr.ent_begin; k < Gr.ent_end; ++k) {
-            const double* g = G + ent_g[k];
-            const uint64_t ld = ent_ld[k];
-            double v[SG_EPT];
+                for (int i = 0; i < MT; ++i) a[i] = (gk && ci[i] != 0xffffffffu) ? gk[ri[i] + ci[i] * ld] : 0.0;
+                const double bk = b;
+                line(k0 + 4, gk, ld, b);
 #pragma unroll
-            for (int u = 0; u < SG_EPT; ++u) v[u] = in[u] ? g[ri[u] + ci[u] * ld] : 0.0;
-            const double2* a2 = reinterpret_cast<const double2*>(ent_a + uint64_t(k) * TG_CELLS);
+                for (int i = 0; i < MT; ++i)
+                    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                        : "+d"(acc[i][0]), "+d"(acc[i][1])
+                        : "d"(a[i]), "d"(bk));
+            }
+            // D tile i: element eb + 8 i + g, cells 2 q + h
 #pragma unroll
-            for (int h = 0; h < TG_CELLS / 2; ++h) {
-                const double2 x = a2[h];
+            for (int i = 0; i < MT; ++i) {
+                const uint32_t e = eb + uint32_t(8 * i) + g;
+                if (e >= n) continue;
 #pragma unroll
-                for (int u = 0; u < SG_EPT; ++u) {
-                    acc[2 * h][u] = fma(x.x, v[u], acc[2 * h][u]);
-                    acc[2 * h + 1][u] = fma(x.y, v[u], acc[2 * h + 1][u]);
+                for (int h = 0; h < 2; ++h) {
+                    const uint32_t c = 2u * q + uint32_t(h);
+                    if (c < Gr.ncells)
+                        gT[Gr.out_base + uint64_t(c) * n + e] = ((Gr.mask >> c) & 1u) ? acc[i][h] : 0.0;
                 }
             }
-        }
-#pragma unroll
-        for (int u = 0; u < SG_EPT; ++u) {
-            if (!in[u]) continue;
-#pragma unroll
-            for (int c = 0; c < TG_CELLS; ++c)
-                if (uint32_t(c) < Gr.ncells)
-                    gT[Gr.out_base + uint64_t(c) * n + el[u]] = ((Gr.mask >> c) & 1u) ? acc[c][u] : 0.0;
         }
     }
 }
@@ -359,7 +387,11 @@ std::string compile_adjoint(FlatPlan const& p, std::vector<uint64_t> const& stag
                 a.gterms.push_back(DevGTerm{p.term_alpha[at.k], at.g_base, at.ld_g, 0});
             }
             L.term_end = uint32_t(a.gterms.size());
-            if (uint64_t(M) * N) a.tlines.push_back(L);
+            if (uint64_t(M) * N) {
+                for (uint64_t e0 = 0; e0 < uint64_t(M) * N; e0 += 32 * SG_EPT)
+                    a.tl_items.push_back(DevSItem{uint32_t(a.tlines.size()), uint32_t(e0)});
+                a.tlines.push_back(L);
+            }
         }
     }
 
@@ -441,6 +473,8 @@ cudaError_t upload_adjoint(AdjointProgram& a) {
     a.n_gram_terms = uint32_t(a.gram_k.size());
     if ((e = up(a.tlines, &a.d_tlines)) != cudaSuccess) return e;
     if ((e = up(a.gterms, &a.d_gterms)) != cudaSuccess) return e;
+    if ((e = up(a.tl_items, &a.d_tl_items)) != cudaSuccess) return e;
+    a.n_tl_items = uint32_t(a.tl_items.size());
     a.n_aterms = uint32_t(a.aterms_walk.size());
     a.n_tlines = uint32_t(a.tlines.size());
     return cudaSuccess;
@@ -452,6 +486,8 @@ void free_adjoint(AdjointProgram& a) {
     cudaFree(a.d_aterms);
     cudaFree(a.d_tlines);
     cudaFree(a.d_gterms);
+    cudaFree(a.d_tl_items);
+    a.d_tl_items = nullptr;
     cudaFree(a.d_gram_items);
     cudaFree(a.d_tgroups);
     cudaFree(a.d_tg_items);
@@ -516,9 +552,9 @@ cudaError_t run_adjoint(DeviceProgram const& fwd, AdjointProgram const& a, uint6
         }
     }
     if (gx) {
-        if (a.n_tlines) {
-            uint32_t grid = std::min<uint32_t>(a.n_tlines, sms * 8);
-            tgrad_cells<<<grid, 256, 0, stream>>>(a.d_tlines, a.d_gterms, a.n_tlines, T, S);
+        if (a.n_tl_items) {
+            uint32_t grid = std::min<uint32_t>((a.n_tl_items + 7) / 8, sms * 8);
+            tgrad_cells<<<grid, 256, 0, stream>>>(a.d_tlines, a.d_gterms, a.d_tl_items, a.n_tl_items, T, S);
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
         }
         if (a.n_tg_items) {

@@ -284,6 +284,7 @@ struct AdjointProgram {
     std::vector<DevATerm> aterms_walk;  // the terms of ungrouped units (galpha term by term)
     std::vector<DevSLine> tlines;       // one per T block: gT cell = sum of its sources
     std::vector<DevGTerm> gterms;
+    std::vector<DevSItem> tl_items;     // warp items of the T blocks: (block, 128-element chunk)
     // galpha of grouped units: Gram blocks per (group, entry batch), then one slot per term
     std::vector<DevSItem> gram_items;
     std::vector<uint32_t> gram_k, gram_slot;
@@ -299,6 +300,7 @@ struct AdjointProgram {
     DevATerm* d_aterms = nullptr;
     DevSLine* d_tlines = nullptr;
     DevGTerm* d_gterms = nullptr;
+    DevSItem* d_tl_items = nullptr;
     DevSItem* d_gram_items = nullptr;
     uint32_t* d_gram_k = nullptr;
     uint32_t* d_gram_slot = nullptr;
@@ -308,7 +310,7 @@ struct AdjointProgram {
     uint64_t* d_tg_g = nullptr;
     uint32_t* d_tg_ld = nullptr;
     double* d_tg_a = nullptr;
-    uint32_t n_aterms = 0, n_tlines = 0, n_gram_items = 0, n_gram_terms = 0, n_tg_items = 0;
+    uint32_t n_aterms = 0, n_tlines = 0, n_tl_items = 0, n_gram_items = 0, n_gram_terms = 0, n_tg_items = 0;
 };
 // Lower the adjoint of an H psi plan; returns an empty string, or why the plan
 // has none (overlapping T slices, a term that is not one whole T block).

@@ -266,10 +266,21 @@ __device__ __forceinline__ uint64_t oz_fixed(double x, int ex, uint32_t& neg) {
     if (sh >= 0) return sh < 64 ? (m << sh) : 0ull;
     return sh > -64 ? (m >> -sh) : 0ull;
 }
-// digit p of a fixed-point value as a byte (two's complement)
-__device__ __forceinline__ uint32_t oz_digit(uint64_t X, uint32_t neg, int p) {
-    const uint32_t d = uint32_t(X >> (49 - 7 * p)) & 127u;
-    return (neg ? 0u - d : d) & 255u;
+// 0xFF in byte j of the word of four elements where element j is negative
+__device__ __forceinline__ uint32_t oz_sign_bytes(uint32_t const* neg) {
+    return ((0u - neg[0]) & 0xFFu) | (((0u - neg[1]) & 0xFFu) << 8) | (((0u - neg[2]) & 0xFFu) << 16) |
+           ((0u - neg[3]) << 24);
+}
+// digit p of four fixed-point values as one word of bytes (two's complement): the four
+// 7-bit magnitudes packed by byte permutes, then negated per byte where the sign byte is
+// 0xFF ((d ^ 0xFF) - 0xFF = -d mod 256, no borrow between bytes).  p is a constant in the
+// unrolled plane loops, so the shifts are immediate.
+__device__ __forceinline__ uint32_t oz_digits4(uint64_t const* X, uint32_t sign, int p) {
+    const int sh = 49 - 7 * p;
+    const uint32_t d0 = uint32_t(X[0] >> sh) & 127u, d1 = uint32_t(X[1] >> sh) & 127u;
+    const uint32_t d2 = uint32_t(X[2] >> sh) & 127u, d3 = uint32_t(X[3] >> sh) & 127u;
+    const uint32_t w = __byte_perm(__byte_perm(d0, d1, 0x0040), __byte_perm(d2, d3, 0x0040), 0x5410);
+    return __vsub4(w ^ sign, sign);
 }
 
 // Digit planes of every job: the s signed 7-bit digits of every element scaled by its
@@ -306,13 +317,15 @@ __global__ void __launch_bounds__(256) oz_split(const OzSplit* __restrict__ jobs
 #pragma unroll
             for (int u = 0; u < 16; ++u) X[u] = oz_fixed((live && k0 + u < job.K) ? row[k0 + u] : 0.0, ex, neg[u]);
             const uint64_t off = (job.out_base + (uint64_t(r / TR) * job.KS + ks) * tile_bytes) * s + tile_off(r % TR, kk);
-            for (int p = 0; p < s; ++p) {
+            uint32_t sign[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) sign[q] = oz_sign_bytes(neg + 4 * q);
+#pragma unroll
+            for (int p = 0; p < OZ_MAX_SLICES; ++p) {
+                if (p >= s) break;
                 uint32_t w[4];
 #pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    w[q] = oz_digit(X[4 * q], neg[4 * q], p) | (oz_digit(X[4 * q + 1], neg[4 * q + 1], p) << 8) |
-                           (oz_digit(X[4 * q + 2], neg[4 * q + 2], p) << 16) |
-                           (oz_digit(X[4 * q + 3], neg[4 * q + 3], p) << 24);
+                for (int q = 0; q < 4; ++q) w[q] = oz_digits4(X + 4 * q, sign[q], p);
                 *reinterpret_cast<uint4*>(out + off + p * tile_bytes) = make_uint4(w[0], w[1], w[2], w[3]);
             }
         } else {
@@ -342,13 +355,15 @@ __global__ void __launch_bounds__(256) oz_split(const OzSplit* __restrict__ jobs
                 X[u] = oz_fixed((live && k0 + u < job.K) ? row[uint64_t(k0 + u) * sk] : 0.0, ex, neg[u]);
             const uint64_t off = (job.out_base + (uint64_t(r / TR) * job.KS + k0 / OZ_BK) * tile_bytes) * s +
                                  tile_off(r % TR, k0 % OZ_BK);
-            for (int p = 0; p < s; ++p) {
+            uint32_t sign[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) sign[q] = oz_sign_bytes(neg + 4 * q);
+#pragma unroll
+            for (int p = 0; p < OZ_MAX_SLICES; ++p) {
+                if (p >= s) break;
                 uint32_t w[4];
 #pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    w[q] = oz_digit(X[4 * q], neg[4 * q], p) | (oz_digit(X[4 * q + 1], neg[4 * q + 1], p) << 8) |
-                           (oz_digit(X[4 * q + 2], neg[4 * q + 2], p) << 16) |
-                           (oz_digit(X[4 * q + 3], neg[4 * q + 3], p) << 24);
+                for (int q = 0; q < 4; ++q) w[q] = oz_digits4(X + 4 * q, sign[q], p);
                 *reinterpret_cast<uint4*>(out + off + p * tile_bytes) = make_uint4(w[0], w[1], w[2], w[3]);
             }
         }

@@ -774,10 +774,13 @@ uint64_t group_unit(FlatPlan const& p, uint32_t c, uint32_t u, std::vector<int64
         }
         // the kernel accumulates 8 lines for groups of up to 8, SG_LINES otherwise
         fmas += uint64_t(G.ent_end - G.ent_begin) * (G.nlines <= 8 ? 8u : uint32_t(SG_LINES));
-        // the kernel walks sources SG_UNROLL at a time: pad with zero-alpha sources at T
-        // offset 0 (their reads stay inside T: an element index is below the cell size)
+        // the kernel walks sources SG_UNROLL at a time: pad with zero-alpha copies of the
+        // group's first source.  A padded source is multiplied by zero, so it must read
+        // written T elements: T blocks are padded to 32 elements and stage 1 never writes
+        // the gaps, which may hold non-finite leftovers (0 * NaN = NaN in every line)
         while ((out.ent_t.size() - G.ent_begin) % SG_UNROLL) {
-            out.ent_t.push_back(0);
+            const uint64_t first = out.ent_t[G.ent_begin];
+            out.ent_t.push_back(first);
             out.ent_a.insert(out.ent_a.end(), SG_LINES, 0.0);
         }
         G.ent_end = uint32_t(out.ent_t.size());

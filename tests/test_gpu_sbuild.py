@@ -92,3 +92,21 @@ def test_boundary_steps_each_sbuild_form(ctx, monkeypatch, mode):
         nidx2, Rbuf = E.device_right_step(ctx, model.phys, bonds[p], bonds[p + 1], W, Ridx, Rbuf, td, td, True)
         assert _rel(Rbuf.cpu().numpy()[:nidx.n_elems], ref) <= TOL, p
         Ridx, Rval = nidx2, ref
+
+
+def test_grouped_sbuild_reads_no_unwritten_scratch(ctx, monkeypatch):
+    """T blocks are padded to 32 elements and stage 1 never writes the gaps; the grouped S
+    build (its zero-alpha padding sources included) must not read them.  Device memory is
+    filled with NaN and handed back to the driver before the plan allocates its scratch, so
+    gaps that were read would turn whole lines into NaN."""
+    monkeypatch.setenv("DMRGB200_SBUILD", "groups")
+    model, bonds, tensors, rng = make_chain("qc", 8, 0, seed=6, synthetic_m=64)
+    ch = OracleChain(model, bonds, tensors, 3)
+    x = random_psi(ch.p12, ch.left, ch.right, rng).data
+    poison = torch.full((64 * 1024 * 1024,), float("nan"), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    del poison
+    torch.cuda.empty_cache()
+    y1, y2 = _hpsi(ctx, ch, x, reps=2)
+    assert np.isfinite(y1).all() and _rel(y1, ch.hpsi(x)) <= TOL
+    assert np.array_equal(y1, y2)

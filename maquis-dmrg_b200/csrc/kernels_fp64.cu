@@ -463,27 +463,26 @@ __device__ __forceinline__ bool sgb_item(SgbRing<SGB_STAGES>& R, DevSGroup const
         if (__any_sync(0xffffffffu, !ok)) return false;
         const uint32_t nc = min(uint32_t(SGB_NC), k1 - kb);
         // D (elements x lines) += T (elements x 4 sources) * alpha (4 sources x lines) per
-        // K step of four sources; sources past nc enter as zeros on both sides, and a
-        // line tile whose 4 x 8 alphas are all zero skips its DMMAs (warp-uniform)
+        // K step of four sources (a group's sources are padded to a multiple of four, so a
+        // stage holds one or two whole steps); the alphas of both steps are read first
+        double b[SGB_NC / 4][NT];
+#pragma unroll
+        for (int ks = 0; ks < SGB_NC / 4; ++ks) {
+            const uint32_t c = uint32_t(ks * 4) + q;
+#pragma unroll
+            for (int j = 0; j < NT; ++j) b[ks][j] = c < nc ? R.alpha[slot][c][j * 8 + g] : 0.0;
+        }
 #pragma unroll
         for (int ks = 0; ks < SGB_NC / 4; ++ks) {
             if (uint32_t(ks * 4) >= nc) break;
             const uint32_t c = uint32_t(ks * 4) + q;
             const bool live = c < nc;
             const double* row = R.rows[slot][c] + R.shift[slot][c] + g;
-            double b[NT];
-            bool nz[NT];
-#pragma unroll
-            for (int j = 0; j < NT; ++j) {
-                b[j] = live ? R.alpha[slot][c][j * 8 + g] : 0.0;
-                nz[j] = __any_sync(0xffffffffu, b[j] != 0.0);
-            }
 #pragma unroll
             for (int i = 0; i < MT; ++i) {
                 const double a = live ? row[i * 8] : 0.0;
 #pragma unroll
-                for (int j = 0; j < NT; ++j)
-                    if (nz[j]) dmma(acc[i][j][0], acc[i][j][1], a, b[j]);
+                for (int j = 0; j < NT; ++j) dmma(acc[i][j][0], acc[i][j][1], a, b[ks][j]);
             }
         }
         ++consumed;

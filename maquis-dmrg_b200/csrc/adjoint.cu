@@ -333,8 +333,9 @@ std::string compile_adjoint(FlatPlan const& p, std::vector<uint64_t> const& stag
     for (uint32_t t = 0; t < nt; ++t) {
         const uint32_t M = p.in_rows[p.t_lb[t]], N = p.t_bcols[t];
         // up to 8 consecutive blocks of the task as one cell group over the union of
-        // their G lines, where that issues at most twice the term walk's multiply-adds
-        // (and the blocks average 4 or more terms); the other blocks keep the walk
+        // their G lines, where that issues at most four times the term walk's
+        // multiply-adds (on the tensor cores they cost far less than the walk's) and the
+        // blocks average 4 or more terms; the other blocks keep the walk
         std::vector<char> grouped_b(p.t_nb[t], 0);
         if (uint64_t(M) * N)
             for (uint32_t b0 = 0; b0 < p.t_nb[t]; b0 += TG_CELLS) {
@@ -346,7 +347,7 @@ std::string compile_adjoint(FlatPlan const& p, std::vector<uint64_t> const& stag
                 for (uint32_t c = 0; c < ncell; ++c)
                     for (uint32_t i : block_terms[tb_base[t] + b0 + c])
                         slot.emplace(std::make_pair(a.aterms[i].g_base, a.aterms[i].ld_g), 0u);
-                if (uint64_t(slot.size()) * TG_CELLS > 2 * nterms) continue;
+                if (uint64_t(slot.size()) * TG_CELLS > 4 * nterms) continue;
                 DevTGroup G{};
                 G.out_base = t_off[t] + uint64_t(b0) * M * N;
                 G.rows = M;

@@ -95,18 +95,80 @@ __global__ void __launch_bounds__(256) tgrad_cells(const DevSLine* __restrict__ 
 // galpha of the terms of grouped units (DevSGroup, built for the forward S build):
 // gram[entry * SG_LINES + j] = <G line j of the group, T source of the entry>, one
 // warp per (group, batch of AG_BATCH entries).  The Gram block of the batch, 16 lines x
-// 16 entries, is a product (lines x elements) * (elements x entries) on the FP64 tensor
+// 32 entries, is a product (lines x elements) * (elements x entries) on the FP64 tensor
 // cores: DMMA m8n8k4 over 8 lines x 8 entries per tile, four elements per K step, each
-// lane loading its line's and its entry's element (lane & 3) of the step from global
-// memory (8 rows x 32 bytes per warp load).  Two accumulator sets take alternate K steps
-// and are added at the end, in a fixed order, so the result is bitwise reproducible.  A
-// term's galpha is then its (entry, line) slot.
-constexpr int AG_BATCH = 16;
-static_assert(SG_LINES == 16 && AG_BATCH == 16, "2 x 2 DMMA tiles of 8 lines x 8 entries");
+// lane loading its lines' and its entries' element (lane & 3) of the step from global
+// memory (8 rows x 32 bytes per warp load), so a G element loaded once serves 32 entries.
+// A batch of at most 16 entries skips the upper entry tiles (warp-uniform).  Two
+// accumulator sets take alternate K steps and are added at the end, in a fixed order, so
+// the result is bitwise reproducible.  A term's galpha is then its (entry, line) slot.
+constexpr int AG_BATCH = 32;
+static_assert(SG_LINES == 16, "2 line tiles of 8");
 __device__ __forceinline__ void gram_dmma(double& c0, double& c1, double a, double b) {
     asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
         : "+d"(c0), "+d"(c1)
         : "d"(a), "d"(b));
+}
+
+template <int ET>  // entry tiles of 8
+__device__ __forceinline__ void gram_batch(DevSGroup const& Gr, uint32_t e0, uint32_t nb,
+                                           const uint64_t* __restrict__ ent_t, const double* __restrict__ G,
+                                           const double* __restrict__ T, double* __restrict__ gram, uint32_t g,
+                                           uint32_t q) {
+    const uint32_t n = Gr.rows * Gr.cols;
+    // this lane's rows of the A (lines g, 8 + g) and B (entries 8 j + g) fragments
+    const bool l0 = g < Gr.nlines, l1 = 8 + g < Gr.nlines;
+    const double* G0 = G + Gr.s_base + uint64_t(g) * Gr.line_stride;
+    const double* G1 = G0 + 8ull * Gr.line_stride;
+    const double* Tj[ET];
+    bool bj[ET];
+#pragma unroll
+    for (int j = 0; j < ET; ++j) {
+        bj[j] = uint32_t(8 * j) + g < nb;
+        Tj[j] = T + (bj[j] ? ent_t[e0 + 8 * j + g] : 0);
+    }
+    double acc[2][2][ET][2];  // [set][line tile][entry tile][pair]
+#pragma unroll
+    for (int s = 0; s < 2; ++s)
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < ET; ++j) acc[s][i][j][0] = acc[s][i][j][1] = 0.0;
+    // element e = 4 step + q of the lane, at (row r, column c) of the lines' cells
+    uint32_t e = q, c = q / max(Gr.rows, 1u), r = q - c * Gr.rows;
+    const uint32_t dc = 4u / max(Gr.rows, 1u), dr = 4u - dc * Gr.rows;
+    for (uint32_t st = 0; st * 4 < n; st += 2) {
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            const bool in = e < n;
+            const uint64_t go = r + uint64_t(c) * Gr.ld_s;
+            const double a0 = (in && l0) ? G0[go] : 0.0, a1 = (in && l1) ? G1[go] : 0.0;
+#pragma unroll
+            for (int j = 0; j < ET; ++j) {
+                const double t = (in && bj[j]) ? Tj[j][e] : 0.0;
+                gram_dmma(acc[s][0][j][0], acc[s][0][j][1], a0, t);
+                gram_dmma(acc[s][1][j][0], acc[s][1][j][1], a1, t);
+            }
+            e += 4;
+            r += dr;
+            c += dc;
+            if (r >= Gr.rows) {
+                r -= Gr.rows;
+                ++c;
+            }
+        }
+    }
+    // D tile (line tile i, entry tile j): line 8 i + g, entries 8 j + 2 q + h
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < ET; ++j)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const uint32_t ent = uint32_t(8 * j) + 2u * q + uint32_t(h);
+                if (ent < nb)
+                    gram[uint64_t(e0 + ent) * SG_LINES + uint32_t(8 * i) + g] = acc[0][i][j][h] + acc[1][i][j][h];
+            }
 }
 
 __global__ void __launch_bounds__(128) gram_groups(const DevSGroup* __restrict__ groups,
@@ -118,54 +180,11 @@ __global__ void __launch_bounds__(128) gram_groups(const DevSGroup* __restrict__
     for (uint32_t it = blockIdx.x * wpb + (threadIdx.x >> 5); it < n_items; it += gridDim.x * wpb) {
         const DevSItem I = items[it];
         const DevSGroup Gr = groups[I.group];
-        const uint32_t n = Gr.rows * Gr.cols, nb = min(uint32_t(AG_BATCH), Gr.ent_end - I.e0);
-        // this lane's rows of the A (lines g, 8 + g) and B (entries g, 8 + g) fragments
-        const bool l0 = g < Gr.nlines, l1 = 8 + g < Gr.nlines, b0 = g < nb, b1 = 8 + g < nb;
-        const double* G0 = G + Gr.s_base + uint64_t(g) * Gr.line_stride;
-        const double* G1 = G0 + 8ull * Gr.line_stride;
-        const double* T0 = T + (b0 ? ent_t[I.e0 + g] : 0);
-        const double* T1 = T + (b1 ? ent_t[I.e0 + 8 + g] : 0);
-        double acc[2][2][2][2];  // [set][line tile][entry tile][pair]
-#pragma unroll
-        for (int s = 0; s < 2; ++s)
-#pragma unroll
-            for (int i = 0; i < 2; ++i)
-#pragma unroll
-                for (int j = 0; j < 2; ++j) acc[s][i][j][0] = acc[s][i][j][1] = 0.0;
-        // element e = 4 step + q of the lane, at (row r, column c) of the lines' cells
-        uint32_t e = q, c = q / max(Gr.rows, 1u), r = q - c * Gr.rows;
-        const uint32_t dc = 4u / max(Gr.rows, 1u), dr = 4u - dc * Gr.rows;
-        for (uint32_t st = 0; st * 4 < n; st += 2) {
-#pragma unroll
-            for (int s = 0; s < 2; ++s) {
-                const bool in = e < n;
-                const uint64_t go = r + uint64_t(c) * Gr.ld_s;
-                const double a0 = (in && l0) ? G0[go] : 0.0, a1 = (in && l1) ? G1[go] : 0.0;
-                const double t0 = (in && b0) ? T0[e] : 0.0, t1 = (in && b1) ? T1[e] : 0.0;
-                gram_dmma(acc[s][0][0][0], acc[s][0][0][1], a0, t0);
-                gram_dmma(acc[s][0][1][0], acc[s][0][1][1], a0, t1);
-                gram_dmma(acc[s][1][0][0], acc[s][1][0][1], a1, t0);
-                gram_dmma(acc[s][1][1][0], acc[s][1][1][1], a1, t1);
-                e += 4;
-                r += dr;
-                c += dc;
-                if (r >= Gr.rows) {
-                    r -= Gr.rows;
-                    ++c;
-                }
-            }
-        }
-        // D tile (line tile i, entry tile j): line 8 i + g, entries 8 j + 2 q + h
-#pragma unroll
-        for (int i = 0; i < 2; ++i)
-#pragma unroll
-            for (int j = 0; j < 2; ++j)
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const uint32_t ent = uint32_t(8 * j) + 2u * q + uint32_t(h);
-                    if (ent < nb)
-                        gram[uint64_t(I.e0 + ent) * SG_LINES + uint32_t(8 * i) + g] = acc[0][i][j][h] + acc[1][i][j][h];
-                }
+        const uint32_t nb = min(uint32_t(AG_BATCH), Gr.ent_end - I.e0);
+        if (nb > 16)
+            gram_batch<4>(Gr, I.e0, nb, ent_t, G, T, gram, g, q);
+        else
+            gram_batch<2>(Gr, I.e0, nb, ent_t, G, T, gram, g, q);
     }
 }
 

@@ -385,8 +385,8 @@ __global__ void __launch_bounds__(256) sbuild_lines(const DevSLine* __restrict__
 // (SG_CHUNK + 4 doubles, 4 mod 16) puts the four sources of a K step in different
 // banks for the fragment loads.
 // Groups of up to 8 lines run as one launch (8 accumulated lines), larger groups as
-// another (SG_LINES lines); both with 2 stages and 3 CTAs (12 warps) per SM, the wide
-// launch's accumulators held in 168 registers.
+// another (SG_LINES lines); both with 2 stages and 3 CTAs (12 warps) per SM, which caps
+// the wide launch (its 128 x 16 accumulators included) at 168 registers.
 constexpr int SGB_WARPS = 4, SGB_NC = 8, SGB_ROW = SG_CHUNK + 4;
 template <int STAGES>
 struct alignas(16) SgbRing {

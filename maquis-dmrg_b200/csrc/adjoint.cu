@@ -414,6 +414,23 @@ std::string compile_adjoint(FlatPlan const& p, std::vector<uint64_t> const& stag
             }
         }
     }
+    // cell groups in the order of the first G line they read (their lines are listed in
+    // address order): groups of different T tasks that read the same G lines run side by
+    // side, so a line's chunk comes from DRAM once and from L2 for the others
+    {
+        std::vector<uint32_t> order(a.tgroups.size());
+        for (uint32_t i = 0; i < order.size(); ++i) order[i] = i;
+        auto first_g = [&](uint32_t gi) {
+            DevTGroup const& G = a.tgroups[gi];
+            return G.ent_end > G.ent_begin ? a.tg_g[G.ent_begin] : 0ull;
+        };
+        std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return first_g(x) < first_g(y); });
+        a.tg_items.clear();
+        for (uint32_t gi : order) {
+            const uint64_t n = uint64_t(a.tgroups[gi].rows) * a.tgroups[gi].cols;
+            for (uint64_t e0 = 0; e0 < n; e0 += 32 * SG_EPT) a.tg_items.push_back(DevSItem{gi, uint32_t(e0)});
+        }
+    }
 
     // ---- gx slices: sum over the slice's T tasks of gT_t R_t^T (transpose of stage 1) ----
     std::map<std::pair<uint32_t, uint32_t>, std::vector<uint32_t>> slices;  // (block, column) -> tasks

@@ -20,6 +20,13 @@ namespace dmrgb200 {
 
 namespace {
 
+// D (8 x 8, two values per lane) += A (8 x 4) * B (4 x 8) on the FP64 tensor cores
+__device__ __forceinline__ void dmma_f64(double& c0, double& c1, double a, double b) {
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+        : "+d"(c0), "+d"(c1)
+        : "d"(a), "d"(b));
+}
+
 // galpha: one warp per term, fixed-order lane sums and a butterfly reduction
 __global__ void __launch_bounds__(256) alpha_grad(const DevATerm* __restrict__ at, uint32_t n,
                                                   const double* __restrict__ G, const double* __restrict__ T,
@@ -104,11 +111,6 @@ __global__ void __launch_bounds__(256) tgrad_cells(const DevSLine* __restrict__ 
 // the result is bitwise reproducible.  A term's galpha is then its (entry, line) slot.
 constexpr int AG_BATCH = 32;
 static_assert(SG_LINES == 16, "2 line tiles of 8");
-__device__ __forceinline__ void gram_dmma(double& c0, double& c1, double a, double b) {
-    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-        : "+d"(c0), "+d"(c1)
-        : "d"(a), "d"(b));
-}
 
 template <int ET>  // entry tiles of 8
 __device__ __forceinline__ void gram_batch(DevSGroup const& Gr, uint32_t e0, uint32_t nb,
@@ -146,8 +148,8 @@ __device__ __forceinline__ void gram_batch(DevSGroup const& Gr, uint32_t e0, uin
 #pragma unroll
             for (int j = 0; j < ET; ++j) {
                 const double t = (in && bj[j]) ? Tj[j][e] : 0.0;
-                gram_dmma(acc[s][0][j][0], acc[s][0][j][1], a0, t);
-                gram_dmma(acc[s][1][j][0], acc[s][1][j][1], a1, t);
+                dmma_f64(acc[s][0][j][0], acc[s][0][j][1], a0, t);
+                dmma_f64(acc[s][1][j][0], acc[s][1][j][1], a1, t);
             }
             e += 4;
             r += dr;
@@ -242,10 +244,7 @@ __global__ void __launch_bounds__(256) tgrad_groups(const DevTGroup* __restrict_
                 const double bk = b;
                 line(k0 + 4, gk, ld, b);
 #pragma unroll
-                for (int i = 0; i < MT; ++i)
-                    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-                        : "+d"(acc[i][0]), "+d"(acc[i][1])
-                        : "d"(a[i]), "d"(bk));
+                for (int i = 0; i < MT; ++i) dmma_f64(acc[i][0], acc[i][1], a[i], bk);
             }
             // D tile i: element eb + 8 i + g, cells 2 q + h
 #pragma unroll
